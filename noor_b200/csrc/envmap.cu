@@ -1,0 +1,184 @@
+// Environment importance-sampling distribution (FP64 prefix sums on the
+// GPU) and the FP64 Hosek-Wilkie coefficient fit.
+//
+// The distribution is PBRT-v3's piecewise-constant Distribution2D over the
+// full environment resolution: func = luminance x sin(theta) per cell, each
+// row a conditional CDF, the row integrals a marginal CDF.  The reference
+// builds an FP32 Blelloch scan over a grid clamped to 1024 x 1024 whose
+// sampling reads one entry past each CDF (noor/cuda/distribution2d.cuh:
+// 63-228, 326-336); this build uses the whole map and the standard n-entry
+// search.  The pdf conversion to solid angle is the reference's
+// (skydome.cuh:138, lightimp.cuh:162-173).
+#include "kernels.h"
+#include "shading.cuh"
+
+namespace nb {
+
+constexpr int kScanThreads = 256;
+
+__global__ void k_env_func_tex(const float4* env, int w, int h, float* func) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= w * h) return;
+    const int row = i / w;
+    const float st = sinf(((float)row + 0.5f) / (float)h * kPi);
+    const float4 t = env[i];
+    func[i] = fmaxf(0.0f, rgb2y(f3(t))) * st;
+}
+
+__global__ void k_env_func_sky(DevHosek H, int w, int h, float* func) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= w * h) return;
+    const int row = i / w, col = i % w;
+    float acc = 0.0f;
+    for (int b = 0; b < 4; ++b) {
+        const float v = ((float)row + ((float)b + 0.5f) * 0.25f) / (float)h;
+        const float theta = v * kPi;
+        const float st = sinf(theta), ct = cosf(theta);
+        for (int a = 0; a < 4; ++a) {
+            const float u = ((float)col + ((float)a + 0.5f) * 0.25f) / (float)w;
+            const float phi = u * k2Pi;
+            const float3 dir = normalize_fast(f3(st * cosf(phi), ct, st * sinf(phi)));
+            acc += fmaxf(0.0f, rgb2y(hosek_query(H, dir))) * st;
+        }
+    }
+    func[i] = acc * (1.0f / 16.0f);
+}
+
+// Inclusive FP64 block scan of kScanThreads values (Hillis-Steele in smem).
+__device__ double block_scan_incl(double v, double* sh) {
+    const int t = threadIdx.x;
+    sh[t] = v;
+    __syncthreads();
+    for (int off = 1; off < kScanThreads; off <<= 1) {
+        const double add = t >= off ? sh[t - off] : 0.0;
+        __syncthreads();
+        sh[t] += add;
+        __syncthreads();
+    }
+    const double r = sh[t];
+    __syncthreads();
+    return r;
+}
+
+// Prefix sums of one row of n values (FP32 in, FP64 accumulate):
+// out[0] = 0, out[i+1] = out[i] + in[i] / n.  Each thread owns a contiguous
+// segment; segment totals are scanned across the block.  Returns the total.
+__device__ double row_prefix(const float* in, const double* in_d, int n, double* out, double* sh) {
+    const int t = threadIdx.x;
+    const int seg = (n + kScanThreads - 1) / kScanThreads;
+    const int b = t * seg, e = min(b + seg, n);
+    const double inv_n = 1.0 / (double)n;
+    double local = 0.0;
+    for (int i = b; i < e; ++i) local += (in ? (double)in[i] : in_d[i]) * inv_n;
+    const double incl = block_scan_incl(local, sh);
+    double run = incl - local;
+    for (int i = b; i < e; ++i) {
+        out[i] = run;
+        run += (in ? (double)in[i] : in_d[i]) * inv_n;
+    }
+    __shared__ double total;
+    if (t == kScanThreads - 1) {
+        total = incl;
+        out[n] = incl;
+    }
+    __syncthreads();
+    return total;
+}
+
+// one block per row: conditional CDF of the row, row integral
+__global__ void __launch_bounds__(kScanThreads) k_row_cdf(const float* func, int w, int h, float* cdf,
+                                                          float* row_int, double* scratch) {
+    __shared__ double sh[kScanThreads];
+    const int row = blockIdx.x;
+    double* cd = scratch + (size_t)row * (w + 1);
+    const double total = row_prefix(func + (size_t)row * w, nullptr, w, cd, sh);
+    float* c = cdf + (size_t)row * (w + 1);
+    for (int i = threadIdx.x; i <= w; i += kScanThreads)
+        c[i] = total > 0.0 ? (float)(cd[i] / total) : (float)((double)i / (double)w);
+    if (threadIdx.x == 0) {
+        row_int[row] = (float)total;
+        scratch[(size_t)h * (w + 1) + row] = total;
+    }
+}
+
+// single block: marginal CDF over the row integrals
+__global__ void __launch_bounds__(kScanThreads) k_marg_cdf(int w, int h, float* marg_cdf, double* scratch,
+                                                           float* marg_int_out) {
+    __shared__ double sh[kScanThreads];
+    const double* rows = scratch + (size_t)h * (w + 1);
+    double* cd = scratch + (size_t)h * (w + 1) + h;
+    // the row integrals are stored as float in row_int; sample with the
+    // float values so pdf(sample) == func / integral exactly in FP32
+    const double total = row_prefix(nullptr, rows, h, cd, sh);
+    for (int i = threadIdx.x; i <= h; i += kScanThreads)
+        marg_cdf[i] = total > 0.0 ? (float)(cd[i] / total) : (float)((double)i / (double)h);
+    if (threadIdx.x == 0) *marg_int_out = (float)total;
+}
+
+cudaError_t launch_env_func_from_texture(const float4* env, int w, int h, float* func, cudaStream_t s) {
+    const int n = w * h;
+    k_env_func_tex<<<(n + 255) / 256, 256, 0, s>>>(env, w, h, func);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_env_func_from_sky(const DevHosek& H, int w, int h, float* func, cudaStream_t s) {
+    const int n = w * h;
+    k_env_func_sky<<<(n + 255) / 256, 256, 0, s>>>(H, w, h, func);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_env_cdf(const EnvBuild& b, cudaStream_t s) {
+    k_row_cdf<<<b.h, kScanThreads, 0, s>>>(b.func, b.w, b.h, b.cdf, b.row_int, b.scratch);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_marg_cdf<<<1, kScanThreads, 0, s>>>(b.w, b.h, b.marg_cdf, b.scratch, b.marg_int_out);
+    return cudaGetLastError();
+}
+
+// --------------------------------------------------------------- Hosek fit
+// Restatement of the published Hosek-Wilkie fit (ArHosekSkyModel.cpp:
+// 147-289): each coefficient is a quintic Bezier in elevation^(1/3), blended
+// linearly over ground albedo (2 tables) and turbidity (10 tables).  One
+// thread per (state, channel, value); value 9 is the radiance scale.
+__device__ double bezier5(const float* m, int stride, double se) {
+    const double a = 1.0 - se;
+    return a * a * a * a * a * (double)m[0] + 5.0 * a * a * a * a * se * (double)m[stride] +
+           10.0 * a * a * a * se * se * (double)m[2 * stride] + 10.0 * a * a * se * se * se * (double)m[3 * stride] +
+           5.0 * a * se * se * se * se * (double)m[4 * stride] + se * se * se * se * se * (double)m[5 * stride];
+}
+
+__global__ void k_hosek_fit(const float* dataset, double turbidity, double a0, double a1, double a2, double elevation,
+                            float* out) {
+    const int tid = threadIdx.x;  // 0..89
+    if (tid >= 90) return;
+    const int state = tid / 30, rem = tid % 30, channel = rem / 10, value = rem % 10;
+    const double albedo = state == 0 ? a0 : (state == 1 ? a1 : a2);
+    const int it = (int)turbidity;
+    const double tr = turbidity - (double)it;
+    const double se = pow(elevation / (3.141592653589793 / 2.0), 1.0 / 3.0);
+    double r;
+    if (value < 9) {
+        const float* ds = dataset + channel * 1080;
+        const int i = value;
+        r = (1.0 - albedo) * (1.0 - tr) * bezier5(ds + 54 * (it - 1) + i, 9, se) +
+            albedo * (1.0 - tr) * bezier5(ds + 540 + 54 * (it - 1) + i, 9, se);
+        if (it != 10)
+            r += (1.0 - albedo) * tr * bezier5(ds + 54 * it + i, 9, se) + albedo * tr * bezier5(ds + 540 + 54 * it + i, 9, se);
+        out[state * 30 + channel * 9 + value] = (float)r;
+    } else {
+        const float* ds = dataset + 3 * 1080 + channel * 120;
+        r = (1.0 - albedo) * (1.0 - tr) * bezier5(ds + 6 * (it - 1), 1, se) +
+            albedo * (1.0 - tr) * bezier5(ds + 60 + 6 * (it - 1), 1, se);
+        if (it != 10)
+            r += (1.0 - albedo) * tr * bezier5(ds + 6 * it, 1, se) + albedo * tr * bezier5(ds + 60 + 6 * it, 1, se);
+        out[state * 30 + 27 + channel] = (float)r;
+    }
+}
+
+cudaError_t launch_hosek_fit(const float* dataset, double turbidity, const double* albedo3, double elevation,
+                             float* out, cudaStream_t s) {
+    k_hosek_fit<<<1, 96, 0, s>>>(dataset, turbidity, albedo3[0], albedo3[1], albedo3[2], elevation, out);
+    return cudaGetLastError();
+}
+
+}  // namespace nb

@@ -1,0 +1,132 @@
+// Device-resident scene: every array the render path reads, in the layouts
+// chosen for B200 (one 32-byte sector per BVH node, 64-byte triangle records
+// whose first sector holds everything the t-range test needs).
+#pragma once
+#include "dmath.cuh"
+#include "../../include/noor_b200.h"
+
+namespace nb {
+
+// One BVH node = 32 B: [0] = min.xyz | right/start/child-root,
+// [1] = max.xyz | flags+count/axis/instance/light.  Same words as the
+// reference's two uint4 arrays (noor/cuda/mesh.cuh:43-45), interleaved so one
+// node is one aligned sector.
+struct __align__(32) DevNode {
+    uint4 lo;
+    uint4 hi;
+};
+
+// Reference-Wald triangle = 64 B: the two records the t-range test reads
+// (ax,nu,nv,nd | cnu,cnv,deg,mat) share the first sector, the barycentric
+// record and the attribute indices (v0,v1,v2,material) the second.
+struct __align__(64) DevWaldTri {
+    uint4 ax_nu_nv_nd;
+    uint4 cnu_cnv_deg_mat;
+    uint4 bnu_bnv_au_av;
+    uint4 attr;
+};
+
+// Watertight triangle = 64 B: object-space vertices (v0.w = material type
+// bits) and the attribute indices.
+struct __align__(64) DevWtTri {
+    float4 v0;
+    float4 v1;
+    float4 v2;
+    uint4 attr;
+};
+
+// Per instance: world->object, object->world and normal rows (9 x float4).
+struct DevXform {
+    float4 w2o[3];
+    float4 o2w[3];
+    float4 nrm[3];
+};
+
+// Constant material parameters resolved from the 1x1 textures at load.
+struct __align__(16) DevMaterial {
+    float3 diffuse;
+    uint32_t type;
+    float3 specular;
+    uint32_t distribution;
+    float3 transmission;
+    float coat_ior;
+    float3 emittance;
+    float emitter_scale;
+    float3 ior;
+    float rough_x;
+    float3 k;
+    float rough_y;
+};
+
+struct DevAreaLight {
+    float3 center;
+    float area;
+    float3 u;
+    int two_sided;
+    float3 v;
+    int type;
+    float3 n;
+    float pad;
+    float3 ke;
+    float pad2;
+};
+
+struct DevHosek {
+    float configs[3][9];  // channel c uses state c's configs[c]
+    float radiance[3];
+    float3 solar_dir;
+    float solar_scale;
+    float solar_radius;
+};
+
+struct DevCamera {
+    float4 c2w[3];
+    float4 r2c[3];
+    uint32_t w, h, center, pad;
+};
+
+// Piecewise-constant 2D distribution over the environment (row = theta).
+struct DevDist2D {
+    const float* func;      // h * w
+    const float* cdf;       // h * (w + 1)
+    const float* row_int;   // h   (integral of each row's func)
+    const float* marg_cdf;  // h + 1
+    float marg_int;         // integral of row_int
+    int w, h;
+};
+
+struct DevScene {
+    const DevNode* nodes;
+    const DevWaldTri* wald;
+    const DevWtTri* wtri;
+    const float4* vertices;
+    const float4* normals;
+    const float2* uvs;
+    const DevXform* xforms;
+    const DevMaterial* materials;
+    const DevAreaLight* area_lights;
+    const float4* env;      // env texels (HDR / baked sky / constant), w*h
+    uint32_t num_nodes;
+    uint32_t num_tris;
+    uint32_t num_instances;
+    uint32_t num_materials;
+    int num_area_lights;
+    int num_lights;         // area lights + infinite light
+    int env_w, env_h;
+    DevDist2D dist;
+    DevHosek hosek;
+    // spec
+    float bias;
+    float world_radius;
+    uint32_t root;
+    uint32_t bounces;
+    uint32_t rr;
+    uint32_t mis;
+    uint32_t sky_on;
+    int sky_type;
+    uint32_t isect;
+    uint32_t film_mode;
+    int stack_cap;
+};
+
+}  // namespace nb

@@ -1,0 +1,661 @@
+// Device shading routines of the render path: RNG, camera, local shading
+// frame, BxDF lobes, Fresnel, microfacet distributions, Hosek-Wilkie sky,
+// environment texture and its piecewise-constant 2D distribution.
+// Each routine states the reference routine it follows.
+#pragma once
+#include "traverse.cuh"
+
+namespace nb {
+
+constexpr float kInf = __builtin_huge_valf();
+
+// ------------------------------------------------------------------- RNG
+// TEA<16> seed of (pixel, frame) and the 24-bit LCG of noor/cuda/rng.cuh:37-76
+NB_HD uint32_t tea16(uint32_t v0, uint32_t v1) {
+    uint32_t s0 = 0;
+    for (int n = 0; n < 16; n++) {
+        s0 += 0x9e3779b9u;
+        v0 += ((v1 << 4) + 0xa341316cu) ^ (v1 + s0) ^ ((v1 >> 5) + 0xc8013ea4u);
+        v1 += ((v0 << 4) + 0xad90777du) ^ (v0 + s0) ^ ((v0 >> 5) + 0x7e95761eu);
+    }
+    return v0;
+}
+
+struct Rng {
+    uint32_t s;
+    NB_HD float next() {
+        s = 1664525u * s + 1013904223u;
+        return (float)(s & 0x00FFFFFFu) / (float)0x01000000;
+    }
+};
+
+// ---------------------------------------------------------------- camera
+// CudaPerspCamera::generateRay (noor/cuda/cameraimp.cuh:182-228), pinhole
+NB_D void camera_ray(const DevCamera& C, uint32_t x, uint32_t y, Rng& rng, float3& o, float3& d) {
+    const float rx = (float)x + rng.next() - 0.5f;
+    const float ry = (float)y + rng.next() - 0.5f;
+    const float3 pc = f3(C.r2c[0].w + (C.r2c[0].x * rx + C.r2c[0].y * ry + C.r2c[0].z * 0.0f),
+                         C.r2c[1].w + (C.r2c[1].x * rx + C.r2c[1].y * ry + C.r2c[1].z * 0.0f),
+                         C.r2c[2].w + (C.r2c[2].x * rx + C.r2c[2].y * ry + C.r2c[2].z * 0.0f));
+    const float3 dc = normalize_fast(pc);
+    o = f3(C.c2w[0].w, C.c2w[1].w, C.c2w[2].w);
+    const float3 dw = f3(C.c2w[0].x * dc.x + C.c2w[0].y * dc.y + C.c2w[0].z * dc.z,
+                         C.c2w[1].x * dc.x + C.c2w[1].y * dc.y + C.c2w[1].z * dc.z,
+                         C.c2w[2].x * dc.x + C.c2w[2].y * dc.y + C.c2w[2].z * dc.z);
+    d = normalize_fast(dw);
+}
+
+// ------------------------------------------------------------ utilities
+NB_D float rgb2y(const float3& c) { return dot(c, f3(0.2126f, 0.7152f, 0.0722f)); }
+NB_D float power_heuristic(float f, float g) { return (f * f) / (f * f + g * g); }
+NB_D bool isinf_f(float v) { return isinf(v); }
+
+// coordinateSystem, noor/cuda/utils.cuh:340-347
+NB_D void coordinate_system(const float3& v1, float3& v2, float3& v3) {
+    if (fabsf(v1.x) > fabsf(v1.y))
+        v2 = f3(-v1.z, 0.0f, v1.x) / sqrtf(v1.x * v1.x + v1.z * v1.z);
+    else
+        v2 = f3(0.0f, v1.z, -v1.y) / sqrtf(v1.y * v1.y + v1.z * v1.z);
+    v3 = cross(v1, v2);
+}
+
+// concentricSampleDisk / cosineSampleHemisphere (utils.cuh:377-404)
+NB_D float2 concentric_disk(float ux, float uy) {
+    const float ox = 2.0f * ux - 1.0f, oy = 2.0f * uy - 1.0f;
+    if (ox == 0.0f && oy == 0.0f) return f2(0.0f, 0.0f);
+    float theta, r;
+    if (fabsf(ox) > fabsf(oy)) {
+        r = ox;
+        theta = kPiOver4 * (oy / ox);
+    } else {
+        r = oy;
+        theta = kPiOver2 - kPiOver4 * (ox / oy);
+    }
+    return f2(r * cosf(theta), r * sinf(theta));
+}
+NB_D float3 cosine_hemisphere(float ux, float uy) {
+    const float2 d = concentric_disk(ux, uy);
+    const float z = sqrtf(fmaxf(0.0f, 1.0f - d.x * d.x - d.y * d.y));
+    return f3(d.x, d.y, z);
+}
+
+NB_D float spherical_phi(const float3& v) {
+    const float p = atan2f(v.z, v.x);
+    return (p < 0.0f) ? (p + k2Pi) : p;
+}
+NB_D float spherical_theta(const float3& v) { return acosf(clampf(v.y, -1.0f, 1.0f)); }
+
+// ----------------------------------------------------------- shading frame
+struct Frame {
+    float3 n;   // shading normal
+    float3 s;   // dpdu after Gram-Schmidt
+    float3 t;   // dpdv
+    float3 ng;  // geometric normal
+};
+NB_D float3 to_local(const Frame& F, const float3& v) { return f3(dot(v, F.s), dot(v, F.t), dot(v, F.n)); }
+NB_D float3 to_world(const Frame& F, const float3& v) { return v.x * F.s + v.y * F.t + v.z * F.n; }
+
+// CudaIntersection::computeTangentSpace (noor/cuda/intersection.cuh:325-377)
+// without the ray-differential part (only texture LOD and bump use it).
+NB_D Frame tangent_frame(const DevScene& S, const uint4& attr, uint32_t ins, float bu, float bv,
+                         const float4* tri_verts /* 3 object-space vertices or null */) {
+    const DevXform* X = S.xforms + ins;
+    float2 uv0 = __ldg(&S.uvs[attr.x]), uv1 = __ldg(&S.uvs[attr.y]), uv2 = __ldg(&S.uvs[attr.z]);
+    uv0.y = 1.0f - uv0.y;
+    uv1.y = 1.0f - uv1.y;
+    uv2.y = 1.0f - uv2.y;
+    float3 v0, v1, v2;
+    if (tri_verts) {
+        v0 = f3(tri_verts[0]);
+        v1 = f3(tri_verts[1]);
+        v2 = f3(tri_verts[2]);
+    } else {
+        v0 = f3(__ldg(&S.vertices[attr.x]));
+        v1 = f3(__ldg(&S.vertices[attr.y]));
+        v2 = f3(__ldg(&S.vertices[attr.z]));
+    }
+    const float3 n0 = f3(__ldg(&S.normals[attr.x]));
+    const float3 n1 = f3(__ldg(&S.normals[attr.y]));
+    const float3 n2 = f3(__ldg(&S.normals[attr.z]));
+    const float4 N0 = __ldg(&X->nrm[0]), N1 = __ldg(&X->nrm[1]), N2 = __ldg(&X->nrm[2]);
+    const float w = 1.0f - bu - bv;
+    const float3 ni = w * n0 + bu * n1 + bv * n2;
+    const float3 nt = f3(N0.x * ni.x + N0.y * ni.y + N0.z * ni.z, N1.x * ni.x + N1.y * ni.y + N1.z * ni.z,
+                         N2.x * ni.x + N2.y * ni.y + N2.z * ni.z);
+    Frame F;
+    F.n = normalize_guard(normalize_fast(nt));
+    const float4 S0 = __ldg(&X->o2w[0]), S1 = __ldg(&X->o2w[1]), S2 = __ldg(&X->o2w[2]);
+    const float3 e1 = v1 - v0, e2 = v2 - v0;
+    const float3 dp01 = f3(S0.x * e1.x + S0.y * e1.y + S0.z * e1.z, S1.x * e1.x + S1.y * e1.y + S1.z * e1.z,
+                           S2.x * e1.x + S2.y * e1.y + S2.z * e1.z);
+    const float3 dp02 = f3(S0.x * e2.x + S0.y * e2.y + S0.z * e2.z, S1.x * e2.x + S1.y * e2.y + S1.z * e2.z,
+                           S2.x * e2.x + S2.y * e2.y + S2.z * e2.z);
+    F.ng = normalize_guard(cross(dp01, dp02));
+    const float2 d1 = f2(uv1.x - uv0.x, uv1.y - uv0.y);
+    const float2 d2 = f2(uv2.x - uv0.x, uv2.y - uv0.y);
+    const float det = d1.x * d2.y - d2.x * d1.y;
+    float3 dpdu, dpdv;
+    if (!(fabsf(det) < 1e-8f)) {
+        const float inv = 1.0f / det;
+        const float a00 = d2.y * inv, a01 = -d1.y * inv, a10 = -d2.x * inv, a11 = d1.x * inv;
+        dpdu = a00 * dp01 + a01 * dp02;
+        dpdv = a10 * dp01 + a11 * dp02;
+        if (length2(cross(dpdu, dpdv)) == 0.0f) coordinate_system(F.ng, dpdu, dpdv);
+    } else {
+        coordinate_system(F.ng, dpdu, dpdv);
+    }
+    F.s = normalize_guard(dpdu - F.n * dot(F.n, dpdu));
+    const float sign = dot(cross(F.n, F.s), dpdv) < 0.0f ? -1.0f : 1.0f;
+    F.t = normalize_guard(sign * cross(F.n, F.s));
+    return F;
+}
+
+// -------------------------------------------------- spherical trig helpers
+// (noor/cuda/bxdf.cuh:58-96), on local-frame vectors
+NB_D float cos2t(const float3& w) { return w.z * w.z; }
+NB_D float sin2t(const float3& w) { return fmaxf(0.0f, 1.0f - cos2t(w)); }
+NB_D float sint(const float3& w) { return sqrtf(sin2t(w)); }
+NB_D float tant(const float3& w) { return sint(w) / w.z; }
+NB_D float tan2t(const float3& w) { return sin2t(w) / cos2t(w); }
+NB_D float cosphi(const float3& w) {
+    const float s = sint(w);
+    return (s == 0.0f) ? 1.0f : clampf(w.x / s, -1.0f, 1.0f);
+}
+NB_D float sinphi(const float3& w) {
+    const float s = sint(w);
+    return (s == 0.0f) ? 0.0f : clampf(w.y / s, -1.0f, 1.0f);
+}
+NB_D float cos2phi(const float3& w) { return cosphi(w) * cosphi(w); }
+NB_D float sin2phi(const float3& w) { return sinphi(w) * sinphi(w); }
+NB_D bool same_hemi(const float3& a, const float3& b) { return a.z * b.z > 0.0f; }
+
+// ---------------------------------------------------------------- Fresnel
+// fresnelDielectric (noor/cuda/fresnel.cuh:58-80)
+NB_D float fresnel_dielectric(float cosI, float etaI, float etaT) {
+    cosI = clampf(cosI, -1.0f, 1.0f);
+    if (!(cosI > 0.0f)) {
+        const float tmp = etaI;
+        etaI = etaT;
+        etaT = tmp;
+        cosI = fabsf(cosI);
+    }
+    const float sinI = sqrtf(fmaxf(0.0f, 1.0f - cosI * cosI));
+    const float sinT = etaI / etaT * sinI;
+    if (sinT >= 1.0f) return 1.0f;
+    const float cosT = sqrtf(fmaxf(0.0f, 1.0f - sinT * sinT));
+    const float rpar = ((etaT * cosI) - (etaI * cosT)) / ((etaT * cosI) + (etaI * cosT));
+    const float rper = ((etaI * cosI) - (etaT * cosT)) / ((etaI * cosI) + (etaT * cosT));
+    return (rpar * rpar + rper * rper) / 2.0f;
+}
+NB_D float3 sqrt3(const float3& v) { return f3(sqrtf(v.x), sqrtf(v.y), sqrtf(v.z)); }
+// fresnelConductor with etaI = 1 (noor/cuda/fresnel.cuh:81-107)
+NB_D float3 fresnel_conductor(float cosI, const float3& etaT, const float3& k) {
+    cosI = clampf(cosI, -1.0f, 1.0f);
+    const float3 eta = etaT / f3(1.0f);
+    const float3 etak = k / f3(1.0f);
+    const float c2 = cosI * cosI;
+    const float s2 = 1.0f - c2;
+    const float3 eta2 = eta * eta;
+    const float3 etak2 = etak * etak;
+    const float3 t0 = eta2 - etak2 - f3(s2);
+    const float3 a2b2 = sqrt3(t0 * t0 + 4.0f * eta2 * etak2);
+    const float3 t1 = a2b2 + f3(c2);
+    const float3 a = sqrt3(0.5f * (a2b2 + t0));
+    const float3 t2 = 2.0f * cosI * a;
+    const float3 Rs = (t1 - t2) / (t1 + t2);
+    const float3 t3 = c2 * a2b2 + f3(s2 * s2);
+    const float3 t4 = t2 * s2;
+    const float3 Rp = Rs * (t3 - t4) / (t3 + t4);
+    return 0.5f * (Rp + Rs);
+}
+
+// ---------------------------------------------- Trowbridge-Reitz (GGX)
+// CudaTrowbridgeReitz (noor/cuda/distribution.cuh:58-183)
+NB_D float ggx_D(const float3& wh, float ax, float ay) {
+    const float t2 = tan2t(wh);
+    if (isinf(t2)) return 0.0f;
+    const float c4 = cos2t(wh) * cos2t(wh);
+    const float e = (cos2phi(wh) / (ax * ax) + sin2phi(wh) / (ay * ay)) * t2;
+    return 1.0f / (kPi * ax * ay * c4 * (1.0f + e) * (1.0f + e));
+}
+NB_D float ggx_lambda(const float3& w, float ax, float ay) {
+    const float at = fabsf(tant(w));
+    if (isinf(at)) return 0.0f;
+    const float alpha = sqrtf(cos2phi(w) * ax * ax + sin2phi(w) * ay * ay);
+    const float a2t2 = (alpha * at) * (alpha * at);
+    return (-1.0f + sqrtf(1.0f + a2t2)) / 2.0f;
+}
+NB_D void ggx_sample11(float cosT, float U1, float U2, float& sx, float& sy) {
+    if (cosT > .9999f) {
+        const float r = sqrtf(U1 / (1.0f - U1));
+        const float phi = 6.28318530718f * U2;
+        sx = r * cosf(phi);
+        sy = r * sinf(phi);
+        return;
+    }
+    const float sinT = sqrtf(fmaxf(0.0f, 1.0f - cosT * cosT));
+    const float tanT = sinT / cosT;
+    const float a = 1.0f / tanT;
+    const float G1 = 2.0f / (1.0f + sqrtf(1.0f + 1.0f / (a * a)));
+    const float A = 2.0f * U1 / G1 - 1.0f;
+    float tmp = 1.0f / (A * A - 1.0f);
+    if (tmp > 1e10f) tmp = 1e10f;
+    const float B = tanT;
+    const float D = sqrtf(fmaxf(B * B * tmp * tmp - (A * A - B * B) * tmp, 0.0f));
+    const float sx1 = B * tmp - D;
+    const float sx2 = B * tmp + D;
+    sx = (A < 0.0f || sx2 > 1.0f / tanT) ? sx1 : sx2;
+    float S;
+    if (U2 > 0.5f) {
+        S = 1.0f;
+        U2 = 2.0f * (U2 - .5f);
+    } else {
+        S = -1.0f;
+        U2 = 2.0f * (.5f - U2);
+    }
+    const float z = (U2 * (U2 * (U2 * 0.27385f - 0.73369f) + 0.46341f)) /
+                    (U2 * (U2 * (U2 * 0.093073f + 0.309420f) - 1.000000f) + 0.597999f);
+    sy = S * z * sqrtf(1.0f + sx * sx);
+}
+
+// ------------------------------------------------------------- Beckmann
+// Erf (Abramowitz & Stegun 7.1.26) and ErfInv (Giles 2010 single-precision
+// polynomial), the two approximations noor/cuda/utils.cuh:487-539 uses
+NB_D float erf_as(float x) {
+    const float a1 = 0.254829592f, a2 = -0.284496736f, a3 = 1.421413741f, a4 = -1.453152027f,
+                a5 = 1.061405429f, p = 0.3275911f;
+    const int sign = x < 0.0f ? -1 : 1;
+    x = fabsf(x);
+    const float t = 1.0f / (1.0f + p * x);
+    const float y = 1.0f - (((((a5 * t + a4) * t) + a3) * t + a2) * t + a1) * t * expf(-x * x);
+    return sign * y;
+}
+NB_D float erfinv_giles(float x) {
+    float w, p;
+    x = clampf(x, -.99999f, .99999f);
+    w = -logf((1.0f - x) * (1.0f + x));
+    if (w < 5.0f) {
+        w = w - 2.5f;
+        p = 2.81022636e-08f;
+        p = 3.43273939e-07f + p * w;
+        p = -3.5233877e-06f + p * w;
+        p = -4.39150654e-06f + p * w;
+        p = 0.00021858087f + p * w;
+        p = -0.00125372503f + p * w;
+        p = -0.00417768164f + p * w;
+        p = 0.246640727f + p * w;
+        p = 1.50140941f + p * w;
+    } else {
+        w = sqrtf(w) - 3.0f;
+        p = -0.000200214257f;
+        p = 0.000100950558f + p * w;
+        p = 0.00134934322f + p * w;
+        p = -0.00367342844f + p * w;
+        p = 0.00573950773f + p * w;
+        p = -0.0076224613f + p * w;
+        p = 0.00943887047f + p * w;
+        p = 1.00167406f + p * w;
+        p = 2.83297682f + p * w;
+    }
+    return p * x;
+}
+// CudaBeckmannDistribution (noor/cuda/distribution.cuh:185-342)
+NB_D float beck_D(const float3& wh, float ax, float ay) {
+    const float t2 = tan2t(wh);
+    if (isinf(t2)) return 0.0f;
+    const float c4 = cos2t(wh) * cos2t(wh);
+    return expf(-t2 * (cos2phi(wh) / (ax * ax) + sin2phi(wh) / (ay * ay))) / (kPi * ax * ay * c4);
+}
+NB_D float beck_lambda(const float3& w, float ax, float ay) {
+    const float at = fabsf(tant(w));
+    if (isinf(at)) return 0.0f;
+    const float alpha = sqrtf(cos2phi(w) * ax * ax + sin2phi(w) * ay * ay);
+    const float a = 1.0f / (alpha * at);
+    if (a >= 1.6f) return 0.0f;
+    return (1.0f - 1.259f * a + 0.396f * a * a) / (3.535f * a + 2.181f * a * a);
+}
+NB_D void beck_sample11(float cosI, float U1, float U2, float& sx, float& sy) {
+    if (cosI > .9999f) {
+        const float r = sqrtf(-logf(1.0f - U1));
+        const float sp = sinf(2.0f * kPi * U2);
+        const float cp = cosf(2.0f * kPi * U2);
+        sx = r * cp;
+        sy = r * sp;
+        return;
+    }
+    const float sinI = sqrtf(fmaxf(0.0f, 1.0f - cosI * cosI));
+    const float tanI = sinI / cosI;
+    const float cotI = 1.0f / tanI;
+    float a = -1.0f;
+    float c = erf_as(cotI);
+    const float sample_x = fmaxf(U1, 1e-6f);
+    const float thetaI = acosf(cosI);
+    const float fit = 1.0f + thetaI * (-0.876f + thetaI * (0.4265f - 0.0594f * thetaI));
+    float b = c - (1.0f + c) * powf(1.0f - sample_x, fit);
+    const float norm = 1.0f / (1.0f + c + sqrtf(kInvPi) * tanI * expf(-cotI * cotI));
+    int it = 0;
+    while (++it < 10) {
+        if (!(b >= a && b <= c)) b = 0.5f * (a + c);
+        const float ie = erfinv_giles(b);
+        const float value = norm * (1.0f + b + sqrtf(kInvPi) * tanI * expf(-ie * ie)) - sample_x;
+        const float deriv = norm * (1.0f - ie * tanI);
+        if (fabsf(value) < 1e-5f) break;
+        if (value > 0.0f)
+            c = b;
+        else
+            a = b;
+        b -= value / deriv;
+    }
+    sx = erfinv_giles(b);
+    sy = erfinv_giles(2.0f * fmaxf(U2, 1e-6f) - 1.0f);
+}
+
+// microfacet distribution dispatch: dist 0 = Trowbridge-Reitz, 1 = Beckmann
+struct Micro {
+    float ax, ay;
+    uint32_t dist;
+    NB_D float D(const float3& wh) const { return dist ? beck_D(wh, ax, ay) : ggx_D(wh, ax, ay); }
+    NB_D float lambda(const float3& w) const { return dist ? beck_lambda(w, ax, ay) : ggx_lambda(w, ax, ay); }
+    NB_D float G(const float3& wo, const float3& wi) const { return 1.0f / (1.0f + lambda(wo) + lambda(wi)); }
+    NB_D float G1(const float3& w) const { return 1.0f / (1.0f + lambda(w)); }
+    NB_D float pdf(const float3& wo, const float3& wh) const { return D(wh) * G1(wo) * absdot(wo, wh) / fabsf(wo.z); }
+    NB_D float3 sample_visible(const float3& wi, float U1, float U2) const {
+        const float3 ws = normalize_fast(f3(ax * wi.x, ay * wi.y, wi.z));
+        float sx, sy;
+        if (dist)
+            beck_sample11(ws.z, U1, U2, sx, sy);
+        else
+            ggx_sample11(ws.z, U1, U2, sx, sy);
+        const float tmp = cosphi(ws) * sx - sinphi(ws) * sy;
+        sy = sinphi(ws) * sx + cosphi(ws) * sy;
+        sx = tmp;
+        sx *= ax;
+        sy *= ay;
+        return normalize_fast(f3(-sx, -sy, 1.0f));
+    }
+    // Sample_wh: TR flips by sign(wo.z) (distribution.cuh:104-107), Beckmann by
+    // wo.z < 0 (distribution.cuh:222-229)
+    NB_D float3 sample_wh(const float3& wo, float u1, float u2) const {
+        if (dist) {
+            const bool flip = wo.z < 0.0f;
+            float3 wh = sample_visible(flip ? -1.0f * wo : wo, u1, u2);
+            return flip ? -1.0f * wh : wh;
+        }
+        const float s = signf_ref(wo.z);
+        return s * sample_visible(s * wo, u1, u2);
+    }
+};
+
+NB_D Micro make_micro(const DevMaterial& m) {
+    Micro mf;
+    mf.ax = fmaxf(m.rough_x * m.rough_x, 1e-3f);
+    mf.ay = fmaxf(m.rough_y * m.rough_y, 1e-3f);
+    mf.dist = m.distribution;
+    return mf;
+}
+
+// -------------------------------------------------------------- lobes
+// BxDF type bits (noor/cuda/path_tracer.cuh:106-119)
+enum : uint32_t {
+    BSDF_REFLECTION = 1u << 0,
+    BSDF_TRANSMISSION = 1u << 1,
+    BSDF_DIFFUSE = 1u << 2,
+    BSDF_GLOSSY = 1u << 3,
+    BSDF_SPECULAR = 1u << 4,
+    BSDF_CONDUCTOR = 1u << 5,
+    BSDF_DIELECTRIC = 1u << 6,
+    BSDF_NOOP = 1u << 7,
+    BSDF_ALL = 0xFFu
+};
+constexpr uint32_t kLobeLambert = BSDF_REFLECTION | BSDF_DIFFUSE | BSDF_DIELECTRIC;
+constexpr uint32_t kLobeConductor = BSDF_CONDUCTOR | BSDF_REFLECTION | BSDF_GLOSSY;
+constexpr uint32_t kLobeFresnelSpec = BSDF_REFLECTION | BSDF_TRANSMISSION | BSDF_SPECULAR | BSDF_DIELECTRIC;
+
+constexpr uint32_t kSpecularMat = NOOR_MIRROR | NOOR_GLASS | NOOR_CLEARCOAT;      // NOOR_SPECULAR
+constexpr uint32_t kTransparentMat = NOOR_TRANSLUCENT | NOOR_GLASS | NOOR_ROUGHGLASS;
+constexpr uint32_t kEmitterMat = NOOR_EMITTER | NOOR_MESHLIGHT;
+
+// the single lobe factoryBSDF builds for a material (noor/cuda/bsdf.cuh:425-461);
+// 0 = none
+NB_D uint32_t lobe_of(uint32_t mtype) {
+    const uint32_t t = mtype & ~(uint32_t)(NOOR_BUMP | NOOR_ALPHA);
+    if (t == NOOR_DIFFUSE) return kLobeLambert;
+    if (t == NOOR_METAL) return kLobeConductor;
+    if (t == NOOR_GLASS) return kLobeFresnelSpec;
+    return 0u;
+}
+NB_D bool lobe_matches(uint32_t lobe, uint32_t flags) { return lobe != 0u && (lobe & flags) == lobe; }
+
+// BxDF::Eval of the lobe, local frame
+NB_D float3 lobe_eval(uint32_t lobe, const DevMaterial& m, const float3& wo, const float3& wi) {
+    if (lobe == kLobeLambert) return m.diffuse * kInvPi;
+    if (lobe == kLobeConductor) {
+        // CudaMicrofacetReflection::Eval (bxdf.cuh:482-506)
+        if (!same_hemi(wo, wi)) return f3(0.0f);
+        const float cO = fabsf(wo.z), cI = fabsf(wi.z);
+        if (cI == 0.0f || cO == 0.0f) return f3(0.0f);
+        float3 wh = normalize_fast(wi + wo);
+        if (is_black(wh)) return f3(0.0f);
+        wh *= signf_ref(wh.z);
+        const float3 F = fresnel_conductor(dot(wo, wh), m.ior, m.k);
+        const Micro mf = make_micro(m);
+        return F * m.specular * mf.D(wh) * mf.G(wo, wi) / (4.0f * cI * cO);
+    }
+    return f3(0.0f);  // specular lobe: delta
+}
+NB_D float lobe_pdf(uint32_t lobe, const DevMaterial& m, const float3& wo, const float3& wi) {
+    if (lobe == kLobeLambert) return same_hemi(wo, wi) ? fabsf(wi.z) * kInvPi : 0.0f;
+    if (lobe == kLobeConductor) {
+        if (!same_hemi(wo, wi)) return 0.0f;
+        const float3 wh = normalize_guard(wo + wi);
+        const Micro mf = make_micro(m);
+        return mf.pdf(wo, wh) / (4.0f * dot(wo, wh));
+    }
+    return 0.0f;
+}
+// BxDF::Sample_f of the lobe; pdf stays 0 on failure
+NB_D float3 lobe_sample(uint32_t lobe, const DevMaterial& m, const float3& wo, float ux, float uy, float3& wi,
+                        float& pdf, uint32_t& stype) {
+    stype = lobe;
+    if (lobe == kLobeLambert) {
+        // CudaLambertianReflection::Sample_f (bxdf.cuh:270-285)
+        wi = cosine_hemisphere(ux, uy);
+        if (wo.z < 0.0f) wi.z *= -1.0f;
+        pdf = same_hemi(wo, wi) ? fabsf(wi.z) * kInvPi : 0.0f;
+        return m.diffuse * kInvPi;
+    }
+    if (lobe == kLobeConductor) {
+        // CudaMicrofacetReflection::Sample_f (bxdf.cuh:520-539)
+        if (wo.z == 0.0f) return f3(0.0f);
+        const Micro mf = make_micro(m);
+        const float3 wh = mf.sample_wh(wo, ux, uy);
+        wi = -1.0f * wo + 2.0f * dot(wo, wh) * wh;
+        if (!same_hemi(wo, wi)) {
+            pdf = 0.0f;
+            return f3(0.0f);
+        }
+        pdf = mf.pdf(wo, wh) / (4.0f * dot(wo, wh));
+        return lobe_eval(lobe, m, wo, wi);
+    }
+    if (lobe == kLobeFresnelSpec) {
+        // CudaFresnelSpecular::Sample_f (bxdf.cuh:775-809), IOR = coat_ior
+        const float ior = m.coat_ior;
+        const float F = fresnel_dielectric(wo.z, 1.0f, ior);
+        if (ux < F) {
+            wi = f3(-wo.x, -wo.y, wo.z);
+            pdf = F;
+            stype = BSDF_REFLECTION | BSDF_SPECULAR;
+            return F * m.specular / fabsf(wi.z);
+        }
+        const bool entering = wo.z > 0.0f;
+        const float eta = entering ? (1.0f / ior) : (ior / 1.0f);
+        const float3 n = faceforward(f3(0.0f, 0.0f, 1.0f), wo);
+        const float cI = dot(n, wo);
+        const float s2I = fmaxf(0.0f, 1.0f - cI * cI);
+        const float s2T = eta * eta * s2I;
+        if (s2T >= 1.0f) return f3(0.0f);
+        const float cT = sqrtf(1.0f - s2T);
+        wi = -eta * wo + (eta * cI - cT) * n;
+        pdf = 1.0f - F;
+        stype = BSDF_TRANSMISSION | BSDF_SPECULAR;
+        return m.transmission * eta * eta * (1.0f - F) / fabsf(wi.z);
+    }
+    return f3(0.0f);
+}
+
+// CudaBSDF over the single lobe (noor/cuda/bsdf.cuh:252-358)
+NB_D float3 bsdf_eval(uint32_t lobe, const DevMaterial& m, const Frame& F, const float3& woW, const float3& wiW,
+                      uint32_t flags) {
+    const float3 wo = to_local(F, woW), wi = to_local(F, wiW);
+    const bool reflect = dot(wiW, F.ng) * dot(woW, F.ng) > 0.0f;
+    if (lobe_matches(lobe, flags) && ((reflect && (lobe & BSDF_REFLECTION)) || (!reflect && (lobe & BSDF_TRANSMISSION))))
+        return lobe_eval(lobe, m, wo, wi);
+    return f3(0.0f);
+}
+NB_D float bsdf_pdf(uint32_t lobe, const DevMaterial& m, const Frame& F, const float3& woW, const float3& wiW,
+                    uint32_t flags) {
+    if (lobe == 0u) return 0.0f;
+    const float3 wo = to_local(F, woW), wi = to_local(F, wiW);
+    if (wo.z == 0.0f) return 0.0f;
+    return lobe_matches(lobe, flags) ? lobe_pdf(lobe, m, wo, wi) : 0.0f;
+}
+// draws two random numbers when a lobe matches; pdf 0 = no sample
+NB_D float3 bsdf_sample(uint32_t lobe, const DevMaterial& m, const Frame& F, const float3& woW, uint32_t flags,
+                        Rng& rng, float3& wiW, float& pdf, uint32_t& stype) {
+    pdf = 0.0f;
+    stype = 0u;
+    if (!lobe_matches(lobe, flags)) return f3(0.0f);
+    const float ux = rng.next();
+    const float uy = rng.next();
+    const float uxr = fminf(ux * 1.0f - 0.0f, kOneMinusEps);
+    const float3 wo = to_local(F, woW);
+    if (wo.z == 0.0f) return f3(0.0f);
+    float3 wi = f3(0.0f);
+    uint32_t st;
+    const float3 f = lobe_sample(lobe, m, wo, uxr, uy, wi, pdf, st);
+    if (pdf == 0.0f) {
+        stype = 0u;
+        return f3(0.0f);
+    }
+    stype = st;
+    wiW = to_world(F, wi);
+    return f;
+}
+
+// ------------------------------------------------------------ sky & env
+NB_D float hosek_radiance_internal(const float* c, float theta, float gamma) {
+    const float cg = cosf(gamma);
+    const float cg2 = cg * cg;
+    const float ct = cosf(theta);
+    const float expM = expf(c[4] * gamma);
+    const float rayM = cg2;
+    const float mieM = (1.0f + cg2) / powf((1.0f + c[8] * c[8] - 2.0f * c[8] * cg), 1.5f);
+    const float zenith = sqrtf(ct);
+    return (1.0f + c[0] * expf(c[1] / (ct + 0.01f))) *
+           (c[2] + c[3] * expM + c[5] * rayM + c[6] * mieM + c[7] * zenith);
+}
+NB_D float inverse_gamma(float v) {
+    if (v <= 0.04045f) return v * 1.0f / 12.92f;
+    return powf((v + 0.055f) * 1.0f / 1.055f, 2.4f);
+}
+// CudaHosekSky::querySkyModel (noor/cuda/hosek.cuh:86-101)
+NB_D float3 hosek_query(const DevHosek& H, const float3& v) {
+    if (v.y < 0.0f) return f3(0.0f);
+    const float theta = clampf(spherical_theta(v), 0.0f, kPiOver2);
+    const float gamma = acosf(clampf(dot(v, H.solar_dir), -1.0f, 1.0f));
+    float3 rgb;
+    rgb.x = hosek_radiance_internal(H.configs[0], theta, gamma) * H.radiance[0];
+    rgb.y = hosek_radiance_internal(H.configs[1], theta, gamma) * H.radiance[1];
+    rgb.z = hosek_radiance_internal(H.configs[2], theta, gamma) * H.radiance[2];
+    if (gamma < H.solar_radius) return H.solar_scale * rgb;
+    const float3 s = rgb * 0.025f;
+    return f3(inverse_gamma(s.x), inverse_gamma(s.y), inverse_gamma(s.z));
+}
+
+// bilinear lookup at normalized (u,v) with clamp addressing, exact weights
+// (the reference filters in hardware: tex2D with cudaFilterModeLinear)
+NB_D float3 env_bilinear(const DevScene& S, float u, float v) {
+    const int W = S.env_w, H = S.env_h;
+    const float x = u * (float)W - 0.5f, y = v * (float)H - 0.5f;
+    const float fx0 = floorf(x), fy0 = floorf(y);
+    const float ax = x - fx0, ay = y - fy0;
+    int x0 = (int)fx0, y0 = (int)fy0;
+    int x1 = x0 + 1, y1 = y0 + 1;
+    x0 = min(max(x0, 0), W - 1);
+    x1 = min(max(x1, 0), W - 1);
+    y0 = min(max(y0, 0), H - 1);
+    y1 = min(max(y1, 0), H - 1);
+    const float4 t00 = __ldg(&S.env[y0 * W + x0]), t10 = __ldg(&S.env[y0 * W + x1]);
+    const float4 t01 = __ldg(&S.env[y1 * W + x0]), t11 = __ldg(&S.env[y1 * W + x1]);
+    const float w00 = (1.0f - ax) * (1.0f - ay), w10 = ax * (1.0f - ay), w01 = (1.0f - ax) * ay, w11 = ax * ay;
+    return w00 * f3(t00) + w10 * f3(t10) + w01 * f3(t01) + w11 * f3(t11);
+}
+
+// CudaSkyDomeManager::evaluate(dir) (noor/cuda/skydome.cuh:93-101)
+NB_D float3 env_eval(const DevScene& S, const float3& dir) {
+    if (S.sky_type == NOOR_SKY_PHYSICAL) return hosek_query(S.hosek, dir);
+    const float phi = spherical_phi(dir) * kInv2Pi;
+    const float theta = spherical_theta(dir) * kInvPi;
+    return env_bilinear(S, phi, theta);
+}
+
+// piecewise-constant 1D sampling over one CDF (PBRT-v3 Distribution1D)
+NB_D float sample_1d(const float* func, const float* cdf, int n, float integral, float u, float& pdf, int& off) {
+    int lo = 0, hi = n;  // largest i in [0, n] with cdf[i] <= u, clamped to [0, n-1]
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&cdf[mid]) <= u)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    off = min(lo, n - 1);
+    const float c0 = __ldg(&cdf[off]), c1 = __ldg(&cdf[off + 1]);
+    float du = u - c0;
+    if (c1 - c0 > 0.0f) du /= (c1 - c0);
+    pdf = integral > 0.0f ? __ldg(&func[off]) / integral : 0.0f;
+    return ((float)off + du) / (float)n;
+}
+
+NB_D float2 dist_sample(const DevDist2D& D, float u0, float u1, float& pdf) {
+    float pv, pu;
+    int row;
+    const float y = sample_1d(D.row_int, D.marg_cdf, D.h, D.marg_int, u1, pv, row);
+    int col;
+    const float x = sample_1d(D.func + (size_t)row * D.w, D.cdf + (size_t)row * (D.w + 1), D.w,
+                              __ldg(&D.row_int[row]), u0, pu, col);
+    pdf = pu * pv;
+    return f2(x, y);
+}
+NB_D float dist_pdf(const DevDist2D& D, float x, float y) {
+    const int iu = min(max((int)(x * D.w), 0), D.w - 1);
+    const int iv = min(max((int)(y * D.h), 0), D.h - 1);
+    return D.marg_int > 0.0f ? __ldg(&D.func[(size_t)iv * D.w + iu]) / D.marg_int : 0.0f;
+}
+
+// importance_sample_dir (noor/cuda/skydome.cuh:130-140) on the build's
+// distribution; draws two random numbers
+NB_D float3 env_sample_dir(const DevScene& S, Rng& rng, float& pdf) {
+    const float u0 = rng.next();
+    const float u1 = rng.next();
+    float mp;
+    const float2 uv = dist_sample(S.dist, u0, u1, mp);
+    const float phi = uv.x * k2Pi;
+    const float theta = uv.y * kPi;
+    const float ct = cosf(theta);
+    const float st = sinf(theta);
+    const float3 dir = normalize_fast(f3(st * cosf(phi), ct, st * sinf(phi)));
+    pdf = (st == 0.0f) ? 0.0f : mp / (2.0f * kPi * kPi * st);
+    return dir;
+}
+// CudaInfiniteLight::pdf_Li (noor/cuda/lightimp.cuh:161-173)
+NB_D float env_pdf(const DevScene& S, const float3& wi) {
+    if (!S.sky_on) return 0.0f;
+    const float theta = spherical_theta(wi);
+    const float phi = spherical_phi(wi);
+    const float st = sinf(theta);
+    if (st == 0.0f) return 0.0f;
+    return dist_pdf(S.dist, phi * kInv2Pi, theta * kInvPi) / (2.0f * kPi * kPi * st);
+}
+
+}  // namespace nb

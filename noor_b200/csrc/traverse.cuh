@@ -1,0 +1,349 @@
+// Two-level BVH traversal (closest hit and any hit) with a per-thread stack
+// in shared memory, and the two ray/triangle tests:
+//   * NOOR_ISECT_REF_WALD: the reference's Wald projection test
+//     (noor/cuda/triangle.cuh:82-198), evaluated with exactly rounded
+//     operations in the order the source writes them;
+//   * NOOR_ISECT_WATERTIGHT: Woop, Benthin & Wald 2013, "Watertight
+//     Ray/Triangle Intersection" (JCGT 2(1)), with its double-precision
+//     fallback on zero edge functions.
+// The traversal order reproduces noor/cuda/bvh.cuh:142-234: pop, slab test,
+// then by node kind; an inner node pushes the far child first so the near
+// child (chosen by the ray's direction sign on the split axis) pops next.
+#pragma once
+#include "scene_dev.cuh"
+
+namespace nb {
+
+// ray in the space of the BVH level being traversed
+struct TRay {
+    float3 o, d, inv;
+    uint32_t neg;  // bit a set when d[a] <= 0 (noor/cuda/ray.cuh:200-206)
+};
+
+NB_D void tray_setup(TRay& r, const float3& o, const float3& d) {
+    r.o = o;
+    r.d = d;
+    r.inv = f3(xdiv(1.0f, d.x), xdiv(1.0f, d.y), xdiv(1.0f, d.z));
+    r.neg = (d.x > 0.0f ? 0u : 1u) | (d.y > 0.0f ? 0u : 2u) | (d.z > 0.0f ? 0u : 4u);
+}
+
+// world -> object: origin as translation + M*o, direction as M*d, no
+// renormalisation, so t is shared by both levels (noor/cuda/ray.cuh:174-180)
+NB_D void tray_to_object(TRay& r, const TRay& w, const DevXform* xf) {
+    const float4 r0 = __ldg(&xf->w2o[0]);
+    const float4 r1 = __ldg(&xf->w2o[1]);
+    const float4 r2 = __ldg(&xf->w2o[2]);
+    const float3 o = f3(xadd(r0.w, xdot3(r0.x, r0.y, r0.z, w.o.x, w.o.y, w.o.z)),
+                        xadd(r1.w, xdot3(r1.x, r1.y, r1.z, w.o.x, w.o.y, w.o.z)),
+                        xadd(r2.w, xdot3(r2.x, r2.y, r2.z, w.o.x, w.o.y, w.o.z)));
+    const float3 d = f3(xdot3(r0.x, r0.y, r0.z, w.d.x, w.d.y, w.d.z),
+                        xdot3(r1.x, r1.y, r1.z, w.d.x, w.d.y, w.d.z),
+                        xdot3(r2.x, r2.y, r2.z, w.d.x, w.d.y, w.d.z));
+    tray_setup(r, o, d);
+}
+
+// slab test of noor/cuda/bbox.cuh:62-80
+NB_D bool slab_hit(const TRay& r, const uint4& lo, const uint4& hi, float tmax) {
+    const float mnx = __uint_as_float(lo.x), mny = __uint_as_float(lo.y), mnz = __uint_as_float(lo.z);
+    const float mxx = __uint_as_float(hi.x), mxy = __uint_as_float(hi.y), mxz = __uint_as_float(hi.z);
+    const bool nx = r.neg & 1u, ny = r.neg & 2u, nz = r.neg & 4u;
+    float tMin = xmul(xsub(nx ? mxx : mnx, r.o.x), r.inv.x);
+    float tMax = xmul(xsub(nx ? mnx : mxx, r.o.x), r.inv.x);
+    const float tyMin = xmul(xsub(ny ? mxy : mny, r.o.y), r.inv.y);
+    const float tyMax = xmul(xsub(ny ? mny : mxy, r.o.y), r.inv.y);
+    if (tMin > tyMax || tyMin > tMax) return false;
+    if (tyMin > tMin) tMin = tyMin;
+    if (tyMax < tMax) tMax = tyMax;
+    const float tzMin = xmul(xsub(nz ? mxz : mnz, r.o.z), r.inv.z);
+    const float tzMax = xmul(xsub(nz ? mnz : mxz, r.o.z), r.inv.z);
+    if (tMin > tzMax || tzMin > tMax) return false;
+    if (tzMin > tMin) tMin = tzMin;
+    if (tzMax < tMax) tMax = tzMax;
+    return (tMin < tmax) && (tMax > 0.0f);
+}
+
+// Wald projection test (noor/cuda/triangle.cuh:82-141); on success writes
+// t into tmax and the barycentrics (u weights v1, v weights v2).
+NB_D bool wald_test(const TRay& r, const DevWaldTri* tri, float& tmax, float& bu, float& bv,
+                    uint32_t& mtype) {
+    const uint4 a = __ldg(&tri->ax_nu_nv_nd);
+    const uint4 c = __ldg(&tri->cnu_cnv_deg_mat);
+    if (c.z == 1u) return false;
+    const uint32_t k = a.x;
+    const uint32_t ku = (k == 0u) ? 1u : (k == 1u ? 2u : 0u);
+    const uint32_t kv = (k == 0u) ? 2u : (k == 1u ? 0u : 1u);
+    const float ro_u = comp(r.o, ku), ro_v = comp(r.o, kv), ro_k = comp(r.o, k);
+    const float rd_u = comp(r.d, ku), rd_v = comp(r.d, kv), rd_k = comp(r.d, k);
+    const float nu = __uint_as_float(a.y), nv = __uint_as_float(a.z), nd = __uint_as_float(a.w);
+    const float denom = xadd(xadd(rd_k, xmul(nu, rd_u)), xmul(nv, rd_v));
+    if (denom == 0.0f) return false;
+    const float t = xdiv(xsub(xsub(xsub(nd, ro_k), xmul(nu, ro_u)), xmul(nv, ro_v)), denom);
+    if (t < 0.0f || t > tmax) return false;
+    const uint4 b = __ldg(&tri->bnu_bnv_au_av);
+    const float hu = xsub(xadd(ro_u, xmul(t, rd_u)), __uint_as_float(b.z));
+    const float hv = xsub(xadd(ro_v, xmul(t, rd_v)), __uint_as_float(b.w));
+    const float u = xadd(xmul(hv, __uint_as_float(b.x)), xmul(hu, __uint_as_float(b.y)));
+    const float v = xadd(xmul(hu, __uint_as_float(c.x)), xmul(hv, __uint_as_float(c.y)));
+    if (!(u >= 0.0f && v >= 0.0f && xadd(u, v) <= 1.0f)) return false;
+    tmax = t;
+    bu = u;
+    bv = v;
+    mtype = c.w;
+    return true;
+}
+
+// per-ray constants of the watertight test
+struct WtRay {
+    int kx, ky, kz;
+    float sx, sy, sz;
+};
+
+NB_D void wt_setup(WtRay& w, const float3& d) {
+    const float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
+    int kz = (ax > ay) ? (ax > az ? 0 : 2) : (ay > az ? 1 : 2);
+    int kx = kz + 1 == 3 ? 0 : kz + 1;
+    int ky = kx + 1 == 3 ? 0 : kx + 1;
+    const float dz = comp(d, kz);
+    if (dz < 0.0f) {
+        const int t = kx;
+        kx = ky;
+        ky = t;
+    }
+    w.kx = kx;
+    w.ky = ky;
+    w.kz = kz;
+    w.sx = xdiv(comp(d, kx), dz);
+    w.sy = xdiv(comp(d, ky), dz);
+    w.sz = xdiv(1.0f, dz);
+}
+
+NB_D float xorsign(float v, uint32_t signbit) { return __uint_as_float(__float_as_uint(v) ^ signbit); }
+
+NB_D bool wt_test(const TRay& r, const WtRay& w, const DevWtTri* tri, float& tmax, float& bu,
+                  float& bv, uint32_t& mtype) {
+    const float4 p0 = __ldg(&tri->v0);
+    const float4 p1 = __ldg(&tri->v1);
+    const float4 p2 = __ldg(&tri->v2);
+    const float3 A = f3(xsub(p0.x, r.o.x), xsub(p0.y, r.o.y), xsub(p0.z, r.o.z));
+    const float3 B = f3(xsub(p1.x, r.o.x), xsub(p1.y, r.o.y), xsub(p1.z, r.o.z));
+    const float3 C = f3(xsub(p2.x, r.o.x), xsub(p2.y, r.o.y), xsub(p2.z, r.o.z));
+    const float Akz = comp(A, w.kz), Bkz = comp(B, w.kz), Ckz = comp(C, w.kz);
+    const float Ax = xsub(comp(A, w.kx), xmul(w.sx, Akz));
+    const float Ay = xsub(comp(A, w.ky), xmul(w.sy, Akz));
+    const float Bx = xsub(comp(B, w.kx), xmul(w.sx, Bkz));
+    const float By = xsub(comp(B, w.ky), xmul(w.sy, Bkz));
+    const float Cx = xsub(comp(C, w.kx), xmul(w.sx, Ckz));
+    const float Cy = xsub(comp(C, w.ky), xmul(w.sy, Ckz));
+    float U = xsub(xmul(Cx, By), xmul(Cy, Bx));
+    float V = xsub(xmul(Ax, Cy), xmul(Ay, Cx));
+    float W = xsub(xmul(Bx, Ay), xmul(By, Ax));
+    if (U == 0.0f || V == 0.0f || W == 0.0f) {
+        // products of two floats are exact in double; one rounding each
+        U = (float)__dsub_rn(__dmul_rn((double)Cx, (double)By), __dmul_rn((double)Cy, (double)Bx));
+        V = (float)__dsub_rn(__dmul_rn((double)Ax, (double)Cy), __dmul_rn((double)Ay, (double)Cx));
+        W = (float)__dsub_rn(__dmul_rn((double)Bx, (double)Ay), __dmul_rn((double)By, (double)Ax));
+    }
+    if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return false;
+    const float det = xadd(xadd(U, V), W);
+    if (det == 0.0f) return false;
+    const float Az = xmul(w.sz, Akz), Bz = xmul(w.sz, Bkz), Cz = xmul(w.sz, Ckz);
+    const float T = xadd(xadd(xmul(U, Az), xmul(V, Bz)), xmul(W, Cz));
+    const uint32_t sgn = __float_as_uint(det) & 0x80000000u;
+    const float Ts = xorsign(T, sgn);
+    if (Ts < 0.0f || Ts > xmul(tmax, xorsign(det, sgn))) return false;
+    const float rcp = xdiv(1.0f, det);
+    tmax = xmul(T, rcp);
+    bu = xmul(V, rcp);
+    bv = xmul(W, rcp);
+    mtype = __float_as_uint(p0.w);
+    return true;
+}
+
+// quad of an area light (noor/cuda/geometry.cuh:105-123); note the
+// reference accepts negative t (no lower bound), kept as is.
+NB_D bool quad_hit(const DevAreaLight& q, const float3& o, const float3& d, float& tmax) {
+    const float denom = dot(q.n, d);
+    if (denom == 0.0f) return false;
+    const float t = -(dot(o, q.n) - dot(q.center, q.n)) / denom;
+    if (t > tmax) return false;
+    const float3 p = o + t * d;
+    const float3 ip = p - q.center;
+    const float t0 = dot(ip, q.u) / dot(q.u, q.u);
+    if (t0 < 0.0f || t0 > 1.0f) return false;
+    const float t1 = dot(ip, q.v) / dot(q.v, q.v);
+    if (t1 < 0.0f || t1 > 1.0f) return false;
+    tmax = t;
+    return true;
+}
+
+struct HitRec {
+    float u, v;
+    uint32_t tri;
+    uint32_t ins;
+    uint32_t mtype;
+};
+
+// Shared-memory stack: entry i of this thread lives at stk[i * stride].
+struct SmemStack {
+    uint32_t* base;
+    int stride;
+    int cap;
+};
+
+// Closest hit.  tmax in: ray extent, out: hit distance.  Returns hit flag;
+// on stack overflow sets *status and returns what was found so far.
+template <int ISECT>
+NB_D bool trace_closest(const DevScene& S, const float3& o, const float3& d, float& tmax,
+                        HitRec& rec, const SmemStack& st, uint32_t* status) {
+    TRay wr;
+    tray_setup(wr, o, d);
+    TRay lr = wr;
+    WtRay wt;
+    if (ISECT == NOOR_ISECT_WATERTIGHT) wt_setup(wt, lr.d);
+    float ltmax = tmax;
+    uint32_t ins = 0;
+    bool hit = false;
+    int top = 0;
+    st.base[0] = S.root;
+    top = 1;
+    while (top > 0) {
+        --top;
+        const uint32_t ni = st.base[top * st.stride];
+        const DevNode* nd = S.nodes + ni;
+        const uint4 lo = __ldg(&nd->lo);
+        const uint4 hi = __ldg(&nd->hi);
+        if (hi.w & NOOR_MESH_NODE_MASK) {
+            lr = wr;
+            ltmax = tmax;
+            if (ISECT == NOOR_ISECT_WATERTIGHT) wt_setup(wt, lr.d);
+        }
+        if (!slab_hit(lr, lo, hi, ltmax)) continue;
+        if (hi.w & NOOR_LIGHT_NODE_MASK) {
+            const uint32_t li = hi.w & NOOR_LIGHT_MASK;
+            if ((int)li < S.num_area_lights && quad_hit(S.area_lights[li], o, d, tmax)) {
+                hit = true;
+                rec.ins = li;
+                rec.mtype = NOOR_MESHLIGHT | NOOR_EMITTER;
+            }
+            continue;
+        } else if (hi.w & NOOR_MESH_INSTANCE_MASK) {
+            ins = hi.w & NOOR_TRANS_MASK;
+            tray_to_object(lr, wr, S.xforms + ins);
+            ltmax = tmax;
+            if (ISECT == NOOR_ISECT_WATERTIGHT) wt_setup(wt, lr.d);
+            if (top >= st.cap) { atomicOr(status, NOOR_DEV_STACK_OVERFLOW); break; }
+            st.base[top * st.stride] = lo.w;
+            ++top;
+        } else if (hi.w & NOOR_MESH_LEAF_MASK) {
+            const uint32_t cnt = hi.w & NOOR_COUNT_MASK;
+            if (top + (int)cnt > st.cap) { atomicOr(status, NOOR_DEV_STACK_OVERFLOW); break; }
+            for (uint32_t i = 1; i <= cnt; ++i) {
+                st.base[top * st.stride] = ni + i;
+                ++top;
+            }
+        } else if (hi.w & NOOR_TRI_LEAF_MASK) {
+            const uint32_t start = lo.w;
+            const uint32_t end = start + (hi.w & NOOR_TRI_COUNT_MASK);
+            bool leaf_hit = false;
+            for (uint32_t ti = start; ti < end; ++ti) {
+                float bu, bv;
+                uint32_t mt;
+                bool h;
+                if (ISECT == NOOR_ISECT_WATERTIGHT)
+                    h = wt_test(lr, wt, S.wtri + ti, ltmax, bu, bv, mt);
+                else
+                    h = wald_test(lr, S.wald + ti, ltmax, bu, bv, mt);
+                if (h) {
+                    leaf_hit = true;
+                    rec.u = bu;
+                    rec.v = bv;
+                    rec.tri = ti;
+                    rec.mtype = mt;
+                }
+            }
+            if (leaf_hit) {
+                hit = true;
+                tmax = ltmax;
+                rec.ins = ins;
+            }
+        } else {
+            if (top + 2 > st.cap) { atomicOr(status, NOOR_DEV_STACK_OVERFLOW); break; }
+            const uint32_t axis = hi.w & NOOR_AXIS_MASK;
+            const bool neg = (lr.neg >> axis) & 1u;
+            st.base[top * st.stride] = neg ? ni + 1 : lo.w;
+            st.base[(top + 1) * st.stride] = neg ? lo.w : ni + 1;
+            top += 2;
+        }
+    }
+    return hit;
+}
+
+// Any hit within (0, tmax]; light nodes count as occluders.
+template <int ISECT>
+NB_D bool trace_any(const DevScene& S, const float3& o, const float3& d, float tmax,
+                    const SmemStack& st, uint32_t* status) {
+    TRay wr;
+    tray_setup(wr, o, d);
+    TRay lr = wr;
+    WtRay wt;
+    if (ISECT == NOOR_ISECT_WATERTIGHT) wt_setup(wt, lr.d);
+    float ltmax = tmax;
+    int top = 0;
+    st.base[0] = S.root;
+    top = 1;
+    while (top > 0) {
+        --top;
+        const uint32_t ni = st.base[top * st.stride];
+        const DevNode* nd = S.nodes + ni;
+        const uint4 lo = __ldg(&nd->lo);
+        const uint4 hi = __ldg(&nd->hi);
+        if (hi.w & NOOR_MESH_NODE_MASK) {
+            lr = wr;
+            ltmax = tmax;
+            if (ISECT == NOOR_ISECT_WATERTIGHT) wt_setup(wt, lr.d);
+        }
+        if (!slab_hit(lr, lo, hi, ltmax)) continue;
+        if (hi.w & NOOR_LIGHT_NODE_MASK) {
+            const uint32_t li = hi.w & NOOR_LIGHT_MASK;
+            float tm = tmax;
+            if ((int)li < S.num_area_lights && quad_hit(S.area_lights[li], o, d, tm)) return true;
+        } else if (hi.w & NOOR_MESH_INSTANCE_MASK) {
+            tray_to_object(lr, wr, S.xforms + (hi.w & NOOR_TRANS_MASK));
+            ltmax = tmax;
+            if (ISECT == NOOR_ISECT_WATERTIGHT) wt_setup(wt, lr.d);
+            if (top >= st.cap) { atomicOr(status, NOOR_DEV_STACK_OVERFLOW); return false; }
+            st.base[top * st.stride] = lo.w;
+            ++top;
+        } else if (hi.w & NOOR_MESH_LEAF_MASK) {
+            const uint32_t cnt = hi.w & NOOR_COUNT_MASK;
+            if (top + (int)cnt > st.cap) { atomicOr(status, NOOR_DEV_STACK_OVERFLOW); return false; }
+            for (uint32_t i = 1; i <= cnt; ++i) {
+                st.base[top * st.stride] = ni + i;
+                ++top;
+            }
+        } else if (hi.w & NOOR_TRI_LEAF_MASK) {
+            const uint32_t start = lo.w;
+            const uint32_t end = start + (hi.w & NOOR_TRI_COUNT_MASK);
+            for (uint32_t ti = start; ti < end; ++ti) {
+                float tm = ltmax, bu, bv;
+                uint32_t mt;
+                bool h;
+                if (ISECT == NOOR_ISECT_WATERTIGHT)
+                    h = wt_test(lr, wt, S.wtri + ti, tm, bu, bv, mt);
+                else
+                    h = wald_test(lr, S.wald + ti, tm, bu, bv, mt);
+                if (h) return true;
+            }
+        } else {
+            if (top + 2 > st.cap) { atomicOr(status, NOOR_DEV_STACK_OVERFLOW); return false; }
+            const uint32_t axis = hi.w & NOOR_AXIS_MASK;
+            const bool neg = (lr.neg >> axis) & 1u;
+            st.base[top * st.stride] = neg ? ni + 1 : lo.w;
+            st.base[(top + 1) * st.stride] = neg ? lo.w : ni + 1;
+            top += 2;
+        }
+    }
+    return false;
+}
+
+}  // namespace nb

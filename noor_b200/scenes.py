@@ -1,0 +1,471 @@
+"""Seeded synthetic scenes for the five configurations, and the host-side
+plumbing that turns them into a payload (BVH + Wald records + materials),
+a camera, a spec and a sky through the C-ABI.
+
+Scenes are generated as the loader output Noor's Model consumes
+(noor/header/assetLoader.h:103-162): shared vertex/normal/uv arrays with
+per-triangle index triples, per-triangle material indices, meshes with
+transforms, constant materials and quad area lights.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from pathlib import Path
+from typing import Optional
+
+import numpy as np
+
+from . import _capi as capi
+
+GOLD_ETA = (0.126052, 0.465040, 1.340442)   # Au, as in the reference's material presets
+GOLD_K = (4.230981, 2.204432, 1.642458)
+DEFAULT_BVH = dict(num_bins=16, max_height=32, Ci=1.0, Ct=0.125, min_leaf_tris=2, max_leaf_tris=4)
+HOSEK_DATASET = Path(__file__).resolve().parent.parent / "tests" / "golden" / "hosek_rgb_dataset.npy"
+
+IDENTITY = np.eye(4, dtype=np.float32).reshape(-1, order="F")
+
+
+def material(kind: str, albedo=(0.5, 0.5, 0.5), roughness: float = 0.1, ior: float = 1.5,
+             emittance=(0.0, 0.0, 0.0), distribution: int = 0) -> dict:
+    """Constant material parameters (AssetLoader getters) for one of
+    'diffuse', 'metal' (gold conductor), 'glass' or 'emitter'."""
+    types = {"diffuse": capi.NOOR_DIFFUSE, "metal": capi.NOOR_METAL, "glass": capi.NOOR_GLASS,
+             "emitter": capi.NOOR_EMITTER}
+    return dict(diffuse=tuple(albedo), specular=(1.0, 1.0, 1.0), transmission=(1.0, 1.0, 1.0),
+                emittance=tuple(emittance), transparency=(1.0, 1.0, 1.0),
+                ior=GOLD_ETA if kind == "metal" else (ior, ior, ior), k=GOLD_K if kind == "metal" else (0, 0, 0),
+                roughness=(roughness, roughness), coat_weight=1.0, coat_roughness=0.001, coat_thickness=1.0,
+                coat_sigma=0.0, coat_ior=ior, emitter_scale=1.0, type=types[kind], distribution=distribution)
+
+
+@dataclass
+class SceneData:
+    vertices: np.ndarray           # (V,4) f32
+    normals: np.ndarray            # (N,4) f32
+    uvs: np.ndarray                # (U,2) f32
+    vindices: np.ndarray           # (T,3) u32
+    nindices: np.ndarray
+    uvindices: np.ndarray
+    material_indices: np.ndarray   # (T,) u32
+    meshes: list
+    materials: list
+    area_lights: list = field(default_factory=list)
+    skydome_type: int = capi.NOOR_SKY_CONSTANT
+    env: Optional[np.ndarray] = None   # (H,W,4) f32
+    bvh: dict = field(default_factory=lambda: dict(DEFAULT_BVH))
+    camera: dict = field(default_factory=dict)
+    render: dict = field(default_factory=dict)
+    hosek: Optional[dict] = None
+    name: str = ""
+
+    @property
+    def num_triangles(self) -> int:
+        return int(self.vindices.shape[0])
+
+
+# ----------------------------------------------------------------- C1 room
+def _quad(points, inward):
+    """two triangles (a,b,c),(a,c,d) wound so cross(b-a, c-a) follows `inward`"""
+    a, b, c, d = [np.asarray(p, np.float64) for p in points]
+    n = np.cross(b - a, c - a)
+    if np.dot(n, inward) < 0:
+        a, b, c, d = a, d, c, b
+    return [a, b, c, d]
+
+
+def _box(center, size, angle_deg):
+    """6 faces (4 corners each) of a y-rotated box with outward orientation"""
+    cx, cy, cz = center
+    sx, sy, sz = size
+    t = np.radians(angle_deg)
+    R = np.array([[np.cos(t), 0, np.sin(t)], [0, 1, 0], [-np.sin(t), 0, np.cos(t)]])
+    c = np.array(center, np.float64)
+    faces = []
+    for axis in range(3):
+        for s in (-1.0, 1.0):
+            n = np.zeros(3)
+            n[axis] = s
+            u = np.zeros(3)
+            v = np.zeros(3)
+            u[(axis + 1) % 3] = 1
+            v[(axis + 2) % 3] = 1
+            half = np.array([sx, sy, sz]) / 2
+            pts = []
+            for du, dv in ((-1, -1), (1, -1), (1, 1), (-1, 1)):
+                p = n * half + du * u * half + dv * v * half
+                pts.append(c + R @ p)
+            faces.append((_quad(pts, R @ n), R @ n))
+    return faces
+
+
+def room_scene(seed: int = 1, width: int = 256, height: int = 256, spp: int = 16, bounces: int = 5,
+               rr: int = 1, mis: bool = False) -> SceneData:
+    """C1: closed room of 5 wall quads + 1 ceiling light quad + 2 rotated
+    boxes = 36 triangles, one mesh; wall albedo U[0.2,0.8]^3 from `seed`."""
+    rng = np.random.default_rng(seed)
+    faces = []   # (corners, normal, material)
+    walls = [
+        ([(-1, 0, 1), (1, 0, 1), (1, 0, -1), (-1, 0, -1)], (0, 1, 0)),     # floor
+        ([(-1, 2, 1), (1, 2, 1), (1, 2, -1), (-1, 2, -1)], (0, -1, 0)),    # ceiling
+        ([(-1, 0, -1), (1, 0, -1), (1, 2, -1), (-1, 2, -1)], (0, 0, 1)),   # back
+        ([(-1, 0, -1), (-1, 0, 1), (-1, 2, 1), (-1, 2, -1)], (1, 0, 0)),   # left
+        ([(1, 0, -1), (1, 0, 1), (1, 2, 1), (1, 2, -1)], (-1, 0, 0)),      # right
+    ]
+    mats = []
+    for i, (pts, n) in enumerate(walls):
+        mats.append(material("diffuse", albedo=tuple(rng.uniform(0.2, 0.8, 3))))
+        faces.append((_quad(pts, np.array(n, np.float64)), np.array(n, np.float64), i))
+    box_mat = len(mats)
+    mats.append(material("diffuse", albedo=(0.7, 0.7, 0.7)))
+    for corners_n in _box((0.35, 0.3, 0.25), (0.6, 0.6, 0.6), 17.0) + _box((-0.33, 0.6, -0.3), (0.6, 1.2, 0.6), -18.0):
+        faces.append((corners_n[0], corners_n[1], box_mat))
+    light_mat = len(mats)
+    ke = (17.0, 12.0, 4.0)
+    mats.append(material("emitter", emittance=ke))
+    ly, h = 1.98, 0.25
+    lpts = _quad([(-h, ly, -h), (h, ly, -h), (h, ly, h), (-h, ly, h)], np.array([0.0, -1.0, 0.0]))
+    faces.append((lpts, np.array([0.0, -1.0, 0.0]), light_mat))
+
+    verts, norms, vidx, nidx, midx = [], [], [], [], []
+    for corners, n, m in faces:
+        base = len(verts)
+        verts.extend(corners)
+        ni = len(norms)
+        norms.append(n / np.linalg.norm(n))
+        for tri in ((0, 1, 2), (0, 2, 3)):
+            vidx.append([base + tri[0], base + tri[1], base + tri[2]])
+            nidx.append([ni, ni, ni])
+            midx.append(m)
+    V = np.zeros((len(verts), 4), np.float32)
+    V[:, :3] = np.array(verts)
+    V[:, 3] = 1.0
+    N = np.zeros((len(norms), 4), np.float32)
+    N[:, :3] = np.array(norms)
+    T = len(vidx)
+    light = dict(center=(-h, ly, -h), u=(2 * h, 0.0, 0.0), v=(0.0, 0.0, 2 * h), ke=ke, two_sided=0)
+    return SceneData(
+        vertices=V, normals=N, uvs=np.zeros((1, 2), np.float32),
+        vindices=np.array(vidx, np.uint32), nindices=np.array(nidx, np.uint32),
+        uvindices=np.zeros((T, 3), np.uint32), material_indices=np.array(midx, np.uint32),
+        meshes=[dict(tri_start=0, tri_count=T, to_global=IDENTITY, instance=-1, light_idx=-1)],
+        materials=mats, area_lights=[light], skydome_type=capi.NOOR_SKY_CONSTANT,
+        camera=dict(eye=(0.0, 1.0, 3.75), look_at=(0.0, 1.0, 0.0), up=(0.0, 1.0, 0.0), fov_deg=40.0,
+                    w=width, h=height),
+        render=dict(spp=spp, bounces=bounces, rr=rr, mis=int(mis)), name="room")
+
+
+# ------------------------------------------------------------- icospheres
+_ICO_CACHE: dict = {}
+
+
+def icosphere(level: int):
+    """unit icosphere: (V,3) float64 vertices, (F,3) int faces wound outward"""
+    if level in _ICO_CACHE:
+        return _ICO_CACHE[level]
+    t = (1.0 + 5.0 ** 0.5) / 2.0
+    V = np.array([(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+                  (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)], np.float64)
+    V /= np.linalg.norm(V, axis=1, keepdims=True)
+    F = np.array([(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2),
+                  (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5),
+                  (2, 4, 11), (6, 2, 10), (8, 6, 7), (9, 8, 1)], np.int64)
+    for _ in range(level):
+        e = np.concatenate([F[:, [0, 1]], F[:, [1, 2]], F[:, [2, 0]]])
+        es = np.sort(e, axis=1)
+        uniq, inv = np.unique(es, axis=0, return_inverse=True)
+        mid = V[uniq[:, 0]] + V[uniq[:, 1]]
+        mid /= np.linalg.norm(mid, axis=1, keepdims=True)
+        base = V.shape[0]
+        V = np.concatenate([V, mid])
+        m = inv.reshape(3, -1).T + base
+        a, b, c = F[:, 0], F[:, 1], F[:, 2]
+        ab, bc, ca = m[:, 0], m[:, 1], m[:, 2]
+        F = np.concatenate([np.stack([a, ab, ca], 1), np.stack([b, bc, ab], 1), np.stack([c, ca, bc], 1),
+                            np.stack([ab, bc, ca], 1)])
+    n = np.cross(V[F[:, 1]] - V[F[:, 0]], V[F[:, 2]] - V[F[:, 0]])
+    flip = np.einsum("ij,ij->i", n, V[F].mean(axis=1)) < 0
+    F[flip] = F[flip][:, [0, 2, 1]]
+    _ICO_CACHE[level] = (V, F)
+    return V, F
+
+
+def sphere_field(seed: int, count: int, level: int, box: float = 20.0, rmin: float = 0.1, rmax: float = 1.0,
+                 kinds=("diffuse", "metal", "glass"), jitter: float = 0.002):
+    """`count` icospheres: radius log-U[rmin,rmax], centre U in a box^3 cube,
+    vertices jittered by N(0, jitter*r), one material per object drawn from
+    `kinds` (Lambert albedo U[0.1,0.9]^3, gold conductor alpha U[0.05,0.5],
+    dielectric IOR 1.5).  Returns the loader arrays."""
+    rng = np.random.default_rng(seed)
+    Vu, F = icosphere(level)
+    nv, nf = Vu.shape[0], F.shape[0]
+    radii = np.exp(rng.uniform(np.log(rmin), np.log(rmax), count))
+    centers = rng.uniform(-box / 2, box / 2, (count, 3))
+    V = np.zeros((count * nv, 4), np.float32)
+    N = np.zeros((count * nv, 4), np.float32)
+    vidx = np.zeros((count * nf, 3), np.uint32)
+    midx = np.zeros(count * nf, np.uint32)
+    meshes, mats = [], []
+    for i in range(count):
+        p = centers[i] + radii[i] * Vu + rng.normal(0.0, jitter * radii[i], Vu.shape)
+        V[i * nv:(i + 1) * nv, :3] = p
+        V[i * nv:(i + 1) * nv, 3] = 1.0
+        N[i * nv:(i + 1) * nv, :3] = Vu
+        vidx[i * nf:(i + 1) * nf] = F + i * nv
+        midx[i * nf:(i + 1) * nf] = i
+        kind = kinds[int(rng.integers(0, len(kinds)))]
+        if kind == "diffuse":
+            mats.append(material("diffuse", albedo=tuple(rng.uniform(0.1, 0.9, 3))))
+        elif kind == "metal":
+            alpha = rng.uniform(0.05, 0.5)
+            mats.append(material("metal", roughness=float(np.sqrt(alpha))))
+        else:
+            mats.append(material("glass", ior=1.5))
+        meshes.append(dict(tri_start=i * nf, tri_count=nf, to_global=IDENTITY, instance=-1, light_idx=-1))
+    T = count * nf
+    return dict(vertices=V, normals=N, uvs=np.zeros((1, 2), np.float32), vindices=vidx, nindices=vidx.copy(),
+                uvindices=np.zeros((T, 3), np.uint32), material_indices=midx, meshes=meshes, materials=mats)
+
+
+SKY_CAMERA = dict(eye=(0.0, 2.0, 16.0), look_at=(0.0, 0.0, 0.0), up=(0.0, 1.0, 0.0), fov_deg=50.0)
+
+
+def sky_scene(seed: int = 2, width: int = 1920, height: int = 1080, spp: int = 64, bounces: int = 8,
+              count: int = 32, level: int = 6, rr: int = 1, mis: bool = False) -> SceneData:
+    """C2: 32 subdivision-6 icospheres (2,621,440 triangles) under a
+    Hosek-Wilkie sky (turbidity 3, sun elevation 30 deg, ground albedo 0.3)."""
+    g = sphere_field(seed, count, level)
+    cam = dict(SKY_CAMERA, w=width, h=height)
+    return SceneData(**g, skydome_type=capi.NOOR_SKY_PHYSICAL, camera=cam,
+                     render=dict(spp=spp, bounces=bounces, rr=rr, mis=int(mis)),
+                     hosek=dict(turbidity=3.0, albedo=0.3, sun_lat=float(np.radians(60.0)),
+                                sun_lon=float(np.pi / 4), solar_scale=250.0, solar_radius_scale=2.0),
+                     name="sky")
+
+
+def env_map(seed: int, width: int = 2048, height: int = 1024, mu: float = -1.0, sigma: float = 0.5,
+            lobes: int = 3, peak: float = 1e4, lobe_sigma_deg=(1.0, 3.0)) -> np.ndarray:
+    """equirectangular RGB map: log-normal background plus Gaussian lobes at
+    seeded directions; texel (row j, col i) is the direction at
+    theta = pi (j+0.5)/H, phi = 2 pi (i+0.5)/W, y up."""
+    rng = np.random.default_rng(seed)
+    img = np.exp(rng.normal(mu, sigma, (height, width, 3))).astype(np.float64)
+    th = (np.arange(height) + 0.5) / height * np.pi
+    ph = (np.arange(width) + 0.5) / width * 2 * np.pi
+    st, ct = np.sin(th)[:, None], np.cos(th)[:, None]
+    dirs = np.stack([st * np.cos(ph)[None, :], np.broadcast_to(ct, (height, width)), st * np.sin(ph)[None, :]], -1)
+    for _ in range(lobes):
+        d = rng.normal(size=3)
+        d /= np.linalg.norm(d)
+        s = np.radians(rng.uniform(*lobe_sigma_deg))
+        ang = np.arccos(np.clip(dirs @ d, -1.0, 1.0))
+        img += (peak * np.exp(-ang * ang / (2 * s * s)))[..., None]
+    out = np.ones((height, width, 4), np.float32)
+    out[..., :3] = img
+    return out
+
+
+def env_scene(seed: int = 3, width: int = 1920, height: int = 1080, spp: int = 128, bounces: int = 8,
+              count: int = 32, level: int = 6, env_w: int = 2048, env_h: int = 1024, rr: int = 1) -> SceneData:
+    """C3: the C2 geometry lit by a 2048x1024 log-normal + lobes map, MIS on."""
+    g = sphere_field(2, count, level)
+    cam = dict(SKY_CAMERA, w=width, h=height)
+    return SceneData(**g, skydome_type=capi.NOOR_SKY_HDR, env=env_map(seed, env_w, env_h), camera=cam,
+                     render=dict(spp=spp, bounces=bounces, rr=rr, mis=1), name="env")
+
+
+# ------------------------------------------------------------ C-ABI glue
+def _ptr(a: np.ndarray, t=C.c_float):
+    return a.ctypes.data_as(C.POINTER(t))
+
+
+class BuiltPayload:
+    """Owns a noor_payload_handle (host arrays the library built)."""
+
+    def __init__(self, scene: SceneData):
+        L = capi.lib()
+        s = scene
+        self.scene = s
+        keep = []
+        V = np.ascontiguousarray(s.vertices, np.float32)
+        N = np.ascontiguousarray(s.normals, np.float32)
+        U = np.ascontiguousarray(s.uvs, np.float32)
+        vi = np.ascontiguousarray(s.vindices, np.uint32)
+        ni = np.ascontiguousarray(s.nindices, np.uint32)
+        ui = np.ascontiguousarray(s.uvindices, np.uint32)
+        mi = np.ascontiguousarray(s.material_indices, np.uint32)
+        keep += [V, N, U, vi, ni, ui, mi]
+        meshes = (capi.Mesh * len(s.meshes))()
+        for k, m in enumerate(s.meshes):
+            meshes[k].tri_start = m["tri_start"]
+            meshes[k].tri_count = m["tri_count"]
+            meshes[k].to_global[:] = [float(x) for x in np.asarray(m["to_global"], np.float32)]
+            meshes[k].instance = m.get("instance", -1)
+            meshes[k].light_idx = m.get("light_idx", -1)
+        mats = (capi.MaterialDesc * len(s.materials))()
+        for k, m in enumerate(s.materials):
+            for f, _ in capi.MaterialDesc._fields_:
+                val = m[f]
+                if isinstance(val, (tuple, list, np.ndarray)):
+                    getattr(mats[k], f)[:] = [float(x) for x in val]
+                else:
+                    setattr(mats[k], f, val)
+        lights = (capi.AreaLight * max(1, len(s.area_lights)))()
+        for k, l in enumerate(s.area_lights):
+            lights[k] = make_area_light(l, k)
+        d = capi.SceneDesc()
+        d.vertices, d.num_vertices = _ptr(V), V.shape[0]
+        d.normals, d.num_normals = _ptr(N), N.shape[0]
+        d.uvs, d.num_uvs = _ptr(U), U.shape[0]
+        d.vindices, d.nindices, d.uvindices = _ptr(vi, C.c_uint32), _ptr(ni, C.c_uint32), _ptr(ui, C.c_uint32)
+        d.material_indices = _ptr(mi, C.c_uint32)
+        d.num_triangles = vi.shape[0]
+        d.meshes, d.num_meshes = meshes, len(s.meshes)
+        d.materials, d.num_materials = mats, len(s.materials)
+        d.area_lights, d.num_area_lights = lights, len(s.area_lights)
+        d.skydome_type = s.skydome_type
+        if s.env is not None:
+            E = np.ascontiguousarray(s.env, np.float32)
+            keep.append(E)
+            d.env_width, d.env_height, d.env_rgba = E.shape[1], E.shape[0], _ptr(E)
+        b = s.bvh
+        d.bvh = capi.BvhSpec(b["num_bins"], b["max_height"], b["Ci"], b["Ct"], b["min_leaf_tris"], b["max_leaf_tris"])
+        self.desc = d
+        self._keep = keep + [meshes, mats, lights]
+        h = C.c_void_p()
+        self.stat = capi.BuildStat()
+        capi.call("noor_build_payload", C.byref(d), C.byref(h), C.byref(self.stat))
+        self.handle = h
+        self.payload = capi.Payload()
+        capi.call("noor_payload_view", h, C.byref(self.payload))
+
+    def triangle_order(self) -> np.ndarray:
+        out = np.zeros(self.payload.num_triangles, np.uint32)
+        capi.call("noor_payload_triangle_order", self.handle, _ptr(out, C.c_uint32), out.size)
+        return out
+
+    def nodes(self) -> np.ndarray:
+        """(n, 8) uint32: min_right_start then max_axis_count words"""
+        n = self.payload.num_bvh_nodes
+        lo = np.ctypeslib.as_array(self.payload.bvh_min_right_start, (n, 4))
+        hi = np.ctypeslib.as_array(self.payload.bvh_max_axis_count, (n, 4))
+        return np.concatenate([lo, hi], axis=1).copy()
+
+    def array(self, name: str, cols: int, dtype=np.uint32) -> np.ndarray:
+        n = self.payload.num_triangles
+        return np.ctypeslib.as_array(getattr(self.payload, name), (n, cols)).copy()
+
+    def default_spec(self, bounces: int, rr: int) -> capi.Spec:
+        sp = capi.Spec()
+        capi.call("noor_payload_default_spec", self.handle, bounces, rr, C.byref(sp))
+        return sp
+
+    def free(self):
+        if getattr(self, "handle", None) is not None and self.handle.value:
+            capi.lib().noor_free_payload(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def make_area_light(l: dict, idx: int) -> capi.AreaLight:
+    """CudaShape(center, u, v, n, QUAD) + CudaAreaLight (shape.cuh:43-69)"""
+    a = capi.AreaLight()
+    c, u, v = (np.asarray(l[k], np.float32) for k in ("center", "u", "v"))
+    n = np.cross(u.astype(np.float64), v.astype(np.float64))
+    n = (n / np.linalg.norm(n)).astype(np.float32)
+    a.shape.center[:] = [float(x) for x in c]
+    a.shape.u[:] = [float(x) for x in u]
+    a.shape.v[:] = [float(x) for x in v]
+    a.shape.n[:] = [float(x) for x in n]
+    a.shape.area = float(np.linalg.norm(np.cross(u.astype(np.float64), v.astype(np.float64))))
+    a.shape.radius = 0.5 * min(float(np.linalg.norm(u)), float(np.linalg.norm(v)))
+    a.shape.radius2 = a.shape.radius ** 2
+    a.shape.light_idx = idx
+    a.shape.type = 0
+    a.ke[:] = [float(x) for x in l["ke"]]
+    a.two_sided = int(l.get("two_sided", 0))
+    return a
+
+
+def make_camera(cam: dict) -> capi.Camera:
+    out = capi.Camera()
+    arr = lambda v: (C.c_float * 3)(*[float(x) for x in v])
+    capi.call("noor_camera_lookat", arr(cam["eye"]), arr(cam["look_at"]), arr(cam["up"]),
+              float(np.radians(cam["fov_deg"])), int(cam["w"]), int(cam["h"]), C.byref(out))
+    return out
+
+
+def hosek_dataset() -> np.ndarray:
+    """RGB coefficient and radiance tables of the Hosek-Wilkie model
+    (3 x 1080 + 3 x 120 floats), stored as a test fixture."""
+    if not HOSEK_DATASET.exists():
+        raise FileNotFoundError(f"{HOSEK_DATASET} missing (generate with tests/golden/make_golden.py)")
+    return np.load(HOSEK_DATASET).astype(np.float32)
+
+
+def make_hosek(h: Optional[dict]) -> capi.HosekSky:
+    out = capi.HosekSky()
+    if h is None:
+        return out
+    ds = np.ascontiguousarray(hosek_dataset())
+    alb = (C.c_float * 3)(h["albedo"], h["albedo"], h["albedo"])
+    capi.call("noor_hosek_fit", _ptr(ds), float(h["turbidity"]), alb, float(h["sun_lat"]), float(h["sun_lon"]),
+              float(h["solar_scale"]), float(h["solar_radius_scale"]), C.byref(out))
+    return out
+
+
+class Renderer:
+    """The reference-facing render context: load_cuda_data on a built
+    payload, then cuda_path_tracer / noor_render_frames and film readback.
+    Keeps the camera, spec and sky structs alive for update_cuda_*."""
+
+    def __init__(self, scene: SceneData, built: Optional[BuiltPayload] = None, intersector: int = 0,
+                 film_mode: int = 0, hosek: Optional[capi.HosekSky] = None):
+        self.scene = scene
+        self.built = built or BuiltPayload(scene)
+        r = scene.render
+        self.spec = self.built.default_spec(r.get("bounces", 5), r.get("rr", 1))
+        self.spec.mis = int(r.get("mis", 0))
+        self.spec.intersector = intersector
+        self.spec.film_mode = film_mode
+        self.camera = make_camera(scene.camera)
+        self.hosek = hosek if hosek is not None else make_hosek(scene.hosek)
+        capi.call("load_cuda_data", C.byref(self.built.payload), C.byref(self.hosek), C.byref(self.camera),
+                  C.byref(self.spec), None)
+        self.frame = C.c_uint(1)
+        self.w, self.h = int(scene.camera["w"]), int(scene.camera["h"])
+
+    def render(self, n_frames: int) -> None:
+        capi.call("noor_render_frames", C.byref(self.frame), n_frames)
+
+    def path_tracer(self) -> None:
+        capi.call("cuda_path_tracer", C.byref(self.frame))
+
+    def framebuffer(self) -> np.ndarray:
+        out = np.zeros((self.h, self.w, 4), np.float32)
+        capi.call("noor_get_framebuffer", _ptr(out), self.w * self.h)
+        return out
+
+    def counters(self, reset: bool = False):
+        c = (C.c_uint64 * 3)()
+        capi.call("noor_ray_counters", c, int(reset))
+        return tuple(int(x) for x in c)
+
+    def status(self, reset: bool = False) -> int:
+        s = C.c_uint32()
+        capi.call("noor_device_status", C.byref(s), int(reset))
+        return s.value
+
+    def update_spec(self, **kw):
+        for k, v in kw.items():
+            setattr(self.spec, k, v)
+        capi.call("update_cuda_spec")
+        self.frame = C.c_uint(1)
+
+    def close(self):
+        capi.call("device_free_memory")

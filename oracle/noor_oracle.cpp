@@ -1,0 +1,1365 @@
+// ORACLE -- test infrastructure, not product code.
+//
+// Scalar C++ restatement of Noor's device render routines, used only by the
+// tests, __graft_entry__.smoke() and bench.py's CPU baseline as the checker.
+// Templated on the scalar type: float is the transcription of the reference
+// routines compiled for the host (compiled with -ffp-contract=off, so every
+// a*b+c rounds twice as the C source is written), double is the FP64 oracle
+// for image RMSE.  Each routine cites the reference file:line it follows
+// (paths relative to the reference project root).  It consumes the same
+// noor_payload / noor_camera / noor_spec / noor_hosek_sky inputs as the
+// CUDA library, reading only the struct layouts from include/noor_b200.h.
+//
+// Parity status: the reference ships no tests or golden vectors.  The BVH
+// builder and Wald precomputation are pinned against the reference's own
+// sources compiled under oracle/_ref; the Hosek fit against the reference's
+// ArHosekSkyModel.cpp compiled under oracle/_ref; the device routines below
+// have no runnable reference (they need an sm_61 GL/CUDA-9 build) and are
+// transcriptions -- "parity unpinned" for those routines beyond this file.
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <thread>
+#include <vector>
+
+#include "../include/noor_b200.h"
+
+#define OR_API extern "C" __attribute__((visibility("default")))
+
+namespace orc {
+
+template <class T>
+struct V {
+    T x, y, z;
+};
+template <class T> inline V<T> mk(T x, T y, T z) { return V<T>{x, y, z}; }
+template <class T> inline V<T> operator+(V<T> a, V<T> b) { return mk(a.x + b.x, a.y + b.y, a.z + b.z); }
+template <class T> inline V<T> operator-(V<T> a, V<T> b) { return mk(a.x - b.x, a.y - b.y, a.z - b.z); }
+template <class T> inline V<T> operator*(V<T> a, V<T> b) { return mk(a.x * b.x, a.y * b.y, a.z * b.z); }
+template <class T> inline V<T> operator/(V<T> a, V<T> b) { return mk(a.x / b.x, a.y / b.y, a.z / b.z); }
+template <class T> inline V<T> operator*(V<T> a, T s) { return mk(a.x * s, a.y * s, a.z * s); }
+template <class T> inline V<T> operator*(T s, V<T> a) { return mk(s * a.x, s * a.y, s * a.z); }
+template <class T> inline V<T> operator/(V<T> a, T s) { return mk(a.x / s, a.y / s, a.z / s); }
+template <class T> inline T dot(V<T> a, V<T> b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+template <class T> inline V<T> cross(V<T> a, V<T> b) {
+    return mk(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+template <class T> inline T len2(V<T> v) { return dot(v, v); }
+template <class T> inline T len(V<T> v) { return std::sqrt(dot(v, v)); }
+// helper_math normalize: v * rsqrt(dot(v,v)); host rsqrt = 1/sqrt
+template <class T> inline V<T> nrm(V<T> v) { return v * (T(1) / std::sqrt(dot(v, v))); }
+// NOOR::normalize (utils.cuh:545-550): zero-length guard
+template <class T> inline V<T> nrm_g(V<T> v) {
+    const T l = len2(v);
+    if (l == T(0)) return v;
+    return v * (T(1) / std::sqrt(l));
+}
+template <class T> inline bool black(V<T> c) { return c.x == 0 && c.y == 0 && c.z == 0; }
+template <class T> inline T clampv(T v, T lo, T hi) { return std::min(std::max(v, lo), hi); }
+template <class T> inline T comp(V<T> v, int i) { return i == 0 ? v.x : (i == 1 ? v.y : v.z); }
+template <class T> inline T maxc(V<T> v) { return std::max(std::max(v.x, v.y), v.z); }
+template <class T> inline T signv(T v) { return (T)((T(0) < v) - (v < T(0))); }
+
+template <class T> struct K {
+    static constexpr T pi = (T)3.14159265358979323846;
+    static constexpr T inv_pi = T(1) / pi;
+    static constexpr T inv_2pi = T(1) / (T(2) * pi);
+    static constexpr T inf = std::numeric_limits<T>::infinity();
+};
+
+inline float u2f(uint32_t u) {
+    float f;
+    std::memcpy(&f, &u, 4);
+    return f;
+}
+inline uint32_t f2u(float f) {
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    return u;
+}
+
+// ---------------------------------------------------------------- RNG
+// noor/cuda/rng.cuh:37-76
+inline uint32_t tea16(uint32_t v0, uint32_t v1) {
+    uint32_t s0 = 0;
+    for (int n = 0; n < 16; n++) {
+        s0 += 0x9e3779b9u;
+        v0 += ((v1 << 4) + 0xa341316cu) ^ (v1 + s0) ^ ((v1 >> 5) + 0xc8013ea4u);
+        v1 += ((v0 << 4) + 0xad90777du) ^ (v0 + s0) ^ ((v0 >> 5) + 0x7e95761eu);
+    }
+    return v0;
+}
+struct Rng {
+    uint32_t s;
+    float next() {
+        s = 1664525u * s + 1013904223u;
+        return (float)(s & 0x00FFFFFFu) / (float)0x01000000;
+    }
+};
+
+// ------------------------------------------------------------ scene view
+struct Scene {
+    const noor_payload* P;
+    const noor_spec* S;
+    const noor_hosek_sky* H;
+    // env distribution (FP64 build, stored in both precisions)
+    int dw = 0, dh = 0;
+    std::vector<double> func, cdf, row_int, marg_cdf;
+    double marg_int = 0;
+    const float* env = nullptr;
+    int ew = 0, eh = 0;
+    int num_lights = 0;
+    bool sky_on = false;
+    // per-material constants resolved from the 1x1 textures
+    struct Mat {
+        float diffuse[3], specular[3], transmission[3], emittance[3], ior[3], k[3];
+        float rx, ry, coat_ior, emitter_scale;
+        uint32_t type, dist;
+    };
+    std::vector<Mat> mats;
+};
+
+// ------------------------------------------------------------ traversal
+template <class T>
+struct TRay {
+    V<T> o, d, inv;
+    int neg[3];
+};
+template <class T> inline void tray(TRay<T>& r, V<T> o, V<T> d) {
+    r.o = o;
+    r.d = d;
+    r.inv = mk(T(1) / d.x, T(1) / d.y, T(1) / d.z);
+    r.neg[0] = d.x > 0 ? 0 : 1;
+    r.neg[1] = d.y > 0 ? 0 : 1;
+    r.neg[2] = d.z > 0 ? 0 : 1;
+}
+// CudaRay::transformToObject (ray.cuh:174-180), CudaTransform (transform.cuh:56-63)
+template <class T> inline void to_object(TRay<T>& r, const TRay<T>& w, const Scene& sc, uint32_t ins) {
+    const noor_payload* P = sc.P;
+    V<T> o, d;
+    T oo[3], dd[3];
+    for (int k = 0; k < 3; ++k) {
+        const float* row = P->world_to_object_row[k] + 4 * (size_t)ins;
+        const T a = row[0], b = row[1], c = row[2], t = row[3];
+        oo[k] = t + ((a * w.o.x + b * w.o.y) + c * w.o.z);
+        dd[k] = (a * w.d.x + b * w.d.y) + c * w.d.z;
+    }
+    o = mk(oo[0], oo[1], oo[2]);
+    d = mk(dd[0], dd[1], dd[2]);
+    tray(r, o, d);
+}
+// CudaBBox::intersect (bbox.cuh:62-80)
+template <class T> inline bool slab(const TRay<T>& r, const uint32_t* lo, const uint32_t* hi, T tmax) {
+    const T mn[3] = {(T)u2f(lo[0]), (T)u2f(lo[1]), (T)u2f(lo[2])};
+    const T mx[3] = {(T)u2f(hi[0]), (T)u2f(hi[1]), (T)u2f(hi[2])};
+    T tMin = ((r.neg[0] ? mx[0] : mn[0]) - r.o.x) * r.inv.x;
+    T tMax = ((r.neg[0] ? mn[0] : mx[0]) - r.o.x) * r.inv.x;
+    const T tyMin = ((r.neg[1] ? mx[1] : mn[1]) - r.o.y) * r.inv.y;
+    const T tyMax = ((r.neg[1] ? mn[1] : mx[1]) - r.o.y) * r.inv.y;
+    if (tMin > tyMax || tyMin > tMax) return false;
+    if (tyMin > tMin) tMin = tyMin;
+    if (tyMax < tMax) tMax = tyMax;
+    const T tzMin = ((r.neg[2] ? mx[2] : mn[2]) - r.o.z) * r.inv.z;
+    const T tzMax = ((r.neg[2] ? mn[2] : mx[2]) - r.o.z) * r.inv.z;
+    if (tMin > tzMax || tzMin > tMax) return false;
+    if (tzMin > tMin) tMin = tzMin;
+    if (tzMax < tMax) tMax = tzMax;
+    return (tMin < tmax) && (tMax > T(0));
+}
+// CudaTriangle::intersect (triangle.cuh:82-141)
+template <class T> inline bool wald(const TRay<T>& r, const Scene& sc, uint32_t ti, T& tmax, T& bu, T& bv,
+                                    uint32_t& mt, uint64_t* ctr) {
+    const uint32_t* a = sc.P->wald_ax_nu_nv_nd + 4 * (size_t)ti;
+    const uint32_t* c = sc.P->wald_cnu_cnv_deg_mat + 4 * (size_t)ti;
+    if (c[2] == 1u) return false;
+    const uint32_t k = a[0];
+    const uint32_t ku = k == 0 ? 1 : (k == 1 ? 2 : 0), kv = k == 0 ? 2 : (k == 1 ? 0 : 1);
+    const T ro_u = comp(r.o, ku), ro_v = comp(r.o, kv), ro_k = comp(r.o, k);
+    const T rd_u = comp(r.d, ku), rd_v = comp(r.d, kv), rd_k = comp(r.d, k);
+    const T nu = u2f(a[1]), nv = u2f(a[2]), nd = u2f(a[3]);
+    const T denom = rd_k + nu * rd_u + nv * rd_v;
+    if (denom == T(0)) return false;
+    const T t = (nd - ro_k - nu * ro_u - nv * ro_v) / denom;
+    if (t < T(0) || t > tmax) return false;
+    if (ctr) ctr[2]++;
+    const uint32_t* b = sc.P->wald_bnu_bnv_au_av + 4 * (size_t)ti;
+    const T hu = ro_u + t * rd_u - (T)u2f(b[2]);
+    const T hv = ro_v + t * rd_v - (T)u2f(b[3]);
+    const T u = hv * (T)u2f(b[0]) + hu * (T)u2f(b[1]);
+    const T v = hu * (T)u2f(c[0]) + hv * (T)u2f(c[1]);
+    if (!(u >= T(0) && v >= T(0) && u + v <= T(1))) return false;
+    tmax = t;
+    bu = u;
+    bv = v;
+    mt = c[3];
+    return true;
+}
+// Woop, Benthin & Wald 2013 watertight test (JCGT 2(1)), same operation order
+// as the device version.
+template <class T> struct WtRay {
+    int kx, ky, kz;
+    T sx, sy, sz;
+};
+template <class T> inline void wt_setup(WtRay<T>& w, V<T> d) {
+    const T ax = std::fabs(d.x), ay = std::fabs(d.y), az = std::fabs(d.z);
+    int kz = (ax > ay) ? (ax > az ? 0 : 2) : (ay > az ? 1 : 2);
+    int kx = kz + 1 == 3 ? 0 : kz + 1;
+    int ky = kx + 1 == 3 ? 0 : kx + 1;
+    const T dz = comp(d, kz);
+    if (dz < T(0)) std::swap(kx, ky);
+    w.kx = kx;
+    w.ky = ky;
+    w.kz = kz;
+    w.sx = comp(d, kx) / dz;
+    w.sy = comp(d, ky) / dz;
+    w.sz = T(1) / dz;
+}
+template <class T> inline T xorsign(T v, bool neg) { return neg ? -v : v; }
+template <class T> inline bool wtt(const TRay<T>& r, const WtRay<T>& w, const Scene& sc, uint32_t ti, T& tmax, T& bu,
+                                   T& bv, uint32_t& mt, uint64_t* ctr) {
+    const uint32_t* at = sc.P->attribute_indices + 4 * (size_t)ti;
+    V<T> p[3];
+    for (int k = 0; k < 3; ++k) {
+        const float* q = sc.P->vertices + 4 * (size_t)at[k];
+        p[k] = mk((T)q[0], (T)q[1], (T)q[2]);
+    }
+    if (ctr) ctr[2]++;
+    const V<T> A = p[0] - r.o, B = p[1] - r.o, C = p[2] - r.o;
+    const T Akz = comp(A, w.kz), Bkz = comp(B, w.kz), Ckz = comp(C, w.kz);
+    const T Ax = comp(A, w.kx) - w.sx * Akz, Ay = comp(A, w.ky) - w.sy * Akz;
+    const T Bx = comp(B, w.kx) - w.sx * Bkz, By = comp(B, w.ky) - w.sy * Bkz;
+    const T Cx = comp(C, w.kx) - w.sx * Ckz, Cy = comp(C, w.ky) - w.sy * Ckz;
+    T U = Cx * By - Cy * Bx;
+    T Vv = Ax * Cy - Ay * Cx;
+    T W = Bx * Ay - By * Ax;
+    if (U == T(0) || Vv == T(0) || W == T(0)) {
+        U = (T)((double)Cx * (double)By - (double)Cy * (double)Bx);
+        Vv = (T)((double)Ax * (double)Cy - (double)Ay * (double)Cx);
+        W = (T)((double)Bx * (double)Ay - (double)By * (double)Ax);
+    }
+    if ((U < T(0) || Vv < T(0) || W < T(0)) && (U > T(0) || Vv > T(0) || W > T(0))) return false;
+    const T det = U + Vv + W;
+    if (det == T(0)) return false;
+    const T Az = w.sz * Akz, Bz = w.sz * Bkz, Cz = w.sz * Ckz;
+    const T Tt = U * Az + Vv * Bz + W * Cz;
+    const bool neg = std::signbit(det);
+    const T Ts = xorsign(Tt, neg);
+    if (Ts < T(0) || Ts > tmax * xorsign(det, neg)) return false;
+    const T rcp = T(1) / det;
+    tmax = Tt * rcp;
+    bu = Vv * rcp;
+    bv = W * rcp;
+    mt = sc.P->wald_cnu_cnv_deg_mat[4 * (size_t)ti + 3];
+    return true;
+}
+// intersectQuad (geometry.cuh:105-123)
+template <class T> inline bool quad_hit(const noor_area_light& L, V<T> o, V<T> d, T& tmax) {
+    const V<T> n = mk((T)L.shape.n[0], (T)L.shape.n[1], (T)L.shape.n[2]);
+    const V<T> c = mk((T)L.shape.center[0], (T)L.shape.center[1], (T)L.shape.center[2]);
+    const V<T> u = mk((T)L.shape.u[0], (T)L.shape.u[1], (T)L.shape.u[2]);
+    const V<T> v = mk((T)L.shape.v[0], (T)L.shape.v[1], (T)L.shape.v[2]);
+    const T denom = dot(n, d);
+    if (denom == T(0)) return false;
+    const T t = -(dot(o, n) - dot(c, n)) / denom;
+    if (t > tmax) return false;
+    const V<T> p = o + t * d;
+    const V<T> ip = p - c;
+    const T t0 = dot(ip, u) / dot(u, u);
+    if (t0 < T(0) || t0 > T(1)) return false;
+    const T t1 = dot(ip, v) / dot(v, v);
+    if (t1 < T(0) || t1 > T(1)) return false;
+    tmax = t;
+    return true;
+}
+
+struct Hit {
+    double u, v;
+    uint32_t tri, ins, mt;
+};
+
+// intersect / intersectP (bvh.cuh:142-234).  ctr (optional): nodes visited,
+// triangles tested, triangles whose t fell in range.
+template <class T>
+bool traverse(const Scene& sc, V<T> o, V<T> d, T& tmax, Hit* rec, bool any, int isect, uint64_t* ctr) {
+    const noor_payload* P = sc.P;
+    TRay<T> wr, lr;
+    tray(wr, o, d);
+    lr = wr;
+    WtRay<T> wt;
+    wt_setup(wt, lr.d);
+    T ltmax = tmax;
+    uint32_t ins = 0;
+    bool hit = false;
+    std::vector<uint32_t> stack;
+    stack.reserve(64);
+    stack.push_back(sc.S->bvh_root_node);
+    while (!stack.empty()) {
+        const uint32_t ni = stack.back();
+        stack.pop_back();
+        if (ctr) ctr[0]++;
+        const uint32_t* lo = P->bvh_min_right_start + 4 * (size_t)ni;
+        const uint32_t* hi = P->bvh_max_axis_count + 4 * (size_t)ni;
+        const uint32_t w1 = hi[3];
+        if (w1 & NOOR_MESH_NODE_MASK) {
+            lr = wr;
+            ltmax = tmax;
+            wt_setup(wt, lr.d);
+        }
+        if (!slab(lr, lo, hi, ltmax)) continue;
+        if (w1 & NOOR_LIGHT_NODE_MASK) {
+            const uint32_t li = w1 & NOOR_LIGHT_MASK;
+            if (any) {
+                T tm = tmax;
+                if (quad_hit(P->area_lights[li], o, d, tm)) return true;
+            } else if (quad_hit(P->area_lights[li], o, d, tmax)) {
+                hit = true;
+                rec->ins = li;
+                rec->mt = NOOR_MESHLIGHT | NOOR_EMITTER;
+            }
+        } else if (w1 & NOOR_MESH_INSTANCE_MASK) {
+            ins = w1 & NOOR_TRANS_MASK;
+            to_object(lr, wr, sc, ins);
+            ltmax = tmax;
+            wt_setup(wt, lr.d);
+            stack.push_back(lo[3]);
+        } else if (w1 & NOOR_MESH_LEAF_MASK) {
+            for (uint32_t i = 1; i <= (w1 & NOOR_COUNT_MASK); ++i) stack.push_back(ni + i);
+        } else if (w1 & NOOR_TRI_LEAF_MASK) {
+            const uint32_t s = lo[3], e = s + (w1 & NOOR_TRI_COUNT_MASK);
+            bool lh = false;
+            for (uint32_t ti = s; ti < e; ++ti) {
+                if (ctr) ctr[1]++;
+                T tm = any ? ltmax : ltmax, bu, bv;
+                uint32_t mt;
+                bool h = isect == NOOR_ISECT_WATERTIGHT ? wtt(lr, wt, sc, ti, tm, bu, bv, mt, ctr)
+                                                        : wald(lr, sc, ti, tm, bu, bv, mt, ctr);
+                if (h) {
+                    if (any) return true;
+                    ltmax = tm;
+                    lh = true;
+                    rec->u = (double)bu;
+                    rec->v = (double)bv;
+                    rec->tri = ti;
+                    rec->mt = mt;
+                }
+            }
+            if (lh) {
+                hit = true;
+                tmax = ltmax;
+                rec->ins = ins;
+            }
+        } else {
+            const uint32_t axis = w1 & NOOR_AXIS_MASK;
+            if (lr.neg[axis]) {
+                stack.push_back(ni + 1);
+                stack.push_back(lo[3]);
+            } else {
+                stack.push_back(lo[3]);
+                stack.push_back(ni + 1);
+            }
+        }
+    }
+    return any ? false : hit;
+}
+
+// ------------------------------------------------------------- shading
+template <class T> struct Frame {
+    V<T> n, s, t, ng;
+};
+template <class T> inline V<T> to_local(const Frame<T>& F, V<T> v) { return mk(dot(v, F.s), dot(v, F.t), dot(v, F.n)); }
+template <class T> inline V<T> to_world(const Frame<T>& F, V<T> v) { return v.x * F.s + v.y * F.t + v.z * F.n; }
+
+// coordinateSystem (utils.cuh:340-347)
+template <class T> inline void coord_sys(V<T> v1, V<T>& v2, V<T>& v3) {
+    if (std::fabs(v1.x) > std::fabs(v1.y))
+        v2 = mk(-v1.z, T(0), v1.x) / std::sqrt(v1.x * v1.x + v1.z * v1.z);
+    else
+        v2 = mk(T(0), v1.z, -v1.y) / std::sqrt(v1.y * v1.y + v1.z * v1.z);
+    v3 = cross(v1, v2);
+}
+
+// computeTangentSpace (intersection.cuh:325-377)
+template <class T> Frame<T> tangent(const Scene& sc, const Hit& h) {
+    const noor_payload* P = sc.P;
+    const uint32_t* a = P->attribute_indices + 4 * (size_t)h.tri;
+    auto vtx = [&](uint32_t i) { const float* q = P->vertices + 4 * (size_t)i; return mk((T)q[0], (T)q[1], (T)q[2]); };
+    auto nrmv = [&](uint32_t i) { const float* q = P->normals + 4 * (size_t)i; return mk((T)q[0], (T)q[1], (T)q[2]); };
+    auto uv = [&](uint32_t i, T& x, T& y) { const float* q = P->uvs + 2 * (size_t)i; x = q[0]; y = T(1) - (T)q[1]; };
+    T u0x, u0y, u1x, u1y, u2x, u2y;
+    uv(a[0], u0x, u0y);
+    uv(a[1], u1x, u1y);
+    uv(a[2], u2x, u2y);
+    const V<T> v0 = vtx(a[0]), v1 = vtx(a[1]), v2 = vtx(a[2]);
+    const V<T> n0 = nrmv(a[0]), n1 = nrmv(a[1]), n2 = nrmv(a[2]);
+    const T bu = (T)h.u, bv = (T)h.v;
+    const T w = T(1) - bu - bv;
+    const V<T> ni = w * n0 + bu * n1 + bv * n2;
+    auto rowmul = [&](const float* const* rows, V<T> x) {
+        T r[3];
+        for (int k = 0; k < 3; ++k) {
+            const float* q = rows[k] + 4 * (size_t)h.ins;
+            r[k] = (T)q[0] * x.x + (T)q[1] * x.y + (T)q[2] * x.z;
+        }
+        return mk(r[0], r[1], r[2]);
+    };
+    Frame<T> F;
+    F.n = nrm_g(nrm(rowmul(P->normal_row, ni)));
+    const V<T> dp01 = rowmul(P->object_to_world_row, v1 - v0);
+    const V<T> dp02 = rowmul(P->object_to_world_row, v2 - v0);
+    F.ng = nrm_g(cross(dp01, dp02));
+    const T d1x = u1x - u0x, d1y = u1y - u0y, d2x = u2x - u0x, d2y = u2y - u0y;
+    const T det = d1x * d2y - d2x * d1y;
+    V<T> dpdu, dpdv;
+    if (!(std::fabs(det) < (T)1e-8f)) {
+        const T inv = T(1) / det;
+        const T a00 = d2y * inv, a01 = -d1y * inv, a10 = -d2x * inv, a11 = d1x * inv;
+        dpdu = a00 * dp01 + a01 * dp02;
+        dpdv = a10 * dp01 + a11 * dp02;
+        if (len2(cross(dpdu, dpdv)) == T(0)) coord_sys(F.ng, dpdu, dpdv);
+    } else {
+        coord_sys(F.ng, dpdu, dpdv);
+    }
+    F.s = nrm_g(dpdu - F.n * dot(F.n, dpdu));
+    const T sg = dot(cross(F.n, F.s), dpdv) < T(0) ? T(-1) : T(1);
+    F.t = nrm_g(sg * cross(F.n, F.s));
+    return F;
+}
+
+// bxdf.cuh:58-96
+template <class T> inline T c2t(V<T> w) { return w.z * w.z; }
+template <class T> inline T s2t(V<T> w) { return std::max(T(0), T(1) - c2t(w)); }
+template <class T> inline T st_(V<T> w) { return std::sqrt(s2t(w)); }
+template <class T> inline T tnt(V<T> w) { return st_(w) / w.z; }
+template <class T> inline T t2t(V<T> w) { return s2t(w) / c2t(w); }
+template <class T> inline T cph(V<T> w) { const T s = st_(w); return s == T(0) ? T(1) : clampv(w.x / s, T(-1), T(1)); }
+template <class T> inline T sph(V<T> w) { const T s = st_(w); return s == T(0) ? T(0) : clampv(w.y / s, T(-1), T(1)); }
+template <class T> inline T c2p(V<T> w) { return cph(w) * cph(w); }
+template <class T> inline T s2p(V<T> w) { return sph(w) * sph(w); }
+template <class T> inline bool same(V<T> a, V<T> b) { return a.z * b.z > T(0); }
+
+// fresnel.cuh:58-107
+template <class T> T fr_diel(T ci, T ei, T et) {
+    ci = clampv(ci, T(-1), T(1));
+    if (!(ci > T(0))) {
+        std::swap(ei, et);
+        ci = std::fabs(ci);
+    }
+    const T si = std::sqrt(std::max(T(0), T(1) - ci * ci));
+    const T st = ei / et * si;
+    if (st >= T(1)) return T(1);
+    const T ct = std::sqrt(std::max(T(0), T(1) - st * st));
+    const T rpa = ((et * ci) - (ei * ct)) / ((et * ci) + (ei * ct));
+    const T rpe = ((ei * ci) - (et * ct)) / ((ei * ci) + (et * ct));
+    return (rpa * rpa + rpe * rpe) / T(2);
+}
+template <class T> V<T> sq3(V<T> v) { return mk(std::sqrt(v.x), std::sqrt(v.y), std::sqrt(v.z)); }
+template <class T> V<T> fr_cond(T ci, V<T> etaT, V<T> k) {
+    ci = clampv(ci, T(-1), T(1));
+    const V<T> one = mk(T(1), T(1), T(1));
+    const V<T> eta = etaT / one, etak = k / one;
+    const T c2 = ci * ci, s2 = T(1) - c2;
+    const V<T> eta2 = eta * eta, etak2 = etak * etak;
+    const V<T> t0 = eta2 - etak2 - mk(s2, s2, s2);
+    const V<T> a2b2 = sq3(t0 * t0 + T(4) * eta2 * etak2);
+    const V<T> t1 = a2b2 + mk(c2, c2, c2);
+    const V<T> a = sq3(T(0.5) * (a2b2 + t0));
+    const V<T> t2 = T(2) * ci * a;
+    const V<T> Rs = (t1 - t2) / (t1 + t2);
+    const V<T> t3 = c2 * a2b2 + mk(s2 * s2, s2 * s2, s2 * s2);
+    const V<T> t4 = t2 * s2;
+    const V<T> Rp = Rs * (t3 - t4) / (t3 + t4);
+    return T(0.5) * (Rp + Rs);
+}
+
+// distribution.cuh:58-342
+template <class T> T erf_as(T x) {
+    const T a1 = (T)0.254829592f, a2 = (T)-0.284496736f, a3 = (T)1.421413741f, a4 = (T)-1.453152027f,
+            a5 = (T)1.061405429f, p = (T)0.3275911f;
+    const int sg = x < T(0) ? -1 : 1;
+    x = std::fabs(x);
+    const T t = T(1) / (T(1) + p * x);
+    const T y = T(1) - (((((a5 * t + a4) * t) + a3) * t + a2) * t + a1) * t * std::exp(-x * x);
+    return (T)sg * y;
+}
+template <class T> T erfinv_g(T x) {
+    T w, p;
+    x = clampv(x, (T)-.99999f, (T).99999f);
+    w = -std::log((T(1) - x) * (T(1) + x));
+    if (w < T(5)) {
+        w = w - (T)2.5f;
+        p = (T)2.81022636e-08f;
+        p = (T)3.43273939e-07f + p * w;
+        p = (T)-3.5233877e-06f + p * w;
+        p = (T)-4.39150654e-06f + p * w;
+        p = (T)0.00021858087f + p * w;
+        p = (T)-0.00125372503f + p * w;
+        p = (T)-0.00417768164f + p * w;
+        p = (T)0.246640727f + p * w;
+        p = (T)1.50140941f + p * w;
+    } else {
+        w = std::sqrt(w) - T(3);
+        p = (T)-0.000200214257f;
+        p = (T)0.000100950558f + p * w;
+        p = (T)0.00134934322f + p * w;
+        p = (T)-0.00367342844f + p * w;
+        p = (T)0.00573950773f + p * w;
+        p = (T)-0.0076224613f + p * w;
+        p = (T)0.00943887047f + p * w;
+        p = (T)1.00167406f + p * w;
+        p = (T)2.83297682f + p * w;
+    }
+    return p * x;
+}
+template <class T> struct Micro {
+    T ax, ay;
+    uint32_t dist;
+    T D(V<T> wh) const {
+        const T t2 = t2t(wh);
+        if (std::isinf(t2)) return T(0);
+        const T c4 = c2t(wh) * c2t(wh);
+        if (dist) return std::exp(-t2 * (c2p(wh) / (ax * ax) + s2p(wh) / (ay * ay))) / (K<T>::pi * ax * ay * c4);
+        const T e = (c2p(wh) / (ax * ax) + s2p(wh) / (ay * ay)) * t2;
+        return T(1) / (K<T>::pi * ax * ay * c4 * (T(1) + e) * (T(1) + e));
+    }
+    T lambda(V<T> w) const {
+        const T at = std::fabs(tnt(w));
+        if (std::isinf(at)) return T(0);
+        const T alpha = std::sqrt(c2p(w) * ax * ax + s2p(w) * ay * ay);
+        if (dist) {
+            const T a = T(1) / (alpha * at);
+            if (a >= (T)1.6f) return T(0);
+            return (T(1) - (T)1.259f * a + (T)0.396f * a * a) / ((T)3.535f * a + (T)2.181f * a * a);
+        }
+        const T a2t2 = (alpha * at) * (alpha * at);
+        return (T(-1) + std::sqrt(T(1) + a2t2)) / T(2);
+    }
+    T G(V<T> wo, V<T> wi) const { return T(1) / (T(1) + lambda(wo) + lambda(wi)); }
+    T G1(V<T> w) const { return T(1) / (T(1) + lambda(w)); }
+    T pdf(V<T> wo, V<T> wh) const { return D(wh) * G1(wo) * std::fabs(dot(wo, wh)) / std::fabs(wo.z); }
+    void s11_tr(T ct, T U1, T U2, T& sx, T& sy) const {
+        if (ct > (T).9999f) {
+            const T r = std::sqrt(U1 / (T(1) - U1));
+            const T phi = (T)6.28318530718f * U2;
+            sx = r * std::cos(phi);
+            sy = r * std::sin(phi);
+            return;
+        }
+        const T s = std::sqrt(std::max(T(0), T(1) - ct * ct));
+        const T tn = s / ct;
+        const T a = T(1) / tn;
+        const T G1v = T(2) / (T(1) + std::sqrt(T(1) + T(1) / (a * a)));
+        const T A = T(2) * U1 / G1v - T(1);
+        T tmp = T(1) / (A * A - T(1));
+        if (tmp > (T)1e10f) tmp = (T)1e10f;
+        const T B = tn;
+        const T Dd = std::sqrt(std::max(B * B * tmp * tmp - (A * A - B * B) * tmp, T(0)));
+        const T x1 = B * tmp - Dd, x2 = B * tmp + Dd;
+        sx = (A < T(0) || x2 > T(1) / tn) ? x1 : x2;
+        T S;
+        if (U2 > (T)0.5f) {
+            S = T(1);
+            U2 = T(2) * (U2 - (T).5f);
+        } else {
+            S = T(-1);
+            U2 = T(2) * ((T).5f - U2);
+        }
+        const T z = (U2 * (U2 * (U2 * (T)0.27385f - (T)0.73369f) + (T)0.46341f)) /
+                    (U2 * (U2 * (U2 * (T)0.093073f + (T)0.309420f) - (T)1.000000f) + (T)0.597999f);
+        sy = S * z * std::sqrt(T(1) + sx * sx);
+    }
+    void s11_bk(T ci, T U1, T U2, T& sx, T& sy) const {
+        if (ci > (T).9999f) {
+            const T r = std::sqrt(-std::log(T(1) - U1));
+            sx = r * std::cos(T(2) * K<T>::pi * U2);
+            sy = r * std::sin(T(2) * K<T>::pi * U2);
+            return;
+        }
+        const T si = std::sqrt(std::max(T(0), T(1) - ci * ci));
+        const T ti = si / ci, coti = T(1) / ti;
+        T a = T(-1), c = erf_as(coti);
+        const T sxx = std::max(U1, (T)1e-6f);
+        const T th = std::acos(ci);
+        const T fit = T(1) + th * ((T)-0.876f + th * ((T)0.4265f - (T)0.0594f * th));
+        T b = c - (T(1) + c) * std::pow(T(1) - sxx, fit);
+        const T nz = T(1) / (T(1) + c + std::sqrt(K<T>::inv_pi) * ti * std::exp(-coti * coti));
+        int it = 0;
+        while (++it < 10) {
+            if (!(b >= a && b <= c)) b = (T)0.5f * (a + c);
+            const T ie = erfinv_g(b);
+            const T val = nz * (T(1) + b + std::sqrt(K<T>::inv_pi) * ti * std::exp(-ie * ie)) - sxx;
+            const T der = nz * (T(1) - ie * ti);
+            if (std::fabs(val) < (T)1e-5f) break;
+            if (val > T(0)) c = b; else a = b;
+            b -= val / der;
+        }
+        sx = erfinv_g(b);
+        sy = erfinv_g(T(2) * std::max(U2, (T)1e-6f) - T(1));
+    }
+    V<T> vis(V<T> wi, T U1, T U2) const {
+        const V<T> ws = nrm(mk(ax * wi.x, ay * wi.y, wi.z));
+        T sx, sy;
+        if (dist) s11_bk(ws.z, U1, U2, sx, sy); else s11_tr(ws.z, U1, U2, sx, sy);
+        const T tmp = cph(ws) * sx - sph(ws) * sy;
+        sy = sph(ws) * sx + cph(ws) * sy;
+        sx = tmp;
+        sx *= ax;
+        sy *= ay;
+        return nrm(mk(-sx, -sy, T(1)));
+    }
+    V<T> sample_wh(V<T> wo, T u1, T u2) const {
+        if (dist) {
+            const bool flip = wo.z < T(0);
+            V<T> wh = vis(flip ? T(-1) * wo : wo, u1, u2);
+            return flip ? T(-1) * wh : wh;
+        }
+        const T s = signv(wo.z);
+        return s * vis(s * wo, u1, u2);
+    }
+};
+
+enum : uint32_t {
+    B_REFL = 1u, B_TRANS = 2u, B_DIFF = 4u, B_GLOSSY = 8u, B_SPEC = 16u, B_COND = 32u, B_DIEL = 64u, B_ALL = 0xFFu
+};
+const uint32_t kLambert = B_REFL | B_DIFF | B_DIEL, kCond = B_COND | B_REFL | B_GLOSSY,
+               kFSpec = B_REFL | B_TRANS | B_SPEC | B_DIEL;
+const uint32_t kSpecMat = NOOR_MIRROR | NOOR_GLASS | NOOR_CLEARCOAT;
+const uint32_t kTranspMat = NOOR_TRANSLUCENT | NOOR_GLASS | NOOR_ROUGHGLASS;
+const uint32_t kEmitMat = NOOR_EMITTER | NOOR_MESHLIGHT;
+
+// factoryBSDF (bsdf.cuh:425-461)
+inline uint32_t lobe_of(uint32_t mt) {
+    const uint32_t t = mt & ~(uint32_t)(NOOR_BUMP | NOOR_ALPHA);
+    if (t == NOOR_DIFFUSE) return kLambert;
+    if (t == NOOR_METAL) return kCond;
+    if (t == NOOR_GLASS) return kFSpec;
+    return 0u;
+}
+inline bool matches(uint32_t lobe, uint32_t flags) { return lobe && (lobe & flags) == lobe; }
+template <class T> V<T> v3f(const float* f) { return mk((T)f[0], (T)f[1], (T)f[2]); }
+
+template <class T> Micro<T> micro(const Scene::Mat& m) {
+    Micro<T> mf;
+    mf.ax = std::max((T)m.rx * (T)m.rx, (T)1e-3f);
+    mf.ay = std::max((T)m.ry * (T)m.ry, (T)1e-3f);
+    mf.dist = m.dist;
+    return mf;
+}
+// BxDF Eval/Pdf/Sample_f of bxdf.cuh:252-299 (Lambert), 472-557
+// (MicrofacetReflection, conductor), 754-839 (FresnelSpecular)
+template <class T> V<T> lobe_eval(uint32_t lobe, const Scene::Mat& m, V<T> wo, V<T> wi) {
+    if (lobe == kLambert) return v3f<T>(m.diffuse) * K<T>::inv_pi;
+    if (lobe == kCond) {
+        if (!same(wo, wi)) return mk(T(0), T(0), T(0));
+        const T cO = std::fabs(wo.z), cI = std::fabs(wi.z);
+        if (cI == T(0) || cO == T(0)) return mk(T(0), T(0), T(0));
+        V<T> wh = nrm(wi + wo);
+        if (black(wh)) return mk(T(0), T(0), T(0));
+        wh = wh * signv(wh.z);
+        const V<T> F = fr_cond(dot(wo, wh), v3f<T>(m.ior), v3f<T>(m.k));
+        const Micro<T> mf = micro<T>(m);
+        return F * v3f<T>(m.specular) * mf.D(wh) * mf.G(wo, wi) / (T(4) * cI * cO);
+    }
+    return mk(T(0), T(0), T(0));
+}
+template <class T> T lobe_pdf(uint32_t lobe, const Scene::Mat& m, V<T> wo, V<T> wi) {
+    if (lobe == kLambert) return same(wo, wi) ? std::fabs(wi.z) * K<T>::inv_pi : T(0);
+    if (lobe == kCond) {
+        if (!same(wo, wi)) return T(0);
+        const V<T> wh = nrm_g(wo + wi);
+        const Micro<T> mf = micro<T>(m);
+        return mf.pdf(wo, wh) / (T(4) * dot(wo, wh));
+    }
+    return T(0);
+}
+// concentricSampleDisk / cosineSampleHemisphere (utils.cuh:377-404)
+template <class T> V<T> cos_hemi(T ux, T uy) {
+    const T ox = T(2) * ux - T(1), oy = T(2) * uy - T(1);
+    T dx = 0, dy = 0;
+    if (!(ox == T(0) && oy == T(0))) {
+        T th, r;
+        if (std::fabs(ox) > std::fabs(oy)) {
+            r = ox;
+            th = (K<T>::pi / T(4)) * (oy / ox);
+        } else {
+            r = oy;
+            th = (K<T>::pi / T(2)) - (K<T>::pi / T(4)) * (ox / oy);
+        }
+        dx = r * std::cos(th);
+        dy = r * std::sin(th);
+    }
+    return mk(dx, dy, std::sqrt(std::max(T(0), T(1) - dx * dx - dy * dy)));
+}
+template <class T> V<T> lobe_sample(uint32_t lobe, const Scene::Mat& m, V<T> wo, T ux, T uy, V<T>& wi, T& pdf,
+                                    uint32_t& st) {
+    st = lobe;
+    const V<T> zero = mk(T(0), T(0), T(0));
+    if (lobe == kLambert) {
+        wi = cos_hemi(ux, uy);
+        if (wo.z < T(0)) wi.z = wi.z * T(-1);
+        pdf = same(wo, wi) ? std::fabs(wi.z) * K<T>::inv_pi : T(0);
+        return v3f<T>(m.diffuse) * K<T>::inv_pi;
+    }
+    if (lobe == kCond) {
+        if (wo.z == T(0)) return zero;
+        const Micro<T> mf = micro<T>(m);
+        const V<T> wh = mf.sample_wh(wo, ux, uy);
+        wi = T(-1) * wo + T(2) * dot(wo, wh) * wh;
+        if (!same(wo, wi)) {
+            pdf = T(0);
+            return zero;
+        }
+        pdf = mf.pdf(wo, wh) / (T(4) * dot(wo, wh));
+        return lobe_eval<T>(lobe, m, wo, wi);
+    }
+    if (lobe == kFSpec) {
+        const T ior = (T)m.coat_ior;
+        const T F = fr_diel(wo.z, T(1), ior);
+        if (ux < F) {
+            wi = mk(-wo.x, -wo.y, wo.z);
+            pdf = F;
+            st = B_REFL | B_SPEC;
+            return F * v3f<T>(m.specular) / std::fabs(wi.z);
+        }
+        const bool entering = wo.z > T(0);
+        const T eta = entering ? (T(1) / ior) : (ior / T(1));
+        const V<T> n = dot(wo, mk(T(0), T(0), T(1))) < T(0) ? mk(T(0), T(0), T(-1)) : mk(T(0), T(0), T(1));
+        const T ci = dot(n, wo);
+        const T s2i = std::max(T(0), T(1) - ci * ci);
+        const T s2t = eta * eta * s2i;
+        if (s2t >= T(1)) return zero;
+        const T ct = std::sqrt(T(1) - s2t);
+        wi = (-eta) * wo + (eta * ci - ct) * n;
+        pdf = T(1) - F;
+        st = B_TRANS | B_SPEC;
+        return v3f<T>(m.transmission) * eta * eta * (T(1) - F) / std::fabs(wi.z);
+    }
+    return zero;
+}
+// CudaBSDF (bsdf.cuh:252-358) over the single lobe
+template <class T> V<T> bsdf_eval(uint32_t lobe, const Scene::Mat& m, const Frame<T>& F, V<T> woW, V<T> wiW,
+                                  uint32_t flags) {
+    const V<T> wo = to_local(F, woW), wi = to_local(F, wiW);
+    const bool refl = dot(wiW, F.ng) * dot(woW, F.ng) > T(0);
+    if (matches(lobe, flags) && ((refl && (lobe & B_REFL)) || (!refl && (lobe & B_TRANS))))
+        return lobe_eval<T>(lobe, m, wo, wi);
+    return mk(T(0), T(0), T(0));
+}
+template <class T> T bsdf_pdf(uint32_t lobe, const Scene::Mat& m, const Frame<T>& F, V<T> woW, V<T> wiW,
+                              uint32_t flags) {
+    if (!lobe) return T(0);
+    const V<T> wo = to_local(F, woW), wi = to_local(F, wiW);
+    if (wo.z == T(0)) return T(0);
+    return matches(lobe, flags) ? lobe_pdf<T>(lobe, m, wo, wi) : T(0);
+}
+template <class T> V<T> bsdf_sample(uint32_t lobe, const Scene::Mat& m, const Frame<T>& F, V<T> woW, uint32_t flags,
+                                    Rng& rng, V<T>& wiW, T& pdf, uint32_t& st) {
+    pdf = T(0);
+    st = 0;
+    const V<T> zero = mk(T(0), T(0), T(0));
+    if (!matches(lobe, flags)) return zero;
+    const float ux = rng.next();
+    const float uy = rng.next();
+    const float uxr = std::min(ux * 1.0f - 0.0f, 1.0f - std::numeric_limits<float>::epsilon());
+    const V<T> wo = to_local(F, woW);
+    if (wo.z == T(0)) return zero;
+    V<T> wi = zero;
+    uint32_t s;
+    const V<T> f = lobe_sample<T>(lobe, m, wo, (T)uxr, (T)uy, wi, pdf, s);
+    if (pdf == T(0)) return zero;
+    st = s;
+    wiW = to_world(F, wi);
+    return f;
+}
+
+// ----------------------------------------------------------- sky & env
+// hosek.cuh:68-101
+template <class T> T hosek_int(const float* c, T th, T ga) {
+    const T cg = std::cos(ga), cg2 = cg * cg, ct = std::cos(th);
+    const T expM = std::exp((T)c[4] * ga);
+    const T mieM = (T(1) + cg2) / std::pow(T(1) + (T)c[8] * (T)c[8] - T(2) * (T)c[8] * cg, (T)1.5);
+    return (T(1) + (T)c[0] * std::exp((T)c[1] / (ct + (T)0.01f))) *
+           ((T)c[2] + (T)c[3] * expM + (T)c[5] * cg2 + (T)c[6] * mieM + (T)c[7] * std::sqrt(ct));
+}
+template <class T> T inv_gamma(T v) {
+    if (v <= (T)0.04045f) return v * T(1) / (T)12.92f;
+    return std::pow((v + (T)0.055f) * T(1) / (T)1.055f, (T)2.4f);
+}
+template <class T> T sph_theta(V<T> v) { return std::acos(clampv(v.y, T(-1), T(1))); }
+template <class T> T sph_phi(V<T> v) {
+    const T p = std::atan2(v.z, v.x);
+    return p < T(0) ? p + T(2) * K<T>::pi : p;
+}
+template <class T> V<T> hosek(const noor_hosek_sky& H, V<T> v) {
+    if (v.y < T(0)) return mk(T(0), T(0), T(0));
+    const T th = clampv(sph_theta(v), T(0), K<T>::pi / T(2));
+    const V<T> sd = v3f<T>(H.solar_dir);
+    const T ga = std::acos(clampv(dot(v, sd), T(-1), T(1)));
+    V<T> rgb = mk(hosek_int(H.state[0].configs[0], th, ga) * (T)H.state[0].radiances[0],
+                  hosek_int(H.state[1].configs[1], th, ga) * (T)H.state[1].radiances[1],
+                  hosek_int(H.state[2].configs[2], th, ga) * (T)H.state[2].radiances[2]);
+    if (ga < (T)H.solar_radius) return (T)H.solar_scale * rgb;
+    const V<T> s = rgb * (T)0.025f;
+    return mk(inv_gamma(s.x), inv_gamma(s.y), inv_gamma(s.z));
+}
+template <class T> V<T> env_bilinear(const Scene& sc, T u, T v) {
+    const int W = sc.ew, H = sc.eh;
+    const T x = u * (T)W - (T)0.5, y = v * (T)H - (T)0.5;
+    const T fx0 = std::floor(x), fy0 = std::floor(y);
+    const T ax = x - fx0, ay = y - fy0;
+    int x0 = (int)fx0, y0 = (int)fy0, x1 = x0 + 1, y1 = y0 + 1;
+    x0 = std::min(std::max(x0, 0), W - 1);
+    x1 = std::min(std::max(x1, 0), W - 1);
+    y0 = std::min(std::max(y0, 0), H - 1);
+    y1 = std::min(std::max(y1, 0), H - 1);
+    auto tx = [&](int xx, int yy) { return v3f<T>(sc.env + 4 * ((size_t)yy * W + xx)); };
+    return ((T(1) - ax) * (T(1) - ay)) * tx(x0, y0) + (ax * (T(1) - ay)) * tx(x1, y0) +
+           ((T(1) - ax) * ay) * tx(x0, y1) + (ax * ay) * tx(x1, y1);
+}
+template <class T> V<T> env_eval(const Scene& sc, V<T> dir) {
+    if (sc.S->skydome_type == NOOR_SKY_PHYSICAL) return hosek<T>(*sc.H, dir);
+    return env_bilinear<T>(sc, sph_phi(dir) * K<T>::inv_2pi, sph_theta(dir) * K<T>::inv_pi);
+}
+inline double lum(double r, double g, double b) { return (double)(0.2126f) * r + (double)(0.7152f) * g + (double)(0.0722f) * b; }
+
+// env distribution: PBRT-v3 Distribution2D over luminance x sin(theta)
+// (the build's definition; the reference's is noor/cuda/distribution2d.cuh)
+void build_dist(Scene& sc) {
+    const bool sky = sc.S->skydome_type == NOOR_SKY_PHYSICAL;
+    const int w = sky ? 2048 : sc.ew, h = sky ? 1024 : sc.eh;
+    sc.dw = w;
+    sc.dh = h;
+    sc.func.assign((size_t)w * h, 0.0);
+    for (int j = 0; j < h; ++j)
+        for (int i = 0; i < w; ++i) {
+            double f = 0;
+            if (sky) {
+                float acc = 0.0f;
+                for (int b = 0; b < 4; ++b) {
+                    const float v = ((float)j + ((float)b + 0.5f) * 0.25f) / (float)h;
+                    const float th = v * K<float>::pi;
+                    const float st = std::sin(th), ct = std::cos(th);
+                    for (int a = 0; a < 4; ++a) {
+                        const float u = ((float)i + ((float)a + 0.5f) * 0.25f) / (float)w;
+                        const float ph = u * 2.0f * K<float>::pi;
+                        const V<float> d = nrm(mk(st * std::cos(ph), ct, st * std::sin(ph)));
+                        const V<float> c = hosek<float>(*sc.H, d);
+                        acc += std::max(0.0f, (float)lum(c.x, c.y, c.z)) * st;
+                    }
+                }
+                f = acc * (1.0f / 16.0f);
+            } else {
+                const float* t = sc.env + 4 * ((size_t)j * w + i);
+                const float st = std::sin(((float)j + 0.5f) / (float)h * K<float>::pi);
+                const float y = 0.2126f * t[0] + 0.7152f * t[1] + 0.0722f * t[2];
+                f = std::max(0.0f, y) * st;
+            }
+            sc.func[(size_t)j * w + i] = (double)(float)f;
+        }
+    sc.cdf.assign((size_t)h * (w + 1), 0.0);
+    sc.row_int.assign(h, 0.0);
+    for (int j = 0; j < h; ++j) {
+        double* c = sc.cdf.data() + (size_t)j * (w + 1);
+        for (int i = 0; i < w; ++i) c[i + 1] = c[i] + sc.func[(size_t)j * w + i] / w;
+        const double tot = c[w];
+        sc.row_int[j] = tot;
+        for (int i = 0; i <= w; ++i) c[i] = tot > 0 ? c[i] / tot : (double)i / w;
+    }
+    sc.marg_cdf.assign(h + 1, 0.0);
+    for (int j = 0; j < h; ++j) sc.marg_cdf[j + 1] = sc.marg_cdf[j] + sc.row_int[j] / h;
+    sc.marg_int = sc.marg_cdf[h];
+    for (int j = 0; j <= h; ++j) sc.marg_cdf[j] = sc.marg_int > 0 ? sc.marg_cdf[j] / sc.marg_int : (double)j / h;
+}
+template <class T> T sample1d(const double* func, const double* cdf, int n, double integral, T u, T& pdf, int& off) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if ((T)cdf[mid] <= u) lo = mid; else hi = mid - 1;
+    }
+    off = std::min(lo, n - 1);
+    const T c0 = (T)cdf[off], c1 = (T)cdf[off + 1];
+    T du = u - c0;
+    if (c1 - c0 > T(0)) du /= (c1 - c0);
+    pdf = integral > 0 ? (T)func[off] / (T)integral : T(0);
+    return ((T)off + du) / (T)n;
+}
+template <class T> void dist_sample(const Scene& sc, T u0, T u1, T& x, T& y, T& pdf) {
+    T pv, pu;
+    int row, col;
+    y = sample1d<T>(sc.row_int.data(), sc.marg_cdf.data(), sc.dh, sc.marg_int, u1, pv, row);
+    x = sample1d<T>(sc.func.data() + (size_t)row * sc.dw, sc.cdf.data() + (size_t)row * (sc.dw + 1), sc.dw,
+                    sc.row_int[row], u0, pu, col);
+    pdf = pu * pv;
+}
+template <class T> T dist_pdf(const Scene& sc, T x, T y) {
+    const int iu = std::min(std::max((int)(x * sc.dw), 0), sc.dw - 1);
+    const int iv = std::min(std::max((int)(y * sc.dh), 0), sc.dh - 1);
+    return sc.marg_int > 0 ? (T)sc.func[(size_t)iv * sc.dw + iu] / (T)sc.marg_int : T(0);
+}
+template <class T> V<T> env_sample_dir(const Scene& sc, Rng& rng, T& pdf) {
+    const T u0 = rng.next(), u1 = rng.next();
+    T x, y, mp;
+    dist_sample<T>(sc, u0, u1, x, y, mp);
+    const T ph = x * T(2) * K<T>::pi, th = y * K<T>::pi;
+    const T ct = std::cos(th), st = std::sin(th);
+    const V<T> d = nrm(mk(st * std::cos(ph), ct, st * std::sin(ph)));
+    pdf = st == T(0) ? T(0) : mp / (T(2) * K<T>::pi * K<T>::pi * st);
+    return d;
+}
+template <class T> T env_pdf(const Scene& sc, V<T> wi) {
+    if (!sc.sky_on) return T(0);
+    const T th = sph_theta(wi), ph = sph_phi(wi), st = std::sin(th);
+    if (st == T(0)) return T(0);
+    return dist_pdf<T>(sc, ph * K<T>::inv_2pi, th * K<T>::inv_pi) / (T(2) * K<T>::pi * K<T>::pi * st);
+}
+
+// ----------------------------------------------------------- integrator
+template <class T> struct Is {
+    V<T> p, wo;
+    Frame<T> F;
+    uint32_t mt, lobe, mat;
+};
+template <class T> V<T> spawn(const Is<T>& I, V<T> dir, T bias) {
+    return dot(dir, I.F.ng) >= T(0) ? I.p + bias * I.F.ng : I.p - bias * I.F.ng;
+}
+template <class T> V<T> area_p(const noor_area_light& A, int which) {
+    return which == 0 ? v3f<T>(A.shape.center) : (which == 1 ? v3f<T>(A.shape.u) : (which == 2 ? v3f<T>(A.shape.v) : v3f<T>(A.shape.n)));
+}
+
+struct Counters {
+    uint64_t ext = 0, shadow = 0, nodes = 0, tris = 0, tri_in_range = 0;
+};
+
+template <class T> bool occl(const Scene& sc, V<T> o, V<T> d, T tmax, int isect, Counters* c) {
+    uint64_t ctr[3] = {0, 0, 0};
+    if (c) c->shadow++;
+    const bool r = traverse<T>(sc, o, d, tmax, nullptr, true, isect, c ? ctr : nullptr);
+    if (c) {
+        c->nodes += ctr[0];
+        c->tris += ctr[1];
+        c->tri_in_range += ctr[2];
+    }
+    return r;
+}
+
+// sampleLight / sampleBSDF (direct.cuh:32-110) with the build's stated
+// choices for the unpicked-light case (no BSDF half, no draws)
+template <class T>
+V<T> direct(const Scene& sc, const Scene::Mat& m, const Is<T>& I, Rng& rng, int isect, Counters* c) {
+    const V<T> zero = mk(T(0), T(0), T(0));
+    if (I.mt & kSpecMat) return zero;
+    const int nl = sc.sky_on ? sc.num_lights : sc.num_lights - 1;
+    if (nl == 0) return zero;
+    const T bias = (T)sc.S->reflection_bias;
+    const bool mis = sc.S->mis != 0;
+    const int li = (int)((float)nl * rng.next());
+    const int na = sc.P->num_area_lights;
+    const uint32_t nonspec = B_ALL & ~B_SPEC;
+    V<T> Ld = zero;
+    {
+        V<T> Li = zero, wi = zero, to = zero;
+        T lpdf = 0;
+        if (li < na) {
+            const noor_area_light& A = sc.P->area_lights[li];
+            const float r1 = rng.next();
+            const float r2 = rng.next();
+            const V<T> n = area_p<T>(A, 3);
+            const V<T> p = area_p<T>(A, 0) + area_p<T>(A, 1) * (T)r1 + area_p<T>(A, 2) * (T)r2 + bias * n;
+            const V<T> w = I.p - p;
+            lpdf = len2(w) / (std::fabs(dot(n, T(-1) * w)) * (T)A.shape.area);
+            if (std::isinf(lpdf)) lpdf = 0;
+            if (lpdf != T(0)) {
+                to = p;
+                const V<T> v = to - I.p;
+                wi = v / len(v);
+                Li = (A.two_sided || dot(wi, n) < T(0)) ? v3f<T>(A.ke) : zero;
+            }
+        } else {
+            const V<T> dir = env_sample_dir<T>(sc, rng, lpdf);
+            if (std::isinf(lpdf) || std::isnan(lpdf)) lpdf = 0;
+            to = I.p + T(2) * (T)sc.S->world_radius * dir;
+            const V<T> v = to - I.p;
+            wi = v / len(v);
+            Li = sc.sky_on ? env_eval<T>(sc, wi) : zero;
+        }
+        Li = Li * (T)nl;
+        if (lpdf != T(0) && !black(Li)) {
+            V<T> f = bsdf_eval<T>(I.lobe, m, I.F, I.wo, wi, nonspec);
+            if (!black(f)) {
+                f = f * std::fabs(dot(wi, I.F.n));
+                const V<T> so = spawn(I, wi, bias);
+                if (!occl<T>(sc, so, wi, len(so - to), isect, c)) {
+                    if (!mis) {
+                        Ld = Li * f / lpdf;
+                    } else {
+                        const T sp = bsdf_pdf<T>(I.lobe, m, I.F, I.wo, wi, nonspec);
+                        Ld = Li * f * ((lpdf * lpdf) / (lpdf * lpdf + sp * sp)) / lpdf;
+                    }
+                }
+            }
+        }
+    }
+    if (!mis) return Ld;
+    // sampleBSDF
+    rng.next();
+    rng.next();
+    V<T> wi;
+    T sp;
+    uint32_t st;
+    V<T> f = bsdf_sample<T>(I.lobe, m, I.F, I.wo, nonspec, rng, wi, sp, st);
+    if (black(f) || sp == T(0)) return Ld;
+    f = f * std::fabs(dot(wi, I.F.n));
+    T w = T(1);
+    if (!(st & B_SPEC)) {
+        T lp = 0;
+        if (li < na) {
+            const noor_area_light& A = sc.P->area_lights[li];
+            T tm = K<T>::inf;
+            if (quad_hit<T>(A, I.p, wi, tm)) {
+                const V<T> p = I.p + tm * wi;
+                lp = len2(p - I.p) / (std::fabs(dot(area_p<T>(A, 3), T(-1) * wi)) * (T)A.shape.area);
+                if (std::isinf(lp)) lp = 0;
+            }
+        } else {
+            lp = env_pdf<T>(sc, wi);
+        }
+        if (std::isinf(lp)) lp = 0;
+        if (lp == T(0)) return Ld;
+        w = (sp * sp) / (sp * sp + lp * lp);
+    }
+    const V<T> so = spawn(I, wi, bias);
+    T tm = T(2) * (T)sc.S->world_radius;
+    bool lh;
+    V<T> Le;
+    if (li < na) {
+        const noor_area_light& A = sc.P->area_lights[li];
+        lh = quad_hit<T>(A, so, wi, tm);
+        Le = (A.two_sided || dot(wi, area_p<T>(A, 3)) < T(0)) ? v3f<T>(A.ke) : zero;
+    } else {
+        lh = sc.sky_on;
+        Le = sc.sky_on ? env_eval<T>(sc, wi) : zero;
+    }
+    if (!lh) return Ld;
+    const V<T> cc = Le * f * w / sp;
+    if (black(cc)) return Ld;
+    const V<T> to = so + tm * wi;
+    const V<T> v = to - I.p;
+    const V<T> vwi = v / len(v);
+    const V<T> so2 = spawn(I, vwi, bias);
+    if (!occl<T>(sc, so2, vwi, len(so2 - to), isect, c)) Ld = Ld + cc;
+    return Ld;
+}
+
+// pathtracer() (path_tracer.cu:26-75)
+template <class T> V<T> radiance(const Scene& sc, V<T> o, V<T> d, Rng& rng, int isect, Counters* c) {
+    V<T> L = mk(T(0), T(0), T(0)), beta = mk(T(1), T(1), T(1));
+    bool specb = false;
+    const T bias = (T)sc.S->reflection_bias;
+    for (uint32_t b = 0; b < sc.S->bounces; ++b) {
+        T tmax = K<T>::inf;
+        Hit h{0, 0, 0, 0, 0};
+        uint64_t ctr[3] = {0, 0, 0};
+        if (c) c->ext++;
+        const bool hit = traverse<T>(sc, o, d, tmax, &h, false, isect, c ? ctr : nullptr);
+        if (c) {
+            c->nodes += ctr[0];
+            c->tris += ctr[1];
+            c->tri_in_range += ctr[2];
+        }
+        if (!hit) {
+            if (sc.sky_on && (b == 0 || specb)) L = L + beta * env_eval<T>(sc, nrm(d));
+            break;
+        }
+        Is<T> I;
+        I.p = o + tmax * d;
+        I.wo = nrm(T(-1) * d);
+        I.mt = h.mt;
+        I.lobe = lobe_of(h.mt);
+        I.mat = sc.P->attribute_indices[4 * (size_t)h.tri + 3];
+        if (I.mt & kEmitMat) {
+            if (b == 0 || specb) {
+                if (I.mt & NOOR_MESHLIGHT) {
+                    const noor_area_light& A = sc.P->area_lights[h.ins];
+                    L = L + beta * ((A.two_sided || dot(d, area_p<T>(A, 3)) < T(0)) ? v3f<T>(A.ke) : mk(T(0), T(0), T(0)));
+                } else {
+                    const Scene::Mat& em = sc.mats[I.mat];
+                    L = L + beta * ((T)em.emitter_scale * v3f<T>(em.emittance));
+                }
+            }
+            break;
+        }
+        I.F = tangent<T>(sc, h);
+        const Scene::Mat& m = sc.mats[I.mat];
+        L = L + beta * direct<T>(sc, m, I, rng, isect, c);
+        rng.next();
+        rng.next();
+        V<T> wi;
+        T pdf;
+        uint32_t st;
+        const V<T> f = bsdf_sample<T>(I.lobe, m, I.F, I.wo, B_ALL, rng, wi, pdf, st);
+        if (pdf == T(0)) break;
+        beta = beta * (f * std::fabs(dot(wi, I.F.n)) / pdf);
+        if (!(I.mt & kTranspMat) && dot(wi, I.F.ng) < T(0)) break;
+        if (b >= sc.S->rr) {
+            const T q = std::max((T)0.05f, T(1) - maxc(beta));
+            if ((T)rng.next() < q) break;
+            beta = beta / (T(1) - q);
+        }
+        specb = (I.mt & kSpecMat) != 0;
+        o = spawn(I, wi, bias);
+        d = wi;
+    }
+    return mk(clampv(L.x, T(0), T(100)), clampv(L.y, T(0), T(100)), clampv(L.z, T(0), T(100)));
+}
+
+// generateRay, pinhole (cameraimp.cuh:182-228)
+template <class T> void cam_ray(const noor_camera& C, uint32_t x, uint32_t y, Rng& rng, V<T>& o, V<T>& d) {
+    const float rxf = (float)x + rng.next() - 0.5f;
+    const float ryf = (float)y + rng.next() - 0.5f;
+    const T rx = rxf, ry = ryf;
+    T pc[3];
+    for (int r = 0; r < 3; ++r)
+        pc[r] = (T)C.raster_to_camera[r][3] +
+                ((T)C.raster_to_camera[r][0] * rx + (T)C.raster_to_camera[r][1] * ry + (T)C.raster_to_camera[r][2] * T(0));
+    const V<T> dc = nrm(mk(pc[0], pc[1], pc[2]));
+    o = mk((T)C.camera_to_world[0][3], (T)C.camera_to_world[1][3], (T)C.camera_to_world[2][3]);
+    T dw[3];
+    for (int r = 0; r < 3; ++r)
+        dw[r] = (T)C.camera_to_world[r][0] * dc.x + (T)C.camera_to_world[r][1] * dc.y + (T)C.camera_to_world[r][2] * dc.z;
+    d = nrm(mk(dw[0], dw[1], dw[2]));
+}
+
+struct Ctx {
+    Scene sc;
+};
+
+}  // namespace orc
+
+using namespace orc;
+
+// --------------------------------------------------------------- C API
+OR_API void* oracle_create(const noor_payload* P, const noor_spec* S, const noor_hosek_sky* H) {
+    Ctx* c = new Ctx();
+    Scene& sc = c->sc;
+    sc.P = P;
+    sc.S = S;
+    sc.H = H;
+    const noor_texture& env = P->textures[P->num_textures - 1];
+    sc.env = env.rgba;
+    sc.ew = env.width;
+    sc.eh = env.height;
+    sc.num_lights = P->num_area_lights + P->num_infinite_lights;
+    sc.sky_on = (S->lighting_type & NOOR_LIGHT_SKY_MASK) != 0;
+    sc.mats.resize(P->num_materials);
+    for (uint32_t i = 0; i < P->num_materials; ++i) {
+        const noor_material& m = P->materials[i];
+        Scene::Mat& d = sc.mats[i];
+        auto t = [&](uint32_t idx, float* o) { std::memcpy(o, P->textures[idx].rgba, 12); };
+        t(m.diffuse_tex_idx, d.diffuse);
+        t(m.specular_tex_idx, d.specular);
+        t(m.transmission_tex_idx, d.transmission);
+        t(m.emittance_tex_idx, d.emittance);
+        t(m.ior_tex_idx, d.ior);
+        t(m.k_tex_idx, d.k);
+        d.rx = P->textures[m.roughness_tex_idx].rgba[0];
+        d.ry = P->textures[m.roughness_tex_idx].rgba[1];
+        d.coat_ior = m.coat_ior;
+        d.emitter_scale = m.emitter_scale;
+        d.type = m.type;
+        d.dist = m.distribution;
+    }
+    build_dist(sc);
+    return c;
+}
+OR_API void oracle_destroy(void* h) { delete (Ctx*)h; }
+
+// closest hit for a ray batch (same struct as the library's noor_ray/noor_hit)
+OR_API void oracle_trace_closest(void* h, const noor_ray* rays, noor_hit* hits, size_t n, int isect, int threads) {
+    const Scene& sc = ((Ctx*)h)->sc;
+    auto work = [&](size_t b, size_t e) {
+        for (size_t i = b; i < e; ++i) {
+            const noor_ray& r = rays[i];
+            float tmax = r.tmax;
+            Hit rec{0, 0, 0, 0, 0};
+            const bool hh = traverse<float>(sc, mk(r.org[0], r.org[1], r.org[2]), mk(r.dir[0], r.dir[1], r.dir[2]),
+                                            tmax, &rec, false, isect, nullptr);
+            noor_hit& o = hits[i];
+            o.t = tmax;
+            o.tri_idx = rec.tri;
+            o.ins_idx = rec.ins;
+            o.material_type = rec.mt;
+            o.u = (float)rec.u;
+            o.v = (float)rec.v;
+            o.hit = hh ? 1u : 0u;
+            o.pad = 0;
+        }
+    };
+    const int T = std::max(1, threads);
+    std::vector<std::thread> th;
+    for (int t = 0; t < T; ++t) th.emplace_back(work, n * t / T, n * (t + 1) / T);
+    for (auto& x : th) x.join();
+}
+
+OR_API void oracle_trace_any(void* h, const noor_ray* rays, uint32_t* occ, size_t n, int isect) {
+    const Scene& sc = ((Ctx*)h)->sc;
+    for (size_t i = 0; i < n; ++i) {
+        const noor_ray& r = rays[i];
+        float tmax = r.tmax;
+        occ[i] = traverse<float>(sc, mk(r.org[0], r.org[1], r.org[2]), mk(r.dir[0], r.dir[1], r.dir[2]), tmax, nullptr,
+                                 true, isect, nullptr)
+                     ? 1u
+                     : 0u;
+    }
+}
+
+// camera rays of frame `frame` for pixels [0, w*h)
+OR_API void oracle_camera_rays(const noor_camera* C, uint32_t frame, noor_ray* rays) {
+    const uint32_t n = C->w * C->h;
+    for (uint32_t p = 0; p < n; ++p) {
+        Rng rng{tea16(p, frame)};
+        V<float> o, d;
+        cam_ray<float>(*C, p % C->w, p / C->w, rng, o, d);
+        noor_ray& r = rays[p];
+        r.org[0] = o.x; r.org[1] = o.y; r.org[2] = o.z;
+        r.dir[0] = d.x; r.dir[1] = d.y; r.dir[2] = d.z;
+        r.tmax = std::numeric_limits<float>::infinity();
+        r.pad = 0;
+    }
+}
+
+// Render pixels [p0, p1) x frames [f0, f0+nf): out = per-pixel mean rgb
+// (sequential Kahan sum in FP32 mode, plain sum in FP64), counters
+// (optional, 5 x uint64: ext rays, shadow rays, nodes, triangles, triangles in range).
+OR_API void oracle_render(void* h, uint32_t f0, uint32_t nf, uint32_t p0, uint32_t p1, const noor_camera* C,
+                          int fp64, int isect, int threads, float* out_rgb, uint64_t* counters) {
+    const Scene& sc = ((Ctx*)h)->sc;
+    const int T = std::max(1, threads);
+    std::atomic<uint32_t> next{p0};
+    std::vector<Counters> cs(T);
+    auto work = [&](int tid) {
+        Counters* c = counters ? &cs[tid] : nullptr;
+        for (;;) {
+            const uint32_t b = next.fetch_add(64);
+            if (b >= p1) break;
+            const uint32_t e = std::min(b + 64, p1);
+            for (uint32_t p = b; p < e; ++p) {
+                const uint32_t x = p % C->w, y = p / C->w;
+                double sd[3] = {0, 0, 0};
+                float sf[3] = {0, 0, 0}, cf[3] = {0, 0, 0};
+                for (uint32_t f = 0; f < nf; ++f) {
+                    Rng rng{tea16(p, f0 + f)};
+                    if (fp64) {
+                        V<double> o, d;
+                        cam_ray<double>(*C, x, y, rng, o, d);
+                        const V<double> L = radiance<double>(sc, o, d, rng, isect, c);
+                        sd[0] += L.x; sd[1] += L.y; sd[2] += L.z;
+                    } else {
+                        V<float> o, d;
+                        cam_ray<float>(*C, x, y, rng, o, d);
+                        const V<float> L = radiance<float>(sc, o, d, rng, isect, c);
+                        const float l[3] = {L.x, L.y, L.z};
+                        for (int k = 0; k < 3; ++k) {
+                            const float yk = l[k] - cf[k];
+                            const float t = sf[k] + yk;
+                            cf[k] = (t - sf[k]) - yk;
+                            sf[k] = t;
+                        }
+                    }
+                }
+                float* q = out_rgb + 3 * (size_t)(p - p0);
+                for (int k = 0; k < 3; ++k) q[k] = fp64 ? (float)(sd[k] / nf) : sf[k] / (float)nf;
+            }
+        }
+    };
+    std::vector<std::thread> th;
+    for (int t = 0; t < T; ++t) th.emplace_back(work, t);
+    for (auto& x : th) x.join();
+    if (counters) {
+        for (int k = 0; k < 5; ++k) counters[k] = 0;
+        for (auto& c : cs) {
+            counters[0] += c.ext;
+            counters[1] += c.shadow;
+            counters[2] += c.nodes;
+            counters[3] += c.tris;
+            counters[4] += c.tri_in_range;
+        }
+    }
+}
+
+// BSDF batch in the local frame (same record layout as noor_eval_bsdf)
+OR_API void oracle_eval_bsdf(void* h, int kind, const float* in, float* out, size_t n, int fp64) {
+    const Scene& sc = ((Ctx*)h)->sc;
+    for (size_t i = 0; i < n; ++i) {
+        const float* p = in + 16 * i;
+        const Scene::Mat& m = sc.mats[(uint32_t)p[8]];
+        const uint32_t lobe = lobe_of(m.type);
+        float* q = out + 8 * i;
+        auto run = [&](auto zero) {
+            using T = decltype(zero);
+            Frame<T> F;
+            F.n = F.ng = mk(T(0), T(0), T(1));
+            F.s = mk(T(1), T(0), T(0));
+            F.t = mk(T(0), T(1), T(0));
+            const V<T> wo = mk((T)p[0], (T)p[1], (T)p[2]), wi = mk((T)p[3], (T)p[4], (T)p[5]);
+            V<T> f = mk(T(0), T(0), T(0)), ws = f;
+            T pdf = 0;
+            uint32_t st = 0;
+            if (kind == 0) f = bsdf_eval<T>(lobe, m, F, wo, wi, B_ALL);
+            else if (kind == 1) pdf = bsdf_pdf<T>(lobe, m, F, wo, wi, B_ALL);
+            else {
+                V<T> w = f;
+                if (lobe && wo.z != T(0))
+                    f = lobe_sample<T>(lobe, m, wo, (T)std::min(p[6], 1.0f - std::numeric_limits<float>::epsilon()),
+                                       (T)p[7], w, pdf, st);
+                if (pdf != T(0)) ws = w;
+            }
+            q[0] = (float)f.x; q[1] = (float)f.y; q[2] = (float)f.z; q[3] = (float)pdf;
+            q[4] = (float)ws.x; q[5] = (float)ws.y; q[6] = (float)ws.z; q[7] = (float)st;
+        };
+        if (fp64) run(0.0); else run(0.0f);
+    }
+}
+
+OR_API void oracle_eval_sky(void* h, const float* dirs, float* rgb, size_t n, int fp64) {
+    const Scene& sc = ((Ctx*)h)->sc;
+    for (size_t i = 0; i < n; ++i) {
+        if (fp64) {
+            const V<double> c = env_eval<double>(sc, mk((double)dirs[3 * i], (double)dirs[3 * i + 1], (double)dirs[3 * i + 2]));
+            rgb[3 * i] = (float)c.x; rgb[3 * i + 1] = (float)c.y; rgb[3 * i + 2] = (float)c.z;
+        } else {
+            const V<float> c = env_eval<float>(sc, mk(dirs[3 * i], dirs[3 * i + 1], dirs[3 * i + 2]));
+            rgb[3 * i] = c.x; rgb[3 * i + 1] = c.y; rgb[3 * i + 2] = c.z;
+        }
+    }
+}
+
+// FP64 env distribution: sizes, func (h*w), normalised cdf (h*(w+1)),
+// row integrals (h), marginal cdf (h+1), marginal integral
+OR_API void oracle_env_distribution(void* h, int* w, int* hh, double* func, double* cdf, double* row_int,
+                                    double* marg_cdf, double* marg_int) {
+    const Scene& sc = ((Ctx*)h)->sc;
+    if (w) *w = sc.dw;
+    if (hh) *hh = sc.dh;
+    if (func) std::memcpy(func, sc.func.data(), sc.func.size() * 8);
+    if (cdf) std::memcpy(cdf, sc.cdf.data(), sc.cdf.size() * 8);
+    if (row_int) std::memcpy(row_int, sc.row_int.data(), sc.row_int.size() * 8);
+    if (marg_cdf) std::memcpy(marg_cdf, sc.marg_cdf.data(), sc.marg_cdf.size() * 8);
+    if (marg_int) *marg_int = sc.marg_int;
+}
+
+// u -> {x, y, pdf_sample, pdf_eval} in FP64
+OR_API void oracle_env_sample(void* h, const float* u, double* out, size_t n) {
+    const Scene& sc = ((Ctx*)h)->sc;
+    for (size_t i = 0; i < n; ++i) {
+        double x, y, pdf;
+        dist_sample<double>(sc, (double)u[2 * i], (double)u[2 * i + 1], x, y, pdf);
+        out[4 * i] = x;
+        out[4 * i + 1] = y;
+        out[4 * i + 2] = pdf;
+        out[4 * i + 3] = dist_pdf<double>(sc, x, y);
+    }
+}
+
+OR_API uint32_t oracle_tea16(uint32_t a, uint32_t b) { return tea16(a, b); }

@@ -1,0 +1,180 @@
+"""ORACLE -- test infrastructure, not product code.
+
+ctypes loader for the CPU restatement (oracle/_build/liboracle.so, built from
+noor_oracle.cpp) and for the reference's own host routines compiled from the
+reference tree (oracle/_ref/libnoor_ref.so).  Only tests/,
+__graft_entry__.smoke() and bench.py's CPU-baseline leg import this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ORACLE_SO = HERE / "_build" / "liboracle.so"
+REF_SO = HERE / "_ref" / "libnoor_ref.so"
+
+
+def build(ref: bool = True) -> None:
+    """make the oracle (and, when the reference tree is present, oracle/_ref)"""
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    if ref and Path("/root/reference/noor").exists():
+        subprocess.run(["make", "-s", "-C", str(HERE), "ref"], check=True)
+
+
+_orc = None
+_ref = None
+
+
+def lib() -> C.CDLL:
+    global _orc
+    if _orc is None:
+        if not ORACLE_SO.exists():
+            build(ref=False)
+        L = C.CDLL(str(ORACLE_SO))
+        vp, sz = C.c_void_p, C.c_size_t
+        L.oracle_create.restype = vp
+        L.oracle_create.argtypes = [vp, vp, vp]
+        L.oracle_destroy.argtypes = [vp]
+        L.oracle_trace_closest.argtypes = [vp, vp, vp, sz, C.c_int, C.c_int]
+        L.oracle_trace_any.argtypes = [vp, vp, vp, sz, C.c_int]
+        L.oracle_camera_rays.argtypes = [vp, C.c_uint32, vp]
+        L.oracle_render.argtypes = [vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, vp, C.c_int, C.c_int,
+                                    C.c_int, vp, vp]
+        L.oracle_eval_bsdf.argtypes = [vp, C.c_int, vp, vp, sz, C.c_int]
+        L.oracle_eval_sky.argtypes = [vp, vp, vp, sz, C.c_int]
+        L.oracle_env_distribution.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp]
+        L.oracle_env_sample.argtypes = [vp, vp, vp, sz]
+        L.oracle_tea16.restype = C.c_uint32
+        L.oracle_tea16.argtypes = [C.c_uint32, C.c_uint32]
+        _orc = L
+    return _orc
+
+
+def ref_available() -> bool:
+    return REF_SO.exists()
+
+
+def ref() -> C.CDLL:
+    global _ref
+    if _ref is None:
+        if not REF_SO.exists():
+            raise FileNotFoundError(f"{REF_SO} not built (needs the reference tree)")
+        L = C.CDLL(str(REF_SO))
+        vp = C.c_void_p
+        L.ref_build_bvh.restype = C.c_int
+        L.ref_build_bvh.argtypes = [vp, vp, C.c_size_t, vp, vp, vp, vp]
+        L.ref_wald.argtypes = [vp, vp]
+        L.ref_hosek_state.argtypes = [C.c_float, C.c_float, C.c_float, vp]
+        L.ref_hosek_dataset.argtypes = [vp]
+        _ref = L
+    return _ref
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class Oracle:
+    """CPU restatement over the same payload/spec/sky structs the library uses."""
+
+    def __init__(self, payload, spec, hosek):
+        self._refs = (payload, spec, hosek)
+        self.h = lib().oracle_create(C.addressof(payload), C.addressof(spec), C.addressof(hosek))
+
+    def close(self):
+        if self.h:
+            lib().oracle_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def trace_closest(self, rays: np.ndarray, isect: int, threads: int = 8) -> np.ndarray:
+        hits = np.zeros(rays.shape[0] * 8, np.uint32)
+        lib().oracle_trace_closest(self.h, _p(rays), _p(hits), rays.shape[0], isect, threads)
+        return hits.reshape(-1, 8)
+
+    def trace_any(self, rays: np.ndarray, isect: int) -> np.ndarray:
+        occ = np.zeros(rays.shape[0], np.uint32)
+        lib().oracle_trace_any(self.h, _p(rays), _p(occ), rays.shape[0], isect)
+        return occ
+
+    def render(self, camera, frame0: int, nframes: int, p0: int = 0, p1: int = None, fp64: bool = False,
+               isect: int = 0, threads: int = 8, counters: bool = False):
+        if p1 is None:
+            p1 = camera.w * camera.h
+        out = np.zeros((p1 - p0) * 3, np.float32)
+        ctr = np.zeros(5, np.uint64)
+        lib().oracle_render(self.h, frame0, nframes, p0, p1, C.addressof(camera), int(fp64), isect, threads,
+                            _p(out), _p(ctr) if counters else None)
+        out = out.reshape(-1, 3)
+        return (out, ctr) if counters else out
+
+    def eval_bsdf(self, kind: int, recs: np.ndarray, fp64: bool = False) -> np.ndarray:
+        out = np.zeros(recs.shape[0] * 8, np.float32)
+        lib().oracle_eval_bsdf(self.h, kind, _p(recs), _p(out), recs.shape[0], int(fp64))
+        return out.reshape(-1, 8)
+
+    def eval_sky(self, dirs: np.ndarray, fp64: bool = False) -> np.ndarray:
+        out = np.zeros(dirs.shape[0] * 3, np.float32)
+        lib().oracle_eval_sky(self.h, _p(dirs), _p(out), dirs.shape[0], int(fp64))
+        return out.reshape(-1, 3)
+
+    def env_distribution(self):
+        w, h = C.c_int(), C.c_int()
+        lib().oracle_env_distribution(self.h, C.addressof(w), C.addressof(h), None, None, None, None, None)
+        W, H = w.value, h.value
+        func = np.zeros(W * H)
+        cdf = np.zeros(H * (W + 1))
+        row = np.zeros(H)
+        mcdf = np.zeros(H + 1)
+        mi = C.c_double()
+        lib().oracle_env_distribution(self.h, None, None, _p(func), _p(cdf), _p(row), _p(mcdf), C.addressof(mi))
+        return dict(w=W, h=H, func=func.reshape(H, W), cdf=cdf.reshape(H, W + 1), row_int=row, marg_cdf=mcdf,
+                    marg_int=mi.value)
+
+    def env_sample(self, u: np.ndarray) -> np.ndarray:
+        out = np.zeros(u.shape[0] * 4)
+        lib().oracle_env_sample(self.h, _p(np.ascontiguousarray(u, np.float32)), _p(out), u.shape[0])
+        return out.reshape(-1, 4)
+
+
+def ref_build_bvh(desc, num_triangles: int):
+    """nodes (n,8) u32, root, triangle order, height from the reference builder"""
+    L = ref()
+    n = C.c_uint32()
+    root = C.c_uint32()
+    height = C.c_uint32()
+    order = np.zeros(num_triangles, np.uint32)
+    rc = L.ref_build_bvh(C.addressof(desc), None, 0, C.addressof(n), C.addressof(root), _p(order),
+                         C.addressof(height))
+    nodes = np.zeros(n.value * 8, np.uint32)
+    rc = L.ref_build_bvh(C.addressof(desc), _p(nodes), n.value, C.addressof(n), C.addressof(root), _p(order),
+                         C.addressof(height))
+    assert rc == 0
+    return nodes.reshape(-1, 8), root.value, order, height.value
+
+
+def ref_wald(v9: np.ndarray) -> np.ndarray:
+    out = np.zeros(12, np.uint32)
+    ref().ref_wald(_p(np.ascontiguousarray(v9, np.float32)), _p(out))
+    return out
+
+
+def ref_hosek_state(turbidity: float, albedo: float, elevation: float) -> np.ndarray:
+    out = np.zeros(30, np.float32)
+    ref().ref_hosek_state(turbidity, albedo, elevation, _p(out))
+    return out
+
+
+def ref_hosek_dataset() -> np.ndarray:
+    out = np.zeros(3 * 1080 + 3 * 120, np.float32)
+    ref().ref_hosek_dataset(_p(out))
+    return out

@@ -1,0 +1,83 @@
+"""The C-ABI library loads without a GPU, exports every entry point the
+header declares, and its struct layouts match the ctypes mirror."""
+import ctypes as C
+import re
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+from noor_b200 import _capi
+
+HEADER = Path(__file__).resolve().parents[1] / "include" / "noor_b200.h"
+
+
+def declared_functions():
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    names = re.findall(r"^\s*(?:const\s+)?[A-Za-z_][\w\s\*]*?\b([a-z_][a-z0-9_A-Z]*)\s*\(", text, flags=re.M)
+    return sorted(set(n for n in names if n not in ("sizeof",)))
+
+
+def test_header_functions_are_exported():
+    so = _capi.LIB_PATH
+    out = subprocess.run(["nm", "-D", "--defined-only", str(so)], capture_output=True, text=True, check=True).stdout
+    exported = {l.split()[-1] for l in out.splitlines() if " T " in l}
+    decl = declared_functions()
+    assert len(decl) >= 40
+    missing = [d for d in decl if d not in exported]
+    assert not missing, missing
+
+
+def test_every_prototype_resolves():
+    L = _capi.lib()
+    for name in _capi.PROTOTYPES:
+        assert hasattr(L, name)
+
+
+def test_struct_sizes_match_c():
+    n = len(_capi.ABI_STRUCTS)
+    out = (C.c_uint32 * n)()
+    got = _capi.lib().noor_abi_sizes(out, n)
+    assert got == n
+    for st, size in zip(_capi.ABI_STRUCTS, out):
+        assert C.sizeof(st) == size, st.__name__
+
+
+def test_errors_without_context():
+    L = _capi.lib()
+    L.device_free_memory()
+    rc = L.update_cuda_spec()
+    assert rc == 3  # NOOR_ERR_NO_CONTEXT
+    assert b"context" in L.noor_last_error()
+    f = C.c_uint(1)
+    assert L.cuda_path_tracer(C.byref(f)) == 3
+    assert f.value == 1
+
+
+def test_camera_lookat_matches_reference_formulas():
+    cam = _capi.Camera()
+    arr = lambda v: (C.c_float * 3)(*v)
+    _capi.call("noor_camera_lookat", arr((0, 1, 3.75)), arr((0, 1, 0)), arr((0, 1, 0)), float(np.radians(40.0)),
+               256, 256, C.byref(cam))
+    c2w = np.array([list(r) for r in cam.camera_to_world])
+    # camera frame: right = x, up = y, forward = +z (eye - lookAt), origin = eye
+    assert np.allclose(c2w[:, :3], np.eye(3), atol=1e-7)
+    assert np.allclose(c2w[:, 3], (0, 1, 3.75))
+    r2c = np.array([list(r) for r in cam.raster_to_camera])
+    cot = 1.0 / np.tan(np.radians(20.0))
+    # raster (0,0) -> screen (-1,-1) -> camera (-1/cot, -1/cot, -1)
+    assert np.allclose(r2c @ np.array([0, 0, 0, 1.0]), (-1 / cot, -1 / cot, -1), rtol=1e-6)
+    assert np.allclose(r2c @ np.array([256, 256, 0, 1.0]), (1 / cot, 1 / cot, -1), rtol=1e-6)
+    assert cam.center == 256 * 128 + 128
+
+
+def test_bad_payload_is_rejected():
+    """load_cuda_data validates before touching the device"""
+    L = _capi.lib()
+    p = _capi.Payload()
+    cam = _capi.Camera()
+    cam.w = cam.h = 4
+    sp = _capi.Spec()
+    rc = L.load_cuda_data(C.byref(p), None, C.byref(cam), C.byref(sp), None)
+    assert rc != 0
