@@ -1,0 +1,330 @@
+"""Benchmark of the B200 render path on the sky-lit 2.6M-triangle scene.
+
+One step = one full render of the workload (1920x1080 pixels x 64 samples,
+depth 8, 32 subdivision-6 icospheres under a Hosek-Wilkie sky) with the scene
+resident in HBM.  Prints one JSON line.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--integrator megakernel|wavefront] [--spp S] [--scale F]
+
+`value` is device-timed Mpaths/s (CUDA events on the render stream, max over
+ranks); `e2e` is the same metric through the reference-facing C-ABI with the
+camera uploaded from host memory and the film read back to host memory every
+step.  --impl reference times the CPU restatement of the reference routines
+(oracle) on the host cores on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOAD = "sky-lit 32 icospheres (2,621,440 tris), 1920x1080, 64 spp, depth 8, Hosek sky T=3 elev 30deg"
+METRIC = "Mpaths/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--integrator", default="megakernel", choices=["megakernel", "wavefront"])
+    ap.add_argument("--spp", type=int, default=64)
+    ap.add_argument("--scale", type=float, default=1.0, help="image size scale (1 = 1920x1080)")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class Clocks:
+    """nvidia-smi sampler during the timed region"""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.p = None
+        self.path = ROOT / "_work" / f"clocks_{os.getpid()}.csv"
+
+    def __enter__(self):
+        try:
+            self.path.parent.mkdir(exist_ok=True)
+            self.f = open(self.path, "w")
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(5)
+            except Exception:
+                self.p.kill()
+            self.f.close()
+
+    def summary(self):
+        if not self.p or not self.path.exists():
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = [l.split(",") for l in self.path.read_text().splitlines() if l.strip()]
+        self.path.unlink(missing_ok=True)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+                for k, n in enumerate(names):
+                    if r[5 + k].strip().lower() == "active":
+                        reasons.add(n)
+            except (ValueError, IndexError):
+                pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build_scene(args):
+    from noor_b200 import scenes
+    w, h = int(round(1920 * args.scale)), int(round(1080 * args.scale))
+    s = scenes.sky_scene(width=w, height=h, spp=args.spp, bounces=8)
+    t = time.time()
+    built = scenes.BuiltPayload(s)
+    return s, built, time.time() - t
+
+
+def algorithmic_bytes(orc, cam, spp, isect, sample_pixels=20000, seed=0):
+    """Bytes a path reads by the traversal/shading model: per traversal step
+    32 B per node, per tested triangle 32 B (Wald: first sector) or 48 B
+    (watertight: three vertices), 16 B per in-range Wald triangle (second
+    record), per extension hit 16 B attributes + 3 x (16+16+8) B vertex data.
+    Counted by the oracle on a pixel subsample with 2 samples each."""
+    n = cam.w * cam.h
+    rng = np.random.default_rng(seed)
+    px = np.sort(rng.choice(n, size=min(sample_pixels, n), replace=False))
+    tot = np.zeros(5, np.uint64)
+    paths = 0
+    # contiguous runs keep the oracle call simple: sample blocks of 64 pixels
+    for b in px[:: 64]:
+        p1 = min(int(b) + 64, n)
+        _, c = orc.render(cam, 1, 2, p0=int(b), p1=p1, isect=isect, threads=1, counters=True)
+        tot += c
+        paths += 2 * (p1 - int(b))
+    ext, shadow, nodes, tris, inrange = [float(x) / paths for x in tot]
+    tri_b = 32.0 if isect == 1 else 48.0
+    per_path = 32.0 * nodes + tri_b * tris + (16.0 * inrange if isect == 1 else 0.0) + ext * (16 + 3 * 40)
+    return per_path, dict(ext_rays_per_path=ext, shadow_rays_per_path=shadow, nodes_per_path=nodes,
+                          tris_per_path=tris, sample_paths=paths)
+
+
+def cpu_baseline(args, s, built, spec, hosek, cam, budget_s):
+    """oracle FP32 on all host threads over a pixel subsample of the workload"""
+    from oracle.oracle import Oracle
+    threads = os.cpu_count() or 1
+    orc = Oracle(built.payload, spec, hosek)
+    n = cam.w * cam.h
+    # probe rate on a small block, then size the sample to the budget
+    t = time.time()
+    orc.render(cam, 1, 2, p0=n // 2, p1=n // 2 + 256, threads=threads)
+    rate = 512 / max(time.time() - t, 1e-3)
+    npx = int(max(256, min(n, rate * budget_s / args.spp)))
+    p0 = max(0, n // 2 - npx // 2)
+    t = time.time()
+    orc.render(cam, 1, args.spp, p0=p0, p1=p0 + npx, threads=threads)
+    dt = time.time() - t
+    orc.close()
+    return {"value": npx * args.spp / dt / 1e6, "unit": METRIC, "cores": threads, "kind": "port",
+            "sample": f"{npx} contiguous pixels around the image centre x {args.spp} spp of the workload "
+                      f"({npx * args.spp} paths, {dt:.1f} s), FP32 transcription of the reference routines"}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from noor_b200 import scenes, _capi
+    from oracle.oracle import Oracle
+    s, built, _ = build_scene(args)
+    spec = built.default_spec(8, 1)
+    cam = scenes.make_camera(s.camera)
+    hosek = reference_hosek(s.hosek)
+    orc = Oracle(built.payload, spec, hosek)
+    threads = os.cpu_count() or 1
+    n = cam.w * cam.h
+    npx = 4096
+    times = []
+    for i in range(args.warmup + args.steps):
+        p0 = (n // 2 + i * npx) % (n - npx)
+        t = time.time()
+        orc.render(cam, 1, args.spp, p0=p0, p1=p0 + npx, threads=threads)
+        if i >= args.warmup:
+            times.append(time.time() - t)
+    orc.close()
+    ms = 1000 * statistics.mean(times)
+    v = npx * args.spp / (ms / 1000) / 1e6
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "sample_per_step": f"{npx} pixels x {args.spp} spp"},
+            "cpu_baseline": {"value": v, "unit": METRIC, "cores": threads, "kind": "port",
+                             "sample": f"{npx} pixels x {args.spp} spp per step, FP32 transcription of the "
+                                       "reference's device routines (the reference has no CPU render path)"},
+            "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def reference_hosek(h):
+    """Hosek sky for the reference arm from the reference's own fit
+    (arhosek_rgb_skymodelstate_alloc_update outputs frozen in
+    tests/golden/hosek_states.npz) and HosekSky::update's sun fields
+    (noor/header/hosek.h:61-83)."""
+    from noor_b200 import _capi
+    g = np.load(ROOT / "tests" / "golden" / "hosek_states.npz")
+    elev = np.pi / 2 - h["sun_lat"]
+    k = int(np.argmin(np.abs(g["cases"] - np.array([h["turbidity"], h["albedo"], elev])).sum(1)))
+    st = g["states"][k]
+    out = _capi.HosekSky()
+    for i in range(3):
+        for c in range(3):
+            for j in range(9):
+                out.state[i].configs[c][j] = float(st[9 * c + j])
+            out.state[i].radiances[c] = float(st[27 + c])
+        out.state[i].solar_radius = float(np.radians(0.51) / 2)
+    d = np.array([np.sin(h["sun_lat"]) * np.cos(h["sun_lon"]), np.cos(h["sun_lat"]),
+                  np.sin(h["sun_lat"]) * np.sin(h["sun_lon"])], np.float32)
+    out.solar_dir[:] = [float(x) for x in d / np.linalg.norm(d)]
+    out.ground_albedo[:] = [h["albedo"]] * 3
+    out.solar_scale = h["solar_scale"]
+    out.solar_radius = float(h["solar_radius_scale"] * np.radians(0.51) / 2)
+    return out
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    rank, world, local = dist_env()
+    import torch
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from noor_b200 import scenes, _capi
+    s, built, build_s = build_scene(args)
+    r = scenes.Renderer(s, built=built)
+
+    def render_step():
+        r.frame = C.c_uint(1)
+        r.render(args.spp)
+
+    # warm-up
+    for _ in range(max(3, args.warmup)):
+        render_step()
+    r.counters(reset=True)
+    l0 = C.c_uint64()
+    _capi.call("noor_launch_count", C.byref(l0))
+    if world > 1:
+        torch.distributed.barrier()
+    with Clocks(local) as clk:
+        _capi.call("noor_event_record", 0)
+        for _ in range(args.steps):
+            render_step()
+        _capi.call("noor_event_record", 1)
+        ms = C.c_float()
+        _capi.call("noor_event_elapsed", 0, 1, C.byref(ms))
+    l1 = C.c_uint64()
+    _capi.call("noor_launch_count", C.byref(l1))
+    ext, shadow, paths = r.counters()
+    ms_step = ms.value / args.steps
+    if world > 1:
+        t = torch.tensor([ms_step], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms_step = float(t.item())
+    npaths = r.w * r.h * args.spp
+    value = world * npaths / (ms_step / 1000) / 1e6
+    mrays = world * (ext + shadow) / args.steps / (ms_step / 1000) / 1e6
+
+    # end to end through the C-ABI: camera from host memory, film to host memory
+    host_film = np.zeros((r.h, r.w, 4), np.float32)
+    e2e_t = []
+    for i in range(args.warmup + args.steps):
+        if world > 1:
+            torch.distributed.barrier()
+        t = time.perf_counter()
+        _capi.call("update_cuda_camera")
+        r.frame = C.c_uint(1)
+        r.render(args.spp)
+        _capi.call("noor_get_framebuffer", host_film.ctypes.data_as(C.POINTER(C.c_float)), r.w * r.h)
+        if i >= args.warmup:
+            e2e_t.append(time.perf_counter() - t)
+    e2e_ms = statistics.mean(e2e_t) * 1000
+    if world > 1:
+        t = torch.tensor([e2e_ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = {"value": world * npaths / (e2e_ms / 1000) / 1e6, "unit": METRIC,
+           "h2d_bytes_per_step": C.sizeof(_capi.Camera), "d2h_bytes_per_step": int(host_film.nbytes)}
+
+    line = None
+    if rank == 0:
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+        hbm = peaks.get("hbm_gbs", 6650.0)
+        roof = {"bound": "hbm", "achieved": None, "peak": hbm, "unit": "GB/s", "frac": None, "traffic": None,
+                "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
+        cpu = None
+        if not args.no_cpu_baseline:
+            from oracle.oracle import Oracle
+            orc = Oracle(built.payload, r.spec, r.hosek)
+            per_path, counts = algorithmic_bytes(orc, r.camera, args.spp, r.spec.intersector)
+            orc.close()
+            achieved = per_path * npaths / (ms_step / 1000) / 1e9
+            roof.update(achieved=achieved, frac=achieved / hbm, algorithmic_bytes_per_path=per_path, **counts)
+            prof = ROOT / "profiles" / "megakernel_sky_traffic.json"
+            if prof.exists():
+                tr = json.loads(prof.read_text())
+                roof["traffic"] = tr.get("dram_bytes_per_path", 0) * npaths
+            cpu = cpu_baseline(args, s, built, r.spec, r.hosek, r.camera, args.cpu_seconds)
+        line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator, random-init sky)",
+                "config": {"workload": WORKLOAD, "integrator": args.integrator, "width": r.w, "height": r.h,
+                           "spp": args.spp, "bounces": 8, "triangles": s.num_triangles,
+                           "intersector": "watertight", "film": "kahan",
+                           "l2": "inputs larger than L2 (scene ~0.5 GB resident)",
+                           "parallelism": f"replicas{world}", "bvh_build_s": round(build_s, 2)},
+                "mrays_per_s": mrays, "rays_per_step": (ext + shadow) / args.steps,
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": int(l1.value - l0.value), "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    r.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -504,6 +504,16 @@ int noor_scene_upload(const noor_payload* payload, const noor_hosek_sky* hosek,
                       const noor_spec* spec, uint32_t* scene_id);
 int noor_wavefront_render(const noor_wf_frame* frames, uint32_t n_frames,
                           const noor_wf_params* params);
+/* as noor_wavefront_render, also returning the device time of the batch */
+int noor_wavefront_render_timed(const noor_wf_frame* frames, uint32_t n_frames,
+                                const noor_wf_params* params, float* ms);
+/* rays and paths the wavefront traced: [0] extension, [1] shadow, [2] paths */
+int noor_wavefront_counters(uint64_t counters[3], int reset);
+/* The same frames rendered one after another by the plain megakernel
+ * (one launch per frame, film folded with Kahan summation); device time of
+ * the whole sequence in *ms. */
+int noor_megakernel_batch(const noor_wf_frame* frames, uint32_t n_frames,
+                          float* ms);
 /* Project-written autotuner: times candidate parameter sets on the given
  * batch and returns the fastest. */
 int noor_wavefront_autotune(const noor_wf_frame* frames, uint32_t n_frames,

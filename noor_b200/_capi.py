@@ -197,6 +197,9 @@ PROTOTYPES = {
     "noor_scene_upload": (C.c_int, [C.POINTER(Payload), C.POINTER(HosekSky), C.POINTER(Spec), pu]),
     "noor_wavefront_render": (C.c_int, [C.POINTER(WfFrame), u32, C.POINTER(WfParams)]),
     "noor_wavefront_autotune": (C.c_int, [C.POINTER(WfFrame), u32, C.POINTER(WfParams), pf]),
+    "noor_wavefront_render_timed": (C.c_int, [C.POINTER(WfFrame), u32, C.POINTER(WfParams), pf]),
+    "noor_wavefront_counters": (C.c_int, [C.POINTER(u64), C.c_int]),
+    "noor_megakernel_batch": (C.c_int, [C.POINTER(WfFrame), u32, pf]),
     "noor_adjoint_forward": (C.c_int, [C.POINTER(AdjointDesc), C.c_void_p]),
     "noor_adjoint_backward": (C.c_int, [C.POINTER(AdjointDesc), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
 }

@@ -3,6 +3,7 @@
 // noor/cuda/render.cuh:67-149, mesh.cuh:64-103, lightimp.cuh:299-371), the
 // reference entry points of noor/cuda/path_tracer.cuh:136-151 and the
 // additions declared in include/noor_b200.h.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -397,6 +398,7 @@ int render_frames(Context& C, uint32_t frame0, uint32_t n) {
     MegaArgs a{};
     a.frame0 = frame0;
     a.nframes = n;
+    a.fresh = frame0 == 1 ? 1u : 0u;
     uint32_t chunks = 1;
     if (st.dev.film_mode == NOOR_FILM_KAHAN) {
         const uint64_t target = (uint64_t)C.sm_count * 1024u;
@@ -418,6 +420,52 @@ int render_frames(Context& C, uint32_t frame0, uint32_t n) {
     C.launches += chunks > 1 ? 2 : 1;
     C.film_count = (frame0 == 1) ? n : C.film_count + n;
     C.last_frame = frame0 + n - 1;
+    return NOOR_OK;
+}
+
+// One frame of a batch with the plain megakernel: film of its own (scratch),
+// mean written into d_film (float4 per pixel) when given.
+int megakernel_frame(Context& C, const noor_wf_frame& f, float4* sum, float4* comp) {
+    if (f.scene_id >= C.scenes.size()) return set_error(NOOR_ERR_INVALID, "megakernel batch: unknown scene id");
+    if (f.width == 0 || f.height == 0 || f.spp == 0 || f.first_frame == 0 || f.width != f.camera.w ||
+        f.height != f.camera.h)
+        return set_error(NOOR_ERR_INVALID, "megakernel batch: bad frame description");
+    DevScene S = C.scenes[f.scene_id]->dev;
+    if (f.bounces) S.bounces = f.bounces;
+    S.film_mode = NOOR_FILM_KAHAN;
+    DevCamera cam{};
+    for (int r = 0; r < 3; ++r) {
+        cam.c2w[r] = make_float4(f.camera.camera_to_world[r][0], f.camera.camera_to_world[r][1],
+                                 f.camera.camera_to_world[r][2], f.camera.camera_to_world[r][3]);
+        cam.r2c[r] = make_float4(f.camera.raster_to_camera[r][0], f.camera.raster_to_camera[r][1],
+                                 f.camera.raster_to_camera[r][2], f.camera.raster_to_camera[r][3]);
+    }
+    cam.w = f.width;
+    cam.h = f.height;
+    cam.center = f.camera.center;
+    const uint32_t npix = f.width * f.height;
+    MegaArgs a{};
+    a.frame0 = f.first_frame;
+    a.nframes = f.spp;
+    a.fresh = 1u;
+    const uint64_t target = (uint64_t)C.sm_count * 1024u;
+    a.chunks = (uint32_t)std::min<uint64_t>(f.spp, std::max<uint64_t>(1, (target + npix - 1) / npix));
+    a.film_sum = sum;
+    a.film_comp = comp;
+    int rc;
+    if (a.chunks > 1) {
+        if ((rc = ensure_parts(C, (size_t)a.chunks * npix))) return rc;
+        a.part_sum = C.part_sum;
+        a.part_comp = C.part_comp;
+    }
+    a.lookat = C.lookat;
+    a.status = C.status;
+    a.counters = C.counters;
+    cudaError_t e = launch_megakernel(S, cam, a, C.stream);
+    if (e == cudaSuccess && f.d_film)
+        e = launch_resolve(npix, NOOR_FILM_KAHAN, 1.0f / (float)f.spp, sum, (float4*)f.d_film, C.stream);
+    if (e != cudaSuccess) return cuda_fail(e, "megakernel batch");
+    C.launches += (a.chunks > 1 ? 2 : 1) + (f.d_film ? 1 : 0);
     return NOOR_OK;
 }
 
@@ -778,6 +826,30 @@ extern "C" int noor_get_env_distribution(int* w, int* h, float* func, float* cdf
     if (e != cudaSuccess) return cuda_fail(e, "env distribution");
     if (marginal_integral) *marginal_integral = C->scenes[0]->dev.dist.marg_int;
     return NOOR_OK;
+}
+
+extern "C" int noor_megakernel_batch(const noor_wf_frame* frames, uint32_t n_frames, float* ms) {
+    Context* C;
+    int rc = need_ctx(C);
+    if (rc) return rc;
+    if (!frames || n_frames == 0) return set_error(NOOR_ERR_INVALID, "megakernel batch: no frames");
+    size_t maxpix = 0;
+    for (uint32_t i = 0; i < n_frames; ++i) maxpix = std::max<size_t>(maxpix, (size_t)frames[i].width * frames[i].height);
+    float4 *sum = nullptr, *comp = nullptr;
+    cudaError_t e = cudaMalloc((void**)&sum, maxpix * 16);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&comp, maxpix * 16);
+    if (e != cudaSuccess) {
+        cudaFree(sum);
+        return cuda_fail(e, "megakernel batch film");
+    }
+    cudaEventRecord(C->events[4], C->stream);
+    for (uint32_t i = 0; i < n_frames && !rc; ++i) rc = megakernel_frame(*C, frames[i], sum, comp);
+    cudaEventRecord(C->events[5], C->stream);
+    if (!rc) rc = sync_and_check(*C, "megakernel batch");
+    if (!rc && ms) cudaEventElapsedTime(ms, C->events[4], C->events[5]);
+    cudaFree(sum);
+    cudaFree(comp);
+    return rc;
 }
 
 extern "C" int noor_scene_upload(const noor_payload* payload, const noor_hosek_sky* hosek, const noor_spec* spec,

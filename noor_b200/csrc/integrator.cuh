@@ -89,10 +89,20 @@ NB_D float light_pdf(const DevScene& S, const Isect& I, int li, const float3& wi
     return isinf(pdf) ? 0.0f : pdf;
 }
 
-// sampleLight (noor/cuda/direct.cuh:32-67)
-template <int ISECT>
-NB_D float3 sample_light(const DevScene& S, const DevMaterial& m, const Isect& I, Rng& rng, bool mis, int& light_idx,
-                         bool& picked, const SmemStack& st, uint32_t* status, RayStats& rs) {
+// A shadow ray whose contribution counts only if nothing blocks it.
+struct ShadowRay {
+    float3 o;
+    float3 d;
+    float tmax;
+};
+
+// sampleLight (noor/cuda/direct.cuh:32-67) up to the occlusion test: returns
+// the contribution it adds when the shadow ray `sr` is unblocked (zero, with
+// no ray needed, on every early exit).  The MIS weight is applied here; the
+// reference evaluates it after the occlusion test, which draws no random
+// numbers, so the order does not change the result.
+NB_D float3 light_sample_contrib(const DevScene& S, const DevMaterial& m, const Isect& I, Rng& rng, bool mis,
+                                 int& light_idx, bool& picked, ShadowRay& sr) {
     picked = false;
     if (I.mtype & kSpecularMat) return f3(0.0f);
     const int nl = S.sky_on ? S.num_lights : S.num_lights - 1;
@@ -107,20 +117,18 @@ NB_D float3 sample_light(const DevScene& S, const DevMaterial& m, const Isect& I
     float3 f = bsdf_eval(I.lobe, m, I.F, I.wo, wi, kNonSpecular);
     if (is_black(f)) return f3(0.0f);
     f *= absdot(wi, I.F.n);
-    const float3 so = spawn_origin(I, wi, S.bias);
-    const float dist = length3(so - to);
-    rs.shadow++;
-    if (trace_any<ISECT>(S, so, wi, dist, st, status)) return f3(0.0f);
+    sr.o = spawn_origin(I, wi, S.bias);
+    sr.d = wi;
+    sr.tmax = length3(sr.o - to);
     if (!mis) return Li * f / lpdf;
     const float spdf = bsdf_pdf(I.lobe, m, I.F, I.wo, wi, kNonSpecular);
     const float w = power_heuristic(lpdf, spdf);
     return Li * f * w / lpdf;
 }
 
-// sampleBSDF (noor/cuda/direct.cuh:69-110)
-template <int ISECT>
-NB_D float3 sample_bsdf_mis(const DevScene& S, const DevMaterial& m, const Isect& I, Rng& rng, int li,
-                            const SmemStack& st, uint32_t* status, RayStats& rs) {
+// sampleBSDF (noor/cuda/direct.cuh:69-110) up to the occlusion test
+NB_D float3 bsdf_mis_contrib(const DevScene& S, const DevMaterial& m, const Isect& I, Rng& rng, int li,
+                             ShadowRay& sr) {
     const uint32_t flags = (I.mtype & kSpecularMat) ? BSDF_ALL : kNonSpecular;
     rng.next();  // two draws the reference makes and never reads (direct.cuh:79)
     rng.next();
@@ -154,10 +162,9 @@ NB_D float3 sample_bsdf_mis(const DevScene& S, const DevMaterial& m, const Isect
     const float3 to = so + tm * wi;
     float3 vwi;
     visibility(I.p, to, vwi);
-    const float3 so2 = spawn_origin(I, vwi, S.bias);
-    const float d2 = length3(so2 - to);
-    rs.shadow++;
-    if (trace_any<ISECT>(S, so2, vwi, d2, st, status)) return f3(0.0f);
+    sr.o = spawn_origin(I, vwi, S.bias);
+    sr.d = vwi;
+    sr.tmax = length3(sr.o - to);
     return c;
 }
 
@@ -224,8 +231,20 @@ NB_D float3 path_radiance(const DevScene& S, float3 o, float3 d, Rng& rng, const
         // accumulate (accumulate.cuh:83-99): direct lighting, then scatter
         int li = 0;
         bool picked;
-        float3 Ld = sample_light<ISECT>(S, m, I, rng, S.mis != 0, li, picked, st, status, rs);
-        if (S.mis && picked) Ld += sample_bsdf_mis<ISECT>(S, m, I, rng, li, st, status, rs);
+        ShadowRay sr;
+        float3 Ld = light_sample_contrib(S, m, I, rng, S.mis != 0, li, picked, sr);
+        if (!is_black(Ld)) {
+            rs.shadow++;
+            if (trace_any<ISECT>(S, sr.o, sr.d, sr.tmax, st, status)) Ld = f3(0.0f);
+        }
+        if (S.mis && picked) {
+            float3 c = bsdf_mis_contrib(S, m, I, rng, li, sr);
+            if (!is_black(c)) {
+                rs.shadow++;
+                if (trace_any<ISECT>(S, sr.o, sr.d, sr.tmax, st, status)) c = f3(0.0f);
+            }
+            Ld += c;
+        }
         L += beta * Ld;
         // scatter (scatter.cuh:27-41)
         rng.next();  // two draws the reference makes and never reads (scatter.cuh:34)

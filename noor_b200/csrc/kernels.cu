@@ -38,7 +38,7 @@ __global__ void __launch_bounds__(kMegaBlock) megakernel(DevScene S, DevCamera C
         const uint32_t x = pix % C.w, y = pix / C.w;
         float3 sum = f3(0.0f), comp = f3(0.0f);
         float4 mean = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
-        if (a.chunks == 1u && a.frame0 > 1u) {
+        if (a.chunks == 1u && !a.fresh) {
             if (FILM == NOOR_FILM_KAHAN) {
                 sum = f3(a.film_sum[pix]);
                 comp = f3(a.film_comp[pix]);
@@ -88,12 +88,12 @@ __global__ void __launch_bounds__(kMegaBlock) megakernel(DevScene S, DevCamera C
 }
 
 // folds the per-chunk partial sums into the Kahan film in chunk order
-__global__ void fold_partials(uint32_t npix, uint32_t chunks, uint32_t frame0, float4* film_sum, float4* film_comp,
+__global__ void fold_partials(uint32_t npix, uint32_t chunks, uint32_t fresh, float4* film_sum, float4* film_comp,
                               const float4* part_sum, const float4* part_comp) {
     const uint32_t pix = blockIdx.x * blockDim.x + threadIdx.x;
     if (pix >= npix) return;
     float3 sum = f3(0.0f), comp = f3(0.0f);
-    if (frame0 > 1u) {
+    if (!fresh) {
         sum = f3(film_sum[pix]);
         comp = f3(film_comp[pix]);
     }
@@ -285,7 +285,7 @@ cudaError_t launch_megakernel(const DevScene& S, const DevCamera& C, const MegaA
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     if (a.chunks > 1u) {
-        fold_partials<<<(npix + 255) / 256, 256, 0, s>>>(npix, a.chunks, a.frame0, a.film_sum, a.film_comp,
+        fold_partials<<<(npix + 255) / 256, 256, 0, s>>>(npix, a.chunks, a.fresh, a.film_sum, a.film_comp,
                                                           a.part_sum, a.part_comp);
         e = cudaGetLastError();
     }

@@ -11,6 +11,7 @@ struct MegaArgs {
     uint32_t frame0;        // RNG frame number of the first sample
     uint32_t nframes;       // samples per pixel in this launch
     uint32_t chunks;        // frame ranges split across threads (>=1)
+    uint32_t fresh;         // 1: start the film from zero, 0: fold into it
     float4* film_sum;       // Kahan sum (or running mean in lerp mode)
     float4* film_comp;      // Kahan compensation
     float4* part_sum;       // chunks * npix partial sums (chunks > 1)

@@ -1,27 +1,733 @@
-// Persistent wavefront integrator (placeholder entry points until the
-// wavefront kernels land).
+// Persistent wavefront integrator: the path loop of the megakernel split
+// into short kernels over a pool of path slots, so that traversal runs at
+// the occupancy of a small kernel, shading runs over slots sorted by
+// material kind, and finished slots are refilled with new paths at every
+// bounce.  Many frames (different resolutions, scenes and sample counts)
+// share one pool and one launch.
+//
+// Per bounce (one iteration of a CUDA-graph while loop):
+//   regen   fold pending shadow results into each path's radiance; add
+//           finished paths to their frame's film; refill free slots with
+//           camera rays of the next (frame, sample, pixel) work item
+//   extend  closest hit for every active slot; misses and emitters finish
+//           the path, surface hits are queued by material kind
+//   shade   one launch per kind: light sample (+ MIS BSDF sample) with the
+//           occlusion test deferred to a shadow-ray queue, then scatter,
+//           Russian roulette and the next ray
+//   shadow  any hit for the queued shadow rays; blocked ones are cancelled
+//   check   stop when no slot is active; bounded by an iteration cap
+//
+// Every path draws the same random numbers in the same order as in the
+// megakernel (seed TEA(pixel, frame), LCG state carried in the slot), so
+// both integrators produce the same samples up to floating-point rounding.
+// Films are accumulated with atomic adds whose rounding error is recovered
+// exactly by TwoSum and added to a compensation buffer (compensated FP32
+// summation that does not depend on completion order).
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <vector>
+
 #include "host_common.h"
+#include "integrator.cuh"
 #include "runtime.h"
 
 namespace nb {
-void wavefront_release(Context& C) { (void)C; }
+
+constexpr int kKinds = 3;  // Lambert, conductor, dielectric
+
+struct WfFrameDev {
+    DevCamera cam;
+    unsigned long long base;   // first global work index
+    unsigned long long count;  // npix * spp
+    uint32_t npix;
+    uint32_t scene;
+    uint32_t first_frame;
+    uint32_t bounces;
+    uint32_t spp;
+    uint32_t pad;
+    float4* sum;   // per pixel compensated sum
+    float4* comp;
+    float* out;    // caller's film (mean, float4 per pixel) or null
+};
+
+// slot state
+enum : uint32_t { kFree = 0, kActive = 1, kFinishing = 2 };
+
+struct WfDev {
+    // path slots
+    float4* o;       // origin, w = frame index bits
+    float4* d;       // direction, w = pixel bits
+    float4* beta;    // throughput, w = bounce | spec << 16
+    float4* L;       // radiance, w = RNG state bits
+    float4* pend;    // 2 per slot: contribution, w = 1 if pending
+    float4* hit;     // t, u, v, tri bits
+    uint2* hit2;     // instance, material type
+    uint32_t* state;
+    uint32_t* qshade;       // kKinds * cap slot indices
+    uint32_t* qshadow;      // 2 * cap entries: slot << 1 | which
+    float4* sh_o;           // origin, tmax
+    float4* sh_d;           // direction
+    uint32_t* counters;     // [0,kKinds) shade counts, [kKinds] shadow count, [kKinds+1] active, [kKinds+2] iteration
+    unsigned long long* work_next;
+    unsigned long long* rays;  // [ext, shadow, paths]
+    uint32_t* status;
+    const WfFrameDev* frames;
+    const DevScene* scenes;
+    uint32_t nframes;
+    uint32_t cap;
+    uint32_t sort;          // 0: one shade queue, 1: one per kind
+    uint32_t max_iters;
+    unsigned long long total;
+    int stack_cap;
+    cudaGraphConditionalHandle cond;
+};
+
+NB_D uint32_t fbits(float f) { return __float_as_uint(f); }
+NB_D float bitsf(uint32_t u) { return __uint_as_float(u); }
+
+// warp-aggregated push: returns this lane's index into the queue
+NB_D uint32_t queue_push(uint32_t* counter) {
+    const uint32_t mask = __activemask();
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(mask) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(counter, (uint32_t)__popc(mask));
+    base = __shfl_sync(mask, base, leader);
+    return base + __popc(mask & ((1u << lane) - 1u));
+}
+
+NB_D void count_add(unsigned long long* ctr, uint32_t v) {
+    const uint32_t mask = __activemask();
+    const uint32_t s = __reduce_add_sync(mask, v);
+    if ((int)(threadIdx.x & 31) == __ffs(mask) - 1 && s) atomicAdd(ctr, (unsigned long long)s);
+}
+
+// compensated atomic add: TwoSum of (old, v) recovers the rounding error of
+// the atomic add exactly; it goes to the compensation buffer
+NB_D void film_add(float* sum, float* comp, float v) {
+    const float old = atomicAdd(sum, v);
+    const float s = old + v;
+    const float bp = s - old;
+    const float err = (old - (s - bp)) + (v - bp);
+    if (err != 0.0f) atomicAdd(comp, err);
+}
+
+NB_D int frame_of(const WfDev& W, unsigned long long k) {
+    int lo = 0, hi = (int)W.nframes - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (W.frames[mid].base <= k)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(256) wf_regen(WfDev W) {
+    const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= W.cap) return;
+    uint32_t st = W.state[slot];
+    if (st != kFree) {
+        // pending shadow results of the last shade step
+        float4 Lw = W.L[slot];
+        const float4 p0 = W.pend[2 * slot], p1 = W.pend[2 * slot + 1];
+        if (p0.w != 0.0f) {
+            Lw.x += p0.x;
+            Lw.y += p0.y;
+            Lw.z += p0.z;
+        }
+        if (p1.w != 0.0f) {
+            Lw.x += p1.x;
+            Lw.y += p1.y;
+            Lw.z += p1.z;
+        }
+        W.pend[2 * slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        W.pend[2 * slot + 1] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (st == kFinishing) {
+            const uint32_t fi = fbits(W.o[slot].w);
+            const uint32_t pix = fbits(W.d[slot].w);
+            const WfFrameDev& F = W.frames[fi];
+            const float3 c = clamp3(f3(Lw.x, Lw.y, Lw.z), 0.0f, 100.0f);
+            float* s = reinterpret_cast<float*>(F.sum + pix);
+            float* cp = reinterpret_cast<float*>(F.comp + pix);
+            film_add(s + 0, cp + 0, c.x);
+            film_add(s + 1, cp + 1, c.y);
+            film_add(s + 2, cp + 2, c.z);
+            st = kFree;
+        } else {
+            W.L[slot] = Lw;
+        }
+    }
+    const bool need = st == kFree;
+    const uint32_t mask = __ballot_sync(__activemask(), need);
+    unsigned long long k = ~0ull;
+    if (need) {
+        const int lane = threadIdx.x & 31;
+        const int leader = __ffs(mask) - 1;
+        unsigned long long base = 0;
+        if (lane == leader) base = atomicAdd(W.work_next, (unsigned long long)__popc(mask));
+        base = __shfl_sync(mask, base, leader);
+        k = base + __popc(mask & ((1u << lane) - 1u));
+    }
+    if (need && k < W.total) {
+        const int fi = frame_of(W, k);
+        const WfFrameDev& F = W.frames[fi];
+        const unsigned long long local = k - F.base;
+        const uint32_t sample = (uint32_t)(local / F.npix);
+        const uint32_t pix = (uint32_t)(local % F.npix);
+        Rng rng{tea16(pix, F.first_frame + sample)};
+        float3 o, d;
+        camera_ray(F.cam, pix % F.cam.w, pix / F.cam.w, rng, o, d);
+        W.o[slot] = make_float4(o.x, o.y, o.z, bitsf((uint32_t)fi));
+        W.d[slot] = make_float4(d.x, d.y, d.z, bitsf(pix));
+        W.beta[slot] = make_float4(1.0f, 1.0f, 1.0f, bitsf(0u));
+        W.L[slot] = make_float4(0.0f, 0.0f, 0.0f, bitsf(rng.s));
+        st = kActive;
+        count_add(W.rays + 2, 1u);
+    }
+    W.state[slot] = st;
+    if (st == kActive) {
+        const uint32_t am = __activemask();
+        const uint32_t n = __popc(am);
+        if ((int)(threadIdx.x & 31) == __ffs(am) - 1) atomicAdd(W.counters + kKinds + 1, n);
+    }
+}
+
+template <int ISECT>
+NB_D void extend_one(const WfDev& W, uint32_t slot, const SmemStack& stk) {
+    const float4 ow = W.o[slot], dw = W.d[slot], bw = W.beta[slot];
+    const uint32_t fi = fbits(ow.w);
+    const WfFrameDev& F = W.frames[fi];
+    const DevScene& S = W.scenes[F.scene];
+    const float3 o = f3(ow.x, ow.y, ow.z), d = f3(dw.x, dw.y, dw.z);
+    const uint32_t bb = fbits(bw.w);
+    const uint32_t bounce = bb & 0xFFFFu;
+    const bool spec = (bb >> 16) & 1u;
+    float tmax = kInf;
+    HitRec rec{0.0f, 0.0f, 0u, 0u, 0u};
+    const bool hit = trace_closest<ISECT>(S, o, d, tmax, rec, stk, W.status);
+    const float3 beta = f3(bw.x, bw.y, bw.z);
+    if (!hit) {
+        if (S.sky_on && (bounce == 0 || spec)) {
+            float4 Lw = W.L[slot];
+            const float3 c = beta * env_eval(S, normalize_fast(d));
+            W.L[slot] = make_float4(Lw.x + c.x, Lw.y + c.y, Lw.z + c.z, Lw.w);
+        }
+        W.state[slot] = kFinishing;
+        return;
+    }
+    if (rec.mtype & kEmitterMat) {
+        if (bounce == 0 || spec) {
+            float3 c;
+            if (rec.mtype & NOOR_MESHLIGHT) {
+                const DevAreaLight& A = S.area_lights[rec.ins];
+                c = beta * ((A.two_sided || dot(d, A.n) < 0.0f) ? A.ke : f3(0.0f));
+            } else {
+                const uint32_t mi = ISECT == NOOR_ISECT_WATERTIGHT ? __ldg(&S.wtri[rec.tri].attr).w
+                                                                   : __ldg(&S.wald[rec.tri].attr).w;
+                const DevMaterial& em = S.materials[mi];
+                c = beta * (em.emitter_scale * em.emittance);
+            }
+            float4 Lw = W.L[slot];
+            W.L[slot] = make_float4(Lw.x + c.x, Lw.y + c.y, Lw.z + c.z, Lw.w);
+        }
+        W.state[slot] = kFinishing;
+        return;
+    }
+    W.hit[slot] = make_float4(tmax, rec.u, rec.v, bitsf(rec.tri));
+    W.hit2[slot] = make_uint2(rec.ins, rec.mtype);
+    const uint32_t lobe = lobe_of(rec.mtype);
+    const uint32_t kind = W.sort ? (lobe == kLobeLambert ? 0u : (lobe == kLobeConductor ? 1u : 2u)) : 0u;
+    const uint32_t i = queue_push(W.counters + kind);
+    W.qshade[kind * W.cap + i] = slot;
+}
+
+__global__ void __launch_bounds__(256) wf_extend(WfDev W) {
+    extern __shared__ uint32_t smem[];
+    const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= W.cap || W.state[slot] != kActive) return;
+    SmemStack stk{smem + threadIdx.x, (int)blockDim.x, W.stack_cap};
+    const uint32_t fi = fbits(W.o[slot].w);
+    const DevScene& S = W.scenes[W.frames[fi].scene];
+    if (S.isect == NOOR_ISECT_WATERTIGHT)
+        extend_one<NOOR_ISECT_WATERTIGHT>(W, slot, stk);
+    else
+        extend_one<NOOR_ISECT_REF_WALD>(W, slot, stk);
+    count_add(W.rays + 0, 1u);
+}
+
+NB_D void push_shadow(const WfDev& W, uint32_t slot, uint32_t which, const ShadowRay& sr) {
+    const uint32_t i = queue_push(W.counters + kKinds);
+    W.qshadow[i] = (slot << 1) | which;
+    W.sh_o[i] = make_float4(sr.o.x, sr.o.y, sr.o.z, sr.tmax);
+    W.sh_d[i] = make_float4(sr.d.x, sr.d.y, sr.d.z, 0.0f);
+}
+
+__global__ void __launch_bounds__(256) wf_shade(WfDev W, uint32_t kind) {
+    const uint32_t n = W.counters[kind];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t slot = W.qshade[kind * W.cap + i];
+        const float4 ow = W.o[slot], dw = W.d[slot], bw = W.beta[slot], Lw = W.L[slot];
+        const float4 hw = W.hit[slot];
+        const uint2 h2 = W.hit2[slot];
+        const uint32_t fi = fbits(ow.w);
+        const WfFrameDev& F = W.frames[fi];
+        const DevScene& S = W.scenes[F.scene];
+        const float3 o = f3(ow.x, ow.y, ow.z), d = f3(dw.x, dw.y, dw.z);
+        float3 beta = f3(bw.x, bw.y, bw.z);
+        const uint32_t bb = fbits(bw.w);
+        const uint32_t bounce = bb & 0xFFFFu;
+        HitRec rec;
+        rec.u = hw.y;
+        rec.v = hw.z;
+        rec.tri = fbits(hw.w);
+        rec.ins = h2.x;
+        rec.mtype = h2.y;
+        Isect I;
+        if (S.isect == NOOR_ISECT_WATERTIGHT)
+            make_isect<NOOR_ISECT_WATERTIGHT>(S, o, d, hw.x, rec, I);
+        else
+            make_isect<NOOR_ISECT_REF_WALD>(S, o, d, hw.x, rec, I);
+        const DevMaterial m = S.materials[I.mat];
+        Rng rng{fbits(Lw.w)};
+        int li = 0;
+        bool picked;
+        ShadowRay sr;
+        const float3 c0 = light_sample_contrib(S, m, I, rng, S.mis != 0, li, picked, sr);
+        if (!is_black(c0)) {
+            const float3 p = beta * c0;
+            W.pend[2 * slot] = make_float4(p.x, p.y, p.z, 1.0f);
+            push_shadow(W, slot, 0, sr);
+        }
+        if (S.mis && picked) {
+            const float3 c1 = bsdf_mis_contrib(S, m, I, rng, li, sr);
+            if (!is_black(c1)) {
+                const float3 p = beta * c1;
+                W.pend[2 * slot + 1] = make_float4(p.x, p.y, p.z, 1.0f);
+                push_shadow(W, slot, 1, sr);
+            }
+        }
+        // scatter, sidedness, Russian roulette, next ray
+        rng.next();
+        rng.next();
+        float3 wi;
+        float pdf;
+        uint32_t stype;
+        const float3 f = bsdf_sample(I.lobe, m, I.F, I.wo, BSDF_ALL, rng, wi, pdf, stype);
+        uint32_t st = kActive;
+        if (pdf == 0.0f) {
+            st = kFinishing;
+        } else {
+            beta *= f * absdot(wi, I.F.n) / pdf;
+            if (!(I.mtype & kTransparentMat) && dot(wi, I.F.ng) < 0.0f) {
+                st = kFinishing;
+            } else if (bounce >= S.rr) {
+                const float q = fmaxf(0.05f, 1.0f - maxcomp(beta));
+                if (rng.next() < q)
+                    st = kFinishing;
+                else
+                    beta /= 1.0f - q;
+            }
+        }
+        if (st == kActive) {
+            const bool spec = (I.mtype & kSpecularMat) != 0;
+            const uint32_t nb_ = bounce + 1;
+            const float3 no = spawn_origin(I, wi, S.bias);
+            W.o[slot] = make_float4(no.x, no.y, no.z, ow.w);
+            W.d[slot] = make_float4(wi.x, wi.y, wi.z, dw.w);
+            W.beta[slot] = make_float4(beta.x, beta.y, beta.z, bitsf(nb_ | (spec ? 1u << 16 : 0u)));
+            if (nb_ >= F.bounces) st = kFinishing;
+        }
+        W.L[slot] = make_float4(Lw.x, Lw.y, Lw.z, bitsf(rng.s));
+        W.state[slot] = st;
+    }
+}
+
+__global__ void __launch_bounds__(256) wf_shadow(WfDev W) {
+    extern __shared__ uint32_t smem[];
+    const uint32_t n = W.counters[kKinds];
+    SmemStack stk{smem + threadIdx.x, (int)blockDim.x, W.stack_cap};
+    uint32_t traced = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        ++traced;
+        const uint32_t e = W.qshadow[i];
+        const uint32_t slot = e >> 1;
+        const float4 so = W.sh_o[i], sd = W.sh_d[i];
+        const uint32_t fi = fbits(W.o[slot].w);
+        const DevScene& S = W.scenes[W.frames[fi].scene];
+        bool occ;
+        if (S.isect == NOOR_ISECT_WATERTIGHT)
+            occ = trace_any<NOOR_ISECT_WATERTIGHT>(S, f3(so.x, so.y, so.z), f3(sd.x, sd.y, sd.z), so.w, stk, W.status);
+        else
+            occ = trace_any<NOOR_ISECT_REF_WALD>(S, f3(so.x, so.y, so.z), f3(sd.x, sd.y, sd.z), so.w, stk, W.status);
+        if (occ) W.pend[e].w = 0.0f;
+    }
+    count_add(W.rays + 1, traced);
+}
+
+__global__ void wf_check(WfDev W) {
+    uint32_t* c = W.counters;
+    const uint32_t active = c[kKinds + 1];
+    const uint32_t it = ++c[kKinds + 2];
+    bool go = active > 0u;
+    if (go && it >= W.max_iters) {
+        atomicOr(W.status, NOOR_DEV_WAIT_TIMEOUT);
+        go = false;
+    }
+    for (int k = 0; k <= kKinds + 1; ++k) c[k] = 0u;
+    cudaGraphSetConditional(W.cond, go ? 1u : 0u);
+}
+
+// host-loop variant of the stop test (no conditional node): publishes the
+// active count for the host to read
+__global__ void wf_check_host(WfDev W, uint32_t* active_out) {
+    uint32_t* c = W.counters;
+    *active_out = c[kKinds + 1];
+    ++c[kKinds + 2];
+    for (int k = 0; k <= kKinds + 1; ++k) c[k] = 0u;
+}
+
+// mean = (sum + comp) / spp into the caller's film
+__global__ void wf_resolve(const WfFrameDev* frames, uint32_t fi) {
+    const WfFrameDev& F = frames[fi];
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= F.npix || !F.out) return;
+    const float4 s = F.sum[p], c = F.comp[p];
+    const float inv = 1.0f / (float)F.spp;
+    reinterpret_cast<float4*>(F.out)[p] = make_float4((s.x + c.x) * inv, (s.y + c.y) * inv, (s.z + c.z) * inv, 1.0f);
+}
+
+// ------------------------------------------------------------------ host
+struct WavefrontState {
+    uint32_t cap = 0;
+    std::vector<void*> bufs;
+    WfDev dev{};
+    uint32_t* active_host_dev = nullptr;
+    // film scratch per frame batch
+    void* films = nullptr;
+    size_t films_bytes = 0;
+    WfFrameDev* frames_dev = nullptr;
+    size_t frames_cap = 0;
+    DevScene* scenes_dev = nullptr;
+    size_t scenes_cap = 0;
+    ~WavefrontState() {
+        for (void* p : bufs) cudaFree(p);
+        if (films) cudaFree(films);
+        if (frames_dev) cudaFree(frames_dev);
+        if (scenes_dev) cudaFree(scenes_dev);
+        if (active_host_dev) cudaFree(active_host_dev);
+    }
+};
+
+void wavefront_release(Context& C) {
+    delete C.wf;
+    C.wf = nullptr;
+}
+
+static int wf_alloc(WavefrontState& S, void** p, size_t bytes) {
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) return cuda_fail(e, "wavefront buffers");
+    S.bufs.push_back(*p);
+    return NOOR_OK;
+}
+
+static int wf_ensure(Context& C, uint32_t cap) {
+    if (C.wf && C.wf->cap >= cap) return NOOR_OK;
+    delete C.wf;
+    C.wf = new WavefrontState();
+    WavefrontState& S = *C.wf;
+    WfDev& W = S.dev;
+    int rc;
+    const size_t n = cap;
+    if ((rc = wf_alloc(S, (void**)&W.o, n * 16)) || (rc = wf_alloc(S, (void**)&W.d, n * 16)) ||
+        (rc = wf_alloc(S, (void**)&W.beta, n * 16)) || (rc = wf_alloc(S, (void**)&W.L, n * 16)) ||
+        (rc = wf_alloc(S, (void**)&W.pend, 2 * n * 16)) || (rc = wf_alloc(S, (void**)&W.hit, n * 16)) ||
+        (rc = wf_alloc(S, (void**)&W.hit2, n * 8)) || (rc = wf_alloc(S, (void**)&W.state, n * 4)) ||
+        (rc = wf_alloc(S, (void**)&W.qshade, kKinds * n * 4)) || (rc = wf_alloc(S, (void**)&W.qshadow, 2 * n * 4)) ||
+        (rc = wf_alloc(S, (void**)&W.sh_o, 2 * n * 16)) || (rc = wf_alloc(S, (void**)&W.sh_d, 2 * n * 16)) ||
+        (rc = wf_alloc(S, (void**)&W.counters, 64)) || (rc = wf_alloc(S, (void**)&W.work_next, 16)) ||
+        (rc = wf_alloc(S, (void**)&W.rays, 32)))
+        return rc;
+    cudaError_t e = cudaMalloc((void**)&S.active_host_dev, 16);
+    if (e != cudaSuccess) return cuda_fail(e, "wavefront buffers");
+    S.cap = cap;
+    return NOOR_OK;
+}
+
+struct WfLaunch {
+    int block;
+    size_t smem;
+    uint32_t grid_slots;
+    uint32_t grid_queue;
+};
+
+static cudaError_t wf_iteration(const WfDev& W, const WfLaunch& L, cudaStream_t s, bool conditional,
+                                uint32_t* active_out) {
+    wf_regen<<<(W.cap + 255) / 256, 256, 0, s>>>(W);
+    wf_extend<<<L.grid_slots, L.block, L.smem, s>>>(W);
+    const int nk = W.sort ? kKinds : 1;
+    for (int k = 0; k < nk; ++k) wf_shade<<<L.grid_queue, 256, 0, s>>>(W, (uint32_t)k);
+    wf_shadow<<<L.grid_queue, L.block, L.smem, s>>>(W);
+    if (conditional)
+        wf_check<<<1, 1, 0, s>>>(W);
+    else
+        wf_check_host<<<1, 1, 0, s>>>(W, active_out);
+    return cudaGetLastError();
+}
+
+// one batch render; returns device-timed ms through `ms` when non-null
+int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames, const noor_wf_params& P,
+                     float* ms_out) {
+    if (!frames || n_frames == 0) return set_error(NOOR_ERR_INVALID, "wavefront: no frames");
+    const uint32_t block = P.block_size ? P.block_size : 128;
+    if (block != 64 && block != 128 && block != 256)
+        return set_error(NOOR_ERR_INVALID, "wavefront: block_size must be 64, 128 or 256");
+    const uint32_t cap = P.queue_capacity ? P.queue_capacity : (1u << 20);
+    if (cap < 1024 || cap > (1u << 26)) return set_error(NOOR_ERR_INVALID, "wavefront: queue capacity out of range");
+    int rc = wf_ensure(C, cap);
+    if (rc) return rc;
+    WavefrontState& WS = *C.wf;
+    // frames and films
+    std::vector<WfFrameDev> fr(n_frames);
+    unsigned long long total = 0;
+    size_t film_px = 0;
+    int stack_cap = 16;
+    uint32_t max_bounces = 1;
+    for (uint32_t i = 0; i < n_frames; ++i) {
+        const noor_wf_frame& f = frames[i];
+        if (f.scene_id >= C.scenes.size()) return set_error(NOOR_ERR_INVALID, "wavefront: unknown scene id");
+        if (f.width == 0 || f.height == 0 || f.spp == 0 || f.first_frame == 0 ||
+            f.width != f.camera.w || f.height != f.camera.h)
+            return set_error(NOOR_ERR_INVALID, "wavefront: bad frame description");
+        if (f.camera.type != NOOR_CAMERA_PERSP || f.camera.lens_radius != 0.0f)
+            return set_error(NOOR_ERR_UNSUPPORTED, "wavefront: only the pinhole camera is implemented");
+        std::memset(&fr[i], 0, sizeof(WfFrameDev));
+        DevCamera& dc = fr[i].cam;
+        for (int r = 0; r < 3; ++r) {
+            dc.c2w[r] = make_float4(f.camera.camera_to_world[r][0], f.camera.camera_to_world[r][1],
+                                    f.camera.camera_to_world[r][2], f.camera.camera_to_world[r][3]);
+            dc.r2c[r] = make_float4(f.camera.raster_to_camera[r][0], f.camera.raster_to_camera[r][1],
+                                    f.camera.raster_to_camera[r][2], f.camera.raster_to_camera[r][3]);
+        }
+        dc.w = f.width;
+        dc.h = f.height;
+        dc.center = f.camera.center;
+        fr[i].npix = f.width * f.height;
+        fr[i].base = total;
+        fr[i].count = (unsigned long long)fr[i].npix * f.spp;
+        fr[i].scene = f.scene_id;
+        fr[i].first_frame = f.first_frame;
+        fr[i].bounces = f.bounces ? f.bounces : C.scenes[f.scene_id]->dev.bounces;
+        fr[i].spp = f.spp;
+        fr[i].out = f.d_film;
+        total += fr[i].count;
+        film_px += fr[i].npix;
+        stack_cap = std::max(stack_cap, C.scenes[f.scene_id]->dev.stack_cap);
+        max_bounces = std::max(max_bounces, fr[i].bounces);
+    }
+    const size_t film_bytes = film_px * 32;
+    if (WS.films_bytes < film_bytes) {
+        if (WS.films) cudaFree(WS.films);
+        WS.films = nullptr;
+        cudaError_t e = cudaMalloc(&WS.films, film_bytes);
+        if (e != cudaSuccess) return cuda_fail(e, "wavefront films");
+        WS.films_bytes = film_bytes;
+    }
+    {
+        size_t off = 0;
+        for (uint32_t i = 0; i < n_frames; ++i) {
+            fr[i].sum = (float4*)((char*)WS.films + off);
+            off += (size_t)fr[i].npix * 16;
+            fr[i].comp = (float4*)((char*)WS.films + off);
+            off += (size_t)fr[i].npix * 16;
+        }
+    }
+    if (WS.frames_cap < n_frames) {
+        if (WS.frames_dev) cudaFree(WS.frames_dev);
+        cudaError_t e = cudaMalloc((void**)&WS.frames_dev, n_frames * sizeof(WfFrameDev));
+        if (e != cudaSuccess) return cuda_fail(e, "wavefront frames");
+        WS.frames_cap = n_frames;
+    }
+    if (WS.scenes_cap < C.scenes.size()) {
+        if (WS.scenes_dev) cudaFree(WS.scenes_dev);
+        cudaError_t e = cudaMalloc((void**)&WS.scenes_dev, C.scenes.size() * sizeof(DevScene));
+        if (e != cudaSuccess) return cuda_fail(e, "wavefront scenes");
+        WS.scenes_cap = C.scenes.size();
+    }
+    std::vector<DevScene> sc(C.scenes.size());
+    for (size_t i = 0; i < sc.size(); ++i) sc[i] = C.scenes[i]->dev;
+    cudaStream_t s = C.stream;
+    cudaError_t e = cudaMemcpyAsync(WS.frames_dev, fr.data(), n_frames * sizeof(WfFrameDev), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(WS.scenes_dev, sc.data(), sc.size() * sizeof(DevScene), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(WS.films, 0, film_bytes, s);
+    WfDev& W = WS.dev;
+    if (e == cudaSuccess) e = cudaMemsetAsync(W.state, 0, (size_t)cap * 4, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(W.pend, 0, (size_t)cap * 32, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(W.counters, 0, 64, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(W.work_next, 0, 16, s);
+    if (e != cudaSuccess) return cuda_fail(e, "wavefront setup");
+    W.status = C.status;
+    W.frames = WS.frames_dev;
+    W.scenes = WS.scenes_dev;
+    W.nframes = n_frames;
+    W.cap = cap;
+    W.sort = P.sort_granularity ? 1u : 0u;
+    W.total = total;
+    W.stack_cap = stack_cap;
+    // every slot finishes within max_bounces iterations of starting; a slot
+    // starts at least every iteration while work remains
+    W.max_iters = (uint32_t)std::min<unsigned long long>(
+        (total + cap - 1) / cap * (max_bounces + 2) + 4 * (max_bounces + 2) + 64, 1u << 30);
+
+    WfLaunch L;
+    L.block = (int)block;
+    L.smem = (size_t)stack_cap * block * 4;
+    L.grid_slots = (cap + block - 1) / block;
+    L.grid_queue = (uint32_t)std::max(1, C.sm_count) * 16;
+    for (auto k : {wf_extend, wf_shadow}) {
+        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem);
+        if (e != cudaSuccess) return cuda_fail(e, "wavefront smem");
+    }
+    if (ms_out) cudaEventRecord(C.events[6], s);
+    bool done = false;
+    if (P.use_graph) {
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        e = cudaGraphCreate(&graph, 0);
+        cudaGraphConditionalHandle h;
+        if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault);
+        cudaGraphNode_t node;
+        cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        if (e == cudaSuccess) e = cudaGraphAddNode(&node, graph, nullptr, 0, &cp);
+        if (e == cudaSuccess) {
+            W.cond = h;
+            cudaGraph_t body = cp.conditional.phGraph_out[0];
+            e = cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+            if (e == cudaSuccess) {
+                cudaError_t e2 = wf_iteration(W, L, s, true, nullptr);
+                e = cudaStreamEndCapture(s, &body);
+                if (e == cudaSuccess) e = e2;
+            }
+        }
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+        if (e == cudaSuccess) e = cudaGraphLaunch(exec, s);
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (e != cudaSuccess) return cuda_fail(e, "wavefront graph");
+        C.launches += (uint64_t)W.max_iters;  // upper bound; refined below
+        done = true;
+    }
+    if (!done) {
+        // host loop: one iteration per launch sequence, reading the active
+        // count back every iteration (bounded by the iteration cap)
+        uint32_t active = 1;
+        for (uint32_t it = 0; it < W.max_iters && active; ++it) {
+            e = wf_iteration(W, L, s, false, WS.active_host_dev);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(&active, WS.active_host_dev, 4, cudaMemcpyDeviceToHost, s);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+            if (e != cudaSuccess) return cuda_fail(e, "wavefront iteration");
+            C.launches += 4 + (W.sort ? kKinds : 1);
+        }
+    }
+    for (uint32_t i = 0; i < n_frames; ++i)
+        if (fr[i].out) wf_resolve<<<(fr[i].npix + 255) / 256, 256, 0, s>>>(WS.frames_dev, i);
+    if (ms_out) cudaEventRecord(C.events[7], s);
+    e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(e, "wavefront render");
+    if (ms_out) cudaEventElapsedTime(ms_out, C.events[6], C.events[7]);
+    // iterations actually run (for the launch count)
+    uint32_t iters = 0;
+    cudaMemcpy(&iters, W.counters + kKinds + 2, 4, cudaMemcpyDeviceToHost);
+    if (P.use_graph) C.launches += (uint64_t)iters * (4 + (W.sort ? kKinds : 1)) - (uint64_t)W.max_iters;
+    return NOOR_OK;
+}
+
 }  // namespace nb
 
+using namespace nb;
+
 extern "C" int noor_wavefront_render(const noor_wf_frame* frames, uint32_t n_frames, const noor_wf_params* params) {
-    (void)frames; (void)n_frames; (void)params;
-    return set_error(NOOR_ERR_UNSUPPORTED, "wavefront integrator not built yet");
+    Context* C;
+    int rc = need_ctx(C);
+    if (rc) return rc;
+    noor_wf_params p{};
+    if (params) p = *params;
+    return wavefront_render(*C, frames, n_frames, p, nullptr);
 }
+
+extern "C" int noor_wavefront_render_timed(const noor_wf_frame* frames, uint32_t n_frames,
+                                           const noor_wf_params* params, float* ms) {
+    Context* C;
+    int rc = need_ctx(C);
+    if (rc) return rc;
+    noor_wf_params p{};
+    if (params) p = *params;
+    return wavefront_render(*C, frames, n_frames, p, ms);
+}
+
+extern "C" int noor_wavefront_counters(uint64_t counters[3], int reset) {
+    Context* C;
+    int rc = need_ctx(C);
+    if (rc) return rc;
+    if (!C->wf) {
+        if (counters) counters[0] = counters[1] = counters[2] = 0;
+        return NOOR_OK;
+    }
+    unsigned long long h[3] = {0, 0, 0};
+    cudaError_t e = cudaMemcpy(h, C->wf->dev.rays, sizeof(h), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && reset) e = cudaMemset(C->wf->dev.rays, 0, sizeof(h));
+    if (e != cudaSuccess) return cuda_fail(e, "wavefront counters");
+    if (counters)
+        for (int i = 0; i < 3; ++i) counters[i] = h[i];
+    return NOOR_OK;
+}
+
+// Autotuner: renders the batch with each candidate (block size x queue
+// capacity x material sort) and keeps the fastest by device time.
 extern "C" int noor_wavefront_autotune(const noor_wf_frame* frames, uint32_t n_frames, noor_wf_params* best,
                                        float* best_ms) {
-    (void)frames; (void)n_frames; (void)best; (void)best_ms;
-    return set_error(NOOR_ERR_UNSUPPORTED, "wavefront integrator not built yet");
+    Context* C;
+    int rc = need_ctx(C);
+    if (rc) return rc;
+    if (!best) return set_error(NOOR_ERR_INVALID, "autotune: best is null");
+    const uint32_t blocks[] = {64, 128, 256};
+    const uint32_t caps[] = {1u << 19, 1u << 20, 1u << 21};
+    const uint32_t sorts[] = {0, 1};
+    float bms = 3.4e38f;
+    noor_wf_params bp{128, 1u << 20, 1, best->use_graph};
+    for (uint32_t b : blocks)
+        for (uint32_t c : caps)
+            for (uint32_t so : sorts) {
+                noor_wf_params p{b, c, so, best->use_graph};
+                float ms = 0.0f;
+                if ((rc = wavefront_render(*C, frames, n_frames, p, &ms))) return rc;
+                if (ms < bms) {
+                    bms = ms;
+                    bp = p;
+                }
+            }
+    *best = bp;
+    if (best_ms) *best_ms = bms;
+    return NOOR_OK;
 }
+
+// ---------------------------------------------------------------- adjoint
 extern "C" int noor_adjoint_forward(const noor_adjoint_desc* desc, float* d_image) {
-    (void)desc; (void)d_image;
+    (void)desc;
+    (void)d_image;
     return set_error(NOOR_ERR_UNSUPPORTED, "adjoint not built yet");
 }
 extern "C" int noor_adjoint_backward(const noor_adjoint_desc* desc, const float* d_grad_image, float* d_grad_albedo,
                                      float* d_grad_roughness, float* d_grad_env) {
-    (void)desc; (void)d_grad_image; (void)d_grad_albedo; (void)d_grad_roughness; (void)d_grad_env;
+    (void)desc;
+    (void)d_grad_image;
+    (void)d_grad_albedo;
+    (void)d_grad_roughness;
+    (void)d_grad_env;
     return set_error(NOOR_ERR_UNSUPPORTED, "adjoint not built yet");
 }

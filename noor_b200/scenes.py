@@ -224,18 +224,56 @@ def sphere_field(seed: int, count: int, level: int, box: float = 20.0, rmin: flo
         meshes.append(dict(tri_start=i * nf, tri_count=nf, to_global=IDENTITY, instance=-1, light_idx=-1))
     T = count * nf
     return dict(vertices=V, normals=N, uvs=np.zeros((1, 2), np.float32), vindices=vidx, nindices=vidx.copy(),
-                uvindices=np.zeros((T, 3), np.uint32), material_indices=midx, meshes=meshes, materials=mats)
+                uvindices=np.zeros((T, 3), np.uint32), material_indices=midx, meshes=meshes, materials=mats), \
+        (centers, radii)
 
 
 SKY_CAMERA = dict(eye=(0.0, 2.0, 16.0), look_at=(0.0, 0.0, 0.0), up=(0.0, 1.0, 0.0), fov_deg=50.0)
+
+
+def frame_spheres(centers: np.ndarray, radii: np.ndarray, seed: int, fov_deg: float = 50.0, aspect: float = 16 / 9,
+                  candidates: int = 256, clearance: float = 1.0) -> dict:
+    """Camera framing a seeded sphere field (the configurations do not fix a
+    camera): among seeded eye positions inside the field's box and look
+    directions, pick the view whose frustum holds the largest summed solid
+    angle of spheres, keeping every sphere surface at least `clearance` away
+    from the eye.  Deterministic in `seed`."""
+    rng = np.random.default_rng(seed + 1000)
+    lo, hi = centers.min(0), centers.max(0)
+    eyes = rng.uniform(lo, hi, (candidates, 3))
+    k = np.arange(candidates) + 0.5
+    phi = np.arccos(1 - 2 * k / candidates)
+    th = np.pi * (1 + 5 ** 0.5) * k
+    dirs = np.stack([np.cos(th) * np.sin(phi), np.cos(phi), np.sin(th) * np.sin(phi)], 1)
+    half_v = np.radians(fov_deg) / 2
+    half_d = np.arctan(np.tan(half_v) * np.sqrt(1 + aspect * aspect))
+    best, best_score = None, -1.0
+    for e in eyes:
+        v = centers - e
+        dist = np.linalg.norm(v, axis=1)
+        if (dist - radii).min() < clearance:
+            continue
+        ang = np.arcsin(np.clip(radii / dist, 0, 1))
+        solid = 2 * np.pi * (1 - np.cos(ang))
+        u = v / dist[:, None]
+        cosang = u @ dirs.T                         # spheres x directions
+        inside = np.arccos(np.clip(cosang, -1, 1)) < (half_v * 0.9)
+        score = (inside * solid[:, None]).sum(0)
+        j = int(np.argmax(score))
+        if score[j] > best_score:
+            best_score, best = float(score[j]), (e, dirs[j])
+    e, d = best
+    up = np.array([0.0, 1.0, 0.0]) if abs(d[1]) < 0.95 else np.array([1.0, 0.0, 0.0])
+    return dict(eye=tuple(float(x) for x in e), look_at=tuple(float(x) for x in e + d), up=tuple(up),
+                fov_deg=fov_deg)
 
 
 def sky_scene(seed: int = 2, width: int = 1920, height: int = 1080, spp: int = 64, bounces: int = 8,
               count: int = 32, level: int = 6, rr: int = 1, mis: bool = False) -> SceneData:
     """C2: 32 subdivision-6 icospheres (2,621,440 triangles) under a
     Hosek-Wilkie sky (turbidity 3, sun elevation 30 deg, ground albedo 0.3)."""
-    g = sphere_field(seed, count, level)
-    cam = dict(SKY_CAMERA, w=width, h=height)
+    g, (c, r) = sphere_field(seed, count, level)
+    cam = dict(frame_spheres(c, r, seed), w=width, h=height)
     return SceneData(**g, skydome_type=capi.NOOR_SKY_PHYSICAL, camera=cam,
                      render=dict(spp=spp, bounces=bounces, rr=rr, mis=int(mis)),
                      hosek=dict(turbidity=3.0, albedo=0.3, sun_lat=float(np.radians(60.0)),
@@ -268,8 +306,8 @@ def env_map(seed: int, width: int = 2048, height: int = 1024, mu: float = -1.0, 
 def env_scene(seed: int = 3, width: int = 1920, height: int = 1080, spp: int = 128, bounces: int = 8,
               count: int = 32, level: int = 6, env_w: int = 2048, env_h: int = 1024, rr: int = 1) -> SceneData:
     """C3: the C2 geometry lit by a 2048x1024 log-normal + lobes map, MIS on."""
-    g = sphere_field(2, count, level)
-    cam = dict(SKY_CAMERA, w=width, h=height)
+    g, (c, r) = sphere_field(2, count, level)
+    cam = dict(frame_spheres(c, r, 2), w=width, h=height)
     return SceneData(**g, skydome_type=capi.NOOR_SKY_HDR, env=env_map(seed, env_w, env_h), camera=cam,
                      render=dict(spp=spp, bounces=bounces, rr=rr, mis=1), name="env")
 
@@ -422,7 +460,11 @@ def make_hosek(h: Optional[dict]) -> capi.HosekSky:
 class Renderer:
     """The reference-facing render context: load_cuda_data on a built
     payload, then cuda_path_tracer / noor_render_frames and film readback.
-    Keeps the camera, spec and sky structs alive for update_cuda_*."""
+    Keeps the camera, spec and sky structs alive for update_cuda_*.
+    The C-ABI keeps one current context per thread, so only the most recently
+    created Renderer of a thread is usable; older ones raise."""
+
+    _current = None
 
     def __init__(self, scene: SceneData, built: Optional[BuiltPayload] = None, intersector: int = 0,
                  film_mode: int = 0, hosek: Optional[capi.HosekSky] = None):
@@ -437,16 +479,24 @@ class Renderer:
         self.hosek = hosek if hosek is not None else make_hosek(scene.hosek)
         capi.call("load_cuda_data", C.byref(self.built.payload), C.byref(self.hosek), C.byref(self.camera),
                   C.byref(self.spec), None)
+        Renderer._current = self
         self.frame = C.c_uint(1)
         self.w, self.h = int(scene.camera["w"]), int(scene.camera["h"])
 
+    def _check(self):
+        if Renderer._current is not self:
+            raise RuntimeError("this Renderer's context was replaced by a newer one on this thread")
+
     def render(self, n_frames: int) -> None:
+        self._check()
         capi.call("noor_render_frames", C.byref(self.frame), n_frames)
 
     def path_tracer(self) -> None:
+        self._check()
         capi.call("cuda_path_tracer", C.byref(self.frame))
 
     def framebuffer(self) -> np.ndarray:
+        self._check()
         out = np.zeros((self.h, self.w, 4), np.float32)
         capi.call("noor_get_framebuffer", _ptr(out), self.w * self.h)
         return out
@@ -462,10 +512,44 @@ class Renderer:
         return s.value
 
     def update_spec(self, **kw):
+        self._check()
         for k, v in kw.items():
             setattr(self.spec, k, v)
         capi.call("update_cuda_spec")
         self.frame = C.c_uint(1)
 
     def close(self):
-        capi.call("device_free_memory")
+        if Renderer._current is self:
+            capi.call("device_free_memory")
+            Renderer._current = None
+
+
+# ------------------------------------------------------- batched frames
+def upload_scene(scene: SceneData, built: Optional[BuiltPayload] = None, intersector: int = 0):
+    """Adds a scene to the current context (noor_scene_upload); returns
+    (scene_id, keep-alive tuple)."""
+    built = built or BuiltPayload(scene)
+    r = scene.render
+    spec = built.default_spec(r.get("bounces", 5), r.get("rr", 1))
+    spec.mis = int(r.get("mis", 0))
+    spec.intersector = intersector
+    hosek = make_hosek(scene.hosek)
+    sid = C.c_uint32()
+    capi.call("noor_scene_upload", C.byref(built.payload), C.byref(hosek), C.byref(spec), C.byref(sid))
+    return sid.value, (built, spec, hosek)
+
+
+def wf_frame(scene_id: int, cam: dict, spp: int, bounces: int = 0, first_frame: int = 1, d_film: int = 0):
+    f = capi.WfFrame()
+    f.scene_id = scene_id
+    f.width, f.height = int(cam["w"]), int(cam["h"])
+    f.spp = spp
+    f.first_frame = first_frame
+    f.bounces = bounces
+    f.camera = make_camera(cam)
+    f.d_film = C.cast(C.c_void_p(d_film), capi.pf) if d_film else capi.pf()
+    return f
+
+
+def wf_params(block: int = 128, capacity: int = 1 << 20, sort: int = 1, graph: int = 1) -> capi.WfParams:
+    return capi.WfParams(block, capacity, sort, graph)

@@ -30,7 +30,7 @@ OUT = Path(__file__).resolve().parent
 # (name, scene constructor) pairs whose reference BVH is frozen
 GOLDEN_SCENES = {
     "room": lambda: scenes.room_scene(seed=1),
-    "spheres": lambda: scenes.SceneData(**scenes.sphere_field(11, 6, 3), name="spheres"),
+    "spheres": lambda: scenes.SceneData(**scenes.sphere_field(11, 6, 3)[0], name="spheres"),
 }
 HOSEK_CASES = [(3.0, 0.3, np.radians(30.0)), (2.0, 0.1, np.radians(10.0)), (5.5, 0.8, np.radians(60.0)),
                (10.0, 0.5, np.radians(45.0)), (1.0, 0.0, np.radians(85.0))]

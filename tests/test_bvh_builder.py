@@ -89,7 +89,7 @@ def test_default_spec_follows_scene_load():
     assert sp.reflection_bias == pytest.approx(1e-4 * r)
     assert sp.bvh_root_node == b.payload.bvh_root_node
     assert sp.lighting_type & _capi.NOOR_LIGHT_SKY_MASK == 0   # 2 lights -> sky off
-    g = scenes.SceneData(**scenes.sphere_field(1, 2, 1), name="x")
+    g = scenes.SceneData(**scenes.sphere_field(1, 2, 1)[0], name="x")
     sp2 = scenes.BuiltPayload(g).default_spec(8, 1)
     assert sp2.lighting_type & _capi.NOOR_LIGHT_SKY_MASK      # infinite light only -> sky on
 
@@ -110,7 +110,7 @@ def test_builder_rejects_bad_input():
 def test_instances_and_transforms():
     """an instance shares its source's bottom-level tree; the top level sees
     the transformed boxes"""
-    g = scenes.sphere_field(3, 1, 2)
+    g = scenes.sphere_field(3, 1, 2)[0]
     T = np.eye(4, dtype=np.float32)
     T[:3, 3] = (5, 0, 0)
     g["meshes"].append(dict(tri_start=0, tri_count=0, to_global=T.reshape(-1, order="F"), instance=0, light_idx=-1))
@@ -129,7 +129,7 @@ def test_live_reference_builder_if_available():
     if not O.ref_available():
         pytest.skip("reference tree not compiled on this machine")
     for seed, count, level in [(21, 5, 3), (22, 3, 4)]:
-        s = scenes.SceneData(**scenes.sphere_field(seed, count, level), name="live")
+        s = scenes.SceneData(**scenes.sphere_field(seed, count, level)[0], name="live")
         b = scenes.BuiltPayload(s)
         nodes, root, order, height = O.ref_build_bvh(b.desc, s.num_triangles)
         assert np.array_equal(b.nodes(), nodes)

@@ -1,0 +1,200 @@
+"""Device shading routines against the oracle: BxDF Eval/Pdf/Sample_f,
+Hosek-Wilkie sky radiance, the FP64-built environment distribution and its
+sampling, and the FP64 GPU Hosek fit against the reference's own fit."""
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from noor_b200 import _capi, scenes
+from oracle.oracle import Oracle
+
+from gpu_util import dev, dev_empty, host
+
+pytestmark = pytest.mark.gpu
+GOLD = Path(__file__).resolve().parent / "golden"
+
+MATS = [scenes.material("diffuse", albedo=(0.2, 0.5, 0.8)),
+        scenes.material("metal", roughness=float(np.sqrt(0.05))),
+        scenes.material("metal", roughness=float(np.sqrt(0.5))),
+        scenes.material("metal", roughness=0.4, distribution=1),
+        scenes.material("glass", ior=1.5)]
+
+
+def _scene(sky=_capi.NOOR_SKY_PHYSICAL, env=None):
+    g = scenes.sphere_field(4, len(MATS), 1)[0]
+    g["materials"] = MATS
+    s = scenes.SceneData(**g, skydome_type=sky, env=env, name="shade")
+    s.camera = dict(scenes.SKY_CAMERA, w=32, h=32)
+    s.render = dict(spp=1, bounces=4, rr=1, mis=0)
+    s.hosek = dict(turbidity=3.0, albedo=0.3, sun_lat=float(np.radians(60)), sun_lon=float(np.pi / 4),
+                   solar_scale=250.0, solar_radius_scale=2.0)
+    return s
+
+
+@pytest.fixture(scope="module")
+def sky():
+    s = _scene()
+    r = scenes.Renderer(s)
+    orc = Oracle(r.built.payload, r.spec, r.hosek)
+    yield r, orc
+    orc.close()
+    r.close()
+
+
+def _dirs(rng, n, zmin=0.05):
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    keep = np.abs(d[:, 2]) > zmin
+    return d[keep]
+
+
+def _records(rng, n):
+    wo = _dirs(rng, 2 * n)[:n]
+    wi = _dirs(rng, 2 * n)[:n]
+    rec = np.zeros((n, 16), np.float32)
+    rec[:, 0:3] = wo
+    rec[:, 3:6] = wi
+    rec[:, 6:8] = rng.random((n, 2))
+    rec[:, 8] = rng.integers(0, len(MATS), n)
+    return rec
+
+
+def _gpu_bsdf(kind, rec):
+    d_in = dev(rec)
+    d_out = dev_empty(rec.shape[0] * 32)
+    _capi.call("noor_eval_bsdf", kind, C.c_void_p(d_in.data_ptr()), C.c_void_p(d_out.data_ptr()), rec.shape[0])
+    return host(d_out, np.float32, (rec.shape[0], 8))
+
+
+def _rel(a, b, floor):
+    return np.abs(a - b) / np.maximum(np.abs(b), floor)
+
+
+@pytest.mark.parametrize("kind", [0, 1, 2])
+def test_bsdf_matches_fp32_transcription(sky, kind):
+    r, orc = sky
+    rec = _records(np.random.default_rng(kind), 50_000)
+    g = _gpu_bsdf(kind, rec)
+    o = orc.eval_bsdf(kind, rec, fp64=False)
+    if kind < 2:
+        cols = [0, 1, 2] if kind == 0 else [3]
+        err = _rel(g[:, cols], o[:, cols], 1e-6)
+        q = np.quantile(err, [0.5, 0.999, 1.0])
+        assert q[1] < 1e-5, q
+        return
+    # Sample_f: the sampled direction (absolute), its value and pdf (relative);
+    # the visible-normal samplers invert numerically, so a few samples near
+    # their branch points may land elsewhere
+    same = g[:, 7] == o[:, 7]
+    assert same.mean() > 0.999
+    werr = np.abs(g[same, 4:7] - o[same, 4:7]).max(1)
+    ferr = _rel(g[same, 0:4], o[same, 0:4], 1e-6).max(1)
+    qw, qf = np.quantile(werr, [0.5, 0.999]), np.quantile(ferr, [0.5, 0.999])
+    assert qw[1] < 1e-3 and qw[0] < 1e-6, qw
+    assert qf[1] < 1e-3 and qf[0] < 1e-5, qf
+
+
+@pytest.mark.parametrize("kind", [0, 1])
+def test_bsdf_against_fp64(sky, kind):
+    r, orc = sky
+    rec = _records(np.random.default_rng(10 + kind), 20_000)
+    g = _gpu_bsdf(kind, rec)
+    o = orc.eval_bsdf(kind, rec, fp64=True)
+    cols = [0, 1, 2] if kind == 0 else [3]
+    assert np.quantile(_rel(g[:, cols], o[:, cols], 1e-6), 0.99) < 1e-5
+
+
+def test_sky_radiance(sky):
+    r, orc = sky
+    rng = np.random.default_rng(3)
+    d = rng.normal(size=(200_000, 3)).astype(np.float32)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    sun = np.array(r.hosek.solar_dir[:], np.float32)
+    gamma = np.arccos(np.clip(d @ sun, -1, 1))
+    keep = np.abs(gamma - r.hosek.solar_radius) > 2e-3
+    d = np.ascontiguousarray(d[keep])
+    d_in = dev(d)
+    d_out = dev_empty(d.shape[0] * 12)
+    _capi.call("noor_eval_sky", C.c_void_p(d_in.data_ptr()), C.c_void_p(d_out.data_ptr()), d.shape[0])
+    g = host(d_out, np.float32, (d.shape[0], 3))
+    o32 = orc.eval_sky(d, fp64=False)
+    o64 = orc.eval_sky(d, fp64=True)
+    assert (g[d[:, 1] < 0] == 0).all()
+    up = d[:, 1] > 0
+    assert np.quantile(_rel(g[up], o32[up], 1e-6), 0.999) < 1e-5
+    assert np.quantile(_rel(g[up], o64[up], 1e-6), 0.99) < 1e-5
+
+
+def test_hosek_fit_matches_reference():
+    g = np.load(GOLD / "hosek_states.npz")
+    ds = scenes.hosek_dataset()
+    for (t, a, e), ref in zip(g["cases"], g["states"]):
+        out = _capi.HosekSky()
+        alb = (C.c_float * 3)(a, a, a)
+        _capi.call("noor_hosek_fit", ds.ctypes.data_as(C.POINTER(C.c_float)), float(t), alb,
+                   float(np.pi / 2 - e), 0.0, 250.0, 2.0, C.byref(out))
+        st = out.state[0]
+        mine = np.array([st.configs[c][i] for c in range(3) for i in range(9)] + list(st.radiances))
+        assert np.allclose(mine, ref, rtol=1e-5, atol=1e-7), (t, a, e)
+
+
+@pytest.mark.parametrize("which", ["sky", "env"])
+def test_env_distribution_fp64(which, sky):
+    if which == "sky":
+        r, orc = sky
+    else:
+        env = scenes.env_map(8, 256, 128)
+        s = _scene(sky=_capi.NOOR_SKY_HDR, env=env)
+        r = scenes.Renderer(s)
+        orc = Oracle(r.built.payload, r.spec, r.hosek)
+    try:
+        w, h = C.c_int(), C.c_int()
+        _capi.call("noor_get_env_distribution", C.byref(w), C.byref(h), None, None, None, None, None)
+        W, H = w.value, h.value
+        func = np.zeros(W * H, np.float32)
+        cdf = np.zeros(H * (W + 1), np.float32)
+        row = np.zeros(H, np.float32)
+        mcdf = np.zeros(H + 1, np.float32)
+        mi = C.c_double()
+        P = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))
+        _capi.call("noor_get_env_distribution", None, None, P(func), P(cdf), P(row), P(mcdf), C.byref(mi))
+        ref = orc.env_distribution()
+        assert (ref["w"], ref["h"]) == (W, H)
+        tol = 1e-6 if which == "env" else 1e-4
+        assert np.quantile(_rel(func, ref["func"].ravel(), 1e-12), 0.999) < tol
+        # rows whose integral is negligible (the sky's horizon row, where the
+        # FP32 sign of cos(theta) decides between zero and a tiny radiance)
+        # fall back to a uniform CDF on one side only; they carry no
+        # probability mass in the marginal
+        live = ref["row_int"] > 1e-6 * ref["row_int"].max()
+        # rows holding a cell whose FP32 value differs by more than 1e-3
+        # (cells the sun disc's edge cuts: a subsample in or out of the disc
+        # changes the radiance 10^4-fold) are compared through their integral
+        frel = _rel(func.reshape(H, W), ref["func"], 1e-12)
+        clean = live & (frel.max(1) < 1e-3)
+        assert clean.sum() >= live.sum() - max(4, live.sum() // 100), (clean.sum(), live.sum())
+        assert np.abs(cdf.reshape(H, W + 1)[clean] - ref["cdf"][clean]).max() < 1e-5
+        assert np.quantile(np.abs(mcdf - ref["marg_cdf"]), 0.999) < 1e-4
+        assert mi.value == pytest.approx(ref["marg_int"], rel=1e-3)
+        # sampling: GPU (x, y, pdf) against FP64
+        u = np.random.default_rng(1).random((50_000, 2)).astype(np.float32)
+        d_u = dev(u)
+        d_o = dev_empty(u.shape[0] * 16)
+        _capi.call("noor_eval_env_sample", C.c_void_p(d_u.data_ptr()), C.c_void_p(d_o.data_ptr()), u.shape[0])
+        gs = host(d_o, np.float32, (u.shape[0], 4))
+        os_ = orc.env_sample(u)
+        same_cell = (np.floor(gs[:, 0] * W) == np.floor(os_[:, 0] * W)) & (np.floor(gs[:, 1] * H) == np.floor(os_[:, 1] * H))
+        rows = np.clip((os_[:, 1] * H).astype(int), 0, H - 1)
+        in_clean = clean[rows]
+        assert same_cell[in_clean].mean() > 0.999
+        m = same_cell & in_clean
+        assert np.quantile(np.abs(gs[m, :2] - os_[m, :2]), 0.999) < 1e-5
+        assert np.quantile(_rel(gs[m, 2], os_[m, 2], 1e-12), 0.999) < 1e-4
+        # the pdf reported at sampling equals the pdf evaluated at the sample
+        assert np.quantile(_rel(gs[:, 2], gs[:, 3], 1e-12), 0.999) < 1e-4
+    finally:
+        if which == "env":
+            orc.close()
+            r.close()
