@@ -716,18 +716,3 @@ extern "C" int noor_wavefront_autotune(const noor_wf_frame* frames, uint32_t n_f
     return NOOR_OK;
 }
 
-// ---------------------------------------------------------------- adjoint
-extern "C" int noor_adjoint_forward(const noor_adjoint_desc* desc, float* d_image) {
-    (void)desc;
-    (void)d_image;
-    return set_error(NOOR_ERR_UNSUPPORTED, "adjoint not built yet");
-}
-extern "C" int noor_adjoint_backward(const noor_adjoint_desc* desc, const float* d_grad_image, float* d_grad_albedo,
-                                     float* d_grad_roughness, float* d_grad_env) {
-    (void)desc;
-    (void)d_grad_image;
-    (void)d_grad_albedo;
-    (void)d_grad_roughness;
-    (void)d_grad_env;
-    return set_error(NOOR_ERR_UNSUPPORTED, "adjoint not built yet");
-}

@@ -27,12 +27,13 @@ IDENTITY = np.eye(4, dtype=np.float32).reshape(-1, order="F")
 
 
 def material(kind: str, albedo=(0.5, 0.5, 0.5), roughness: float = 0.1, ior: float = 1.5,
-             emittance=(0.0, 0.0, 0.0), distribution: int = 0) -> dict:
+             emittance=(0.0, 0.0, 0.0), distribution: int = 0, specular=(1.0, 1.0, 1.0)) -> dict:
     """Constant material parameters (AssetLoader getters) for one of
-    'diffuse', 'metal' (gold conductor), 'glass' or 'emitter'."""
+    'diffuse', 'metal' (gold conductor, `specular` tints it), 'glass' or
+    'emitter'."""
     types = {"diffuse": capi.NOOR_DIFFUSE, "metal": capi.NOOR_METAL, "glass": capi.NOOR_GLASS,
              "emitter": capi.NOOR_EMITTER}
-    return dict(diffuse=tuple(albedo), specular=(1.0, 1.0, 1.0), transmission=(1.0, 1.0, 1.0),
+    return dict(diffuse=tuple(albedo), specular=tuple(float(x) for x in specular), transmission=(1.0, 1.0, 1.0),
                 emittance=tuple(emittance), transparency=(1.0, 1.0, 1.0),
                 ior=GOLD_ETA if kind == "metal" else (ior, ior, ior), k=GOLD_K if kind == "metal" else (0, 0, 0),
                 roughness=(roughness, roughness), coat_weight=1.0, coat_roughness=0.001, coat_thickness=1.0,
@@ -310,6 +311,35 @@ def env_scene(seed: int = 3, width: int = 1920, height: int = 1080, spp: int = 1
     cam = dict(frame_spheres(c, r, 2), w=width, h=height)
     return SceneData(**g, skydome_type=capi.NOOR_SKY_HDR, env=env_map(seed, env_w, env_h), camera=cam,
                      render=dict(spp=spp, bounces=bounces, rr=rr, mis=1), name="env")
+
+
+def adjoint_scene(seed: int = 5, width: int = 512, height: int = 512, spp: int = 16, bounces: int = 4,
+                  count: int = 10, level: int = 5, n_materials: int = 64, env_w: int = 512,
+                  env_h: int = 256) -> SceneData:
+    """C5: `count` subdivision-`level` icospheres (10 x 20,480 = 204,800
+    triangles by default) with `n_materials` materials assigned per triangle
+    as (sphere * 20 + base icosahedron face) mod n_materials: the first half
+    Lambert (albedo U[0.1,0.9]^3), the second half GGX gold conductors
+    (tint U[0.1,0.9]^3, alpha U[0.05,0.5]); lit by an env_w x env_h map
+    (log-normal background plus three lobes of peak 20, below the radiance
+    clamp); MIS on, Russian roulette off (rr = bounces)."""
+    g, (c, r) = sphere_field(seed, count, level, box=6.0, rmin=0.5, rmax=1.5, kinds=("diffuse",))
+    rng = np.random.default_rng(seed + 77)
+    nf = 20 * 4 ** level
+    tri = np.arange(count * nf)
+    # subdivision keeps a face's children at indices congruent mod 20
+    g["material_indices"] = (((tri // nf) * 20 + (tri % nf) % 20) % n_materials).astype(np.uint32)
+    mats = []
+    for i in range(n_materials):
+        if i < n_materials // 2:
+            mats.append(material("diffuse", albedo=tuple(rng.uniform(0.1, 0.9, 3))))
+        else:
+            mats.append(material("metal", roughness=float(np.sqrt(rng.uniform(0.05, 0.5))),
+                                 specular=tuple(rng.uniform(0.1, 0.9, 3))))
+    g["materials"] = mats
+    cam = dict(frame_spheres(c, r, seed, aspect=width / height, clearance=0.5), w=width, h=height)
+    return SceneData(**g, skydome_type=capi.NOOR_SKY_HDR, env=env_map(seed, env_w, env_h, peak=20.0), camera=cam,
+                     render=dict(spp=spp, bounces=bounces, rr=bounces, mis=1), name="adjoint")
 
 
 # ------------------------------------------------------------ C-ABI glue

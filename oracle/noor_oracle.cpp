@@ -1135,6 +1135,319 @@ struct Ctx {
     Scene sc;
 };
 
+// ------------------------------------------------ adjoint reference (FP64)
+// The library's differentiable estimator: sampling detached (directions,
+// light picks, MIS weights, pdfs and every early exit from the scene as
+// loaded), BSDF values and environment radiance from parameter arrays
+// (albedo M x 3 -- Lambert reflectance or conductor tint --, roughness M,
+// env texels H x W x 3).  Its gradient is taken here by the product rule
+// over the stored path (L = sum_t B_k(t) * v_t, B_k the product of the
+// scatter factors before vertex k), with the roughness derivative of f by
+// an FP64 central difference -- an independent restatement of what the
+// library computes by path replay with analytic derivatives.
+struct AdjPar {
+    const float* alb;
+    const float* rough;
+    const float* env;
+    uint32_t bounces;
+};
+struct BW {
+    size_t idx[4];
+    double w[4];
+};
+// texel weights of env_bilinear for direction dir
+inline BW env_weights_d(const Scene& sc, V<double> dir) {
+    const double u = sph_phi(dir) * K<double>::inv_2pi, v = sph_theta(dir) * K<double>::inv_pi;
+    const int W = sc.ew, H = sc.eh;
+    const double x = u * W - 0.5, y = v * H - 0.5;
+    const double fx0 = std::floor(x), fy0 = std::floor(y);
+    const double ax = x - fx0, ay = y - fy0;
+    int x0 = (int)fx0, y0 = (int)fy0, x1 = x0 + 1, y1 = y0 + 1;
+    x0 = std::min(std::max(x0, 0), W - 1);
+    x1 = std::min(std::max(x1, 0), W - 1);
+    y0 = std::min(std::max(y0, 0), H - 1);
+    y1 = std::min(std::max(y1, 0), H - 1);
+    BW b;
+    b.idx[0] = (size_t)y0 * W + x0;
+    b.idx[1] = (size_t)y0 * W + x1;
+    b.idx[2] = (size_t)y1 * W + x0;
+    b.idx[3] = (size_t)y1 * W + x1;
+    b.w[0] = (1 - ax) * (1 - ay);
+    b.w[1] = ax * (1 - ay);
+    b.w[2] = (1 - ax) * ay;
+    b.w[3] = ax * ay;
+    return b;
+}
+inline V<double> env_param(const AdjPar& P, const BW& b) {
+    V<double> c = mk(0.0, 0.0, 0.0);
+    for (int k = 0; k < 4; ++k) c = c + b.w[k] * v3f<double>(P.env + 3 * b.idx[k]);
+    return c;
+}
+// conductor value without tint, alpha = max(r^2, 1e-3) on both axes
+inline V<double> cond_untinted(const Scene::Mat& m, V<double> wo, V<double> wi, double r) {
+    const V<double> z = mk(0.0, 0.0, 0.0);
+    if (!same(wo, wi)) return z;
+    const double cO = std::fabs(wo.z), cI = std::fabs(wi.z);
+    if (cI == 0 || cO == 0) return z;
+    V<double> wh = nrm(wi + wo);
+    if (black(wh)) return z;
+    wh = wh * signv(wh.z);
+    const V<double> F = fr_cond(dot(wo, wh), v3f<double>(m.ior), v3f<double>(m.k));
+    Micro<double> mf;
+    mf.ax = mf.ay = std::max(r * r, (double)1e-3f);
+    mf.dist = m.dist;
+    return F * mf.D(wh) * mf.G(wo, wi) / (4.0 * cI * cO);
+}
+// f with the parameters, df/dalbedo (per channel) and df/droughness
+struct FVal {
+    V<double> f, f_alb, f_r;
+    bool has;
+};
+inline FVal eval_f(uint32_t lobe, const Scene::Mat& m0, const AdjPar& P, uint32_t mi, const Frame<double>& F,
+                   V<double> woW, V<double> wiW) {
+    const V<double> z = mk(0.0, 0.0, 0.0);
+    FVal r{z, z, z, false};
+    const V<double> wo = to_local(F, woW), wi = to_local(F, wiW);
+    if (!(dot(wiW, F.ng) * dot(woW, F.ng) > 0)) return r;
+    const V<double> a = v3f<double>(P.alb + 3 * mi);
+    if (lobe == kLambert) {
+        r.f_alb = mk(K<double>::inv_pi, K<double>::inv_pi, K<double>::inv_pi);
+        r.f = a * K<double>::inv_pi;
+        r.has = true;
+    } else if (lobe == kCond) {
+        const double rr = P.rough[mi];
+        const V<double> fu = cond_untinted(m0, wo, wi, rr);
+        r.f_alb = fu;
+        r.f = fu * a;
+        const double h = 1e-6;
+        if (rr * rr > (double)1e-3f && (rr - h) * (rr - h) > (double)1e-3f)
+            r.f_r = (cond_untinted(m0, wo, wi, rr + h) - cond_untinted(m0, wo, wi, rr - h)) * a / (2 * h);
+        r.has = true;
+    }
+    return r;
+}
+struct ATerm {
+    size_t k;             // scatter factors before this term
+    V<double> val, d_alb, d_r, fs;
+    uint32_t mat;
+    bool has_mat, env;
+    BW bw;
+    double xscale;
+};
+struct AVtx {
+    V<double> s, ds_alb, ds_r;
+    uint32_t mat;
+    bool has_mat;
+};
+inline void add_term(std::vector<ATerm>& ts, size_t k, V<double> X, const FVal& fv, double s, uint32_t mat, bool env,
+                     const BW& bw, double xscale) {
+    ATerm t;
+    t.k = k;
+    t.val = X * fv.f * s;
+    t.d_alb = X * fv.f_alb * s;
+    t.d_r = X * fv.f_r * s;
+    t.fs = fv.f * s;
+    t.mat = mat;
+    t.has_mat = fv.has;
+    t.env = env;
+    t.bw = bw;
+    t.xscale = xscale;
+    ts.push_back(t);
+}
+// one path of the detached estimator (pathtracer() with the parameter
+// substitution, Russian roulette off)
+inline void adj_path(const Scene& sc, const AdjPar& P, V<double> o, V<double> d, Rng& rng, int isect,
+                     std::vector<AVtx>& vs, std::vector<ATerm>& ts) {
+    vs.clear();
+    ts.clear();
+    const V<double> zero = mk(0.0, 0.0, 0.0);
+    const double bias = sc.S->reflection_bias;
+    const bool hdr = sc.S->skydome_type == NOOR_SKY_HDR;
+    const bool mis = sc.S->mis != 0;
+    const uint32_t nonspec = B_ALL & ~B_SPEC;
+    const int na = sc.P->num_area_lights;
+    bool specb = false;
+    for (uint32_t b = 0; b < P.bounces; ++b) {
+        double tmax = K<double>::inf;
+        Hit h{0, 0, 0, 0, 0};
+        if (!traverse<double>(sc, o, d, tmax, &h, false, isect, nullptr)) {
+            if (sc.sky_on && (b == 0 || specb)) {
+                const V<double> dir = nrm(d);
+                FVal one{mk(1.0, 1.0, 1.0), zero, zero, false};
+                BW bw{};
+                if (hdr) {
+                    bw = env_weights_d(sc, dir);
+                    add_term(ts, vs.size(), env_param(P, bw), one, 1.0, 0, true, bw, 1.0);
+                } else {
+                    add_term(ts, vs.size(), env_eval<double>(sc, dir), one, 1.0, 0, false, bw, 1.0);
+                }
+            }
+            break;
+        }
+        Is<double> I;
+        I.p = o + tmax * d;
+        I.wo = nrm(-1.0 * d);
+        I.mt = h.mt;
+        I.lobe = lobe_of(h.mt);
+        I.mat = sc.P->attribute_indices[4 * (size_t)h.tri + 3];
+        if (I.mt & kEmitMat) {
+            if (b == 0 || specb) {
+                V<double> Le;
+                if (I.mt & NOOR_MESHLIGHT) {
+                    const noor_area_light& A = sc.P->area_lights[h.ins];
+                    Le = (A.two_sided || dot(d, area_p<double>(A, 3)) < 0) ? v3f<double>(A.ke) : zero;
+                } else {
+                    const Scene::Mat& em = sc.mats[I.mat];
+                    Le = (double)em.emitter_scale * v3f<double>(em.emittance);
+                }
+                FVal one{mk(1.0, 1.0, 1.0), zero, zero, false};
+                add_term(ts, vs.size(), Le, one, 1.0, 0, false, BW{}, 1.0);
+            }
+            break;
+        }
+        I.F = tangent<double>(sc, h);
+        const Scene::Mat& m0 = sc.mats[I.mat];
+        const size_t k = vs.size();
+        // direct lighting (direct<T> with the substitution)
+        const int nl = sc.sky_on ? sc.num_lights : sc.num_lights - 1;
+        if (!(I.mt & kSpecMat) && nl > 0) {
+            const int li = (int)((float)nl * rng.next());
+            V<double> Li = zero, wi = zero, to = zero;
+            double lpdf = 0;
+            if (li < na) {
+                const noor_area_light& A = sc.P->area_lights[li];
+                const float r1 = rng.next();
+                const float r2 = rng.next();
+                const V<double> n = area_p<double>(A, 3);
+                const V<double> p = area_p<double>(A, 0) + area_p<double>(A, 1) * (double)r1 +
+                                    area_p<double>(A, 2) * (double)r2 + bias * n;
+                const V<double> w = I.p - p;
+                lpdf = len2(w) / (std::fabs(dot(n, -1.0 * w)) * (double)A.shape.area);
+                if (std::isinf(lpdf)) lpdf = 0;
+                if (lpdf != 0) {
+                    to = p;
+                    const V<double> v = to - I.p;
+                    wi = v / len(v);
+                    Li = (A.two_sided || dot(wi, n) < 0) ? v3f<double>(A.ke) : zero;
+                }
+            } else {
+                const V<double> dir = env_sample_dir<double>(sc, rng, lpdf);
+                if (std::isinf(lpdf) || std::isnan(lpdf)) lpdf = 0;
+                to = I.p + 2.0 * (double)sc.S->world_radius * dir;
+                const V<double> v = to - I.p;
+                wi = v / len(v);
+                Li = sc.sky_on ? env_eval<double>(sc, wi) : zero;
+            }
+            Li = Li * (double)nl;
+            if (lpdf != 0 && !black(Li)) {
+                const V<double> f0 = bsdf_eval<double>(I.lobe, m0, I.F, I.wo, wi, nonspec);
+                if (!black(f0)) {
+                    const V<double> so = spawn(I, wi, bias);
+                    if (!occl<double>(sc, so, wi, len(so - to), isect, nullptr)) {
+                        const FVal fv = eval_f(I.lobe, m0, P, I.mat, I.F, I.wo, wi);
+                        double w = 1;
+                        if (mis) {
+                            const double sp = bsdf_pdf<double>(I.lobe, m0, I.F, I.wo, wi, nonspec);
+                            w = (lpdf * lpdf) / (lpdf * lpdf + sp * sp);
+                        }
+                        const double s = std::fabs(dot(wi, I.F.n)) * w / lpdf;
+                        const bool env = li >= na && hdr;
+                        BW bw{};
+                        V<double> X = Li;
+                        if (env) {
+                            bw = env_weights_d(sc, wi);
+                            X = env_param(P, bw) * (double)nl;
+                        }
+                        add_term(ts, k, X, fv, s, I.mat, env, bw, (double)nl);
+                    }
+                }
+            }
+            if (mis) {
+                rng.next();
+                rng.next();
+                double sp;
+                uint32_t st;
+                const V<double> f0 = bsdf_sample<double>(I.lobe, m0, I.F, I.wo, nonspec, rng, wi, sp, st);
+                bool go = !black(f0) && sp != 0;
+                double w = 1;
+                if (go && !(st & B_SPEC)) {
+                    double lp = 0;
+                    if (li < na) {
+                        const noor_area_light& A = sc.P->area_lights[li];
+                        double tm = K<double>::inf;
+                        if (quad_hit<double>(A, I.p, wi, tm)) {
+                            const V<double> p = I.p + tm * wi;
+                            lp = len2(p - I.p) / (std::fabs(dot(area_p<double>(A, 3), -1.0 * wi)) * (double)A.shape.area);
+                            if (std::isinf(lp)) lp = 0;
+                        }
+                    } else {
+                        lp = env_pdf<double>(sc, wi);
+                    }
+                    if (std::isinf(lp)) lp = 0;
+                    if (lp == 0) go = false;
+                    else w = (sp * sp) / (sp * sp + lp * lp);
+                }
+                if (go) {
+                    const V<double> so = spawn(I, wi, bias);
+                    double tm = 2.0 * (double)sc.S->world_radius;
+                    bool lh;
+                    V<double> Le;
+                    if (li < na) {
+                        const noor_area_light& A = sc.P->area_lights[li];
+                        lh = quad_hit<double>(A, so, wi, tm);
+                        Le = (A.two_sided || dot(wi, area_p<double>(A, 3)) < 0) ? v3f<double>(A.ke) : zero;
+                    } else {
+                        lh = sc.sky_on;
+                        Le = sc.sky_on ? env_eval<double>(sc, wi) : zero;
+                    }
+                    if (lh && !black(Le)) {
+                        const V<double> to2 = so + tm * wi;
+                        const V<double> v = to2 - I.p;
+                        const V<double> vwi = v / len(v);
+                        const V<double> so2 = spawn(I, vwi, bias);
+                        if (!occl<double>(sc, so2, vwi, len(so2 - to2), isect, nullptr)) {
+                            const FVal fv = eval_f(I.lobe, m0, P, I.mat, I.F, I.wo, wi);
+                            const double s = std::fabs(dot(wi, I.F.n)) * w / sp;
+                            const bool env = li >= na && hdr;
+                            BW bw{};
+                            V<double> X = Le;
+                            if (env) {
+                                bw = env_weights_d(sc, wi);
+                                X = env_param(P, bw);
+                            }
+                            add_term(ts, k, X, fv, s, I.mat, env, bw, 1.0);
+                        }
+                    }
+                }
+            }
+        }
+        // scatter
+        rng.next();
+        rng.next();
+        V<double> wi;
+        double pdf;
+        uint32_t st;
+        const V<double> f0 = bsdf_sample<double>(I.lobe, m0, I.F, I.wo, B_ALL, rng, wi, pdf, st);
+        if (pdf == 0) break;
+        const double cs = std::fabs(dot(wi, I.F.n)) / pdf;
+        AVtx v{zero, zero, zero, I.mat, false};
+        if (st & B_SPEC) {
+            v.s = f0 * cs;
+        } else {
+            const FVal fv = eval_f(I.lobe, m0, P, I.mat, I.F, I.wo, wi);
+            v.s = fv.f * cs;
+            v.ds_alb = fv.f_alb * cs;
+            v.ds_r = fv.f_r * cs;
+            v.has_mat = fv.has;
+        }
+        vs.push_back(v);
+        if (!(I.mt & kTranspMat) && dot(wi, I.F.ng) < 0) break;
+        specb = (I.mt & kSpecMat) != 0;
+        o = spawn(I, wi, bias);
+        d = wi;
+    }
+}
+
 }  // namespace orc
 
 using namespace orc;
@@ -1363,3 +1676,116 @@ OR_API void oracle_env_sample(void* h, const float* u, double* out, size_t n) {
 }
 
 OR_API uint32_t oracle_tea16(uint32_t a, uint32_t b) { return tea16(a, b); }
+
+// FP64 reference of the library's adjoint (noor_adjoint_forward/backward):
+// img = per-pixel mean of clamp(L, 0, 100) over frames [f0, f0 + spp);
+// gradients of sum(grad_img * img) with respect to albedo (M x 3),
+// roughness (M) and env texels (env_h x env_w x 3), accumulated in FP64.
+// grad_img may be null (forward only).
+OR_API void oracle_adjoint(void* h, const noor_camera* C, uint32_t f0, uint32_t spp, uint32_t bounces,
+                           const float* alb, const float* rough, const float* env3, const float* grad_img, int isect,
+                           int threads, double* img, double* g_alb, double* g_rough, double* g_env) {
+    const Scene& sc = ((Ctx*)h)->sc;
+    const AdjPar P{alb, rough, env3, bounces};
+    const uint32_t M = sc.P->num_materials;
+    const size_t NE = (size_t)sc.ew * sc.eh * 3;
+    const uint32_t npix = C->w * C->h;
+    const int T = std::max(1, threads);
+    std::atomic<uint32_t> next{0};
+    struct Acc {
+        std::vector<double> alb, rough, env;
+    };
+    std::vector<Acc> acc(T);
+    auto work = [&](int tid) {
+        Acc& A = acc[tid];
+        if (grad_img) {
+            A.alb.assign((size_t)M * 3, 0.0);
+            A.rough.assign(M, 0.0);
+            A.env.assign(NE, 0.0);
+        }
+        std::vector<AVtx> vs;
+        std::vector<ATerm> ts;
+        std::vector<V<double>> B;
+        for (;;) {
+            const uint32_t b0 = next.fetch_add(16);
+            if (b0 >= npix) break;
+            const uint32_t e0 = std::min(b0 + 16, npix);
+            for (uint32_t p = b0; p < e0; ++p) {
+                V<double> sum = mk(0.0, 0.0, 0.0);
+                const V<double> gi = grad_img ? v3f<double>(grad_img + 3 * (size_t)p) * (1.0 / spp) : mk(0.0, 0.0, 0.0);
+                for (uint32_t f = 0; f < spp; ++f) {
+                    Rng rng{tea16(p, f0 + f)};
+                    V<double> o, d;
+                    cam_ray<double>(*C, p % C->w, p / C->w, rng, o, d);
+                    adj_path(sc, P, o, d, rng, isect, vs, ts);
+                    B.assign(vs.size() + 1, mk(1.0, 1.0, 1.0));
+                    for (size_t j = 0; j < vs.size(); ++j) B[j + 1] = B[j] * vs[j].s;
+                    V<double> L = mk(0.0, 0.0, 0.0);
+                    for (const ATerm& t : ts) L = L + B[t.k] * t.val;
+                    sum = sum + mk(clampv(L.x, 0.0, 100.0), clampv(L.y, 0.0, 100.0), clampv(L.z, 0.0, 100.0));
+                    if (!grad_img) continue;
+                    // derivative of the final clamp
+                    const V<double> g = mk(L.x > 0 && L.x < 100 ? gi.x : 0.0, L.y > 0 && L.y < 100 ? gi.y : 0.0,
+                                           L.z > 0 && L.z < 100 ? gi.z : 0.0);
+                    if (black(g)) continue;
+                    for (const ATerm& t : ts) {
+                        const V<double> gB = g * B[t.k];
+                        if (t.has_mat) {
+                            const V<double> da = gB * t.d_alb;
+                            A.alb[3 * t.mat] += da.x;
+                            A.alb[3 * t.mat + 1] += da.y;
+                            A.alb[3 * t.mat + 2] += da.z;
+                            const V<double> dr = gB * t.d_r;
+                            A.rough[t.mat] += dr.x + dr.y + dr.z;
+                        }
+                        if (t.env) {
+                            const V<double> ge = gB * t.fs * t.xscale;
+                            for (int q = 0; q < 4; ++q) {
+                                double* e = &A.env[3 * t.bw.idx[q]];
+                                e[0] += ge.x * t.bw.w[q];
+                                e[1] += ge.y * t.bw.w[q];
+                                e[2] += ge.z * t.bw.w[q];
+                            }
+                        }
+                        // scatter factors before the term
+                        for (size_t j = 0; j < t.k; ++j) {
+                            if (!vs[j].has_mat) continue;
+                            V<double> pj = mk(1.0, 1.0, 1.0);
+                            for (size_t i = 0; i < t.k; ++i)
+                                if (i != j) pj = pj * vs[i].s;
+                            const V<double> base = g * pj * t.val;
+                            const V<double> da = base * vs[j].ds_alb;
+                            A.alb[3 * vs[j].mat] += da.x;
+                            A.alb[3 * vs[j].mat + 1] += da.y;
+                            A.alb[3 * vs[j].mat + 2] += da.z;
+                            const V<double> dr = base * vs[j].ds_r;
+                            A.rough[vs[j].mat] += dr.x + dr.y + dr.z;
+                        }
+                    }
+                }
+                if (img) {
+                    img[3 * (size_t)p] = sum.x / spp;
+                    img[3 * (size_t)p + 1] = sum.y / spp;
+                    img[3 * (size_t)p + 2] = sum.z / spp;
+                }
+            }
+        }
+    };
+    std::vector<std::thread> th;
+    for (int t = 0; t < T; ++t) th.emplace_back(work, t);
+    for (auto& x : th) x.join();
+    if (!grad_img) return;
+    for (size_t i = 0; i < (size_t)M * 3; ++i) {
+        g_alb[i] = 0;
+        for (auto& a : acc) g_alb[i] += a.alb[i];
+    }
+    for (size_t i = 0; i < M; ++i) {
+        g_rough[i] = 0;
+        for (auto& a : acc) g_rough[i] += a.rough[i];
+    }
+    if (g_env)
+        for (size_t i = 0; i < NE; ++i) {
+            g_env[i] = 0;
+            for (auto& a : acc) g_env[i] += a.env[i];
+        }
+}

@@ -48,6 +48,8 @@ def lib() -> C.CDLL:
         L.oracle_eval_sky.argtypes = [vp, vp, vp, sz, C.c_int]
         L.oracle_env_distribution.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp]
         L.oracle_env_sample.argtypes = [vp, vp, vp, sz]
+        L.oracle_adjoint.argtypes = [vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, vp, vp, vp, vp, C.c_int, C.c_int,
+                                     vp, vp, vp, vp]
         L.oracle_tea16.restype = C.c_uint32
         L.oracle_tea16.argtypes = [C.c_uint32, C.c_uint32]
         _orc = L
@@ -139,6 +141,24 @@ class Oracle:
         lib().oracle_env_distribution(self.h, None, None, _p(func), _p(cdf), _p(row), _p(mcdf), C.addressof(mi))
         return dict(w=W, h=H, func=func.reshape(H, W), cdf=cdf.reshape(H, W + 1), row_int=row, marg_cdf=mcdf,
                     marg_int=mi.value)
+
+    def adjoint(self, camera, frame0: int, spp: int, bounces: int, albedo: np.ndarray, roughness: np.ndarray,
+                env: np.ndarray, grad_img: np.ndarray = None, isect: int = 0, threads: int = 8):
+        """FP64 detached-sampling estimator: image (h*w, 3) and, when grad_img
+        is given, the gradients of sum(grad_img * image) w.r.t. albedo (M,3),
+        roughness (M,) and env texels (H,W,3)."""
+        alb = np.ascontiguousarray(albedo, np.float32)
+        rough = np.ascontiguousarray(roughness, np.float32)
+        env3 = np.ascontiguousarray(env, np.float32)
+        npix = camera.w * camera.h
+        img = np.zeros((npix, 3))
+        ga = np.zeros(alb.shape)
+        gr = np.zeros(rough.shape)
+        ge = np.zeros(env3.shape)
+        gi = None if grad_img is None else np.ascontiguousarray(grad_img, np.float32)
+        lib().oracle_adjoint(self.h, C.addressof(camera), frame0, spp, bounces, _p(alb), _p(rough), _p(env3),
+                             None if gi is None else _p(gi), isect, threads, _p(img), _p(ga), _p(gr), _p(ge))
+        return (img, ga, gr, ge) if gi is not None else img
 
     def env_sample(self, u: np.ndarray) -> np.ndarray:
         out = np.zeros(u.shape[0] * 4)

@@ -1,0 +1,179 @@
+"""Path-replay adjoint (noor_adjoint_forward / noor_adjoint_backward) on the
+differentiable-rendering configuration: 10 subdivision-5 icospheres
+(204,800 triangles), 64 materials, a 512x256 env map, depth 4, MIS on,
+Russian roulette off.
+
+  * forward at the loaded parameters equals the megakernel's render;
+  * gradients equal the FP64 oracle's (stored-path product rule, an
+    independent formulation) on a 64x64 / 4 spp image;
+  * gradients equal central finite differences (eps = 1e-3) of the forward
+    on 256 random parameters at the full 512x512 / 16 spp size;
+  * the torch.autograd.Function wrapper returns the entry points' gradients.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+import torch
+
+from noor_b200 import _capi, scenes
+from noor_b200.adjoint import render, scene_parameters
+from oracle.oracle import Oracle
+
+from gpu_util import THREADS
+
+pytestmark = pytest.mark.gpu
+
+EPS = 1e-3
+
+
+@pytest.fixture(scope="module")
+def full():
+    s = scenes.adjoint_scene()
+    r = scenes.Renderer(s)
+    yield s, r
+    r.close()
+
+
+def _grads(s, alb, rough, env, gi, spp, first_frame=1):
+    """direct C-ABI backward"""
+    from noor_b200.adjoint import _desc
+    ga, gr, ge = torch.zeros_like(alb), torch.zeros_like(rough), torch.zeros_like(env)
+    torch.cuda.synchronize()
+    d = _desc((s.camera["w"], s.camera["h"], spp, first_frame, 0), alb, rough, env)
+    _capi.call("noor_adjoint_backward", C.byref(d), C.c_void_p(gi.data_ptr()), C.c_void_p(ga.data_ptr()),
+               C.c_void_p(gr.data_ptr()), C.c_void_p(ge.data_ptr()))
+    return ga, gr, ge
+
+
+def test_forward_at_loaded_parameters_equals_megakernel():
+    s = scenes.adjoint_scene(width=128, height=96, spp=4)
+    r = scenes.Renderer(s)
+    try:
+        alb, rough, env = scene_parameters(s)
+        img = render(alb, rough, env, 128, 96, 4).cpu().numpy()
+        r.render(4)
+        ref = r.framebuffer()[..., :3]
+        rel = np.abs(img - ref) / np.maximum(np.abs(ref), 1e-2)
+        assert img.mean() > 0.01
+        assert np.median(rel) < 1e-5, float(np.median(rel))
+        assert (rel > 1e-3).mean() < 0.01, float((rel > 1e-3).mean())
+    finally:
+        r.close()
+
+
+def test_gradients_match_fp64_oracle():
+    s = scenes.adjoint_scene(width=64, height=64, spp=4)
+    r = scenes.Renderer(s)
+    try:
+        alb, rough, env = scene_parameters(s)
+        gi_np = np.random.default_rng(3).normal(size=(64 * 64, 3)).astype(np.float32)
+        gi = torch.from_numpy(gi_np).cuda()
+        img = render(alb, rough, env, 64, 64, 4).cpu().numpy().reshape(-1, 3)
+        ga, gr, ge = _grads(s, alb, rough, env, gi, 4)
+        o = Oracle(r.built.payload, r.spec, r.hosek)
+        oimg, oa, orough, oenv = o.adjoint(r.camera, 1, 4, 4, alb.cpu().numpy(), rough.cpu().numpy(),
+                                           env.cpu().numpy(), gi_np, threads=THREADS)
+        o.close()
+        # image: FP32 against FP64 (a few paths may take other branches)
+        rel = np.abs(img - oimg) / np.maximum(np.abs(oimg), 1e-2)
+        assert np.median(rel) < 1e-4, float(np.median(rel))
+        ga, gr, ge = ga.cpu().numpy(), gr.cpu().numpy(), ge.cpu().numpy()
+        err = lambda a, b: float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
+        print("relative L2 error: albedo", err(ga, oa), "roughness", err(gr, orough), "env", err(ge, oenv))
+        assert np.count_nonzero(oa) > 100 and np.count_nonzero(orough) > 16 and np.count_nonzero(oenv) > 1000
+        assert err(ga, oa) < 2e-3
+        assert err(gr, orough) < 5e-3
+        assert err(ge, oenv) < 2e-2
+    finally:
+        r.close()
+
+
+def test_gradients_match_central_differences(full):
+    """256 parameters: 96 albedo channels and 32 roughnesses drawn among the
+    materials, 128 env texel channels drawn among the texels the estimator
+    reaches (non-zero gradient).  The loss difference is formed as
+    sum((a - b) * (a + b - 2 t)) in FP64, so only the FP32 rounding of the
+    rendered pixels limits the differences; the tolerance adds that noise."""
+    s, r = full
+    W, H, spp = s.camera["w"], s.camera["h"], s.render["spp"]
+    alb, rough, env = scene_parameters(s)
+    rng = np.random.default_rng(11)
+    # seeded target: perturbed parameters, other sample seeds
+    ta = (alb * torch.from_numpy(rng.uniform(0.8, 1.2, alb.shape).astype(np.float32)).cuda()).contiguous()
+    tr = (rough + torch.from_numpy(rng.uniform(-0.05, 0.05, rough.shape).astype(np.float32)).cuda()).contiguous()
+    te = (env * 1.1).contiguous()
+    target = render(ta, tr, te, W, H, spp, first_frame=1000).double()
+    img0 = render(alb, rough, env, W, H, spp)
+    gi = (2.0 * (img0.double() - target)).float().contiguous()
+    ga, gr, ge = _grads(s, alb, rough, env, gi, spp)
+
+    mi = rng.choice(alb.shape[0], 32, replace=False)
+    metal = [i for i in range(alb.shape[0]) if s.materials[i]["type"] == _capi.NOOR_METAL]
+    picks = [("alb", (int(i), int(c))) for i, c in zip(rng.choice(alb.shape[0], 96), rng.integers(0, 3, 96))]
+    picks += [("rough", (int(i),)) for i in rng.choice(metal, 32, replace=False)]
+    nz = torch.nonzero(ge != 0).cpu().numpy()
+    for k in rng.choice(len(nz), 128, replace=False):
+        picks.append(("env", tuple(int(x) for x in nz[k])))
+    assert len(picks) == 256
+
+    def perturbed(kind, idx, sign):
+        a, ro, e = alb.clone(), rough.clone(), env.clone()
+        t = {"alb": a, "rough": ro, "env": e}[kind]
+        t[idx] += sign * EPS
+        return a, ro, e, float(t[idx])
+
+    bad = []
+    checked = 0
+    for kind, idx in picks:
+        a1, r1, e1, v1 = perturbed(kind, idx, 1)
+        a2, r2, e2, v2 = perturbed(kind, idx, -1)
+        ip = render(a1, r1, e1, W, H, spp).double()
+        im = render(a2, r2, e2, W, H, spp).double()
+        diff = ip - im
+        dl = float((diff * (ip + im - 2 * target)).sum())
+        fd = dl / (v1 - v2)
+        touched = diff != 0
+        noise = float(torch.sqrt(((2 * (ip - target)) ** 2 * (2e-6 * ip.abs()) ** 2)[touched].sum())) / (v1 - v2)
+        ad = float({"alb": ga, "rough": gr, "env": ge}[kind][idx])
+        if abs(ad) > 10 * noise:
+            checked += 1
+        if abs(fd - ad) > 2e-2 * abs(ad) + 4 * noise + 1e-9:
+            bad.append((kind, idx, ad, fd, noise))
+    print("checked above noise:", checked, "failures:", bad[:10])
+    assert checked >= 200
+    assert len(bad) <= 2, bad
+
+
+def test_autograd_function_returns_entry_point_gradients():
+    s = scenes.adjoint_scene(width=64, height=48, spp=2)
+    r = scenes.Renderer(s)
+    try:
+        alb, rough, env = scene_parameters(s)
+        p = [t.clone().requires_grad_(True) for t in (alb, rough, env)]
+        target = torch.full((48, 64, 3), 0.3, device="cuda")
+        img = render(*p, 64, 48, 2)
+        loss = ((img - target) ** 2).sum()
+        loss.backward()
+        gi = (2 * (img.detach() - target)).contiguous()
+        ga, gr, ge = _grads(s, alb, rough, env, gi, 2)
+        for got, want in zip((p[0].grad, p[1].grad, p[2].grad), (ga, gr, ge)):
+            assert torch.allclose(got, want, rtol=1e-4, atol=1e-6 * float(want.abs().max()))
+        assert float(p[0].grad.abs().sum()) > 0 and float(p[2].grad.abs().sum()) > 0
+    finally:
+        r.close()
+
+
+def test_adjoint_rejects_bad_configurations(full):
+    s, r = full
+    alb, rough, env = scene_parameters(s)
+    with pytest.raises(_capi.NoorError):
+        render(alb, rough, env, 64, 64, 1)        # image size differs from the camera's
+    r.update_spec(rr=1)
+    try:
+        with pytest.raises(_capi.NoorError, match="Russian roulette"):
+            render(alb, rough, env, s.camera["w"], s.camera["h"], 1)
+    finally:
+        r.update_spec(rr=s.render["bounces"])
+    with pytest.raises(ValueError):
+        render(alb[:3], rough, env, s.camera["w"], s.camera["h"], 1)
