@@ -86,15 +86,18 @@ struct WfDev {
 NB_D uint32_t fbits(float f) { return __float_as_uint(f); }
 NB_D float bitsf(uint32_t u) { return __uint_as_float(u); }
 
-// warp-aggregated push: returns this lane's index into the queue
+// warp-aggregated push: returns this lane's index into the queue.  Lanes of
+// one warp may push onto different queues (one per material kind), so the
+// lanes are grouped by counter and each group reserves its own range.
 NB_D uint32_t queue_push(uint32_t* counter) {
-    const uint32_t mask = __activemask();
+    const uint32_t active = __activemask();
+    const uint32_t peers = __match_any_sync(active, reinterpret_cast<unsigned long long>(counter));
     const int lane = threadIdx.x & 31;
-    const int leader = __ffs(mask) - 1;
+    const int leader = __ffs(peers) - 1;
     uint32_t base = 0;
-    if (lane == leader) base = atomicAdd(counter, (uint32_t)__popc(mask));
-    base = __shfl_sync(mask, base, leader);
-    return base + __popc(mask & ((1u << lane) - 1u));
+    if (lane == leader) base = atomicAdd(counter, (uint32_t)__popc(peers));
+    base = __shfl_sync(active, base, leader);
+    return base + __popc(peers & ((1u << lane) - 1u));
 }
 
 NB_D void count_add(unsigned long long* ctr, uint32_t v) {

@@ -67,24 +67,32 @@ def test_gradients_match_fp64_oracle():
     r = scenes.Renderer(s)
     try:
         alb, rough, env = scene_parameters(s)
-        gi_np = np.random.default_rng(3).normal(size=(64 * 64, 3)).astype(np.float32)
-        gi = torch.from_numpy(gi_np).cuda()
+        a_np, r_np, e_np = alb.cpu().numpy(), rough.cpu().numpy(), env.cpu().numpy()
         img = render(alb, rough, env, 64, 64, 4).cpu().numpy().reshape(-1, 3)
-        ga, gr, ge = _grads(s, alb, rough, env, gi, 4)
         o = Oracle(r.built.payload, r.spec, r.hosek)
-        oimg, oa, orough, oenv = o.adjoint(r.camera, 1, 4, 4, alb.cpu().numpy(), rough.cpu().numpy(),
-                                           env.cpu().numpy(), gi_np, threads=THREADS)
-        o.close()
-        # image: FP32 against FP64 (a few paths may take other branches)
+        oimg = o.adjoint(r.camera, 1, 4, 4, a_np, r_np, e_np, threads=THREADS)
+        # image: FP32 against FP64; a few paths take other branches (grazing
+        # hits, directions on a sampler's branch point)
         rel = np.abs(img - oimg) / np.maximum(np.abs(oimg), 1e-2)
         assert np.median(rel) < 1e-4, float(np.median(rel))
+        diverged = rel.max(1) > 1e-4
+        assert diverged.mean() < 0.05, float(diverged.mean())
+        # the gradient is linear in dLoss/dimage: leave out the pixels whose
+        # paths diverged, in both computations
+        gi_np = np.random.default_rng(3).normal(size=(64 * 64, 3)).astype(np.float32)
+        gi_np[diverged] = 0.0
+        gi = torch.from_numpy(gi_np).cuda()
+        ga, gr, ge = _grads(s, alb, rough, env, gi, 4)
+        _, oa, orough, oenv = o.adjoint(r.camera, 1, 4, 4, a_np, r_np, e_np, gi_np, threads=THREADS)
+        o.close()
         ga, gr, ge = ga.cpu().numpy(), gr.cpu().numpy(), ge.cpu().numpy()
         err = lambda a, b: float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
-        print("relative L2 error: albedo", err(ga, oa), "roughness", err(gr, orough), "env", err(ge, oenv))
+        print("diverged pixels", float(diverged.mean()), "relative L2 error: albedo", err(ga, oa),
+              "roughness", err(gr, orough), "env", err(ge, oenv))
         assert np.count_nonzero(oa) > 100 and np.count_nonzero(orough) > 16 and np.count_nonzero(oenv) > 1000
-        assert err(ga, oa) < 2e-3
-        assert err(gr, orough) < 5e-3
-        assert err(ge, oenv) < 2e-2
+        assert err(ga, oa) < 1e-3
+        assert err(gr, orough) < 1e-3
+        assert err(ge, oenv) < 1e-3
     finally:
         r.close()
 
