@@ -45,6 +45,11 @@ def parse():
     ap.add_argument("--scale", type=float, default=1.0, help="image size scale (1 = 1920x1080)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="wavefront: fixed launch parameters")
+    ap.add_argument("--wf-block", type=int, default=128)
+    ap.add_argument("--wf-slots", type=int, default=1 << 21)
+    ap.add_argument("--wf-sort", type=int, default=0)
+    ap.add_argument("--wf-graph", type=int, default=1, help="wavefront: 1 CUDA-graph while loop, 0 host loop")
     return ap.parse_args()
 
 
@@ -222,6 +227,99 @@ def reference_hosek(h):
     return out
 
 
+class MegakernelPath:
+    """reference-facing path: noor_render_frames (the megakernel) into the
+    context film; e2e adds update_cuda_camera and noor_get_framebuffer"""
+
+    def __init__(self, args, s, built):
+        from noor_b200 import scenes
+        self.args = args
+        self.r = scenes.Renderer(s, built=built)
+        self.w, self.h = self.r.w, self.r.h
+        self.host_film = np.zeros((self.h, self.w, 4), np.float32)
+
+    def step(self):
+        self.r.frame = C.c_uint(1)
+        self.r.render(self.args.spp)
+
+    def e2e_step(self):
+        from noor_b200 import _capi
+        _capi.call("update_cuda_camera")
+        self.step()
+        _capi.call("noor_get_framebuffer", self.host_film.ctypes.data_as(C.POINTER(C.c_float)), self.w * self.h)
+
+    def e2e_bytes(self):
+        from noor_b200 import _capi
+        return C.sizeof(_capi.Camera), int(self.host_film.nbytes)
+
+    def counters(self, reset=False):
+        return self.r.counters(reset)
+
+    def warm(self):
+        pass
+
+    def describe(self):
+        return {"entry_point": "noor_render_frames"}
+
+    def close(self):
+        self.r.close()
+
+
+class WavefrontPath:
+    """persistent wavefront integrator through noor_wavefront_render (CUDA
+    graph while loop, parameters from noor_wavefront_autotune during warm-up);
+    e2e adds the frame description from host memory and the film copied back
+    to pinned host memory"""
+
+    def __init__(self, args, s, built):
+        import torch
+        from noor_b200 import scenes, _capi
+        self.args = args
+        self.r = scenes.Renderer(s, built=built)
+        self.w, self.h = self.r.w, self.r.h
+        self.film = torch.zeros((self.h, self.w, 4), dtype=torch.float32, device="cuda")
+        self.host_film = torch.zeros((self.h, self.w, 4), dtype=torch.float32).pin_memory()
+        self.frames = (_capi.WfFrame * 1)(scenes.wf_frame(0, s.camera, args.spp, 8, d_film=self.film.data_ptr()))
+        self.params = scenes.wf_params(args.wf_block, args.wf_slots, args.wf_sort, args.wf_graph)
+        self.tuned_ms = None
+
+    def warm(self):
+        from noor_b200 import _capi
+        if self.args.no_autotune:
+            return
+        best = _capi.WfParams(0, 0, 0, self.args.wf_graph)
+        ms = C.c_float()
+        _capi.call("noor_wavefront_autotune", self.frames, 1, C.byref(best), C.byref(ms))
+        self.params, self.tuned_ms = best, ms.value
+
+    def step(self):
+        from noor_b200 import _capi
+        _capi.call("noor_wavefront_render", self.frames, 1, C.byref(self.params))
+
+    def e2e_step(self):
+        self.step()
+        self.host_film.copy_(self.film)
+
+    def e2e_bytes(self):
+        from noor_b200 import _capi
+        return C.sizeof(_capi.WfFrame), int(self.host_film.numel() * 4)
+
+    def counters(self, reset=False):
+        from noor_b200 import _capi
+        c = (C.c_uint64 * 3)()
+        _capi.call("noor_wavefront_counters", c, int(reset))
+        return tuple(int(x) for x in c)
+
+    def describe(self):
+        p = self.params
+        return {"entry_point": "noor_wavefront_render",
+                "wavefront": {"block": p.block_size, "slots": p.queue_capacity, "material_sort": p.sort_granularity,
+                              "graph": p.use_graph, "autotune_best_ms": self.tuned_ms}}
+
+    def close(self):
+        self.r.close()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -236,16 +334,14 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     from noor_b200 import scenes, _capi
     s, built, build_s = build_scene(args)
-    r = scenes.Renderer(s, built=built)
+    path = (WavefrontPath if args.integrator == "wavefront" else MegakernelPath)(args, s, built)
+    r = path.r
 
-    def render_step():
-        r.frame = C.c_uint(1)
-        r.render(args.spp)
-
-    # warm-up
+    # warm-up (the wavefront path autotunes its launch parameters here)
+    path.warm()
     for _ in range(max(3, args.warmup)):
-        render_step()
-    r.counters(reset=True)
+        path.step()
+    path.counters(reset=True)
     l0 = C.c_uint64()
     _capi.call("noor_launch_count", C.byref(l0))
     if world > 1:
@@ -253,33 +349,29 @@ def main():
     with Clocks(local) as clk:
         _capi.call("noor_event_record", 0)
         for _ in range(args.steps):
-            render_step()
+            path.step()
         _capi.call("noor_event_record", 1)
         ms = C.c_float()
         _capi.call("noor_event_elapsed", 0, 1, C.byref(ms))
     l1 = C.c_uint64()
     _capi.call("noor_launch_count", C.byref(l1))
-    ext, shadow, paths = r.counters()
+    ext, shadow, paths = path.counters()
     ms_step = ms.value / args.steps
     if world > 1:
         t = torch.tensor([ms_step], device="cuda")
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         ms_step = float(t.item())
-    npaths = r.w * r.h * args.spp
+    npaths = path.w * path.h * args.spp
     value = world * npaths / (ms_step / 1000) / 1e6
     mrays = world * (ext + shadow) / args.steps / (ms_step / 1000) / 1e6
 
-    # end to end through the C-ABI: camera from host memory, film to host memory
-    host_film = np.zeros((r.h, r.w, 4), np.float32)
+    # end to end through the public C-ABI with host buffers
     e2e_t = []
     for i in range(args.warmup + args.steps):
         if world > 1:
             torch.distributed.barrier()
         t = time.perf_counter()
-        _capi.call("update_cuda_camera")
-        r.frame = C.c_uint(1)
-        r.render(args.spp)
-        _capi.call("noor_get_framebuffer", host_film.ctypes.data_as(C.POINTER(C.c_float)), r.w * r.h)
+        path.e2e_step()
         if i >= args.warmup:
             e2e_t.append(time.perf_counter() - t)
     e2e_ms = statistics.mean(e2e_t) * 1000
@@ -287,10 +379,10 @@ def main():
         t = torch.tensor([e2e_ms], device="cuda")
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         e2e_ms = float(t.item())
-    e2e = {"value": world * npaths / (e2e_ms / 1000) / 1e6, "unit": METRIC,
-           "h2d_bytes_per_step": C.sizeof(_capi.Camera), "d2h_bytes_per_step": int(host_film.nbytes)}
+    h2d, d2h = path.e2e_bytes()
+    e2e = {"value": world * npaths / (e2e_ms / 1000) / 1e6, "unit": METRIC, "h2d_bytes_per_step": h2d,
+           "d2h_bytes_per_step": d2h}
 
-    line = None
     if rank == 0:
         peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
         hbm = peaks.get("hbm_gbs", 6650.0)
@@ -304,7 +396,7 @@ def main():
             orc.close()
             achieved = per_path * npaths / (ms_step / 1000) / 1e9
             roof.update(achieved=achieved, frac=achieved / hbm, algorithmic_bytes_per_path=per_path, **counts)
-            prof = ROOT / "profiles" / "megakernel_sky_traffic.json"
+            prof = ROOT / "profiles" / f"{args.integrator}_sky_traffic.json"
             if prof.exists():
                 tr = json.loads(prof.read_text())
                 roof["traffic"] = tr.get("dram_bytes_per_path", 0) * npaths
@@ -312,16 +404,16 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator, random-init sky)",
-                "config": {"workload": WORKLOAD, "integrator": args.integrator, "width": r.w, "height": r.h,
+                "config": {"workload": WORKLOAD, "integrator": args.integrator, "width": path.w, "height": path.h,
                            "spp": args.spp, "bounces": 8, "triangles": s.num_triangles,
                            "intersector": "watertight", "film": "kahan",
                            "l2": "inputs larger than L2 (scene ~0.5 GB resident)",
-                           "parallelism": f"replicas{world}", "bvh_build_s": round(build_s, 2)},
+                           "parallelism": f"replicas{world}", "bvh_build_s": round(build_s, 2), **path.describe()},
                 "mrays_per_s": mrays, "rays_per_step": (ext + shadow) / args.steps,
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": int(l1.value - l0.value), "clocks": clk.summary()}
         print(json.dumps(line), flush=True)
-    r.close()
+    path.close()
     if world > 1:
         torch.distributed.destroy_process_group()
 

@@ -223,7 +223,7 @@ def lib() -> C.CDLL:
     global _lib
     if _lib is None:
         if not LIB_PATH.exists():
-            raise ImportError(f"{LIB_PATH} is missing: run `python -m noor_b200.build` (nvcc, sm_100a)")
+            raise ImportError(f"{LIB_PATH} is missing: run `python noor_b200/build.py` (nvcc, sm_100a)")
         L = C.CDLL(str(LIB_PATH), mode=os.RTLD_NOW | C.RTLD_GLOBAL)
         for name, (res, args) in PROTOTYPES.items():
             fn = getattr(L, name)

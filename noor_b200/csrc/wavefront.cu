@@ -454,6 +454,7 @@ static int wf_ensure(Context& C, uint32_t cap) {
         (rc = wf_alloc(S, (void**)&W.rays, 32)))
         return rc;
     cudaError_t e = cudaMalloc((void**)&S.active_host_dev, 16);
+    if (e == cudaSuccess) e = cudaMemset(W.rays, 0, 32);
     if (e != cudaSuccess) return cuda_fail(e, "wavefront buffers");
     S.cap = cap;
     return NOOR_OK;
@@ -699,7 +700,7 @@ extern "C" int noor_wavefront_autotune(const noor_wf_frame* frames, uint32_t n_f
     if (rc) return rc;
     if (!best) return set_error(NOOR_ERR_INVALID, "autotune: best is null");
     const uint32_t blocks[] = {64, 128, 256};
-    const uint32_t caps[] = {1u << 19, 1u << 20, 1u << 21};
+    const uint32_t caps[] = {1u << 20, 1u << 21, 1u << 22};
     const uint32_t sorts[] = {0, 1};
     float bms = 3.4e38f;
     noor_wf_params bp{128, 1u << 20, 1, best->use_graph};

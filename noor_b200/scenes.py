@@ -313,6 +313,63 @@ def env_scene(seed: int = 3, width: int = 1920, height: int = 1080, spp: int = 1
                      render=dict(spp=spp, bounces=bounces, rr=rr, mis=1), name="env")
 
 
+def batched_workload(seed: int = 4, n_frames: int = 64, sides=(128, 256, 512, 1024), tri_range=(1e4, 2.6e6),
+                     spp_range=(4, 64), bounces: int = 6):
+    """C4: `n_frames` independent frames.  Per frame: square side uniform in
+    `sides`; a triangle budget T log-uniform in `tri_range`, realised as
+    ceil(T / 81,920) subdivision-6 icospheres of one seeded field (the first
+    N spheres of it), or one icosphere at subdivision floor(log4(T / 20))
+    when T < 81,920; spp uniform in spp_range (inclusive); sky or env-map
+    lighting by a coin flip.  Frames whose geometry and lighting coincide
+    share one scene.  Returns (scenes: dict key -> SceneData, frames: list of
+    dict(key, camera, spp, bounces))."""
+    rng = np.random.default_rng(seed)
+    field, (c_all, r_all) = sphere_field(seed, 32, 6)
+    nf6 = 20 * 4 ** 6
+    scenes_: dict = {}
+    frames = []
+    env = None
+    for _ in range(n_frames):
+        side = int(rng.choice(sides))
+        T = float(np.exp(rng.uniform(np.log(tri_range[0]), np.log(tri_range[1]))))
+        spp = int(rng.integers(spp_range[0], spp_range[1] + 1))
+        light = "sky" if rng.random() < 0.5 else "env"
+        if T >= nf6:
+            geo = ("field", int(min(32, np.ceil(T / nf6))))
+        else:
+            geo = ("single", int(max(0, np.floor(np.log(T / 20.0) / np.log(4.0)))))
+        key = (geo, light)
+        if key not in scenes_:
+            if geo[0] == "field":
+                n = geo[1]
+                nv = field["vertices"].shape[0] // 32
+                g = dict(vertices=field["vertices"][: n * nv], normals=field["normals"][: n * nv],
+                         uvs=field["uvs"], vindices=field["vindices"][: n * nf6],
+                         nindices=field["nindices"][: n * nf6], uvindices=field["uvindices"][: n * nf6],
+                         material_indices=field["material_indices"][: n * nf6], meshes=field["meshes"][:n],
+                         materials=field["materials"][:n])
+                cam = frame_spheres(c_all[:n], r_all[:n], seed, aspect=1.0, clearance=0.5)
+            else:
+                g, (c1, r1) = sphere_field(seed + 100 + geo[1], 1, geo[1], rmin=1.0, rmax=1.0)
+                ctr = c1[0]
+                cam = dict(eye=tuple(float(x) for x in ctr + np.array([0.0, 1.0, 3.0])),
+                           look_at=tuple(float(x) for x in ctr), up=(0.0, 1.0, 0.0), fov_deg=50.0)
+            if light == "sky":
+                sd = SceneData(**g, skydome_type=capi.NOOR_SKY_PHYSICAL, camera=cam,
+                               render=dict(spp=spp, bounces=bounces, rr=1, mis=0),
+                               hosek=dict(turbidity=3.0, albedo=0.3, sun_lat=float(np.radians(60.0)),
+                                          sun_lon=float(np.pi / 4), solar_scale=250.0, solar_radius_scale=2.0),
+                               name=f"{geo[0]}{geo[1]}-sky")
+            else:
+                if env is None:
+                    env = env_map(seed, 2048, 1024)
+                sd = SceneData(**g, skydome_type=capi.NOOR_SKY_HDR, env=env, camera=cam,
+                               render=dict(spp=spp, bounces=bounces, rr=1, mis=1), name=f"{geo[0]}{geo[1]}-env")
+            scenes_[key] = sd
+        frames.append(dict(key=key, camera=dict(scenes_[key].camera, w=side, h=side), spp=spp, bounces=bounces))
+    return scenes_, frames
+
+
 def adjoint_scene(seed: int = 5, width: int = 512, height: int = 512, spp: int = 16, bounces: int = 4,
                   count: int = 10, level: int = 5, n_materials: int = 64, env_w: int = 512,
                   env_h: int = 256) -> SceneData:

@@ -179,8 +179,8 @@ def test_env_distribution_fp64(which, sky):
         assert clean.sum() >= live.sum() - max(4, live.sum() // 100), (clean.sum(), live.sum())
         assert np.abs(cdf.reshape(H, W + 1)[clean] - ref["cdf"][clean]).max() < 1e-5
         # the sky's marginal carries the sun-edge cells' FP32/FP64 differences
-    # (excluded from the per-row comparison above) into every later row
-    assert np.quantile(np.abs(mcdf - ref["marg_cdf"]), 0.999) < (1e-4 if which == "env" else 2e-3)
+        # (excluded from the per-row comparison above) into every later row
+        assert np.quantile(np.abs(mcdf - ref["marg_cdf"]), 0.999) < (1e-4 if which == "env" else 2e-3)
         assert mi.value == pytest.approx(ref["marg_int"], rel=1e-3)
         # sampling: GPU (x, y, pdf) against FP64
         u = np.random.default_rng(1).random((50_000, 2)).astype(np.float32)
