@@ -514,6 +514,19 @@ int noor_wavefront_counters(uint64_t counters[3], int reset);
  * the whole sequence in *ms. */
 int noor_megakernel_batch(const noor_wf_frame* frames, uint32_t n_frames,
                           float* ms);
+/* No counterpart in the reference.  One frame with the plain megakernel into
+ * the caller's film (frame->d_film, required: float4 per pixel, the mean over
+ * frame->spp samples), allocating no device memory: for callers that cannot
+ * call cudaMalloc while they render (memory they do not own, hosts that forbid
+ * device allocation after start-up).  Scratch comes from one fixed device
+ * array of NOOR_NOALLOC_SCRATCH_BYTES, which bounds a frame to
+ * NOOR_NOALLOC_SCRATCH_BYTES / 16 pixels (larger frames return
+ * NOOR_ERR_CAPACITY).  The first call on a device looks up the array's
+ * address (cudaGetSymbolAddress); make it before any stream capture.  All
+ * calls on a device share the array, so calls that overlap on the GPU race;
+ * nothing in it needs clearing between calls. */
+#define NOOR_NOALLOC_SCRATCH_BYTES (32u << 20)
+int noor_megakernel_frame_noalloc(const noor_wf_frame* frame);
 /* Project-written autotuner: times candidate parameter sets on the given
  * batch and returns the fastest. */
 int noor_wavefront_autotune(const noor_wf_frame* frames, uint32_t n_frames,
