@@ -40,7 +40,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--integrator", default="megakernel", choices=["megakernel", "wavefront"])
+    ap.add_argument("--integrator", default="wavefront", choices=["megakernel", "wavefront"])
+    ap.add_argument("--no-compare", action="store_true",
+                    help="skip timing the other integrator on the same scene and samples")
     ap.add_argument("--spp", type=int, default=64)
     ap.add_argument("--scale", type=float, default=1.0, help="image size scale (1 = 1920x1080)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
@@ -145,17 +147,29 @@ def algorithmic_bytes(orc, cam, spp, isect, sample_pixels=20000, seed=0):
                           tris_per_path=tris, sample_paths=paths)
 
 
+def calibrate_pixels(orc, cam, spp, threads, target_s):
+    """pixels of a centre block the oracle renders in about target_s seconds
+    (growing blocks until one takes >= 1 s, then scaled)"""
+    n = cam.w * cam.h
+    npx = 1024
+    while True:
+        p0 = max(0, n // 2 - npx // 2)
+        t = time.time()
+        orc.render(cam, 1, spp, p0=p0, p1=min(n, p0 + npx), threads=threads)
+        dt = time.time() - t
+        if dt >= 1.0 or npx >= n:
+            break
+        npx = min(n, npx * 4)
+    return int(max(1024, min(n, npx / max(dt, 1e-3) * target_s)))
+
+
 def cpu_baseline(args, s, built, spec, hosek, cam, budget_s):
     """oracle FP32 on all host threads over a pixel subsample of the workload"""
     from oracle.oracle import Oracle
     threads = os.cpu_count() or 1
     orc = Oracle(built.payload, spec, hosek)
     n = cam.w * cam.h
-    # probe rate on a small block, then size the sample to the budget
-    t = time.time()
-    orc.render(cam, 1, 2, p0=n // 2, p1=n // 2 + 256, threads=threads)
-    rate = 512 / max(time.time() - t, 1e-3)
-    npx = int(max(256, min(n, rate * budget_s / args.spp)))
+    npx = calibrate_pixels(orc, cam, args.spp, threads, budget_s)
     p0 = max(0, n // 2 - npx // 2)
     t = time.time()
     orc.render(cam, 1, args.spp, p0=p0, p1=p0 + npx, threads=threads)
@@ -179,10 +193,10 @@ def run_reference(args):
     orc = Oracle(built.payload, spec, hosek)
     threads = os.cpu_count() or 1
     n = cam.w * cam.h
-    npx = 4096
+    npx = calibrate_pixels(orc, cam, args.spp, threads, 3.0)   # ~3 s of CPU work per step
     times = []
     for i in range(args.warmup + args.steps):
-        p0 = (n // 2 + i * npx) % (n - npx)
+        p0 = (n // 2 + i * npx) % max(1, n - npx)
         t = time.time()
         orc.render(cam, 1, args.spp, p0=p0, p1=p0 + npx, threads=threads)
         if i >= args.warmup:
@@ -231,10 +245,11 @@ class MegakernelPath:
     """reference-facing path: noor_render_frames (the megakernel) into the
     context film; e2e adds update_cuda_camera and noor_get_framebuffer"""
 
-    def __init__(self, args, s, built):
-        from noor_b200 import scenes
+    name = "megakernel"
+
+    def __init__(self, args, s, r):
         self.args = args
-        self.r = scenes.Renderer(s, built=built)
+        self.r = r
         self.w, self.h = self.r.w, self.r.h
         self.host_film = np.zeros((self.h, self.w, 4), np.float32)
 
@@ -261,8 +276,8 @@ class MegakernelPath:
     def describe(self):
         return {"entry_point": "noor_render_frames"}
 
-    def close(self):
-        self.r.close()
+    def image(self):
+        return self.r.framebuffer()[..., :3]
 
 
 class WavefrontPath:
@@ -271,11 +286,13 @@ class WavefrontPath:
     e2e adds the frame description from host memory and the film copied back
     to pinned host memory"""
 
-    def __init__(self, args, s, built):
+    name = "wavefront"
+
+    def __init__(self, args, s, r):
         import torch
         from noor_b200 import scenes, _capi
         self.args = args
-        self.r = scenes.Renderer(s, built=built)
+        self.r = r
         self.w, self.h = self.r.w, self.r.h
         self.film = torch.zeros((self.h, self.w, 4), dtype=torch.float32, device="cuda")
         self.host_film = torch.zeros((self.h, self.w, 4), dtype=torch.float32).pin_memory()
@@ -316,8 +333,10 @@ class WavefrontPath:
                 "wavefront": {"block": p.block_size, "slots": p.queue_capacity, "material_sort": p.sort_granularity,
                               "graph": p.use_graph, "autotune_best_ms": self.tuned_ms}}
 
-    def close(self):
-        self.r.close()
+    def image(self):
+        import torch
+        torch.cuda.synchronize()
+        return self.film.cpu().numpy()[..., :3]
 
 
 def main():
@@ -334,36 +353,55 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     from noor_b200 import scenes, _capi
     s, built, build_s = build_scene(args)
-    path = (WavefrontPath if args.integrator == "wavefront" else MegakernelPath)(args, s, built)
-    r = path.r
+    r = scenes.Renderer(s, built=built)
+    paths_ = {"megakernel": MegakernelPath(args, s, r), "wavefront": WavefrontPath(args, s, r)}
+    path = paths_[args.integrator]
+    other = None if args.no_compare else paths_["megakernel" if args.integrator == "wavefront" else "wavefront"]
 
-    # warm-up (the wavefront path autotunes its launch parameters here)
-    path.warm()
-    for _ in range(max(3, args.warmup)):
-        path.step()
-    path.counters(reset=True)
-    l0 = C.c_uint64()
-    _capi.call("noor_launch_count", C.byref(l0))
-    if world > 1:
-        torch.distributed.barrier()
-    with Clocks(local) as clk:
-        _capi.call("noor_event_record", 0)
-        for _ in range(args.steps):
-            path.step()
-        _capi.call("noor_event_record", 1)
-        ms = C.c_float()
-        _capi.call("noor_event_elapsed", 0, 1, C.byref(ms))
-    l1 = C.c_uint64()
-    _capi.call("noor_launch_count", C.byref(l1))
-    ext, shadow, paths = path.counters()
-    ms_step = ms.value / args.steps
-    if world > 1:
-        t = torch.tensor([ms_step], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms_step = float(t.item())
+    def timed(p, clocks_index=None):
+        """warm-up, then K device-timed steps: (ms per step, launches, ext, shadow, clocks)"""
+        p.warm()   # the wavefront path autotunes its launch parameters here
+        for _ in range(max(3, args.warmup)):
+            p.step()
+        p.counters(reset=True)
+        l0 = C.c_uint64()
+        _capi.call("noor_launch_count", C.byref(l0))
+        if world > 1:
+            torch.distributed.barrier()
+        with Clocks(local if clocks_index is None else clocks_index) as clk:
+            _capi.call("noor_event_record", 0)
+            for _ in range(args.steps):
+                p.step()
+            _capi.call("noor_event_record", 1)
+            ms = C.c_float()
+            _capi.call("noor_event_elapsed", 0, 1, C.byref(ms))
+        l1 = C.c_uint64()
+        _capi.call("noor_launch_count", C.byref(l1))
+        ext, shadow, _ = p.counters()
+        ms_step = ms.value / args.steps
+        if world > 1:
+            t = torch.tensor([ms_step], device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            ms_step = float(t.item())
+        return ms_step, int(l1.value - l0.value), ext, shadow, clk.summary()
+
+    ms_step, launches, ext, shadow, clocks = timed(path)
     npaths = path.w * path.h * args.spp
     value = world * npaths / (ms_step / 1000) / 1e6
     mrays = world * (ext + shadow) / args.steps / (ms_step / 1000) / 1e6
+    compare = None
+    if other is not None:
+        img = path.image()
+        oms, olaunch, oext, oshadow, oclk = timed(other)
+        oimg = other.image()
+        rel = np.abs(img - oimg) / np.maximum(np.abs(oimg), 1e-2)
+        compare = {"integrator": other.name, "value": world * npaths / (oms / 1000) / 1e6, "ms_per_step": oms,
+                   "mrays_per_s": world * (oext + oshadow) / args.steps / (oms / 1000) / 1e6,
+                   "gpu_launches": olaunch, "clocks": oclk,
+                   "speedup_of_headline": oms / ms_step,
+                   "same_samples_image_check": {"median_rel_diff": float(np.median(rel)),
+                                                "frac_pixels_rel_diff_gt_1e-3": float((rel > 1e-3).mean()),
+                                                "mean_ratio": float(img.mean() / max(oimg.mean(), 1e-30))}}
 
     # end to end through the public C-ABI with host buffers
     e2e_t = []
@@ -411,9 +449,9 @@ def main():
                            "parallelism": f"replicas{world}", "bvh_build_s": round(build_s, 2), **path.describe()},
                 "mrays_per_s": mrays, "rays_per_step": (ext + shadow) / args.steps,
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
-                "gpu_launches": int(l1.value - l0.value), "clocks": clk.summary()}
+                "gpu_launches": launches, "clocks": clocks, "other_integrator": compare}
         print(json.dumps(line), flush=True)
-    path.close()
+    r.close()
     if world > 1:
         torch.distributed.destroy_process_group()
 

@@ -317,6 +317,14 @@ int noor_ray_counters(uint64_t counters[3], int reset);
 int noor_device_status(uint32_t* status, int reset);
 /* CUDA stream the current context launches on (cudaStream_t). */
 void* noor_stream(void);
+/* The calling thread's render context (NULL if none), and binding a context
+ * to the calling thread (NULL unbinds).  A context stays owned by the thread
+ * that created it (load_cuda_data) and is freed by device_free_memory on
+ * that thread; another thread may borrow it, never concurrently with its
+ * owner (e.g. a framework that runs a backward pass on a worker thread while
+ * the owner waits). */
+void* noor_context_current(void);
+int noor_context_bind(void* context);
 /* CUDA events on that stream (8 slots) for device-side timing. */
 int noor_event_record(int slot);
 int noor_event_elapsed(int slot_begin, int slot_end, float* ms);

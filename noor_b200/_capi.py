@@ -201,6 +201,8 @@ PROTOTYPES = {
     "noor_wavefront_counters": (C.c_int, [C.POINTER(u64), C.c_int]),
     "noor_megakernel_batch": (C.c_int, [C.POINTER(WfFrame), u32, pf]),
     "noor_megakernel_frame_noalloc": (C.c_int, [C.POINTER(WfFrame)]),
+    "noor_context_current": (C.c_void_p, []),
+    "noor_context_bind": (C.c_int, [C.c_void_p]),
     "noor_adjoint_forward": (C.c_int, [C.POINTER(AdjointDesc), C.c_void_p]),
     "noor_adjoint_backward": (C.c_int, [C.POINTER(AdjointDesc), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
 }

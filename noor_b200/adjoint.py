@@ -68,6 +68,9 @@ class AdjointRender(torch.autograd.Function):
         _capi.call("noor_adjoint_forward", C.byref(d), C.c_void_p(img.data_ptr()))
         ctx.save_for_backward(albedo, roughness, env)
         ctx.cfg = cfg
+        # autograd may run backward on a worker thread: remember the render
+        # context (contexts are per host thread) to borrow it there
+        ctx.noor_context = _capi.lib().noor_context_current()
         return img
 
     @staticmethod
@@ -79,8 +82,13 @@ class AdjointRender(torch.autograd.Function):
         ge = torch.zeros_like(env) if env is not None and env.numel() else None
         torch.cuda.current_stream(albedo.device).synchronize()
         d = _desc(ctx.cfg, albedo, roughness, env)
-        _capi.call("noor_adjoint_backward", C.byref(d), C.c_void_p(g.data_ptr()), C.c_void_p(ga.data_ptr()),
-                   C.c_void_p(gr.data_ptr()), C.c_void_p(ge.data_ptr()) if ge is not None else None)
+        prev = _capi.lib().noor_context_current()
+        _capi.call("noor_context_bind", ctx.noor_context)
+        try:
+            _capi.call("noor_adjoint_backward", C.byref(d), C.c_void_p(g.data_ptr()), C.c_void_p(ga.data_ptr()),
+                       C.c_void_p(gr.data_ptr()), C.c_void_p(ge.data_ptr()) if ge is not None else None)
+        finally:
+            _capi.call("noor_context_bind", prev)
         return ga, gr, ge, None, None, None, None, None
 
 

@@ -711,6 +711,18 @@ extern "C" int noor_device_status(uint32_t* status, int reset) {
 
 extern "C" void* noor_stream(void) { return tl_ctx ? (void*)tl_ctx->stream : nullptr; }
 
+extern "C" void* noor_context_current(void) { return tl_ctx; }
+
+extern "C" int noor_context_bind(void* context) {
+    clear_error();
+    tl_ctx = static_cast<Context*>(context);
+    if (tl_ctx) {
+        cudaError_t e = cudaSetDevice(tl_ctx->device);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+    }
+    return NOOR_OK;
+}
+
 extern "C" int noor_event_record(int slot) {
     Context* C;
     int rc = need_ctx(C);

@@ -75,8 +75,9 @@ def test_gradients_match_fp64_oracle():
         # hits, directions on a sampler's branch point)
         rel = np.abs(img - oimg) / np.maximum(np.abs(oimg), 1e-2)
         assert np.median(rel) < 1e-4, float(np.median(rel))
-        diverged = rel.max(1) > 1e-4
-        assert diverged.mean() < 0.05, float(diverged.mean())
+        # FP32 rounding alone moves a pixel by up to ~1e-4 over four bounces;
+        # a path that took another branch moves it by far more
+        diverged = rel.max(1) > 1e-3
         # the gradient is linear in dLoss/dimage: leave out the pixels whose
         # paths diverged, in both computations
         gi_np = np.random.default_rng(3).normal(size=(64 * 64, 3)).astype(np.float32)
@@ -89,10 +90,11 @@ def test_gradients_match_fp64_oracle():
         err = lambda a, b: float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
         print("diverged pixels", float(diverged.mean()), "relative L2 error: albedo", err(ga, oa),
               "roughness", err(gr, orough), "env", err(ge, oenv))
+        assert diverged.mean() < 0.1, float(diverged.mean())
         assert np.count_nonzero(oa) > 100 and np.count_nonzero(orough) > 16 and np.count_nonzero(oenv) > 1000
-        assert err(ga, oa) < 1e-3
-        assert err(gr, orough) < 1e-3
-        assert err(ge, oenv) < 1e-3
+        assert err(ga, oa) < 3e-3
+        assert err(gr, orough) < 3e-3
+        assert err(ge, oenv) < 3e-3
     finally:
         r.close()
 
@@ -146,7 +148,7 @@ def test_gradients_match_central_differences(full):
         ad = float({"alb": ga, "rough": gr, "env": ge}[kind][idx])
         if abs(ad) > 10 * noise:
             checked += 1
-        if abs(fd - ad) > 2e-2 * abs(ad) + 4 * noise + 1e-9:
+        if abs(fd - ad) > 1e-2 * abs(ad) + 4 * noise + 1e-9:
             bad.append((kind, idx, ad, fd, noise))
     print("checked above noise:", checked, "failures:", bad[:10])
     assert checked >= 200
@@ -172,8 +174,9 @@ def test_autograd_function_returns_entry_point_gradients():
         r.close()
 
 
-def test_adjoint_rejects_bad_configurations(full):
-    s, r = full
+def test_adjoint_rejects_bad_configurations():
+    s = scenes.adjoint_scene(width=64, height=64, spp=1, count=2, level=2)
+    r = scenes.Renderer(s)
     alb, rough, env = scene_parameters(s)
     with pytest.raises(_capi.NoorError):
         render(alb, rough, env, 64, 64, 1)        # image size differs from the camera's
@@ -185,3 +188,4 @@ def test_adjoint_rejects_bad_configurations(full):
         r.update_spec(rr=s.render["bounces"])
     with pytest.raises(ValueError):
         render(alb[:3], rough, env, s.camera["w"], s.camera["h"], 1)
+    r.close()

@@ -181,7 +181,8 @@ def test_env_distribution_fp64(which, sky):
         # the sky's marginal carries the sun-edge cells' FP32/FP64 differences
         # (excluded from the per-row comparison above) into every later row
         assert np.quantile(np.abs(mcdf - ref["marg_cdf"]), 0.999) < (1e-4 if which == "env" else 2e-3)
-        assert mi.value == pytest.approx(ref["marg_int"], rel=1e-3)
+        # (the sky's integral includes the sun-edge cells)
+        assert mi.value == pytest.approx(ref["marg_int"], rel=1e-3 if which == "env" else 3e-3)
         # sampling: GPU (x, y, pdf) against FP64
         u = np.random.default_rng(1).random((50_000, 2)).astype(np.float32)
         d_u = dev(u)
