@@ -52,6 +52,10 @@ def parse():
     ap.add_argument("--wf-slots", type=int, default=1 << 21)
     ap.add_argument("--wf-sort", type=int, default=0)
     ap.add_argument("--wf-graph", type=int, default=1, help="wavefront: 1 CUDA-graph while loop, 0 host loop")
+    ap.add_argument("--workload", default="sky", choices=["sky", "batched", "adjoint"],
+                    help="sky: the headline sky-lit scene; batched: 64 uneven frames in one wavefront launch "
+                         "against 64 sequential megakernel renders; adjoint: forward+backward of the "
+                         "differentiable-rendering configuration")
     return ap.parse_args()
 
 
@@ -339,10 +343,170 @@ class WavefrontPath:
         return self.film.cpu().numpy()[..., :3]
 
 
+def device_timed(fn, steps):
+    """device time of `steps` calls of fn on the library's stream (ms per call)"""
+    from noor_b200 import _capi
+    _capi.call("noor_event_record", 0)
+    for _ in range(steps):
+        fn()
+    _capi.call("noor_event_record", 1)
+    ms = C.c_float()
+    _capi.call("noor_event_elapsed", 0, 1, C.byref(ms))
+    return ms.value / steps
+
+
+def run_batched(args):
+    """C4: 64 frames of uneven resolution, scene size and spp (sky or env map)
+    rendered in one wavefront launch (CUDA-graph device loop, launch
+    parameters from the autotuner), against the same 64 frames rendered one
+    after another by the plain megakernel."""
+    import torch
+    from noor_b200 import scenes, _capi
+    sc, frames = scenes.batched_workload()
+    keys = list(sc.keys())
+    t = time.time()
+    r = scenes.Renderer(sc[keys[0]])
+    ids, keep = {keys[0]: 0}, []
+    for k in keys[1:]:
+        sid, kp = scenes.upload_scene(sc[k])
+        ids[k] = sid
+        keep.append(kp)
+    setup_s = time.time() - t
+    films = [torch.zeros((f["camera"]["h"], f["camera"]["w"], 4), dtype=torch.float32, device="cuda") for f in frames]
+    desc = (_capi.WfFrame * len(frames))(*[scenes.wf_frame(ids[f["key"]], f["camera"], f["spp"], f["bounces"],
+                                                           d_film=t_.data_ptr()) for f, t_ in zip(frames, films)])
+    npaths = sum(f["camera"]["w"] * f["camera"]["h"] * f["spp"] for f in frames)
+    best = _capi.WfParams(0, 0, 0, 1)
+    tms = C.c_float()
+    _capi.call("noor_wavefront_autotune", desc, len(frames), C.byref(best), C.byref(tms))
+    wf = lambda: _capi.call("noor_wavefront_render", desc, len(frames), C.byref(best))
+    mk = lambda: _capi.call("noor_megakernel_batch", desc, len(frames), None)
+    for _ in range(max(3, args.warmup)):
+        wf()
+    l0 = C.c_uint64()
+    _capi.call("noor_launch_count", C.byref(l0))
+    with Clocks(0) as clk:
+        wf_ms = device_timed(wf, args.steps)
+    l1 = C.c_uint64()
+    _capi.call("noor_launch_count", C.byref(l1))
+    img_wf = [f_.cpu().numpy()[..., :3] for f_ in films]
+    for _ in range(2):
+        mk()
+    mk_ms = device_timed(mk, max(1, args.steps // 2))
+    img_mk = [f_.cpu().numpy()[..., :3] for f_ in films]
+    rel = np.concatenate([(np.abs(a - b) / np.maximum(np.abs(b), 1e-2)).ravel() for a, b in zip(img_wf, img_mk)])
+    # end to end: frame descriptions from host memory, films back to pinned host memory
+    host = [torch.zeros(f_.shape, dtype=torch.float32).pin_memory() for f_ in films]
+    e2e_t = []
+    for i in range(args.warmup + args.steps):
+        t = time.perf_counter()
+        wf()
+        for h_, f_ in zip(host, films):
+            h_.copy_(f_)
+        if i >= args.warmup:
+            e2e_t.append(time.perf_counter() - t)
+    e2e_ms = statistics.mean(e2e_t) * 1000
+    line = {"metric": METRIC, "value": npaths / (wf_ms / 1000) / 1e6, "unit": METRIC, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": wf_ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator)",
+            "config": {"workload": "64 uneven frames (sides 128-1024, 5k-2.6M triangles, 4-64 spp, depth 6, "
+                                   "sky or env map) in one wavefront launch",
+                       "frames": len(frames), "scenes": len(keys), "paths_per_step": npaths,
+                       "triangles_uploaded": int(sum(x.num_triangles for x in sc.values())),
+                       "setup_s": round(setup_s, 1),
+                       "wavefront": {"block": best.block_size, "slots": best.queue_capacity,
+                                     "material_sort": best.sort_granularity, "graph": best.use_graph}},
+            "other_integrator": {"integrator": "megakernel, 64 sequential renders (noor_megakernel_batch)",
+                                 "value": npaths / (mk_ms / 1000) / 1e6, "ms_per_step": mk_ms,
+                                 "speedup_of_headline": mk_ms / wf_ms,
+                                 "same_samples_image_check": {"median_rel_diff": float(np.median(rel)),
+                                                              "frac_pixels_rel_diff_gt_1e-3": float((rel > 1e-3).mean())}},
+            "e2e": {"value": npaths / (e2e_ms / 1000) / 1e6, "unit": METRIC,
+                    "h2d_bytes_per_step": C.sizeof(_capi.WfFrame) * len(frames),
+                    "d2h_bytes_per_step": int(sum(f_.numel() * 4 for f_ in films))},
+            "gpu_launches": int(l1.value - l0.value) // max(1, args.steps) * args.steps, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    r.close()
+
+
+def run_adjoint(args):
+    """C5: forward + backward of the path-replay adjoint on the
+    differentiable-rendering configuration (512x512, 16 spp, depth 4,
+    204,800 triangles, 64 materials, 512x256 env map), L2 loss against a
+    seeded target render."""
+    import torch
+    from noor_b200 import scenes, _capi
+    from noor_b200.adjoint import render, scene_parameters
+    s = scenes.adjoint_scene()
+    r = scenes.Renderer(s)
+    W, H, spp = s.camera["w"], s.camera["h"], s.render["spp"]
+    alb, rough, env = scene_parameters(s)
+    rng = np.random.default_rng(11)
+    with torch.no_grad():
+        target = render((alb * torch.from_numpy(rng.uniform(0.8, 1.2, alb.shape).astype(np.float32)).cuda()).contiguous(),
+                        rough, (env * 1.1).contiguous(), W, H, spp, first_frame=1000)
+    params = [t.clone().requires_grad_(True) for t in (alb, rough, env)]
+
+    def step():
+        for p in params:
+            p.grad = None
+        img = render(*params, W, H, spp)
+        loss = ((img - target) ** 2).sum()
+        loss.backward()
+        return loss
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    l0 = C.c_uint64()
+    _capi.call("noor_launch_count", C.byref(l0))
+    fwd, bwd = [], []
+    with Clocks(0) as clk:
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            for p in params:
+                p.grad = None
+            a = time.perf_counter()
+            img = render(*params, W, H, spp)
+            loss = ((img - target) ** 2).sum()
+            torch.cuda.synchronize()
+            b = time.perf_counter()
+            loss.backward()
+            torch.cuda.synchronize()
+            c = time.perf_counter()
+            fwd.append(b - a)
+            bwd.append(c - b)
+        total = (time.perf_counter() - t0) / args.steps
+    l1 = C.c_uint64()
+    _capi.call("noor_launch_count", C.byref(l1))
+    ms = total * 1000
+    npaths = W * H * spp
+    line = {"metric": "ms per forward+backward iteration", "value": ms, "unit": "ms", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator)",
+            "config": {"workload": "differentiable rendering: 10 subdivision-5 icospheres (204,800 tris), 64 "
+                                   "materials, 512x256 env map, 512x512, 16 spp, depth 4, L2 loss",
+                       "params": int(sum(p.numel() for p in params))},
+            "forward_ms": 1000 * statistics.mean(fwd), "backward_ms": 1000 * statistics.mean(bwd),
+            "forward_mpaths_per_s": npaths / statistics.mean(fwd) / 1e6,
+            "backward_mpaths_per_s": npaths / statistics.mean(bwd) / 1e6,
+            "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 4},
+            "gpu_launches": int(l1.value - l0.value), "clocks": clk.summary(),
+            "timing": "host wall clock around synchronised calls (the adjoint entry points synchronise)"}
+    print(json.dumps(line), flush=True)
+    r.close()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.workload == "batched":
+        run_batched(args)
+        return
+    if args.workload == "adjoint":
+        run_adjoint(args)
         return
     rank, world, local = dist_env()
     import torch

@@ -10,7 +10,9 @@ import os
 from pathlib import Path
 
 _HERE = Path(__file__).resolve().parent
-LIB_PATH = _HERE / "libnoor_b200.so"
+# the in-tree build; NOOR_B200_LIB names another build of the same sources
+# (e.g. one compiled with different launch bounds)
+LIB_PATH = Path(os.environ.get("NOOR_B200_LIB", str(_HERE / "libnoor_b200.so")))
 
 f32 = C.c_float
 u32 = C.c_uint32

@@ -53,36 +53,39 @@ def _stale(obj: Path, deps: list[Path]) -> bool:
     return any(d.stat().st_mtime > t for d in deps)
 
 
-def build(force: bool = False, verbose: bool = False) -> Path:
-    """Compile every source that changed and relink the library."""
-    OBJ.mkdir(parents=True, exist_ok=True)
+def build(force: bool = False, verbose: bool = False, out: Path = OUT, obj: Path = OBJ,
+          defines: tuple = ()) -> Path:
+    """Compile every source that changed and relink the library (into `out`,
+    objects under `obj`, with extra -D `defines`)."""
+    OBJ_, OUT_ = obj, out
+    obj.mkdir(parents=True, exist_ok=True)
     nvcc = _nvcc()
     headers = list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + [ROOT / "include" / "noor_b200.h"]
     jobs = []
     objs = []
     for src in CU_SOURCES:
         s = CSRC / src
-        o = OBJ / (src + ".o")
+        o = OBJ_ / (src + ".o")
         objs.append(o)
         if force or _stale(o, [s] + headers):
-            jobs.append([nvcc, *NVCC_FLAGS, "-c", str(s), "-o", str(o)])
+            jobs.append([nvcc, *NVCC_FLAGS, *[f"-D{d}" for d in defines], "-c", str(s), "-o", str(o)])
     for src in CPP_SOURCES:
         s = CSRC / src
-        o = OBJ / (src + ".o")
+        o = OBJ_ / (src + ".o")
         objs.append(o)
         if force or _stale(o, [s] + headers):
             jobs.append(["g++", *CXX_FLAGS, "-I", str(ROOT / "include"), "-c", str(s), "-o", str(o)])
     if jobs:
         with ThreadPoolExecutor(max_workers=min(8, len(jobs))) as ex:
             list(ex.map(_run, jobs))
-    if force or jobs or _stale(OUT, objs):
-        tmp = OUT.with_suffix(".so.tmp")
+    if force or jobs or _stale(OUT_, objs):
+        tmp = OUT_.with_suffix(".so.tmp")
         _run([nvcc, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-cudart", "static",
               *[str(o) for o in objs], "-o", str(tmp)])
-        os.replace(tmp, OUT)
+        os.replace(tmp, OUT_)
     if verbose:
-        print(f"built {OUT}")
-    return OUT
+        print(f"built {OUT_}")
+    return OUT_
 
 
 if __name__ == "__main__":

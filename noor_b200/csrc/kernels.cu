@@ -21,8 +21,17 @@ NB_D void kahan_add(float3& sum, float3& c, const float3& x) {
     sum = t;
 }
 
+// minimum resident blocks per SM the megakernel is compiled for: 5 caps its
+// registers at 65536 / (128 * 5) = 102, i.e. 20 warps per SM instead of 12
+// at its natural ~155 registers; the traversal is latency-bound, so the
+// occupancy is worth the few spilled values (measured faster on the sky-lit
+// 2.6M-triangle scene)
+#ifndef NB_MEGA_MIN_BLOCKS
+#define NB_MEGA_MIN_BLOCKS 5
+#endif
+
 template <int ISECT, int FILM>
-__global__ void __launch_bounds__(kMegaBlock) megakernel(DevScene S, DevCamera C, MegaArgs a) {
+__global__ void __launch_bounds__(kMegaBlock, NB_MEGA_MIN_BLOCKS) megakernel(DevScene S, DevCamera C, MegaArgs a) {
     extern __shared__ uint32_t smem[];
     const uint32_t npix = C.w * C.h;
     const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;

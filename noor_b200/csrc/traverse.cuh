@@ -43,9 +43,7 @@ NB_D void tray_to_object(TRay& r, const TRay& w, const DevXform* xf) {
 }
 
 // slab test of noor/cuda/bbox.cuh:62-80
-NB_D bool slab_hit(const TRay& r, const uint4& lo, const uint4& hi, float tmax) {
-    const float mnx = __uint_as_float(lo.x), mny = __uint_as_float(lo.y), mnz = __uint_as_float(lo.z);
-    const float mxx = __uint_as_float(hi.x), mxy = __uint_as_float(hi.y), mxz = __uint_as_float(hi.z);
+NB_D bool slab_hit_f(const TRay& r, float mnx, float mny, float mnz, float mxx, float mxy, float mxz, float tmax) {
     const bool nx = r.neg & 1u, ny = r.neg & 2u, nz = r.neg & 4u;
     float tMin = xmul(xsub(nx ? mxx : mnx, r.o.x), r.inv.x);
     float tMax = xmul(xsub(nx ? mnx : mxx, r.o.x), r.inv.x);
@@ -60,6 +58,10 @@ NB_D bool slab_hit(const TRay& r, const uint4& lo, const uint4& hi, float tmax) 
     if (tzMin > tMin) tMin = tzMin;
     if (tzMax < tMax) tMax = tzMax;
     return (tMin < tmax) && (tMax > 0.0f);
+}
+NB_D bool slab_hit(const TRay& r, const uint4& lo, const uint4& hi, float tmax) {
+    return slab_hit_f(r, __uint_as_float(lo.x), __uint_as_float(lo.y), __uint_as_float(lo.z), __uint_as_float(hi.x),
+                      __uint_as_float(hi.y), __uint_as_float(hi.z), tmax);
 }
 
 // Wald projection test (noor/cuda/triangle.cuh:82-141); on success writes
@@ -345,5 +347,6 @@ NB_D bool trace_any(const DevScene& S, const float3& o, const float3& d, float t
     }
     return false;
 }
+
 
 }  // namespace nb

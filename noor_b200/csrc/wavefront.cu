@@ -6,7 +6,8 @@
 // share one pool and one launch.
 //
 // Per bounce (one iteration of a CUDA-graph while loop):
-//   regen   fold pending shadow results into each path's radiance; add
+//   regen   fold the last step's unblocked direct lighting into each
+//           path's radiance (L += beta * (c0' + c1'), as the megakernel); add
 //           finished paths to their frame's film; refill free slots with
 //           camera rays of the next (frame, sample, pixel) work item
 //   extend  closest hit for every active slot; misses and emitters finish
@@ -15,6 +16,7 @@
 //           occlusion test deferred to a shadow-ray queue, then scatter,
 //           Russian roulette and the next ray
 //   shadow  any hit for the queued shadow rays; blocked ones are cancelled
+//           (one ray per thread)
 //   check   stop when no slot is active; bounded by an iteration cap
 //
 // Every path draws the same random numbers in the same order as in the
@@ -60,13 +62,14 @@ struct WfDev {
     float4* d;       // direction, w = pixel bits
     float4* beta;    // throughput, w = bounce | spec << 16
     float4* L;       // radiance, w = RNG state bits
-    float4* pend;    // 2 per slot: contribution, w = 1 if pending
+    float4* pend;    // 2 per slot: direct-light contribution, w = 1 while it counts
+    float4* pbeta;   // throughput the contributions are weighted by (before the scatter)
     float4* hit;     // t, u, v, tri bits
     uint2* hit2;     // instance, material type
     uint32_t* state;
     uint32_t* qshade;       // kKinds * cap slot indices
     uint32_t* qshadow;      // 2 * cap entries: slot << 1 | which
-    float4* sh_o;           // origin, tmax
+    float4* sh_o;           // origin, tmax (by queue entry)
     float4* sh_d;           // direction
     uint32_t* counters;     // [0,kKinds) shade counts, [kKinds] shadow count, [kKinds+1] active, [kKinds+2] iteration
     unsigned long long* work_next;
@@ -82,6 +85,18 @@ struct WfDev {
     int stack_cap;
     cudaGraphConditionalHandle cond;
 };
+
+// minimum resident 256-thread blocks per SM the traversal stages (extend,
+// shadow) are compiled for: 4 caps their registers at 64, i.e. 32 warps per
+// SM instead of 24 at their natural ~80 (measured faster on the sky-lit
+// 2.6M-triangle scene)
+#ifndef NB_TRAV_MIN_BLOCKS
+#define NB_TRAV_MIN_BLOCKS 4
+#endif
+// the same for the shading stage
+#ifndef NB_SHADE_MIN_BLOCKS
+#define NB_SHADE_MIN_BLOCKS 1
+#endif
 
 NB_D uint32_t fbits(float f) { return __float_as_uint(f); }
 NB_D float bitsf(uint32_t u) { return __uint_as_float(u); }
@@ -133,21 +148,22 @@ __global__ void __launch_bounds__(256) wf_regen(WfDev W) {
     if (slot >= W.cap) return;
     uint32_t st = W.state[slot];
     if (st != kFree) {
-        // pending shadow results of the last shade step
-        float4 Lw = W.L[slot];
+        // fold the last shade step's direct lighting: L += beta * (c0' + c1')
+        // with c' = c if its shadow ray was unblocked, as the megakernel adds it
         const float4 p0 = W.pend[2 * slot], p1 = W.pend[2 * slot + 1];
-        if (p0.w != 0.0f) {
-            Lw.x += p0.x;
-            Lw.y += p0.y;
-            Lw.z += p0.z;
+        float4 Lw = W.L[slot];
+        if (p0.w != 0.0f || p1.w != 0.0f) {
+            float3 Ld = f3(0.0f);
+            if (p0.w != 0.0f) Ld += f3(p0.x, p0.y, p0.z);
+            if (p1.w != 0.0f) Ld += f3(p1.x, p1.y, p1.z);
+            const float4 b = W.pbeta[slot];
+            const float3 c = f3(b.x, b.y, b.z) * Ld;
+            Lw.x += c.x;
+            Lw.y += c.y;
+            Lw.z += c.z;
+            W.pend[2 * slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            W.pend[2 * slot + 1] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         }
-        if (p1.w != 0.0f) {
-            Lw.x += p1.x;
-            Lw.y += p1.y;
-            Lw.z += p1.z;
-        }
-        W.pend[2 * slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        W.pend[2 * slot + 1] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         if (st == kFinishing) {
             const uint32_t fi = fbits(W.o[slot].w);
             const uint32_t pix = fbits(W.d[slot].w);
@@ -159,7 +175,7 @@ __global__ void __launch_bounds__(256) wf_regen(WfDev W) {
             film_add(s + 1, cp + 1, c.y);
             film_add(s + 2, cp + 2, c.z);
             st = kFree;
-        } else {
+        } else if (p0.w != 0.0f || p1.w != 0.0f) {
             W.L[slot] = Lw;
         }
     }
@@ -247,7 +263,7 @@ NB_D void extend_one(const WfDev& W, uint32_t slot, const SmemStack& stk) {
     W.qshade[kind * W.cap + i] = slot;
 }
 
-__global__ void __launch_bounds__(256) wf_extend(WfDev W) {
+__global__ void __launch_bounds__(256, NB_TRAV_MIN_BLOCKS) wf_extend(WfDev W) {
     extern __shared__ uint32_t smem[];
     const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= W.cap || W.state[slot] != kActive) return;
@@ -261,6 +277,7 @@ __global__ void __launch_bounds__(256) wf_extend(WfDev W) {
     count_add(W.rays + 0, 1u);
 }
 
+// queues shadow ray `which` (0: light sample, 1: BSDF sample of MIS) of a slot
 NB_D void push_shadow(const WfDev& W, uint32_t slot, uint32_t which, const ShadowRay& sr) {
     const uint32_t i = queue_push(W.counters + kKinds);
     W.qshadow[i] = (slot << 1) | which;
@@ -268,7 +285,7 @@ NB_D void push_shadow(const WfDev& W, uint32_t slot, uint32_t which, const Shado
     W.sh_d[i] = make_float4(sr.d.x, sr.d.y, sr.d.z, 0.0f);
 }
 
-__global__ void __launch_bounds__(256) wf_shade(WfDev W, uint32_t kind) {
+__global__ void __launch_bounds__(256, NB_SHADE_MIN_BLOCKS) wf_shade(WfDev W, uint32_t kind) {
     const uint32_t n = W.counters[kind];
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint32_t slot = W.qshade[kind * W.cap + i];
@@ -298,20 +315,25 @@ __global__ void __launch_bounds__(256) wf_shade(WfDev W, uint32_t kind) {
         int li = 0;
         bool picked;
         ShadowRay sr;
+        // direct lighting: up to two contributions, each counted only if its
+        // shadow ray comes back unblocked; the next regen adds
+        // beta * (c0' + c1') to L as the megakernel does
         const float3 c0 = light_sample_contrib(S, m, I, rng, S.mis != 0, li, picked, sr);
-        if (!is_black(c0)) {
-            const float3 p = beta * c0;
-            W.pend[2 * slot] = make_float4(p.x, p.y, p.z, 1.0f);
+        const bool has0 = !is_black(c0);
+        if (has0) {
+            W.pend[2 * slot] = make_float4(c0.x, c0.y, c0.z, 1.0f);
             push_shadow(W, slot, 0, sr);
         }
+        bool has1 = false;
         if (S.mis && picked) {
             const float3 c1 = bsdf_mis_contrib(S, m, I, rng, li, sr);
-            if (!is_black(c1)) {
-                const float3 p = beta * c1;
-                W.pend[2 * slot + 1] = make_float4(p.x, p.y, p.z, 1.0f);
+            has1 = !is_black(c1);
+            if (has1) {
+                W.pend[2 * slot + 1] = make_float4(c1.x, c1.y, c1.z, 1.0f);
                 push_shadow(W, slot, 1, sr);
             }
         }
+        if (has0 || has1) W.pbeta[slot] = make_float4(beta.x, beta.y, beta.z, 0.0f);
         // scatter, sidedness, Russian roulette, next ray
         rng.next();
         rng.next();
@@ -348,7 +370,9 @@ __global__ void __launch_bounds__(256) wf_shade(WfDev W, uint32_t kind) {
     }
 }
 
-__global__ void __launch_bounds__(256) wf_shadow(WfDev W) {
+// Any hit for each queued shadow ray; a blocked one cancels its pending
+// contribution.
+__global__ void __launch_bounds__(256, NB_TRAV_MIN_BLOCKS) wf_shadow(WfDev W) {
     extern __shared__ uint32_t smem[];
     const uint32_t n = W.counters[kKinds];
     SmemStack stk{smem + threadIdx.x, (int)blockDim.x, W.stack_cap};
@@ -446,7 +470,8 @@ static int wf_ensure(Context& C, uint32_t cap) {
     const size_t n = cap;
     if ((rc = wf_alloc(S, (void**)&W.o, n * 16)) || (rc = wf_alloc(S, (void**)&W.d, n * 16)) ||
         (rc = wf_alloc(S, (void**)&W.beta, n * 16)) || (rc = wf_alloc(S, (void**)&W.L, n * 16)) ||
-        (rc = wf_alloc(S, (void**)&W.pend, 2 * n * 16)) || (rc = wf_alloc(S, (void**)&W.hit, n * 16)) ||
+        (rc = wf_alloc(S, (void**)&W.pend, 2 * n * 16)) || (rc = wf_alloc(S, (void**)&W.pbeta, n * 16)) ||
+        (rc = wf_alloc(S, (void**)&W.hit, n * 16)) ||
         (rc = wf_alloc(S, (void**)&W.hit2, n * 8)) || (rc = wf_alloc(S, (void**)&W.state, n * 4)) ||
         (rc = wf_alloc(S, (void**)&W.qshade, kKinds * n * 4)) || (rc = wf_alloc(S, (void**)&W.qshadow, 2 * n * 4)) ||
         (rc = wf_alloc(S, (void**)&W.sh_o, 2 * n * 16)) || (rc = wf_alloc(S, (void**)&W.sh_d, 2 * n * 16)) ||

@@ -175,11 +175,11 @@ def test_autograd_function_returns_entry_point_gradients():
 
 
 def test_adjoint_rejects_bad_configurations():
-    s = scenes.adjoint_scene(width=64, height=64, spp=1, count=2, level=2)
+    s = scenes.adjoint_scene(width=64, height=64, spp=1, count=4, level=2)
     r = scenes.Renderer(s)
     alb, rough, env = scene_parameters(s)
     with pytest.raises(_capi.NoorError):
-        render(alb, rough, env, 64, 64, 1)        # image size differs from the camera's
+        render(alb, rough, env, 32, 32, 1)        # image size differs from the camera's
     r.update_spec(rr=1)
     try:
         with pytest.raises(_capi.NoorError, match="Russian roulette"):
