@@ -128,15 +128,17 @@ def build_scene(args):
 
 
 def algorithmic_bytes(orc, cam, spp, isect, sample_pixels=20000, seed=0):
-    """Bytes a path reads by the traversal/shading model: per traversal step
-    32 B per node, per tested triangle 32 B (Wald: first sector) or 48 B
-    (watertight: three vertices), 16 B per in-range Wald triangle (second
+    """Bytes the path reads by the traversal/shading model: per traversal step
+    32 B per node, per tested triangle 48 B (watertight: three vertices) or
+    32 B (Wald: first sector) + 16 B per in-range triangle (Wald second
     record), per extension hit 16 B attributes + 3 x (16+16+8) B vertex data.
-    Counted by the oracle on a pixel subsample with 2 samples each."""
+    Counted by the oracle on a pixel subsample with 2 samples each.  Returns
+    bytes per path and the counts per path, with the traversal of extension
+    rays and of shadow rays apart."""
     n = cam.w * cam.h
     rng = np.random.default_rng(seed)
     px = np.sort(rng.choice(n, size=min(sample_pixels, n), replace=False))
-    tot = np.zeros(5, np.uint64)
+    tot = np.zeros(8, np.uint64)
     paths = 0
     # contiguous runs keep the oracle call simple: sample blocks of 64 pixels
     for b in px[:: 64]:
@@ -144,11 +146,34 @@ def algorithmic_bytes(orc, cam, spp, isect, sample_pixels=20000, seed=0):
         _, c = orc.render(cam, 1, 2, p0=int(b), p1=p1, isect=isect, threads=1, counters=True)
         tot += c
         paths += 2 * (p1 - int(b))
-    ext, shadow, nodes, tris, inrange = [float(x) / paths for x in tot]
+    ext, shadow, nodes, tris, inrange, sh_nodes, sh_tris, sh_inrange = [float(x) / paths for x in tot]
     tri_b = 32.0 if isect == 1 else 48.0
-    per_path = 32.0 * nodes + tri_b * tris + (16.0 * inrange if isect == 1 else 0.0) + ext * (16 + 3 * 40)
+
+    def trav(nd, tr, ir):
+        return 32.0 * nd + tri_b * tr + (16.0 * ir if isect == 1 else 0.0)
+
+    per_path = trav(nodes, tris, inrange) + ext * (16 + 3 * 40)
     return per_path, dict(ext_rays_per_path=ext, shadow_rays_per_path=shadow, nodes_per_path=nodes,
-                          tris_per_path=tris, sample_paths=paths)
+                          tris_per_path=tris, ext_nodes_per_path=nodes - sh_nodes, ext_tris_per_path=tris - sh_tris,
+                          ext_traversal_bytes_per_path=trav(nodes - sh_nodes, tris - sh_tris, inrange - sh_inrange),
+                          shadow_traversal_bytes_per_path=trav(sh_nodes, sh_tris, sh_inrange), sample_paths=paths)
+
+
+# slot state the extend kernel moves per ray besides the traversal: reads
+# origin + direction (32 B) and the queue entry (4 B); writes the hit record
+# (16 B + 8 B) and one queue entry (4 B)
+EXTEND_SLOT_BYTES = 64.0
+# ncu DRAM bytes per extension ray of wf_extend, from the capture summarised
+# in profiles/wf_extend_sky.md (the line "dram_bytes_per_ext_ray: X")
+TRAFFIC_PROFILE = ROOT / "profiles" / "wf_extend_sky.md"
+
+
+def profiled_traffic_per_ray():
+    import re
+    if not TRAFFIC_PROFILE.exists():
+        return None
+    m = re.search(r"dram_bytes_per_ext_ray:\s*([0-9.eE+]+)", TRAFFIC_PROFILE.read_text())
+    return float(m.group(1)) if m else None
 
 
 def calibrate_pixels(orc, cam, spp, threads, target_s):
@@ -280,6 +305,10 @@ class MegakernelPath:
     def describe(self):
         return {"entry_point": "noor_render_frames"}
 
+    def profile(self):
+        """(kernel, device ms, launches) of the dominant kernel of one step"""
+        return "megakernel", device_timed(self.step, 1), 1, {}
+
     def image(self):
         return self.r.framebuffer()[..., :3]
 
@@ -341,6 +370,18 @@ class WavefrontPath:
         import torch
         torch.cuda.synchronize()
         return self.film.cpu().numpy()[..., :3]
+
+    def profile(self):
+        """one render with CUDA events around every stage launch
+        (noor_wavefront_profile): (dominant kernel, its device ms summed over
+        its launches, launches, ms per stage)"""
+        from noor_b200 import _capi
+        prof = _capi.WfProfile()
+        _capi.call("noor_wavefront_profile", self.frames, 1, C.byref(self.params), C.byref(prof))
+        names = ["wf_regen", "wf_extend", "wf_shade", "wf_shadow", "wf_check"]
+        stages = {n: {"ms": float(prof.ms[i]), "launches": int(prof.launches[i])} for i, n in enumerate(names)}
+        top = max(range(5), key=lambda i: prof.ms[i])
+        return names[top], float(prof.ms[top]), int(prof.launches[top]), stages
 
 
 def device_timed(fn, steps):
@@ -567,6 +608,10 @@ def main():
                                                 "frac_pixels_rel_diff_gt_1e-3": float((rel > 1e-3).mean()),
                                                 "mean_ratio": float(img.mean() / max(oimg.mean(), 1e-30))}}
 
+    # the dominant kernel's device time, for the roofline (one extra render
+    # with events around every stage launch, outside the timed region)
+    top_kernel, top_ms, top_launches, stages = path.profile()
+
     # end to end through the public C-ABI with host buffers
     e2e_t = []
     for i in range(args.warmup + args.steps):
@@ -588,20 +633,29 @@ def main():
     if rank == 0:
         peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
         hbm = peaks.get("hbm_gbs", 6650.0)
-        roof = {"bound": "hbm", "achieved": None, "peak": hbm, "unit": "GB/s", "frac": None, "traffic": None,
-                "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
+        roof = {"bound": "hbm", "kernel": top_kernel, "achieved": None, "peak": hbm, "unit": "GB/s", "frac": None,
+                "traffic": None, "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+                "kernel_ms_per_step": top_ms, "kernel_launches_per_step": top_launches,
+                "kernel_share_of_step": top_ms / sum(v["ms"] for v in stages.values()) if stages else 1.0,
+                "stages": stages}
         cpu = None
         if not args.no_cpu_baseline:
             from oracle.oracle import Oracle
             orc = Oracle(built.payload, r.spec, r.hosek)
             per_path, counts = algorithmic_bytes(orc, r.camera, args.spp, r.spec.intersector)
             orc.close()
-            achieved = per_path * npaths / (ms_step / 1000) / 1e9
-            roof.update(achieved=achieved, frac=achieved / hbm, algorithmic_bytes_per_path=per_path, **counts)
-            prof = ROOT / "profiles" / f"{args.integrator}_sky_traffic.json"
-            if prof.exists():
-                tr = json.loads(prof.read_text())
-                roof["traffic"] = tr.get("dram_bytes_per_path", 0) * npaths
+            if top_kernel == "wf_extend":
+                # traversal bytes of the extension rays + the slot state of every ray
+                alg = counts["ext_traversal_bytes_per_path"] * npaths + EXTEND_SLOT_BYTES * ext / args.steps
+                tr = profiled_traffic_per_ray()
+                traffic = tr * ext / args.steps / top_launches if tr else None
+            else:
+                alg = per_path * npaths
+                traffic = None
+            achieved = alg / (top_ms / 1000) / 1e9
+            roof.update(achieved=achieved, frac=achieved / hbm, traffic=traffic,
+                        algorithmic_bytes_per_launch=alg / top_launches, algorithmic_bytes_per_path=per_path,
+                        **counts)
             cpu = cpu_baseline(args, s, built, r.spec, r.hosek, r.camera, args.cpu_seconds)
         line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
@@ -611,7 +665,7 @@ def main():
                            "intersector": "watertight", "film": "kahan",
                            "l2": "inputs larger than L2 (scene ~0.5 GB resident)",
                            "parallelism": f"replicas{world}", "bvh_build_s": round(build_s, 2), **path.describe()},
-                "mrays_per_s": mrays, "rays_per_step": (ext + shadow) / args.steps,
+                "mrays_per_s": mrays, "rays_per_step": (ext + shadow) / args.steps, "ext_rays_per_step": ext / args.steps,
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": launches, "clocks": clocks, "other_integrator": compare}
         print(json.dumps(line), flush=True)

@@ -517,6 +517,17 @@ int noor_wavefront_render_timed(const noor_wf_frame* frames, uint32_t n_frames,
                                 const noor_wf_params* params, float* ms);
 /* rays and paths the wavefront traced: [0] extension, [1] shadow, [2] paths */
 int noor_wavefront_counters(uint64_t counters[3], int reset);
+/* Device time per stage of one wavefront render, for measurement: the batch
+ * is rendered in the host-loop form (use_graph ignored) with CUDA events
+ * around every stage launch.  Stages: 0 regen, 1 extend, 2 shade (queue
+ * binning and all material kinds), 3 shadow, 4 stop test. */
+typedef struct noor_wf_profile {
+    float ms[5];                /* summed over iterations                   */
+    uint32_t launches[5];
+    uint32_t iterations;
+} noor_wf_profile;
+int noor_wavefront_profile(const noor_wf_frame* frames, uint32_t n_frames,
+                           const noor_wf_params* params, noor_wf_profile* out);
 /* The same frames rendered one after another by the plain megakernel
  * (one launch per frame, film folded with Kahan summation); device time of
  * the whole sequence in *ms. */

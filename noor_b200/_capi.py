@@ -152,6 +152,10 @@ class WfParams(C.Structure):
     _fields_ = [("block_size", u32), ("queue_capacity", u32), ("sort_granularity", u32), ("use_graph", u32)]
 
 
+class WfProfile(C.Structure):
+    _fields_ = [("ms", f32 * 5), ("launches", u32 * 5), ("iterations", u32)]
+
+
 class AdjointDesc(C.Structure):
     _fields_ = [("width", u32), ("height", u32), ("spp", u32), ("first_frame", u32), ("bounces", u32),
                 ("d_albedo", pf), ("d_roughness", pf), ("d_env", pf)]
@@ -201,6 +205,7 @@ PROTOTYPES = {
     "noor_wavefront_autotune": (C.c_int, [C.POINTER(WfFrame), u32, C.POINTER(WfParams), pf]),
     "noor_wavefront_render_timed": (C.c_int, [C.POINTER(WfFrame), u32, C.POINTER(WfParams), pf]),
     "noor_wavefront_counters": (C.c_int, [C.POINTER(u64), C.c_int]),
+    "noor_wavefront_profile": (C.c_int, [C.POINTER(WfFrame), u32, C.POINTER(WfParams), C.POINTER(WfProfile)]),
     "noor_megakernel_batch": (C.c_int, [C.POINTER(WfFrame), u32, pf]),
     "noor_megakernel_frame_noalloc": (C.c_int, [C.POINTER(WfFrame)]),
     "noor_context_current": (C.c_void_p, []),
@@ -211,7 +216,7 @@ PROTOTYPES = {
 
 
 ABI_STRUCTS = [Shape, AreaLight, Texture, Material, Payload, Camera, HosekState, HosekSky, Spec, Ray, Hit, BvhSpec,
-               Mesh, MaterialDesc, SceneDesc, BuildStat, WfFrame, WfParams, AdjointDesc]
+               Mesh, MaterialDesc, SceneDesc, BuildStat, WfFrame, WfParams, AdjointDesc, WfProfile]
 
 
 class NoorError(RuntimeError):

@@ -636,7 +636,7 @@ extern "C" int noor_abi_sizes(uint32_t* out, int n) {
                           sizeof(noor_spec), sizeof(noor_ray), sizeof(noor_hit), sizeof(noor_bvh_spec),
                           sizeof(noor_mesh), sizeof(noor_material_desc), sizeof(noor_scene_desc),
                           sizeof(noor_build_stat), sizeof(noor_wf_frame), sizeof(noor_wf_params),
-                          sizeof(noor_adjoint_desc)};
+                          sizeof(noor_adjoint_desc), sizeof(noor_wf_profile)};
     const int k = (int)(sizeof(s) / sizeof(s[0]));
     int w = 0;
     for (; out && w < n && w < k; ++w) out[w] = s[w];

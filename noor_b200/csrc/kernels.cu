@@ -21,13 +21,13 @@ NB_D void kahan_add(float3& sum, float3& c, const float3& x) {
     sum = t;
 }
 
-// minimum resident blocks per SM the megakernel is compiled for: 5 caps its
-// registers at 65536 / (128 * 5) = 102, i.e. 20 warps per SM instead of 12
+// minimum resident blocks per SM the megakernel is compiled for: 7 caps its
+// registers at 65536 / (128 * 7) = 73, i.e. 28 warps per SM instead of 12
 // at its natural ~155 registers; the traversal is latency-bound, so the
-// occupancy is worth the few spilled values (measured faster on the sky-lit
-// 2.6M-triangle scene)
+// occupancy is worth the spilled values (measured faster on the sky-lit
+// 2.6M-triangle scene than 5 or 6)
 #ifndef NB_MEGA_MIN_BLOCKS
-#define NB_MEGA_MIN_BLOCKS 5
+#define NB_MEGA_MIN_BLOCKS 7
 #endif
 
 template <int ISECT, int FILM>

@@ -9,15 +9,21 @@
 //   regen   fold the last step's unblocked direct lighting into each
 //           path's radiance (L += beta * (c0' + c1'), as the megakernel); add
 //           finished paths to their frame's film; refill free slots with
-//           camera rays of the next (frame, sample, pixel) work item
+//           camera rays of the next (frame, sample, pixel) work items, one
+//           8x4 pixel tile per warp
 //   extend  closest hit for every active slot; misses and emitters finish
-//           the path, surface hits are queued by material kind
+//           the path, surface hits are marked with their material kind
+//   bin     shading queues per material kind, in slot order
 //   shade   one launch per kind: light sample (+ MIS BSDF sample) with the
 //           occlusion test deferred to a shadow-ray queue, then scatter,
 //           Russian roulette and the next ray
 //   shadow  any hit for the queued shadow rays; blocked ones are cancelled
 //           (one ray per thread)
-//   check   stop when no slot is active; bounded by an iteration cap
+//   check   count rays; stop when no slot is active; bounded by an
+//           iteration cap
+// Counters that every slot touches (work items taken, active slots, queue
+// lengths) are reserved with one atomic per block, not per warp: a single
+// address serialises its atomics in L2.
 //
 // Every path draws the same random numbers in the same order as in the
 // megakernel (seed TEA(pixel, frame), LCG state carried in the slot), so
@@ -53,8 +59,22 @@ struct WfFrameDev {
     float* out;    // caller's film (mean, float4 per pixel) or null
 };
 
-// slot state
-enum : uint32_t { kFree = 0, kActive = 1, kFinishing = 2 };
+// slot state: bits 0-1 kFree / kActive / kFinishing; kPend while the direct
+// lighting of the last shade step waits for regen to fold it into L; bits
+// 3-4 the shading queue (1 + material kind) extend assigned to a surface hit
+enum : uint32_t { kFree = 0, kActive = 1, kFinishing = 2, kLifeMask = 3, kPend = 4, kKindShift = 3 };
+
+// counter words
+enum : int {
+    kCntShadow = kKinds,       // [0, kKinds) shade queue lengths, then the shadow queue length
+    kCntActive = kKinds + 1,   // slots holding a path after regen (= rays extend traces)
+    kCntIter = kKinds + 2,     // iterations run
+    kCntWords = kKinds + 3
+};
+
+// block sizes of the slot sweeps (one block-wide atomic per counter)
+constexpr int kRegenBlock = 512;
+constexpr int kBinBlock = 1024;
 
 struct WfDev {
     // path slots
@@ -71,9 +91,9 @@ struct WfDev {
     uint32_t* qshadow;      // 2 * cap entries: slot << 1 | which
     float4* sh_o;           // origin, tmax (by queue entry)
     float4* sh_d;           // direction
-    uint32_t* counters;     // [0,kKinds) shade counts, [kKinds] shadow count, [kKinds+1] active, [kKinds+2] iteration
+    uint32_t* counters;     // kCntWords words
     unsigned long long* work_next;
-    unsigned long long* rays;  // [ext, shadow, paths]
+    unsigned long long* rays;  // [ext, shadow, paths], added up by wf_check
     uint32_t* status;
     const WfFrameDev* frames;
     const DevScene* scenes;
@@ -115,12 +135,6 @@ NB_D uint32_t queue_push(uint32_t* counter) {
     return base + __popc(peers & ((1u << lane) - 1u));
 }
 
-NB_D void count_add(unsigned long long* ctr, uint32_t v) {
-    const uint32_t mask = __activemask();
-    const uint32_t s = __reduce_add_sync(mask, v);
-    if ((int)(threadIdx.x & 31) == __ffs(mask) - 1 && s) atomicAdd(ctr, (unsigned long long)s);
-}
-
 // compensated atomic add: TwoSum of (old, v) recovers the rounding error of
 // the atomic add exactly; it goes to the compensation buffer
 NB_D void film_add(float* sum, float* comp, float v) {
@@ -143,16 +157,46 @@ NB_D int frame_of(const WfDev& W, unsigned long long k) {
     return lo;
 }
 
-__global__ void __launch_bounds__(256) wf_regen(WfDev W) {
+NB_D uint32_t lanes_below() { return (1u << (threadIdx.x & 31)) - 1u; }
+
+// pixel of the q-th camera ray of a sample: 8x4 tiles in row-major tile
+// order, row-major inside a tile, so that the 32 lanes of a warp trace a
+// compact bundle; pixels outside the whole tiles follow row by row (the
+// right strip, then the bottom rows)
+NB_D uint32_t tile_pixel(uint32_t q, uint32_t w, uint32_t h) {
+    const uint32_t w8 = w & ~7u, h4 = h & ~3u;
+    const uint32_t full = w8 * h4;
+    if (q < full) {
+        const uint32_t t = q >> 5, r = q & 31u;
+        const uint32_t tx = t % (w8 >> 3), ty = t / (w8 >> 3);
+        return (ty * 4u + (r >> 3)) * w + tx * 8u + (r & 7u);
+    }
+    q -= full;
+    const uint32_t rw = w - w8;
+    if (q < rw * h4) return (q / rw) * w + w8 + q % rw;
+    q -= rw * h4;
+    return (h4 + q / w) * w + q % w;
+}
+
+// Regen (every slot): fold the last shade step's direct lighting into L; add
+// finished paths to their frame's film; refill free slots with the camera
+// rays of the next work items.  The block takes its work items with one
+// atomic, in lane order (consecutive lanes: consecutive pixels of one 8x4
+// tile), and adds its active slots to the active count with one atomic.
+__global__ void __launch_bounds__(kRegenBlock) wf_regen(WfDev W) {
+    __shared__ uint32_t warp_off[kRegenBlock / 32];
+    __shared__ unsigned long long block_base;
     const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
-    if (slot >= W.cap) return;
-    uint32_t st = W.state[slot];
-    if (st != kFree) {
-        // fold the last shade step's direct lighting: L += beta * (c0' + c1')
-        // with c' = c if its shadow ray was unblocked, as the megakernel adds it
-        const float4 p0 = W.pend[2 * slot], p1 = W.pend[2 * slot + 1];
-        float4 Lw = W.L[slot];
-        if (p0.w != 0.0f || p1.w != 0.0f) {
+    const bool valid = slot < W.cap;
+    uint32_t st = kFree;
+    if (valid) {
+        st = W.state[slot];
+        float4 Lw;
+        if (st & kPend) {
+            // L += beta * (c0' + c1') with c' = c if its shadow ray was
+            // unblocked, as the megakernel adds its direct lighting
+            const float4 p0 = W.pend[2 * slot], p1 = W.pend[2 * slot + 1];
+            Lw = W.L[slot];
             float3 Ld = f3(0.0f);
             if (p0.w != 0.0f) Ld += f3(p0.x, p0.y, p0.z);
             if (p1.w != 0.0f) Ld += f3(p1.x, p1.y, p1.z);
@@ -161,10 +205,10 @@ __global__ void __launch_bounds__(256) wf_regen(WfDev W) {
             Lw.x += c.x;
             Lw.y += c.y;
             Lw.z += c.z;
-            W.pend[2 * slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            W.pend[2 * slot + 1] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            if ((st & kLifeMask) == kActive) W.L[slot] = Lw;
         }
-        if (st == kFinishing) {
+        if ((st & kLifeMask) == kFinishing) {
+            if (!(st & kPend)) Lw = W.L[slot];
             const uint32_t fi = fbits(W.o[slot].w);
             const uint32_t pix = fbits(W.d[slot].w);
             const WfFrameDev& F = W.frames[fi];
@@ -175,43 +219,45 @@ __global__ void __launch_bounds__(256) wf_regen(WfDev W) {
             film_add(s + 1, cp + 1, c.y);
             film_add(s + 2, cp + 2, c.z);
             st = kFree;
-        } else if (p0.w != 0.0f || p1.w != 0.0f) {
-            W.L[slot] = Lw;
+        }
+        st &= kLifeMask;
+    }
+    const bool need = valid && st == kFree;
+    const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const uint32_t ball = __ballot_sync(0xFFFFFFFFu, need);
+    if (lane == 0) warp_off[wid] = __popc(ball);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t tot = 0;
+        for (int w = 0; w < kRegenBlock / 32; ++w) {
+            const uint32_t c = warp_off[w];
+            warp_off[w] = tot;
+            tot += c;
+        }
+        block_base = tot ? atomicAdd(W.work_next, (unsigned long long)tot) : 0ull;
+    }
+    __syncthreads();
+    if (need) {
+        const unsigned long long k = block_base + warp_off[wid] + __popc(ball & lanes_below());
+        if (k < W.total) {
+            const int fi = frame_of(W, k);
+            const WfFrameDev& F = W.frames[fi];
+            const unsigned long long local = k - F.base;
+            const uint32_t sample = (uint32_t)(local / F.npix);
+            const uint32_t pix = tile_pixel((uint32_t)(local % F.npix), F.cam.w, F.cam.h);
+            Rng rng{tea16(pix, F.first_frame + sample)};
+            float3 o, d;
+            camera_ray(F.cam, pix % F.cam.w, pix / F.cam.w, rng, o, d);
+            W.o[slot] = make_float4(o.x, o.y, o.z, bitsf((uint32_t)fi));
+            W.d[slot] = make_float4(d.x, d.y, d.z, bitsf(pix));
+            W.beta[slot] = make_float4(1.0f, 1.0f, 1.0f, bitsf(0u));
+            W.L[slot] = make_float4(0.0f, 0.0f, 0.0f, bitsf(rng.s));
+            st = kActive;
         }
     }
-    const bool need = st == kFree;
-    const uint32_t mask = __ballot_sync(__activemask(), need);
-    unsigned long long k = ~0ull;
-    if (need) {
-        const int lane = threadIdx.x & 31;
-        const int leader = __ffs(mask) - 1;
-        unsigned long long base = 0;
-        if (lane == leader) base = atomicAdd(W.work_next, (unsigned long long)__popc(mask));
-        base = __shfl_sync(mask, base, leader);
-        k = base + __popc(mask & ((1u << lane) - 1u));
-    }
-    if (need && k < W.total) {
-        const int fi = frame_of(W, k);
-        const WfFrameDev& F = W.frames[fi];
-        const unsigned long long local = k - F.base;
-        const uint32_t sample = (uint32_t)(local / F.npix);
-        const uint32_t pix = (uint32_t)(local % F.npix);
-        Rng rng{tea16(pix, F.first_frame + sample)};
-        float3 o, d;
-        camera_ray(F.cam, pix % F.cam.w, pix / F.cam.w, rng, o, d);
-        W.o[slot] = make_float4(o.x, o.y, o.z, bitsf((uint32_t)fi));
-        W.d[slot] = make_float4(d.x, d.y, d.z, bitsf(pix));
-        W.beta[slot] = make_float4(1.0f, 1.0f, 1.0f, bitsf(0u));
-        W.L[slot] = make_float4(0.0f, 0.0f, 0.0f, bitsf(rng.s));
-        st = kActive;
-        count_add(W.rays + 2, 1u);
-    }
-    W.state[slot] = st;
-    if (st == kActive) {
-        const uint32_t am = __activemask();
-        const uint32_t n = __popc(am);
-        if ((int)(threadIdx.x & 31) == __ffs(am) - 1) atomicAdd(W.counters + kKinds + 1, n);
-    }
+    if (valid) W.state[slot] = st;
+    const int nact = __syncthreads_count(valid && st == kActive);
+    if (threadIdx.x == 0 && nact) atomicAdd(W.counters + kCntActive, (uint32_t)nact);
 }
 
 template <int ISECT>
@@ -259,8 +305,7 @@ NB_D void extend_one(const WfDev& W, uint32_t slot, const SmemStack& stk) {
     W.hit2[slot] = make_uint2(rec.ins, rec.mtype);
     const uint32_t lobe = lobe_of(rec.mtype);
     const uint32_t kind = W.sort ? (lobe == kLobeLambert ? 0u : (lobe == kLobeConductor ? 1u : 2u)) : 0u;
-    const uint32_t i = queue_push(W.counters + kind);
-    W.qshade[kind * W.cap + i] = slot;
+    W.state[slot] = kActive | ((kind + 1u) << kKindShift);  // wf_bin queues it for shading
 }
 
 __global__ void __launch_bounds__(256, NB_TRAV_MIN_BLOCKS) wf_extend(WfDev W) {
@@ -274,12 +319,44 @@ __global__ void __launch_bounds__(256, NB_TRAV_MIN_BLOCKS) wf_extend(WfDev W) {
         extend_one<NOOR_ISECT_WATERTIGHT>(W, slot, stk);
     else
         extend_one<NOOR_ISECT_REF_WALD>(W, slot, stk);
-    count_add(W.rays + 0, 1u);
+}
+
+// Shading queues in slot order: every slot extend left a surface hit goes to
+// the queue of its material kind (one block-wide atomic per kind), so that
+// shade reads the slots' state in nearly ascending order.
+__global__ void __launch_bounds__(kBinBlock) wf_bin(WfDev W) {
+    __shared__ uint32_t cnt[kKinds][kBinBlock / 32];
+    __shared__ uint32_t base[kKinds];
+    const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t kq = slot < W.cap ? (W.state[slot] >> kKindShift) & 3u : 0u;  // 1 + kind, 0: none
+    const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    uint32_t mine = 0;
+    for (uint32_t k = 0; k < (uint32_t)kKinds; ++k) {
+        const uint32_t b = __ballot_sync(0xFFFFFFFFu, kq == k + 1u);
+        if (kq == k + 1u) mine = __popc(b & lanes_below());
+        if (lane == 0) cnt[k][wid] = __popc(b);
+    }
+    __syncthreads();
+    if (threadIdx.x < (uint32_t)kKinds) {
+        const uint32_t k = threadIdx.x;
+        uint32_t tot = 0;
+        for (int w = 0; w < kBinBlock / 32; ++w) {
+            const uint32_t c = cnt[k][w];
+            cnt[k][w] = tot;
+            tot += c;
+        }
+        base[k] = tot ? atomicAdd(W.counters + k, tot) : 0u;
+    }
+    __syncthreads();
+    if (kq) {
+        const uint32_t k = kq - 1u;
+        W.qshade[k * W.cap + base[k] + cnt[k][wid] + mine] = slot;
+    }
 }
 
 // queues shadow ray `which` (0: light sample, 1: BSDF sample of MIS) of a slot
 NB_D void push_shadow(const WfDev& W, uint32_t slot, uint32_t which, const ShadowRay& sr) {
-    const uint32_t i = queue_push(W.counters + kKinds);
+    const uint32_t i = queue_push(W.counters + kCntShadow);
     W.qshadow[i] = (slot << 1) | which;
     W.sh_o[i] = make_float4(sr.o.x, sr.o.y, sr.o.z, sr.tmax);
     W.sh_d[i] = make_float4(sr.d.x, sr.d.y, sr.d.z, 0.0f);
@@ -289,7 +366,7 @@ __global__ void __launch_bounds__(256, NB_SHADE_MIN_BLOCKS) wf_shade(WfDev W, ui
     const uint32_t n = W.counters[kind];
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint32_t slot = W.qshade[kind * W.cap + i];
-        const float4 ow = W.o[slot], dw = W.d[slot], bw = W.beta[slot], Lw = W.L[slot];
+        const float4 ow = W.o[slot], dw = W.d[slot], bw = W.beta[slot], Lw = W.L[slot];  // Lw.w: RNG state
         const float4 hw = W.hit[slot];
         const uint2 h2 = W.hit2[slot];
         const uint32_t fi = fbits(ow.w);
@@ -320,20 +397,20 @@ __global__ void __launch_bounds__(256, NB_SHADE_MIN_BLOCKS) wf_shade(WfDev W, ui
         // beta * (c0' + c1') to L as the megakernel does
         const float3 c0 = light_sample_contrib(S, m, I, rng, S.mis != 0, li, picked, sr);
         const bool has0 = !is_black(c0);
-        if (has0) {
-            W.pend[2 * slot] = make_float4(c0.x, c0.y, c0.z, 1.0f);
-            push_shadow(W, slot, 0, sr);
-        }
+        if (has0) push_shadow(W, slot, 0, sr);
+        float3 c1 = f3(0.0f);
         bool has1 = false;
         if (S.mis && picked) {
-            const float3 c1 = bsdf_mis_contrib(S, m, I, rng, li, sr);
+            c1 = bsdf_mis_contrib(S, m, I, rng, li, sr);
             has1 = !is_black(c1);
-            if (has1) {
-                W.pend[2 * slot + 1] = make_float4(c1.x, c1.y, c1.z, 1.0f);
-                push_shadow(W, slot, 1, sr);
-            }
+            if (has1) push_shadow(W, slot, 1, sr);
         }
-        if (has0 || has1) W.pbeta[slot] = make_float4(beta.x, beta.y, beta.z, 0.0f);
+        const bool pend = has0 || has1;
+        if (pend) {
+            W.pend[2 * slot] = has0 ? make_float4(c0.x, c0.y, c0.z, 1.0f) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            W.pend[2 * slot + 1] = has1 ? make_float4(c1.x, c1.y, c1.z, 1.0f) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            W.pbeta[slot] = make_float4(beta.x, beta.y, beta.z, 0.0f);
+        }
         // scatter, sidedness, Russian roulette, next ray
         rng.next();
         rng.next();
@@ -366,7 +443,7 @@ __global__ void __launch_bounds__(256, NB_SHADE_MIN_BLOCKS) wf_shade(WfDev W, ui
             if (nb_ >= F.bounces) st = kFinishing;
         }
         W.L[slot] = make_float4(Lw.x, Lw.y, Lw.z, bitsf(rng.s));
-        W.state[slot] = st;
+        W.state[slot] = st | (pend ? kPend : 0u);
     }
 }
 
@@ -374,11 +451,9 @@ __global__ void __launch_bounds__(256, NB_SHADE_MIN_BLOCKS) wf_shade(WfDev W, ui
 // contribution.
 __global__ void __launch_bounds__(256, NB_TRAV_MIN_BLOCKS) wf_shadow(WfDev W) {
     extern __shared__ uint32_t smem[];
-    const uint32_t n = W.counters[kKinds];
+    const uint32_t n = W.counters[kCntShadow];
     SmemStack stk{smem + threadIdx.x, (int)blockDim.x, W.stack_cap};
-    uint32_t traced = 0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        ++traced;
         const uint32_t e = W.qshadow[i];
         const uint32_t slot = e >> 1;
         const float4 so = W.sh_o[i], sd = W.sh_d[i];
@@ -391,29 +466,28 @@ __global__ void __launch_bounds__(256, NB_TRAV_MIN_BLOCKS) wf_shadow(WfDev W) {
             occ = trace_any<NOOR_ISECT_REF_WALD>(S, f3(so.x, so.y, so.z), f3(sd.x, sd.y, sd.z), so.w, stk, W.status);
         if (occ) W.pend[e].w = 0.0f;
     }
-    count_add(W.rays + 1, traced);
 }
 
-__global__ void wf_check(WfDev W) {
+// End of an iteration: count the rays traced (extend traced every active
+// slot), stop when regen found no slot holding a path (bounded by an
+// iteration cap), reset the per-iteration counters.
+__global__ void wf_check(WfDev W, uint32_t* go_out, uint32_t conditional) {
     uint32_t* c = W.counters;
-    const uint32_t active = c[kKinds + 1];
-    const uint32_t it = ++c[kKinds + 2];
+    const uint32_t active = c[kCntActive];
+    W.rays[0] += active;
+    W.rays[1] += c[kCntShadow];
+    const uint32_t it = ++c[kCntIter];
     bool go = active > 0u;
     if (go && it >= W.max_iters) {
         atomicOr(W.status, NOOR_DEV_WAIT_TIMEOUT);
         go = false;
     }
-    for (int k = 0; k <= kKinds + 1; ++k) c[k] = 0u;
-    cudaGraphSetConditional(W.cond, go ? 1u : 0u);
-}
-
-// host-loop variant of the stop test (no conditional node): publishes the
-// active count for the host to read
-__global__ void wf_check_host(WfDev W, uint32_t* active_out) {
-    uint32_t* c = W.counters;
-    *active_out = c[kKinds + 1];
-    ++c[kKinds + 2];
-    for (int k = 0; k <= kKinds + 1; ++k) c[k] = 0u;
+    if (!go) W.rays[2] += *W.work_next < W.total ? *W.work_next : W.total;
+    for (int k = 0; k <= kCntActive; ++k) c[k] = 0u;
+    if (conditional)
+        cudaGraphSetConditional(W.cond, go ? 1u : 0u);
+    else
+        *go_out = go ? 1u : 0u;
 }
 
 // mean = (sum + comp) / spp into the caller's film
@@ -475,7 +549,7 @@ static int wf_ensure(Context& C, uint32_t cap) {
         (rc = wf_alloc(S, (void**)&W.hit2, n * 8)) || (rc = wf_alloc(S, (void**)&W.state, n * 4)) ||
         (rc = wf_alloc(S, (void**)&W.qshade, kKinds * n * 4)) || (rc = wf_alloc(S, (void**)&W.qshadow, 2 * n * 4)) ||
         (rc = wf_alloc(S, (void**)&W.sh_o, 2 * n * 16)) || (rc = wf_alloc(S, (void**)&W.sh_d, 2 * n * 16)) ||
-        (rc = wf_alloc(S, (void**)&W.counters, 64)) || (rc = wf_alloc(S, (void**)&W.work_next, 16)) ||
+        (rc = wf_alloc(S, (void**)&W.counters, kCntWords * 4)) || (rc = wf_alloc(S, (void**)&W.work_next, 16)) ||
         (rc = wf_alloc(S, (void**)&W.rays, 32)))
         return rc;
     cudaError_t e = cudaMalloc((void**)&S.active_host_dev, 16);
@@ -488,27 +562,34 @@ static int wf_ensure(Context& C, uint32_t cap) {
 struct WfLaunch {
     int block;
     size_t smem;
-    uint32_t grid_slots;
-    uint32_t grid_queue;
+    uint32_t grid_slots;    // one thread per slot / queue entry
+    uint32_t grid_queue;    // grid-stride stages
 };
 
+// one iteration; with `ev` (6 events), records ev[0] before the first stage
+// and ev[k + 1] after stage k (regen, extend, shade with its queue binning,
+// shadow, stop test)
 static cudaError_t wf_iteration(const WfDev& W, const WfLaunch& L, cudaStream_t s, bool conditional,
-                                uint32_t* active_out) {
-    wf_regen<<<(W.cap + 255) / 256, 256, 0, s>>>(W);
+                                uint32_t* go_out, cudaEvent_t* ev = nullptr) {
+    if (ev) cudaEventRecord(ev[0], s);
+    wf_regen<<<(W.cap + kRegenBlock - 1) / kRegenBlock, kRegenBlock, 0, s>>>(W);
+    if (ev) cudaEventRecord(ev[1], s);
     wf_extend<<<L.grid_slots, L.block, L.smem, s>>>(W);
+    if (ev) cudaEventRecord(ev[2], s);
+    wf_bin<<<(W.cap + kBinBlock - 1) / kBinBlock, kBinBlock, 0, s>>>(W);
     const int nk = W.sort ? kKinds : 1;
     for (int k = 0; k < nk; ++k) wf_shade<<<L.grid_queue, 256, 0, s>>>(W, (uint32_t)k);
+    if (ev) cudaEventRecord(ev[3], s);
     wf_shadow<<<L.grid_queue, L.block, L.smem, s>>>(W);
-    if (conditional)
-        wf_check<<<1, 1, 0, s>>>(W);
-    else
-        wf_check_host<<<1, 1, 0, s>>>(W, active_out);
+    if (ev) cudaEventRecord(ev[4], s);
+    wf_check<<<1, 1, 0, s>>>(W, go_out, conditional ? 1u : 0u);
+    if (ev) cudaEventRecord(ev[5], s);
     return cudaGetLastError();
 }
 
 // one batch render; returns device-timed ms through `ms` when non-null
 int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames, const noor_wf_params& P,
-                     float* ms_out) {
+                     float* ms_out, noor_wf_profile* prof = nullptr) {
     if (!frames || n_frames == 0) return set_error(NOOR_ERR_INVALID, "wavefront: no frames");
     const uint32_t block = P.block_size ? P.block_size : 128;
     if (block != 64 && block != 128 && block != 256)
@@ -593,8 +674,7 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
     if (e == cudaSuccess) e = cudaMemsetAsync(WS.films, 0, film_bytes, s);
     WfDev& W = WS.dev;
     if (e == cudaSuccess) e = cudaMemsetAsync(W.state, 0, (size_t)cap * 4, s);
-    if (e == cudaSuccess) e = cudaMemsetAsync(W.pend, 0, (size_t)cap * 32, s);
-    if (e == cudaSuccess) e = cudaMemsetAsync(W.counters, 0, 64, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(W.counters, 0, kCntWords * 4, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(W.work_next, 0, 16, s);
     if (e != cudaSuccess) return cuda_fail(e, "wavefront setup");
     W.status = C.status;
@@ -621,7 +701,7 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
     }
     if (ms_out) cudaEventRecord(C.events[6], s);
     bool done = false;
-    if (P.use_graph) {
+    if (P.use_graph && !prof) {
         cudaGraph_t graph = nullptr;
         cudaGraphExec_t exec = nullptr;
         e = cudaGraphCreate(&graph, 0);
@@ -655,13 +735,32 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
         // host loop: one iteration per launch sequence, reading the active
         // count back every iteration (bounded by the iteration cap)
         uint32_t active = 1;
-        for (uint32_t it = 0; it < W.max_iters && active; ++it) {
-            e = wf_iteration(W, L, s, false, WS.active_host_dev);
+        cudaEvent_t ev[6] = {};
+        if (prof) {
+            std::memset(prof, 0, sizeof(*prof));
+            for (auto& x : ev)
+                if (e == cudaSuccess) e = cudaEventCreate(&x);
+        }
+        const uint32_t nk = W.sort ? kKinds : 1;
+        for (uint32_t it = 0; e == cudaSuccess && it < W.max_iters && active; ++it) {
+            e = wf_iteration(W, L, s, false, WS.active_host_dev, prof ? ev : nullptr);
             if (e == cudaSuccess) e = cudaMemcpyAsync(&active, WS.active_host_dev, 4, cudaMemcpyDeviceToHost, s);
             if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-            if (e != cudaSuccess) return cuda_fail(e, "wavefront iteration");
-            C.launches += 4 + (W.sort ? kKinds : 1);
+            C.launches += 5 + nk;
+            if (prof && e == cudaSuccess) {
+                for (int k = 0; k < 5; ++k) {
+                    float ms = 0.0f;
+                    cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
+                    prof->ms[k] += ms;
+                    prof->launches[k] += k == 2 ? nk + 1 : 1u;
+                }
+                ++prof->iterations;
+            }
         }
+        if (prof)
+            for (auto& x : ev)
+                if (x) cudaEventDestroy(x);
+        if (e != cudaSuccess) return cuda_fail(e, "wavefront iteration");
     }
     for (uint32_t i = 0; i < n_frames; ++i)
         if (fr[i].out) wf_resolve<<<(fr[i].npix + 255) / 256, 256, 0, s>>>(WS.frames_dev, i);
@@ -671,8 +770,8 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
     if (ms_out) cudaEventElapsedTime(ms_out, C.events[6], C.events[7]);
     // iterations actually run (for the launch count)
     uint32_t iters = 0;
-    cudaMemcpy(&iters, W.counters + kKinds + 2, 4, cudaMemcpyDeviceToHost);
-    if (P.use_graph) C.launches += (uint64_t)iters * (4 + (W.sort ? kKinds : 1)) - (uint64_t)W.max_iters;
+    cudaMemcpy(&iters, W.counters + kCntIter, 4, cudaMemcpyDeviceToHost);
+    if (P.use_graph) C.launches += (uint64_t)iters * (5 + (W.sort ? kKinds : 1)) - (uint64_t)W.max_iters;
     return NOOR_OK;
 }
 
@@ -697,6 +796,17 @@ extern "C" int noor_wavefront_render_timed(const noor_wf_frame* frames, uint32_t
     noor_wf_params p{};
     if (params) p = *params;
     return wavefront_render(*C, frames, n_frames, p, ms);
+}
+
+extern "C" int noor_wavefront_profile(const noor_wf_frame* frames, uint32_t n_frames,
+                                      const noor_wf_params* params, noor_wf_profile* out) {
+    Context* C;
+    int rc = need_ctx(C);
+    if (rc) return rc;
+    if (!out) return set_error(NOOR_ERR_INVALID, "wavefront profile: out is null");
+    noor_wf_params p{};
+    if (params) p = *params;
+    return wavefront_render(*C, frames, n_frames, p, nullptr, out);
 }
 
 extern "C" int noor_wavefront_counters(uint64_t counters[3], int reset) {
@@ -725,7 +835,7 @@ extern "C" int noor_wavefront_autotune(const noor_wf_frame* frames, uint32_t n_f
     if (rc) return rc;
     if (!best) return set_error(NOOR_ERR_INVALID, "autotune: best is null");
     const uint32_t blocks[] = {64, 128, 256};
-    const uint32_t caps[] = {1u << 20, 1u << 21, 1u << 22};
+    const uint32_t caps[] = {1u << 21, 1u << 22, 1u << 23};
     const uint32_t sorts[] = {0, 1};
     float bms = 3.4e38f;
     noor_wf_params bp{128, 1u << 20, 1, best->use_graph};

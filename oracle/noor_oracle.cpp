@@ -928,8 +928,11 @@ template <class T> V<T> area_p(const noor_area_light& A, int which) {
     return which == 0 ? v3f<T>(A.shape.center) : (which == 1 ? v3f<T>(A.shape.u) : (which == 2 ? v3f<T>(A.shape.v) : v3f<T>(A.shape.n)));
 }
 
+// traversal work: rays, nodes popped, triangles tested, triangles whose t
+// passed the range test (all rays), and the same three for shadow rays alone
 struct Counters {
     uint64_t ext = 0, shadow = 0, nodes = 0, tris = 0, tri_in_range = 0;
+    uint64_t sh_nodes = 0, sh_tris = 0, sh_in_range = 0;
 };
 
 template <class T> bool occl(const Scene& sc, V<T> o, V<T> d, T tmax, int isect, Counters* c) {
@@ -940,6 +943,9 @@ template <class T> bool occl(const Scene& sc, V<T> o, V<T> d, T tmax, int isect,
         c->nodes += ctr[0];
         c->tris += ctr[1];
         c->tri_in_range += ctr[2];
+        c->sh_nodes += ctr[0];
+        c->sh_tris += ctr[1];
+        c->sh_in_range += ctr[2];
     }
     return r;
 }
@@ -1544,7 +1550,8 @@ OR_API void oracle_camera_rays(const noor_camera* C, uint32_t frame, noor_ray* r
 
 // Render pixels [p0, p1) x frames [f0, f0+nf): out = per-pixel mean rgb
 // (sequential Kahan sum in FP32 mode, plain sum in FP64), counters
-// (optional, 5 x uint64: ext rays, shadow rays, nodes, triangles, triangles in range).
+// (optional, 8 x uint64: ext rays, shadow rays, nodes, triangles, triangles
+// in range, then nodes, triangles, triangles in range of the shadow rays alone).
 OR_API void oracle_render(void* h, uint32_t f0, uint32_t nf, uint32_t p0, uint32_t p1, const noor_camera* C,
                           int fp64, int isect, int threads, float* out_rgb, uint64_t* counters) {
     const Scene& sc = ((Ctx*)h)->sc;
@@ -1590,13 +1597,16 @@ OR_API void oracle_render(void* h, uint32_t f0, uint32_t nf, uint32_t p0, uint32
     for (int t = 0; t < T; ++t) th.emplace_back(work, t);
     for (auto& x : th) x.join();
     if (counters) {
-        for (int k = 0; k < 5; ++k) counters[k] = 0;
+        for (int k = 0; k < 8; ++k) counters[k] = 0;
         for (auto& c : cs) {
             counters[0] += c.ext;
             counters[1] += c.shadow;
             counters[2] += c.nodes;
             counters[3] += c.tris;
             counters[4] += c.tri_in_range;
+            counters[5] += c.sh_nodes;
+            counters[6] += c.sh_tris;
+            counters[7] += c.sh_in_range;
         }
     }
 }

@@ -113,7 +113,7 @@ class Oracle:
         if p1 is None:
             p1 = camera.w * camera.h
         out = np.zeros((p1 - p0) * 3, np.float32)
-        ctr = np.zeros(5, np.uint64)
+        ctr = np.zeros(8, np.uint64)  # ext, shadow, nodes, tris, in range (all rays); the last three of shadow rays
         lib().oracle_render(self.h, frame0, nframes, p0, p1, C.addressof(camera), int(fp64), isect, threads,
                             _p(out), _p(ctr) if counters else None)
         out = out.reshape(-1, 3)
