@@ -192,134 +192,6 @@ struct SmemStack {
     int cap;
 };
 
-// Traversal state of one ray for the persistent wavefront kernels: they run
-// trav_step, one node per step, so that a lane whose ray finished can take
-// a new ray while the other lanes of its warp continue theirs.  A step is
-// one iteration of the loop of trace_closest / trace_any below (the same
-// nodes in the same order).
-struct Trav {
-    TRay wr;      // world space (also the ray the light quads are tested with)
-    TRay lr;      // space of the BVH level being traversed
-    WtRay wt;     // watertight constants of lr
-    float ltmax;  // tmax in the current level
-    float tmax;   // closest hit so far
-    uint32_t ins; // instance of the current level
-    int top;      // stack depth; 0 when the traversal is done
-};
-
-template <int ISECT>
-NB_D void trav_begin(Trav& T, uint32_t root, const float3& o, const float3& d, float tmax, const SmemStack& st) {
-    tray_setup(T.wr, o, d);
-    T.lr = T.wr;
-    if (ISECT == NOOR_ISECT_WATERTIGHT) wt_setup(T.wt, T.lr.d);
-    T.ltmax = tmax;
-    T.tmax = tmax;
-    T.ins = 0;
-    st.base[0] = root;
-    T.top = 1;
-}
-
-// pops one node; ANY: stop at the first hit (returns true), else returns
-// true when the step recorded a closer hit in rec.  On stack overflow sets
-// *status and ends the traversal with what was found so far.
-template <int ISECT, bool ANY>
-NB_D bool trav_step(Trav& T, const DevScene& S, HitRec& rec, const SmemStack& st, uint32_t* status) {
-    --T.top;
-    const uint32_t ni = st.base[T.top * st.stride];
-    const DevNode* nd = S.nodes + ni;
-    const uint4 lo = __ldg(&nd->lo);
-    const uint4 hi = __ldg(&nd->hi);
-    if (hi.w & NOOR_MESH_NODE_MASK) {
-        T.lr = T.wr;
-        T.ltmax = T.tmax;
-        if (ISECT == NOOR_ISECT_WATERTIGHT) wt_setup(T.wt, T.lr.d);
-    }
-    if (!slab_hit(T.lr, lo, hi, T.ltmax)) return false;
-    if (hi.w & NOOR_LIGHT_NODE_MASK) {
-        const uint32_t li = hi.w & NOOR_LIGHT_MASK;
-        float tm = T.tmax;
-        if ((int)li < S.num_area_lights && quad_hit(S.area_lights[li], T.wr.o, T.wr.d, tm)) {
-            if (ANY) {
-                T.top = 0;
-                return true;
-            }
-            T.tmax = tm;
-            rec.ins = li;
-            rec.mtype = NOOR_MESHLIGHT | NOOR_EMITTER;
-            return true;
-        }
-        return false;
-    }
-    if (hi.w & NOOR_MESH_INSTANCE_MASK) {
-        T.ins = hi.w & NOOR_TRANS_MASK;
-        tray_to_object(T.lr, T.wr, S.xforms + T.ins);
-        T.ltmax = T.tmax;
-        if (ISECT == NOOR_ISECT_WATERTIGHT) wt_setup(T.wt, T.lr.d);
-        if (T.top >= st.cap) {
-            atomicOr(status, NOOR_DEV_STACK_OVERFLOW);
-            T.top = 0;
-            return false;
-        }
-        st.base[T.top * st.stride] = lo.w;
-        ++T.top;
-        return false;
-    }
-    if (hi.w & NOOR_MESH_LEAF_MASK) {
-        const uint32_t cnt = hi.w & NOOR_COUNT_MASK;
-        if (T.top + (int)cnt > st.cap) {
-            atomicOr(status, NOOR_DEV_STACK_OVERFLOW);
-            T.top = 0;
-            return false;
-        }
-        for (uint32_t i = 1; i <= cnt; ++i) {
-            st.base[T.top * st.stride] = ni + i;
-            ++T.top;
-        }
-        return false;
-    }
-    if (hi.w & NOOR_TRI_LEAF_MASK) {
-        const uint32_t start = lo.w;
-        const uint32_t end = start + (hi.w & NOOR_TRI_COUNT_MASK);
-        bool leaf_hit = false;
-        for (uint32_t ti = start; ti < end; ++ti) {
-            float bu, bv, tm = T.ltmax;
-            uint32_t mt;
-            bool h;
-            if (ISECT == NOOR_ISECT_WATERTIGHT)
-                h = wt_test(T.lr, T.wt, S.wtri + ti, ANY ? tm : T.ltmax, bu, bv, mt);
-            else
-                h = wald_test(T.lr, S.wald + ti, ANY ? tm : T.ltmax, bu, bv, mt);
-            if (h) {
-                if (ANY) {
-                    T.top = 0;
-                    return true;
-                }
-                leaf_hit = true;
-                rec.u = bu;
-                rec.v = bv;
-                rec.tri = ti;
-                rec.mtype = mt;
-            }
-        }
-        if (leaf_hit) {
-            T.tmax = T.ltmax;
-            rec.ins = T.ins;
-        }
-        return leaf_hit;
-    }
-    if (T.top + 2 > st.cap) {
-        atomicOr(status, NOOR_DEV_STACK_OVERFLOW);
-        T.top = 0;
-        return false;
-    }
-    const uint32_t axis = hi.w & NOOR_AXIS_MASK;
-    const bool neg = (T.lr.neg >> axis) & 1u;
-    st.base[T.top * st.stride] = neg ? ni + 1 : lo.w;
-    st.base[(T.top + 1) * st.stride] = neg ? lo.w : ni + 1;
-    T.top += 2;
-    return false;
-}
-
 // Closest hit.  tmax in: ray extent, out: hit distance.  Returns hit flag;
 // on stack overflow sets *status and returns what was found so far.
 template <int ISECT>

@@ -513,7 +513,12 @@ struct WavefrontState {
     size_t frames_cap = 0;
     DevScene* scenes_dev = nullptr;
     size_t scenes_cap = 0;
+    // the instantiated while-loop graph of the last render, reused while the
+    // launch (slot buffers, sizes, parameters) is the same
+    cudaGraphExec_t exec = nullptr;
+    uint64_t graph_key[8] = {};
     ~WavefrontState() {
+        if (exec) cudaGraphExecDestroy(exec);
         for (void* p : bufs) cudaFree(p);
         if (films) cudaFree(films);
         if (frames_dev) cudaFree(frames_dev);
@@ -702,31 +707,50 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
     if (ms_out) cudaEventRecord(C.events[6], s);
     bool done = false;
     if (P.use_graph && !prof) {
-        cudaGraph_t graph = nullptr;
-        cudaGraphExec_t exec = nullptr;
-        e = cudaGraphCreate(&graph, 0);
-        cudaGraphConditionalHandle h;
-        if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault);
-        cudaGraphNode_t node;
-        cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
-        cp.conditional.handle = h;
-        cp.conditional.type = cudaGraphCondTypeWhile;
-        cp.conditional.size = 1;
-        if (e == cudaSuccess) e = cudaGraphAddNode(&node, graph, nullptr, 0, &cp);
-        if (e == cudaSuccess) {
-            W.cond = h;
-            cudaGraph_t body = cp.conditional.phGraph_out[0];
-            e = cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
-            if (e == cudaSuccess) {
-                cudaError_t e2 = wf_iteration(W, L, s, true, nullptr);
-                e = cudaStreamEndCapture(s, &body);
-                if (e == cudaSuccess) e = e2;
-            }
+        // everything the captured launches take as arguments, apart from the
+        // conditional handle (the frames and scenes are read from device
+        // memory at run time)
+        const uint64_t key[8] = {(uint64_t)W.cap | (uint64_t)W.sort << 32, W.total,
+                                 (uint64_t)W.max_iters | (uint64_t)W.nframes << 32,
+                                 (uint64_t)(uint32_t)W.stack_cap | (uint64_t)L.block << 32,
+                                 (uint64_t)L.smem, (uint64_t)L.grid_slots | (uint64_t)L.grid_queue << 32,
+                                 (uint64_t)(uintptr_t)W.frames ^ ((uint64_t)(uintptr_t)W.scenes << 1),
+                                 (uint64_t)(uintptr_t)W.status};
+        if (WS.exec && std::memcmp(key, WS.graph_key, sizeof(key)) != 0) {
+            cudaGraphExecDestroy(WS.exec);
+            WS.exec = nullptr;
         }
-        if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
-        if (e == cudaSuccess) e = cudaGraphLaunch(exec, s);
-        if (exec) cudaGraphExecDestroy(exec);
-        if (graph) cudaGraphDestroy(graph);
+        if (!WS.exec) {
+            cudaGraph_t graph = nullptr;
+            e = cudaGraphCreate(&graph, 0);
+            cudaGraphConditionalHandle h;
+            if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault);
+            cudaGraphNode_t node;
+            cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+            cp.conditional.handle = h;
+            cp.conditional.type = cudaGraphCondTypeWhile;
+            cp.conditional.size = 1;
+            if (e == cudaSuccess) e = cudaGraphAddNode(&node, graph, nullptr, 0, &cp);
+            if (e == cudaSuccess) {
+                W.cond = h;
+                cudaGraph_t body = cp.conditional.phGraph_out[0];
+                e = cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+                if (e == cudaSuccess) {
+                    cudaError_t e2 = wf_iteration(W, L, s, true, nullptr);
+                    e = cudaStreamEndCapture(s, &body);
+                    if (e == cudaSuccess) e = e2;
+                }
+            }
+            if (e == cudaSuccess) e = cudaGraphInstantiate(&WS.exec, graph, 0);
+            if (graph) cudaGraphDestroy(graph);
+            if (e != cudaSuccess) {
+                if (WS.exec) cudaGraphExecDestroy(WS.exec);
+                WS.exec = nullptr;
+                return cuda_fail(e, "wavefront graph");
+            }
+            std::memcpy(WS.graph_key, key, sizeof(key));
+        }
+        e = cudaGraphLaunch(WS.exec, s);
         if (e != cudaSuccess) return cuda_fail(e, "wavefront graph");
         C.launches += (uint64_t)W.max_iters;  // upper bound; refined below
         done = true;
