@@ -192,8 +192,17 @@ struct SmemStack {
     int cap;
 };
 
+// Node kinds that are not inner nodes (an inner node has none of these bits)
+constexpr uint32_t kNodeKindMask =
+    NOOR_LIGHT_NODE_MASK | NOOR_MESH_INSTANCE_MASK | NOOR_MESH_LEAF_MASK | NOOR_TRI_LEAF_MASK;
+constexpr uint32_t kNoNode = 0xFFFFFFFFu;
+
 // Closest hit.  tmax in: ray extent, out: hit distance.  Returns hit flag;
 // on stack overflow sets *status and returns what was found so far.
+// The visit order is that of the reference's stack loop: the node the
+// reference would pop next (the near child of an inner node, the last child
+// of a mesh leaf, the root of an instance) is kept in a register instead of
+// being pushed and popped at once, and inner nodes are dispatched first.
 template <int ISECT>
 NB_D bool trace_closest(const DevScene& S, const float3& o, const float3& d, float& tmax,
                         HitRec& rec, const SmemStack& st, uint32_t* status) {
@@ -206,81 +215,86 @@ NB_D bool trace_closest(const DevScene& S, const float3& o, const float3& d, flo
     uint32_t ins = 0;
     bool hit = false;
     int top = 0;
-    st.base[0] = S.root;
-    top = 1;
-    while (top > 0) {
-        --top;
-        const uint32_t ni = st.base[top * st.stride];
+    uint32_t ni = S.root;
+    for (;;) {
         const DevNode* nd = S.nodes + ni;
         const uint4 lo = __ldg(&nd->lo);
         const uint4 hi = __ldg(&nd->hi);
+        uint32_t next = kNoNode;
         if (hi.w & NOOR_MESH_NODE_MASK) {
             lr = wr;
             ltmax = tmax;
             if (ISECT == NOOR_ISECT_WATERTIGHT) wt_setup(wt, lr.d);
         }
-        if (!slab_hit(lr, lo, hi, ltmax)) continue;
-        if (hi.w & NOOR_LIGHT_NODE_MASK) {
-            const uint32_t li = hi.w & NOOR_LIGHT_MASK;
-            if ((int)li < S.num_area_lights && quad_hit(S.area_lights[li], o, d, tmax)) {
-                hit = true;
-                rec.ins = li;
-                rec.mtype = NOOR_MESHLIGHT | NOOR_EMITTER;
-            }
-            continue;
-        } else if (hi.w & NOOR_MESH_INSTANCE_MASK) {
-            ins = hi.w & NOOR_TRANS_MASK;
-            tray_to_object(lr, wr, S.xforms + ins);
-            ltmax = tmax;
-            if (ISECT == NOOR_ISECT_WATERTIGHT) wt_setup(wt, lr.d);
-            if (top >= st.cap) { atomicOr(status, NOOR_DEV_STACK_OVERFLOW); break; }
-            st.base[top * st.stride] = lo.w;
-            ++top;
-        } else if (hi.w & NOOR_MESH_LEAF_MASK) {
-            const uint32_t cnt = hi.w & NOOR_COUNT_MASK;
-            if (top + (int)cnt > st.cap) { atomicOr(status, NOOR_DEV_STACK_OVERFLOW); break; }
-            for (uint32_t i = 1; i <= cnt; ++i) {
-                st.base[top * st.stride] = ni + i;
+        if (slab_hit(lr, lo, hi, ltmax)) {
+            if (!(hi.w & kNodeKindMask)) {
+                // inner: the near child (by the ray's sign on the split axis) next, the far one pushed
+                if (top + 1 > st.cap) { atomicOr(status, NOOR_DEV_STACK_OVERFLOW); break; }
+                const uint32_t axis = hi.w & NOOR_AXIS_MASK;
+                const bool neg = (lr.neg >> axis) & 1u;
+                st.base[top * st.stride] = neg ? ni + 1 : lo.w;
                 ++top;
-            }
-        } else if (hi.w & NOOR_TRI_LEAF_MASK) {
-            const uint32_t start = lo.w;
-            const uint32_t end = start + (hi.w & NOOR_TRI_COUNT_MASK);
-            bool leaf_hit = false;
-            for (uint32_t ti = start; ti < end; ++ti) {
-                float bu, bv;
-                uint32_t mt;
-                bool h;
-                if (ISECT == NOOR_ISECT_WATERTIGHT)
-                    h = wt_test(lr, wt, S.wtri + ti, ltmax, bu, bv, mt);
-                else
-                    h = wald_test(lr, S.wald + ti, ltmax, bu, bv, mt);
-                if (h) {
-                    leaf_hit = true;
-                    rec.u = bu;
-                    rec.v = bv;
-                    rec.tri = ti;
-                    rec.mtype = mt;
+                next = neg ? lo.w : ni + 1;
+            } else if (hi.w & NOOR_LIGHT_NODE_MASK) {
+                const uint32_t li = hi.w & NOOR_LIGHT_MASK;
+                if ((int)li < S.num_area_lights && quad_hit(S.area_lights[li], o, d, tmax)) {
+                    hit = true;
+                    rec.ins = li;
+                    rec.mtype = NOOR_MESHLIGHT | NOOR_EMITTER;
+                }
+            } else if (hi.w & NOOR_MESH_INSTANCE_MASK) {
+                ins = hi.w & NOOR_TRANS_MASK;
+                tray_to_object(lr, wr, S.xforms + ins);
+                ltmax = tmax;
+                if (ISECT == NOOR_ISECT_WATERTIGHT) wt_setup(wt, lr.d);
+                next = lo.w;
+            } else if (hi.w & NOOR_MESH_LEAF_MASK) {
+                const uint32_t cnt = hi.w & NOOR_COUNT_MASK;
+                if (top + (int)cnt > st.cap + 1) { atomicOr(status, NOOR_DEV_STACK_OVERFLOW); break; }
+                for (uint32_t i = 1; i < cnt; ++i) {
+                    st.base[top * st.stride] = ni + i;
+                    ++top;
+                }
+                if (cnt) next = ni + cnt;
+            } else {
+                const uint32_t start = lo.w;
+                const uint32_t end = start + (hi.w & NOOR_TRI_COUNT_MASK);
+                bool leaf_hit = false;
+                for (uint32_t ti = start; ti < end; ++ti) {
+                    float bu, bv;
+                    uint32_t mt;
+                    bool h;
+                    if (ISECT == NOOR_ISECT_WATERTIGHT)
+                        h = wt_test(lr, wt, S.wtri + ti, ltmax, bu, bv, mt);
+                    else
+                        h = wald_test(lr, S.wald + ti, ltmax, bu, bv, mt);
+                    if (h) {
+                        leaf_hit = true;
+                        rec.u = bu;
+                        rec.v = bv;
+                        rec.tri = ti;
+                        rec.mtype = mt;
+                    }
+                }
+                if (leaf_hit) {
+                    hit = true;
+                    tmax = ltmax;
+                    rec.ins = ins;
                 }
             }
-            if (leaf_hit) {
-                hit = true;
-                tmax = ltmax;
-                rec.ins = ins;
-            }
-        } else {
-            if (top + 2 > st.cap) { atomicOr(status, NOOR_DEV_STACK_OVERFLOW); break; }
-            const uint32_t axis = hi.w & NOOR_AXIS_MASK;
-            const bool neg = (lr.neg >> axis) & 1u;
-            st.base[top * st.stride] = neg ? ni + 1 : lo.w;
-            st.base[(top + 1) * st.stride] = neg ? lo.w : ni + 1;
-            top += 2;
         }
+        if (next == kNoNode) {
+            if (top == 0) break;
+            --top;
+            next = st.base[top * st.stride];
+        }
+        ni = next;
     }
     return hit;
 }
 
-// Any hit within (0, tmax]; light nodes count as occluders.
+// Any hit within (0, tmax]; light nodes count as occluders.  Same visit
+// order and register-held next node as trace_closest.
 template <int ISECT>
 NB_D bool trace_any(const DevScene& S, const float3& o, const float3& d, float tmax,
                     const SmemStack& st, uint32_t* status) {
@@ -291,62 +305,65 @@ NB_D bool trace_any(const DevScene& S, const float3& o, const float3& d, float t
     if (ISECT == NOOR_ISECT_WATERTIGHT) wt_setup(wt, lr.d);
     float ltmax = tmax;
     int top = 0;
-    st.base[0] = S.root;
-    top = 1;
-    while (top > 0) {
-        --top;
-        const uint32_t ni = st.base[top * st.stride];
+    uint32_t ni = S.root;
+    for (;;) {
         const DevNode* nd = S.nodes + ni;
         const uint4 lo = __ldg(&nd->lo);
         const uint4 hi = __ldg(&nd->hi);
+        uint32_t next = kNoNode;
         if (hi.w & NOOR_MESH_NODE_MASK) {
             lr = wr;
             ltmax = tmax;
             if (ISECT == NOOR_ISECT_WATERTIGHT) wt_setup(wt, lr.d);
         }
-        if (!slab_hit(lr, lo, hi, ltmax)) continue;
-        if (hi.w & NOOR_LIGHT_NODE_MASK) {
-            const uint32_t li = hi.w & NOOR_LIGHT_MASK;
-            float tm = tmax;
-            if ((int)li < S.num_area_lights && quad_hit(S.area_lights[li], o, d, tm)) return true;
-        } else if (hi.w & NOOR_MESH_INSTANCE_MASK) {
-            tray_to_object(lr, wr, S.xforms + (hi.w & NOOR_TRANS_MASK));
-            ltmax = tmax;
-            if (ISECT == NOOR_ISECT_WATERTIGHT) wt_setup(wt, lr.d);
-            if (top >= st.cap) { atomicOr(status, NOOR_DEV_STACK_OVERFLOW); return false; }
-            st.base[top * st.stride] = lo.w;
-            ++top;
-        } else if (hi.w & NOOR_MESH_LEAF_MASK) {
-            const uint32_t cnt = hi.w & NOOR_COUNT_MASK;
-            if (top + (int)cnt > st.cap) { atomicOr(status, NOOR_DEV_STACK_OVERFLOW); return false; }
-            for (uint32_t i = 1; i <= cnt; ++i) {
-                st.base[top * st.stride] = ni + i;
+        if (slab_hit(lr, lo, hi, ltmax)) {
+            if (!(hi.w & kNodeKindMask)) {
+                if (top + 1 > st.cap) { atomicOr(status, NOOR_DEV_STACK_OVERFLOW); return false; }
+                const uint32_t axis = hi.w & NOOR_AXIS_MASK;
+                const bool neg = (lr.neg >> axis) & 1u;
+                st.base[top * st.stride] = neg ? ni + 1 : lo.w;
                 ++top;
+                next = neg ? lo.w : ni + 1;
+            } else if (hi.w & NOOR_LIGHT_NODE_MASK) {
+                const uint32_t li = hi.w & NOOR_LIGHT_MASK;
+                float tm = tmax;
+                if ((int)li < S.num_area_lights && quad_hit(S.area_lights[li], o, d, tm)) return true;
+            } else if (hi.w & NOOR_MESH_INSTANCE_MASK) {
+                tray_to_object(lr, wr, S.xforms + (hi.w & NOOR_TRANS_MASK));
+                ltmax = tmax;
+                if (ISECT == NOOR_ISECT_WATERTIGHT) wt_setup(wt, lr.d);
+                next = lo.w;
+            } else if (hi.w & NOOR_MESH_LEAF_MASK) {
+                const uint32_t cnt = hi.w & NOOR_COUNT_MASK;
+                if (top + (int)cnt > st.cap + 1) { atomicOr(status, NOOR_DEV_STACK_OVERFLOW); return false; }
+                for (uint32_t i = 1; i < cnt; ++i) {
+                    st.base[top * st.stride] = ni + i;
+                    ++top;
+                }
+                if (cnt) next = ni + cnt;
+            } else {
+                const uint32_t start = lo.w;
+                const uint32_t end = start + (hi.w & NOOR_TRI_COUNT_MASK);
+                for (uint32_t ti = start; ti < end; ++ti) {
+                    float tm = ltmax, bu, bv;
+                    uint32_t mt;
+                    bool h;
+                    if (ISECT == NOOR_ISECT_WATERTIGHT)
+                        h = wt_test(lr, wt, S.wtri + ti, tm, bu, bv, mt);
+                    else
+                        h = wald_test(lr, S.wald + ti, tm, bu, bv, mt);
+                    if (h) return true;
+                }
             }
-        } else if (hi.w & NOOR_TRI_LEAF_MASK) {
-            const uint32_t start = lo.w;
-            const uint32_t end = start + (hi.w & NOOR_TRI_COUNT_MASK);
-            for (uint32_t ti = start; ti < end; ++ti) {
-                float tm = ltmax, bu, bv;
-                uint32_t mt;
-                bool h;
-                if (ISECT == NOOR_ISECT_WATERTIGHT)
-                    h = wt_test(lr, wt, S.wtri + ti, tm, bu, bv, mt);
-                else
-                    h = wald_test(lr, S.wald + ti, tm, bu, bv, mt);
-                if (h) return true;
-            }
-        } else {
-            if (top + 2 > st.cap) { atomicOr(status, NOOR_DEV_STACK_OVERFLOW); return false; }
-            const uint32_t axis = hi.w & NOOR_AXIS_MASK;
-            const bool neg = (lr.neg >> axis) & 1u;
-            st.base[top * st.stride] = neg ? ni + 1 : lo.w;
-            st.base[(top + 1) * st.stride] = neg ? lo.w : ni + 1;
-            top += 2;
         }
+        if (next == kNoNode) {
+            if (top == 0) break;
+            --top;
+            next = st.base[top * st.stride];
+        }
+        ni = next;
     }
     return false;
 }
-
 
 }  // namespace nb

@@ -69,7 +69,8 @@ enum : int {
     kCntShadow = kKinds,       // [0, kKinds) shade queue lengths, then the shadow queue length
     kCntActive = kKinds + 1,   // slots holding a path after regen (= rays extend traces)
     kCntIter = kKinds + 2,     // iterations run
-    kCntWords = kKinds + 3
+    kCntTake = kKinds + 3,     // shadow queue entries taken by wf_shadow's warps
+    kCntWords = kKinds + 4
 };
 
 // block sizes of the slot sweeps (one block-wide atomic per counter)
@@ -116,6 +117,10 @@ struct WfDev {
 // the same for the shading stage
 #ifndef NB_SHADE_MIN_BLOCKS
 #define NB_SHADE_MIN_BLOCKS 1
+#endif
+// 1: shadow rays taken 32 at a time per warp from a counter; 0: grid-stride
+#ifndef NB_SHADOW_FETCH
+#define NB_SHADOW_FETCH 1
 #endif
 
 NB_D uint32_t fbits(float f) { return __float_as_uint(f); }
@@ -261,11 +266,9 @@ __global__ void __launch_bounds__(kRegenBlock) wf_regen(WfDev W) {
 }
 
 template <int ISECT>
-NB_D void extend_one(const WfDev& W, uint32_t slot, const SmemStack& stk) {
-    const float4 ow = W.o[slot], dw = W.d[slot], bw = W.beta[slot];
-    const uint32_t fi = fbits(ow.w);
-    const WfFrameDev& F = W.frames[fi];
-    const DevScene& S = W.scenes[F.scene];
+NB_D void extend_one(const WfDev& W, const DevScene& S, uint32_t slot, const float4& ow,
+                     const SmemStack& stk) {
+    const float4 dw = W.d[slot], bw = W.beta[slot];
     const float3 o = f3(ow.x, ow.y, ow.z), d = f3(dw.x, dw.y, dw.z);
     const uint32_t bb = fbits(bw.w);
     const uint32_t bounce = bb & 0xFFFFu;
@@ -308,17 +311,36 @@ NB_D void extend_one(const WfDev& W, uint32_t slot, const SmemStack& stk) {
     W.state[slot] = kActive | ((kind + 1u) << kKindShift);  // wf_bin queues it for shading
 }
 
-__global__ void __launch_bounds__(256, NB_TRAV_MIN_BLOCKS) wf_extend(WfDev W) {
+// The traversal kernels are instantiated per intersector and per scene
+// source: with MULTI false every frame of the launch uses the scene passed as
+// the kernel parameter S1 (read from the constant bank); with MULTI true each
+// slot's scene comes from its frame, and ISECT may be kIsectMixed (the
+// intersector read from that scene).
+constexpr int kIsectMixed = -1;
+
+template <int ISECT, bool MULTI>
+NB_D const DevScene& slot_scene(const WfDev& W, const DevScene& S1, uint32_t frame) {
+    if (!MULTI) return S1;
+    return W.scenes[W.frames[frame].scene];
+}
+
+// Extend: closest hit for every active slot (one thread per slot)
+template <int ISECT, bool MULTI>
+__global__ void __launch_bounds__(256, NB_TRAV_MIN_BLOCKS) wf_extend(WfDev W, DevScene S1) {
     extern __shared__ uint32_t smem[];
     const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= W.cap || W.state[slot] != kActive) return;
     SmemStack stk{smem + threadIdx.x, (int)blockDim.x, W.stack_cap};
-    const uint32_t fi = fbits(W.o[slot].w);
-    const DevScene& S = W.scenes[W.frames[fi].scene];
-    if (S.isect == NOOR_ISECT_WATERTIGHT)
-        extend_one<NOOR_ISECT_WATERTIGHT>(W, slot, stk);
-    else
-        extend_one<NOOR_ISECT_REF_WALD>(W, slot, stk);
+    const float4 ow = W.o[slot];
+    const DevScene& S = slot_scene<ISECT, MULTI>(W, S1, fbits(ow.w));
+    if (ISECT == kIsectMixed) {
+        if (S.isect == NOOR_ISECT_WATERTIGHT)
+            extend_one<NOOR_ISECT_WATERTIGHT>(W, S, slot, ow, stk);
+        else
+            extend_one<NOOR_ISECT_REF_WALD>(W, S, slot, ow, stk);
+    } else {
+        extend_one<ISECT == kIsectMixed ? 0 : ISECT>(W, S, slot, ow, stk);
+    }
 }
 
 // Shading queues in slot order: every slot extend left a surface hit goes to
@@ -448,22 +470,40 @@ __global__ void __launch_bounds__(256, NB_SHADE_MIN_BLOCKS) wf_shade(WfDev W, ui
 }
 
 // Any hit for each queued shadow ray; a blocked one cancels its pending
-// contribution.
-__global__ void __launch_bounds__(256, NB_TRAV_MIN_BLOCKS) wf_shadow(WfDev W) {
+// contribution.  Each warp takes the next 32 queue entries when it is done
+// with its last ones, so warps that drew long rays do not hold up the launch
+// with a fixed share of the queue.
+template <int ISECT, bool MULTI>
+__global__ void __launch_bounds__(256, NB_TRAV_MIN_BLOCKS) wf_shadow(WfDev W, DevScene S1) {
     extern __shared__ uint32_t smem[];
     const uint32_t n = W.counters[kCntShadow];
     SmemStack stk{smem + threadIdx.x, (int)blockDim.x, W.stack_cap};
+#if NB_SHADOW_FETCH
+    const uint32_t lane = threadIdx.x & 31;
+    for (;;) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(W.counters + kCntTake, 32u);
+        base = __shfl_sync(0xFFFFFFFFu, base, 0);
+        if (base >= n) break;
+        const uint32_t i = base + lane;
+        if (i >= n) continue;
+#else
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+#endif
         const uint32_t e = W.qshadow[i];
         const uint32_t slot = e >> 1;
         const float4 so = W.sh_o[i], sd = W.sh_d[i];
-        const uint32_t fi = fbits(W.o[slot].w);
-        const DevScene& S = W.scenes[W.frames[fi].scene];
+        const DevScene& S = slot_scene<ISECT, MULTI>(W, S1, MULTI ? fbits(W.o[slot].w) : 0u);
+        const float3 o = f3(so.x, so.y, so.z), d = f3(sd.x, sd.y, sd.z);
         bool occ;
-        if (S.isect == NOOR_ISECT_WATERTIGHT)
-            occ = trace_any<NOOR_ISECT_WATERTIGHT>(S, f3(so.x, so.y, so.z), f3(sd.x, sd.y, sd.z), so.w, stk, W.status);
-        else
-            occ = trace_any<NOOR_ISECT_REF_WALD>(S, f3(so.x, so.y, so.z), f3(sd.x, sd.y, sd.z), so.w, stk, W.status);
+        if (ISECT == kIsectMixed) {
+            if (S.isect == NOOR_ISECT_WATERTIGHT)
+                occ = trace_any<NOOR_ISECT_WATERTIGHT>(S, o, d, so.w, stk, W.status);
+            else
+                occ = trace_any<NOOR_ISECT_REF_WALD>(S, o, d, so.w, stk, W.status);
+        } else {
+            occ = trace_any<ISECT == kIsectMixed ? 0 : ISECT>(S, o, d, so.w, stk, W.status);
+        }
         if (occ) W.pend[e].w = 0.0f;
     }
 }
@@ -484,6 +524,7 @@ __global__ void wf_check(WfDev W, uint32_t* go_out, uint32_t conditional) {
     }
     if (!go) W.rays[2] += *W.work_next < W.total ? *W.work_next : W.total;
     for (int k = 0; k <= kCntActive; ++k) c[k] = 0u;
+    c[kCntTake] = 0u;
     if (conditional)
         cudaGraphSetConditional(W.cond, go ? 1u : 0u);
     else
@@ -516,7 +557,7 @@ struct WavefrontState {
     // the instantiated while-loop graph of the last render, reused while the
     // launch (slot buffers, sizes, parameters) is the same
     cudaGraphExec_t exec = nullptr;
-    uint64_t graph_key[8] = {};
+    uint64_t graph_key[10] = {};
     ~WavefrontState() {
         if (exec) cudaGraphExecDestroy(exec);
         for (void* p : bufs) cudaFree(p);
@@ -564,11 +605,16 @@ static int wf_ensure(Context& C, uint32_t cap) {
     return NOOR_OK;
 }
 
+using WfTravKernel = void (*)(WfDev, DevScene);
+
 struct WfLaunch {
     int block;
     size_t smem;
     uint32_t grid_slots;    // one thread per slot / queue entry
     uint32_t grid_queue;    // grid-stride stages
+    WfTravKernel extend;
+    WfTravKernel shadow;
+    DevScene scene;         // the launch's scene when every frame uses the same one
 };
 
 // one iteration; with `ev` (6 events), records ev[0] before the first stage
@@ -579,13 +625,13 @@ static cudaError_t wf_iteration(const WfDev& W, const WfLaunch& L, cudaStream_t 
     if (ev) cudaEventRecord(ev[0], s);
     wf_regen<<<(W.cap + kRegenBlock - 1) / kRegenBlock, kRegenBlock, 0, s>>>(W);
     if (ev) cudaEventRecord(ev[1], s);
-    wf_extend<<<L.grid_slots, L.block, L.smem, s>>>(W);
+    L.extend<<<L.grid_slots, L.block, L.smem, s>>>(W, L.scene);
     if (ev) cudaEventRecord(ev[2], s);
     wf_bin<<<(W.cap + kBinBlock - 1) / kBinBlock, kBinBlock, 0, s>>>(W);
     const int nk = W.sort ? kKinds : 1;
     for (int k = 0; k < nk; ++k) wf_shade<<<L.grid_queue, 256, 0, s>>>(W, (uint32_t)k);
     if (ev) cudaEventRecord(ev[3], s);
-    wf_shadow<<<L.grid_queue, L.block, L.smem, s>>>(W);
+    L.shadow<<<L.grid_queue, L.block, L.smem, s>>>(W, L.scene);
     if (ev) cudaEventRecord(ev[4], s);
     wf_check<<<1, 1, 0, s>>>(W, go_out, conditional ? 1u : 0u);
     if (ev) cudaEventRecord(ev[5], s);
@@ -700,7 +746,24 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
     L.smem = (size_t)stack_cap * block * 4;
     L.grid_slots = (cap + block - 1) / block;
     L.grid_queue = (uint32_t)std::max(1, C.sm_count) * 16;
-    for (auto k : {wf_extend, wf_shadow}) {
+    const uint32_t scene0 = frames[0].scene_id;
+    bool multi = false, mixed = false;
+    for (uint32_t i = 1; i < n_frames; ++i) {
+        multi |= frames[i].scene_id != scene0;
+        mixed |= C.scenes[frames[i].scene_id]->dev.isect != C.scenes[scene0]->dev.isect;
+    }
+    L.scene = C.scenes[scene0]->dev;
+    if (mixed) {
+        L.extend = wf_extend<kIsectMixed, true>;
+        L.shadow = wf_shadow<kIsectMixed, true>;
+    } else if (L.scene.isect == NOOR_ISECT_WATERTIGHT) {
+        L.extend = multi ? wf_extend<NOOR_ISECT_WATERTIGHT, true> : wf_extend<NOOR_ISECT_WATERTIGHT, false>;
+        L.shadow = multi ? wf_shadow<NOOR_ISECT_WATERTIGHT, true> : wf_shadow<NOOR_ISECT_WATERTIGHT, false>;
+    } else {
+        L.extend = multi ? wf_extend<NOOR_ISECT_REF_WALD, true> : wf_extend<NOOR_ISECT_REF_WALD, false>;
+        L.shadow = multi ? wf_shadow<NOOR_ISECT_REF_WALD, true> : wf_shadow<NOOR_ISECT_REF_WALD, false>;
+    }
+    for (WfTravKernel k : {L.extend, L.shadow}) {
         e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem);
         if (e != cudaSuccess) return cuda_fail(e, "wavefront smem");
     }
@@ -708,14 +771,19 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
     bool done = false;
     if (P.use_graph && !prof) {
         // everything the captured launches take as arguments, apart from the
-        // conditional handle (the frames and scenes are read from device
-        // memory at run time)
-        const uint64_t key[8] = {(uint64_t)W.cap | (uint64_t)W.sort << 32, W.total,
-                                 (uint64_t)W.max_iters | (uint64_t)W.nframes << 32,
-                                 (uint64_t)(uint32_t)W.stack_cap | (uint64_t)L.block << 32,
-                                 (uint64_t)L.smem, (uint64_t)L.grid_slots | (uint64_t)L.grid_queue << 32,
-                                 (uint64_t)(uintptr_t)W.frames ^ ((uint64_t)(uintptr_t)W.scenes << 1),
-                                 (uint64_t)(uintptr_t)W.status};
+        // conditional handle (the frame descriptions and the scene table are
+        // read from device memory at run time; the single-scene kernels take
+        // the scene by value, hashed here)
+        uint64_t scene_hash = 1469598103934665603ull;  // FNV-1a over the scene parameter's bytes
+        for (size_t b = 0; b < sizeof(DevScene); ++b)
+            scene_hash = (scene_hash ^ reinterpret_cast<const unsigned char*>(&L.scene)[b]) * 1099511628211ull;
+        const uint64_t key[10] = {(uint64_t)W.cap | (uint64_t)W.sort << 32, W.total,
+                                  (uint64_t)W.max_iters | (uint64_t)W.nframes << 32,
+                                  (uint64_t)(uint32_t)W.stack_cap | (uint64_t)L.block << 32,
+                                  (uint64_t)L.smem, (uint64_t)L.grid_slots | (uint64_t)L.grid_queue << 32,
+                                  (uint64_t)(uintptr_t)W.frames ^ ((uint64_t)(uintptr_t)W.scenes << 1),
+                                  (uint64_t)(uintptr_t)W.status, (uint64_t)(uintptr_t)L.extend ^ (uint64_t)(uintptr_t)L.shadow << 1,
+                                  scene_hash};
         if (WS.exec && std::memcmp(key, WS.graph_key, sizeof(key)) != 0) {
             cudaGraphExecDestroy(WS.exec);
             WS.exec = nullptr;
