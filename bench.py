@@ -31,6 +31,14 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 WORKLOAD = "sky-lit 32 icospheres (2,621,440 tris), 1920x1080, 64 spp, depth 8, Hosek sky T=3 elev 30deg"
+# the single-frame workloads: scene generator, full-size image, description
+SCENES = {
+    "sky": ("sky_scene", (1920, 1080), WORKLOAD),
+    "room": ("room_scene", (256, 256), "closed room, 36 tris (5 walls, ceiling light quad, 2 boxes), 256x256, "
+                                       "16 spp, depth 5"),
+    "env": ("env_scene", (1920, 1080), "32 icospheres (2,621,440 tris) lit by a 2048x1024 log-normal + 3 lobes "
+                                       "env map, MIS, FP64 CDF, 1920x1080, 128 spp, depth 8"),
+}
 METRIC = "Mpaths/s"
 
 
@@ -43,8 +51,8 @@ def parse():
     ap.add_argument("--integrator", default="wavefront", choices=["megakernel", "wavefront"])
     ap.add_argument("--no-compare", action="store_true",
                     help="skip timing the other integrator on the same scene and samples")
-    ap.add_argument("--spp", type=int, default=64)
-    ap.add_argument("--scale", type=float, default=1.0, help="image size scale (1 = 1920x1080)")
+    ap.add_argument("--spp", type=int, default=None, help="samples per pixel (default: the workload's)")
+    ap.add_argument("--scale", type=float, default=1.0, help="image size scale (1 = the workload's full size)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="wavefront: fixed launch parameters")
@@ -52,10 +60,11 @@ def parse():
     ap.add_argument("--wf-slots", type=int, default=1 << 21)
     ap.add_argument("--wf-sort", type=int, default=0)
     ap.add_argument("--wf-graph", type=int, default=1, help="wavefront: 1 CUDA-graph while loop, 0 host loop")
-    ap.add_argument("--workload", default="sky", choices=["sky", "batched", "adjoint"],
-                    help="sky: the headline sky-lit scene; batched: 64 uneven frames in one wavefront launch "
-                         "against 64 sequential megakernel renders; adjoint: forward+backward of the "
-                         "differentiable-rendering configuration")
+    ap.add_argument("--workload", default="sky", choices=["sky", "room", "env", "batched", "adjoint"],
+                    help="sky: the headline sky-lit scene; room: the 36-triangle room; env: the env-map MIS "
+                         "scene; batched: 64 uneven frames in one wavefront launch against 64 sequential "
+                         "megakernel renders; adjoint: forward+backward of the differentiable-rendering "
+                         "configuration")
     return ap.parse_args()
 
 
@@ -119,9 +128,16 @@ class Clocks:
 
 
 def build_scene(args):
+    """the workload's scene at --scale of its image size; fills args.spp
+    with the workload's sample count when not given"""
     from noor_b200 import scenes
-    w, h = int(round(1920 * args.scale)), int(round(1080 * args.scale))
-    s = scenes.sky_scene(width=w, height=h, spp=args.spp, bounces=8)
+    fn, (w0, h0), _ = SCENES[args.workload]
+    w, h = int(round(w0 * args.scale)), int(round(h0 * args.scale))
+    kw = dict(width=w, height=h)
+    if args.spp:
+        kw["spp"] = args.spp
+    s = getattr(scenes, fn)(**kw)
+    args.spp = s.render["spp"]
     t = time.time()
     built = scenes.BuiltPayload(s)
     return s, built, time.time() - t
@@ -215,10 +231,15 @@ def run_reference(args):
         return
     from noor_b200 import scenes, _capi
     from oracle.oracle import Oracle
+    if args.workload not in SCENES:
+        print(json.dumps({"impl": "reference", "unavailable": f"the reference arm times the single-frame "
+                          f"workloads ({', '.join(SCENES)}); the reference has no {args.workload} path"}))
+        return
     s, built, _ = build_scene(args)
-    spec = built.default_spec(8, 1)
+    spec = built.default_spec(s.render["bounces"], s.render.get("rr", 1))
+    spec.mis = int(s.render.get("mis", 0))
     cam = scenes.make_camera(s.camera)
-    hosek = reference_hosek(s.hosek)
+    hosek = reference_hosek(s.hosek) if s.hosek is not None else _capi.HosekSky()
     orc = Oracle(built.payload, spec, hosek)
     threads = os.cpu_count() or 1
     n = cam.w * cam.h
@@ -236,7 +257,7 @@ def run_reference(args):
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "sample_per_step": f"{npx} pixels x {args.spp} spp"},
+            "config": {"workload": SCENES[args.workload][2], "sample_per_step": f"{npx} pixels x {args.spp} spp"},
             "cpu_baseline": {"value": v, "unit": METRIC, "cores": threads, "kind": "port",
                              "sample": f"{npx} pixels x {args.spp} spp per step, FP32 transcription of the "
                                        "reference's device routines (the reference has no CPU render path)"},
@@ -329,7 +350,8 @@ class WavefrontPath:
         self.w, self.h = self.r.w, self.r.h
         self.film = torch.zeros((self.h, self.w, 4), dtype=torch.float32, device="cuda")
         self.host_film = torch.zeros((self.h, self.w, 4), dtype=torch.float32).pin_memory()
-        self.frames = (_capi.WfFrame * 1)(scenes.wf_frame(0, s.camera, args.spp, 8, d_film=self.film.data_ptr()))
+        self.frames = (_capi.WfFrame * 1)(scenes.wf_frame(0, s.camera, args.spp, s.render["bounces"],
+                                                          d_film=self.film.data_ptr()))
         self.params = scenes.wf_params(args.wf_block, args.wf_slots, args.wf_sort, args.wf_graph)
         self.tuned_ms = None
 
@@ -660,8 +682,9 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator, random-init sky)",
-                "config": {"workload": WORKLOAD, "integrator": args.integrator, "width": path.w, "height": path.h,
-                           "spp": args.spp, "bounces": 8, "triangles": s.num_triangles,
+                "config": {"workload": SCENES[args.workload][2], "integrator": args.integrator, "width": path.w,
+                           "height": path.h, "spp": args.spp, "bounces": s.render["bounces"],
+                           "triangles": s.num_triangles,
                            "intersector": "watertight", "film": "kahan",
                            "l2": "inputs larger than L2 (scene ~0.5 GB resident)",
                            "parallelism": f"replicas{world}", "bvh_build_s": round(build_s, 2), **path.describe()},
