@@ -669,7 +669,8 @@ def main():
             if top_kernel == "wf_extend":
                 # traversal bytes of the extension rays + the slot state of every ray
                 alg = counts["ext_traversal_bytes_per_path"] * npaths + EXTEND_SLOT_BYTES * ext / args.steps
-                tr = profiled_traffic_per_ray()
+                # the ncu capture is of the sky-lit scene
+                tr = profiled_traffic_per_ray() if args.workload == "sky" else None
                 traffic = tr * ext / args.steps / top_launches if tr else None
             else:
                 alg = per_path * npaths

@@ -354,6 +354,7 @@ def batched_workload(seed: int = 4, n_frames: int = 64, sides=(128, 256, 512, 10
                 ctr = c1[0]
                 cam = dict(eye=tuple(float(x) for x in ctr + np.array([0.0, 1.0, 3.0])),
                            look_at=tuple(float(x) for x in ctr), up=(0.0, 1.0, 0.0), fov_deg=50.0)
+            cam = dict(cam, w=side, h=side)  # the first frame's size (frames set their own)
             if light == "sky":
                 sd = SceneData(**g, skydome_type=capi.NOOR_SKY_PHYSICAL, camera=cam,
                                render=dict(spp=spp, bounces=bounces, rr=1, mis=0),
