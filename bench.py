@@ -500,7 +500,10 @@ def run_adjoint(args):
     import torch
     from noor_b200 import scenes, _capi
     from noor_b200.adjoint import render, scene_parameters
-    s = scenes.adjoint_scene()
+    kw = dict(width=int(round(512 * args.scale)), height=int(round(512 * args.scale)))
+    if args.spp:
+        kw["spp"] = args.spp
+    s = scenes.adjoint_scene(**kw)
     r = scenes.Renderer(s)
     W, H, spp = s.camera["w"], s.camera["h"], s.render["spp"]
     alb, rough, env = scene_parameters(s)
@@ -544,14 +547,20 @@ def run_adjoint(args):
     _capi.call("noor_launch_count", C.byref(l1))
     ms = total * 1000
     npaths = W * H * spp
+    # the plain megakernel rendering the same image at the loaded parameters
+    for _ in range(2):
+        r.frame = C.c_uint(1)
+        r.render(spp)
+    mk_ms = device_timed(lambda: (setattr(r, "frame", C.c_uint(1)), r.render(spp)), max(1, args.steps))
     line = {"metric": "ms per forward+backward iteration", "value": ms, "unit": "ms", "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator)",
-            "config": {"workload": "differentiable rendering: 10 subdivision-5 icospheres (204,800 tris), 64 "
-                                   "materials, 512x256 env map, 512x512, 16 spp, depth 4, L2 loss",
+            "config": {"workload": f"differentiable rendering: 10 subdivision-5 icospheres (204,800 tris), 64 "
+                                   f"materials, 512x256 env map, {W}x{H}, {spp} spp, depth 4, L2 loss",
                        "params": int(sum(p.numel() for p in params))},
             "forward_ms": 1000 * statistics.mean(fwd), "backward_ms": 1000 * statistics.mean(bwd),
             "forward_mpaths_per_s": npaths / statistics.mean(fwd) / 1e6,
+            "megakernel_render_ms": mk_ms, "megakernel_mpaths_per_s": npaths / (mk_ms / 1000) / 1e6,
             "backward_mpaths_per_s": npaths / statistics.mean(bwd) / 1e6,
             "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 4},
             "gpu_launches": int(l1.value - l0.value), "clocks": clk.summary(),

@@ -293,10 +293,10 @@ NB_D void term_grad(const PathCtx& C, const Term& t, const float3& beta, const f
     }
 }
 
-// One replay of a path.  mode 0: return its radiance.  mode 1: push
-// dl (dLoss/dL) through the path, with Ltot its radiance from mode 0.
-template <int ISECT>
-NB_D float3 replay(const PathCtx& C, uint32_t pix, uint32_t frame, const DevCamera& cam, int mode, const float3& dl,
+// One replay of a path.  MODE 0: return its radiance.  MODE 1: push
+// dl (dLoss/dL) through the path, with Ltot its radiance from MODE 0.
+template <int ISECT, int MODE>
+NB_D float3 replay(const PathCtx& C, uint32_t pix, uint32_t frame, const DevCamera& cam, const float3& dl,
                    float3 Ltot, float* sm_alb, float* sm_rough) {
     const DevScene& S = C.S;
     Rng rng{tea16(pix, frame)};
@@ -321,7 +321,7 @@ NB_D float3 replay(const PathCtx& C, uint32_t pix, uint32_t frame, const DevCame
                     Le = env_eval(S, dir);
                 }
                 L += beta * Le;
-                if (mode == 1 && env) {
+                if (MODE == 1 && env) {
                     const float3 ge = dl * beta;
                     for (int k = 0; k < 4; ++k) {
                         if (bl.w[k] == 0.0f) continue;
@@ -356,7 +356,7 @@ NB_D float3 replay(const PathCtx& C, uint32_t pix, uint32_t frame, const DevCame
         for (int k = 0; k < nt; ++k) Ld += term_value(T[k]);
         const float3 contrib = beta * Ld;
         L += contrib;
-        if (mode == 1) {
+        if (MODE == 1) {
             for (int k = 0; k < nt; ++k) term_grad(C, T[k], beta, dl, I.mat, I.lobe, sm_alb, sm_rough);
             Lrem = Lrem - contrib;
         }
@@ -375,7 +375,7 @@ NB_D float3 replay(const PathCtx& C, uint32_t pix, uint32_t frame, const DevCame
             fd = lobe_value(I.lobe, me, I.F, I.wo, wi);
             fe = fd.f;
         }
-        if (mode == 1 && !(stype & BSDF_SPECULAR)) {
+        if (MODE == 1 && !(stype & BSDF_SPECULAR)) {
             // Lrem scales with f at this vertex
             const float3 g = dl * Lrem;
             if (I.lobe == kLobeLambert || I.lobe == kLobeConductor) {
@@ -401,8 +401,10 @@ NB_D float3 replay(const PathCtx& C, uint32_t pix, uint32_t frame, const DevCame
 constexpr int kAdjBlock = 128;
 constexpr int kAdjMaxMats = 256;
 
-template <int ISECT>
-__global__ void __launch_bounds__(kAdjBlock) adj_kernel(DevScene S, DevCamera cam, AdjParams P, int mode) {
+// MODE 0: forward (image); MODE 1: backward (gradients).  Separate kernels,
+// so that the forward carries none of the gradient code.
+template <int ISECT, int MODE>
+__global__ void __launch_bounds__(kAdjBlock) adj_kernel(DevScene S, DevCamera cam, AdjParams P) {
     extern __shared__ uint32_t smem[];
     __shared__ float sm_alb[3 * kAdjMaxMats];
     __shared__ float sm_rough[kAdjMaxMats];
@@ -414,10 +416,10 @@ __global__ void __launch_bounds__(kAdjBlock) adj_kernel(DevScene S, DevCamera ca
     if (pix < npix) {
         SmemStack st{smem + threadIdx.x, (int)blockDim.x, S.stack_cap};
         const PathCtx ctx{S, P, st, P.status};
-        if (mode == 0) {
+        if (MODE == 0) {
             float3 sum = f3(0.0f), comp = f3(0.0f);
             for (uint32_t s = 0; s < P.spp; ++s) {
-                const float3 L = replay<ISECT>(ctx, pix, P.frame0 + s, cam, 0, f3(0.0f), f3(0.0f), nullptr, nullptr);
+                const float3 L = replay<ISECT, 0>(ctx, pix, P.frame0 + s, cam, f3(0.0f), f3(0.0f), nullptr, nullptr);
                 const float3 Lc = clamp3(L, 0.0f, 100.0f);
                 const float3 y = Lc - comp;
                 const float3 t = sum + y;
@@ -432,16 +434,16 @@ __global__ void __launch_bounds__(kAdjBlock) adj_kernel(DevScene S, DevCamera ca
             const float3 gi = f3(P.grad_img[3 * pix], P.grad_img[3 * pix + 1], P.grad_img[3 * pix + 2]) *
                               (1.0f / (float)P.spp);
             for (uint32_t s = 0; s < P.spp; ++s) {
-                const float3 L = replay<ISECT>(ctx, pix, P.frame0 + s, cam, 0, f3(0.0f), f3(0.0f), nullptr, nullptr);
+                const float3 L = replay<ISECT, 0>(ctx, pix, P.frame0 + s, cam, f3(0.0f), f3(0.0f), nullptr, nullptr);
                 // derivative of the final clamp to [0, 100]
                 const float3 dl = f3(L.x > 0.0f && L.x < 100.0f ? gi.x : 0.0f, L.y > 0.0f && L.y < 100.0f ? gi.y : 0.0f,
                                      L.z > 0.0f && L.z < 100.0f ? gi.z : 0.0f);
                 if (is_black(dl)) continue;
-                replay<ISECT>(ctx, pix, P.frame0 + s, cam, 1, dl, L, sm_alb, sm_rough);
+                replay<ISECT, 1>(ctx, pix, P.frame0 + s, cam, dl, L, sm_alb, sm_rough);
             }
         }
     }
-    if (mode == 1) {
+    if (MODE == 1) {
         __syncthreads();
         const uint32_t nm = min(P.num_mats, (uint32_t)kAdjMaxMats);
         for (uint32_t i = threadIdx.x; i < 3 * nm; i += blockDim.x)
@@ -486,14 +488,12 @@ static int adjoint_run(const noor_adjoint_desc* desc, int mode, float* image, co
     const uint32_t npix = C->cam.w * C->cam.h;
     const size_t sm = (size_t)S.stack_cap * kAdjBlock * 4;
     const uint32_t grid = (npix + kAdjBlock - 1) / kAdjBlock;
-    cudaError_t e;
-    if (S.isect == NOOR_ISECT_WATERTIGHT) {
-        e = cudaFuncSetAttribute(adj_kernel<NOOR_ISECT_WATERTIGHT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        if (e == cudaSuccess) adj_kernel<NOOR_ISECT_WATERTIGHT><<<grid, kAdjBlock, sm, C->stream>>>(S, C->cam, P, mode);
-    } else {
-        e = cudaFuncSetAttribute(adj_kernel<NOOR_ISECT_REF_WALD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        if (e == cudaSuccess) adj_kernel<NOOR_ISECT_REF_WALD><<<grid, kAdjBlock, sm, C->stream>>>(S, C->cam, P, mode);
-    }
+    using AdjKernel = void (*)(DevScene, DevCamera, AdjParams);
+    const bool wt = S.isect == NOOR_ISECT_WATERTIGHT;
+    const AdjKernel k = mode == 0 ? (wt ? adj_kernel<NOOR_ISECT_WATERTIGHT, 0> : adj_kernel<NOOR_ISECT_REF_WALD, 0>)
+                                  : (wt ? adj_kernel<NOOR_ISECT_WATERTIGHT, 1> : adj_kernel<NOOR_ISECT_REF_WALD, 1>);
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e == cudaSuccess) k<<<grid, kAdjBlock, sm, C->stream>>>(S, C->cam, P);
     if (e == cudaSuccess) e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "adjoint");
     C->launches++;
