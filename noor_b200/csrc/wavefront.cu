@@ -107,16 +107,20 @@ struct WfDev {
     cudaGraphConditionalHandle cond;
 };
 
-// minimum resident 256-thread blocks per SM the traversal stages (extend,
-// shadow) are compiled for: 4 caps their registers at 64, i.e. 32 warps per
-// SM instead of 24 at their natural ~80 (measured faster on the sky-lit
-// 2.6M-triangle scene)
-#ifndef NB_TRAV_MIN_BLOCKS
-#define NB_TRAV_MIN_BLOCKS 4
+// Launch bounds of the traversal stages (extend, shadow): at most 128
+// threads per block and 9 such blocks per SM cap their registers at 56
+// (36 warps per SM at 64-thread blocks instead of 32 at their natural 64-80;
+// measured faster on the sky-lit 2.6M-triangle scene than 64 or 48)
+#ifndef NB_TRAV_THREADS
+#define NB_TRAV_THREADS 128
 #endif
-// the same for the shading stage
+#ifndef NB_TRAV_MIN_BLOCKS
+#define NB_TRAV_MIN_BLOCKS 9
+#endif
+// minimum resident 256-thread blocks per SM of the shading stage: 3 caps
+// its registers at 85 (24 warps per SM instead of 16 at its natural 128)
 #ifndef NB_SHADE_MIN_BLOCKS
-#define NB_SHADE_MIN_BLOCKS 1
+#define NB_SHADE_MIN_BLOCKS 3
 #endif
 // 1: shadow rays taken 32 at a time per warp from a counter; 0: grid-stride
 #ifndef NB_SHADOW_FETCH
@@ -326,7 +330,7 @@ NB_D const DevScene& slot_scene(const WfDev& W, const DevScene& S1, uint32_t fra
 
 // Extend: closest hit for every active slot (one thread per slot)
 template <int ISECT, bool MULTI>
-__global__ void __launch_bounds__(256, NB_TRAV_MIN_BLOCKS) wf_extend(WfDev W, DevScene S1) {
+__global__ void __launch_bounds__(NB_TRAV_THREADS, NB_TRAV_MIN_BLOCKS) wf_extend(WfDev W, DevScene S1) {
     extern __shared__ uint32_t smem[];
     const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= W.cap || W.state[slot] != kActive) return;
@@ -474,7 +478,7 @@ __global__ void __launch_bounds__(256, NB_SHADE_MIN_BLOCKS) wf_shade(WfDev W, ui
 // with its last ones, so warps that drew long rays do not hold up the launch
 // with a fixed share of the queue.
 template <int ISECT, bool MULTI>
-__global__ void __launch_bounds__(256, NB_TRAV_MIN_BLOCKS) wf_shadow(WfDev W, DevScene S1) {
+__global__ void __launch_bounds__(NB_TRAV_THREADS, NB_TRAV_MIN_BLOCKS) wf_shadow(WfDev W, DevScene S1) {
     extern __shared__ uint32_t smem[];
     const uint32_t n = W.counters[kCntShadow];
     SmemStack stk{smem + threadIdx.x, (int)blockDim.x, W.stack_cap};
@@ -643,8 +647,10 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
                      float* ms_out, noor_wf_profile* prof = nullptr) {
     if (!frames || n_frames == 0) return set_error(NOOR_ERR_INVALID, "wavefront: no frames");
     const uint32_t block = P.block_size ? P.block_size : 128;
-    if (block != 64 && block != 128 && block != 256)
-        return set_error(NOOR_ERR_INVALID, "wavefront: block_size must be 64, 128 or 256");
+    if (block != 32 && block != 64 && block != 128 && block != 256)
+        return set_error(NOOR_ERR_INVALID, "wavefront: block_size must be 32, 64, 128 or 256");
+    if ((int)block > NB_TRAV_THREADS)
+        return set_error(NOOR_ERR_INVALID, "wavefront: block_size above the traversal kernels' launch bound");
     const uint32_t cap = P.queue_capacity ? P.queue_capacity : (1u << 20);
     if (cap < 1024 || cap > (1u << 26)) return set_error(NOOR_ERR_INVALID, "wavefront: queue capacity out of range");
     int rc = wf_ensure(C, cap);
@@ -926,7 +932,7 @@ extern "C" int noor_wavefront_autotune(const noor_wf_frame* frames, uint32_t n_f
     int rc = need_ctx(C);
     if (rc) return rc;
     if (!best) return set_error(NOOR_ERR_INVALID, "autotune: best is null");
-    const uint32_t blocks[] = {64, 128, 256};
+    const uint32_t blocks[] = {32, 64, 128};
     const uint32_t caps[] = {1u << 21, 1u << 22, 1u << 23};
     const uint32_t sorts[] = {0, 1};
     float bms = 3.4e38f;
