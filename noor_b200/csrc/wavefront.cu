@@ -11,8 +11,9 @@
 //           finished paths to their frame's film; refill free slots with
 //           camera rays of the next (frame, sample, pixel) work items, one
 //           8x4 pixel tile per warp
-//   extend  closest hit for every active slot; misses and emitters finish
-//           the path, surface hits are marked with their material kind
+//   extend  closest hit for every active slot; misses (their sky term added
+//           by the next regen) and emitters finish the path, surface hits
+//           are marked with their material kind
 //   bin     shading queues per material kind, in slot order
 //   shade   one launch per kind: light sample (+ MIS BSDF sample) with the
 //           occlusion test deferred to a shadow-ray queue, then scatter,
@@ -61,8 +62,10 @@ struct WfFrameDev {
 
 // slot state: bits 0-1 kFree / kActive / kFinishing; kPend while the direct
 // lighting of the last shade step waits for regen to fold it into L; bits
-// 3-4 the shading queue (1 + material kind) extend assigned to a surface hit
-enum : uint32_t { kFree = 0, kActive = 1, kFinishing = 2, kLifeMask = 3, kPend = 4, kKindShift = 3 };
+// 3-4 the shading queue (1 + material kind) extend assigned to a surface hit;
+// kSkySeen on a finishing slot whose last ray escaped to a sky it counts
+// (regen adds beta * sky radiance, evaluated there with converged lanes)
+enum : uint32_t { kFree = 0, kActive = 1, kFinishing = 2, kLifeMask = 3, kPend = 4, kKindShift = 3, kSkySeen = 32 };
 
 // counter words
 enum : int {
@@ -144,14 +147,18 @@ NB_D uint32_t queue_push(uint32_t* counter) {
     return base + __popc(peers & ((1u << lane) - 1u));
 }
 
-// compensated atomic add: TwoSum of (old, v) recovers the rounding error of
-// the atomic add exactly; it goes to the compensation buffer
-NB_D void film_add(float* sum, float* comp, float v) {
-    const float old = atomicAdd(sum, v);
+NB_D float two_sum_err(float old, float v) {
     const float s = old + v;
     const float bp = s - old;
-    const float err = (old - (s - bp)) + (v - bp);
-    if (err != 0.0f) atomicAdd(comp, err);
+    return (old - (s - bp)) + (v - bp);
+}
+// compensated atomic add of an rgb value to a float4 pixel: one vector
+// atomic returns the old sum, TwoSum of (old, v) recovers each channel's
+// rounding error exactly, and the errors go to the compensation pixel
+NB_D void film_add3(float4* sum, float4* comp, const float3& v) {
+    const float4 old = atomicAdd(sum, make_float4(v.x, v.y, v.z, 0.0f));
+    const float4 err = make_float4(two_sum_err(old.x, v.x), two_sum_err(old.y, v.y), two_sum_err(old.z, v.z), 0.0f);
+    if (err.x != 0.0f || err.y != 0.0f || err.z != 0.0f) atomicAdd(comp, err);
 }
 
 NB_D int frame_of(const WfDev& W, unsigned long long k) {
@@ -188,7 +195,9 @@ NB_D uint32_t tile_pixel(uint32_t q, uint32_t w, uint32_t h) {
 }
 
 // Regen (every slot): fold the last shade step's direct lighting into L; add
-// finished paths to their frame's film; refill free slots with the camera
+// the sky term of paths whose last ray escaped, and add finished paths to
+// their frame's film (one float4 atomic per path, TwoSum-compensated);
+// refill free slots with the camera
 // rays of the next work items.  The block takes its work items with one
 // atomic, in lane order (consecutive lanes: consecutive pixels of one 8x4
 // tile), and adds its active slots to the active count with one atomic.
@@ -221,12 +230,14 @@ __global__ void __launch_bounds__(kRegenBlock) wf_regen(WfDev W) {
             const uint32_t fi = fbits(W.o[slot].w);
             const uint32_t pix = fbits(W.d[slot].w);
             const WfFrameDev& F = W.frames[fi];
-            const float3 c = clamp3(f3(Lw.x, Lw.y, Lw.z), 0.0f, 100.0f);
-            float* s = reinterpret_cast<float*>(F.sum + pix);
-            float* cp = reinterpret_cast<float*>(F.comp + pix);
-            film_add(s + 0, cp + 0, c.x);
-            film_add(s + 1, cp + 1, c.y);
-            film_add(s + 2, cp + 2, c.z);
+            if (st & kSkySeen) {
+                const float4 bw = W.beta[slot], dw = W.d[slot];
+                const float3 c = f3(bw.x, bw.y, bw.z) * env_eval(W.scenes[F.scene], normalize_fast(f3(dw.x, dw.y, dw.z)));
+                Lw.x += c.x;
+                Lw.y += c.y;
+                Lw.z += c.z;
+            }
+            film_add3(F.sum + pix, F.comp + pix, clamp3(f3(Lw.x, Lw.y, Lw.z), 0.0f, 100.0f));
             st = kFree;
         }
         st &= kLifeMask;
@@ -282,12 +293,9 @@ NB_D void extend_one(const WfDev& W, const DevScene& S, uint32_t slot, const flo
     const bool hit = trace_closest<ISECT>(S, o, d, tmax, rec, stk, W.status);
     const float3 beta = f3(bw.x, bw.y, bw.z);
     if (!hit) {
-        if (S.sky_on && (bounce == 0 || spec)) {
-            float4 Lw = W.L[slot];
-            const float3 c = beta * env_eval(S, normalize_fast(d));
-            W.L[slot] = make_float4(Lw.x + c.x, Lw.y + c.y, Lw.z + c.z, Lw.w);
-        }
-        W.state[slot] = kFinishing;
+        // the sky term is added by regen (converged lanes), after the
+        // direct light regen folded before this extension, as the megakernel
+        W.state[slot] = kFinishing | (S.sky_on && (bounce == 0 || spec) ? kSkySeen : 0u);
         return;
     }
     if (rec.mtype & kEmitterMat) {
