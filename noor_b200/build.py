@@ -30,7 +30,7 @@ NVCC_FLAGS = [
     "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
     "-Xptxas", "-warn-spills",
 ]
-CXX_FLAGS = ["-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-fvisibility=hidden", "-Wall"]
+CXX_FLAGS = ["-std=c++17", "-O2", "-fPIC", "-pthread", "-ffp-contract=off", "-fvisibility=hidden", "-Wall"]
 
 
 def _nvcc() -> str:

@@ -20,6 +20,9 @@
 //   * vertex de-duplication on (vertex, normal, uv) index triples in
 //     BVH triangle order, Wald precomputation per triangle.
 #include <algorithm>
+#include <atomic>
+#include <exception>
+#include <thread>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -178,6 +181,50 @@ struct AttrKeyHash {
     }
 };
 
+// find-or-insert table of (vertex, normal, uv) index triples, linear probing
+struct AttrTable {
+    std::vector<AttrKey> keys;
+    std::vector<uint32_t> vals;
+    size_t mask;
+    explicit AttrTable(size_t n) {
+        size_t cap = 16;
+        while (cap < 2 * n) cap <<= 1;
+        keys.resize(cap);
+        vals.assign(cap, 0xFFFFFFFFu);
+        mask = cap - 1;
+    }
+    uint32_t find_or_add(const AttrKey& k, uint32_t v, bool& added) {
+        for (size_t i = AttrKeyHash()(k) & mask;; i = (i + 1) & mask) {
+            if (vals[i] == 0xFFFFFFFFu) {
+                keys[i] = k;
+                vals[i] = v;
+                added = true;
+                return v;
+            }
+            if (keys[i] == k) {
+                added = false;
+                return vals[i];
+            }
+        }
+    }
+};
+
+// f(i) for i in [0, n) on all host threads (contiguous chunks)
+template <class F>
+static void parallel_for(uint32_t n, const F& f) {
+    const uint32_t nt = std::max(1u, std::min(std::thread::hardware_concurrency(), (n + 65535u) / 65536u));
+    std::vector<std::thread> pool;
+    const uint32_t chunk = (n + nt - 1) / nt;
+    for (uint32_t t = 0; t < nt; ++t) {
+        const uint32_t b = t * chunk, e = std::min(n, b + chunk);
+        if (b >= e) break;
+        pool.emplace_back([&f, b, e]() {
+            for (uint32_t i = b; i < e; ++i) f(i);
+        });
+    }
+    for (auto& th : pool) th.join();
+}
+
 struct Range {
     uint32_t* b;
     uint32_t* e;
@@ -200,6 +247,31 @@ struct MeshInfo {
     const noor_mesh* src;
 };
 
+// Per-tree state of a build: split scratch, the nodes of the tree, and its
+// statistics.  Each mesh's tree is built in its own Work (on its own host
+// thread); node indices written into a tree are relative to `base`.
+struct Work {
+    uint32_t nb = 0;
+    std::vector<Box> edge;  // slab edges: edge[i].lo/.hi = lower/upper edge
+    std::vector<Box> L[3], R[3], LC[3], RC[3];
+    std::vector<uint32_t> NL[3], NR[3];
+    std::vector<uint32_t> nodes;  // 8 words per node: min.xyz,w0,max.xyz,w1
+    uint32_t base = 0;            // index of nodes[0] in the final node array
+    noor_build_stat stat{};
+    void init(uint32_t bins) {
+        nb = bins;
+        edge.assign(nb, Box());
+        for (int a = 0; a < 3; ++a) {
+            L[a].assign(nb, Box());
+            R[a].assign(nb, Box());
+            LC[a].assign(nb, Box());
+            RC[a].assign(nb, Box());
+            NL[a].assign(nb, 0u);
+            NR[a].assign(nb, 0u);
+        }
+    }
+};
+
 class Builder {
 public:
     Builder(const noor_scene_desc& d) : D(d) {}
@@ -209,15 +281,9 @@ public:
     std::vector<MeshInfo> meshes;
     Box scene_box, scene_cbox;
     std::vector<uint32_t> tri_order, mesh_order, mesh_start;
-    std::vector<uint32_t> nodes;  // 8 words per node: min.xyz,w0,max.xyz,w1
+    std::vector<uint32_t> nodes;  // the final node array: mesh trees in mesh order, then the top tree
     uint32_t root = 0;
     noor_build_stat stat{};
-
-    // per-split scratch (one axis-major set, reused at every node)
-    uint32_t nb = 0;
-    std::vector<Box> edge;  // slab edges: edge[i].lo/.hi = lower/upper edge
-    std::vector<Box> L[3], R[3], LC[3], RC[3];
-    std::vector<uint32_t> NL[3], NR[3];
 
     V3 vtx(uint32_t t, int k) const {
         const float* p = D.vertices + 4 * (size_t)D.vindices[3 * (size_t)t + k];
@@ -275,37 +341,38 @@ public:
 
     const Box& item_box(BinKind k, uint32_t i) const { return k == kTriBin ? tri_box[i] : meshes[i].ibox; }
 
-    void reset_split(const Range& r) {
+    void reset_split(Work& w, const Range& r) const {
+        const uint32_t nb = w.nb;
         const V3 cl = r.cbox.lo, ch = r.cbox.hi;
         const float inv = 1.0f / (float)nb;
         const V3 dt = vscale(vsub(ch, cl), inv);
-        edge[0].lo = cl;
-        edge[0].hi = vadd(cl, dt);
+        w.edge[0].lo = cl;
+        w.edge[0].hi = vadd(cl, dt);
         for (uint32_t i = 1; i < nb; ++i) {
-            edge[i].lo = vadd(edge[i - 1].lo, dt);
-            edge[i].hi = vadd(edge[i - 1].hi, dt);
+            w.edge[i].lo = vadd(w.edge[i - 1].lo, dt);
+            w.edge[i].hi = vadd(w.edge[i - 1].hi, dt);
         }
-        edge[nb - 1].hi = ch;
+        w.edge[nb - 1].hi = ch;
         for (int a = 0; a < 3; ++a) {
-            std::fill(L[a].begin(), L[a].end(), Box());
-            std::fill(R[a].begin(), R[a].end(), Box());
-            std::fill(LC[a].begin(), LC[a].end(), Box());
-            std::fill(RC[a].begin(), RC[a].end(), Box());
-            std::fill(NL[a].begin(), NL[a].end(), 0u);
-            std::fill(NR[a].begin(), NR[a].end(), 0u);
+            std::fill(w.L[a].begin(), w.L[a].end(), Box());
+            std::fill(w.R[a].begin(), w.R[a].end(), Box());
+            std::fill(w.LC[a].begin(), w.LC[a].end(), Box());
+            std::fill(w.RC[a].begin(), w.RC[a].end(), Box());
+            std::fill(w.NL[a].begin(), w.NL[a].end(), 0u);
+            std::fill(w.NR[a].begin(), w.NR[a].end(), 0u);
         }
     }
 
     // first bin whose upper edge is >= c; the last bin for c above the last
     // lower edge.  Edges are non-decreasing, so this is a lower-bound search.
-    uint32_t bin_of(float c, int a) const {
-        const uint32_t last = nb - 1;
-        if (c <= edge[0].hi[a]) return 0;
-        if (c > edge[last].lo[a]) return last;
+    static uint32_t bin_of(const Work& w, float c, int a) {
+        const uint32_t last = w.nb - 1;
+        if (c <= w.edge[0].hi[a]) return 0;
+        if (c > w.edge[last].lo[a]) return last;
         uint32_t lo = 1, hi = last - 1;
         while (lo < hi) {
             const uint32_t mid = (lo + hi) >> 1;
-            if (c <= edge[mid].hi[a])
+            if (c <= w.edge[mid].hi[a])
                 hi = mid;
             else
                 lo = mid + 1;
@@ -313,36 +380,42 @@ public:
         return lo;
     }
 
-    Plane best_on_axis(const Range& r, int a) {
+    Plane best_on_axis(Work& w, const Range& r, int a) const {
+        auto& L = w.L[a];
+        auto& R = w.R[a];
+        auto& LC = w.LC[a];
+        auto& RC = w.RC[a];
+        auto& NL = w.NL[a];
+        auto& NR = w.NR[a];
         for (uint32_t* it = r.b; it != r.e; ++it) {
             const Box& bb = item_box(r.kind, *it);
             const V3 c = bb.centroid();
-            const uint32_t k = bin_of(c[a], a);
-            L[a][k].merge(bb);
-            LC[a][k].include(c);
-            ++NL[a][k];
+            const uint32_t k = bin_of(w, c[a], a);
+            L[k].merge(bb);
+            LC[k].include(c);
+            ++NL[k];
         }
-        const uint32_t n = nb - 1;
-        R[a][n] = L[a][n];
-        RC[a][n] = LC[a][n];
-        NR[a][n] = NL[a][n];
+        const uint32_t n = w.nb - 1;
+        R[n] = L[n];
+        RC[n] = LC[n];
+        NR[n] = NL[n];
         for (uint32_t i = n - 1; i > 0; --i) {
-            R[a][i] = merged(L[a][i], R[a][i + 1]);
-            RC[a][i] = merged(LC[a][i], RC[a][i + 1]);
-            NR[a][i] = NL[a][i] + NR[a][i + 1];
+            R[i] = merged(L[i], R[i + 1]);
+            RC[i] = merged(LC[i], RC[i + 1]);
+            NR[i] = NL[i] + NR[i + 1];
         }
         for (uint32_t i = 1; i < n; ++i) {
-            L[a][i].merge(L[a][i - 1]);
-            LC[a][i].merge(LC[a][i - 1]);
-            NL[a][i] += NL[a][i - 1];
+            L[i].merge(L[i - 1]);
+            LC[i].merge(LC[i - 1]);
+            NL[i] += NL[i - 1];
         }
         Plane best;
         const float parent = r.box.area();
         for (uint32_t i = 0; i < n; ++i) {
-            const uint32_t nl = NL[a][i], nr = NR[a][i + 1];
+            const uint32_t nl = NL[i], nr = NR[i + 1];
             if (nl == 0 || nr == 0) continue;
-            const float lc = (float)nl * L[a][i].area();
-            const float rc = (float)nr * R[a][i + 1].area();
+            const float lc = (float)nl * L[i].area();
+            const float rc = (float)nr * R[i + 1].area();
             const float cost = D.bvh.Ct + D.bvh.Ci * (lc + rc) / parent;
             if (cost < best.cost) {
                 best.cost = cost;
@@ -355,112 +428,143 @@ public:
         return best;
     }
 
-    Plane best_split(const Range& r) {
-        reset_split(r);
+    Plane best_split(Work& w, const Range& r) const {
+        reset_split(w, r);
         Plane best;
         for (int a = 0; a < 3; ++a) {
-            const Plane p = best_on_axis(r, a);
+            const Plane p = best_on_axis(w, r, a);
             if (p.valid() && p.cost < best.cost) best = p;
         }
         return best;
     }
 
-    uint32_t push_node(const Box& b, uint32_t w0, uint32_t w1) {
-        nodes.push_back(f2u(b.lo.x));
-        nodes.push_back(f2u(b.lo.y));
-        nodes.push_back(f2u(b.lo.z));
-        nodes.push_back(w0);
-        nodes.push_back(f2u(b.hi.x));
-        nodes.push_back(f2u(b.hi.y));
-        nodes.push_back(f2u(b.hi.z));
-        nodes.push_back(w1);
-        return (uint32_t)(nodes.size() / 8 - 1);
+    static uint32_t push_node(Work& w, const Box& b, uint32_t w0, uint32_t w1) {
+        const uint32_t v[8] = {f2u(b.lo.x), f2u(b.lo.y), f2u(b.lo.z), w0, f2u(b.hi.x), f2u(b.hi.y), f2u(b.hi.z), w1};
+        w.nodes.insert(w.nodes.end(), v, v + 8);
+        return num_nodes(w) - 1;
     }
+    static uint32_t num_nodes(const Work& w) { return w.base + (uint32_t)(w.nodes.size() / 8); }
     uint32_t num_nodes() const { return (uint32_t)(nodes.size() / 8); }
 
     // BVH::makeLeaf (bvh.cpp:88-153)
-    uint32_t make_leaf(const Range& r, uint32_t level) {
+    uint32_t make_leaf(Work& w, const Range& r, uint32_t level) {
         const uint32_t cnt = r.count();
-        const uint32_t start = r.kind == kTriBin ? (uint32_t)(r.b - tri_order.data()) : num_nodes() + 1;
+        const uint32_t start = r.kind == kTriBin ? (uint32_t)(r.b - tri_order.data()) : num_nodes(w) + 1;
         const uint32_t w1 = (r.kind == kTriBin ? NOOR_TRI_LEAF_MASK : NOOR_MESH_LEAF_MASK) | cnt;
-        const uint32_t id = push_node(r.box, start, w1);
+        const uint32_t id = push_node(w, r.box, start, w1);
         if (r.kind == kMeshBin) {
             uint32_t pos = (uint32_t)(r.b - mesh_order.data());
             for (uint32_t* it = r.b; it != r.e; ++it, ++pos) {
                 const MeshInfo& m = meshes[*it];
-                uint32_t w = NOOR_MESH_INSTANCE_MASK | pos;
-                if (m.src->light_idx >= 0) w = NOOR_LIGHT_NODE_MASK | (uint32_t)m.src->light_idx;
-                push_node(m.ibox, mesh_start[*it], w);
+                uint32_t ww = NOOR_MESH_INSTANCE_MASK | pos;
+                if (m.src->light_idx >= 0) ww = NOOR_LIGHT_NODE_MASK | (uint32_t)m.src->light_idx;
+                push_node(w, m.ibox, mesh_start[*it], ww);
             }
         }
-        if (stat.height < level) stat.height = level;
+        if (w.stat.height < level) w.stat.height = level;
         if (r.kind == kTriBin) {
-            ++stat.num_leaf_nodes;
-            stat.max_leaf_tris = std::max(stat.max_leaf_tris, cnt);
+            ++w.stat.num_leaf_nodes;
+            w.stat.max_leaf_tris = std::max(w.stat.max_leaf_tris, cnt);
         }
         return id;
     }
 
     // BVH::recursiveBuild (bvh.cpp:180-214)
-    uint32_t build(const Range& r, uint32_t level) {
+    uint32_t build(Work& w, const Range& r, uint32_t level) {
         const uint32_t cnt = r.count();
         if (r.kind == kTriBin) {
-            if (level >= D.bvh.max_height || cnt <= D.bvh.min_leaf_tris) return make_leaf(r, level);
+            if (level >= D.bvh.max_height || cnt <= D.bvh.min_leaf_tris) return make_leaf(w, r, level);
         } else if (cnt < 2) {
-            return make_leaf(r, level);
+            return make_leaf(w, r, level);
         }
-        const Plane p = best_split(r);
+        const Plane p = best_split(w, r);
         const float leaf_cost = D.bvh.Ci * (float)cnt;
         if (r.kind == kTriBin) {
-            if (!p.valid() || (leaf_cost < p.cost && cnt <= D.bvh.max_leaf_tris)) return make_leaf(r, level);
+            if (!p.valid() || (leaf_cost < p.cost && cnt <= D.bvh.max_leaf_tris)) return make_leaf(w, r, level);
         } else if (!p.valid()) {
-            return make_leaf(r, level);
+            return make_leaf(w, r, level);
         }
         const int a = (int)p.axis;
-        const float plane_hi = edge[p.index].hi[a];
+        const float plane_hi = w.edge[p.index].hi[a];
         const BinKind k = r.kind;
         uint32_t* mid = std::partition(r.b, r.e, [&](uint32_t i) { return item_box(k, i).centroid()[a] <= plane_hi; });
-        Range left{r.b, mid, L[a][p.index], LC[a][p.index], k};
-        Range right{mid, r.e, R[a][p.index + 1], RC[a][p.index + 1], k};
-        const uint32_t id = push_node(r.box, 0u, (k == kTriBin ? 0u : NOOR_MESH_INNER_MASK) | p.axis);
-        ++stat.num_inner_nodes;
-        build(left, level + 1);
-        const uint32_t rid = build(right, level + 1);
-        nodes[8 * (size_t)id + 3] = rid;
+        Range left{r.b, mid, w.L[a][p.index], w.LC[a][p.index], k};
+        Range right{mid, r.e, w.R[a][p.index + 1], w.RC[a][p.index + 1], k};
+        const uint32_t id = push_node(w, r.box, 0u, (k == kTriBin ? 0u : NOOR_MESH_INNER_MASK) | p.axis);
+        ++w.stat.num_inner_nodes;
+        build(w, left, level + 1);
+        const uint32_t rid = build(w, right, level + 1);
+        w.nodes[8 * (size_t)(id - w.base) + 3] = rid;
         return id;
     }
 
-    // BVH::build (bvh.cpp:216-258)
+    // BVH::build (bvh.cpp:216-258).  The mesh trees are independent (each
+    // partitions its own slice of the triangle order and numbers its nodes
+    // from 0), so they are built on all host threads; appended in mesh order
+    // with their inner nodes' right-child indices moved by the tree's offset,
+    // they are the same bytes as the reference's one-after-another build.
     void build_all() {
-        nb = D.bvh.num_bins;
-        edge.assign(nb, Box());
-        for (int a = 0; a < 3; ++a) {
-            L[a].assign(nb, Box());
-            R[a].assign(nb, Box());
-            LC[a].assign(nb, Box());
-            RC[a].assign(nb, Box());
-            NL[a].assign(nb, 0u);
-            NR[a].assign(nb, 0u);
-        }
         tri_order.resize(D.num_triangles);
         for (uint32_t i = 0; i < D.num_triangles; ++i) tri_order[i] = i;
         mesh_order.resize(D.num_meshes);
         for (uint32_t i = 0; i < D.num_meshes; ++i) mesh_order[i] = i;
         mesh_start.assign(D.num_meshes, 0u);
-        nodes.reserve(8 * (size_t)2 * (D.num_triangles + D.num_meshes));
-        for (uint32_t i = 0; i < D.num_meshes; ++i) {
-            const noor_mesh& m = D.meshes[i];
-            if (m.instance >= 0 || m.light_idx >= 0) continue;
-            mesh_start[i] = num_nodes();
-            Range r{tri_order.data() + m.tri_start, tri_order.data() + m.tri_start + m.tri_count, meshes[i].box,
-                    meshes[i].cbox, kTriBin};
-            build(r, 0);
+        std::vector<uint32_t> src;
+        for (uint32_t i = 0; i < D.num_meshes; ++i)
+            if (D.meshes[i].instance < 0 && D.meshes[i].light_idx < 0) src.push_back(i);
+        std::vector<Work> trees(src.size());
+        std::atomic<size_t> next{0};
+        std::vector<std::exception_ptr> errs(src.size());
+        auto worker = [&]() {
+            for (size_t j; (j = next.fetch_add(1)) < src.size();) {
+                try {
+                    const uint32_t i = src[j];
+                    const noor_mesh& m = D.meshes[i];
+                    Work& w = trees[j];
+                    w.init(D.bvh.num_bins);
+                    w.nodes.reserve(8 * (size_t)2 * m.tri_count);
+                    Range r{tri_order.data() + m.tri_start, tri_order.data() + m.tri_start + m.tri_count,
+                            meshes[i].box, meshes[i].cbox, kTriBin};
+                    build(w, r, 0);
+                } catch (...) {
+                    errs[j] = std::current_exception();
+                }
+            }
+        };
+        const size_t nthreads = std::min<size_t>(src.size(), std::max(1u, std::thread::hardware_concurrency()));
+        std::vector<std::thread> pool;
+        for (size_t t = 1; t < nthreads; ++t) pool.emplace_back(worker);
+        worker();
+        for (auto& t : pool) t.join();
+        for (auto& e : errs)
+            if (e) std::rethrow_exception(e);
+        size_t total = 0;
+        for (const Work& w : trees) total += w.nodes.size();
+        nodes.reserve(total + 8 * (size_t)2 * (D.num_meshes + 1));
+        for (size_t j = 0; j < src.size(); ++j) {
+            Work& w = trees[j];
+            const uint32_t off = num_nodes();
+            mesh_start[src[j]] = off;
+            for (size_t n = 0; n < w.nodes.size(); n += 8)
+                if (!(w.nodes[n + 7] & NOOR_TRI_LEAF_MASK)) w.nodes[n + 3] += off;  // inner: right child
+            nodes.insert(nodes.end(), w.nodes.begin(), w.nodes.end());
+            stat.height = std::max(stat.height, w.stat.height);
+            stat.num_inner_nodes += w.stat.num_inner_nodes;
+            stat.num_leaf_nodes += w.stat.num_leaf_nodes;
+            stat.max_leaf_tris = std::max(stat.max_leaf_tris, w.stat.max_leaf_tris);
+            std::vector<uint32_t>().swap(w.nodes);
         }
         for (uint32_t i = 0; i < D.num_meshes; ++i)
             if (D.meshes[i].instance >= 0) mesh_start[i] = mesh_start[D.meshes[i].instance];
         root = num_nodes();
-        Range top{mesh_order.data(), mesh_order.data() + D.num_meshes, scene_box, scene_cbox, kMeshBin};
-        build(top, stat.height);
+        Work top;
+        top.init(D.bvh.num_bins);
+        top.base = root;
+        top.stat = stat;
+        Range r{mesh_order.data(), mesh_order.data() + D.num_meshes, scene_box, scene_cbox, kMeshBin};
+        build(top, r, stat.height);
+        nodes.insert(nodes.end(), top.nodes.begin(), top.nodes.end());
+        stat = top.stat;
         stat.height += 1;
     }
 };
@@ -666,8 +770,9 @@ extern "C" int noor_build_payload(const noor_scene_desc* d, noor_payload_handle*
         // vertex de-duplication in BVH order (Model::loadCudaPayload, model.cpp:376-401):
         // the first occurrence of a (vertex, normal, uv) index triple appends a
         // vertex; later occurrences reuse its index
-        std::unordered_map<AttrKey, uint32_t, AttrKeyHash> seen;
-        seen.reserve(3 * (size_t)d->num_triangles);
+        // (an open-addressing table: the same first-occurrence numbering as a
+        // map, without a node allocation per key)
+        AttrTable seen(3 * (size_t)d->num_triangles);
         std::vector<uint32_t> element(3 * (size_t)d->num_triangles);
         uint32_t nv = 0;
         for (uint32_t i = 0; i < d->num_triangles; ++i) {
@@ -675,8 +780,9 @@ extern "C" int noor_build_payload(const noor_scene_desc* d, noor_payload_handle*
             for (int j = 0; j < 3; ++j) {
                 const AttrKey key{d->vindices[3 * (size_t)t + j], d->nindices[3 * (size_t)t + j],
                                   d->uvindices[3 * (size_t)t + j]};
-                auto ins = seen.emplace(key, nv);
-                if (ins.second) {
+                bool added;
+                const uint32_t id = seen.find_or_add(key, nv, added);
+                if (added) {
                     h->vertices.insert(h->vertices.end(), d->vertices + 4 * (size_t)key.v,
                                        d->vertices + 4 * (size_t)key.v + 4);
                     h->normals.insert(h->normals.end(), d->normals + 4 * (size_t)key.n,
@@ -684,13 +790,14 @@ extern "C" int noor_build_payload(const noor_scene_desc* d, noor_payload_handle*
                     h->uvs.insert(h->uvs.end(), d->uvs + 2 * (size_t)key.u, d->uvs + 2 * (size_t)key.u + 2);
                     ++nv;
                 }
-                element[3 * (size_t)i + j] = ins.first->second;
+                element[3 * (size_t)i + j] = id;
             }
         }
         // Wald triangles + attribute indices (Model::buildWaldTriangles, model.cpp:333-360)
         for (int k = 0; k < 3; ++k) h->wald[k].resize(4 * (size_t)d->num_triangles);
         h->attr.resize(4 * (size_t)d->num_triangles);
-        for (uint32_t i = 0; i < d->num_triangles; ++i) {
+        // independent per triangle: split over the host threads
+        parallel_for(d->num_triangles, [&](uint32_t i) {
             V3 p[3];
             for (int j = 0; j < 3; ++j) {
                 const float* q = h->vertices.data() + 4 * (size_t)element[3 * (size_t)i + j];
@@ -707,7 +814,7 @@ extern "C" int noor_build_payload(const noor_scene_desc* d, noor_payload_handle*
             a[1] = element[3 * (size_t)i + 1];
             a[2] = element[3 * (size_t)i + 2];
             a[3] = mi;
-        }
+        });
         if (stat) {
             *stat = B.stat;
             stat->scene_min[0] = B.scene_box.lo.x;
