@@ -15,6 +15,7 @@
 //   L_remaining is the radiance the path collects after the vertex.
 // Russian roulette must be off (rr >= bounces): its decision depends on
 // the throughput and would make the estimator discontinuous.
+#include <algorithm>
 #include <cstring>
 
 #include "host_common.h"
@@ -400,11 +401,64 @@ NB_D float3 replay(const PathCtx& C, uint32_t pix, uint32_t frame, const DevCame
 
 constexpr int kAdjBlock = 128;
 constexpr int kAdjMaxMats = 256;
+// samples per pass: the per-sample radiance of a chunk (npix x kAdjChunk
+// float4) is the only buffer that grows with the sample count
+constexpr uint32_t kAdjChunk = 4;
 
-// MODE 0: forward (image); MODE 1: backward (gradients).  Separate kernels,
-// so that the forward carries none of the gradient code.
-template <int ISECT, int MODE>
-__global__ void __launch_bounds__(kAdjBlock) adj_kernel(DevScene S, DevCamera cam, AdjParams P) {
+// Work items of a chunk: item i = (sample c0 + i / npix, pixel i % npix), so
+// the lanes of a warp trace neighbouring pixels of one sample.
+
+// Radiance of every path of a chunk (the MODE 0 replay), unclamped
+template <int ISECT>
+__global__ void __launch_bounds__(kAdjBlock) adj_radiance(DevScene S, DevCamera cam, AdjParams P, uint32_t c0,
+                                                          uint32_t nc, float4* Lbuf) {
+    extern __shared__ uint32_t smem[];
+    const uint32_t npix = cam.w * cam.h;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= npix * nc) return;
+    const uint32_t pix = i % npix, s = c0 + i / npix;
+    SmemStack st{smem + threadIdx.x, (int)blockDim.x, S.stack_cap};
+    const PathCtx ctx{S, P, st, P.status};
+    const float3 L = replay<ISECT, 0>(ctx, pix, P.frame0 + s, cam, f3(0.0f), f3(0.0f), nullptr, nullptr);
+    Lbuf[i] = make_float4(L.x, L.y, L.z, 0.0f);
+}
+
+// Forward: each pixel's clamped samples added in sample order with Kahan's
+// compensation (the state carried across chunks); the last chunk writes the
+// mean
+__global__ void adj_accumulate(uint32_t npix, uint32_t nc, const float4* Lbuf, float4* kahan, int first, int last,
+                               float inv_spp, float* image) {
+    const uint32_t pix = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pix >= npix) return;
+    float3 sum = f3(0.0f), comp = f3(0.0f);
+    if (!first) {
+        sum = f3(kahan[2 * pix]);
+        comp = f3(kahan[2 * pix + 1]);
+    }
+    for (uint32_t c = 0; c < nc; ++c) {
+        const float3 Lc = clamp3(f3(Lbuf[(size_t)c * npix + pix]), 0.0f, 100.0f);
+        const float3 y = Lc - comp;
+        const float3 t = sum + y;
+        comp = (t - sum) - y;
+        sum = t;
+    }
+    if (last) {
+        image[3 * pix + 0] = sum.x * inv_spp;
+        image[3 * pix + 1] = sum.y * inv_spp;
+        image[3 * pix + 2] = sum.z * inv_spp;
+    } else {
+        kahan[2 * pix] = make_float4(sum.x, sum.y, sum.z, 0.0f);
+        kahan[2 * pix + 1] = make_float4(comp.x, comp.y, comp.z, 0.0f);
+    }
+}
+
+// Backward: for every path of a chunk, dLoss/dL through the final clamp,
+// then the MODE 1 replay pushes it to the parameters.  Resident blocks loop
+// over the items, so each block adds its material gradients (accumulated in
+// shared memory) to the global ones once.
+template <int ISECT>
+__global__ void __launch_bounds__(kAdjBlock) adj_gradient(DevScene S, DevCamera cam, AdjParams P, uint32_t c0,
+                                                          uint32_t nc, const float4* Lbuf) {
     extern __shared__ uint32_t smem[];
     __shared__ float sm_alb[3 * kAdjMaxMats];
     __shared__ float sm_rough[kAdjMaxMats];
@@ -412,45 +466,25 @@ __global__ void __launch_bounds__(kAdjBlock) adj_kernel(DevScene S, DevCamera ca
     for (int i = threadIdx.x; i < kAdjMaxMats; i += blockDim.x) sm_rough[i] = 0.0f;
     __syncthreads();
     const uint32_t npix = cam.w * cam.h;
-    const uint32_t pix = blockIdx.x * blockDim.x + threadIdx.x;
-    if (pix < npix) {
-        SmemStack st{smem + threadIdx.x, (int)blockDim.x, S.stack_cap};
-        const PathCtx ctx{S, P, st, P.status};
-        if (MODE == 0) {
-            float3 sum = f3(0.0f), comp = f3(0.0f);
-            for (uint32_t s = 0; s < P.spp; ++s) {
-                const float3 L = replay<ISECT, 0>(ctx, pix, P.frame0 + s, cam, f3(0.0f), f3(0.0f), nullptr, nullptr);
-                const float3 Lc = clamp3(L, 0.0f, 100.0f);
-                const float3 y = Lc - comp;
-                const float3 t = sum + y;
-                comp = (t - sum) - y;
-                sum = t;
-            }
-            const float inv = 1.0f / (float)P.spp;
-            P.image[3 * pix + 0] = sum.x * inv;
-            P.image[3 * pix + 1] = sum.y * inv;
-            P.image[3 * pix + 2] = sum.z * inv;
-        } else {
-            const float3 gi = f3(P.grad_img[3 * pix], P.grad_img[3 * pix + 1], P.grad_img[3 * pix + 2]) *
-                              (1.0f / (float)P.spp);
-            for (uint32_t s = 0; s < P.spp; ++s) {
-                const float3 L = replay<ISECT, 0>(ctx, pix, P.frame0 + s, cam, f3(0.0f), f3(0.0f), nullptr, nullptr);
-                // derivative of the final clamp to [0, 100]
-                const float3 dl = f3(L.x > 0.0f && L.x < 100.0f ? gi.x : 0.0f, L.y > 0.0f && L.y < 100.0f ? gi.y : 0.0f,
-                                     L.z > 0.0f && L.z < 100.0f ? gi.z : 0.0f);
-                if (is_black(dl)) continue;
-                replay<ISECT, 1>(ctx, pix, P.frame0 + s, cam, dl, L, sm_alb, sm_rough);
-            }
-        }
+    SmemStack st{smem + threadIdx.x, (int)blockDim.x, S.stack_cap};
+    const PathCtx ctx{S, P, st, P.status};
+    const float inv_spp = 1.0f / (float)P.spp;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < npix * nc; i += gridDim.x * blockDim.x) {
+        const uint32_t pix = i % npix, s = c0 + i / npix;
+        const float3 gi = f3(P.grad_img[3 * pix], P.grad_img[3 * pix + 1], P.grad_img[3 * pix + 2]) * inv_spp;
+        const float3 L = f3(Lbuf[i]);
+        // derivative of the final clamp to [0, 100]
+        const float3 dl = f3(L.x > 0.0f && L.x < 100.0f ? gi.x : 0.0f, L.y > 0.0f && L.y < 100.0f ? gi.y : 0.0f,
+                             L.z > 0.0f && L.z < 100.0f ? gi.z : 0.0f);
+        if (is_black(dl)) continue;
+        replay<ISECT, 1>(ctx, pix, P.frame0 + s, cam, dl, L, sm_alb, sm_rough);
     }
-    if (MODE == 1) {
-        __syncthreads();
-        const uint32_t nm = min(P.num_mats, (uint32_t)kAdjMaxMats);
-        for (uint32_t i = threadIdx.x; i < 3 * nm; i += blockDim.x)
-            if (sm_alb[i] != 0.0f) atomicAdd(&P.g_albedo[i], sm_alb[i]);
-        for (uint32_t i = threadIdx.x; i < nm; i += blockDim.x)
-            if (sm_rough[i] != 0.0f) atomicAdd(&P.g_rough[i], sm_rough[i]);
-    }
+    __syncthreads();
+    const uint32_t nm = min(P.num_mats, (uint32_t)kAdjMaxMats);
+    for (uint32_t i = threadIdx.x; i < 3 * nm; i += blockDim.x)
+        if (sm_alb[i] != 0.0f) atomicAdd(&P.g_albedo[i], sm_alb[i]);
+    for (uint32_t i = threadIdx.x; i < nm; i += blockDim.x)
+        if (sm_rough[i] != 0.0f) atomicAdd(&P.g_rough[i], sm_rough[i]);
 }
 
 static int adjoint_run(const noor_adjoint_desc* desc, int mode, float* image, const float* grad_img, float* g_alb,
@@ -459,6 +493,7 @@ static int adjoint_run(const noor_adjoint_desc* desc, int mode, float* image, co
     int rc = need_ctx(C);
     if (rc) return rc;
     if (!desc || !desc->d_albedo || !desc->d_roughness) return set_error(NOOR_ERR_INVALID, "adjoint: null buffer");
+    if (desc->spp == 0) return set_error(NOOR_ERR_INVALID, "adjoint: spp must be positive");
     SceneState& st = *C->scenes[0];
     DevScene S = st.dev;
     if (desc->bounces) S.bounces = desc->bounces;
@@ -487,16 +522,44 @@ static int adjoint_run(const noor_adjoint_desc* desc, int mode, float* image, co
     P.status = C->status;
     const uint32_t npix = C->cam.w * C->cam.h;
     const size_t sm = (size_t)S.stack_cap * kAdjBlock * 4;
-    const uint32_t grid = (npix + kAdjBlock - 1) / kAdjBlock;
-    using AdjKernel = void (*)(DevScene, DevCamera, AdjParams);
+    // buffers: per-sample radiance of one chunk, and (forward) the Kahan
+    // state per pixel across chunks; kept in the context between calls
+    const uint32_t chunk = std::min<uint32_t>(P.spp, kAdjChunk);
+    const size_t need = ((size_t)chunk + 2) * npix * sizeof(float4);
+    cudaError_t e = cudaSuccess;
+    if (C->adj_bytes < need) {
+        if (C->adj_buf) cudaFree(C->adj_buf);
+        C->adj_buf = nullptr;
+        C->adj_bytes = 0;
+        e = cudaMalloc(&C->adj_buf, need);
+        if (e != cudaSuccess) return cuda_fail(e, "adjoint buffers");
+        C->adj_bytes = need;
+    }
+    float4* Lbuf = static_cast<float4*>(C->adj_buf);
+    float4* kahan = Lbuf + (size_t)chunk * npix;
+    using RadKernel = void (*)(DevScene, DevCamera, AdjParams, uint32_t, uint32_t, float4*);
+    using GradKernel = void (*)(DevScene, DevCamera, AdjParams, uint32_t, uint32_t, const float4*);
     const bool wt = S.isect == NOOR_ISECT_WATERTIGHT;
-    const AdjKernel k = mode == 0 ? (wt ? adj_kernel<NOOR_ISECT_WATERTIGHT, 0> : adj_kernel<NOOR_ISECT_REF_WALD, 0>)
-                                  : (wt ? adj_kernel<NOOR_ISECT_WATERTIGHT, 1> : adj_kernel<NOOR_ISECT_REF_WALD, 1>);
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (e == cudaSuccess) k<<<grid, kAdjBlock, sm, C->stream>>>(S, C->cam, P);
-    if (e == cudaSuccess) e = cudaGetLastError();
+    const RadKernel kr = wt ? adj_radiance<NOOR_ISECT_WATERTIGHT> : adj_radiance<NOOR_ISECT_REF_WALD>;
+    const GradKernel kg = wt ? adj_gradient<NOOR_ISECT_WATERTIGHT> : adj_gradient<NOOR_ISECT_REF_WALD>;
+    e = cudaFuncSetAttribute(kr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(kg, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    int per_sm = 1;
+    if (e == cudaSuccess && mode == 1) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kg, kAdjBlock, sm);
+    if (e != cudaSuccess) return cuda_fail(e, "adjoint setup");
+    const uint32_t grid_g = (uint32_t)std::max(1, per_sm) * (uint32_t)std::max(1, C->sm_count);
+    for (uint32_t c0 = 0; c0 < P.spp && e == cudaSuccess; c0 += chunk) {
+        const uint32_t nc = std::min(chunk, P.spp - c0);
+        kr<<<(npix * nc + kAdjBlock - 1) / kAdjBlock, kAdjBlock, sm, C->stream>>>(S, C->cam, P, c0, nc, Lbuf);
+        if (mode == 0)
+            adj_accumulate<<<(npix + 255) / 256, 256, 0, C->stream>>>(npix, nc, Lbuf, kahan, c0 == 0,
+                                                                      c0 + nc >= P.spp, 1.0f / (float)P.spp, image);
+        else
+            kg<<<grid_g, kAdjBlock, sm, C->stream>>>(S, C->cam, P, c0, nc, Lbuf);
+        e = cudaGetLastError();
+        C->launches += 2;
+    }
     if (e != cudaSuccess) return cuda_fail(e, "adjoint");
-    C->launches++;
     return sync_and_check(*C, "adjoint");
 }
 

@@ -59,7 +59,7 @@ Context::~Context() {
     if (stream) cudaStreamSynchronize(stream);
     scenes.clear();
     for (void* p : {(void*)film_sum, (void*)film_comp, (void*)film_out, (void*)part_sum, (void*)part_comp,
-                    (void*)lookat, (void*)status, (void*)counters, (void*)scratch})
+                    (void*)lookat, (void*)status, (void*)counters, (void*)scratch, adj_buf})
         if (p) cudaFree(p);
     for (auto& e : events)
         if (e) cudaEventDestroy(e);

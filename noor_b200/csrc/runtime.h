@@ -46,6 +46,8 @@ struct Context {
     uint32_t* status = nullptr;
     unsigned long long* counters = nullptr;
     void* scratch = nullptr;
+    void* adj_buf = nullptr;  // adjoint: per-sample radiance of one chunk + the forward's Kahan state
+    size_t adj_bytes = 0;
     cudaEvent_t events[8] = {};
     uint64_t launches = 0;
     WavefrontState* wf = nullptr;
