@@ -932,22 +932,27 @@ extern "C" int noor_wavefront_counters(uint64_t counters[3], int reset) {
     return NOOR_OK;
 }
 
-// Autotuner: renders the batch with each candidate (block size x queue
-// capacity x material sort) and keeps the fastest by device time.
+// Autotuner: renders the batch with each candidate (block size x slot count
+// x material sort) and keeps the fastest by device time.
 extern "C" int noor_wavefront_autotune(const noor_wf_frame* frames, uint32_t n_frames, noor_wf_params* best,
                                        float* best_ms) {
     Context* C;
     int rc = need_ctx(C);
     if (rc) return rc;
     if (!best) return set_error(NOOR_ERR_INVALID, "autotune: best is null");
-    const uint32_t blocks[] = {32, 64, 128};
-    const uint32_t caps[] = {1u << 21, 1u << 22, 1u << 23};
+    // slot counts beyond twice the batch's paths only add empty sweeps
+    unsigned long long paths = 0;
+    for (uint32_t i = 0; i < n_frames && frames; ++i)
+        paths += (unsigned long long)frames[i].width * frames[i].height * frames[i].spp;
+    const uint32_t blocks[] = {64, 128};
+    const uint32_t caps[] = {1u << 18, 1u << 20, 1u << 21, 1u << 22, 1u << 23};
     const uint32_t sorts[] = {0, 1};
     float bms = 3.4e38f;
     noor_wf_params bp{128, 1u << 20, 1, best->use_graph};
     for (uint32_t b : blocks)
         for (uint32_t c : caps)
             for (uint32_t so : sorts) {
+                if (c != caps[0] && c > 2 * paths) continue;
                 noor_wf_params p{b, c, so, best->use_graph};
                 float ms = 0.0f;
                 if ((rc = wavefront_render(*C, frames, n_frames, p, &ms))) return rc;
