@@ -25,9 +25,13 @@ NOOR_OK = 0
 ERRORS = {1: "INVALID", 2: "CUDA", 3: "NO_CONTEXT", 4: "UNSUPPORTED", 5: "OOM", 6: "DEVICE", 7: "CAPACITY"}
 
 NOOR_DIFFUSE = 1 << 0
+NOOR_TRANSLUCENT = 1 << 2
+NOOR_GLOSSY = 1 << 3
 NOOR_MIRROR = 1 << 4
 NOOR_GLASS = 1 << 5
+NOOR_ROUGHGLASS = 1 << 6
 NOOR_METAL = 1 << 7
+NOOR_SUBSTRATE = 1 << 8
 NOOR_EMITTER = 1 << 9
 NOOR_MESHLIGHT = 1 << 14
 NOOR_SKY_HDR, NOOR_SKY_PHYSICAL, NOOR_SKY_CONSTANT = 0, 1, 2

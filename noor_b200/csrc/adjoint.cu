@@ -501,6 +501,14 @@ static int adjoint_run(const noor_adjoint_desc* desc, int mode, float* image, co
         return set_error(NOOR_ERR_INVALID, "adjoint: Russian roulette must be off (spec.rr >= bounces)");
     if (st.materials_host.size() > (size_t)kAdjMaxMats)
         return set_error(NOOR_ERR_CAPACITY, "adjoint: at most 256 materials");
+    // the estimator is differentiated for Lambert and conductor lobes; glass
+    // (specular, no parameter) and emitters pass through
+    for (const auto& m : st.materials_host) {
+        const uint32_t l = lobe_of(m.type);
+        if (!(m.type & (NOOR_EMITTER | NOOR_MESHLIGHT)) && l != kLobeLambert && l != kLobeConductor &&
+            l != kLobeFresnelSpec)
+            return set_error(NOOR_ERR_UNSUPPORTED, "adjoint: materials other than diffuse, metal and glass");
+    }
     if (S.sky_type == NOOR_SKY_HDR && (!desc->d_env || (mode == 1 && !g_env)))
         return set_error(NOOR_ERR_INVALID, "adjoint: env buffer missing");
     if (desc->width != C->cam.w || desc->height != C->cam.h)

@@ -13,6 +13,7 @@
 #include "host_common.h"
 #include "kernels.h"
 #include "runtime.h"
+#include "shading.cuh"
 
 // ------------------------------------------------------------------ errors
 static thread_local std::string tl_err;
@@ -121,9 +122,10 @@ static int validate_payload(const noor_payload* P) {
         if (t & (NOOR_ALPHA | NOOR_BUMP))
             return set_error(NOOR_ERR_UNSUPPORTED, "payload: alpha and bump maps are not implemented");
         const uint32_t base = t & ~(uint32_t)NOOR_MESHLIGHT;
-        if (!(base == NOOR_DIFFUSE || base == NOOR_METAL || base == NOOR_GLASS || base == NOOR_EMITTER))
-            return set_error(NOOR_ERR_UNSUPPORTED,
-                             "payload: material type " + std::to_string(t) + " is outside DIFFUSE/METAL/GLASS/EMITTER");
+        if (base != NOOR_EMITTER && lobe_of(base) == 0u)
+            return set_error(NOOR_ERR_UNSUPPORTED, "payload: material type " + std::to_string(t) +
+                                                       " (Oren-Nayar, clear coat, shadow catcher or a mix of "
+                                                       "types) is not implemented");
         if (m.distribution > 1u) return set_error(NOOR_ERR_INVALID, "payload: unknown microfacet distribution");
     }
     for (int i = 0; i < P->num_area_lights; ++i)

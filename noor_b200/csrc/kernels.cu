@@ -205,10 +205,9 @@ __global__ void k_eval_bsdf(DevScene S, int kind, const float* in, float* out, s
     } else if (kind == 1) {
         pdf = bsdf_pdf(lobe, m, F, wo, wi, BSDF_ALL);
     } else {
-        // feed u through an RNG-free path: sample the lobe directly
-        float3 w;
-        const float3 wl = wo;
-        if (lobe != 0u && wl.z != 0.0f) f = lobe_sample(lobe, m, wl, fminf(p[6], kOneMinusEps), p[7], w, pdf, st);
+        // the BSDF's Sample_f with its two uniforms given (no RNG)
+        float3 w = f3(0.0f);
+        f = bsdf_sample_u(lobe, m, F, wo, BSDF_ALL, p[6], p[7], w, pdf, st);
         if (pdf != 0.0f) wo_s = w;
     }
     q[0] = f.x;

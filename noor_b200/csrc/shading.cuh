@@ -407,29 +407,80 @@ enum : uint32_t {
     BSDF_NOOP = 1u << 7,
     BSDF_ALL = 0xFFu
 };
-constexpr uint32_t kLobeLambert = BSDF_REFLECTION | BSDF_DIFFUSE | BSDF_DIELECTRIC;
-constexpr uint32_t kLobeConductor = BSDF_CONDUCTOR | BSDF_REFLECTION | BSDF_GLOSSY;
-constexpr uint32_t kLobeFresnelSpec = BSDF_REFLECTION | BSDF_TRANSMISSION | BSDF_SPECULAR | BSDF_DIELECTRIC;
+// Lobe ids (one per BxDF class the material factory builds,
+// noor/cuda/bxdf.cuh:119-137) and their BxDF type flags.
+enum : uint32_t {
+    kLobeNone = 0,
+    kLobeLambert = 1,       // CudaLambertianReflection (bxdf.cuh:252-299)
+    kLobeConductor = 2,     // CudaMicrofacetReflection, conductor Fresnel (bxdf.cuh:472-557)
+    kLobeFresnelSpec = 3,   // CudaFresnelSpecular (bxdf.cuh:754-839)
+    kLobeLambertT = 4,      // CudaLambertianTransmission (bxdf.cuh:301-352)
+    kLobeMirror = 5,        // CudaSpecularReflection, no-op Fresnel (bxdf.cuh:354-404)
+    kLobeMicroDiel = 6,     // CudaMicrofacetReflection, dielectric Fresnel
+    kLobeMicroT = 7,        // CudaMicrofacetTransmission (bxdf.cuh:559-656)
+    kLobeFresnelBlend = 8,  // CudaFresnelBlend (bxdf.cuh:658-752)
+};
+NB_HD uint32_t lobe_type(uint32_t id) {
+    switch (id) {
+        case kLobeLambert: return BSDF_REFLECTION | BSDF_DIFFUSE | BSDF_DIELECTRIC;
+        case kLobeConductor: return BSDF_CONDUCTOR | BSDF_REFLECTION | BSDF_GLOSSY;
+        case kLobeFresnelSpec: return BSDF_REFLECTION | BSDF_TRANSMISSION | BSDF_SPECULAR | BSDF_DIELECTRIC;
+        case kLobeLambertT: return BSDF_TRANSMISSION | BSDF_DIFFUSE | BSDF_DIELECTRIC;
+        case kLobeMirror: return BSDF_NOOP | BSDF_REFLECTION | BSDF_SPECULAR;
+        case kLobeMicroDiel: return BSDF_DIELECTRIC | BSDF_REFLECTION | BSDF_GLOSSY;
+        case kLobeMicroT: return BSDF_TRANSMISSION | BSDF_GLOSSY | BSDF_DIELECTRIC;
+        case kLobeFresnelBlend: return BSDF_REFLECTION | BSDF_GLOSSY | BSDF_DIELECTRIC;
+        default: return 0u;
+    }
+}
 
 constexpr uint32_t kSpecularMat = NOOR_MIRROR | NOOR_GLASS | NOOR_CLEARCOAT;      // NOOR_SPECULAR
 constexpr uint32_t kTransparentMat = NOOR_TRANSLUCENT | NOOR_GLASS | NOOR_ROUGHGLASS;
 constexpr uint32_t kEmitterMat = NOOR_EMITTER | NOOR_MESHLIGHT;
 
-// the single lobe factoryBSDF builds for a material (noor/cuda/bsdf.cuh:425-461);
-// 0 = none
-NB_D uint32_t lobe_of(uint32_t mtype) {
+// The lobes factoryBSDF builds for a material (noor/cuda/bsdf.cuh:383-461),
+// in the order it adds them: lobe k in bits 8k..8k+7; 0 = none.  Clear-coat
+// and shadow-catcher materials build none here.
+NB_HD uint32_t lobe_of(uint32_t mtype) {
     const uint32_t t = mtype & ~(uint32_t)(NOOR_BUMP | NOOR_ALPHA);
-    if (t == NOOR_DIFFUSE) return kLobeLambert;
-    if (t == NOOR_METAL) return kLobeConductor;
-    if (t == NOOR_GLASS) return kLobeFresnelSpec;
-    return 0u;
+    switch (t) {
+        case NOOR_DIFFUSE: return kLobeLambert;
+        case NOOR_METAL: return kLobeConductor;
+        case NOOR_GLASS: return kLobeFresnelSpec;
+        case NOOR_MIRROR: return kLobeMirror;
+        case NOOR_SUBSTRATE: return kLobeFresnelBlend;
+        case NOOR_TRANSLUCENT: return kLobeLambert | kLobeLambertT << 8;
+        case NOOR_GLOSSY: return kLobeLambert | kLobeMicroDiel << 8;
+        case NOOR_ROUGHGLASS: return kLobeMicroDiel | kLobeMicroT << 8;
+        default: return 0u;
+    }
 }
-NB_D bool lobe_matches(uint32_t lobe, uint32_t flags) { return lobe != 0u && (lobe & flags) == lobe; }
+NB_D uint32_t lobe_at(uint32_t lobes, int k) { return (lobes >> (8 * k)) & 0xFFu; }
+NB_D bool lobe_matches(uint32_t id, uint32_t flags) {
+    const uint32_t t = lobe_type(id);
+    return t != 0u && (t & flags) == t;
+}
 
-// BxDF::Eval of the lobe, local frame
+// Refract (bxdf.cuh:103-116)
+NB_D bool refract_ref(const float3& wi, const float3& n, float eta, float3& wt) {
+    const float cosThetaI = dot(n, wi);
+    const float sin2ThetaI = fmaxf(0.0f, 1.0f - cosThetaI * cosThetaI);
+    const float sin2ThetaT = eta * eta * sin2ThetaI;
+    if (sin2ThetaT >= 1.0f) return false;
+    const float cosThetaT = sqrtf(1.0f - sin2ThetaT);
+    wt = -eta * wi + (eta * cosThetaI - cosThetaT) * n;
+    return true;
+}
+NB_D float pow5(float v) {
+    const float a = v * v;
+    return a * a * v;
+}
+NB_D float3 schlick(const DevMaterial& m, float c) { return m.specular + pow5(1.0f - c) * (f3(1.0f) - m.specular); }
+
+// BxDF::Eval of a lobe, local frame
 NB_D float3 lobe_eval(uint32_t lobe, const DevMaterial& m, const float3& wo, const float3& wi) {
-    if (lobe == kLobeLambert) return m.diffuse * kInvPi;
-    if (lobe == kLobeConductor) {
+    if (lobe == kLobeLambert || lobe == kLobeLambertT) return m.diffuse * kInvPi;
+    if (lobe == kLobeConductor || lobe == kLobeMicroDiel) {
         // CudaMicrofacetReflection::Eval (bxdf.cuh:482-506)
         if (!same_hemi(wo, wi)) return f3(0.0f);
         const float cO = fabsf(wo.z), cI = fabsf(wi.z);
@@ -437,34 +488,81 @@ NB_D float3 lobe_eval(uint32_t lobe, const DevMaterial& m, const float3& wo, con
         float3 wh = normalize_fast(wi + wo);
         if (is_black(wh)) return f3(0.0f);
         wh *= signf_ref(wh.z);
-        const float3 F = fresnel_conductor(dot(wo, wh), m.ior, m.k);
+        const float3 F = lobe == kLobeConductor ? fresnel_conductor(dot(wo, wh), m.ior, m.k)
+                                                : f3(fresnel_dielectric(dot(wo, wh), 1.0f, m.coat_ior));
         const Micro mf = make_micro(m);
         return F * m.specular * mf.D(wh) * mf.G(wo, wi) / (4.0f * cI * cO);
     }
-    return f3(0.0f);  // specular lobe: delta
+    if (lobe == kLobeMicroT) {
+        // CudaMicrofacetTransmission::Eval (bxdf.cuh:567-590); etaI = 1, etaT = coat_ior
+        if (same_hemi(wo, wi)) return f3(0.0f);
+        const float cO = wo.z, cI = wi.z;
+        if (cI == 0.0f || cO == 0.0f) return f3(0.0f);
+        const float eta = wo.z > 0.0f ? m.coat_ior / 1.0f : 1.0f / m.coat_ior;
+        float3 wh = normalize_guard(wo + wi * eta);
+        wh *= signf_ref(wh.z);
+        const float F = fresnel_dielectric(dot(wo, wh), 1.0f, m.coat_ior);
+        const float sd = dot(wo, wh) + eta * dot(wi, wh);
+        const Micro mf = make_micro(m);
+        return (1.0f - F) * m.transmission *
+               fabsf(mf.D(wh) * mf.G(wo, wi) * eta * eta * absdot(wi, wh) * absdot(wo, wh) / (cI * cO * sd * sd));
+    }
+    if (lobe == kLobeFresnelBlend) {
+        // CudaFresnelBlend::Eval (bxdf.cuh:670-688)
+        const float3 diffuse = (28.0f / (23.0f * kPi)) * m.diffuse * (f3(1.0f) - m.specular) *
+                               (1.0f - pow5(1.0f - 0.5f * fabsf(wi.z))) * (1.0f - pow5(1.0f - 0.5f * fabsf(wo.z)));
+        float3 wh = wi + wo;
+        if (wh.x == 0.0f && wh.y == 0.0f && wh.z == 0.0f) return f3(0.0f);
+        wh = normalize_guard(wh);
+        const Micro mf = make_micro(m);
+        const float3 specular =
+            mf.D(wh) / (4.0f * absdot(wi, wh) * fmaxf(fabsf(wi.z), fabsf(wo.z))) * schlick(m, dot(wi, wh));
+        return diffuse + specular;
+    }
+    return f3(0.0f);  // specular lobes: delta
 }
 NB_D float lobe_pdf(uint32_t lobe, const DevMaterial& m, const float3& wo, const float3& wi) {
     if (lobe == kLobeLambert) return same_hemi(wo, wi) ? fabsf(wi.z) * kInvPi : 0.0f;
-    if (lobe == kLobeConductor) {
+    if (lobe == kLobeLambertT) return !same_hemi(wo, wi) ? fabsf(wi.z) * kInvPi : 0.0f;
+    if (lobe == kLobeConductor || lobe == kLobeMicroDiel) {
         if (!same_hemi(wo, wi)) return 0.0f;
         const float3 wh = normalize_guard(wo + wi);
         const Micro mf = make_micro(m);
         return mf.pdf(wo, wh) / (4.0f * dot(wo, wh));
     }
+    if (lobe == kLobeMicroT) {
+        // CudaMicrofacetTransmission::Pdf (bxdf.cuh:592-606)
+        if (same_hemi(wo, wi)) return 0.0f;
+        const float eta = wo.z > 0.0f ? m.coat_ior / 1.0f : 1.0f / m.coat_ior;
+        const float3 wh = normalize_guard(wo + wi * eta);
+        const float sd = dot(wo, wh) + eta * dot(wi, wh);
+        const float dwh_dwi = fabsf((eta * eta * dot(wi, wh)) / (sd * sd));
+        const Micro mf = make_micro(m);
+        return mf.pdf(wo, wh) * dwh_dwi;
+    }
+    if (lobe == kLobeFresnelBlend) {
+        // CudaFresnelBlend::Pdf (bxdf.cuh:690-699)
+        if (!same_hemi(wo, wi)) return 0.0f;
+        const float3 wh = normalize_guard(wo + wi);
+        const Micro mf = make_micro(m);
+        const float pdf_wh = mf.pdf(wo, wh);
+        return 0.5f * (fabsf(wi.z) * kInvPi + pdf_wh / (4.0f * dot(wo, wh)));
+    }
     return 0.0f;
 }
-// BxDF::Sample_f of the lobe; pdf stays 0 on failure
+// BxDF::Sample_f of a lobe (u already remapped by the BSDF); pdf stays 0 on
+// failure; stype = the sampled BxDF type
 NB_D float3 lobe_sample(uint32_t lobe, const DevMaterial& m, const float3& wo, float ux, float uy, float3& wi,
                         float& pdf, uint32_t& stype) {
-    stype = lobe;
-    if (lobe == kLobeLambert) {
-        // CudaLambertianReflection::Sample_f (bxdf.cuh:270-285)
+    stype = lobe_type(lobe);
+    if (lobe == kLobeLambert || lobe == kLobeLambertT) {
+        // CudaLambertianReflection / Transmission::Sample_f (bxdf.cuh:270-285, 321-336)
         wi = cosine_hemisphere(ux, uy);
-        if (wo.z < 0.0f) wi.z *= -1.0f;
-        pdf = same_hemi(wo, wi) ? fabsf(wi.z) * kInvPi : 0.0f;
+        if (lobe == kLobeLambert ? wo.z < 0.0f : wo.z > 0.0f) wi.z *= -1.0f;
+        pdf = lobe_pdf(lobe, m, wo, wi);
         return m.diffuse * kInvPi;
     }
-    if (lobe == kLobeConductor) {
+    if (lobe == kLobeConductor || lobe == kLobeMicroDiel) {
         // CudaMicrofacetReflection::Sample_f (bxdf.cuh:520-539)
         if (wo.z == 0.0f) return f3(0.0f);
         const Micro mf = make_micro(m);
@@ -475,6 +573,48 @@ NB_D float3 lobe_sample(uint32_t lobe, const DevMaterial& m, const float3& wo, f
             return f3(0.0f);
         }
         pdf = mf.pdf(wo, wh) / (4.0f * dot(wo, wh));
+        return lobe_eval(lobe, m, wo, wi);
+    }
+    if (lobe == kLobeMirror) {
+        // CudaSpecularReflection::Sample_f (bxdf.cuh:377-392), no-op Fresnel
+        wi = f3(-wo.x, -wo.y, wo.z);
+        pdf = 1.0f;
+        return m.diffuse / fabsf(wi.z);
+    }
+    if (lobe == kLobeMicroT) {
+        // CudaMicrofacetTransmission::Sample_f (bxdf.cuh:609-637)
+        if (wo.z == 0.0f) return f3(0.0f);
+        const Micro mf = make_micro(m);
+        float3 wh = mf.sample_wh(wo, ux, uy);
+        const float eta = wo.z > 0.0f ? 1.0f / m.coat_ior : m.coat_ior / 1.0f;
+        if (!refract_ref(wo, wh, eta, wi)) {
+            // total internal reflection: the reference reflects with
+            // helper_math's reflect(i, n) = i - 2 n (n . i)
+            wi = wo - 2.0f * wh * dot(wh, wo);
+            wh *= signf_ref(wh.z);
+            const float F = fresnel_dielectric(dot(wi, wh), 1.0f, m.coat_ior);
+            const float cO = wo.z, cI = wi.z;
+            const float3 r = F * m.specular * mf.D(wh) * mf.G(wo, wi) / (4.0f * cI * cO);
+            pdf = mf.pdf(wo, wh) / (4.0f * dot(wo, wh));
+            return r;
+        }
+        pdf = lobe_pdf(lobe, m, wo, wi);
+        return lobe_eval(lobe, m, wo, wi);
+    }
+    if (lobe == kLobeFresnelBlend) {
+        // CudaFresnelBlend::Sample_f (bxdf.cuh:701-727)
+        if (ux < 0.5f) {
+            const float lx = fminf(2.0f * ux, kOneMinusEps);
+            wi = cosine_hemisphere(lx, uy);
+            wi.z *= signf_ref(wi.z);
+        } else {
+            const float lx = fminf(2.0f * (ux - 0.5f), kOneMinusEps);
+            const Micro mf = make_micro(m);
+            const float3 wh = mf.sample_wh(wo, lx, uy);
+            wi = -1.0f * wo + 2.0f * dot(wo, wh) * wh;
+            if (!same_hemi(wo, wi)) return f3(0.0f);
+        }
+        pdf = lobe_pdf(lobe, m, wo, wi);
         return lobe_eval(lobe, m, wo, wi);
     }
     if (lobe == kLobeFresnelSpec) {
@@ -503,43 +643,87 @@ NB_D float3 lobe_sample(uint32_t lobe, const DevMaterial& m, const float3& wo, f
     return f3(0.0f);
 }
 
-// CudaBSDF over the single lobe (noor/cuda/bsdf.cuh:252-358)
-NB_D float3 bsdf_eval(uint32_t lobe, const DevMaterial& m, const Frame& F, const float3& woW, const float3& wiW,
+// CudaBSDF (noor/cuda/bsdf.cuh:232-358) over a material's lobes
+NB_D int lobes_matching(uint32_t lobes, uint32_t flags) {
+    return (lobe_matches(lobe_at(lobes, 0), flags) ? 1 : 0) + (lobe_matches(lobe_at(lobes, 1), flags) ? 1 : 0);
+}
+NB_D bool lobe_sided(uint32_t id, bool reflect) {
+    return (reflect && (lobe_type(id) & BSDF_REFLECTION)) || (!reflect && (lobe_type(id) & BSDF_TRANSMISSION));
+}
+NB_D float3 bsdf_eval(uint32_t lobes, const DevMaterial& m, const Frame& F, const float3& woW, const float3& wiW,
                       uint32_t flags) {
     const float3 wo = to_local(F, woW), wi = to_local(F, wiW);
     const bool reflect = dot(wiW, F.ng) * dot(woW, F.ng) > 0.0f;
-    if (lobe_matches(lobe, flags) && ((reflect && (lobe & BSDF_REFLECTION)) || (!reflect && (lobe & BSDF_TRANSMISSION))))
-        return lobe_eval(lobe, m, wo, wi);
-    return f3(0.0f);
+    float3 f = f3(0.0f);
+    for (int k = 0; k < 2; ++k) {
+        const uint32_t id = lobe_at(lobes, k);
+        if (lobe_matches(id, flags) && lobe_sided(id, reflect)) f += lobe_eval(id, m, wo, wi);
+    }
+    return f;
 }
-NB_D float bsdf_pdf(uint32_t lobe, const DevMaterial& m, const Frame& F, const float3& woW, const float3& wiW,
+NB_D float bsdf_pdf(uint32_t lobes, const DevMaterial& m, const Frame& F, const float3& woW, const float3& wiW,
                     uint32_t flags) {
-    if (lobe == 0u) return 0.0f;
+    if (lobes == 0u) return 0.0f;
     const float3 wo = to_local(F, woW), wi = to_local(F, wiW);
     if (wo.z == 0.0f) return 0.0f;
-    return lobe_matches(lobe, flags) ? lobe_pdf(lobe, m, wo, wi) : 0.0f;
+    float pdf = 0.0f;
+    int n = 0;
+    for (int k = 0; k < 2; ++k) {
+        const uint32_t id = lobe_at(lobes, k);
+        if (lobe_matches(id, flags)) {
+            ++n;
+            pdf += lobe_pdf(id, m, wo, wi);
+        }
+    }
+    return n > 0 ? pdf / (float)n : 0.0f;
 }
-// draws two random numbers when a lobe matches; pdf 0 = no sample
-NB_D float3 bsdf_sample(uint32_t lobe, const DevMaterial& m, const Frame& F, const float3& woW, uint32_t flags,
-                        Rng& rng, float3& wiW, float& pdf, uint32_t& stype) {
+// one lobe chosen uniformly among the matching ones by ux (remapped for the
+// lobe), with the other matching lobes' pdf and value added unless the
+// chosen lobe is specular; pdf 0 = no sample
+NB_D float3 bsdf_sample_u(uint32_t lobes, const DevMaterial& m, const Frame& F, const float3& woW, uint32_t flags,
+                          float ux, float uy, float3& wiW, float& pdf, uint32_t& stype) {
     pdf = 0.0f;
     stype = 0u;
-    if (!lobe_matches(lobe, flags)) return f3(0.0f);
-    const float ux = rng.next();
-    const float uy = rng.next();
-    const float uxr = fminf(ux * 1.0f - 0.0f, kOneMinusEps);
+    const int n = lobes_matching(lobes, flags);
+    if (n == 0) return f3(0.0f);
+    const int comp = min((int)floorf(ux * (float)n), n - 1);
+    const float uxr = fminf(ux * (float)n - (float)comp, kOneMinusEps);
+    int chosen = -1;
+    for (int k = 0, c = comp; k < 2; ++k)
+        if (lobe_matches(lobe_at(lobes, k), flags) && c-- == 0) {
+            chosen = k;
+            break;
+        }
+    const uint32_t id = lobe_at(lobes, chosen);
     const float3 wo = to_local(F, woW);
     if (wo.z == 0.0f) return f3(0.0f);
     float3 wi = f3(0.0f);
     uint32_t st;
-    const float3 f = lobe_sample(lobe, m, wo, uxr, uy, wi, pdf, st);
-    if (pdf == 0.0f) {
+    float3 f = lobe_sample(id, m, wo, uxr, uy, wi, pdf, st);
+    if (pdf == 0.0f) return f3(0.0f);
+    stype = st;
+    wiW = to_world(F, wi);
+    const bool specular = (lobe_type(id) & BSDF_SPECULAR) != 0u;
+    const uint32_t other = lobe_at(lobes, 1 - chosen);
+    if (!specular && n > 1 && lobe_matches(other, flags)) pdf += lobe_pdf(other, m, wo, wi);
+    if (n > 1) pdf /= (float)n;
+    if (!specular) {
+        const bool reflect = dot(wiW, F.ng) * dot(woW, F.ng) > 0.0f;
+        if (lobe_matches(other, flags) && lobe_sided(other, reflect)) f += lobe_eval(other, m, wo, wi);
+    }
+    return f;
+}
+// draws two random numbers when a lobe matches
+NB_D float3 bsdf_sample(uint32_t lobes, const DevMaterial& m, const Frame& F, const float3& woW, uint32_t flags,
+                        Rng& rng, float3& wiW, float& pdf, uint32_t& stype) {
+    if (lobes_matching(lobes, flags) == 0) {
+        pdf = 0.0f;
         stype = 0u;
         return f3(0.0f);
     }
-    stype = st;
-    wiW = to_world(F, wi);
-    return f;
+    const float ux = rng.next();
+    const float uy = rng.next();
+    return bsdf_sample_u(lobes, m, F, woW, flags, ux, uy, wiW, pdf, stype);
 }
 
 // ------------------------------------------------------------ sky & env

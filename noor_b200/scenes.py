@@ -29,10 +29,15 @@ IDENTITY = np.eye(4, dtype=np.float32).reshape(-1, order="F")
 def material(kind: str, albedo=(0.5, 0.5, 0.5), roughness: float = 0.1, ior: float = 1.5,
              emittance=(0.0, 0.0, 0.0), distribution: int = 0, specular=(1.0, 1.0, 1.0)) -> dict:
     """Constant material parameters (AssetLoader getters) for one of
-    'diffuse', 'metal' (gold conductor, `specular` tints it), 'glass' or
-    'emitter'."""
+    'diffuse', 'metal' (gold conductor, `specular` tints it), 'glass',
+    'emitter', 'mirror' (albedo is the reflectance), 'substrate' (Fresnel
+    blend of the albedo under a `specular` coat), 'translucent' (albedo
+    reflected and transmitted), 'glossy' (albedo under a dielectric
+    microfacet coat) or 'roughglass' (dielectric microfacet reflection and
+    transmission)."""
     types = {"diffuse": capi.NOOR_DIFFUSE, "metal": capi.NOOR_METAL, "glass": capi.NOOR_GLASS,
-             "emitter": capi.NOOR_EMITTER}
+             "emitter": capi.NOOR_EMITTER, "mirror": capi.NOOR_MIRROR, "substrate": capi.NOOR_SUBSTRATE,
+             "translucent": capi.NOOR_TRANSLUCENT, "glossy": capi.NOOR_GLOSSY, "roughglass": capi.NOOR_ROUGHGLASS}
     return dict(diffuse=tuple(albedo), specular=tuple(float(x) for x in specular), transmission=(1.0, 1.0, 1.0),
                 emittance=tuple(emittance), transparency=(1.0, 1.0, 1.0),
                 ior=GOLD_ETA if kind == "metal" else (ior, ior, ior), k=GOLD_K if kind == "metal" else (0, 0, 0),
@@ -101,9 +106,11 @@ def _box(center, size, angle_deg):
 
 
 def room_scene(seed: int = 1, width: int = 256, height: int = 256, spp: int = 16, bounces: int = 5,
-               rr: int = 1, mis: bool = False) -> SceneData:
+               rr: int = 1, mis: bool = False, box_materials=None) -> SceneData:
     """C1: closed room of 5 wall quads + 1 ceiling light quad + 2 rotated
-    boxes = 36 triangles, one mesh; wall albedo U[0.2,0.8]^3 from `seed`."""
+    boxes = 36 triangles, one mesh; wall albedo U[0.2,0.8]^3 from `seed`.
+    `box_materials`: two material dicts for the short and the tall box
+    (default: one diffuse grey for both)."""
     rng = np.random.default_rng(seed)
     faces = []   # (corners, normal, material)
     walls = [
@@ -118,9 +125,16 @@ def room_scene(seed: int = 1, width: int = 256, height: int = 256, spp: int = 16
         mats.append(material("diffuse", albedo=tuple(rng.uniform(0.2, 0.8, 3))))
         faces.append((_quad(pts, np.array(n, np.float64)), np.array(n, np.float64), i))
     box_mat = len(mats)
-    mats.append(material("diffuse", albedo=(0.7, 0.7, 0.7)))
-    for corners_n in _box((0.35, 0.3, 0.25), (0.6, 0.6, 0.6), 17.0) + _box((-0.33, 0.6, -0.3), (0.6, 1.2, 0.6), -18.0):
-        faces.append((corners_n[0], corners_n[1], box_mat))
+    if box_materials is None:
+        mats.append(material("diffuse", albedo=(0.7, 0.7, 0.7)))
+        box_ids = (box_mat, box_mat)
+    else:
+        mats.extend(box_materials)
+        box_ids = (box_mat, box_mat + 1)
+    for b, corners_list in enumerate((_box((0.35, 0.3, 0.25), (0.6, 0.6, 0.6), 17.0),
+                                      _box((-0.33, 0.6, -0.3), (0.6, 1.2, 0.6), -18.0))):
+        for corners_n in corners_list:
+            faces.append((corners_n[0], corners_n[1], box_ids[b]))
     light_mat = len(mats)
     ke = (17.0, 12.0, 4.0)
     mats.append(material("emitter", emittance=ke))

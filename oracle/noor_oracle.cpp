@@ -621,23 +621,51 @@ template <class T> struct Micro {
 };
 
 enum : uint32_t {
-    B_REFL = 1u, B_TRANS = 2u, B_DIFF = 4u, B_GLOSSY = 8u, B_SPEC = 16u, B_COND = 32u, B_DIEL = 64u, B_ALL = 0xFFu
+    B_REFL = 1u, B_TRANS = 2u, B_DIFF = 4u, B_GLOSSY = 8u, B_SPEC = 16u, B_COND = 32u, B_DIEL = 64u, B_NOOP = 128u,
+    B_ALL = 0xFFu
 };
-const uint32_t kLambert = B_REFL | B_DIFF | B_DIEL, kCond = B_COND | B_REFL | B_GLOSSY,
-               kFSpec = B_REFL | B_TRANS | B_SPEC | B_DIEL;
+// lobe ids, one per BxDF class of bxdf.cuh:119-137 the factory builds
+enum : uint32_t {
+    kLambert = 1, kCond = 2, kFSpec = 3, kLambertT = 4, kMirror = 5, kMicroDiel = 6, kMicroT = 7, kFBlend = 8
+};
+// the BxDF type flags of each lobe (the constructors in bxdf.cuh)
+inline uint32_t ltype(uint32_t id) {
+    switch (id) {
+        case kLambert: return B_REFL | B_DIFF | B_DIEL;
+        case kCond: return B_COND | B_REFL | B_GLOSSY;
+        case kFSpec: return B_REFL | B_TRANS | B_SPEC | B_DIEL;
+        case kLambertT: return B_TRANS | B_DIFF | B_DIEL;
+        case kMirror: return B_NOOP | B_REFL | B_SPEC;
+        case kMicroDiel: return B_DIEL | B_REFL | B_GLOSSY;
+        case kMicroT: return B_TRANS | B_GLOSSY | B_DIEL;
+        case kFBlend: return B_REFL | B_GLOSSY | B_DIEL;
+        default: return 0u;
+    }
+}
 const uint32_t kSpecMat = NOOR_MIRROR | NOOR_GLASS | NOOR_CLEARCOAT;
 const uint32_t kTranspMat = NOOR_TRANSLUCENT | NOOR_GLASS | NOOR_ROUGHGLASS;
 const uint32_t kEmitMat = NOOR_EMITTER | NOOR_MESHLIGHT;
 
-// factoryBSDF (bsdf.cuh:425-461)
+// factoryBSDF (bsdf.cuh:383-461): the lobes in Add order, 8 bits each
 inline uint32_t lobe_of(uint32_t mt) {
     const uint32_t t = mt & ~(uint32_t)(NOOR_BUMP | NOOR_ALPHA);
-    if (t == NOOR_DIFFUSE) return kLambert;
-    if (t == NOOR_METAL) return kCond;
-    if (t == NOOR_GLASS) return kFSpec;
-    return 0u;
+    switch (t) {
+        case NOOR_DIFFUSE: return kLambert;
+        case NOOR_METAL: return kCond;
+        case NOOR_GLASS: return kFSpec;
+        case NOOR_MIRROR: return kMirror;
+        case NOOR_SUBSTRATE: return kFBlend;
+        case NOOR_TRANSLUCENT: return kLambert | kLambertT << 8;
+        case NOOR_GLOSSY: return kLambert | kMicroDiel << 8;
+        case NOOR_ROUGHGLASS: return kMicroDiel | kMicroT << 8;
+        default: return 0u;
+    }
 }
-inline bool matches(uint32_t lobe, uint32_t flags) { return lobe && (lobe & flags) == lobe; }
+inline uint32_t lobe_at(uint32_t lobes, int k) { return (lobes >> (8 * k)) & 0xFFu; }
+inline bool matches(uint32_t id, uint32_t flags) {
+    const uint32_t t = ltype(id);
+    return t && (t & flags) == t;
+}
 template <class T> V<T> v3f(const float* f) { return mk((T)f[0], (T)f[1], (T)f[2]); }
 
 template <class T> Micro<T> micro(const Scene::Mat& m) {
@@ -647,30 +675,95 @@ template <class T> Micro<T> micro(const Scene::Mat& m) {
     mf.dist = m.dist;
     return mf;
 }
-// BxDF Eval/Pdf/Sample_f of bxdf.cuh:252-299 (Lambert), 472-557
-// (MicrofacetReflection, conductor), 754-839 (FresnelSpecular)
+// Refract (bxdf.cuh:103-116)
+template <class T> bool refract_r(V<T> wi, V<T> n, T eta, V<T>& wt) {
+    const T ci = dot(n, wi);
+    const T s2i = std::max(T(0), T(1) - ci * ci);
+    const T s2t = eta * eta * s2i;
+    if (s2t >= T(1)) return false;
+    const T ct = std::sqrt(T(1) - s2t);
+    wt = (-eta) * wi + (eta * ci - ct) * n;
+    return true;
+}
+template <class T> T pow5(T v) {
+    const T a = v * v;
+    return a * a * v;
+}
+// BxDF Eval of bxdf.cuh: 252-299 (Lambert), 301-352 (Lambert
+// transmission), 472-557 (MicrofacetReflection), 559-656 (Microfacet-
+// Transmission), 658-752 (FresnelBlend)
 template <class T> V<T> lobe_eval(uint32_t lobe, const Scene::Mat& m, V<T> wo, V<T> wi) {
-    if (lobe == kLambert) return v3f<T>(m.diffuse) * K<T>::inv_pi;
-    if (lobe == kCond) {
-        if (!same(wo, wi)) return mk(T(0), T(0), T(0));
+    const V<T> zero = mk(T(0), T(0), T(0));
+    if (lobe == kLambert || lobe == kLambertT) return v3f<T>(m.diffuse) * K<T>::inv_pi;
+    if (lobe == kCond || lobe == kMicroDiel) {
+        if (!same(wo, wi)) return zero;
         const T cO = std::fabs(wo.z), cI = std::fabs(wi.z);
-        if (cI == T(0) || cO == T(0)) return mk(T(0), T(0), T(0));
+        if (cI == T(0) || cO == T(0)) return zero;
         V<T> wh = nrm(wi + wo);
-        if (black(wh)) return mk(T(0), T(0), T(0));
+        if (black(wh)) return zero;
         wh = wh * signv(wh.z);
-        const V<T> F = fr_cond(dot(wo, wh), v3f<T>(m.ior), v3f<T>(m.k));
+        const V<T> F = lobe == kCond ? fr_cond(dot(wo, wh), v3f<T>(m.ior), v3f<T>(m.k))
+                                     : mk(T(1), T(1), T(1)) * fr_diel(dot(wo, wh), T(1), (T)m.coat_ior);
         const Micro<T> mf = micro<T>(m);
         return F * v3f<T>(m.specular) * mf.D(wh) * mf.G(wo, wi) / (T(4) * cI * cO);
     }
-    return mk(T(0), T(0), T(0));
+    if (lobe == kMicroT) {
+        if (same(wo, wi)) return zero;
+        const T cO = wo.z, cI = wi.z;
+        if (cI == T(0) || cO == T(0)) return zero;
+        const T ior = (T)m.coat_ior;
+        const T eta = wo.z > T(0) ? ior / T(1) : T(1) / ior;
+        V<T> wh = nrm_g(wo + wi * eta);
+        wh = wh * signv(wh.z);
+        const T F = fr_diel(dot(wo, wh), T(1), ior);
+        const T sd = dot(wo, wh) + eta * dot(wi, wh);
+        const Micro<T> mf = micro<T>(m);
+        return (T(1) - F) * v3f<T>(m.transmission) *
+               std::fabs(mf.D(wh) * mf.G(wo, wi) * eta * eta * std::fabs(dot(wi, wh)) * std::fabs(dot(wo, wh)) /
+                         (cI * cO * sd * sd));
+    }
+    if (lobe == kFBlend) {
+        const V<T> S = v3f<T>(m.specular), one = mk(T(1), T(1), T(1));
+        const V<T> diffuse = (T(28) / (T(23) * K<T>::pi)) * v3f<T>(m.diffuse) * (one - S) *
+                             (T(1) - pow5(T(1) - T(0.5) * std::fabs(wi.z))) *
+                             (T(1) - pow5(T(1) - T(0.5) * std::fabs(wo.z)));
+        V<T> wh = wi + wo;
+        if (wh.x == T(0) && wh.y == T(0) && wh.z == T(0)) return zero;
+        wh = nrm_g(wh);
+        const Micro<T> mf = micro<T>(m);
+        const T c = dot(wi, wh);
+        const V<T> schlick = S + pow5(T(1) - c) * (one - S);
+        const V<T> specular =
+            mf.D(wh) / (T(4) * std::fabs(dot(wi, wh)) * std::max(std::fabs(wi.z), std::fabs(wo.z))) * schlick;
+        return diffuse + specular;
+    }
+    return zero;
 }
 template <class T> T lobe_pdf(uint32_t lobe, const Scene::Mat& m, V<T> wo, V<T> wi) {
     if (lobe == kLambert) return same(wo, wi) ? std::fabs(wi.z) * K<T>::inv_pi : T(0);
-    if (lobe == kCond) {
+    if (lobe == kLambertT) return !same(wo, wi) ? std::fabs(wi.z) * K<T>::inv_pi : T(0);
+    if (lobe == kCond || lobe == kMicroDiel) {
         if (!same(wo, wi)) return T(0);
         const V<T> wh = nrm_g(wo + wi);
         const Micro<T> mf = micro<T>(m);
         return mf.pdf(wo, wh) / (T(4) * dot(wo, wh));
+    }
+    if (lobe == kMicroT) {
+        if (same(wo, wi)) return T(0);
+        const T ior = (T)m.coat_ior;
+        const T eta = wo.z > T(0) ? ior / T(1) : T(1) / ior;
+        const V<T> wh = nrm_g(wo + wi * eta);
+        const T sd = dot(wo, wh) + eta * dot(wi, wh);
+        const T dwh = std::fabs((eta * eta * dot(wi, wh)) / (sd * sd));
+        const Micro<T> mf = micro<T>(m);
+        return mf.pdf(wo, wh) * dwh;
+    }
+    if (lobe == kFBlend) {
+        if (!same(wo, wi)) return T(0);
+        const V<T> wh = nrm_g(wo + wi);
+        const Micro<T> mf = micro<T>(m);
+        const T pwh = mf.pdf(wo, wh);
+        return T(0.5) * (std::fabs(wi.z) * K<T>::inv_pi + pwh / (T(4) * dot(wo, wh)));
     }
     return T(0);
 }
@@ -692,17 +785,19 @@ template <class T> V<T> cos_hemi(T ux, T uy) {
     }
     return mk(dx, dy, std::sqrt(std::max(T(0), T(1) - dx * dx - dy * dy)));
 }
+const float kOneMinusEpsF = 1.0f - std::numeric_limits<float>::epsilon();
+// BxDF Sample_f (u already remapped by the BSDF); st = the sampled type
 template <class T> V<T> lobe_sample(uint32_t lobe, const Scene::Mat& m, V<T> wo, T ux, T uy, V<T>& wi, T& pdf,
                                     uint32_t& st) {
-    st = lobe;
+    st = ltype(lobe);
     const V<T> zero = mk(T(0), T(0), T(0));
-    if (lobe == kLambert) {
+    if (lobe == kLambert || lobe == kLambertT) {
         wi = cos_hemi(ux, uy);
-        if (wo.z < T(0)) wi.z = wi.z * T(-1);
-        pdf = same(wo, wi) ? std::fabs(wi.z) * K<T>::inv_pi : T(0);
+        if (lobe == kLambert ? wo.z < T(0) : wo.z > T(0)) wi.z = wi.z * T(-1);
+        pdf = lobe_pdf<T>(lobe, m, wo, wi);
         return v3f<T>(m.diffuse) * K<T>::inv_pi;
     }
-    if (lobe == kCond) {
+    if (lobe == kCond || lobe == kMicroDiel) {
         if (wo.z == T(0)) return zero;
         const Micro<T> mf = micro<T>(m);
         const V<T> wh = mf.sample_wh(wo, ux, uy);
@@ -712,6 +807,46 @@ template <class T> V<T> lobe_sample(uint32_t lobe, const Scene::Mat& m, V<T> wo,
             return zero;
         }
         pdf = mf.pdf(wo, wh) / (T(4) * dot(wo, wh));
+        return lobe_eval<T>(lobe, m, wo, wi);
+    }
+    if (lobe == kMirror) {
+        // specular reflection with the no-op Fresnel (bxdf.cuh:377-392)
+        wi = mk(-wo.x, -wo.y, wo.z);
+        pdf = T(1);
+        return v3f<T>(m.diffuse) / std::fabs(wi.z);
+    }
+    if (lobe == kMicroT) {
+        if (wo.z == T(0)) return zero;
+        const Micro<T> mf = micro<T>(m);
+        V<T> wh = mf.sample_wh(wo, ux, uy);
+        const T ior = (T)m.coat_ior;
+        const T eta = wo.z > T(0) ? T(1) / ior : ior / T(1);
+        if (!refract_r(wo, wh, eta, wi)) {
+            // helper_math's reflect(i, n) = i - 2 n (n . i), as the reference calls it
+            wi = wo - T(2) * wh * dot(wh, wo);
+            wh = wh * signv(wh.z);
+            const T F = fr_diel(dot(wi, wh), T(1), ior);
+            const T cO = wo.z, cI = wi.z;
+            const V<T> r = F * v3f<T>(m.specular) * mf.D(wh) * mf.G(wo, wi) / (T(4) * cI * cO);
+            pdf = mf.pdf(wo, wh) / (T(4) * dot(wo, wh));
+            return r;
+        }
+        pdf = lobe_pdf<T>(lobe, m, wo, wi);
+        return lobe_eval<T>(lobe, m, wo, wi);
+    }
+    if (lobe == kFBlend) {
+        if (ux < T(0.5)) {
+            const T lx = (T)std::min((float)(T(2) * ux), kOneMinusEpsF);
+            wi = cos_hemi(lx, uy);
+            wi.z = wi.z * signv(wi.z);
+        } else {
+            const T lx = (T)std::min((float)(T(2) * (ux - T(0.5))), kOneMinusEpsF);
+            const Micro<T> mf = micro<T>(m);
+            const V<T> wh = mf.sample_wh(wo, lx, uy);
+            wi = T(-1) * wo + T(2) * dot(wo, wh) * wh;
+            if (!same(wo, wi)) return zero;
+        }
+        pdf = lobe_pdf<T>(lobe, m, wo, wi);
         return lobe_eval<T>(lobe, m, wo, wi);
     }
     if (lobe == kFSpec) {
@@ -738,40 +873,83 @@ template <class T> V<T> lobe_sample(uint32_t lobe, const Scene::Mat& m, V<T> wo,
     }
     return zero;
 }
-// CudaBSDF (bsdf.cuh:252-358) over the single lobe
-template <class T> V<T> bsdf_eval(uint32_t lobe, const Scene::Mat& m, const Frame<T>& F, V<T> woW, V<T> wiW,
+// CudaBSDF (bsdf.cuh:232-358) over the material's lobes
+inline int n_matching(uint32_t lobes, uint32_t flags) {
+    return (matches(lobe_at(lobes, 0), flags) ? 1 : 0) + (matches(lobe_at(lobes, 1), flags) ? 1 : 0);
+}
+inline bool sided(uint32_t id, bool refl) { return (refl && (ltype(id) & B_REFL)) || (!refl && (ltype(id) & B_TRANS)); }
+template <class T> V<T> bsdf_eval(uint32_t lobes, const Scene::Mat& m, const Frame<T>& F, V<T> woW, V<T> wiW,
                                   uint32_t flags) {
     const V<T> wo = to_local(F, woW), wi = to_local(F, wiW);
     const bool refl = dot(wiW, F.ng) * dot(woW, F.ng) > T(0);
-    if (matches(lobe, flags) && ((refl && (lobe & B_REFL)) || (!refl && (lobe & B_TRANS))))
-        return lobe_eval<T>(lobe, m, wo, wi);
-    return mk(T(0), T(0), T(0));
+    V<T> f = mk(T(0), T(0), T(0));
+    for (int k = 0; k < 2; ++k) {
+        const uint32_t id = lobe_at(lobes, k);
+        if (matches(id, flags) && sided(id, refl)) f = f + lobe_eval<T>(id, m, wo, wi);
+    }
+    return f;
 }
-template <class T> T bsdf_pdf(uint32_t lobe, const Scene::Mat& m, const Frame<T>& F, V<T> woW, V<T> wiW,
+template <class T> T bsdf_pdf(uint32_t lobes, const Scene::Mat& m, const Frame<T>& F, V<T> woW, V<T> wiW,
                               uint32_t flags) {
-    if (!lobe) return T(0);
+    if (!lobes) return T(0);
     const V<T> wo = to_local(F, woW), wi = to_local(F, wiW);
     if (wo.z == T(0)) return T(0);
-    return matches(lobe, flags) ? lobe_pdf<T>(lobe, m, wo, wi) : T(0);
+    T pdf = T(0);
+    int n = 0;
+    for (int k = 0; k < 2; ++k) {
+        const uint32_t id = lobe_at(lobes, k);
+        if (matches(id, flags)) {
+            ++n;
+            pdf += lobe_pdf<T>(id, m, wo, wi);
+        }
+    }
+    return n > 0 ? pdf / T(n) : T(0);
 }
-template <class T> V<T> bsdf_sample(uint32_t lobe, const Scene::Mat& m, const Frame<T>& F, V<T> woW, uint32_t flags,
-                                    Rng& rng, V<T>& wiW, T& pdf, uint32_t& st) {
+// the BSDF half of Sample_f with its two uniforms given
+template <class T> V<T> bsdf_sample_u(uint32_t lobes, const Scene::Mat& m, const Frame<T>& F, V<T> woW,
+                                      uint32_t flags, float ux, float uy, V<T>& wiW, T& pdf, uint32_t& st) {
     pdf = T(0);
     st = 0;
     const V<T> zero = mk(T(0), T(0), T(0));
-    if (!matches(lobe, flags)) return zero;
-    const float ux = rng.next();
-    const float uy = rng.next();
-    const float uxr = std::min(ux * 1.0f - 0.0f, 1.0f - std::numeric_limits<float>::epsilon());
+    const int n = n_matching(lobes, flags);
+    if (n == 0) return zero;
+    const int comp = std::min((int)std::floor(ux * (float)n), n - 1);
+    const float uxr = std::min(ux * (float)n - (float)comp, kOneMinusEpsF);
+    int chosen = 0;
+    for (int k = 0, c = comp; k < 2; ++k)
+        if (matches(lobe_at(lobes, k), flags) && c-- == 0) {
+            chosen = k;
+            break;
+        }
+    const uint32_t id = lobe_at(lobes, chosen);
     const V<T> wo = to_local(F, woW);
     if (wo.z == T(0)) return zero;
     V<T> wi = zero;
     uint32_t s;
-    const V<T> f = lobe_sample<T>(lobe, m, wo, (T)uxr, (T)uy, wi, pdf, s);
+    V<T> f = lobe_sample<T>(id, m, wo, (T)uxr, (T)uy, wi, pdf, s);
     if (pdf == T(0)) return zero;
     st = s;
     wiW = to_world(F, wi);
+    const bool spec = (ltype(id) & B_SPEC) != 0;
+    const uint32_t other = lobe_at(lobes, 1 - chosen);
+    if (!spec && n > 1 && matches(other, flags)) pdf += lobe_pdf<T>(other, m, wo, wi);
+    if (n > 1) pdf /= T(n);
+    if (!spec) {
+        const bool refl = dot(wiW, F.ng) * dot(woW, F.ng) > T(0);
+        if (matches(other, flags) && sided(other, refl)) f = f + lobe_eval<T>(other, m, wo, wi);
+    }
     return f;
+}
+template <class T> V<T> bsdf_sample(uint32_t lobes, const Scene::Mat& m, const Frame<T>& F, V<T> woW,
+                                    uint32_t flags, Rng& rng, V<T>& wiW, T& pdf, uint32_t& st) {
+    if (n_matching(lobes, flags) == 0) {
+        pdf = T(0);
+        st = 0;
+        return mk(T(0), T(0), T(0));
+    }
+    const float ux = rng.next();
+    const float uy = rng.next();
+    return bsdf_sample_u<T>(lobes, m, F, woW, flags, ux, uy, wiW, pdf, st);
 }
 
 // ----------------------------------------------------------- sky & env
@@ -1633,9 +1811,7 @@ OR_API void oracle_eval_bsdf(void* h, int kind, const float* in, float* out, siz
             else if (kind == 1) pdf = bsdf_pdf<T>(lobe, m, F, wo, wi, B_ALL);
             else {
                 V<T> w = f;
-                if (lobe && wo.z != T(0))
-                    f = lobe_sample<T>(lobe, m, wo, (T)std::min(p[6], 1.0f - std::numeric_limits<float>::epsilon()),
-                                       (T)p[7], w, pdf, st);
+                f = bsdf_sample_u<T>(lobe, m, F, wo, B_ALL, p[6], p[7], w, pdf, st);
                 if (pdf != T(0)) ws = w;
             }
             q[0] = (float)f.x; q[1] = (float)f.y; q[2] = (float)f.z; q[3] = (float)pdf;

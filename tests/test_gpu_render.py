@@ -1,8 +1,11 @@
 """Plain megakernel images against the oracle: the FP32 transcription on the
 same seeds (per-pixel agreement where the paths coincide), and RMSE against
 an FP64 high-spp render."""
+import ctypes
+
 import numpy as np
 import pytest
+import torch
 
 from noor_b200 import _capi, scenes
 from oracle.oracle import Oracle
@@ -117,4 +120,49 @@ def test_sphere_field_matches_oracle(kind):
         assert r.status() == 0
     finally:
         orc.close()
+        r.close()
+
+
+@pytest.mark.parametrize("pair", [("glossy", "roughglass"), ("substrate", "mirror"), ("translucent", "glossy")])
+def test_room_with_other_materials_matches_oracle(pair):
+    """the lobes no configuration uses, on the two boxes: GPU megakernel and
+    wavefront against the oracle on the same seeds"""
+    kw = {"glossy": dict(albedo=(0.6, 0.4, 0.3), roughness=0.25, ior=1.5),
+          "roughglass": dict(roughness=0.3, ior=1.5),
+          "substrate": dict(albedo=(0.3, 0.5, 0.7), specular=(0.05, 0.05, 0.05), roughness=0.3),
+          "mirror": dict(albedo=(0.9, 0.9, 0.9)),
+          "translucent": dict(albedo=(0.6, 0.6, 0.5))}
+    boxes = [scenes.material(k, **kw[k]) for k in pair]
+    s = scenes.room_scene(width=64, height=64, spp=16, box_materials=boxes)
+    r = scenes.Renderer(s)
+    try:
+        for mis in (0, 1):
+            r.update_spec(mis=mis)
+            r.render(16)
+            img = r.framebuffer()[..., :3]
+            # the wavefront on the same samples
+            film = torch.zeros((64, 64, 4), dtype=torch.float32, device="cuda")
+            fr = (_capi.WfFrame * 1)(scenes.wf_frame(0, s.camera, 16, 5, d_film=film.data_ptr()))
+            _capi.call("noor_wavefront_render", fr, 1, ctypes.byref(scenes.wf_params(64, 1 << 16, 1, 1)))
+            wf = film.cpu().numpy()[..., :3]
+            relw = np.abs(wf - img) / np.maximum(np.abs(img), 1e-2)
+            assert np.median(relw) < 1e-5 and (relw > 1e-3).mean() < 0.05, (pair, mis)
+            orc = Oracle(r.built.payload, r.spec, r.hosek)
+            o32 = orc.render(r.camera, 1, 16, fp64=False, threads=THREADS).reshape(64, 64, 3)
+            o64 = orc.render(r.camera, 1, 256, fp64=True, threads=THREADS).reshape(64, 64, 3)
+            orc.close()
+            rel = np.abs(img - o32) / np.maximum(np.abs(o32), 1e-2)
+            assert np.isfinite(img).all() and img.mean() > 0.01
+            assert np.median(rel) < 1e-5, (pair, mis, float(np.median(rel)))
+            # paths that enter a translucent box bounce between its inner
+            # faces, where the last bit of a float (the GPU fuses multiply-
+            # adds, the oracle does not) can send a path elsewhere: ~6 % of
+            # pixels then differ by more than 1e-3, with the same error
+            # against the FP64 oracle
+            frac = 0.10 if "translucent" in pair else 0.05
+            assert (rel > 1e-3).mean() < frac, (pair, mis, float((rel > 1e-3).mean()))
+            e_gpu, e_orc = rmse(img, o64), rmse(o32, o64)
+            assert abs(e_gpu - e_orc) <= 0.01 * e_orc, (pair, mis, e_gpu, e_orc)
+        assert r.status(reset=True) == 0
+    finally:
         r.close()

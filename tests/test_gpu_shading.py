@@ -19,7 +19,14 @@ MATS = [scenes.material("diffuse", albedo=(0.2, 0.5, 0.8)),
         scenes.material("metal", roughness=float(np.sqrt(0.05))),
         scenes.material("metal", roughness=float(np.sqrt(0.5))),
         scenes.material("metal", roughness=0.4, distribution=1),
-        scenes.material("glass", ior=1.5)]
+        scenes.material("glass", ior=1.5),
+        # the lobes no configuration uses: mirror, Fresnel blend, and the
+        # two-lobe materials (translucent, glossy, rough glass)
+        scenes.material("mirror", albedo=(0.9, 0.8, 0.7)),
+        scenes.material("substrate", albedo=(0.3, 0.5, 0.7), specular=(0.04, 0.05, 0.06), roughness=0.3),
+        scenes.material("translucent", albedo=(0.6, 0.5, 0.4)),
+        scenes.material("glossy", albedo=(0.5, 0.3, 0.2), roughness=0.2, ior=1.5),
+        scenes.material("roughglass", roughness=0.3, ior=1.5)]
 
 
 def _scene(sky=_capi.NOOR_SKY_PHYSICAL, env=None):
@@ -80,7 +87,13 @@ def test_bsdf_matches_fp32_transcription(sky, kind):
     o = orc.eval_bsdf(kind, rec, fp64=False)
     if kind < 2:
         cols = [0, 1, 2] if kind == 0 else [3]
-        err = _rel(g[:, cols], o[:, cols], 1e-6)
+        # where FP32 itself cannot reach 1e-5 (the microfacet transmission's
+        # refraction half-vector cancels: FP32 oracle vs FP64 up to 1e-3 at
+        # the 99.9th percentile), the two FP32 evaluations are not compared
+        o64 = orc.eval_bsdf(kind, rec, fp64=True)
+        cond = _rel(o[:, cols], o64[:, cols], 1e-6).max(1) < 1e-5
+        assert cond.mean() > 0.99, cond.mean()
+        err = _rel(g[cond][:, cols], o[cond][:, cols], 1e-6)
         q = np.quantile(err, [0.5, 0.999, 1.0])
         assert q[1] < 1e-5, q
         return
@@ -105,7 +118,12 @@ def test_bsdf_against_fp64(sky, kind):
     g = _gpu_bsdf(kind, rec)
     o = orc.eval_bsdf(kind, rec, fp64=True)
     cols = [0, 1, 2] if kind == 0 else [3]
-    assert np.quantile(_rel(g[:, cols], o[:, cols], 1e-6), 0.99) < 1e-5
+    err = _rel(g[:, cols], o[:, cols], 1e-6).max(1)
+    # the microfacet transmission (rough glass) is ill-conditioned in FP32
+    # at the tail; every other lobe meets 1e-5 at the 99th percentile
+    rough_glass = np.array([MATS[int(i)]["type"] == _capi.NOOR_ROUGHGLASS for i in rec[:, 8]])
+    assert np.quantile(err[~rough_glass], 0.99) < 1e-5
+    assert np.quantile(err[rough_glass], 0.99) < 1e-4
 
 
 def test_sky_radiance(sky):
