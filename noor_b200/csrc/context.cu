@@ -269,6 +269,8 @@ int upload_scene(Context& C, const noor_payload* P, const noor_hosek_sky* H, con
         for (uint32_t i = 0; i < P->num_materials; ++i) {
             std::memset(&m[i], 0, sizeof(DevMaterial));
             resolve_material(P, P->materials[i], m[i]);
+            const uint32_t l = lobe_of(m[i].type);
+            if (l > 0xFFFFu || !lobe_common(l)) D.ext_lobes = 1u;
         }
         st.materials_host = m;
         if ((rc = st.upload((void**)&D.materials, m.data(), m.size() * sizeof(DevMaterial), "materials"))) return rc;

@@ -101,6 +101,7 @@ struct ShadowRay {
 // no ray needed, on every early exit).  The MIS weight is applied here; the
 // reference evaluates it after the occlusion test, which draws no random
 // numbers, so the order does not change the result.
+template <bool EXT = true>
 NB_D float3 light_sample_contrib(const DevScene& S, const DevMaterial& m, const Isect& I, Rng& rng, bool mis,
                                  int& light_idx, bool& picked, ShadowRay& sr) {
     picked = false;
@@ -114,19 +115,20 @@ NB_D float3 light_sample_contrib(const DevScene& S, const DevMaterial& m, const 
     float lpdf;
     const float3 Li = sample_li(S, I, rng, nl, li, wi, to, lpdf);
     if (lpdf == 0.0f || is_black(Li)) return f3(0.0f);
-    float3 f = bsdf_eval(I.lobe, m, I.F, I.wo, wi, kNonSpecular);
+    float3 f = bsdf_eval<EXT>(I.lobe, m, I.F, I.wo, wi, kNonSpecular);
     if (is_black(f)) return f3(0.0f);
     f *= absdot(wi, I.F.n);
     sr.o = spawn_origin(I, wi, S.bias);
     sr.d = wi;
     sr.tmax = length3(sr.o - to);
     if (!mis) return Li * f / lpdf;
-    const float spdf = bsdf_pdf(I.lobe, m, I.F, I.wo, wi, kNonSpecular);
+    const float spdf = bsdf_pdf<EXT>(I.lobe, m, I.F, I.wo, wi, kNonSpecular);
     const float w = power_heuristic(lpdf, spdf);
     return Li * f * w / lpdf;
 }
 
 // sampleBSDF (noor/cuda/direct.cuh:69-110) up to the occlusion test
+template <bool EXT = true>
 NB_D float3 bsdf_mis_contrib(const DevScene& S, const DevMaterial& m, const Isect& I, Rng& rng, int li,
                              ShadowRay& sr) {
     const uint32_t flags = (I.mtype & kSpecularMat) ? BSDF_ALL : kNonSpecular;
@@ -135,7 +137,7 @@ NB_D float3 bsdf_mis_contrib(const DevScene& S, const DevMaterial& m, const Isec
     float3 wi;
     float spdf;
     uint32_t stype;
-    float3 f = bsdf_sample(I.lobe, m, I.F, I.wo, flags, rng, wi, spdf, stype);
+    float3 f = bsdf_sample<EXT>(I.lobe, m, I.F, I.wo, flags, rng, wi, spdf, stype);
     if (is_black(f) || spdf == 0.0f) return f3(0.0f);
     f *= absdot(wi, I.F.n);
     float w = 1.0f;
@@ -169,12 +171,12 @@ NB_D float3 bsdf_mis_contrib(const DevScene& S, const DevMaterial& m, const Isec
 }
 
 // Builds the hit record of CudaIntersection (intersection.cuh:319-377).
-template <int ISECT>
+template <int ISECT, bool EXT = true>
 NB_D void make_isect(const DevScene& S, const float3& o, const float3& d, float t, const HitRec& rec, Isect& I) {
     I.p = o + t * d;
     I.wo = normalize_fast(-1.0f * d);
     I.mtype = rec.mtype;
-    I.lobe = lobe_of(rec.mtype);
+    I.lobe = lobe_of<EXT>(rec.mtype);
     if (ISECT == NOOR_ISECT_WATERTIGHT) {
         const DevWtTri* T = S.wtri + rec.tri;
         const uint4 attr = __ldg(&T->attr);
@@ -194,7 +196,9 @@ NB_D void make_isect(const DevScene& S, const float3& o, const float3& d, float 
 }
 
 // pathtracer() of noor/cuda/path_tracer.cu:26-75; returns clamp(L, 0, 100)
-template <int ISECT>
+// EXT false: the specialisation for scenes whose materials use only the
+// Lambert, conductor and Fresnel-specular lobes
+template <int ISECT, bool EXT = true>
 NB_D float3 path_radiance(const DevScene& S, float3 o, float3 d, Rng& rng, const SmemStack& st, uint32_t* status,
                           RayStats& rs, float3* first_hit, bool* first_hit_valid) {
     float3 L = f3(0.0f);
@@ -209,7 +213,7 @@ NB_D float3 path_radiance(const DevScene& S, float3 o, float3 d, Rng& rng, const
             break;
         }
         Isect I;
-        make_isect<ISECT>(S, o, d, tmax, rec, I);
+        make_isect<ISECT, EXT>(S, o, d, tmax, rec, I);
         if (bounce == 0 && first_hit) {
             *first_hit = I.p;
             *first_hit_valid = true;
@@ -232,13 +236,13 @@ NB_D float3 path_radiance(const DevScene& S, float3 o, float3 d, Rng& rng, const
         int li = 0;
         bool picked;
         ShadowRay sr;
-        float3 Ld = light_sample_contrib(S, m, I, rng, S.mis != 0, li, picked, sr);
+        float3 Ld = light_sample_contrib<EXT>(S, m, I, rng, S.mis != 0, li, picked, sr);
         if (!is_black(Ld)) {
             rs.shadow++;
             if (trace_any<ISECT>(S, sr.o, sr.d, sr.tmax, st, status)) Ld = f3(0.0f);
         }
         if (S.mis && picked) {
-            float3 c = bsdf_mis_contrib(S, m, I, rng, li, sr);
+            float3 c = bsdf_mis_contrib<EXT>(S, m, I, rng, li, sr);
             if (!is_black(c)) {
                 rs.shadow++;
                 if (trace_any<ISECT>(S, sr.o, sr.d, sr.tmax, st, status)) c = f3(0.0f);
@@ -252,7 +256,7 @@ NB_D float3 path_radiance(const DevScene& S, float3 o, float3 d, Rng& rng, const
         float3 wi;
         float pdf;
         uint32_t stype;
-        const float3 f = bsdf_sample(I.lobe, m, I.F, I.wo, BSDF_ALL, rng, wi, pdf, stype);
+        const float3 f = bsdf_sample<EXT>(I.lobe, m, I.F, I.wo, BSDF_ALL, rng, wi, pdf, stype);
         if (pdf == 0.0f) break;
         beta *= f * absdot(wi, I.F.n) / pdf;
         // correct_sidedness (accumulate.cuh:40-45)

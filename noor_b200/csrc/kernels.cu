@@ -30,7 +30,7 @@ NB_D void kahan_add(float3& sum, float3& c, const float3& x) {
 #define NB_MEGA_MIN_BLOCKS 7
 #endif
 
-template <int ISECT, int FILM>
+template <int ISECT, int FILM, bool EXT>
 __global__ void __launch_bounds__(kMegaBlock, NB_MEGA_MIN_BLOCKS) megakernel(DevScene S, DevCamera C, MegaArgs a) {
     extern __shared__ uint32_t smem[];
     const uint32_t npix = C.w * C.h;
@@ -64,8 +64,8 @@ __global__ void __launch_bounds__(kMegaBlock, NB_MEGA_MIN_BLOCKS) megakernel(Dev
             float3 o, d;
             camera_ray(C, x, y, rng, o, d);
             hit_valid = false;
-            const float3 L = path_radiance<ISECT>(S, o, d, rng, st, a.status, rs, want_hit ? &hitp : nullptr,
-                                                  &hit_valid);
+            const float3 L = path_radiance<ISECT, EXT>(S, o, d, rng, st, a.status, rs,
+                                                       want_hit ? &hitp : nullptr, &hit_valid);
             ++paths;
             if (FILM == NOOR_FILM_KAHAN) {
                 kahan_add(sum, comp, L);
@@ -276,11 +276,18 @@ cudaError_t launch_megakernel(const DevScene& S, const DevCamera& C, const MegaA
     const uint32_t grid = (uint32_t)((threads + kMegaBlock - 1) / kMegaBlock);
     const size_t sm = stack_bytes(S, kMegaBlock);
     cudaError_t e;
-#define NB_MK(I, F)                                                                          \
-    do {                                                                                     \
-        e = cudaFuncSetAttribute(megakernel<I, F>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm); \
-        if (e != cudaSuccess) return e;                                                      \
-        megakernel<I, F><<<grid, kMegaBlock, sm, s>>>(S, C, a);                              \
+    // scenes without the extra lobes run a specialisation without their code
+    // (the kernel's registers are capped, so unused branches cost spills)
+#define NB_MK2(I, F, X)                                                                         \
+    do {                                                                                        \
+        e = cudaFuncSetAttribute(megakernel<I, F, X>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm); \
+        if (e != cudaSuccess) return e;                                                         \
+        megakernel<I, F, X><<<grid, kMegaBlock, sm, s>>>(S, C, a);                              \
+    } while (0)
+#define NB_MK(I, F)                     \
+    do {                                \
+        if (S.ext_lobes) NB_MK2(I, F, true); \
+        else NB_MK2(I, F, false);       \
     } while (0)
     if (S.isect == NOOR_ISECT_WATERTIGHT) {
         if (S.film_mode == NOOR_FILM_KAHAN) NB_MK(NOOR_ISECT_WATERTIGHT, NOOR_FILM_KAHAN);
@@ -290,6 +297,7 @@ cudaError_t launch_megakernel(const DevScene& S, const DevCamera& C, const MegaA
         else NB_MK(NOOR_ISECT_REF_WALD, NOOR_FILM_REF_LERP);
     }
 #undef NB_MK
+#undef NB_MK2
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     if (a.chunks > 1u) {

@@ -127,6 +127,7 @@ struct DevScene {
     uint32_t isect;
     uint32_t film_mode;
     int stack_cap;
+    uint32_t ext_lobes;     // some material uses a lobe beyond Lambert, conductor, Fresnel specular
 };
 
 }  // namespace nb

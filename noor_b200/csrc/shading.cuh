@@ -407,40 +407,46 @@ enum : uint32_t {
     BSDF_NOOP = 1u << 7,
     BSDF_ALL = 0xFFu
 };
-// Lobe ids (one per BxDF class the material factory builds,
-// noor/cuda/bxdf.cuh:119-137) and their BxDF type flags.
+#ifndef NB_LOBE_OUTLINE
+#define NB_LOBE_OUTLINE 1
+#endif
+#if NB_LOBE_OUTLINE
+#define NB_OUTLINE static __device__ __noinline__
+#else
+#define NB_OUTLINE NB_D
+#endif
+
+// Lobe ids, one per BxDF class the material factory builds
+// (noor/cuda/bxdf.cuh:119-137): the low 8 bits are the class's BxDF type
+// flags (its constructor's), bits 8-15 tell apart classes with equal flags.
 enum : uint32_t {
     kLobeNone = 0,
-    kLobeLambert = 1,       // CudaLambertianReflection (bxdf.cuh:252-299)
-    kLobeConductor = 2,     // CudaMicrofacetReflection, conductor Fresnel (bxdf.cuh:472-557)
-    kLobeFresnelSpec = 3,   // CudaFresnelSpecular (bxdf.cuh:754-839)
-    kLobeLambertT = 4,      // CudaLambertianTransmission (bxdf.cuh:301-352)
-    kLobeMirror = 5,        // CudaSpecularReflection, no-op Fresnel (bxdf.cuh:354-404)
-    kLobeMicroDiel = 6,     // CudaMicrofacetReflection, dielectric Fresnel
-    kLobeMicroT = 7,        // CudaMicrofacetTransmission (bxdf.cuh:559-656)
-    kLobeFresnelBlend = 8,  // CudaFresnelBlend (bxdf.cuh:658-752)
+    // CudaLambertianReflection (bxdf.cuh:252-299)
+    kLobeLambert = BSDF_REFLECTION | BSDF_DIFFUSE | BSDF_DIELECTRIC,
+    // CudaMicrofacetReflection with the conductor Fresnel (bxdf.cuh:472-557)
+    kLobeConductor = BSDF_CONDUCTOR | BSDF_REFLECTION | BSDF_GLOSSY,
+    // CudaFresnelSpecular (bxdf.cuh:754-839)
+    kLobeFresnelSpec = BSDF_REFLECTION | BSDF_TRANSMISSION | BSDF_SPECULAR | BSDF_DIELECTRIC,
+    // CudaLambertianTransmission (bxdf.cuh:301-352)
+    kLobeLambertT = BSDF_TRANSMISSION | BSDF_DIFFUSE | BSDF_DIELECTRIC,
+    // CudaSpecularReflection with the no-op Fresnel (bxdf.cuh:354-404)
+    kLobeMirror = BSDF_NOOP | BSDF_REFLECTION | BSDF_SPECULAR,
+    // CudaMicrofacetReflection with the dielectric Fresnel
+    kLobeMicroDiel = (BSDF_DIELECTRIC | BSDF_REFLECTION | BSDF_GLOSSY) | 1u << 8,
+    // CudaMicrofacetTransmission (bxdf.cuh:559-656)
+    kLobeMicroT = BSDF_TRANSMISSION | BSDF_GLOSSY | BSDF_DIELECTRIC,
+    // CudaFresnelBlend (bxdf.cuh:658-752)
+    kLobeFresnelBlend = (BSDF_REFLECTION | BSDF_GLOSSY | BSDF_DIELECTRIC) | 2u << 8,
 };
-NB_HD uint32_t lobe_type(uint32_t id) {
-    switch (id) {
-        case kLobeLambert: return BSDF_REFLECTION | BSDF_DIFFUSE | BSDF_DIELECTRIC;
-        case kLobeConductor: return BSDF_CONDUCTOR | BSDF_REFLECTION | BSDF_GLOSSY;
-        case kLobeFresnelSpec: return BSDF_REFLECTION | BSDF_TRANSMISSION | BSDF_SPECULAR | BSDF_DIELECTRIC;
-        case kLobeLambertT: return BSDF_TRANSMISSION | BSDF_DIFFUSE | BSDF_DIELECTRIC;
-        case kLobeMirror: return BSDF_NOOP | BSDF_REFLECTION | BSDF_SPECULAR;
-        case kLobeMicroDiel: return BSDF_DIELECTRIC | BSDF_REFLECTION | BSDF_GLOSSY;
-        case kLobeMicroT: return BSDF_TRANSMISSION | BSDF_GLOSSY | BSDF_DIELECTRIC;
-        case kLobeFresnelBlend: return BSDF_REFLECTION | BSDF_GLOSSY | BSDF_DIELECTRIC;
-        default: return 0u;
-    }
-}
+NB_HD uint32_t lobe_type(uint32_t id) { return id & 0xFFu; }
 
 constexpr uint32_t kSpecularMat = NOOR_MIRROR | NOOR_GLASS | NOOR_CLEARCOAT;      // NOOR_SPECULAR
 constexpr uint32_t kTransparentMat = NOOR_TRANSLUCENT | NOOR_GLASS | NOOR_ROUGHGLASS;
 constexpr uint32_t kEmitterMat = NOOR_EMITTER | NOOR_MESHLIGHT;
 
 // The lobes factoryBSDF builds for a material (noor/cuda/bsdf.cuh:383-461),
-// in the order it adds them: lobe k in bits 8k..8k+7; 0 = none.  Clear-coat
-// and shadow-catcher materials build none here.
+// in the order it adds them: lobe k in bits 16k..16k+15; 0 = none.
+// Clear-coat and shadow-catcher materials build none here.
 NB_HD uint32_t lobe_of(uint32_t mtype) {
     const uint32_t t = mtype & ~(uint32_t)(NOOR_BUMP | NOOR_ALPHA);
     switch (t) {
@@ -449,15 +455,27 @@ NB_HD uint32_t lobe_of(uint32_t mtype) {
         case NOOR_GLASS: return kLobeFresnelSpec;
         case NOOR_MIRROR: return kLobeMirror;
         case NOOR_SUBSTRATE: return kLobeFresnelBlend;
-        case NOOR_TRANSLUCENT: return kLobeLambert | kLobeLambertT << 8;
-        case NOOR_GLOSSY: return kLobeLambert | kLobeMicroDiel << 8;
-        case NOOR_ROUGHGLASS: return kLobeMicroDiel | kLobeMicroT << 8;
+        case NOOR_TRANSLUCENT: return kLobeLambert | kLobeLambertT << 16;
+        case NOOR_GLOSSY: return kLobeLambert | kLobeMicroDiel << 16;
+        case NOOR_ROUGHGLASS: return kLobeMicroDiel | kLobeMicroT << 16;
         default: return 0u;
     }
 }
-NB_D uint32_t lobe_at(uint32_t lobes, int k) { return (lobes >> (8 * k)) & 0xFFu; }
+// EXT false: only the three lobes a specialised kernel handles
+template <bool EXT>
+NB_D uint32_t lobe_of(uint32_t mtype) {
+    if (EXT) return lobe_of(mtype);
+    const uint32_t t = mtype & ~(uint32_t)(NOOR_BUMP | NOOR_ALPHA);
+    if (t == NOOR_DIFFUSE) return kLobeLambert;
+    if (t == NOOR_METAL) return kLobeConductor;
+    if (t == NOOR_GLASS) return kLobeFresnelSpec;
+    return 0u;
+}
+NB_D uint32_t lobe_at(uint32_t lobes, int k) { return (lobes >> (16 * k)) & 0xFFFFu; }
+// EXT false: the id is one of the three lobes whose ids are their flags
+template <bool EXT = true>
 NB_D bool lobe_matches(uint32_t id, uint32_t flags) {
-    const uint32_t t = lobe_type(id);
+    const uint32_t t = EXT ? lobe_type(id) : id;
     return t != 0u && (t & flags) == t;
 }
 
@@ -477,8 +495,11 @@ NB_D float pow5(float v) {
 }
 NB_D float3 schlick(const DevMaterial& m, float c) { return m.specular + pow5(1.0f - c) * (f3(1.0f) - m.specular); }
 
-// BxDF::Eval of a lobe, local frame
-NB_D float3 lobe_eval(uint32_t lobe, const DevMaterial& m, const float3& wo, const float3& wi) {
+NB_D float3 lobe_eval(uint32_t lobe, const DevMaterial& m, const float3& wo, const float3& wi);
+NB_D float lobe_pdf(uint32_t lobe, const DevMaterial& m, const float3& wo, const float3& wi);
+
+// BxDF::Eval of a lobe, local frame (every lobe)
+NB_D float3 lobe_eval_all(uint32_t lobe, const DevMaterial& m, const float3& wo, const float3& wi) {
     if (lobe == kLobeLambert || lobe == kLobeLambertT) return m.diffuse * kInvPi;
     if (lobe == kLobeConductor || lobe == kLobeMicroDiel) {
         // CudaMicrofacetReflection::Eval (bxdf.cuh:482-506)
@@ -521,7 +542,7 @@ NB_D float3 lobe_eval(uint32_t lobe, const DevMaterial& m, const float3& wo, con
     }
     return f3(0.0f);  // specular lobes: delta
 }
-NB_D float lobe_pdf(uint32_t lobe, const DevMaterial& m, const float3& wo, const float3& wi) {
+NB_D float lobe_pdf_all(uint32_t lobe, const DevMaterial& m, const float3& wo, const float3& wi) {
     if (lobe == kLobeLambert) return same_hemi(wo, wi) ? fabsf(wi.z) * kInvPi : 0.0f;
     if (lobe == kLobeLambertT) return !same_hemi(wo, wi) ? fabsf(wi.z) * kInvPi : 0.0f;
     if (lobe == kLobeConductor || lobe == kLobeMicroDiel) {
@@ -552,8 +573,8 @@ NB_D float lobe_pdf(uint32_t lobe, const DevMaterial& m, const float3& wo, const
 }
 // BxDF::Sample_f of a lobe (u already remapped by the BSDF); pdf stays 0 on
 // failure; stype = the sampled BxDF type
-NB_D float3 lobe_sample(uint32_t lobe, const DevMaterial& m, const float3& wo, float ux, float uy, float3& wi,
-                        float& pdf, uint32_t& stype) {
+NB_D float3 lobe_sample_all(uint32_t lobe, const DevMaterial& m, const float3& wo, float ux, float uy, float3& wi,
+                            float& pdf, uint32_t& stype) {
     stype = lobe_type(lobe);
     if (lobe == kLobeLambert || lobe == kLobeLambertT) {
         // CudaLambertianReflection / Transmission::Sample_f (bxdf.cuh:270-285, 321-336)
@@ -643,15 +664,73 @@ NB_D float3 lobe_sample(uint32_t lobe, const DevMaterial& m, const float3& wo, f
     return f3(0.0f);
 }
 
-// CudaBSDF (noor/cuda/bsdf.cuh:232-358) over a material's lobes
+// The lobes the configurations use (Lambert, conductor, Fresnel specular)
+// are expanded inline; the others are one shared out-of-line copy, so that
+// their code does not grow the registers and spills of the integrators'
+// hot loops.
+NB_OUTLINE float3 lobe_eval_extra(uint32_t lobe, const DevMaterial& m, float3 wo, float3 wi) {
+    return lobe_eval_all(lobe, m, wo, wi);
+}
+NB_OUTLINE float lobe_pdf_extra(uint32_t lobe, const DevMaterial& m, float3 wo, float3 wi) {
+    return lobe_pdf_all(lobe, m, wo, wi);
+}
+NB_OUTLINE float3 lobe_sample_extra(uint32_t lobe, const DevMaterial& m, float3 wo, float ux, float uy,
+                                                 float3& wi, float& pdf, uint32_t& stype) {
+    return lobe_sample_all(lobe, m, wo, ux, uy, wi, pdf, stype);
+}
+NB_HD bool lobe_common(uint32_t lobe) {
+    return lobe == kLobeNone || lobe == kLobeLambert || lobe == kLobeConductor || lobe == kLobeFresnelSpec;
+}
+// EXT false: a kernel specialised for scenes whose materials use only the
+// lobes above (the other lobes' code is left out)
+template <bool EXT>
+NB_D float3 lobe_eval(uint32_t lobe, const DevMaterial& m, const float3& wo, const float3& wi) {
+    if (lobe == kLobeLambert) return m.diffuse * kInvPi;
+    if (lobe == kLobeConductor) return lobe_eval_all(kLobeConductor, m, wo, wi);
+    if (!EXT || lobe_common(lobe)) return f3(0.0f);
+    return lobe_eval_extra(lobe, m, wo, wi);
+}
+NB_D float3 lobe_eval(uint32_t lobe, const DevMaterial& m, const float3& wo, const float3& wi) {
+    return lobe_eval<true>(lobe, m, wo, wi);
+}
+template <bool EXT>
+NB_D float lobe_pdf(uint32_t lobe, const DevMaterial& m, const float3& wo, const float3& wi) {
+    if (lobe == kLobeLambert) return same_hemi(wo, wi) ? fabsf(wi.z) * kInvPi : 0.0f;
+    if (lobe == kLobeConductor) return lobe_pdf_all(kLobeConductor, m, wo, wi);
+    if (!EXT || lobe_common(lobe)) return 0.0f;
+    return lobe_pdf_extra(lobe, m, wo, wi);
+}
+NB_D float lobe_pdf(uint32_t lobe, const DevMaterial& m, const float3& wo, const float3& wi) {
+    return lobe_pdf<true>(lobe, m, wo, wi);
+}
+template <bool EXT = true>
+NB_D float3 lobe_sample(uint32_t lobe, const DevMaterial& m, const float3& wo, float ux, float uy, float3& wi,
+                        float& pdf, uint32_t& stype) {
+    if (lobe == kLobeLambert) return lobe_sample_all(kLobeLambert, m, wo, ux, uy, wi, pdf, stype);
+    if (lobe == kLobeConductor) return lobe_sample_all(kLobeConductor, m, wo, ux, uy, wi, pdf, stype);
+    if (lobe == kLobeFresnelSpec) return lobe_sample_all(kLobeFresnelSpec, m, wo, ux, uy, wi, pdf, stype);
+    if (!EXT || lobe_common(lobe)) {
+        stype = 0u;
+        return f3(0.0f);
+    }
+    return lobe_sample_extra(lobe, m, wo, ux, uy, wi, pdf, stype);
+}
+
+// CudaBSDF (noor/cuda/bsdf.cuh:232-358) over a material's lobes.  A
+// one-lobe material (every material the configurations use) takes the
+// inline path; two-lobe materials go through one shared out-of-line copy of
+// the general aggregation, which keeps the integrators' hot loops as lean
+// as for one lobe.
 NB_D int lobes_matching(uint32_t lobes, uint32_t flags) {
     return (lobe_matches(lobe_at(lobes, 0), flags) ? 1 : 0) + (lobe_matches(lobe_at(lobes, 1), flags) ? 1 : 0);
 }
+template <bool EXT = true>
 NB_D bool lobe_sided(uint32_t id, bool reflect) {
-    return (reflect && (lobe_type(id) & BSDF_REFLECTION)) || (!reflect && (lobe_type(id) & BSDF_TRANSMISSION));
+    const uint32_t t = EXT ? lobe_type(id) : id;
+    return (reflect && (t & BSDF_REFLECTION)) || (!reflect && (t & BSDF_TRANSMISSION));
 }
-NB_D float3 bsdf_eval(uint32_t lobes, const DevMaterial& m, const Frame& F, const float3& woW, const float3& wiW,
-                      uint32_t flags) {
+NB_D float3 bsdf_eval_n(uint32_t lobes, const DevMaterial& m, const Frame& F, const float3& woW, const float3& wiW,
+                        uint32_t flags) {
     const float3 wo = to_local(F, woW), wi = to_local(F, wiW);
     const bool reflect = dot(wiW, F.ng) * dot(woW, F.ng) > 0.0f;
     float3 f = f3(0.0f);
@@ -661,8 +740,8 @@ NB_D float3 bsdf_eval(uint32_t lobes, const DevMaterial& m, const Frame& F, cons
     }
     return f;
 }
-NB_D float bsdf_pdf(uint32_t lobes, const DevMaterial& m, const Frame& F, const float3& woW, const float3& wiW,
-                    uint32_t flags) {
+NB_D float bsdf_pdf_n(uint32_t lobes, const DevMaterial& m, const Frame& F, const float3& woW, const float3& wiW,
+                      uint32_t flags) {
     if (lobes == 0u) return 0.0f;
     const float3 wo = to_local(F, woW), wi = to_local(F, wiW);
     if (wo.z == 0.0f) return 0.0f;
@@ -680,7 +759,7 @@ NB_D float bsdf_pdf(uint32_t lobes, const DevMaterial& m, const Frame& F, const 
 // one lobe chosen uniformly among the matching ones by ux (remapped for the
 // lobe), with the other matching lobes' pdf and value added unless the
 // chosen lobe is specular; pdf 0 = no sample
-NB_D float3 bsdf_sample_u(uint32_t lobes, const DevMaterial& m, const Frame& F, const float3& woW, uint32_t flags,
+NB_D float3 bsdf_sample_n(uint32_t lobes, const DevMaterial& m, const Frame& F, const float3& woW, uint32_t flags,
                           float ux, float uy, float3& wiW, float& pdf, uint32_t& stype) {
     pdf = 0.0f;
     stype = 0u;
@@ -713,17 +792,69 @@ NB_D float3 bsdf_sample_u(uint32_t lobes, const DevMaterial& m, const Frame& F, 
     }
     return f;
 }
+NB_OUTLINE float3 bsdf_eval_two(uint32_t lobes, const DevMaterial& m, const Frame& F, float3 woW,
+                                                    float3 wiW, uint32_t flags) {
+    return bsdf_eval_n(lobes, m, F, woW, wiW, flags);
+}
+NB_OUTLINE float bsdf_pdf_two(uint32_t lobes, const DevMaterial& m, const Frame& F, float3 woW,
+                                                  float3 wiW, uint32_t flags) {
+    return bsdf_pdf_n(lobes, m, F, woW, wiW, flags);
+}
+NB_OUTLINE float3 bsdf_sample_two(uint32_t lobes, const DevMaterial& m, const Frame& F,
+                                                      float3 woW, uint32_t flags, float ux, float uy, float3& wiW,
+                                                      float& pdf, uint32_t& stype) {
+    return bsdf_sample_n(lobes, m, F, woW, flags, ux, uy, wiW, pdf, stype);
+}
+
+// one lobe: the aggregation above with n <= 1, written out
+template <bool EXT = true>
+NB_D float3 bsdf_eval(uint32_t lobes, const DevMaterial& m, const Frame& F, const float3& woW, const float3& wiW,
+                      uint32_t flags) {
+    if (EXT && lobes > 0xFFFFu) return bsdf_eval_two(lobes, m, F, woW, wiW, flags);
+    const float3 wo = to_local(F, woW), wi = to_local(F, wiW);
+    const bool reflect = dot(wiW, F.ng) * dot(woW, F.ng) > 0.0f;
+    if (lobe_matches<EXT>(lobes, flags) && lobe_sided<EXT>(lobes, reflect)) return lobe_eval<EXT>(lobes, m, wo, wi);
+    return f3(0.0f);
+}
+template <bool EXT = true>
+NB_D float bsdf_pdf(uint32_t lobes, const DevMaterial& m, const Frame& F, const float3& woW, const float3& wiW,
+                    uint32_t flags) {
+    if (EXT && lobes > 0xFFFFu) return bsdf_pdf_two(lobes, m, F, woW, wiW, flags);
+    if (lobes == 0u) return 0.0f;
+    const float3 wo = to_local(F, woW), wi = to_local(F, wiW);
+    if (wo.z == 0.0f) return 0.0f;
+    return lobe_matches<EXT>(lobes, flags) ? lobe_pdf<EXT>(lobes, m, wo, wi) : 0.0f;
+}
+template <bool EXT = true>
+NB_D float3 bsdf_sample_u(uint32_t lobes, const DevMaterial& m, const Frame& F, const float3& woW, uint32_t flags,
+                          float ux, float uy, float3& wiW, float& pdf, uint32_t& stype) {
+    if (EXT && lobes > 0xFFFFu) return bsdf_sample_two(lobes, m, F, woW, flags, ux, uy, wiW, pdf, stype);
+    pdf = 0.0f;
+    stype = 0u;
+    if (!lobe_matches<EXT>(lobes, flags)) return f3(0.0f);
+    const float uxr = fminf(ux * 1.0f - 0.0f, kOneMinusEps);
+    const float3 wo = to_local(F, woW);
+    if (wo.z == 0.0f) return f3(0.0f);
+    float3 wi = f3(0.0f);
+    uint32_t st;
+    const float3 f = lobe_sample<EXT>(lobes, m, wo, uxr, uy, wi, pdf, st);
+    if (pdf == 0.0f) return f3(0.0f);
+    stype = st;
+    wiW = to_world(F, wi);
+    return f;
+}
 // draws two random numbers when a lobe matches
+template <bool EXT = true>
 NB_D float3 bsdf_sample(uint32_t lobes, const DevMaterial& m, const Frame& F, const float3& woW, uint32_t flags,
                         Rng& rng, float3& wiW, float& pdf, uint32_t& stype) {
-    if (lobes_matching(lobes, flags) == 0) {
+    if (EXT ? lobes_matching(lobes, flags) == 0 : !lobe_matches<false>(lobes, flags)) {
         pdf = 0.0f;
         stype = 0u;
         return f3(0.0f);
     }
     const float ux = rng.next();
     const float uy = rng.next();
-    return bsdf_sample_u(lobes, m, F, woW, flags, ux, uy, wiW, pdf, stype);
+    return bsdf_sample_u<EXT>(lobes, m, F, woW, flags, ux, uy, wiW, pdf, stype);
 }
 
 // ------------------------------------------------------------ sky & env
