@@ -396,6 +396,9 @@ NB_D void push_shadow(const WfDev& W, uint32_t slot, uint32_t which, const Shado
     W.sh_d[i] = make_float4(sr.d.x, sr.d.y, sr.d.z, 0.0f);
 }
 
+// EXT false: the queue holds no material with a lobe beyond Lambert,
+// conductor and Fresnel specular (those lobes' code is left out)
+template <bool EXT>
 __global__ void __launch_bounds__(256, NB_SHADE_MIN_BLOCKS) wf_shade(WfDev W, uint32_t kind) {
     const uint32_t n = W.counters[kind];
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -418,9 +421,9 @@ __global__ void __launch_bounds__(256, NB_SHADE_MIN_BLOCKS) wf_shade(WfDev W, ui
         rec.mtype = h2.y;
         Isect I;
         if (S.isect == NOOR_ISECT_WATERTIGHT)
-            make_isect<NOOR_ISECT_WATERTIGHT>(S, o, d, hw.x, rec, I);
+            make_isect<NOOR_ISECT_WATERTIGHT, EXT>(S, o, d, hw.x, rec, I);
         else
-            make_isect<NOOR_ISECT_REF_WALD>(S, o, d, hw.x, rec, I);
+            make_isect<NOOR_ISECT_REF_WALD, EXT>(S, o, d, hw.x, rec, I);
         const DevMaterial m = S.materials[I.mat];
         Rng rng{fbits(Lw.w)};
         int li = 0;
@@ -429,13 +432,13 @@ __global__ void __launch_bounds__(256, NB_SHADE_MIN_BLOCKS) wf_shade(WfDev W, ui
         // direct lighting: up to two contributions, each counted only if its
         // shadow ray comes back unblocked; the next regen adds
         // beta * (c0' + c1') to L as the megakernel does
-        const float3 c0 = light_sample_contrib(S, m, I, rng, S.mis != 0, li, picked, sr);
+        const float3 c0 = light_sample_contrib<EXT>(S, m, I, rng, S.mis != 0, li, picked, sr);
         const bool has0 = !is_black(c0);
         if (has0) push_shadow(W, slot, 0, sr);
         float3 c1 = f3(0.0f);
         bool has1 = false;
         if (S.mis && picked) {
-            c1 = bsdf_mis_contrib(S, m, I, rng, li, sr);
+            c1 = bsdf_mis_contrib<EXT>(S, m, I, rng, li, sr);
             has1 = !is_black(c1);
             if (has1) push_shadow(W, slot, 1, sr);
         }
@@ -451,7 +454,7 @@ __global__ void __launch_bounds__(256, NB_SHADE_MIN_BLOCKS) wf_shade(WfDev W, ui
         float3 wi;
         float pdf;
         uint32_t stype;
-        const float3 f = bsdf_sample(I.lobe, m, I.F, I.wo, BSDF_ALL, rng, wi, pdf, stype);
+        const float3 f = bsdf_sample<EXT>(I.lobe, m, I.F, I.wo, BSDF_ALL, rng, wi, pdf, stype);
         uint32_t st = kActive;
         if (pdf == 0.0f) {
             st = kFinishing;
@@ -627,6 +630,7 @@ struct WfLaunch {
     WfTravKernel extend;
     WfTravKernel shadow;
     DevScene scene;         // the launch's scene when every frame uses the same one
+    bool ext;               // some frame's scene has a material with lobes beyond the first three
 };
 
 // one iteration; with `ev` (6 events), records ev[0] before the first stage
@@ -641,7 +645,13 @@ static cudaError_t wf_iteration(const WfDev& W, const WfLaunch& L, cudaStream_t 
     if (ev) cudaEventRecord(ev[2], s);
     wf_bin<<<(W.cap + kBinBlock - 1) / kBinBlock, kBinBlock, 0, s>>>(W);
     const int nk = W.sort ? kKinds : 1;
-    for (int k = 0; k < nk; ++k) wf_shade<<<L.grid_queue, 256, 0, s>>>(W, (uint32_t)k);
+    for (int k = 0; k < nk; ++k) {
+        // sorted queues 0 and 1 hold Lambert and conductor hits only
+        if (L.ext && !(W.sort && k < 2))
+            wf_shade<true><<<L.grid_queue, 256, 0, s>>>(W, (uint32_t)k);
+        else
+            wf_shade<false><<<L.grid_queue, 256, 0, s>>>(W, (uint32_t)k);
+    }
     if (ev) cudaEventRecord(ev[3], s);
     L.shadow<<<L.grid_queue, L.block, L.smem, s>>>(W, L.scene);
     if (ev) cudaEventRecord(ev[4], s);
@@ -762,9 +772,11 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
     L.grid_queue = (uint32_t)std::max(1, C.sm_count) * 16;
     const uint32_t scene0 = frames[0].scene_id;
     bool multi = false, mixed = false;
-    for (uint32_t i = 1; i < n_frames; ++i) {
+    L.ext = false;
+    for (uint32_t i = 0; i < n_frames; ++i) {
         multi |= frames[i].scene_id != scene0;
         mixed |= C.scenes[frames[i].scene_id]->dev.isect != C.scenes[scene0]->dev.isect;
+        L.ext |= C.scenes[frames[i].scene_id]->dev.ext_lobes != 0u;
     }
     L.scene = C.scenes[scene0]->dev;
     if (mixed) {
@@ -791,7 +803,7 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
         uint64_t scene_hash = 1469598103934665603ull;  // FNV-1a over the scene parameter's bytes
         for (size_t b = 0; b < sizeof(DevScene); ++b)
             scene_hash = (scene_hash ^ reinterpret_cast<const unsigned char*>(&L.scene)[b]) * 1099511628211ull;
-        const uint64_t key[10] = {(uint64_t)W.cap | (uint64_t)W.sort << 32, W.total,
+        const uint64_t key[10] = {(uint64_t)W.cap | (uint64_t)W.sort << 32 | (uint64_t)L.ext << 33, W.total,
                                   (uint64_t)W.max_iters | (uint64_t)W.nframes << 32,
                                   (uint64_t)(uint32_t)W.stack_cap | (uint64_t)L.block << 32,
                                   (uint64_t)L.smem, (uint64_t)L.grid_slots | (uint64_t)L.grid_queue << 32,
