@@ -196,7 +196,7 @@ NB_D int direct_terms(const PathCtx& C, const DevMaterial& m0, const DevMaterial
         // the primal does), evaluation radiance below
         const float3 Li0 = sample_li(S, I, rng, nl, li, wi, to, lpdf);
         if (lpdf != 0.0f && !is_black(Li0)) {
-            const float3 f0 = bsdf_eval(I.lobe, m0, I.F, I.wo, wi, kNonSpecular);
+            const float3 f0 = bsdf_eval<false>(I.lobe, m0, I.F, I.wo, wi, kNonSpecular);
             if (!is_black(f0)) {
                 const ShadowRay sr{spawn_origin(I, wi, S.bias), wi, 0.0f};
                 const float tmax = length3(sr.o - to);
@@ -204,7 +204,7 @@ NB_D int direct_terms(const PathCtx& C, const DevMaterial& m0, const DevMaterial
                     Term& t = T[nt++];
                     t.f = lobe_value(I.lobe, me, I.F, I.wo, wi);
                     float w = 1.0f;
-                    if (S.mis) w = power_heuristic(lpdf, bsdf_pdf(I.lobe, m0, I.F, I.wo, wi, kNonSpecular));
+                    if (S.mis) w = power_heuristic(lpdf, bsdf_pdf<false>(I.lobe, m0, I.F, I.wo, wi, kNonSpecular));
                     t.s = absdot(wi, I.F.n) * w / lpdf;
                     t.env = li >= S.num_area_lights && S.sky_type == NOOR_SKY_HDR;
                     t.xscale = (float)nl;
@@ -224,7 +224,7 @@ NB_D int direct_terms(const PathCtx& C, const DevMaterial& m0, const DevMaterial
     float3 wi;
     float spdf;
     uint32_t stype;
-    const float3 f0 = bsdf_sample(I.lobe, m0, I.F, I.wo, kNonSpecular, rng, wi, spdf, stype);
+    const float3 f0 = bsdf_sample<false>(I.lobe, m0, I.F, I.wo, kNonSpecular, rng, wi, spdf, stype);
     if (is_black(f0) || spdf == 0.0f) return nt;
     float w = 1.0f;
     if (!(stype & BSDF_SPECULAR)) {
@@ -336,7 +336,7 @@ NB_D float3 replay(const PathCtx& C, uint32_t pix, uint32_t frame, const DevCame
             break;
         }
         Isect I;
-        make_isect<ISECT>(S, o, d, tmax, rec, I);
+        make_isect<ISECT, false>(S, o, d, tmax, rec, I);
         if (I.mtype & kEmitterMat) {
             if (bounce == 0 || spec) {
                 if (I.mtype & NOOR_MESHLIGHT) {
@@ -366,7 +366,7 @@ NB_D float3 replay(const PathCtx& C, uint32_t pix, uint32_t frame, const DevCame
         float3 wi;
         float pdf;
         uint32_t stype;
-        const float3 f0 = bsdf_sample(I.lobe, m0, I.F, I.wo, BSDF_ALL, rng, wi, pdf, stype);
+        const float3 f0 = bsdf_sample<false>(I.lobe, m0, I.F, I.wo, BSDF_ALL, rng, wi, pdf, stype);
         if (pdf == 0.0f) break;
         float3 fe;
         FDeriv fd{f3(0.0f), f3(0.0f), 0.0f};
