@@ -124,8 +124,12 @@ typedef struct noor_shape {
     float radius;
     float radius2;
     int32_t light_idx;
-    int32_t type;               /* NOOR_SHAPE_* ; only QUAD is implemented */
+    int32_t type;               /* NOOR_SHAPE_*: QUAD, SPHERE or DISK      */
 } noor_shape;
+/* The fields hold what the CudaShape constructor (shape.cuh:44-69) leaves:
+ * radius = min(|u|, |v|) / 2; for SPHERE and DISK the center is moved to
+ * center + (u + v) / 2 and area = 4 pi r^2 (sphere) or pi r^2 (disk); for
+ * QUAD area = |u x v|.  n is the quad / disk normal. */
 
 /* CudaAreaLight, noor/cuda/light.cuh:76-121 */
 typedef struct noor_area_light {
@@ -133,6 +137,32 @@ typedef struct noor_area_light {
     float ke[3];
     int32_t two_sided;
 } noor_area_light;
+
+/* CudaPointLight, noor/cuda/light.cuh:158-178 (CudaLight::_ke first) */
+typedef struct noor_point_light {
+    float ke[3];
+    float position[3];
+} noor_point_light;
+
+/* CudaSpotLight, noor/cuda/light.cuh:180-214.  falloff() compares
+ * `direction` with the direction from the shaded point TO the light:
+ * cos >= cos_inner gives 1, cos < cos_outer 0, between ((cos - cos_outer) /
+ * (cos_inner - cos_outer))^4. */
+typedef struct noor_spot_light {
+    float ke[3];
+    float position[3];
+    float direction[3];
+    float cos_inner;
+    float cos_outer;
+} noor_spot_light;
+
+/* CudaDistantLight, noor/cuda/light.cuh:216-238: `direction` points from
+ * the scene towards the light and is a unit vector (the constructor
+ * normalises it; noor_build_payload does the same for its input). */
+typedef struct noor_distant_light {
+    float ke[3];
+    float direction[3];
+} noor_distant_light;
 
 /* ImageTexture entry of CudaPayload::_textures: constant material
  * parameters are 1x1 textures; the environment texture is the LAST entry
@@ -198,11 +228,16 @@ typedef struct noor_payload {
     uint32_t num_bvh_nodes;
     const noor_texture* textures;
     uint32_t num_textures;
+    /* lights, indexed in this order: area, point, spot, distant, infinite
+     * (setup_lights, noor/cuda/lightimp.cuh:244-281) */
     const noor_area_light* area_lights;
     int32_t num_area_lights;
-    int32_t num_point_lights;            /* must be 0 (not implemented)       */
-    int32_t num_spot_lights;             /* must be 0                         */
-    int32_t num_distant_lights;          /* must be 0                         */
+    const noor_point_light* point_lights;
+    int32_t num_point_lights;
+    const noor_spot_light* spot_lights;
+    int32_t num_spot_lights;
+    const noor_distant_light* distant_lights;
+    int32_t num_distant_lights;
     int32_t num_infinite_lights;         /* 0 or 1                            */
     const noor_material* materials;
     uint32_t num_materials;
@@ -299,7 +334,8 @@ int noor_device_count(int* count);
 /* sizeof of the ABI structs, in declaration order: shape, area_light,
  * texture, material, payload, camera, hosek_state, hosek_sky, spec, ray,
  * hit, bvh_spec, mesh, material_desc, scene_desc, build_stat, wf_frame,
- * wf_params, adjoint_desc.  Returns how many were written (<= n). */
+ * wf_params, adjoint_desc, wf_profile, point_light, spot_light,
+ * distant_light.  Returns how many were written (<= n). */
 int noor_abi_sizes(uint32_t* out, int n);
 
 /* Render frames *frame_count .. *frame_count+n_frames-1 in one launch of the
@@ -385,7 +421,9 @@ typedef struct noor_bvh_spec {
 
 /* Mesh, noor/header/assetLoader.h:45-101.  to_global is column-major
  * (glm::mat4 layout).  instance >= 0 makes this an instance of that source
- * mesh; light_idx >= 0 makes it a light node over area light light_idx. */
+ * mesh; light_idx >= 0 makes it a light node over area light light_idx
+ * (tri_count 0; its bounds are the light shape's, and it gets an empty
+ * bottom-level leaf starting at tri_start, as in the reference). */
 typedef struct noor_mesh {
     uint32_t tri_start;
     uint32_t tri_count;
@@ -434,6 +472,12 @@ typedef struct noor_scene_desc {
     uint32_t num_materials;
     const noor_area_light* area_lights;
     uint32_t num_area_lights;
+    const noor_point_light* point_lights;
+    uint32_t num_point_lights;
+    const noor_spot_light* spot_lights;
+    uint32_t num_spot_lights;
+    const noor_distant_light* distant_lights;
+    uint32_t num_distant_lights;
     int32_t skydome_type;           /* NOOR_SKY_*                            */
     int32_t env_width;              /* HDR environment map (skydome_type 0)  */
     int32_t env_height;

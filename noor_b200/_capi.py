@@ -38,6 +38,7 @@ NOOR_SKY_HDR, NOOR_SKY_PHYSICAL, NOOR_SKY_CONSTANT = 0, 1, 2
 NOOR_LIGHT_SKY_MASK = 0x20
 NOOR_ISECT_WATERTIGHT, NOOR_ISECT_REF_WALD = 0, 1
 NOOR_FILM_KAHAN, NOOR_FILM_REF_LERP = 0, 1
+NOOR_SHAPE_QUAD, NOOR_SHAPE_SPHERE, NOOR_SHAPE_DISK = 0, 1, 2
 NOOR_DEV_STACK_OVERFLOW = 1
 
 TRI_LEAF_MASK = 0x80000000
@@ -53,6 +54,19 @@ class Shape(C.Structure):
 
 class AreaLight(C.Structure):
     _fields_ = [("shape", Shape), ("ke", f32 * 3), ("two_sided", i32)]
+
+
+class PointLight(C.Structure):
+    _fields_ = [("ke", f32 * 3), ("position", f32 * 3)]
+
+
+class SpotLight(C.Structure):
+    _fields_ = [("ke", f32 * 3), ("position", f32 * 3), ("direction", f32 * 3), ("cos_inner", f32),
+                ("cos_outer", f32)]
+
+
+class DistantLight(C.Structure):
+    _fields_ = [("ke", f32 * 3), ("direction", f32 * 3)]
 
 
 class Texture(C.Structure):
@@ -77,9 +91,10 @@ class Payload(C.Structure):
                 ("wald_bnu_bnv_au_av", pu), ("wald_cnu_cnv_deg_mat", pu), ("bvh_root_node", u32),
                 ("bvh_min_right_start", pu), ("bvh_max_axis_count", pu), ("num_bvh_nodes", u32),
                 ("textures", C.POINTER(Texture)), ("num_textures", u32), ("area_lights", C.POINTER(AreaLight)),
-                ("num_area_lights", i32), ("num_point_lights", i32), ("num_spot_lights", i32),
-                ("num_distant_lights", i32), ("num_infinite_lights", i32), ("materials", C.POINTER(Material)),
-                ("num_materials", u32)]
+                ("num_area_lights", i32), ("point_lights", C.POINTER(PointLight)), ("num_point_lights", i32),
+                ("spot_lights", C.POINTER(SpotLight)), ("num_spot_lights", i32),
+                ("distant_lights", C.POINTER(DistantLight)), ("num_distant_lights", i32),
+                ("num_infinite_lights", i32), ("materials", C.POINTER(Material)), ("num_materials", u32)]
 
 
 class Camera(C.Structure):
@@ -138,7 +153,10 @@ class SceneDesc(C.Structure):
                 ("num_uvs", u32), ("vindices", pu), ("nindices", pu), ("uvindices", pu), ("material_indices", pu),
                 ("num_triangles", u32), ("meshes", C.POINTER(Mesh)), ("num_meshes", u32),
                 ("materials", C.POINTER(MaterialDesc)), ("num_materials", u32),
-                ("area_lights", C.POINTER(AreaLight)), ("num_area_lights", u32), ("skydome_type", i32),
+                ("area_lights", C.POINTER(AreaLight)), ("num_area_lights", u32),
+                ("point_lights", C.POINTER(PointLight)), ("num_point_lights", u32),
+                ("spot_lights", C.POINTER(SpotLight)), ("num_spot_lights", u32),
+                ("distant_lights", C.POINTER(DistantLight)), ("num_distant_lights", u32), ("skydome_type", i32),
                 ("env_width", i32), ("env_height", i32), ("env_rgba", pf), ("bvh", BvhSpec)]
 
 
@@ -220,7 +238,8 @@ PROTOTYPES = {
 
 
 ABI_STRUCTS = [Shape, AreaLight, Texture, Material, Payload, Camera, HosekState, HosekSky, Spec, Ray, Hit, BvhSpec,
-               Mesh, MaterialDesc, SceneDesc, BuildStat, WfFrame, WfParams, AdjointDesc, WfProfile]
+               Mesh, MaterialDesc, SceneDesc, BuildStat, WfFrame, WfParams, AdjointDesc, WfProfile, PointLight,
+               SpotLight, DistantLight]
 
 
 class NoorError(RuntimeError):

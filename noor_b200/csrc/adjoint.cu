@@ -200,7 +200,7 @@ NB_D int direct_terms(const PathCtx& C, const DevMaterial& m0, const DevMaterial
             if (!is_black(f0)) {
                 const ShadowRay sr{spawn_origin(I, wi, S.bias), wi, 0.0f};
                 const float tmax = length3(sr.o - to);
-                if (!trace_any<ISECT>(S, sr.o, sr.d, tmax, C.st, C.status)) {
+                if (!trace_any<ISECT, false>(S, sr.o, sr.d, tmax, C.st, C.status)) {
                     Term& t = T[nt++];
                     t.f = lobe_value(I.lobe, me, I.F, I.wo, wi);
                     float w = 1.0f;
@@ -250,7 +250,7 @@ NB_D int direct_terms(const PathCtx& C, const DevMaterial& m0, const DevMaterial
     float3 vwi;
     visibility(I.p, to, vwi);
     const float3 so2 = spawn_origin(I, vwi, S.bias);
-    if (trace_any<ISECT>(S, so2, vwi, length3(so2 - to), C.st, C.status)) return nt;
+    if (trace_any<ISECT, false>(S, so2, vwi, length3(so2 - to), C.st, C.status)) return nt;
     Term& t = T[nt++];
     t.f = lobe_value(I.lobe, me, I.F, I.wo, wi);
     t.s = absdot(wi, I.F.n) * w / spdf;
@@ -309,7 +309,7 @@ NB_D float3 replay(const PathCtx& C, uint32_t pix, uint32_t frame, const DevCame
     for (uint32_t bounce = 0; bounce < S.bounces; ++bounce) {
         float tmax = kInf;
         HitRec rec;
-        if (!trace_closest<ISECT>(S, o, d, tmax, rec, C.st, C.status)) {
+        if (!trace_closest<ISECT, false>(S, o, d, tmax, rec, C.st, C.status)) {
             if (S.sky_on && (bounce == 0 || spec)) {
                 const float3 dir = normalize_fast(d);
                 float3 Le;
@@ -509,6 +509,8 @@ static int adjoint_run(const noor_adjoint_desc* desc, int mode, float* image, co
             l != kLobeFresnelSpec)
             return set_error(NOOR_ERR_UNSUPPORTED, "adjoint: materials other than diffuse, metal and glass");
     }
+    if (!st.quad_lights_only || S.num_delta_lights > 0)
+        return set_error(NOOR_ERR_UNSUPPORTED, "adjoint: lights other than quad area lights and the sky");
     if (S.sky_type == NOOR_SKY_HDR && (!desc->d_env || (mode == 1 && !g_env)))
         return set_error(NOOR_ERR_INVALID, "adjoint: env buffer missing");
     if (desc->width != C->cam.w || desc->height != C->cam.h)

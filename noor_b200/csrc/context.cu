@@ -95,10 +95,12 @@ static int validate_payload(const noor_payload* P) {
         !P->vertices || !P->normals || !P->uvs || P->num_vertices == 0)
         return set_error(NOOR_ERR_INVALID, "payload: missing geometry or BVH arrays");
     if (P->bvh_root_node >= P->num_bvh_nodes) return set_error(NOOR_ERR_INVALID, "payload: BVH root out of range");
-    if (P->num_point_lights || P->num_spot_lights || P->num_distant_lights)
-        return set_error(NOOR_ERR_UNSUPPORTED, "payload: point, spot and distant lights are not implemented");
     if (P->num_area_lights < 0 || (P->num_area_lights > 0 && !P->area_lights))
         return set_error(NOOR_ERR_INVALID, "payload: bad area light array");
+    if (P->num_point_lights < 0 || (P->num_point_lights > 0 && !P->point_lights) || P->num_spot_lights < 0 ||
+        (P->num_spot_lights > 0 && !P->spot_lights) || P->num_distant_lights < 0 ||
+        (P->num_distant_lights > 0 && !P->distant_lights))
+        return set_error(NOOR_ERR_INVALID, "payload: bad point, spot or distant light array");
     if (P->num_infinite_lights < 0 || P->num_infinite_lights > 1)
         return set_error(NOOR_ERR_INVALID, "payload: at most one infinite light");
     if (P->num_materials == 0 || !P->materials) return set_error(NOOR_ERR_INVALID, "payload: no materials");
@@ -128,9 +130,13 @@ static int validate_payload(const noor_payload* P) {
                                                        "types) is not implemented");
         if (m.distribution > 1u) return set_error(NOOR_ERR_INVALID, "payload: unknown microfacet distribution");
     }
-    for (int i = 0; i < P->num_area_lights; ++i)
-        if (P->area_lights[i].shape.type != NOOR_SHAPE_QUAD)
-            return set_error(NOOR_ERR_UNSUPPORTED, "payload: only quad area lights are implemented");
+    for (int i = 0; i < P->num_area_lights; ++i) {
+        const noor_shape& sh = P->area_lights[i].shape;
+        if (sh.type != NOOR_SHAPE_QUAD && sh.type != NOOR_SHAPE_SPHERE && sh.type != NOOR_SHAPE_DISK)
+            return set_error(NOOR_ERR_INVALID, "payload: unknown area light shape type");
+        if (sh.type != NOOR_SHAPE_QUAD && !(sh.radius > 0.0f))
+            return set_error(NOOR_ERR_INVALID, "payload: sphere or disk light without a radius");
+    }
     // attribute and node indices
     for (size_t i = 0; i < (size_t)P->num_triangles; ++i) {
         const uint32_t* a = P->attribute_indices + 4 * i;
@@ -277,6 +283,7 @@ int upload_scene(Context& C, const noor_payload* P, const noor_hosek_sky* H, con
     }
     {
         std::vector<DevAreaLight> l(P->num_area_lights);
+        st.quad_lights_only = true;
         for (int i = 0; i < P->num_area_lights; ++i) {
             const noor_area_light& a = P->area_lights[i];
             std::memset(&l[i], 0, sizeof(DevAreaLight));
@@ -288,15 +295,56 @@ int upload_scene(Context& C, const noor_payload* P, const noor_hosek_sky* H, con
             l[i].ke = make_float3(a.ke[0], a.ke[1], a.ke[2]);
             l[i].two_sided = a.two_sided;
             l[i].type = a.shape.type;
+            l[i].radius = a.shape.radius;
+            l[i].radius2 = a.shape.radius2;
+            if (a.shape.type != NOOR_SHAPE_QUAD) {
+                st.quad_lights_only = false;
+                D.ext_lights = 1u;
+            }
         }
         if ((rc = st.upload((void**)&D.area_lights, l.data(), l.size() * sizeof(DevAreaLight), "area lights"))) return rc;
+    }
+    {
+        // point, spot and distant lights in one array, in light-index order
+        std::vector<DevDeltaLight> l;
+        auto v = [](const float* x) { return make_float3(x[0], x[1], x[2]); };
+        for (int i = 0; i < P->num_point_lights; ++i) {
+            DevDeltaLight d{};
+            d.kind = kDeltaPoint;
+            d.pos = v(P->point_lights[i].position);
+            d.ke = v(P->point_lights[i].ke);
+            l.push_back(d);
+        }
+        for (int i = 0; i < P->num_spot_lights; ++i) {
+            const noor_spot_light& sl = P->spot_lights[i];
+            DevDeltaLight d{};
+            d.kind = kDeltaSpot;
+            d.pos = v(sl.position);
+            d.dir = v(sl.direction);
+            d.ke = v(sl.ke);
+            d.cos_inner = sl.cos_inner;
+            d.cos_outer = sl.cos_outer;
+            l.push_back(d);
+        }
+        for (int i = 0; i < P->num_distant_lights; ++i) {
+            DevDeltaLight d{};
+            d.kind = kDeltaDistant;
+            d.dir = v(P->distant_lights[i].direction);
+            d.ke = v(P->distant_lights[i].ke);
+            l.push_back(d);
+        }
+        if (!l.empty() &&
+            (rc = st.upload((void**)&D.delta_lights, l.data(), l.size() * sizeof(DevDeltaLight), "delta lights")))
+            return rc;
+        D.num_delta_lights = (int)l.size();
+        if (!l.empty()) D.ext_lights = 1u;
     }
     D.num_nodes = (uint32_t)nn;
     D.num_tris = (uint32_t)nt;
     D.num_instances = (uint32_t)ni;
     D.num_materials = P->num_materials;
     D.num_area_lights = P->num_area_lights;
-    D.num_lights = P->num_area_lights + P->num_infinite_lights;
+    D.num_lights = P->num_area_lights + D.num_delta_lights + P->num_infinite_lights;
     // environment texture (last texture)
     const noor_texture& env = P->textures[P->num_textures - 1];
     D.env_w = env.width;
@@ -640,7 +688,8 @@ extern "C" int noor_abi_sizes(uint32_t* out, int n) {
                           sizeof(noor_spec), sizeof(noor_ray), sizeof(noor_hit), sizeof(noor_bvh_spec),
                           sizeof(noor_mesh), sizeof(noor_material_desc), sizeof(noor_scene_desc),
                           sizeof(noor_build_stat), sizeof(noor_wf_frame), sizeof(noor_wf_params),
-                          sizeof(noor_adjoint_desc), sizeof(noor_wf_profile)};
+                          sizeof(noor_adjoint_desc), sizeof(noor_wf_profile), sizeof(noor_point_light),
+                          sizeof(noor_spot_light), sizeof(noor_distant_light)};
     const int k = (int)(sizeof(s) / sizeof(s[0]));
     int w = 0;
     for (; out && w < n && w < k; ++w) out[w] = s[w];

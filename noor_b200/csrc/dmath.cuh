@@ -10,6 +10,17 @@
 
 #define NB_HD __host__ __device__ __forceinline__
 #define NB_D __device__ __forceinline__
+// code of the BSDF lobes beyond Lambert, conductor and Fresnel specular is
+// kept out of line, so that kernels built with it spend no registers on it
+// until a scene uses it
+#ifndef NB_LOBE_OUTLINE
+#define NB_LOBE_OUTLINE 1
+#endif
+#if NB_LOBE_OUTLINE
+#define NB_OUTLINE static __device__ __noinline__
+#else
+#define NB_OUTLINE NB_D
+#endif
 
 namespace nb {
 

@@ -44,24 +44,129 @@ NB_D void visibility(const float3& from, const float3& to, float3& wi) {
     wi = v / dist;
 }
 
-// light pick + sample_Li (noor/cuda/lightimp.cuh:412-453, 97-108, 175-187)
+// CudaAreaLight::Le (noor/cuda/lightimp.cuh:29-36): a sphere emits on
+// both sides, a quad or disk towards -n unless two-sided; w is the
+// direction of the ray arriving at the light
+template <bool EXT = true>
+NB_D float3 area_le(const DevAreaLight& A, const float3& w) {
+    if (EXT && A.type == NOOR_SHAPE_SPHERE) return A.ke;
+    return (A.two_sided || dot(w, A.n) < 0.0f) ? A.ke : f3(0.0f);
+}
+
+template <bool EXT = true>
+NB_D bool is_delta_light(const DevScene& S, int li) {
+    return EXT && li >= S.num_area_lights && li < S.num_area_lights + S.num_delta_lights;
+}
+
+// sampleQuad / sampleSphere / sampleDisk (noor/cuda/geometry.cuh:27-103):
+// a point p on the shape (offset by the reflection bias along its normal)
+// and the pdf of reaching it from I.p.  For quads and disks that pdf is the
+// reference's dist^2 / (|n . w| area) with w = P - p NOT normalised
+// (geometry.cuh:37-38, 98-100), i.e. the solid-angle pdf divided by the
+// distance: those lights come out brighter by the distance to them.  Kept
+// as is, since the point is the reference's image; the MIS pdf of the same
+// lights (light_pdf) uses the unit direction, as the reference's does.
+NB_D float3 curved_sample(const DevAreaLight& A, float bias, const float3& P, Rng& rng, float& pdf) {
+    if (A.type == NOOR_SHAPE_SPHERE) {
+        // uniform cone of directions towards the sphere (pbrt's method);
+        // the sampled point is rescaled as the reference does (p, not
+        // p - center, scaled by radius / |p - center|)
+        const float r1 = rng.next();
+        const float r2 = rng.next();
+        const float3 w = normalize_fast(A.center - P);
+        float3 u, v;
+        coordinate_system(w, u, v);
+        const float sin2max = A.radius2 / length2(P - A.center);
+        const float cosmax = sqrtf(fmaxf(0.0f, 1.0f - sin2max));
+        const float ct = (1.0f - r1) + r1 * cosmax;
+        const float st = sqrtf(fmaxf(0.0f, 1.0f - ct * ct));
+        const float phi = r2 * k2Pi;
+        const float dc = length3(P - A.center);
+        const float ds = dc * ct - sqrtf(fmaxf(0.0f, A.radius2 - dc * dc * st * st));
+        const float ca = (dc * dc + A.radius2 - ds * ds) / (2.0f * dc * A.radius);
+        const float sa = sqrtf(fmaxf(0.0f, 1.0f - ca * ca));
+        const float3 N = sa * cosf(phi) * (-1.0f * u) + sa * sinf(phi) * (-1.0f * v) + ca * (-1.0f * w);
+        float3 p = A.center + A.radius * N;
+        p *= A.radius / length3(p - A.center);
+        p += bias * N;
+        pdf = kInv2Pi / (1.0f - cosmax);
+        return p;
+    }
+    const float ux = rng.next();
+    const float uy = rng.next();
+    const float2 cd = concentric_disk(ux, uy);
+    const float px = cd.x * A.radius, py = cd.y * A.radius;
+    float3 u, v;
+    coordinate_system(A.n, u, v);
+    const float3 p = px * u + py * v + 0.0f * A.n + A.center + bias * A.n;
+    const float3 w = P - p;
+    pdf = length2(w) / (absdot(A.n, -1.0f * w) * A.area);
+    if (isinf(pdf)) pdf = 0.0f;
+    return p;
+}
+template <bool EXT = true>
+NB_D float3 area_sample(const DevScene& S, const DevAreaLight& A, const float3& P, Rng& rng, float& pdf) {
+    if (EXT && A.type != NOOR_SHAPE_QUAD) return curved_sample(A, S.bias, P, rng, pdf);
+    const float r1 = rng.next();
+    const float r2 = rng.next();
+    const float3 p = A.center + A.u * r1 + A.v * r2 + S.bias * A.n;
+    const float3 w = P - p;
+    pdf = length2(w) / (absdot(A.n, -1.0f * w) * A.area);
+    if (isinf(pdf)) pdf = 0.0f;
+    return p;
+}
+
+// point / spot / distant sample_Li (lightimp.cuh:191-241): pdf 1, or 0
+// when the light gives nothing
+NB_D float3 delta_sample(const DevDeltaLight& D, float world_radius, const float3& P, float3& to, float3& wi,
+                               float& pdf) {
+    pdf = 1.0f;
+    if (D.kind == kDeltaDistant) {
+        to = P + 2.0f * world_radius * D.dir;
+        visibility(P, to, wi);
+        return D.ke;
+    }
+    to = D.pos;
+    visibility(P, to, wi);
+    const float dist2 = length2(to - P);
+    if (dist2 == 0.0f) {
+        pdf = 0.0f;
+        return f3(0.0f);
+    }
+    if (D.kind != kDeltaSpot) return D.ke / dist2;
+    // CudaSpotLight::falloff (light.cuh:198-206)
+    const float c = dot(D.dir, wi);
+    float fo = 1.0f;
+    if (c < D.cos_outer) {
+        fo = 0.0f;
+    } else if (c < D.cos_inner) {
+        const float dl = (c - D.cos_outer) / (D.cos_inner - D.cos_outer);
+        fo = (dl * dl) * (dl * dl);
+    }
+    if (fo == 0.0f) {
+        pdf = 0.0f;
+        return f3(0.0f);
+    }
+    return D.ke * fo / dist2;
+}
+
+// light pick + sample_Li (noor/cuda/lightimp.cuh:412-453; area 97-108,
+// infinite 175-187).  EXT false: quad area lights and the infinite light only
+template <bool EXT = true>
 NB_D float3 sample_li(const DevScene& S, const Isect& I, Rng& rng, int nl, int li, float3& wi, float3& to,
                       float& pdf) {
     float3 Li = f3(0.0f);
     pdf = 0.0f;
     if (li < S.num_area_lights) {
         const DevAreaLight& A = S.area_lights[li];
-        const float r1 = rng.next();
-        const float r2 = rng.next();
-        const float3 p = A.center + A.u * r1 + A.v * r2 + S.bias * A.n;
-        const float3 w = I.p - p;
-        const float dist2 = length2(w);
-        pdf = dist2 / (absdot(A.n, -1.0f * w) * A.area);
-        if (isinf(pdf)) pdf = 0.0f;
+        const float3 p = area_sample<EXT>(S, A, I.p, rng, pdf);
         if (pdf == 0.0f) return f3(0.0f);
         to = p;
         visibility(I.p, to, wi);
-        Li = (A.two_sided || dot(wi, A.n) < 0.0f) ? A.ke : f3(0.0f);
+        Li = area_le<EXT>(A, wi);
+    } else if (is_delta_light<EXT>(S, li)) {
+        Li = delta_sample(S.delta_lights[li - S.num_area_lights], S.world_radius, I.p, to, wi, pdf);
+        if (pdf == 0.0f) return f3(0.0f);
     } else {
         const float3 dir = env_sample_dir(S, rng, pdf);
         if (isinf(pdf) || isnan(pdf)) pdf = 0.0f;
@@ -73,16 +178,36 @@ NB_D float3 sample_li(const DevScene& S, const Isect& I, Rng& rng, int nl, int l
     return Li * (float)nl;
 }
 
-// pdf_Li of light li for direction wi (lightimp.cuh:89-95,161-173; shapeimp.cuh:28-52)
+NB_D float curved_pdf(const DevAreaLight& A, const float3& P, const float3& wi) {
+    if (A.type == NOOR_SHAPE_SPHERE) {
+        const float sin2max = A.radius2 / length2(P - A.center);
+        const float cosmax = sqrtf(fmaxf(0.0f, 1.0f - sin2max));
+        return kInv2Pi / (1.0f - cosmax);
+    }
+    float tm = kInf;
+    if (!disk_hit(A, P, wi, tm)) return 0.0f;
+    const float3 p = P + tm * wi;
+    return length2(p - P) / (absdot(A.n, -1.0f * wi) * A.area);
+}
+
+// pdf_Li of light li for direction wi (lightimp.cuh:89-95,161-173;
+// shapeimp.cuh:28-52); delta lights are never asked
+template <bool EXT = true>
 NB_D float light_pdf(const DevScene& S, const Isect& I, int li, const float3& wi) {
     float pdf = 0.0f;
     if (li < S.num_area_lights) {
         const DevAreaLight& A = S.area_lights[li];
-        float tm = kInf;
-        if (!quad_hit(A, I.p, wi, tm)) return 0.0f;
-        const float3 p = I.p + tm * wi;
-        pdf = length2(p - I.p) / (absdot(A.n, -1.0f * wi) * A.area);
+        if (EXT && A.type != NOOR_SHAPE_QUAD) {
+            pdf = curved_pdf(A, I.p, wi);
+        } else {
+            float tm = kInf;
+            if (!quad_hit(A, I.p, wi, tm)) return 0.0f;
+            const float3 p = I.p + tm * wi;
+            pdf = length2(p - I.p) / (absdot(A.n, -1.0f * wi) * A.area);
+        }
         if (isinf(pdf)) pdf = 0.0f;
+    } else if (is_delta_light<EXT>(S, li)) {
+        pdf = 0.0f;
     } else {
         pdf = env_pdf(S, wi);
     }
@@ -113,7 +238,7 @@ NB_D float3 light_sample_contrib(const DevScene& S, const DevMaterial& m, const 
     picked = true;
     float3 wi, to;
     float lpdf;
-    const float3 Li = sample_li(S, I, rng, nl, li, wi, to, lpdf);
+    const float3 Li = sample_li<EXT>(S, I, rng, nl, li, wi, to, lpdf);
     if (lpdf == 0.0f || is_black(Li)) return f3(0.0f);
     float3 f = bsdf_eval<EXT>(I.lobe, m, I.F, I.wo, wi, kNonSpecular);
     if (is_black(f)) return f3(0.0f);
@@ -121,7 +246,7 @@ NB_D float3 light_sample_contrib(const DevScene& S, const DevMaterial& m, const 
     sr.o = spawn_origin(I, wi, S.bias);
     sr.d = wi;
     sr.tmax = length3(sr.o - to);
-    if (!mis) return Li * f / lpdf;
+    if (!mis || is_delta_light<EXT>(S, li)) return Li * f / lpdf;
     const float spdf = bsdf_pdf<EXT>(I.lobe, m, I.F, I.wo, wi, kNonSpecular);
     const float w = power_heuristic(lpdf, spdf);
     return Li * f * w / lpdf;
@@ -132,6 +257,7 @@ template <bool EXT = true>
 NB_D float3 bsdf_mis_contrib(const DevScene& S, const DevMaterial& m, const Isect& I, Rng& rng, int li,
                              ShadowRay& sr) {
     const uint32_t flags = (I.mtype & kSpecularMat) ? BSDF_ALL : kNonSpecular;
+    if (is_delta_light<EXT>(S, li)) return f3(0.0f);  // before any draw (direct.cuh:77)
     rng.next();  // two draws the reference makes and never reads (direct.cuh:79)
     rng.next();
     float3 wi;
@@ -142,7 +268,7 @@ NB_D float3 bsdf_mis_contrib(const DevScene& S, const DevMaterial& m, const Isec
     f *= absdot(wi, I.F.n);
     float w = 1.0f;
     if (!(stype & BSDF_SPECULAR)) {
-        const float lp = light_pdf(S, I, li, wi);
+        const float lp = light_pdf<EXT>(S, I, li, wi);
         if (lp == 0.0f) return f3(0.0f);
         w = power_heuristic(spdf, lp);
     }
@@ -152,8 +278,8 @@ NB_D float3 bsdf_mis_contrib(const DevScene& S, const DevMaterial& m, const Isec
     float3 Le;
     if (li < S.num_area_lights) {
         const DevAreaLight& A = S.area_lights[li];
-        lh = quad_hit(A, so, wi, tm);
-        Le = (A.two_sided || dot(wi, A.n) < 0.0f) ? A.ke : f3(0.0f);
+        lh = shape_hit<EXT>(A, so, wi, tm);
+        Le = area_le<EXT>(A, wi);
     } else {
         lh = S.sky_on != 0;
         Le = S.sky_on ? env_eval(S, wi) : f3(0.0f);
@@ -208,7 +334,7 @@ NB_D float3 path_radiance(const DevScene& S, float3 o, float3 d, Rng& rng, const
         float tmax = kInf;
         HitRec rec;
         rs.ext++;
-        if (!trace_closest<ISECT>(S, o, d, tmax, rec, st, status)) {
+        if (!trace_closest<ISECT, EXT>(S, o, d, tmax, rec, st, status)) {
             if (S.sky_on && (bounce == 0 || spec_bounce)) L += beta * env_eval(S, normalize_fast(d));
             break;
         }
@@ -221,8 +347,7 @@ NB_D float3 path_radiance(const DevScene& S, float3 o, float3 d, Rng& rng, const
         if (I.mtype & kEmitterMat) {
             if (bounce == 0 || spec_bounce) {
                 if (I.mtype & NOOR_MESHLIGHT) {
-                    const DevAreaLight& A = S.area_lights[rec.ins];
-                    L += beta * ((A.two_sided || dot(d, A.n) < 0.0f) ? A.ke : f3(0.0f));
+                    L += beta * area_le<EXT>(S.area_lights[rec.ins], d);
                 } else {
                     const DevMaterial& em = S.materials[I.mat];
                     L += beta * (em.emitter_scale * em.emittance);
@@ -239,13 +364,13 @@ NB_D float3 path_radiance(const DevScene& S, float3 o, float3 d, Rng& rng, const
         float3 Ld = light_sample_contrib<EXT>(S, m, I, rng, S.mis != 0, li, picked, sr);
         if (!is_black(Ld)) {
             rs.shadow++;
-            if (trace_any<ISECT>(S, sr.o, sr.d, sr.tmax, st, status)) Ld = f3(0.0f);
+            if (trace_any<ISECT, EXT>(S, sr.o, sr.d, sr.tmax, st, status)) Ld = f3(0.0f);
         }
         if (S.mis && picked) {
             float3 c = bsdf_mis_contrib<EXT>(S, m, I, rng, li, sr);
             if (!is_black(c)) {
                 rs.shadow++;
-                if (trace_any<ISECT>(S, sr.o, sr.d, sr.tmax, st, status)) c = f3(0.0f);
+                if (trace_any<ISECT, EXT>(S, sr.o, sr.d, sr.tmax, st, status)) c = f3(0.0f);
             }
             Ld += c;
         }

@@ -276,8 +276,9 @@ cudaError_t launch_megakernel(const DevScene& S, const DevCamera& C, const MegaA
     const uint32_t grid = (uint32_t)((threads + kMegaBlock - 1) / kMegaBlock);
     const size_t sm = stack_bytes(S, kMegaBlock);
     cudaError_t e;
-    // scenes without the extra lobes run a specialisation without their code
-    // (the kernel's registers are capped, so unused branches cost spills)
+    // scenes without the extra lobes and lights run a specialisation without
+    // their code (the kernel's registers are capped, so unused branches cost
+    // spills)
 #define NB_MK2(I, F, X)                                                                         \
     do {                                                                                        \
         e = cudaFuncSetAttribute(megakernel<I, F, X>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm); \
@@ -286,7 +287,7 @@ cudaError_t launch_megakernel(const DevScene& S, const DevCamera& C, const MegaA
     } while (0)
 #define NB_MK(I, F)                     \
     do {                                \
-        if (S.ext_lobes) NB_MK2(I, F, true); \
+        if (S.ext_lobes || S.ext_lights) NB_MK2(I, F, true); \
         else NB_MK2(I, F, false);       \
     } while (0)
     if (S.isect == NOOR_ISECT_WATERTIGHT) {

@@ -14,6 +14,7 @@ struct SceneState {
     EnvBuild env{};
     std::vector<void*> allocs;
     std::vector<DevMaterial> materials_host;
+    bool quad_lights_only = true;   // every area light a quad
     int sky_type = 0;
     uint32_t max_mesh_leaf = 0;
     ~SceneState();

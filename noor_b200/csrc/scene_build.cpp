@@ -320,9 +320,23 @@ public:
                 V3 c = v3(s.center[0], s.center[1], s.center[2]);
                 V3 u = v3(s.u[0], s.u[1], s.u[2]), v = v3(s.v[0], s.v[1], s.v[2]);
                 Box b;
-                const V3 cu = vadd(c, u), cv = vadd(c, v), cuv = vadd(vadd(c, u), v);
-                b.lo = vmin(vmin(vmin(c, cu), cv), cuv);
-                b.hi = vmax(vmax(vmax(c, cu), cv), cuv);
+                if (s.type == NOOR_SHAPE_SPHERE) {
+                    const V3 r = v3(s.radius, s.radius, s.radius);
+                    b.lo = vsub(c, r);
+                    b.hi = vadd(c, r);
+                } else if (s.type == NOOR_SHAPE_DISK) {
+                    // the four points at radius along +-u and +-v (unit)
+                    auto unit = [](const V3& a) { return vscale(a, 1.0f / std::sqrt(a.x * a.x + a.y * a.y + a.z * a.z)); };
+                    const V3 un = unit(u), vn = unit(v);
+                    const V3 pr = vadd(c, vscale(un, s.radius)), pt = vadd(c, vscale(vn, s.radius));
+                    const V3 pl = vsub(c, vscale(un, s.radius)), pb = vsub(c, vscale(vn, s.radius));
+                    b.lo = vmin(vmin(vmin(pl, pr), pt), pb);
+                    b.hi = vmax(vmax(vmax(pl, pr), pt), pb);
+                } else {
+                    const V3 cu = vadd(c, u), cv = vadd(c, v), cuv = vadd(vadd(c, u), v);
+                    b.lo = vmin(vmin(vmin(c, cu), cv), cuv);
+                    b.hi = vmax(vmax(vmax(c, cu), cv), cuv);
+                }
                 mi.box = mi.ibox = b;
                 mi.cbox.lo = mi.cbox.hi = b.centroid();
                 mi.icbox = mi.cbox;
@@ -510,8 +524,11 @@ public:
         for (uint32_t i = 0; i < D.num_meshes; ++i) mesh_order[i] = i;
         mesh_start.assign(D.num_meshes, 0u);
         std::vector<uint32_t> src;
+        // light meshes too: the reference builds each one a bottom-level
+        // tree (one empty leaf with the shape's bounds), which its light
+        // node points at
         for (uint32_t i = 0; i < D.num_meshes; ++i)
-            if (D.meshes[i].instance < 0 && D.meshes[i].light_idx < 0) src.push_back(i);
+            if (D.meshes[i].instance < 0) src.push_back(i);
         std::vector<Work> trees(src.size());
         std::atomic<size_t> next{0};
         std::vector<std::exception_ptr> errs(src.size());
@@ -621,6 +638,9 @@ struct noor_payload_handle {
     std::vector<std::vector<float>> tex_data;
     std::vector<noor_texture> textures;
     std::vector<noor_area_light> lights;
+    std::vector<noor_point_light> point_lights;
+    std::vector<noor_spot_light> spot_lights;
+    std::vector<noor_distant_light> distant_lights;
     std::vector<noor_material> materials;
     std::vector<uint32_t> tri_order;
     uint32_t num_tris = 0;
@@ -643,6 +663,9 @@ extern "C" int noor_build_payload(const noor_scene_desc* d, noor_payload_handle*
         return set_error(NOOR_ERR_INVALID, "noor_build_payload: empty or incomplete scene");
     if (d->num_materials == 0 || !d->materials) return set_error(NOOR_ERR_INVALID, "noor_build_payload: no materials");
     if (d->bvh.num_bins < 2) return set_error(NOOR_ERR_INVALID, "noor_build_payload: num_bins must be >= 2");
+    if ((d->num_area_lights && !d->area_lights) || (d->num_point_lights && !d->point_lights) ||
+        (d->num_spot_lights && !d->spot_lights) || (d->num_distant_lights && !d->distant_lights))
+        return set_error(NOOR_ERR_INVALID, "noor_build_payload: light count without an array");
     // validate indices and mesh ranges (source meshes cover [0,N) in order)
     uint32_t next = 0;
     for (uint32_t i = 0; i < d->num_meshes; ++i) {
@@ -650,6 +673,8 @@ extern "C" int noor_build_payload(const noor_scene_desc* d, noor_payload_handle*
         if (m.light_idx >= 0) {
             if ((uint32_t)m.light_idx >= d->num_area_lights)
                 return set_error(NOOR_ERR_INVALID, "noor_build_payload: light mesh names a missing light");
+            if (m.tri_count != 0 || m.tri_start > d->num_triangles)
+                return set_error(NOOR_ERR_INVALID, "noor_build_payload: a light mesh carries no triangles");
             continue;
         }
         if (m.instance >= 0) {
@@ -766,6 +791,17 @@ extern "C" int noor_build_payload(const noor_scene_desc* d, noor_payload_handle*
             h->textures.push_back(t);
         }
         h->lights.assign(d->area_lights, d->area_lights + d->num_area_lights);
+        if (d->num_point_lights) h->point_lights.assign(d->point_lights, d->point_lights + d->num_point_lights);
+        if (d->num_spot_lights) h->spot_lights.assign(d->spot_lights, d->spot_lights + d->num_spot_lights);
+        if (d->num_distant_lights) {
+            // CudaDistantLight's constructor normalises the direction (light.cuh:222)
+            h->distant_lights.assign(d->distant_lights, d->distant_lights + d->num_distant_lights);
+            for (noor_distant_light& l : h->distant_lights) {
+                const float* w = l.direction;
+                const float inv = 1.0f / std::sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+                for (int k = 0; k < 3; ++k) l.direction[k] = w[k] * inv;
+            }
+        }
 
         // vertex de-duplication in BVH order (Model::loadCudaPayload, model.cpp:376-401):
         // the first occurrence of a (vertex, normal, uv) index triple appends a
@@ -859,6 +895,12 @@ extern "C" int noor_payload_view(const noor_payload_handle* h, noor_payload* p) 
     p->num_textures = (uint32_t)h->textures.size();
     p->area_lights = h->lights.empty() ? nullptr : h->lights.data();
     p->num_area_lights = (int32_t)h->lights.size();
+    p->point_lights = h->point_lights.empty() ? nullptr : h->point_lights.data();
+    p->num_point_lights = (int32_t)h->point_lights.size();
+    p->spot_lights = h->spot_lights.empty() ? nullptr : h->spot_lights.data();
+    p->num_spot_lights = (int32_t)h->spot_lights.size();
+    p->distant_lights = h->distant_lights.empty() ? nullptr : h->distant_lights.data();
+    p->num_distant_lights = (int32_t)h->distant_lights.size();
     p->num_infinite_lights = 1;
     p->materials = h->materials.data();
     p->num_materials = (uint32_t)h->materials.size();
@@ -886,7 +928,8 @@ extern "C" int noor_payload_default_spec(const noor_payload_handle* h, uint32_t 
     s->rr = rr;
     s->num_gpus = 1;
     s->skydome_type = h->skydome_type;
-    const int num_lights = (int)h->lights.size() + 1;
+    const int num_lights = (int)(h->lights.size() + h->point_lights.size() + h->spot_lights.size() +
+                                 h->distant_lights.size()) + 1;
     s->lighting_type = num_lights < 2 ? NOOR_LIGHT_SKY_MASK : 0u;
     s->mis = 0;
     s->intersector = NOOR_ISECT_WATERTIGHT;

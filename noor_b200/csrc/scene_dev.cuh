@@ -64,11 +64,23 @@ struct DevAreaLight {
     float3 u;
     int two_sided;
     float3 v;
-    int type;
+    int type;               // NOOR_SHAPE_*
     float3 n;
-    float pad;
+    float radius;           // sphere / disk
     float3 ke;
-    float pad2;
+    float radius2;
+};
+
+// point, spot and distant lights (noor/cuda/light.cuh:158-238), stored in
+// one array in light-index order
+enum : int { kDeltaPoint = 0, kDeltaSpot = 1, kDeltaDistant = 2 };
+struct DevDeltaLight {
+    float3 pos;
+    int kind;
+    float3 dir;             // spot axis / direction towards a distant light
+    float cos_inner;
+    float3 ke;
+    float cos_outer;
 };
 
 struct DevHosek {
@@ -105,12 +117,14 @@ struct DevScene {
     const DevXform* xforms;
     const DevMaterial* materials;
     const DevAreaLight* area_lights;
+    const DevDeltaLight* delta_lights;
     const float4* env;      // env texels (HDR / baked sky / constant), w*h
     uint32_t num_nodes;
     uint32_t num_tris;
     uint32_t num_instances;
     uint32_t num_materials;
     int num_area_lights;
+    int num_delta_lights;   // lights num_area_lights .. + num_delta_lights - 1
     int num_lights;         // area lights + infinite light
     int env_w, env_h;
     DevDist2D dist;
@@ -128,6 +142,7 @@ struct DevScene {
     uint32_t film_mode;
     int stack_cap;
     uint32_t ext_lobes;     // some material uses a lobe beyond Lambert, conductor, Fresnel specular
+    uint32_t ext_lights;    // sphere or disk area lights, point, spot or distant lights
 };
 
 }  // namespace nb

@@ -407,14 +407,7 @@ enum : uint32_t {
     BSDF_NOOP = 1u << 7,
     BSDF_ALL = 0xFFu
 };
-#ifndef NB_LOBE_OUTLINE
-#define NB_LOBE_OUTLINE 1
-#endif
-#if NB_LOBE_OUTLINE
-#define NB_OUTLINE static __device__ __noinline__
-#else
-#define NB_OUTLINE NB_D
-#endif
+
 
 // Lobe ids, one per BxDF class the material factory builds
 // (noor/cuda/bxdf.cuh:119-137): the low 8 bits are the class's BxDF type

@@ -178,6 +178,69 @@ NB_D bool quad_hit(const DevAreaLight& q, const float3& o, const float3& d, floa
     return true;
 }
 
+// solveQuadratic (noor/cuda/utils.cuh:52-91): the root of larger magnitude
+// first, the other from x0 * x1 = c / a; returns x0 <= x1
+NB_D bool solve_quadratic(float a, float b, float c, float& x0, float& x1) {
+    if (a == 0.0f) {
+        if (b != 0.0f) {
+            x0 = x1 = -c / b;
+            return true;
+        }
+        return false;
+    }
+    const float disc = b * b - 4.0f * a * c;
+    if (disc < 0.0f) return false;
+    const float sd = sqrtf(disc);
+    const float q = b < 0.0f ? -0.5f * (b - sd) : -0.5f * (b + sd);
+    x0 = q / a;
+    x1 = c / q;
+    if (x0 > x1) {
+        const float t = x0;
+        x0 = x1;
+        x1 = t;
+    }
+    return true;
+}
+
+// sphere of an area light (noor/cuda/geometry.cuh:125-150): nearest root in
+// [0, tmax], else the far root when the near one is behind the origin
+NB_D bool sphere_hit(const DevAreaLight& s, const float3& o, const float3& d, float& tmax) {
+    const float3 oc = o - s.center;
+    float t0, t1;
+    if (!solve_quadratic(length2(d), 2.0f * dot(oc, d), length2(oc) - s.radius2, t0, t1)) return false;
+    if (!(t0 <= tmax && t1 >= 0.0f)) return false;
+    if (t0 < 0.0f) {
+        if (t1 > tmax) return false;
+        tmax = t1;
+    } else {
+        tmax = t0;
+    }
+    return true;
+}
+
+// disk of an area light (noor/cuda/geometry.cuh:152-163); like the quad, no
+// lower bound on t
+NB_D bool disk_hit(const DevAreaLight& q, const float3& o, const float3& d, float& tmax) {
+    const float denom = dot(q.n, d);
+    if (denom == 0.0f) return false;
+    const float t = -(dot(o, q.n) - dot(q.center, q.n)) / denom;
+    if (t > tmax) return false;
+    const float3 p = (o + t * d) - q.center;
+    if (length2(p) > q.radius2) return false;
+    tmax = t;
+    return true;
+}
+
+// CudaShape::intersect (noor/cuda/shapeimp.cuh:73-87).  EXT false: the
+// scene's area lights are all quads (kernels for such scenes leave the
+// other shapes' code out)
+template <bool EXT = true>
+NB_D bool shape_hit(const DevAreaLight& a, const float3& o, const float3& d, float& tmax) {
+    if (!EXT || a.type == NOOR_SHAPE_QUAD) return quad_hit(a, o, d, tmax);
+    if (a.type == NOOR_SHAPE_SPHERE) return sphere_hit(a, o, d, tmax);
+    return disk_hit(a, o, d, tmax);
+}
+
 struct HitRec {
     float u, v;
     uint32_t tri;
@@ -203,7 +266,7 @@ constexpr uint32_t kNoNode = 0xFFFFFFFFu;
 // reference would pop next (the near child of an inner node, the last child
 // of a mesh leaf, the root of an instance) is kept in a register instead of
 // being pushed and popped at once, and inner nodes are dispatched first.
-template <int ISECT>
+template <int ISECT, bool EXT = true>
 NB_D bool trace_closest(const DevScene& S, const float3& o, const float3& d, float& tmax,
                         HitRec& rec, const SmemStack& st, uint32_t* status) {
     TRay wr;
@@ -237,7 +300,7 @@ NB_D bool trace_closest(const DevScene& S, const float3& o, const float3& d, flo
                 next = neg ? lo.w : ni + 1;
             } else if (hi.w & NOOR_LIGHT_NODE_MASK) {
                 const uint32_t li = hi.w & NOOR_LIGHT_MASK;
-                if ((int)li < S.num_area_lights && quad_hit(S.area_lights[li], o, d, tmax)) {
+                if ((int)li < S.num_area_lights && shape_hit<EXT>(S.area_lights[li], o, d, tmax)) {
                     hit = true;
                     rec.ins = li;
                     rec.mtype = NOOR_MESHLIGHT | NOOR_EMITTER;
@@ -295,7 +358,7 @@ NB_D bool trace_closest(const DevScene& S, const float3& o, const float3& d, flo
 
 // Any hit within (0, tmax]; light nodes count as occluders.  Same visit
 // order and register-held next node as trace_closest.
-template <int ISECT>
+template <int ISECT, bool EXT = true>
 NB_D bool trace_any(const DevScene& S, const float3& o, const float3& d, float tmax,
                     const SmemStack& st, uint32_t* status) {
     TRay wr;
@@ -327,7 +390,7 @@ NB_D bool trace_any(const DevScene& S, const float3& o, const float3& d, float t
             } else if (hi.w & NOOR_LIGHT_NODE_MASK) {
                 const uint32_t li = hi.w & NOOR_LIGHT_MASK;
                 float tm = tmax;
-                if ((int)li < S.num_area_lights && quad_hit(S.area_lights[li], o, d, tm)) return true;
+                if ((int)li < S.num_area_lights && shape_hit<EXT>(S.area_lights[li], o, d, tm)) return true;
             } else if (hi.w & NOOR_MESH_INSTANCE_MASK) {
                 tray_to_object(lr, wr, S.xforms + (hi.w & NOOR_TRANS_MASK));
                 ltmax = tmax;

@@ -280,7 +280,7 @@ __global__ void __launch_bounds__(kRegenBlock) wf_regen(WfDev W) {
     if (threadIdx.x == 0 && nact) atomicAdd(W.counters + kCntActive, (uint32_t)nact);
 }
 
-template <int ISECT>
+template <int ISECT, bool EXT>
 NB_D void extend_one(const WfDev& W, const DevScene& S, uint32_t slot, const float4& ow,
                      const SmemStack& stk) {
     const float4 dw = W.d[slot], bw = W.beta[slot];
@@ -290,7 +290,7 @@ NB_D void extend_one(const WfDev& W, const DevScene& S, uint32_t slot, const flo
     const bool spec = (bb >> 16) & 1u;
     float tmax = kInf;
     HitRec rec{0.0f, 0.0f, 0u, 0u, 0u};
-    const bool hit = trace_closest<ISECT>(S, o, d, tmax, rec, stk, W.status);
+    const bool hit = trace_closest<ISECT, EXT>(S, o, d, tmax, rec, stk, W.status);
     const float3 beta = f3(bw.x, bw.y, bw.z);
     if (!hit) {
         // the sky term is added by regen (converged lanes), after the
@@ -302,8 +302,7 @@ NB_D void extend_one(const WfDev& W, const DevScene& S, uint32_t slot, const flo
         if (bounce == 0 || spec) {
             float3 c;
             if (rec.mtype & NOOR_MESHLIGHT) {
-                const DevAreaLight& A = S.area_lights[rec.ins];
-                c = beta * ((A.two_sided || dot(d, A.n) < 0.0f) ? A.ke : f3(0.0f));
+                c = beta * area_le<EXT>(S.area_lights[rec.ins], d);
             } else {
                 const uint32_t mi = ISECT == NOOR_ISECT_WATERTIGHT ? __ldg(&S.wtri[rec.tri].attr).w
                                                                    : __ldg(&S.wald[rec.tri].attr).w;
@@ -336,8 +335,9 @@ NB_D const DevScene& slot_scene(const WfDev& W, const DevScene& S1, uint32_t fra
     return W.scenes[W.frames[frame].scene];
 }
 
-// Extend: closest hit for every active slot (one thread per slot)
-template <int ISECT, bool MULTI>
+// Extend: closest hit for every active slot (one thread per slot).  EXT
+// false: no scene of the launch has sphere or disk lights
+template <int ISECT, bool MULTI, bool EXT>
 __global__ void __launch_bounds__(NB_TRAV_THREADS, NB_TRAV_MIN_BLOCKS) wf_extend(WfDev W, DevScene S1) {
     extern __shared__ uint32_t smem[];
     const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
@@ -347,11 +347,11 @@ __global__ void __launch_bounds__(NB_TRAV_THREADS, NB_TRAV_MIN_BLOCKS) wf_extend
     const DevScene& S = slot_scene<ISECT, MULTI>(W, S1, fbits(ow.w));
     if (ISECT == kIsectMixed) {
         if (S.isect == NOOR_ISECT_WATERTIGHT)
-            extend_one<NOOR_ISECT_WATERTIGHT>(W, S, slot, ow, stk);
+            extend_one<NOOR_ISECT_WATERTIGHT, EXT>(W, S, slot, ow, stk);
         else
-            extend_one<NOOR_ISECT_REF_WALD>(W, S, slot, ow, stk);
+            extend_one<NOOR_ISECT_REF_WALD, EXT>(W, S, slot, ow, stk);
     } else {
-        extend_one<ISECT == kIsectMixed ? 0 : ISECT>(W, S, slot, ow, stk);
+        extend_one<ISECT == kIsectMixed ? 0 : ISECT, EXT>(W, S, slot, ow, stk);
     }
 }
 
@@ -488,7 +488,7 @@ __global__ void __launch_bounds__(256, NB_SHADE_MIN_BLOCKS) wf_shade(WfDev W, ui
 // contribution.  Each warp takes the next 32 queue entries when it is done
 // with its last ones, so warps that drew long rays do not hold up the launch
 // with a fixed share of the queue.
-template <int ISECT, bool MULTI>
+template <int ISECT, bool MULTI, bool EXT>
 __global__ void __launch_bounds__(NB_TRAV_THREADS, NB_TRAV_MIN_BLOCKS) wf_shadow(WfDev W, DevScene S1) {
     extern __shared__ uint32_t smem[];
     const uint32_t n = W.counters[kCntShadow];
@@ -513,11 +513,11 @@ __global__ void __launch_bounds__(NB_TRAV_THREADS, NB_TRAV_MIN_BLOCKS) wf_shadow
         bool occ;
         if (ISECT == kIsectMixed) {
             if (S.isect == NOOR_ISECT_WATERTIGHT)
-                occ = trace_any<NOOR_ISECT_WATERTIGHT>(S, o, d, so.w, stk, W.status);
+                occ = trace_any<NOOR_ISECT_WATERTIGHT, EXT>(S, o, d, so.w, stk, W.status);
             else
-                occ = trace_any<NOOR_ISECT_REF_WALD>(S, o, d, so.w, stk, W.status);
+                occ = trace_any<NOOR_ISECT_REF_WALD, EXT>(S, o, d, so.w, stk, W.status);
         } else {
-            occ = trace_any<ISECT == kIsectMixed ? 0 : ISECT>(S, o, d, so.w, stk, W.status);
+            occ = trace_any<ISECT == kIsectMixed ? 0 : ISECT, EXT>(S, o, d, so.w, stk, W.status);
         }
         if (occ) W.pend[e].w = 0.0f;
     }
@@ -630,7 +630,8 @@ struct WfLaunch {
     WfTravKernel extend;
     WfTravKernel shadow;
     DevScene scene;         // the launch's scene when every frame uses the same one
-    bool ext;               // some frame's scene has a material with lobes beyond the first three
+    bool ext;               // some frame's scene has extra lobes or lights
+    bool ext_lights;        // ... has sphere, disk, point, spot or distant lights
 };
 
 // one iteration; with `ev` (6 events), records ev[0] before the first stage
@@ -647,7 +648,7 @@ static cudaError_t wf_iteration(const WfDev& W, const WfLaunch& L, cudaStream_t 
     const int nk = W.sort ? kKinds : 1;
     for (int k = 0; k < nk; ++k) {
         // sorted queues 0 and 1 hold Lambert and conductor hits only
-        if (L.ext && !(W.sort && k < 2))
+        if (L.ext && !(W.sort && k < 2 && !L.ext_lights))
             wf_shade<true><<<L.grid_queue, 256, 0, s>>>(W, (uint32_t)k);
         else
             wf_shade<false><<<L.grid_queue, 256, 0, s>>>(W, (uint32_t)k);
@@ -772,23 +773,31 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
     L.grid_queue = (uint32_t)std::max(1, C.sm_count) * 16;
     const uint32_t scene0 = frames[0].scene_id;
     bool multi = false, mixed = false;
-    L.ext = false;
+    L.ext = L.ext_lights = false;
     for (uint32_t i = 0; i < n_frames; ++i) {
+        const DevScene& fs = C.scenes[frames[i].scene_id]->dev;
         multi |= frames[i].scene_id != scene0;
-        mixed |= C.scenes[frames[i].scene_id]->dev.isect != C.scenes[scene0]->dev.isect;
-        L.ext |= C.scenes[frames[i].scene_id]->dev.ext_lobes != 0u;
+        mixed |= fs.isect != C.scenes[scene0]->dev.isect;
+        L.ext |= fs.ext_lobes != 0u || fs.ext_lights != 0u;
+        L.ext_lights |= fs.ext_lights != 0u;
     }
     L.scene = C.scenes[scene0]->dev;
+    // traversal kernels: per intersector, scene source and light shapes
+#define NB_TRAV(I, M)                                                                   \
+    do {                                                                                \
+        L.extend = L.ext_lights ? wf_extend<I, M, true> : wf_extend<I, M, false>;     \
+        L.shadow = L.ext_lights ? wf_shadow<I, M, true> : wf_shadow<I, M, false>;     \
+    } while (0)
     if (mixed) {
-        L.extend = wf_extend<kIsectMixed, true>;
-        L.shadow = wf_shadow<kIsectMixed, true>;
+        NB_TRAV(kIsectMixed, true);
     } else if (L.scene.isect == NOOR_ISECT_WATERTIGHT) {
-        L.extend = multi ? wf_extend<NOOR_ISECT_WATERTIGHT, true> : wf_extend<NOOR_ISECT_WATERTIGHT, false>;
-        L.shadow = multi ? wf_shadow<NOOR_ISECT_WATERTIGHT, true> : wf_shadow<NOOR_ISECT_WATERTIGHT, false>;
+        if (multi) NB_TRAV(NOOR_ISECT_WATERTIGHT, true);
+        else NB_TRAV(NOOR_ISECT_WATERTIGHT, false);
     } else {
-        L.extend = multi ? wf_extend<NOOR_ISECT_REF_WALD, true> : wf_extend<NOOR_ISECT_REF_WALD, false>;
-        L.shadow = multi ? wf_shadow<NOOR_ISECT_REF_WALD, true> : wf_shadow<NOOR_ISECT_REF_WALD, false>;
+        if (multi) NB_TRAV(NOOR_ISECT_REF_WALD, true);
+        else NB_TRAV(NOOR_ISECT_REF_WALD, false);
     }
+#undef NB_TRAV
     for (WfTravKernel k : {L.extend, L.shadow}) {
         e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem);
         if (e != cudaSuccess) return cuda_fail(e, "wavefront smem");

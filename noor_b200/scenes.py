@@ -57,6 +57,9 @@ class SceneData:
     meshes: list
     materials: list
     area_lights: list = field(default_factory=list)
+    point_lights: list = field(default_factory=list)     # dict(position, ke)
+    spot_lights: list = field(default_factory=list)      # dict(position, direction, ke, cos_inner, cos_outer)
+    distant_lights: list = field(default_factory=list)   # dict(direction, ke)
     skydome_type: int = capi.NOOR_SKY_CONSTANT
     env: Optional[np.ndarray] = None   # (H,W,4) f32
     bvh: dict = field(default_factory=lambda: dict(DEFAULT_BVH))
@@ -106,11 +109,14 @@ def _box(center, size, angle_deg):
 
 
 def room_scene(seed: int = 1, width: int = 256, height: int = 256, spp: int = 16, bounces: int = 5,
-               rr: int = 1, mis: bool = False, box_materials=None) -> SceneData:
+               rr: int = 1, mis: bool = False, box_materials=None, light: str = "quad") -> SceneData:
     """C1: closed room of 5 wall quads + 1 ceiling light quad + 2 rotated
     boxes = 36 triangles, one mesh; wall albedo U[0.2,0.8]^3 from `seed`.
     `box_materials`: two material dicts for the short and the tall box
-    (default: one diffuse grey for both)."""
+    (default: one diffuse grey for both).  `light` replaces the emissive
+    ceiling quad: "sphere" or "disk" (an area light under the ceiling, in
+    the BVH as a light node), "point", "spot" (aimed at the floor) or
+    "distant" (the ceiling removed, light from above at an angle)."""
     rng = np.random.default_rng(seed)
     faces = []   # (corners, normal, material)
     walls = [
@@ -120,6 +126,8 @@ def room_scene(seed: int = 1, width: int = 256, height: int = 256, spp: int = 16
         ([(-1, 0, -1), (-1, 0, 1), (-1, 2, 1), (-1, 2, -1)], (1, 0, 0)),   # left
         ([(1, 0, -1), (1, 0, 1), (1, 2, 1), (1, 2, -1)], (-1, 0, 0)),      # right
     ]
+    if light == "distant":
+        walls = walls[:1] + walls[2:]
     mats = []
     for i, (pts, n) in enumerate(walls):
         mats.append(material("diffuse", albedo=tuple(rng.uniform(0.2, 0.8, 3))))
@@ -135,12 +143,13 @@ def room_scene(seed: int = 1, width: int = 256, height: int = 256, spp: int = 16
                                       _box((-0.33, 0.6, -0.3), (0.6, 1.2, 0.6), -18.0))):
         for corners_n in corners_list:
             faces.append((corners_n[0], corners_n[1], box_ids[b]))
-    light_mat = len(mats)
     ke = (17.0, 12.0, 4.0)
-    mats.append(material("emitter", emittance=ke))
     ly, h = 1.98, 0.25
-    lpts = _quad([(-h, ly, -h), (h, ly, -h), (h, ly, h), (-h, ly, h)], np.array([0.0, -1.0, 0.0]))
-    faces.append((lpts, np.array([0.0, -1.0, 0.0]), light_mat))
+    if light == "quad":
+        light_mat = len(mats)
+        mats.append(material("emitter", emittance=ke))
+        lpts = _quad([(-h, ly, -h), (h, ly, -h), (h, ly, h), (-h, ly, h)], np.array([0.0, -1.0, 0.0]))
+        faces.append((lpts, np.array([0.0, -1.0, 0.0]), light_mat))
 
     verts, norms, vidx, nidx, midx = [], [], [], [], []
     for corners, n, m in faces:
@@ -158,13 +167,33 @@ def room_scene(seed: int = 1, width: int = 256, height: int = 256, spp: int = 16
     N = np.zeros((len(norms), 4), np.float32)
     N[:, :3] = np.array(norms)
     T = len(vidx)
-    light = dict(center=(-h, ly, -h), u=(2 * h, 0.0, 0.0), v=(0.0, 0.0, 2 * h), ke=ke, two_sided=0)
+    meshes = [dict(tri_start=0, tri_count=T, to_global=IDENTITY, instance=-1, light_idx=-1)]
+    area, point, spot, distant = [], [], [], []
+    if light == "quad":
+        area.append(dict(center=(-h, ly, -h), u=(2 * h, 0.0, 0.0), v=(0.0, 0.0, 2 * h), ke=ke, two_sided=0))
+    elif light == "sphere":
+        area.append(dict(type="sphere", center=(-0.2, 1.45, -0.2), u=(0.4, 0.0, 0.0), v=(0.0, 0.0, 0.4),
+                         ke=(6.0, 4.5, 2.0)))
+        meshes.append(dict(tri_start=0, tri_count=0, to_global=IDENTITY, instance=-1, light_idx=0))
+    elif light == "disk":
+        area.append(dict(type="disk", center=(-0.3, 1.9, -0.3), u=(0.6, 0.0, 0.0), v=(0.0, 0.0, 0.6),
+                         ke=(12.0, 9.0, 4.0)))
+        meshes.append(dict(tri_start=0, tri_count=0, to_global=IDENTITY, instance=-1, light_idx=0))
+    elif light == "point":
+        point.append(dict(position=(0.1, 1.75, 0.2), ke=(3.0, 2.4, 1.2)))
+    elif light == "spot":
+        spot.append(dict(position=(0.0, 1.9, 0.3), direction=(0.0, 1.0, 0.0), ke=(5.0, 4.0, 2.5),
+                         cos_inner=float(np.cos(np.radians(20.0))), cos_outer=float(np.cos(np.radians(35.0)))))
+    elif light == "distant":
+        distant.append(dict(direction=(0.35, 1.0, 0.25), ke=(2.0, 1.8, 1.5)))
+    else:
+        raise ValueError(f"unknown room light {light!r}")
     return SceneData(
         vertices=V, normals=N, uvs=np.zeros((1, 2), np.float32),
         vindices=np.array(vidx, np.uint32), nindices=np.array(nidx, np.uint32),
         uvindices=np.zeros((T, 3), np.uint32), material_indices=np.array(midx, np.uint32),
-        meshes=[dict(tri_start=0, tri_count=T, to_global=IDENTITY, instance=-1, light_idx=-1)],
-        materials=mats, area_lights=[light], skydome_type=capi.NOOR_SKY_CONSTANT,
+        meshes=meshes, materials=mats, area_lights=area, point_lights=point, spot_lights=spot,
+        distant_lights=distant, skydome_type=capi.NOOR_SKY_CONSTANT,
         camera=dict(eye=(0.0, 1.0, 3.75), look_at=(0.0, 1.0, 0.0), up=(0.0, 1.0, 0.0), fov_deg=40.0,
                     w=width, h=height),
         render=dict(spp=spp, bounces=bounces, rr=rr, mis=int(mis)), name="room")
@@ -453,6 +482,7 @@ class BuiltPayload:
         lights = (capi.AreaLight * max(1, len(s.area_lights)))()
         for k, l in enumerate(s.area_lights):
             lights[k] = make_area_light(l, k)
+        delta = make_delta_lights(s)
         d = capi.SceneDesc()
         d.vertices, d.num_vertices = _ptr(V), V.shape[0]
         d.normals, d.num_normals = _ptr(N), N.shape[0]
@@ -463,6 +493,9 @@ class BuiltPayload:
         d.meshes, d.num_meshes = meshes, len(s.meshes)
         d.materials, d.num_materials = mats, len(s.materials)
         d.area_lights, d.num_area_lights = lights, len(s.area_lights)
+        d.point_lights, d.num_point_lights = delta[0], len(s.point_lights)
+        d.spot_lights, d.num_spot_lights = delta[1], len(s.spot_lights)
+        d.distant_lights, d.num_distant_lights = delta[2], len(s.distant_lights)
         d.skydome_type = s.skydome_type
         if s.env is not None:
             E = np.ascontiguousarray(s.env, np.float32)
@@ -471,7 +504,7 @@ class BuiltPayload:
         b = s.bvh
         d.bvh = capi.BvhSpec(b["num_bins"], b["max_height"], b["Ci"], b["Ct"], b["min_leaf_tris"], b["max_leaf_tris"])
         self.desc = d
-        self._keep = keep + [meshes, mats, lights]
+        self._keep = keep + [meshes, mats, lights, delta]
         h = C.c_void_p()
         self.stat = capi.BuildStat()
         capi.call("noor_build_payload", C.byref(d), C.byref(h), C.byref(self.stat))
@@ -513,23 +546,56 @@ class BuiltPayload:
 
 
 def make_area_light(l: dict, idx: int) -> capi.AreaLight:
-    """CudaShape(center, u, v, n, QUAD) + CudaAreaLight (shape.cuh:43-69)"""
+    """CudaShape(center, u, v, n, type) + CudaAreaLight (shape.cuh:43-69):
+    `center` is the corner the edges u and v start from; a sphere or disk is
+    centred at center + (u + v) / 2 with radius min(|u|, |v|) / 2.  `type`:
+    "quad" (default), "sphere" or "disk"."""
     a = capi.AreaLight()
+    kind = {"quad": capi.NOOR_SHAPE_QUAD, "sphere": capi.NOOR_SHAPE_SPHERE,
+            "disk": capi.NOOR_SHAPE_DISK}[l.get("type", "quad")]
     c, u, v = (np.asarray(l[k], np.float32) for k in ("center", "u", "v"))
     n = np.cross(u.astype(np.float64), v.astype(np.float64))
     n = (n / np.linalg.norm(n)).astype(np.float32)
+    r = np.float32(0.5) * min(np.float32(np.linalg.norm(u)), np.float32(np.linalg.norm(v)))
+    r2 = np.float32(r * r)
+    if kind == capi.NOOR_SHAPE_QUAD:
+        area = float(np.linalg.norm(np.cross(u.astype(np.float64), v.astype(np.float64))))
+    else:
+        c = (c + np.float32(0.5) * (u + v)).astype(np.float32)
+        area = float(np.float32(4.0 * np.pi if kind == capi.NOOR_SHAPE_SPHERE else np.pi) * r2)
     a.shape.center[:] = [float(x) for x in c]
     a.shape.u[:] = [float(x) for x in u]
     a.shape.v[:] = [float(x) for x in v]
     a.shape.n[:] = [float(x) for x in n]
-    a.shape.area = float(np.linalg.norm(np.cross(u.astype(np.float64), v.astype(np.float64))))
-    a.shape.radius = 0.5 * min(float(np.linalg.norm(u)), float(np.linalg.norm(v)))
-    a.shape.radius2 = a.shape.radius ** 2
+    a.shape.area = area
+    a.shape.radius = float(r)
+    a.shape.radius2 = float(r2)
     a.shape.light_idx = idx
-    a.shape.type = 0
+    a.shape.type = kind
     a.ke[:] = [float(x) for x in l["ke"]]
     a.two_sided = int(l.get("two_sided", 0))
     return a
+
+
+def make_delta_lights(s: "SceneData"):
+    """noor_point_light / noor_spot_light / noor_distant_light arrays (one
+    element at least, so that each is a valid pointer)"""
+    pts = (capi.PointLight * max(1, len(s.point_lights)))()
+    for k, l in enumerate(s.point_lights):
+        pts[k].ke[:] = [float(x) for x in l["ke"]]
+        pts[k].position[:] = [float(x) for x in l["position"]]
+    spots = (capi.SpotLight * max(1, len(s.spot_lights)))()
+    for k, l in enumerate(s.spot_lights):
+        spots[k].ke[:] = [float(x) for x in l["ke"]]
+        spots[k].position[:] = [float(x) for x in l["position"]]
+        spots[k].direction[:] = [float(x) for x in l["direction"]]
+        spots[k].cos_inner = float(l["cos_inner"])
+        spots[k].cos_outer = float(l["cos_outer"])
+    dist = (capi.DistantLight * max(1, len(s.distant_lights)))()
+    for k, l in enumerate(s.distant_lights):
+        dist[k].ke[:] = [float(x) for x in l["ke"]]
+        dist[k].direction[:] = [float(x) for x in l["direction"]]
+    return pts, spots, dist
 
 
 def make_camera(cam: dict) -> capi.Camera:

@@ -274,6 +274,56 @@ template <class T> inline bool quad_hit(const noor_area_light& L, V<T> o, V<T> d
     tmax = t;
     return true;
 }
+// solveQuadratic (utils.cuh:52-91)
+template <class T> inline bool solve_quad(T a, T b, T c, T& x0, T& x1) {
+    if (a == T(0)) {
+        if (b != T(0)) {
+            x0 = x1 = -c / b;
+            return true;
+        }
+        return false;
+    }
+    const T disc = b * b - T(4) * a * c;
+    if (disc < T(0)) return false;
+    const T sd = std::sqrt(disc);
+    const T q = b < T(0) ? T(-0.5) * (b - sd) : T(-0.5) * (b + sd);
+    x0 = q / a;
+    x1 = c / q;
+    if (x0 > x1) std::swap(x0, x1);
+    return true;
+}
+// intersectSphere / intersectDisk (geometry.cuh:125-163)
+template <class T> inline bool sphere_hit(const noor_area_light& L, V<T> o, V<T> d, T& tmax) {
+    const V<T> oc = o - mk((T)L.shape.center[0], (T)L.shape.center[1], (T)L.shape.center[2]);
+    T t0, t1;
+    if (!solve_quad<T>(dot(d, d), T(2) * dot(oc, d), dot(oc, oc) - (T)L.shape.radius2, t0, t1)) return false;
+    if (!(t0 <= tmax && t1 >= T(0))) return false;
+    if (t0 < T(0)) {
+        if (t1 > tmax) return false;
+        tmax = t1;
+    } else {
+        tmax = t0;
+    }
+    return true;
+}
+template <class T> inline bool disk_hit(const noor_area_light& L, V<T> o, V<T> d, T& tmax) {
+    const V<T> n = mk((T)L.shape.n[0], (T)L.shape.n[1], (T)L.shape.n[2]);
+    const V<T> c = mk((T)L.shape.center[0], (T)L.shape.center[1], (T)L.shape.center[2]);
+    const T denom = dot(n, d);
+    if (denom == T(0)) return false;
+    const T t = -(dot(o, n) - dot(c, n)) / denom;
+    if (t > tmax) return false;
+    const V<T> p = (o + t * d) - c;
+    if (dot(p, p) > (T)L.shape.radius2) return false;
+    tmax = t;
+    return true;
+}
+// CudaShape::intersect (shapeimp.cuh:73-87)
+template <class T> inline bool shape_hit(const noor_area_light& L, V<T> o, V<T> d, T& tmax) {
+    if (L.shape.type == NOOR_SHAPE_SPHERE) return sphere_hit<T>(L, o, d, tmax);
+    if (L.shape.type == NOOR_SHAPE_DISK) return disk_hit<T>(L, o, d, tmax);
+    return quad_hit<T>(L, o, d, tmax);
+}
 
 struct Hit {
     double u, v;
@@ -313,8 +363,8 @@ bool traverse(const Scene& sc, V<T> o, V<T> d, T& tmax, Hit* rec, bool any, int 
             const uint32_t li = w1 & NOOR_LIGHT_MASK;
             if (any) {
                 T tm = tmax;
-                if (quad_hit(P->area_lights[li], o, d, tm)) return true;
-            } else if (quad_hit(P->area_lights[li], o, d, tmax)) {
+                if (shape_hit(P->area_lights[li], o, d, tm)) return true;
+            } else if (shape_hit(P->area_lights[li], o, d, tmax)) {
                 hit = true;
                 rec->ins = li;
                 rec->mt = NOOR_MESHLIGHT | NOOR_EMITTER;
@@ -768,9 +818,10 @@ template <class T> T lobe_pdf(uint32_t lobe, const Scene::Mat& m, V<T> wo, V<T> 
     return T(0);
 }
 // concentricSampleDisk / cosineSampleHemisphere (utils.cuh:377-404)
-template <class T> V<T> cos_hemi(T ux, T uy) {
+template <class T> void conc_disk(T ux, T uy, T& dx, T& dy) {
     const T ox = T(2) * ux - T(1), oy = T(2) * uy - T(1);
-    T dx = 0, dy = 0;
+    dx = 0;
+    dy = 0;
     if (!(ox == T(0) && oy == T(0))) {
         T th, r;
         if (std::fabs(ox) > std::fabs(oy)) {
@@ -783,6 +834,10 @@ template <class T> V<T> cos_hemi(T ux, T uy) {
         dx = r * std::cos(th);
         dy = r * std::sin(th);
     }
+}
+template <class T> V<T> cos_hemi(T ux, T uy) {
+    T dx, dy;
+    conc_disk<T>(ux, uy, dx, dy);
     return mk(dx, dy, std::sqrt(std::max(T(0), T(1) - dx * dx - dy * dy)));
 }
 const float kOneMinusEpsF = 1.0f - std::numeric_limits<float>::epsilon();
@@ -1106,6 +1161,115 @@ template <class T> V<T> area_p(const noor_area_light& A, int which) {
     return which == 0 ? v3f<T>(A.shape.center) : (which == 1 ? v3f<T>(A.shape.u) : (which == 2 ? v3f<T>(A.shape.v) : v3f<T>(A.shape.n)));
 }
 
+// CudaAreaLight::Le (lightimp.cuh:29-36): w is the direction of the ray
+// arriving at the light
+template <class T> V<T> area_le(const noor_area_light& A, V<T> w) {
+    if (A.shape.type == NOOR_SHAPE_SPHERE) return v3f<T>(A.ke);
+    return (A.two_sided || dot(w, area_p<T>(A, 3)) < T(0)) ? v3f<T>(A.ke) : mk(T(0), T(0), T(0));
+}
+// sampleQuad / sampleSphere / sampleDisk (geometry.cuh:27-103); the quad
+// and disk pdf divide by |n . w| with w = P - p unnormalised, as there
+template <class T> V<T> area_sample(const Scene& sc, const noor_area_light& A, V<T> P, Rng& rng, T& pdf) {
+    const T bias = (T)sc.S->reflection_bias;
+    const V<T> c = area_p<T>(A, 0), n = area_p<T>(A, 3);
+    const T rad = (T)A.shape.radius, rad2 = (T)A.shape.radius2;
+    if (A.shape.type == NOOR_SHAPE_SPHERE) {
+        const float r1 = rng.next();
+        const float r2 = rng.next();
+        const V<T> w = nrm(c - P);
+        V<T> u, v;
+        coord_sys<T>(w, u, v);
+        const T sin2max = rad2 / len2(P - c);
+        const T cosmax = std::sqrt(std::max(T(0), T(1) - sin2max));
+        const T ct = (T(1) - (T)r1) + (T)r1 * cosmax;
+        const T st = std::sqrt(std::max(T(0), T(1) - ct * ct));
+        const T phi = (T)r2 * (T(2) * K<T>::pi);
+        const T dc = len(P - c);
+        const T ds = dc * ct - std::sqrt(std::max(T(0), rad2 - dc * dc * st * st));
+        const T ca = (dc * dc + rad2 - ds * ds) / (T(2) * dc * rad);
+        const T sa = std::sqrt(std::max(T(0), T(1) - ca * ca));
+        const V<T> N = sa * std::cos(phi) * (T(-1) * u) + sa * std::sin(phi) * (T(-1) * v) + ca * (T(-1) * w);
+        V<T> p = c + rad * N;
+        p = p * (rad / len(p - c));
+        p = p + bias * N;
+        pdf = (T(1) / (T(2) * K<T>::pi)) / (T(1) - cosmax);
+        return p;
+    }
+    V<T> p;
+    if (A.shape.type == NOOR_SHAPE_DISK) {
+        const float ux = rng.next();
+        const float uy = rng.next();
+        T dx, dy;
+        conc_disk<T>((T)ux, (T)uy, dx, dy);
+        V<T> u, v;
+        coord_sys<T>(n, u, v);
+        p = (dx * rad) * u + (dy * rad) * v + T(0) * n + c + bias * n;
+    } else {
+        const float r1 = rng.next();
+        const float r2 = rng.next();
+        p = c + area_p<T>(A, 1) * (T)r1 + area_p<T>(A, 2) * (T)r2 + bias * n;
+    }
+    const V<T> w = P - p;
+    pdf = len2(w) / (std::fabs(dot(n, T(-1) * w)) * (T)A.shape.area);
+    if (std::isinf(pdf)) pdf = 0;
+    return p;
+}
+// CudaShape::pdf (shapeimp.cuh:28-52)
+template <class T> T area_pdf(const noor_area_light& A, V<T> P, V<T> wi) {
+    T lp = 0;
+    if (A.shape.type == NOOR_SHAPE_SPHERE) {
+        const T sin2max = (T)A.shape.radius2 / len2(P - area_p<T>(A, 0));
+        const T cosmax = std::sqrt(std::max(T(0), T(1) - sin2max));
+        lp = (T(1) / (T(2) * K<T>::pi)) / (T(1) - cosmax);
+    } else {
+        T tm = K<T>::inf;
+        if (shape_hit<T>(A, P, wi, tm)) {
+            const V<T> p = P + tm * wi;
+            lp = len2(p - P) / (std::fabs(dot(area_p<T>(A, 3), T(-1) * wi)) * (T)A.shape.area);
+        }
+    }
+    if (std::isinf(lp)) lp = 0;
+    return lp;
+}
+// point / spot / distant sample_Li (lightimp.cuh:191-241); k counts from
+// the first point light
+template <class T> V<T> delta_sample(const Scene& sc, int k, V<T> P, V<T>& to, T& pdf) {
+    const noor_payload* Pl = sc.P;
+    const V<T> zero = mk(T(0), T(0), T(0));
+    pdf = 1;
+    if (k >= Pl->num_point_lights + Pl->num_spot_lights) {
+        const noor_distant_light& L = Pl->distant_lights[k - Pl->num_point_lights - Pl->num_spot_lights];
+        to = P + T(2) * (T)sc.S->world_radius * v3f<T>(L.direction);
+        return v3f<T>(L.ke);
+    }
+    const bool spot = k >= Pl->num_point_lights;
+    const float* pos = spot ? Pl->spot_lights[k - Pl->num_point_lights].position : Pl->point_lights[k].position;
+    const float* ke = spot ? Pl->spot_lights[k - Pl->num_point_lights].ke : Pl->point_lights[k].ke;
+    to = v3f<T>(pos);
+    const T dist2 = len2(to - P);
+    if (dist2 == T(0)) {
+        pdf = 0;
+        return zero;
+    }
+    if (!spot) return v3f<T>(ke) / dist2;
+    // CudaSpotLight::falloff (light.cuh:198-206)
+    const noor_spot_light& L = Pl->spot_lights[k - Pl->num_point_lights];
+    const V<T> v = to - P;
+    const T c = dot(v3f<T>(L.direction), v / len(v));
+    T fo = 1;
+    if (c < (T)L.cos_outer) {
+        fo = 0;
+    } else if (c < (T)L.cos_inner) {
+        const T dl = (c - (T)L.cos_outer) / ((T)L.cos_inner - (T)L.cos_outer);
+        fo = (dl * dl) * (dl * dl);
+    }
+    if (fo == T(0)) {
+        pdf = 0;
+        return zero;
+    }
+    return v3f<T>(ke) * fo / dist2;
+}
+
 // traversal work: rays, nodes popped, triangles tested, triangles whose t
 // passed the range test (all rays), and the same three for shadow rays alone
 struct Counters {
@@ -1140,6 +1304,8 @@ V<T> direct(const Scene& sc, const Scene::Mat& m, const Is<T>& I, Rng& rng, int 
     const bool mis = sc.S->mis != 0;
     const int li = (int)((float)nl * rng.next());
     const int na = sc.P->num_area_lights;
+    const int nd = sc.P->num_point_lights + sc.P->num_spot_lights + sc.P->num_distant_lights;
+    const bool delta = li >= na && li < na + nd;
     const uint32_t nonspec = B_ALL & ~B_SPEC;
     V<T> Ld = zero;
     {
@@ -1147,19 +1313,17 @@ V<T> direct(const Scene& sc, const Scene::Mat& m, const Is<T>& I, Rng& rng, int 
         T lpdf = 0;
         if (li < na) {
             const noor_area_light& A = sc.P->area_lights[li];
-            const float r1 = rng.next();
-            const float r2 = rng.next();
-            const V<T> n = area_p<T>(A, 3);
-            const V<T> p = area_p<T>(A, 0) + area_p<T>(A, 1) * (T)r1 + area_p<T>(A, 2) * (T)r2 + bias * n;
-            const V<T> w = I.p - p;
-            lpdf = len2(w) / (std::fabs(dot(n, T(-1) * w)) * (T)A.shape.area);
-            if (std::isinf(lpdf)) lpdf = 0;
+            const V<T> p = area_sample<T>(sc, A, I.p, rng, lpdf);
             if (lpdf != T(0)) {
                 to = p;
                 const V<T> v = to - I.p;
                 wi = v / len(v);
-                Li = (A.two_sided || dot(wi, n) < T(0)) ? v3f<T>(A.ke) : zero;
+                Li = area_le<T>(A, wi);
             }
+        } else if (delta) {
+            Li = delta_sample<T>(sc, li - na, I.p, to, lpdf);
+            const V<T> v = to - I.p;
+            wi = v / len(v);
         } else {
             const V<T> dir = env_sample_dir<T>(sc, rng, lpdf);
             if (std::isinf(lpdf) || std::isnan(lpdf)) lpdf = 0;
@@ -1175,7 +1339,7 @@ V<T> direct(const Scene& sc, const Scene::Mat& m, const Is<T>& I, Rng& rng, int 
                 f = f * std::fabs(dot(wi, I.F.n));
                 const V<T> so = spawn(I, wi, bias);
                 if (!occl<T>(sc, so, wi, len(so - to), isect, c)) {
-                    if (!mis) {
+                    if (!mis || delta) {
                         Ld = Li * f / lpdf;
                     } else {
                         const T sp = bsdf_pdf<T>(I.lobe, m, I.F, I.wo, wi, nonspec);
@@ -1186,7 +1350,8 @@ V<T> direct(const Scene& sc, const Scene::Mat& m, const Is<T>& I, Rng& rng, int 
         }
     }
     if (!mis) return Ld;
-    // sampleBSDF
+    // sampleBSDF: nothing (and no draw) for a delta light
+    if (delta) return Ld;
     rng.next();
     rng.next();
     V<T> wi;
@@ -1199,13 +1364,7 @@ V<T> direct(const Scene& sc, const Scene::Mat& m, const Is<T>& I, Rng& rng, int 
     if (!(st & B_SPEC)) {
         T lp = 0;
         if (li < na) {
-            const noor_area_light& A = sc.P->area_lights[li];
-            T tm = K<T>::inf;
-            if (quad_hit<T>(A, I.p, wi, tm)) {
-                const V<T> p = I.p + tm * wi;
-                lp = len2(p - I.p) / (std::fabs(dot(area_p<T>(A, 3), T(-1) * wi)) * (T)A.shape.area);
-                if (std::isinf(lp)) lp = 0;
-            }
+            lp = area_pdf<T>(sc.P->area_lights[li], I.p, wi);
         } else {
             lp = env_pdf<T>(sc, wi);
         }
@@ -1219,8 +1378,8 @@ V<T> direct(const Scene& sc, const Scene::Mat& m, const Is<T>& I, Rng& rng, int 
     V<T> Le;
     if (li < na) {
         const noor_area_light& A = sc.P->area_lights[li];
-        lh = quad_hit<T>(A, so, wi, tm);
-        Le = (A.two_sided || dot(wi, area_p<T>(A, 3)) < T(0)) ? v3f<T>(A.ke) : zero;
+        lh = shape_hit<T>(A, so, wi, tm);
+        Le = area_le<T>(A, wi);
     } else {
         lh = sc.sky_on;
         Le = sc.sky_on ? env_eval<T>(sc, wi) : zero;
@@ -1265,8 +1424,7 @@ template <class T> V<T> radiance(const Scene& sc, V<T> o, V<T> d, Rng& rng, int 
         if (I.mt & kEmitMat) {
             if (b == 0 || specb) {
                 if (I.mt & NOOR_MESHLIGHT) {
-                    const noor_area_light& A = sc.P->area_lights[h.ins];
-                    L = L + beta * ((A.two_sided || dot(d, area_p<T>(A, 3)) < T(0)) ? v3f<T>(A.ke) : mk(T(0), T(0), T(0)));
+                    L = L + beta * area_le<T>(sc.P->area_lights[h.ins], d);
                 } else {
                     const Scene::Mat& em = sc.mats[I.mat];
                     L = L + beta * ((T)em.emitter_scale * v3f<T>(em.emittance));
@@ -1647,7 +1805,8 @@ OR_API void* oracle_create(const noor_payload* P, const noor_spec* S, const noor
     sc.env = env.rgba;
     sc.ew = env.width;
     sc.eh = env.height;
-    sc.num_lights = P->num_area_lights + P->num_infinite_lights;
+    sc.num_lights = P->num_area_lights + P->num_point_lights + P->num_spot_lights + P->num_distant_lights +
+                    P->num_infinite_lights;
     sc.sky_on = (S->lighting_type & NOOR_LIGHT_SKY_MASK) != 0;
     sc.mats.resize(P->num_materials);
     for (uint32_t i = 0; i < P->num_materials; ++i) {

@@ -74,8 +74,21 @@ REF_API int ref_build_bvh(const noor_scene_desc* d, uint32_t* nodes, size_t node
             const glm::vec3 c(s.center[0], s.center[1], s.center[2]), u(s.u[0], s.u[1], s.u[2]),
                 v(s.v[0], s.v[1], s.v[2]);
             BBox b;
-            b.setMin(glm::min(glm::min(glm::min(c, c + u), c + v), c + u + v));
-            b.setMax(glm::max(glm::max(glm::max(c, c + u), c + v), c + u + v));
+            // CudaShape::getBounds (noor/cuda/shape.cuh:71-90)
+            if (s.type == NOOR_SHAPE_SPHERE) {
+                const glm::vec3 r(s.radius);
+                b.setMin(c - r);
+                b.setMax(c + r);
+            } else if (s.type == NOOR_SHAPE_DISK) {
+                const glm::vec3 un = glm::normalize(u), vn = glm::normalize(v);
+                const glm::vec3 pr = c + s.radius * un, pt = c + s.radius * vn;
+                const glm::vec3 pl = c - s.radius * un, pb = c - s.radius * vn;
+                b.setMin(glm::min(glm::min(glm::min(pl, pr), pt), pb));
+                b.setMax(glm::max(glm::max(glm::max(pl, pr), pt), pb));
+            } else {
+                b.setMin(glm::min(glm::min(glm::min(c, c + u), c + v), c + u + v));
+                b.setMax(glm::max(glm::max(glm::max(c, c + u), c + v), c + u + v));
+            }
             mesh._instance_bbox = b;
             mesh._bbox = b;
             mesh._instance_centbox.setMin(b.centroid());

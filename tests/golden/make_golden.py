@@ -7,7 +7,7 @@ oracle/_ref/libnoor_ref.so (oracle/Makefile, target `ref`).
                          (BSD-3, Hosek & Wilkie 2012)
   hosek_states.npz       arhosek_rgb_skymodelstate_alloc_update outputs
   bvh_golden.npz         BVH node words, root, height and triangle order of
-                         the reference builder for two seeded scenes
+                         the reference builder for four seeded scenes
   wald_golden.npz        WaldTriangle records for seeded triangles
 
 Run from the repository root:  python tests/golden/make_golden.py
@@ -31,6 +31,9 @@ OUT = Path(__file__).resolve().parent
 GOLDEN_SCENES = {
     "room": lambda: scenes.room_scene(seed=1),
     "spheres": lambda: scenes.SceneData(**scenes.sphere_field(11, 6, 3)[0], name="spheres"),
+    # light nodes with sphere and disk bounds
+    "room_sphere": lambda: scenes.room_scene(seed=1, light="sphere"),
+    "room_disk": lambda: scenes.room_scene(seed=1, light="disk"),
 }
 HOSEK_CASES = [(3.0, 0.3, np.radians(30.0)), (2.0, 0.1, np.radians(10.0)), (5.5, 0.8, np.radians(60.0)),
                (10.0, 0.5, np.radians(45.0)), (1.0, 0.0, np.radians(85.0))]
