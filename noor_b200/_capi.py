@@ -33,6 +33,8 @@ NOOR_ROUGHGLASS = 1 << 6
 NOOR_METAL = 1 << 7
 NOOR_SUBSTRATE = 1 << 8
 NOOR_EMITTER = 1 << 9
+NOOR_CLEARCOAT = 1 << 10
+NOOR_SHADOWCATCHER = 1 << 11
 NOOR_MESHLIGHT = 1 << 14
 NOOR_SKY_HDR, NOOR_SKY_PHYSICAL, NOOR_SKY_CONSTANT = 0, 1, 2
 NOOR_LIGHT_SKY_MASK = 0x20

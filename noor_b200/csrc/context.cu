@@ -83,6 +83,9 @@ static void resolve_material(const noor_payload* P, const noor_material& m, DevM
     d.rough_x = r.x;
     d.rough_y = r.y;
     d.coat_ior = m.coat_ior;
+    d.coat_weight = m.coat_weight;
+    d.coat_sigma = m.coat_sigma;
+    d.coat_thickness = m.coat_thickness;
     d.emitter_scale = m.emitter_scale;
     d.type = m.type;
     d.distribution = m.distribution;
@@ -123,11 +126,9 @@ static int validate_payload(const noor_payload* P) {
         const uint32_t t = m.type;
         if (t & (NOOR_ALPHA | NOOR_BUMP))
             return set_error(NOOR_ERR_UNSUPPORTED, "payload: alpha and bump maps are not implemented");
-        const uint32_t base = t & ~(uint32_t)NOOR_MESHLIGHT;
-        if (base != NOOR_EMITTER && lobe_of(base) == 0u)
-            return set_error(NOOR_ERR_UNSUPPORTED, "payload: material type " + std::to_string(t) +
-                                                       " (Oren-Nayar, clear coat, shadow catcher or a mix of "
-                                                       "types) is not implemented");
+        // every other type is accepted: the ones factoryBSDF builds no lobe
+        // for (Oren-Nayar, mixes of type bits) absorb, as in the reference
+        // (bsdf.cuh:425-461)
         if (m.distribution > 1u) return set_error(NOOR_ERR_INVALID, "payload: unknown microfacet distribution");
     }
     for (int i = 0; i < P->num_area_lights; ++i) {

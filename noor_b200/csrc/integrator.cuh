@@ -214,6 +214,16 @@ NB_D float light_pdf(const DevScene& S, const Isect& I, int li, const float3& wi
     return isinf(pdf) ? 0.0f : pdf;
 }
 
+// The shadow catcher's sky factor: the sky along -toWorld(wo)
+// (noor/cuda/bxdf.cuh:213-218, the local wo taken back to world space)
+template <bool EXT>
+NB_D bool is_catcher(const Isect& I) {
+    return EXT && I.lobe == kLobeCatcher;
+}
+NB_D float3 catcher_sky(const DevScene& S, const Isect& I) {
+    return env_eval(S, -1.0f * to_world(I.F, to_local(I.F, I.wo)));
+}
+
 // A shadow ray whose contribution counts only if nothing blocks it.
 struct ShadowRay {
     float3 o;
@@ -241,11 +251,15 @@ NB_D float3 light_sample_contrib(const DevScene& S, const DevMaterial& m, const 
     const float3 Li = sample_li<EXT>(S, I, rng, nl, li, wi, to, lpdf);
     if (lpdf == 0.0f || is_black(Li)) return f3(0.0f);
     float3 f = bsdf_eval<EXT>(I.lobe, m, I.F, I.wo, wi, kNonSpecular);
+    if (is_catcher<EXT>(I)) f *= catcher_sky(S, I);
     if (is_black(f)) return f3(0.0f);
     f *= absdot(wi, I.F.n);
     sr.o = spawn_origin(I, wi, S.bias);
     sr.d = wi;
     sr.tmax = length3(sr.o - to);
+    // a shadow catcher adds its value wherever the light is unblocked
+    // (direct.cuh:51)
+    if (is_catcher<EXT>(I)) return f;
     if (!mis || is_delta_light<EXT>(S, li)) return Li * f / lpdf;
     const float spdf = bsdf_pdf<EXT>(I.lobe, m, I.F, I.wo, wi, kNonSpecular);
     const float w = power_heuristic(lpdf, spdf);
@@ -258,6 +272,7 @@ NB_D float3 bsdf_mis_contrib(const DevScene& S, const DevMaterial& m, const Isec
                              ShadowRay& sr) {
     const uint32_t flags = (I.mtype & kSpecularMat) ? BSDF_ALL : kNonSpecular;
     if (is_delta_light<EXT>(S, li)) return f3(0.0f);  // before any draw (direct.cuh:77)
+    if (is_catcher<EXT>(I)) return f3(0.0f);         // directMIS skips it (direct.cuh:129)
     rng.next();  // two draws the reference makes and never reads (direct.cuh:79)
     rng.next();
     float3 wi;
@@ -383,7 +398,7 @@ NB_D float3 path_radiance(const DevScene& S, float3 o, float3 d, Rng& rng, const
         uint32_t stype;
         const float3 f = bsdf_sample<EXT>(I.lobe, m, I.F, I.wo, BSDF_ALL, rng, wi, pdf, stype);
         if (pdf == 0.0f) break;
-        beta *= f * absdot(wi, I.F.n) / pdf;
+        beta *= (is_catcher<EXT>(I) ? f * catcher_sky(S, I) : f) * absdot(wi, I.F.n) / pdf;
         // correct_sidedness (accumulate.cuh:40-45)
         if (!(I.mtype & kTransparentMat) && dot(wi, I.F.ng) < 0.0f) break;
         // rr_terminate (accumulate.cuh:27-38)

@@ -56,6 +56,10 @@ struct __align__(16) DevMaterial {
     float rough_x;
     float3 k;
     float rough_y;
+    float coat_weight;      // clear coat
+    float coat_sigma;
+    float coat_thickness;
+    float pad;
 };
 
 struct DevAreaLight {

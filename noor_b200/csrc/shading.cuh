@@ -430,6 +430,13 @@ enum : uint32_t {
     kLobeMicroT = BSDF_TRANSMISSION | BSDF_GLOSSY | BSDF_DIELECTRIC,
     // CudaFresnelBlend (bxdf.cuh:658-752)
     kLobeFresnelBlend = (BSDF_REFLECTION | BSDF_GLOSSY | BSDF_DIELECTRIC) | 2u << 8,
+    // CudaClearCoat (bxdf.cuh:842-992): a conductor microfacet substrate
+    // under a dielectric specular coat
+    kLobeClearCoat = (BSDF_GLOSSY | BSDF_REFLECTION | BSDF_SPECULAR) | 3u << 8,
+    // CudaShadowCatcher (bxdf.cuh:203-250).  Its value is the sky seen
+    // along the incoming ray over |cos wi|; the lobe functions return the
+    // 1 / |cos wi| part and the integrator multiplies in the sky
+    kLobeCatcher = (BSDF_REFLECTION | BSDF_TRANSMISSION | BSDF_DIFFUSE) | 4u << 8,
 };
 NB_HD uint32_t lobe_type(uint32_t id) { return id & 0xFFu; }
 
@@ -438,8 +445,8 @@ constexpr uint32_t kTransparentMat = NOOR_TRANSLUCENT | NOOR_GLASS | NOOR_ROUGHG
 constexpr uint32_t kEmitterMat = NOOR_EMITTER | NOOR_MESHLIGHT;
 
 // The lobes factoryBSDF builds for a material (noor/cuda/bsdf.cuh:383-461),
-// in the order it adds them: lobe k in bits 16k..16k+15; 0 = none.
-// Clear-coat and shadow-catcher materials build none here.
+// in the order it adds them: lobe k in bits 16k..16k+15; 0 = none (an
+// Oren-Nayar material or a mix of type bits builds none there either).
 NB_HD uint32_t lobe_of(uint32_t mtype) {
     const uint32_t t = mtype & ~(uint32_t)(NOOR_BUMP | NOOR_ALPHA);
     switch (t) {
@@ -451,6 +458,8 @@ NB_HD uint32_t lobe_of(uint32_t mtype) {
         case NOOR_TRANSLUCENT: return kLobeLambert | kLobeLambertT << 16;
         case NOOR_GLOSSY: return kLobeLambert | kLobeMicroDiel << 16;
         case NOOR_ROUGHGLASS: return kLobeMicroDiel | kLobeMicroT << 16;
+        case NOOR_CLEARCOAT: return kLobeClearCoat;
+        case NOOR_SHADOWCATCHER: return kLobeCatcher;
         default: return 0u;
     }
 }
@@ -491,22 +500,71 @@ NB_D float3 schlick(const DevMaterial& m, float c) { return m.specular + pow5(1.
 NB_D float3 lobe_eval(uint32_t lobe, const DevMaterial& m, const float3& wo, const float3& wi);
 NB_D float lobe_pdf(uint32_t lobe, const DevMaterial& m, const float3& wo, const float3& wi);
 
+// CudaMicrofacetReflection (bxdf.cuh:472-557) with the conductor or the
+// dielectric Fresnel
+NB_D float3 micro_refl_eval(const DevMaterial& m, const float3& wo, const float3& wi, bool conductor) {
+    // CudaMicrofacetReflection::Eval (bxdf.cuh:482-506)
+    if (!same_hemi(wo, wi)) return f3(0.0f);
+    const float cO = fabsf(wo.z), cI = fabsf(wi.z);
+    if (cI == 0.0f || cO == 0.0f) return f3(0.0f);
+    float3 wh = normalize_fast(wi + wo);
+    if (is_black(wh)) return f3(0.0f);
+    wh *= signf_ref(wh.z);
+    const float3 F = conductor ? fresnel_conductor(dot(wo, wh), m.ior, m.k)
+                                            : f3(fresnel_dielectric(dot(wo, wh), 1.0f, m.coat_ior));
+    const Micro mf = make_micro(m);
+    return F * m.specular * mf.D(wh) * mf.G(wo, wi) / (4.0f * cI * cO);
+}
+NB_D float micro_refl_pdf(const DevMaterial& m, const float3& wo, const float3& wi) {
+    if (!same_hemi(wo, wi)) return 0.0f;
+    const float3 wh = normalize_guard(wo + wi);
+    const Micro mf = make_micro(m);
+    return mf.pdf(wo, wh) / (4.0f * dot(wo, wh));
+}
+NB_D float3 micro_refl_sample(const DevMaterial& m, const float3& wo, float ux, float uy, float3& wi, float& pdf,
+                              bool conductor) {
+    // CudaMicrofacetReflection::Sample_f (bxdf.cuh:520-539)
+    if (wo.z == 0.0f) return f3(0.0f);
+    const Micro mf = make_micro(m);
+    const float3 wh = mf.sample_wh(wo, ux, uy);
+    wi = -1.0f * wo + 2.0f * dot(wo, wh) * wh;
+    if (!same_hemi(wo, wi)) {
+        pdf = 0.0f;
+        return f3(0.0f);
+    }
+    pdf = mf.pdf(wo, wh) / (4.0f * dot(wo, wh));
+    return micro_refl_eval(m, wo, wi, conductor);
+}
+
+// CudaClearCoat::absorption (bxdf.cuh:849-860)
+NB_D float coat_absorption(const DevMaterial& m, const float3& wo, const float3& wi) {
+    const float sa = m.coat_sigma * m.coat_thickness;
+    if (sa != 0.0f) return expf(-sa * (1.0f / fabsf(wo.z) + 1.0f / fabsf(wi.z)));
+    return 1.0f;
+}
+// the coat's Refract of wo and wi into the substrate, negated
+// (bxdf.cuh:869-874); a failed refraction leaves the zero vector (the
+// reference leaves the vector unset; with coat_ior > 1 it cannot fail)
+NB_D void coat_refract(const DevMaterial& m, const float3& wo, const float3& wi, float3& wo_c, float3& wi_c) {
+    const float eta = 1.0f / m.coat_ior;
+    const float3 n = f3(0.0f, 0.0f, 1.0f);
+    wo_c = f3(0.0f);
+    wi_c = f3(0.0f);
+    refract_ref(wo, n, eta, wo_c);
+    refract_ref(wi, n, eta, wi_c);
+    wo_c *= -1.0f;
+    wi_c *= -1.0f;
+}
+// probability of sampling the coat (bxdf.cuh:891, 908)
+NB_D float coat_prob(const DevMaterial& m, float F) {
+    const float w = m.coat_weight;
+    return F * w / (F * w + (1.0f - F) * (1.0f - w));
+}
+
 // BxDF::Eval of a lobe, local frame (every lobe)
 NB_D float3 lobe_eval_all(uint32_t lobe, const DevMaterial& m, const float3& wo, const float3& wi) {
     if (lobe == kLobeLambert || lobe == kLobeLambertT) return m.diffuse * kInvPi;
-    if (lobe == kLobeConductor || lobe == kLobeMicroDiel) {
-        // CudaMicrofacetReflection::Eval (bxdf.cuh:482-506)
-        if (!same_hemi(wo, wi)) return f3(0.0f);
-        const float cO = fabsf(wo.z), cI = fabsf(wi.z);
-        if (cI == 0.0f || cO == 0.0f) return f3(0.0f);
-        float3 wh = normalize_fast(wi + wo);
-        if (is_black(wh)) return f3(0.0f);
-        wh *= signf_ref(wh.z);
-        const float3 F = lobe == kLobeConductor ? fresnel_conductor(dot(wo, wh), m.ior, m.k)
-                                                : f3(fresnel_dielectric(dot(wo, wh), 1.0f, m.coat_ior));
-        const Micro mf = make_micro(m);
-        return F * m.specular * mf.D(wh) * mf.G(wo, wi) / (4.0f * cI * cO);
-    }
+    if (lobe == kLobeConductor || lobe == kLobeMicroDiel) return micro_refl_eval(m, wo, wi, lobe == kLobeConductor);
     if (lobe == kLobeMicroT) {
         // CudaMicrofacetTransmission::Eval (bxdf.cuh:567-590); etaI = 1, etaT = coat_ior
         if (same_hemi(wo, wi)) return f3(0.0f);
@@ -533,17 +591,22 @@ NB_D float3 lobe_eval_all(uint32_t lobe, const DevMaterial& m, const float3& wo,
             mf.D(wh) / (4.0f * absdot(wi, wh) * fmaxf(fabsf(wi.z), fabsf(wo.z))) * schlick(m, dot(wi, wh));
         return diffuse + specular;
     }
+    if (lobe == kLobeClearCoat) {
+        // CudaClearCoat::Eval (bxdf.cuh:862-880)
+        const float F0 = fresnel_dielectric(wo.z, 1.0f, m.coat_ior);
+        const float F1 = fresnel_dielectric(wi.z, 1.0f, m.coat_ior);
+        float3 wo_c, wi_c;
+        coat_refract(m, wo, wi, wo_c, wi_c);
+        const float3 r = micro_refl_eval(m, wo_c, wi_c, true) * (1.0f - F0) * (1.0f - F1);
+        return r * coat_absorption(m, wo_c, wi_c);
+    }
+    if (lobe == kLobeCatcher) return f3(1.0f / fabsf(wi.z));  // times the sky (bxdf.cuh:213-218)
     return f3(0.0f);  // specular lobes: delta
 }
 NB_D float lobe_pdf_all(uint32_t lobe, const DevMaterial& m, const float3& wo, const float3& wi) {
     if (lobe == kLobeLambert) return same_hemi(wo, wi) ? fabsf(wi.z) * kInvPi : 0.0f;
     if (lobe == kLobeLambertT) return !same_hemi(wo, wi) ? fabsf(wi.z) * kInvPi : 0.0f;
-    if (lobe == kLobeConductor || lobe == kLobeMicroDiel) {
-        if (!same_hemi(wo, wi)) return 0.0f;
-        const float3 wh = normalize_guard(wo + wi);
-        const Micro mf = make_micro(m);
-        return mf.pdf(wo, wh) / (4.0f * dot(wo, wh));
-    }
+    if (lobe == kLobeConductor || lobe == kLobeMicroDiel) return micro_refl_pdf(m, wo, wi);
     if (lobe == kLobeMicroT) {
         // CudaMicrofacetTransmission::Pdf (bxdf.cuh:592-606)
         if (same_hemi(wo, wi)) return 0.0f;
@@ -562,6 +625,16 @@ NB_D float lobe_pdf_all(uint32_t lobe, const DevMaterial& m, const float3& wo, c
         const float pdf_wh = mf.pdf(wo, wh);
         return 0.5f * (fabsf(wi.z) * kInvPi + pdf_wh / (4.0f * dot(wo, wh)));
     }
+    if (lobe == kLobeClearCoat) {
+        // CudaClearCoat::Pdf (bxdf.cuh:882-902): the substrate's density
+        // plus the coat's probability
+        const float F = fresnel_dielectric(wo.z, 1.0f, m.coat_ior);
+        float3 wo_c, wi_c;
+        coat_refract(m, wo, wi, wo_c, wi_c);
+        const float c = coat_prob(m, F);
+        return micro_refl_pdf(m, wo_c, wi_c) * (1.0f - c) + c;
+    }
+    if (lobe == kLobeCatcher) return 1.0f;
     return 0.0f;
 }
 // BxDF::Sample_f of a lobe (u already remapped by the BSDF); pdf stays 0 on
@@ -576,19 +649,8 @@ NB_D float3 lobe_sample_all(uint32_t lobe, const DevMaterial& m, const float3& w
         pdf = lobe_pdf(lobe, m, wo, wi);
         return m.diffuse * kInvPi;
     }
-    if (lobe == kLobeConductor || lobe == kLobeMicroDiel) {
-        // CudaMicrofacetReflection::Sample_f (bxdf.cuh:520-539)
-        if (wo.z == 0.0f) return f3(0.0f);
-        const Micro mf = make_micro(m);
-        const float3 wh = mf.sample_wh(wo, ux, uy);
-        wi = -1.0f * wo + 2.0f * dot(wo, wh) * wh;
-        if (!same_hemi(wo, wi)) {
-            pdf = 0.0f;
-            return f3(0.0f);
-        }
-        pdf = mf.pdf(wo, wh) / (4.0f * dot(wo, wh));
-        return lobe_eval(lobe, m, wo, wi);
-    }
+    if (lobe == kLobeConductor || lobe == kLobeMicroDiel)
+        return micro_refl_sample(m, wo, ux, uy, wi, pdf, lobe == kLobeConductor);
     if (lobe == kLobeMirror) {
         // CudaSpecularReflection::Sample_f (bxdf.cuh:377-392), no-op Fresnel
         wi = f3(-wo.x, -wo.y, wo.z);
@@ -630,6 +692,46 @@ NB_D float3 lobe_sample_all(uint32_t lobe, const DevMaterial& m, const float3& w
         }
         pdf = lobe_pdf(lobe, m, wo, wi);
         return lobe_eval(lobe, m, wo, wi);
+    }
+    if (lobe == kLobeClearCoat) {
+        // CudaClearCoat::Sample_f (bxdf.cuh:904-950): the second number
+        // chooses coat or substrate and is rescaled for the choice
+        const float F0 = fresnel_dielectric(wo.z, 1.0f, m.coat_ior);
+        const float ps = coat_prob(m, F0);
+        if (uy < ps) {
+            // CudaSpecularReflection::Sample_f with the dielectric Fresnel
+            wi = f3(-wo.x, -wo.y, wo.z);
+            pdf = ps;
+            stype = BSDF_DIELECTRIC | BSDF_REFLECTION | BSDF_SPECULAR;
+            return fresnel_dielectric(wi.z, 1.0f, m.coat_ior) * m.diffuse / fabsf(wi.z);
+        }
+        const float sy = (uy - ps) / (1.0f - ps);
+        const float eta = 1.0f / m.coat_ior;
+        float3 wo_c = f3(0.0f), wi_c;
+        refract_ref(wo, f3(0.0f, 0.0f, 1.0f), eta, wo_c);
+        float p = 0.0f;
+        float3 r = micro_refl_sample(m, -1.0f * wo_c, ux, sy, wi_c, p, true);
+        stype = kLobeConductor;
+        if (p == 0.0f) return f3(0.0f);
+        const float F1 = fresnel_dielectric(-wi_c.z, 1.0f, m.coat_ior);
+        // refract out; under total internal reflection the reference
+        // leaves wi unset, here the sample fails
+        if (!refract_ref(-1.0f * wi_c, f3(0.0f, 0.0f, -1.0f), 1.0f / eta, wi)) return f3(0.0f);
+        if (F1 == 1.0f) return f3(0.0f);
+        r *= coat_absorption(m, wo_c, wi_c) * (1.0f - F0) * (1.0f - F1);
+        r /= fabsf(wi_c.z);
+        pdf = p * (1.0f - ps);
+        return r;
+    }
+    if (lobe == kLobeCatcher) {
+        // CudaShadowCatcher::Sample_f: uniformSampleHemisphere (utils.cuh,
+        // left-handed: z = u.x) with pdf 1, as the reference has it
+        const float z = ux;
+        const float r = sqrtf(fmaxf(0.0f, 1.0f - z * z));
+        const float phi = k2Pi * uy;
+        wi = f3(r * cosf(phi), r * sinf(phi), z);
+        pdf = 1.0f;
+        return f3(1.0f / fabsf(wi.z));
     }
     if (lobe == kLobeFresnelSpec) {
         // CudaFresnelSpecular::Sample_f (bxdf.cuh:775-809), IOR = coat_ior

@@ -459,7 +459,7 @@ __global__ void __launch_bounds__(256, NB_SHADE_MIN_BLOCKS) wf_shade(WfDev W, ui
         if (pdf == 0.0f) {
             st = kFinishing;
         } else {
-            beta *= f * absdot(wi, I.F.n) / pdf;
+            beta *= (is_catcher<EXT>(I) ? f * catcher_sky(S, I) : f) * absdot(wi, I.F.n) / pdf;
             if (!(I.mtype & kTransparentMat) && dot(wi, I.F.ng) < 0.0f) {
                 st = kFinishing;
             } else if (bounce >= S.rr) {

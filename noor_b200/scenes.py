@@ -27,22 +27,30 @@ IDENTITY = np.eye(4, dtype=np.float32).reshape(-1, order="F")
 
 
 def material(kind: str, albedo=(0.5, 0.5, 0.5), roughness: float = 0.1, ior: float = 1.5,
-             emittance=(0.0, 0.0, 0.0), distribution: int = 0, specular=(1.0, 1.0, 1.0)) -> dict:
+             emittance=(0.0, 0.0, 0.0), distribution: int = 0, specular=(1.0, 1.0, 1.0), coat_weight: float = 1.0,
+             coat_sigma: float = 0.0, coat_thickness: float = 1.0) -> dict:
     """Constant material parameters (AssetLoader getters) for one of
     'diffuse', 'metal' (gold conductor, `specular` tints it), 'glass',
     'emitter', 'mirror' (albedo is the reflectance), 'substrate' (Fresnel
     blend of the albedo under a `specular` coat), 'translucent' (albedo
     reflected and transmitted), 'glossy' (albedo under a dielectric
-    microfacet coat) or 'roughglass' (dielectric microfacet reflection and
-    transmission)."""
+    microfacet coat), 'roughglass' (dielectric microfacet reflection and
+    transmission), 'clearcoat' (a gold microfacet substrate tinted by
+    `specular` under a dielectric coat of index `ior` whose reflection is
+    tinted by `albedo`; `coat_weight` sets how often the coat is sampled,
+    `coat_sigma` x `coat_thickness` its absorption) or 'shadowcatcher'
+    (shows the sky where lights reach it)."""
     types = {"diffuse": capi.NOOR_DIFFUSE, "metal": capi.NOOR_METAL, "glass": capi.NOOR_GLASS,
              "emitter": capi.NOOR_EMITTER, "mirror": capi.NOOR_MIRROR, "substrate": capi.NOOR_SUBSTRATE,
-             "translucent": capi.NOOR_TRANSLUCENT, "glossy": capi.NOOR_GLOSSY, "roughglass": capi.NOOR_ROUGHGLASS}
+             "translucent": capi.NOOR_TRANSLUCENT, "glossy": capi.NOOR_GLOSSY, "roughglass": capi.NOOR_ROUGHGLASS,
+             "clearcoat": capi.NOOR_CLEARCOAT, "shadowcatcher": capi.NOOR_SHADOWCATCHER}
+    gold = kind in ("metal", "clearcoat")
     return dict(diffuse=tuple(albedo), specular=tuple(float(x) for x in specular), transmission=(1.0, 1.0, 1.0),
                 emittance=tuple(emittance), transparency=(1.0, 1.0, 1.0),
-                ior=GOLD_ETA if kind == "metal" else (ior, ior, ior), k=GOLD_K if kind == "metal" else (0, 0, 0),
-                roughness=(roughness, roughness), coat_weight=1.0, coat_roughness=0.001, coat_thickness=1.0,
-                coat_sigma=0.0, coat_ior=ior, emitter_scale=1.0, type=types[kind], distribution=distribution)
+                ior=GOLD_ETA if gold else (ior, ior, ior), k=GOLD_K if gold else (0, 0, 0),
+                roughness=(roughness, roughness), coat_weight=coat_weight, coat_roughness=0.001,
+                coat_thickness=coat_thickness, coat_sigma=coat_sigma, coat_ior=ior, emitter_scale=1.0,
+                type=types[kind], distribution=distribution)
 
 
 @dataclass

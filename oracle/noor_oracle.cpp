@@ -116,7 +116,7 @@ struct Scene {
     // per-material constants resolved from the 1x1 textures
     struct Mat {
         float diffuse[3], specular[3], transmission[3], emittance[3], ior[3], k[3];
-        float rx, ry, coat_ior, emitter_scale;
+        float rx, ry, coat_ior, emitter_scale, coat_weight, coat_sigma, coat_thickness;
         uint32_t type, dist;
     };
     std::vector<Mat> mats;
@@ -676,7 +676,8 @@ enum : uint32_t {
 };
 // lobe ids, one per BxDF class of bxdf.cuh:119-137 the factory builds
 enum : uint32_t {
-    kLambert = 1, kCond = 2, kFSpec = 3, kLambertT = 4, kMirror = 5, kMicroDiel = 6, kMicroT = 7, kFBlend = 8
+    kLambert = 1, kCond = 2, kFSpec = 3, kLambertT = 4, kMirror = 5, kMicroDiel = 6, kMicroT = 7, kFBlend = 8,
+    kCoat = 9, kCatcher = 10
 };
 // the BxDF type flags of each lobe (the constructors in bxdf.cuh)
 inline uint32_t ltype(uint32_t id) {
@@ -689,6 +690,8 @@ inline uint32_t ltype(uint32_t id) {
         case kMicroDiel: return B_DIEL | B_REFL | B_GLOSSY;
         case kMicroT: return B_TRANS | B_GLOSSY | B_DIEL;
         case kFBlend: return B_REFL | B_GLOSSY | B_DIEL;
+        case kCoat: return B_GLOSSY | B_REFL | B_SPEC;
+        case kCatcher: return B_REFL | B_TRANS | B_DIFF;
         default: return 0u;
     }
 }
@@ -708,6 +711,8 @@ inline uint32_t lobe_of(uint32_t mt) {
         case NOOR_TRANSLUCENT: return kLambert | kLambertT << 8;
         case NOOR_GLOSSY: return kLambert | kMicroDiel << 8;
         case NOOR_ROUGHGLASS: return kMicroDiel | kMicroT << 8;
+        case NOOR_CLEARCOAT: return kCoat;
+        case NOOR_SHADOWCATCHER: return kCatcher;
         default: return 0u;
     }
 }
@@ -739,6 +744,30 @@ template <class T> T pow5(T v) {
     const T a = v * v;
     return a * a * v;
 }
+// CudaClearCoat helpers (bxdf.cuh:849-908): absorption, the refraction of
+// wo and wi into the substrate (negated; a failed one leaves zero), the
+// probability of the coat
+template <class T> T coat_abs(const Scene::Mat& m, V<T> wo, V<T> wi) {
+    const T sa = (T)m.coat_sigma * (T)m.coat_thickness;
+    if (sa != T(0)) return std::exp(-sa * (T(1) / std::fabs(wo.z) + T(1) / std::fabs(wi.z)));
+    return T(1);
+}
+template <class T> void coat_in(const Scene::Mat& m, V<T> wo, V<T> wi, V<T>& wo_c, V<T>& wi_c) {
+    const T eta = T(1) / (T)m.coat_ior;
+    const V<T> n = mk(T(0), T(0), T(1));
+    wo_c = mk(T(0), T(0), T(0));
+    wi_c = wo_c;
+    refract_r<T>(wo, n, eta, wo_c);
+    refract_r<T>(wi, n, eta, wi_c);
+    wo_c = T(-1) * wo_c;
+    wi_c = T(-1) * wi_c;
+}
+template <class T> T coat_p(const Scene::Mat& m, T F) {
+    const T w = (T)m.coat_weight;
+    return F * w / (F * w + (T(1) - F) * (T(1) - w));
+}
+template <class T> V<T> lobe_eval(uint32_t lobe, const Scene::Mat& m, V<T> wo, V<T> wi);
+
 // BxDF Eval of bxdf.cuh: 252-299 (Lambert), 301-352 (Lambert
 // transmission), 472-557 (MicrofacetReflection), 559-656 (Microfacet-
 // Transmission), 658-752 (FresnelBlend)
@@ -787,6 +816,14 @@ template <class T> V<T> lobe_eval(uint32_t lobe, const Scene::Mat& m, V<T> wo, V
             mf.D(wh) / (T(4) * std::fabs(dot(wi, wh)) * std::max(std::fabs(wi.z), std::fabs(wo.z))) * schlick;
         return diffuse + specular;
     }
+    if (lobe == kCoat) {
+        const T F0 = fr_diel(wo.z, T(1), (T)m.coat_ior), F1 = fr_diel(wi.z, T(1), (T)m.coat_ior);
+        V<T> wo_c, wi_c;
+        coat_in<T>(m, wo, wi, wo_c, wi_c);
+        return lobe_eval<T>(kCond, m, wo_c, wi_c) * (T(1) - F0) * (T(1) - F1) * coat_abs<T>(m, wo_c, wi_c);
+    }
+    // the shadow catcher's 1 / |cos wi|; the caller multiplies in the sky
+    if (lobe == kCatcher) return mk(T(1), T(1), T(1)) * (T(1) / std::fabs(wi.z));
     return zero;
 }
 template <class T> T lobe_pdf(uint32_t lobe, const Scene::Mat& m, V<T> wo, V<T> wi) {
@@ -815,6 +852,14 @@ template <class T> T lobe_pdf(uint32_t lobe, const Scene::Mat& m, V<T> wo, V<T> 
         const T pwh = mf.pdf(wo, wh);
         return T(0.5) * (std::fabs(wi.z) * K<T>::inv_pi + pwh / (T(4) * dot(wo, wh)));
     }
+    if (lobe == kCoat) {
+        const T F = fr_diel(wo.z, T(1), (T)m.coat_ior);
+        V<T> wo_c, wi_c;
+        coat_in<T>(m, wo, wi, wo_c, wi_c);
+        const T c = coat_p<T>(m, F);
+        return lobe_pdf<T>(kCond, m, wo_c, wi_c) * (T(1) - c) + c;
+    }
+    if (lobe == kCatcher) return T(1);
     return T(0);
 }
 // concentricSampleDisk / cosineSampleHemisphere (utils.cuh:377-404)
@@ -903,6 +948,42 @@ template <class T> V<T> lobe_sample(uint32_t lobe, const Scene::Mat& m, V<T> wo,
         }
         pdf = lobe_pdf<T>(lobe, m, wo, wi);
         return lobe_eval<T>(lobe, m, wo, wi);
+    }
+    if (lobe == kCoat) {
+        const T ior = (T)m.coat_ior;
+        const T F0 = fr_diel(wo.z, T(1), ior);
+        const T ps = coat_p<T>(m, F0);
+        if (uy < ps) {
+            wi = mk(-wo.x, -wo.y, wo.z);
+            pdf = ps;
+            st = B_DIEL | B_REFL | B_SPEC;
+            return fr_diel(wi.z, T(1), ior) * v3f<T>(m.diffuse) / std::fabs(wi.z);
+        }
+        const T sy = (uy - ps) / (T(1) - ps);
+        const T eta = T(1) / ior;
+        V<T> wo_c = zero, wi_c = zero;
+        refract_r<T>(wo, mk(T(0), T(0), T(1)), eta, wo_c);
+        T p = 0;
+        uint32_t st2;
+        V<T> r = lobe_sample<T>(kCond, m, T(-1) * wo_c, ux, sy, wi_c, p, st2);
+        st = ltype(kCond);
+        if (p == T(0)) return zero;
+        const T F1 = fr_diel(-wi_c.z, T(1), ior);
+        if (!refract_r<T>(T(-1) * wi_c, mk(T(0), T(0), T(-1)), T(1) / eta, wi)) return zero;
+        if (F1 == T(1)) return zero;
+        r = r * (coat_abs<T>(m, wo_c, wi_c) * (T(1) - F0) * (T(1) - F1));
+        r = r / std::fabs(wi_c.z);
+        pdf = p * (T(1) - ps);
+        return r;
+    }
+    if (lobe == kCatcher) {
+        // uniformSampleHemisphere, left-handed (z = u.x), pdf 1 as in the reference
+        const T z = ux;
+        const T r = std::sqrt(std::max(T(0), T(1) - z * z));
+        const T phi = T(2) * K<T>::pi * uy;
+        wi = mk(r * std::cos(phi), r * std::sin(phi), z);
+        pdf = T(1);
+        return mk(T(1), T(1), T(1)) * (T(1) / std::fabs(wi.z));
     }
     if (lobe == kFSpec) {
         const T ior = (T)m.coat_ior;
@@ -1292,6 +1373,11 @@ template <class T> bool occl(const Scene& sc, V<T> o, V<T> d, T tmax, int isect,
     return r;
 }
 
+// the shadow catcher's sky factor (bxdf.cuh:213-218)
+template <class T> V<T> catcher_sky(const Scene& sc, const Is<T>& I) {
+    return env_eval<T>(sc, T(-1) * to_world(I.F, to_local(I.F, I.wo)));
+}
+
 // sampleLight / sampleBSDF (direct.cuh:32-110) with the build's stated
 // choices for the unpicked-light case (no BSDF half, no draws)
 template <class T>
@@ -1306,6 +1392,7 @@ V<T> direct(const Scene& sc, const Scene::Mat& m, const Is<T>& I, Rng& rng, int 
     const int na = sc.P->num_area_lights;
     const int nd = sc.P->num_point_lights + sc.P->num_spot_lights + sc.P->num_distant_lights;
     const bool delta = li >= na && li < na + nd;
+    const bool catcher = I.lobe == kCatcher;
     const uint32_t nonspec = B_ALL & ~B_SPEC;
     V<T> Ld = zero;
     {
@@ -1335,11 +1422,14 @@ V<T> direct(const Scene& sc, const Scene::Mat& m, const Is<T>& I, Rng& rng, int 
         Li = Li * (T)nl;
         if (lpdf != T(0) && !black(Li)) {
             V<T> f = bsdf_eval<T>(I.lobe, m, I.F, I.wo, wi, nonspec);
+            if (catcher) f = f * catcher_sky<T>(sc, I);
             if (!black(f)) {
                 f = f * std::fabs(dot(wi, I.F.n));
                 const V<T> so = spawn(I, wi, bias);
                 if (!occl<T>(sc, so, wi, len(so - to), isect, c)) {
-                    if (!mis || delta) {
+                    if (catcher) {
+                        Ld = f;   // direct.cuh:51
+                    } else if (!mis || delta) {
                         Ld = Li * f / lpdf;
                     } else {
                         const T sp = bsdf_pdf<T>(I.lobe, m, I.F, I.wo, wi, nonspec);
@@ -1350,8 +1440,9 @@ V<T> direct(const Scene& sc, const Scene::Mat& m, const Is<T>& I, Rng& rng, int 
         }
     }
     if (!mis) return Ld;
-    // sampleBSDF: nothing (and no draw) for a delta light
-    if (delta) return Ld;
+    // sampleBSDF: nothing (and no draw) for a delta light or a shadow
+    // catcher (direct.cuh:77, 129)
+    if (delta || catcher) return Ld;
     rng.next();
     rng.next();
     V<T> wi;
@@ -1440,8 +1531,9 @@ template <class T> V<T> radiance(const Scene& sc, V<T> o, V<T> d, Rng& rng, int 
         V<T> wi;
         T pdf;
         uint32_t st;
-        const V<T> f = bsdf_sample<T>(I.lobe, m, I.F, I.wo, B_ALL, rng, wi, pdf, st);
+        V<T> f = bsdf_sample<T>(I.lobe, m, I.F, I.wo, B_ALL, rng, wi, pdf, st);
         if (pdf == T(0)) break;
+        if (I.lobe == kCatcher) f = f * catcher_sky<T>(sc, I);
         beta = beta * (f * std::fabs(dot(wi, I.F.n)) / pdf);
         if (!(I.mt & kTranspMat) && dot(wi, I.F.ng) < T(0)) break;
         if (b >= sc.S->rr) {
@@ -1822,6 +1914,9 @@ OR_API void* oracle_create(const noor_payload* P, const noor_spec* S, const noor
         d.rx = P->textures[m.roughness_tex_idx].rgba[0];
         d.ry = P->textures[m.roughness_tex_idx].rgba[1];
         d.coat_ior = m.coat_ior;
+        d.coat_weight = m.coat_weight;
+        d.coat_sigma = m.coat_sigma;
+        d.coat_thickness = m.coat_thickness;
         d.emitter_scale = m.emitter_scale;
         d.type = m.type;
         d.dist = m.distribution;

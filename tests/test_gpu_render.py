@@ -123,7 +123,8 @@ def test_sphere_field_matches_oracle(kind):
         r.close()
 
 
-@pytest.mark.parametrize("pair", [("glossy", "roughglass"), ("substrate", "mirror"), ("translucent", "glossy")])
+@pytest.mark.parametrize("pair", [("glossy", "roughglass"), ("substrate", "mirror"), ("translucent", "glossy"),
+                                  ("clearcoat", "shadowcatcher")])
 def test_room_with_other_materials_matches_oracle(pair):
     """the lobes no configuration uses, on the two boxes: GPU megakernel and
     wavefront against the oracle on the same seeds"""
@@ -131,7 +132,10 @@ def test_room_with_other_materials_matches_oracle(pair):
           "roughglass": dict(roughness=0.3, ior=1.5),
           "substrate": dict(albedo=(0.3, 0.5, 0.7), specular=(0.05, 0.05, 0.05), roughness=0.3),
           "mirror": dict(albedo=(0.9, 0.9, 0.9)),
-          "translucent": dict(albedo=(0.6, 0.6, 0.5))}
+          "translucent": dict(albedo=(0.6, 0.6, 0.5)),
+          "clearcoat": dict(albedo=(0.9, 0.9, 0.9), specular=(0.8, 0.6, 0.5), roughness=0.3, coat_weight=0.5,
+                            coat_sigma=0.4, coat_thickness=0.5),
+          "shadowcatcher": dict()}
     boxes = [scenes.material(k, **kw[k]) for k in pair]
     s = scenes.room_scene(width=64, height=64, spp=16, box_materials=boxes)
     r = scenes.Renderer(s)

@@ -20,13 +20,19 @@ MATS = [scenes.material("diffuse", albedo=(0.2, 0.5, 0.8)),
         scenes.material("metal", roughness=float(np.sqrt(0.5))),
         scenes.material("metal", roughness=0.4, distribution=1),
         scenes.material("glass", ior=1.5),
-        # the lobes no configuration uses: mirror, Fresnel blend, and the
+        # the lobes no configuration uses: mirror, Fresnel blend, the
         # two-lobe materials (translucent, glossy, rough glass)
         scenes.material("mirror", albedo=(0.9, 0.8, 0.7)),
         scenes.material("substrate", albedo=(0.3, 0.5, 0.7), specular=(0.04, 0.05, 0.06), roughness=0.3),
         scenes.material("translucent", albedo=(0.6, 0.5, 0.4)),
         scenes.material("glossy", albedo=(0.5, 0.3, 0.2), roughness=0.2, ior=1.5),
-        scenes.material("roughglass", roughness=0.3, ior=1.5)]
+        scenes.material("roughglass", roughness=0.3, ior=1.5),
+        # clear coat (substrate sampled half the time, with absorption) and
+        # the shadow catcher (without its sky factor, which the integrator
+        # applies)
+        scenes.material("clearcoat", albedo=(0.9, 0.9, 0.9), specular=(0.8, 0.6, 0.5), roughness=0.3, ior=1.5,
+                        coat_weight=0.5, coat_sigma=0.4, coat_thickness=0.5),
+        scenes.material("shadowcatcher")]
 
 
 def _scene(sky=_capi.NOOR_SKY_PHYSICAL, env=None):

@@ -151,3 +151,44 @@ def test_one_sided_disk_facing_away_is_dark():
     disk = dict(type="disk", center=(-r, h, -r), u=(0.0, 0.0, 2 * r), v=(2 * r, 0.0, 0.0), ke=(3.0, 3.0, 3.0))
     img, _, _ = render(floor_scene(area_lights=[disk]), 64)
     assert img.max() == 0.0
+
+
+def test_shadow_catcher_is_a_shadow_matte():
+    """a shadow-catcher floor under a point light, one bounce: where the
+    light is unblocked the pixel is the sky seen along the camera ray
+    (direct.cuh:51, bxdf.cuh:213-218), under the blocker it is 0"""
+    s = floor_scene(point_lights=[dict(position=(0.6, 1.5, 0.0), ke=(3.0, 3.0, 3.0))])
+    s.materials = [scenes.material("shadowcatcher"), scenes.material("diffuse")]
+    # a small blocker between the light and part of the floor (material 1)
+    q = np.array([[-0.05, 0.5, -0.05, 1], [0.15, 0.5, -0.05, 1], [0.15, 0.5, 0.15, 1], [-0.05, 0.5, 0.15, 1]],
+                 np.float32)
+    s.vertices = np.concatenate([s.vertices, q])
+    s.vindices = np.concatenate([s.vindices, np.array([[4, 5, 6], [4, 6, 7]], np.uint32)])
+    s.nindices = np.zeros((4, 3), np.uint32)
+    s.uvindices = np.zeros((4, 3), np.uint32)
+    s.material_indices = np.array([0, 0, 1, 1], np.uint32)
+    s.meshes = [dict(tri_start=0, tri_count=4, to_global=scenes.IDENTITY, instance=-1, light_idx=-1)]
+    img, rays, b = render(s, 1)
+    env = b.payload.textures[b.payload.num_textures - 1]
+    sky = np.array(env.rgba[0:3])
+    assert env.width == 1 and env.height == 1 and sky.max() > 0
+    # floor pixels in the blocker's shadow (the light is off to the side, so
+    # part of the shadow is not hidden behind the blocker)
+    x = floor_points(rays)
+    P = np.array([0.6, 1.5, 0.0])
+    t = (0.5 - x[:, 1]) / (P[1] - x[:, 1])
+    hit = x + t[:, None] * (P - x)
+    shadow = (hit[:, 0] > -0.05) & (hit[:, 0] < 0.15) & (hit[:, 2] > -0.05) & (hit[:, 2] < 0.15)
+    # pixels whose camera ray meets the blocker first show the blocker
+    o, d = rays[:, 0:3].astype(np.float64), rays[:, 4:7].astype(np.float64)
+    tb = (0.5 - o[:, 1]) / d[:, 1]
+    pb = o + tb[:, None] * d
+    on_blocker = (pb[:, 0] > -0.05) & (pb[:, 0] < 0.15) & (pb[:, 2] > -0.05) & (pb[:, 2] < 0.15)
+    pix = img.reshape(-1, 3)
+    lit = ~shadow & ~on_blocker
+    assert lit.sum() > 50 and (shadow & ~on_blocker).sum() > 3
+    np.testing.assert_allclose(pix[lit], np.broadcast_to(sky, (lit.sum(), 3)), rtol=1e-5)
+    # pixels whose shadow ray passes within the blocker's edge may go
+    # either way (the shadow ray starts off the floor by the bias)
+    dark = pix[shadow & ~on_blocker].max(1) == 0
+    assert dark.mean() > 0.8, dark.mean()
