@@ -346,6 +346,21 @@ int noor_render_frames(unsigned int* frame_count, unsigned int n_frames);
 int noor_get_framebuffer(float* host_rgba, size_t n_pixels);
 int noor_get_framebuffer_device(float* device_rgba, size_t n_pixels);
 int noor_reset_film(void);
+/* Headless display (noor/shader/cuda.fs:36-78, which the reference runs as
+ * a GL fragment shader over the film texture): the transforms of its
+ * `tonemap` subroutine, applied to exposure * rgb, then stored as 8-bit
+ * unorm (clamp to [0, 1], round to nearest) with alpha 255. */
+enum { NOOR_TONEMAP_NONE = -1, NOOR_TONEMAP_GAMMA = 0, NOOR_TONEMAP_REINHARD = 1, NOOR_TONEMAP_FILMIC = 2,
+       NOOR_TONEMAP_UNCHARTED2 = 3 };
+/* d_film_rgba: float4 per pixel (16-byte aligned device memory, e.g. from
+ * noor_get_framebuffer_device or a wavefront film); d_rgba8: 4 bytes per
+ * pixel, device memory, same pixel order. */
+int noor_tonemap_device(const float* d_film_rgba, size_t n_pixels, int op, float exposure, uint8_t* d_rgba8);
+/* The context's film as an image file: op NOOR_TONEMAP_NONE writes the
+ * linear film as PFM (bottom row first, as film row 0 is the bottom of the
+ * reference's GL window), any other op writes a binary PPM of the tonemapped
+ * film, top row first. */
+int noor_save_image(const char* path, int op, float exposure);
 /* Rays traced by the megakernel since the last reset (device counters):
  * [0] extension (closest-hit) rays, [1] shadow (any-hit) rays, [2] paths. */
 int noor_ray_counters(uint64_t counters[3], int reset);

@@ -41,6 +41,7 @@ NOOR_LIGHT_SKY_MASK = 0x20
 NOOR_ISECT_WATERTIGHT, NOOR_ISECT_REF_WALD = 0, 1
 NOOR_FILM_KAHAN, NOOR_FILM_REF_LERP = 0, 1
 NOOR_SHAPE_QUAD, NOOR_SHAPE_SPHERE, NOOR_SHAPE_DISK = 0, 1, 2
+NOOR_TONEMAP_NONE, NOOR_TONEMAP_GAMMA, NOOR_TONEMAP_REINHARD, NOOR_TONEMAP_FILMIC, NOOR_TONEMAP_UNCHARTED2 = -1, 0, 1, 2, 3
 NOOR_DEV_STACK_OVERFLOW = 1
 
 TRI_LEAF_MASK = 0x80000000
@@ -199,6 +200,8 @@ PROTOTYPES = {
     "noor_last_error": (C.c_char_p, []),
     "noor_device_count": (C.c_int, [C.POINTER(C.c_int)]),
     "noor_abi_sizes": (C.c_int, [pu, C.c_int]),
+    "noor_tonemap_device": (C.c_int, [C.c_void_p, C.c_size_t, C.c_int, C.c_float, C.c_void_p]),
+    "noor_save_image": (C.c_int, [C.c_char_p, C.c_int, C.c_float]),
     "noor_render_frames": (C.c_int, [C.POINTER(C.c_uint), C.c_uint]),
     "noor_get_framebuffer": (C.c_int, [pf, C.c_size_t]),
     "noor_get_framebuffer_device": (C.c_int, [C.c_void_p, C.c_size_t]),

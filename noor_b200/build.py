@@ -21,7 +21,7 @@ CSRC = PKG / "csrc"
 OUT = PKG / "libnoor_b200.so"
 OBJ = ROOT / "_build" / "noor_b200"
 
-CU_SOURCES = ["kernels.cu", "envmap.cu", "context.cu", "wavefront.cu", "adjoint.cu", "noalloc.cu"]
+CU_SOURCES = ["kernels.cu", "envmap.cu", "context.cu", "wavefront.cu", "adjoint.cu", "noalloc.cu", "tonemap.cu"]
 CPP_SOURCES = ["scene_build.cpp"]
 
 NVCC_FLAGS = [

@@ -198,3 +198,35 @@ def ref_hosek_dataset() -> np.ndarray:
     out = np.zeros(3 * 1080 + 3 * 120, np.float32)
     ref().ref_hosek_dataset(_p(out))
     return out
+
+
+# ------------------------------------------------- display (noor/shader/cuda.fs)
+def tonemap(film: np.ndarray, op: int, exposure: float = 1.0) -> np.ndarray:
+    """The display shader's transforms (noor/shader/cuda.fs:36-78) in FP32
+    numpy: op 0 gammaCorrect (c^(1/2.2)), 1 tonemapReinhard, 2 tonemapFilmic
+    (Hejl-Burgess-Dawson, gamma included), 3 tonemapUncharted2 (Hable's
+    curve, exposure bias 4, white 11.2); then an 8-bit unorm store (clamp to
+    [0, 1], round to nearest).  film: (..., 4) float; returns (..., 4) uint8
+    with alpha 255."""
+    f32 = np.float32
+    c = f32(exposure) * np.asarray(film, f32)[..., :3]
+    g = f32(1.0) / f32(2.2)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        if op == 1:
+            out = np.power(c / (c + f32(1)), g)
+        elif op == 2:
+            x = np.maximum(f32(0), c - f32(0.004))
+            out = (x * (f32(6.2) * x + f32(0.5))) / (x * (f32(6.2) * x + f32(1.7)) + f32(0.06))
+        elif op == 3:
+            A, B, Cc, D, E, F = (f32(v) for v in (0.15, 0.50, 0.10, 0.20, 0.02, 0.30))
+
+            def hable(x):
+                return ((x * (A * x + Cc * B) + D * E) / (x * (A * x + B) + D * F)) - E / F
+            ws = f32(1) / hable(f32(11.2))
+            out = np.power(hable(f32(4) * c) * ws, g)
+        else:
+            out = np.power(c, g)
+    out = np.nan_to_num(out.astype(f32), nan=0.0)
+    q = np.rint(np.clip(out, 0, 1) * f32(255)).astype(np.uint8)
+    alpha = np.full(q.shape[:-1] + (1,), 255, np.uint8)
+    return np.concatenate([q, alpha], axis=-1)
