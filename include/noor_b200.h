@@ -509,13 +509,22 @@ typedef struct noor_build_stat {
     float scene_min[3];
     float scene_max[3];
     float scene_radius;
-    double build_seconds;
+    double build_seconds;        /* the whole call                           */
+    double box_seconds;          /* triangle and mesh boxes (host)           */
+    double tree_seconds;         /* the trees: host, or GPU with transfers   */
+    double tree_device_ms;       /* GPU build: device time of the trees      */
 } noor_build_stat;
 
 typedef struct noor_payload_handle noor_payload_handle;
 /* Model::load + BVH build + Model::loadCudaPayload on the host. */
 int noor_build_payload(const noor_scene_desc* desc, noor_payload_handle** out,
                        noor_build_stat* stat);
+/* The same payload, bit for bit, with the per-mesh bottom-level trees built
+ * on the current CUDA device (level by level: binning, split search and
+ * partition in kernels; the top level over the meshes stays on the host).
+ * Needs a GPU; errors as noor_build_payload, plus NOOR_ERR_CUDA. */
+int noor_build_payload_gpu(const noor_scene_desc* desc, noor_payload_handle** out,
+                           noor_build_stat* stat);
 /* View of the owned arrays (valid until noor_free_payload). */
 int noor_payload_view(const noor_payload_handle* h, noor_payload* out);
 /* source triangle index of each BVH-ordered triangle */

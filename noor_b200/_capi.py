@@ -165,7 +165,8 @@ class SceneDesc(C.Structure):
 
 class BuildStat(C.Structure):
     _fields_ = [("height", u32), ("num_inner_nodes", u32), ("num_leaf_nodes", u32), ("max_leaf_tris", u32),
-                ("scene_min", f32 * 3), ("scene_max", f32 * 3), ("scene_radius", f32), ("build_seconds", C.c_double)]
+                ("scene_min", f32 * 3), ("scene_max", f32 * 3), ("scene_radius", f32), ("build_seconds", C.c_double),
+                ("box_seconds", C.c_double), ("tree_seconds", C.c_double), ("tree_device_ms", C.c_double)]
 
 
 class WfFrame(C.Structure):
@@ -200,6 +201,7 @@ PROTOTYPES = {
     "noor_last_error": (C.c_char_p, []),
     "noor_device_count": (C.c_int, [C.POINTER(C.c_int)]),
     "noor_abi_sizes": (C.c_int, [pu, C.c_int]),
+    "noor_build_payload_gpu": (C.c_int, [C.POINTER(SceneDesc), C.POINTER(C.c_void_p), C.POINTER(BuildStat)]),
     "noor_tonemap_device": (C.c_int, [C.c_void_p, C.c_size_t, C.c_int, C.c_float, C.c_void_p]),
     "noor_save_image": (C.c_int, [C.c_char_p, C.c_int, C.c_float]),
     "noor_render_frames": (C.c_int, [C.POINTER(C.c_uint), C.c_uint]),

@@ -21,7 +21,10 @@ CSRC = PKG / "csrc"
 OUT = PKG / "libnoor_b200.so"
 OBJ = ROOT / "_build" / "noor_b200"
 
-CU_SOURCES = ["kernels.cu", "envmap.cu", "context.cu", "wavefront.cu", "adjoint.cu", "noalloc.cu", "tonemap.cu"]
+CU_SOURCES = ["kernels.cu", "envmap.cu", "context.cu", "wavefront.cu", "adjoint.cu", "noalloc.cu", "tonemap.cu",
+              "bvh_gpu.cu"]
+# the GPU BVH builder rounds its split search as the host builder does
+CU_EXTRA = {"bvh_gpu.cu": ["-fmad=false"]}
 CPP_SOURCES = ["scene_build.cpp"]
 
 NVCC_FLAGS = [
@@ -68,7 +71,8 @@ def build(force: bool = False, verbose: bool = False, out: Path = OUT, obj: Path
         o = OBJ_ / (src + ".o")
         objs.append(o)
         if force or _stale(o, [s] + headers):
-            jobs.append([nvcc, *NVCC_FLAGS, *[f"-D{d}" for d in defines], "-c", str(s), "-o", str(o)])
+            jobs.append([nvcc, *NVCC_FLAGS, *CU_EXTRA.get(src, []), *[f"-D{d}" for d in defines], "-c", str(s),
+                         "-o", str(o)])
     for src in CPP_SOURCES:
         s = CSRC / src
         o = OBJ_ / (src + ".o")

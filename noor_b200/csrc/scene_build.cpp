@@ -35,6 +35,7 @@
 #include <vector>
 
 #include "../../include/noor_b200.h"
+#include "bvh_gpu.h"
 #include "host_common.h"
 
 namespace nbh {
@@ -272,11 +273,18 @@ struct Work {
     }
 };
 
+// a failure of the GPU tree build
+struct GpuBuildError {
+    int code;
+    std::string msg;
+};
+
 class Builder {
 public:
-    Builder(const noor_scene_desc& d) : D(d) {}
+    Builder(const noor_scene_desc& d, bool gpu) : D(d), use_gpu(gpu) {}
 
     const noor_scene_desc& D;
+    bool use_gpu;  // bottom-level trees built on the current CUDA device
     std::vector<Box> tri_box;
     std::vector<MeshInfo> meshes;
     Box scene_box, scene_cbox;
@@ -284,6 +292,7 @@ public:
     std::vector<uint32_t> nodes;  // the final node array: mesh trees in mesh order, then the top tree
     uint32_t root = 0;
     noor_build_stat stat{};
+    double gpu_ms = 0.0;
 
     V3 vtx(uint32_t t, int k) const {
         const float* p = D.vertices + 4 * (size_t)D.vindices[3 * (size_t)t + k];
@@ -530,10 +539,49 @@ public:
         for (uint32_t i = 0; i < D.num_meshes; ++i)
             if (D.meshes[i].instance < 0) src.push_back(i);
         std::vector<Work> trees(src.size());
+        std::vector<char> done(src.size(), 0);
+        if (use_gpu) {
+            // the triangle meshes on the device (bvh_gpu.cu), the light
+            // meshes' one-leaf trees below
+            std::vector<nbg::GpuMesh> gm;
+            std::vector<size_t> gj;
+            for (size_t j = 0; j < src.size(); ++j) {
+                const noor_mesh& m = D.meshes[src[j]];
+                if (m.light_idx >= 0) continue;
+                nbg::GpuMesh g;
+                g.start = m.tri_start;
+                g.count = m.tri_count;
+                const MeshInfo& mi = meshes[src[j]];
+                const float b[12] = {mi.box.lo.x,  mi.box.lo.y,  mi.box.lo.z,  mi.box.hi.x,  mi.box.hi.y,  mi.box.hi.z,
+                                     mi.cbox.lo.x, mi.cbox.lo.y, mi.cbox.lo.z, mi.cbox.hi.x, mi.cbox.hi.y, mi.cbox.hi.z};
+                std::memcpy(g.box, b, 24);
+                std::memcpy(g.cbox, b + 6, 24);
+                gm.push_back(g);
+                gj.push_back(j);
+            }
+            nbg::GpuBvhParams bp{D.bvh.num_bins, D.bvh.max_height, D.bvh.min_leaf_tris, D.bvh.max_leaf_tris,
+                                 D.bvh.Ci, D.bvh.Ct};
+            std::vector<nbg::GpuTree> gt;
+            std::string err;
+            static_assert(sizeof(Box) == 24, "Box is 6 floats");
+            const int rc = nbg::gpu_build_blas(reinterpret_cast<const float*>(tri_box.data()), D.num_triangles, gm, bp,
+                                               tri_order, gt, &gpu_ms, err);
+            if (rc) throw GpuBuildError{rc, err};
+            for (size_t k = 0; k < gj.size(); ++k) {
+                Work& w = trees[gj[k]];
+                w.nodes = std::move(gt[k].nodes);
+                w.stat.height = gt[k].height;
+                w.stat.num_inner_nodes = gt[k].num_inner;
+                w.stat.num_leaf_nodes = gt[k].num_leaf;
+                w.stat.max_leaf_tris = gt[k].max_leaf_tris;
+                done[gj[k]] = 1;
+            }
+        }
         std::atomic<size_t> next{0};
         std::vector<std::exception_ptr> errs(src.size());
         auto worker = [&]() {
             for (size_t j; (j = next.fetch_add(1)) < src.size();) {
+                if (done[j]) continue;
                 try {
                     const uint32_t i = src[j];
                     const noor_mesh& m = D.meshes[i];
@@ -654,7 +702,7 @@ static uint32_t add_texture(noor_payload_handle* h, const float* rgb, float a) {
     return (uint32_t)h->tex_data.size() - 1;
 }
 
-extern "C" int noor_build_payload(const noor_scene_desc* d, noor_payload_handle** out, noor_build_stat* stat) {
+static int build_payload(const noor_scene_desc* d, bool gpu, noor_payload_handle** out, noor_build_stat* stat) {
     using namespace nbh;
     if (!d || !out) return set_error(NOOR_ERR_INVALID, "noor_build_payload: null argument");
     *out = nullptr;
@@ -701,9 +749,11 @@ extern "C" int noor_build_payload(const noor_scene_desc* d, noor_payload_handle*
     std::unique_ptr<noor_payload_handle> h(new (std::nothrow) noor_payload_handle());
     if (!h) return set_error(NOOR_ERR_OOM, "noor_build_payload: out of host memory");
     try {
-        Builder B(*d);
+        Builder B(*d, gpu);
         B.compute_boxes();
+        const auto t1 = std::chrono::steady_clock::now();
         B.build_all();
+        const auto t2 = std::chrono::steady_clock::now();
 
         h->num_tris = d->num_triangles;
         h->root = B.root;
@@ -861,12 +911,24 @@ extern "C" int noor_build_payload(const noor_scene_desc* d, noor_payload_handle*
             stat->scene_max[2] = B.scene_box.hi.z;
             stat->scene_radius = h->scene_radius;
             stat->build_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+            stat->box_seconds = std::chrono::duration<double>(t1 - t0).count();
+            stat->tree_seconds = std::chrono::duration<double>(t2 - t1).count();
+            stat->tree_device_ms = B.gpu_ms;
         }
     } catch (const std::bad_alloc&) {
         return set_error(NOOR_ERR_OOM, "noor_build_payload: out of host memory");
+    } catch (const GpuBuildError& g) {
+        return set_error(g.code, g.msg);
     }
     *out = h.release();
     return NOOR_OK;
+}
+
+extern "C" int noor_build_payload(const noor_scene_desc* d, noor_payload_handle** out, noor_build_stat* stat) {
+    return build_payload(d, false, out, stat);
+}
+extern "C" int noor_build_payload_gpu(const noor_scene_desc* d, noor_payload_handle** out, noor_build_stat* stat) {
+    return build_payload(d, true, out, stat);
 }
 
 extern "C" int noor_payload_view(const noor_payload_handle* h, noor_payload* p) {

@@ -457,9 +457,11 @@ def _ptr(a: np.ndarray, t=C.c_float):
 
 
 class BuiltPayload:
-    """Owns a noor_payload_handle (host arrays the library built)."""
+    """Owns a noor_payload_handle (host arrays the library built); `gpu`
+    builds the bottom-level trees on the current CUDA device (the same
+    bytes)."""
 
-    def __init__(self, scene: SceneData):
+    def __init__(self, scene: SceneData, gpu: bool = False):
         L = capi.lib()
         s = scene
         self.scene = s
@@ -515,7 +517,8 @@ class BuiltPayload:
         self._keep = keep + [meshes, mats, lights, delta]
         h = C.c_void_p()
         self.stat = capi.BuildStat()
-        capi.call("noor_build_payload", C.byref(d), C.byref(h), C.byref(self.stat))
+        capi.call("noor_build_payload_gpu" if gpu else "noor_build_payload", C.byref(d), C.byref(h),
+                  C.byref(self.stat))
         self.handle = h
         self.payload = capi.Payload()
         capi.call("noor_payload_view", h, C.byref(self.payload))
