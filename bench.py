@@ -590,6 +590,15 @@ def main():
     from noor_b200 import scenes, _capi
     s, built, build_s = build_scene(args)
     r = scenes.Renderer(s, built=built)
+    # the same payload with the bottom-level trees built on the GPU (context
+    # up): its timings beside the host build's, and a byte check of the nodes
+    gb = scenes.BuiltPayload(s, gpu=True)
+    bvh_build = {"host_payload_s": round(built.stat.build_seconds, 3), "host_tree_s": round(built.stat.tree_seconds, 3),
+                 "gpu_payload_s": round(gb.stat.build_seconds, 3), "gpu_tree_s": round(gb.stat.tree_seconds, 3),
+                 "gpu_tree_device_ms": round(gb.stat.tree_device_ms, 1),
+                 "identical_nodes": bool(np.array_equal(gb.nodes(), built.nodes()) and
+                                         np.array_equal(gb.triangle_order(), built.triangle_order()))}
+    gb.free()
     paths_ = {"megakernel": MegakernelPath(args, s, r), "wavefront": WavefrontPath(args, s, r)}
     path = paths_[args.integrator]
     other = None if args.no_compare else paths_["megakernel" if args.integrator == "wavefront" else "wavefront"]
@@ -697,7 +706,8 @@ def main():
                            "triangles": s.num_triangles,
                            "intersector": "watertight", "film": "kahan",
                            "l2": "inputs larger than L2 (scene ~0.5 GB resident)",
-                           "parallelism": f"replicas{world}", "bvh_build_s": round(build_s, 2), **path.describe()},
+                           "parallelism": f"replicas{world}", "bvh_build_s": round(build_s, 2), "bvh_build": bvh_build,
+                           **path.describe()},
                 "mrays_per_s": mrays, "rays_per_step": (ext + shadow) / args.steps, "ext_rays_per_step": ext / args.steps,
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": launches, "clocks": clocks, "other_integrator": compare}
