@@ -431,7 +431,9 @@ def run_batched(args):
     r = scenes.Renderer(sc[keys[0]])
     ids, keep = {keys[0]: 0}, []
     for k in keys[1:]:
-        sid, kp = scenes.upload_scene(sc[k])
+        # the other scenes' payloads on the GPU (the same bytes as the host
+        # builder's, noor_build_payload_gpu) now that the context is up
+        sid, kp = scenes.upload_scene(sc[k], built=scenes.BuiltPayload(sc[k], gpu=True))
         ids[k] = sid
         keep.append(kp)
     setup_s = time.time() - t
@@ -476,7 +478,7 @@ def run_batched(args):
                                    "sky or env map) in one wavefront launch",
                        "frames": len(frames), "scenes": len(keys), "paths_per_step": npaths,
                        "triangles_uploaded": int(sum(x.num_triangles for x in sc.values())),
-                       "setup_s": round(setup_s, 1),
+                       "setup_s": round(setup_s, 1), "payload_builder": "host for the first scene, GPU for the rest",
                        "wavefront": {"block": best.block_size, "slots": best.queue_capacity,
                                      "material_sort": best.sort_granularity, "graph": best.use_graph}},
             "other_integrator": {"integrator": "megakernel, 64 sequential renders (noor_megakernel_batch)",

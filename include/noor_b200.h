@@ -513,16 +513,20 @@ typedef struct noor_build_stat {
     double box_seconds;          /* triangle and mesh boxes (host)           */
     double tree_seconds;         /* the trees: host, or GPU with transfers   */
     double tree_device_ms;       /* GPU build: device time of the trees      */
+    double tail_seconds;         /* vertex de-duplication, Wald records      */
+    double tail_device_ms;       /* GPU build: device time of those          */
 } noor_build_stat;
 
 typedef struct noor_payload_handle noor_payload_handle;
 /* Model::load + BVH build + Model::loadCudaPayload on the host. */
 int noor_build_payload(const noor_scene_desc* desc, noor_payload_handle** out,
                        noor_build_stat* stat);
-/* The same payload, bit for bit, with the per-mesh bottom-level trees built
- * on the current CUDA device (level by level: binning, split search and
- * partition in kernels; the top level over the meshes stays on the host).
- * Needs a GPU; errors as noor_build_payload, plus NOOR_ERR_CUDA. */
+/* The same payload, bit for bit, built on the current CUDA device: the
+ * per-mesh bottom-level trees level by level (binning, split search and
+ * partition in kernels; the top level over the meshes stays on the host),
+ * then the vertex de-duplication in BVH order, the Wald records and the
+ * attribute words.  Needs a GPU; errors as noor_build_payload, plus
+ * NOOR_ERR_CUDA. */
 int noor_build_payload_gpu(const noor_scene_desc* desc, noor_payload_handle** out,
                            noor_build_stat* stat);
 /* View of the owned arrays (valid until noor_free_payload). */

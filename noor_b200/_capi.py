@@ -166,7 +166,8 @@ class SceneDesc(C.Structure):
 class BuildStat(C.Structure):
     _fields_ = [("height", u32), ("num_inner_nodes", u32), ("num_leaf_nodes", u32), ("max_leaf_tris", u32),
                 ("scene_min", f32 * 3), ("scene_max", f32 * 3), ("scene_radius", f32), ("build_seconds", C.c_double),
-                ("box_seconds", C.c_double), ("tree_seconds", C.c_double), ("tree_device_ms", C.c_double)]
+                ("box_seconds", C.c_double), ("tree_seconds", C.c_double), ("tree_device_ms", C.c_double),
+                ("tail_seconds", C.c_double), ("tail_device_ms", C.c_double)]
 
 
 class WfFrame(C.Structure):

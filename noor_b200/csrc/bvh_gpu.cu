@@ -57,7 +57,8 @@ struct Ctl {
 struct Params {
     uint32_t nb, max_height, min_leaf, max_leaf;
     float Ci, Ct;
-    uint32_t cap;  // capacity of the task and record arrays
+    uint32_t cap;       // capacity of the record array
+    uint32_t task_cap;  // capacity of one level's task array
 };
 
 // ------------------------------------------------------------ box algebra
@@ -250,7 +251,7 @@ __device__ bool write_inner(const Out& o, const Params& P, const Task& t, uint32
                             const float* lbox, const float* lcbox, const float* rbox, const float* rcbox) {
     const uint32_t r0 = atomicAdd(&o.ctl->n_rec, 2u);
     const uint32_t q0 = atomicAdd(&o.ctl->n_next, 2u);
-    if (r0 + 2 > P.cap || q0 + 2 > P.cap) {
+    if (r0 + 2 > P.cap || q0 + 2 > P.task_cap) {
         atomicOr(&o.ctl->overflow, 1u);
         return false;
     }
@@ -748,6 +749,173 @@ __global__ void k_write(const Rec* recs, uint32_t n_rec, const uint32_t* mesh_of
     }
 }
 
+
+// ---------------------------------------------------- payload tail kernels
+constexpr uint32_t kEmptySlot = 0xffffffffu;
+struct TailArgs {
+    const uint32_t *order, *vi, *ni, *ui;
+    uint32_t n_corners;
+    uint32_t* slots;       // representative corner of each key
+    uint32_t* pmin;        // first corner of each key
+    uint32_t* corner_slot;
+    uint32_t mask;
+    uint32_t* fail;
+};
+__device__ __forceinline__ void corner_key(const TailArgs& A, uint32_t p, uint32_t& v, uint32_t& n, uint32_t& u) {
+    const size_t c = 3 * (size_t)A.order[p / 3] + p % 3;
+    v = A.vi[c];
+    n = A.ni[c];
+    u = A.ui[c];
+}
+__device__ __forceinline__ uint32_t key_hash(uint32_t v, uint32_t n, uint32_t u) {
+    uint32_t h = v * 0x9E3779B1u;
+    h ^= (n + 0x7F4A7C15u) * 0x85EBCA77u + (h << 6) + (h >> 2);
+    h ^= (u + 0x165667B1u) * 0xC2B2AE3Du + (h << 6) + (h >> 2);
+    return h ^ (h >> 16);
+}
+// each corner finds its key's slot (open addressing; a slot holds any corner
+// with that key), and the key's first corner by atomicMin
+__global__ void k_dedup_insert(TailArgs A) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= A.n_corners) return;
+    uint32_t v, n, u;
+    corner_key(A, p, v, n, u);
+    uint32_t slot = key_hash(v, n, u) & A.mask;
+    for (uint32_t probe = 0; probe <= A.mask; ++probe) {
+        uint32_t s = A.slots[slot];
+        if (s == kEmptySlot) {
+            s = atomicCAS(A.slots + slot, kEmptySlot, p);
+            if (s == kEmptySlot) s = p;
+        }
+        uint32_t sv, sn, su;
+        corner_key(A, s, sv, sn, su);
+        if (sv == v && sn == n && su == u) {
+            A.corner_slot[p] = slot;
+            atomicMin(A.pmin + slot, p);
+            return;
+        }
+        slot = (slot + 1) & A.mask;
+    }
+    atomicOr(A.fail, 1u);  // table full (cannot happen at half load)
+}
+__global__ void k_dedup_flags(TailArgs A, uint32_t* flag) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= A.n_corners) return;
+    flag[p] = A.pmin[A.corner_slot[p]] == p ? 1u : 0u;
+}
+// exclusive scan of n values in three passes: block sums, their scan (one
+// block), then each block's scan plus its offset
+constexpr uint32_t kScanBlock = 1024;
+__global__ void k_scan_sums(const uint32_t* in, uint32_t n, uint32_t* sums) {
+    __shared__ uint32_t acc;
+    if (threadIdx.x == 0) acc = 0;
+    __syncthreads();
+    const uint32_t i = blockIdx.x * kScanBlock + threadIdx.x;
+    if (i < n) atomicAdd(&acc, in[i]);
+    __syncthreads();
+    if (threadIdx.x == 0) sums[blockIdx.x] = acc;
+}
+__global__ void k_scan_top(uint32_t* sums, uint32_t nb, uint32_t* total) {
+    // one block of kScanBlock threads; each takes a contiguous run
+    __shared__ uint32_t part[kScanBlock + 1];
+    const uint32_t per = (nb + kScanBlock - 1) / kScanBlock;
+    const uint32_t b0 = min(nb, threadIdx.x * per), b1 = min(nb, b0 + per);
+    uint32_t s = 0;
+    for (uint32_t i = b0; i < b1; ++i) s += sums[i];
+    part[threadIdx.x] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t a = 0;
+        for (uint32_t i = 0; i < kScanBlock; ++i) {
+            const uint32_t v = part[i];
+            part[i] = a;
+            a += v;
+        }
+        *total = a;
+    }
+    __syncthreads();
+    uint32_t a = part[threadIdx.x];
+    for (uint32_t i = b0; i < b1; ++i) {
+        const uint32_t v = sums[i];
+        sums[i] = a;
+        a += v;
+    }
+}
+__global__ void k_scan_block(const uint32_t* in, uint32_t n, const uint32_t* offs, uint32_t* out) {
+    __shared__ uint32_t sh[kScanBlock];
+    const uint32_t i = blockIdx.x * kScanBlock + threadIdx.x;
+    sh[threadIdx.x] = i < n ? in[i] : 0u;
+    __syncthreads();
+    // Hillis-Steele inclusive scan in shared memory
+    for (uint32_t d = 1; d < kScanBlock; d <<= 1) {
+        const uint32_t v = threadIdx.x >= d ? sh[threadIdx.x - d] : 0u;
+        __syncthreads();
+        sh[threadIdx.x] += v;
+        __syncthreads();
+    }
+    if (i < n) out[i] = offs[blockIdx.x] + sh[threadIdx.x] - (i < n ? in[i] : 0u);
+}
+// the new vertex arrays (first occurrences, in corner order)
+__global__ void k_dedup_vertices(TailArgs A, const uint32_t* flag, const uint32_t* first_id, const float4* vtx,
+                                 const float4* nrm, const float2* uv, float4* ovtx, float4* onrm, float2* ouv) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= A.n_corners || !flag[p]) return;
+    uint32_t v, n, u;
+    corner_key(A, p, v, n, u);
+    const uint32_t k = first_id[p];
+    ovtx[k] = vtx[v];
+    onrm[k] = nrm[n];
+    ouv[k] = uv[u];
+}
+// Wald record (header/triangle.h:73-107) of the triangle's de-duplicated
+// vertices, as the host computes it (no contraction in this file)
+__global__ void k_wald(TailArgs A, const uint32_t* first_id, uint32_t n_tris, const float4* ovtx,
+                       const uint32_t* mat_idx, const uint32_t* mat_type, uint4* w0, uint4* w1, uint4* w2,
+                       uint4* attr) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_tris) return;
+    uint32_t e[3];
+    float3 P[3];
+    for (int j = 0; j < 3; ++j) {
+        e[j] = first_id[A.pmin[A.corner_slot[3 * i + j]]];
+        const float4 q = ovtx[e[j]];
+        P[j] = make_float3(q.x, q.y, q.z);
+    }
+    const float3 A0 = P[0];
+    const float b[3] = {P[2].x - A0.x, P[2].y - A0.y, P[2].z - A0.z};
+    const float c[3] = {P[1].x - A0.x, P[1].y - A0.y, P[1].z - A0.z};
+    float N[3] = {c[1] * b[2] - b[1] * c[2], c[2] * b[0] - b[2] * c[0], c[0] * b[1] - b[0] * c[1]};
+    const float inv = 1.0f / sqrtf((N[0] * N[0] + N[1] * N[1]) + N[2] * N[2]);
+    for (int k = 0; k < 3; ++k) N[k] = N[k] * inv;
+    uint32_t axis = 0;
+    for (uint32_t k = 0; k < 3; ++k) axis = fabsf(N[k]) > fabsf(N[axis]) ? k : axis;
+    const uint32_t mod[4] = {1u, 2u, 0u, 1u};
+    const uint32_t u = mod[axis], v = mod[axis + 1];
+    const float denom = b[u] * c[v] - b[v] * c[u];
+    const float Nk = N[axis];
+    const float Aa[3] = {A0.x, A0.y, A0.z};
+    uint4 r0 = make_uint4(axis, 0, 0, 0), r1 = make_uint4(0, 0, 0, 0), r2 = make_uint4(0, 0, 0, 0);
+    if (denom == 0.0f) {
+        r2.z = 1u;
+    } else {
+        r0.y = __float_as_uint(N[u] / Nk);
+        r0.z = __float_as_uint(N[v] / Nk);
+        r0.w = __float_as_uint(((N[0] * Aa[0] + N[1] * Aa[1]) + N[2] * Aa[2]) / Nk);
+        r1.x = __float_as_uint(b[u] / denom);
+        r1.y = __float_as_uint(-b[v] / denom);
+        r1.z = __float_as_uint(Aa[u]);
+        r1.w = __float_as_uint(Aa[v]);
+        r2.x = __float_as_uint(c[v] / denom);
+        r2.y = __float_as_uint(-c[u] / denom);
+    }
+    const uint32_t mi = mat_idx[A.order[i]];
+    r2.w = mat_type[mi];
+    w0[i] = r0;
+    w1[i] = r1;
+    w2[i] = r2;
+    attr[i] = make_uint4(e[0], e[1], e[2], mi);
+}
+
 // ------------------------------------------------------------ host side
 struct DevBuf {
     void* p = nullptr;
@@ -789,10 +957,11 @@ int gpu_build_blas(const float* tri_box, uint32_t n_tris, const std::vector<GpuM
     P.max_leaf = bp.max_leaf;
     P.Ci = bp.Ci;
     P.Ct = bp.Ct;
-    // a binary tree over n items has 2n - 1 nodes; empty children (a
-    // partition the bins did not foresee) are covered by the slack and
-    // otherwise reported as an overflow
-    P.cap = 4 * (n_tris + M) + 64;
+    // a binary tree over n items has 2n - 1 nodes, and a level has at most
+    // one task per triangle; empty children (a partition the bins did not
+    // foresee) are covered by the slack and otherwise reported as an overflow
+    P.cap = 2 * (n_tris + M) + 64;
+    P.task_cap = n_tris + 2 * M + 64;
     // a large task has more than kChunk triangles, so it spans fewer than
     // 2 * count / kChunk chunks
     const size_t max_chunks = 2 * ((size_t)n_tris / kChunk) + M + 8;
@@ -824,10 +993,10 @@ int gpu_build_blas(const float* tri_box, uint32_t n_tris, const std::vector<GpuM
     const size_t N = n_tris;
     if ((e = dalloc(b_box, 6 * N, &d_box)) || (e = dalloc(b_order, N, &d_order)) || (e = dalloc(b_tmp, N, &d_tmp)) ||
         (e = dalloc(b_rank, N, &d_rank)) || (e = dalloc(b_sF, N, &d_sF)) || (e = dalloc(b_sT, N, &d_sT)) ||
-        (e = dalloc(b_pred, N, &d_pred)) || (e = dalloc(b_tasks0, P.cap, &d_tasks[0])) ||
-        (e = dalloc(b_tasks1, P.cap, &d_tasks[1])) || (e = dalloc(b_recs, P.cap, &d_recs)) ||
-        (e = dalloc(b_levels, P.cap, &d_levels)) || (e = dalloc(b_tiny, P.cap, &d_tiny)) ||
-        (e = dalloc(b_small, P.cap, &d_small)) || (e = dalloc(b_large, max_large, &d_large)) ||
+        (e = dalloc(b_pred, N, &d_pred)) || (e = dalloc(b_tasks0, P.task_cap, &d_tasks[0])) ||
+        (e = dalloc(b_tasks1, P.task_cap, &d_tasks[1])) || (e = dalloc(b_recs, P.cap, &d_recs)) ||
+        (e = dalloc(b_levels, P.cap, &d_levels)) || (e = dalloc(b_tiny, P.task_cap, &d_tiny)) ||
+        (e = dalloc(b_small, P.task_cap, &d_small)) || (e = dalloc(b_large, max_large, &d_large)) ||
         (e = dalloc(b_ctl, 1, &d_ctl)) || (e = dalloc(b_stats, 4 * (size_t)M, &d_stats)) ||
         (e = dalloc(b_splits, max_large, &d_splits)) || (e = dalloc(b_chunks, max_chunks, &d_chunks)) ||
         (e = dalloc(b_c0, max_large + 1, &d_c0)) || (e = dalloc(b_ctrue, max_chunks, &d_ctrue)) ||
@@ -882,7 +1051,7 @@ int gpu_build_blas(const float* tri_box, uint32_t n_tris, const std::vector<GpuM
     std::vector<Chunk> chunks;
     std::vector<uint32_t> c0;
     for (uint32_t level = 0; n_cur > 0; ++level) {
-        if (level > bp.max_height + 1 || level_off.back() + (size_t)n_cur > P.cap) {
+        if (level > bp.max_height + 1 || level_off.back() + (size_t)n_cur > P.cap || n_cur > P.task_cap) {
             err = "GPU BVH build: tree deeper or larger than expected";
             return NOOR_ERR_CAPACITY;
         }
@@ -907,18 +1076,19 @@ int gpu_build_blas(const float* tri_box, uint32_t n_tris, const std::vector<GpuM
                 err = "GPU BVH build: too many large tasks";
                 return NOOR_ERR_CAPACITY;
             }
-            // chunk table on the host (large tasks are few)
+            // chunk table on the host (large tasks are few; a level that has
+            // them has few tasks in all)
             std::vector<uint32_t> lidx(h.n_large);
-            ltasks.resize(h.n_large);
+            ltasks.resize(n_cur);
             if ((e = cudaMemcpyAsync(lidx.data(), d_large, 4 * (size_t)h.n_large, cudaMemcpyDeviceToHost, s)) ||
+                (e = cudaMemcpyAsync(ltasks.data(), d_tasks[cur], sizeof(Task) * (size_t)n_cur, cudaMemcpyDeviceToHost,
+                                     s)) ||
                 (e = cudaStreamSynchronize(s)))
                 return fail("large list", e);
             chunks.clear();
             c0.assign(h.n_large + 1, 0);
             for (uint32_t j = 0; j < h.n_large; ++j) {
-                Task t;
-                if ((e = cudaMemcpy(&t, d_tasks[cur] + lidx[j], sizeof(Task), cudaMemcpyDeviceToHost)))
-                    return fail("large task", e);
+                const Task& t = ltasks[lidx[j]];
                 c0[j] = (uint32_t)chunks.size();
                 for (uint32_t b = 0; b < t.count; b += kChunk) chunks.push_back(Chunk{j, b, std::min(t.count, b + kChunk)});
             }
@@ -1010,6 +1180,102 @@ int gpu_build_blas(const float* tri_box, uint32_t n_tris, const std::vector<GpuM
         t.num_leaf = stats[4 * i + 2];
         t.max_leaf_tris = stats[4 * i + 3];
     }
+    return NOOR_OK;
+}
+
+int gpu_payload_tail(const GpuTailIn& in, GpuTailOut& out, double* device_ms, std::string& err) {
+    auto fail = [&](const char* what, cudaError_t e) {
+        err = std::string("GPU payload: ") + what + ": " + cudaGetErrorString(e);
+        return NOOR_ERR_CUDA;
+    };
+    const size_t T = in.n_tris, C = 3 * T;
+    if (C >= 0x7fffffffu) {
+        err = "GPU payload: too many triangles";
+        return NOOR_ERR_INVALID;
+    }
+    size_t cap = 16;
+    while (cap < 2 * C) cap <<= 1;
+    const uint32_t nblk = (uint32_t)((C + kScanBlock - 1) / kScanBlock);
+    cudaStream_t s;
+    cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return fail("stream", e);
+    struct StreamGuard {
+        cudaStream_t s;
+        ~StreamGuard() { cudaStreamDestroy(s); }
+    } sg{s};
+    cudaEvent_t ev0, ev1;
+    cudaEventCreate(&ev0);
+    cudaEventCreate(&ev1);
+    DevBuf b_order, b_vi, b_ni, b_ui, b_vtx, b_nrm, b_uv, b_mi, b_mt, b_slots, b_pmin, b_cs, b_flag, b_first, b_sums,
+        b_total, b_fail, b_ovtx, b_onrm, b_ouv, b_w0, b_w1, b_w2, b_attr;
+    uint32_t *d_order, *d_vi, *d_ni, *d_ui, *d_mi, *d_mt, *d_slots, *d_pmin, *d_cs, *d_flag, *d_first, *d_sums,
+        *d_total, *d_fail;
+    float4 *d_vtx, *d_nrm, *d_ovtx, *d_onrm;
+    float2 *d_uv, *d_ouv;
+    uint4 *d_w0, *d_w1, *d_w2, *d_attr;
+    if ((e = dalloc(b_order, T, &d_order)) || (e = dalloc(b_vi, C, &d_vi)) || (e = dalloc(b_ni, C, &d_ni)) ||
+        (e = dalloc(b_ui, C, &d_ui)) || (e = dalloc(b_vtx, in.n_vertices, &d_vtx)) ||
+        (e = dalloc(b_nrm, in.n_normals, &d_nrm)) || (e = dalloc(b_uv, in.n_uvs, &d_uv)) ||
+        (e = dalloc(b_mi, T, &d_mi)) || (e = dalloc(b_mt, in.n_materials, &d_mt)) ||
+        (e = dalloc(b_slots, cap, &d_slots)) || (e = dalloc(b_pmin, cap, &d_pmin)) || (e = dalloc(b_cs, C, &d_cs)) ||
+        (e = dalloc(b_flag, C, &d_flag)) || (e = dalloc(b_first, C, &d_first)) ||
+        (e = dalloc(b_sums, nblk, &d_sums)) || (e = dalloc(b_total, 1, &d_total)) ||
+        (e = dalloc(b_fail, 1, &d_fail)) || (e = dalloc(b_w0, T, &d_w0)) || (e = dalloc(b_w1, T, &d_w1)) ||
+        (e = dalloc(b_w2, T, &d_w2)) || (e = dalloc(b_attr, T, &d_attr)))
+        return fail("allocation", e);
+    cudaEventRecord(ev0, s);
+    if ((e = cudaMemcpyAsync(d_order, in.tri_order, 4 * T, cudaMemcpyHostToDevice, s)) ||
+        (e = cudaMemcpyAsync(d_vi, in.vindices, 4 * C, cudaMemcpyHostToDevice, s)) ||
+        (e = cudaMemcpyAsync(d_ni, in.nindices, 4 * C, cudaMemcpyHostToDevice, s)) ||
+        (e = cudaMemcpyAsync(d_ui, in.uvindices, 4 * C, cudaMemcpyHostToDevice, s)) ||
+        (e = cudaMemcpyAsync(d_vtx, in.vertices, 16 * (size_t)in.n_vertices, cudaMemcpyHostToDevice, s)) ||
+        (e = cudaMemcpyAsync(d_nrm, in.normals, 16 * (size_t)in.n_normals, cudaMemcpyHostToDevice, s)) ||
+        (e = cudaMemcpyAsync(d_uv, in.uvs, 8 * (size_t)in.n_uvs, cudaMemcpyHostToDevice, s)) ||
+        (e = cudaMemcpyAsync(d_mi, in.material_indices, 4 * T, cudaMemcpyHostToDevice, s)) ||
+        (e = cudaMemcpyAsync(d_mt, in.material_types, 4 * (size_t)in.n_materials, cudaMemcpyHostToDevice, s)) ||
+        (e = cudaMemsetAsync(d_slots, 0xff, 4 * cap, s)) || (e = cudaMemsetAsync(d_pmin, 0xff, 4 * cap, s)) ||
+        (e = cudaMemsetAsync(d_fail, 0, 4, s)))
+        return fail("upload", e);
+    TailArgs A{d_order, d_vi, d_ni, d_ui, (uint32_t)C, d_slots, d_pmin, d_cs, (uint32_t)(cap - 1), d_fail};
+    const uint32_t g = (uint32_t)((C + 255) / 256);
+    k_dedup_insert<<<g, 256, 0, s>>>(A);
+    k_dedup_flags<<<g, 256, 0, s>>>(A, d_flag);
+    k_scan_sums<<<nblk, kScanBlock, 0, s>>>(d_flag, (uint32_t)C, d_sums);
+    k_scan_top<<<1, kScanBlock, 0, s>>>(d_sums, nblk, d_total);
+    k_scan_block<<<nblk, kScanBlock, 0, s>>>(d_flag, (uint32_t)C, d_sums, d_first);
+    uint32_t nv = 0, failed = 0;
+    if ((e = cudaGetLastError()) || (e = cudaMemcpyAsync(&nv, d_total, 4, cudaMemcpyDeviceToHost, s)) ||
+        (e = cudaMemcpyAsync(&failed, d_fail, 4, cudaMemcpyDeviceToHost, s)) || (e = cudaStreamSynchronize(s)))
+        return fail("de-duplication", e);
+    if (failed) {
+        err = "GPU payload: vertex table full";
+        return NOOR_ERR_CAPACITY;
+    }
+    if ((e = dalloc(b_ovtx, nv, &d_ovtx)) || (e = dalloc(b_onrm, nv, &d_onrm)) || (e = dalloc(b_ouv, nv, &d_ouv)))
+        return fail("allocation", e);
+    k_dedup_vertices<<<g, 256, 0, s>>>(A, d_flag, d_first, d_vtx, d_nrm, d_uv, d_ovtx, d_onrm, d_ouv);
+    k_wald<<<(uint32_t)((T + 255) / 256), 256, 0, s>>>(A, d_first, (uint32_t)T, d_ovtx, d_mi, d_mt, d_w0, d_w1, d_w2,
+                                                       d_attr);
+    cudaEventRecord(ev1, s);
+    out.vertices.resize(4 * (size_t)nv);
+    out.normals.resize(4 * (size_t)nv);
+    out.uvs.resize(2 * (size_t)nv);
+    for (auto* w : {&out.wald[0], &out.wald[1], &out.wald[2], &out.attr}) w->resize(4 * T);
+    if ((e = cudaGetLastError()) ||
+        (e = cudaMemcpyAsync(out.vertices.data(), d_ovtx, 16 * (size_t)nv, cudaMemcpyDeviceToHost, s)) ||
+        (e = cudaMemcpyAsync(out.normals.data(), d_onrm, 16 * (size_t)nv, cudaMemcpyDeviceToHost, s)) ||
+        (e = cudaMemcpyAsync(out.uvs.data(), d_ouv, 8 * (size_t)nv, cudaMemcpyDeviceToHost, s)) ||
+        (e = cudaMemcpyAsync(out.wald[0].data(), d_w0, 16 * T, cudaMemcpyDeviceToHost, s)) ||
+        (e = cudaMemcpyAsync(out.wald[1].data(), d_w1, 16 * T, cudaMemcpyDeviceToHost, s)) ||
+        (e = cudaMemcpyAsync(out.wald[2].data(), d_w2, 16 * T, cudaMemcpyDeviceToHost, s)) ||
+        (e = cudaMemcpyAsync(out.attr.data(), d_attr, 16 * T, cudaMemcpyDeviceToHost, s)) ||
+        (e = cudaStreamSynchronize(s)))
+        return fail("download", e);
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, ev0, ev1);
+    cudaEventDestroy(ev0);
+    cudaEventDestroy(ev1);
+    if (device_ms) *device_ms = ms;
     return NOOR_OK;
 }
 

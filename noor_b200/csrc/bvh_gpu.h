@@ -32,4 +32,28 @@ int gpu_build_blas(const float* tri_box, uint32_t n_tris, const std::vector<GpuM
                    const GpuBvhParams& p, std::vector<uint32_t>& tri_order, std::vector<GpuTree>& trees,
                    double* device_ms, std::string& err);
 
+// The rest of Model::loadCudaPayload on the device (model.cpp:333-458):
+// vertex de-duplication in BVH order (the first occurrence of a (vertex,
+// normal, uv) index triple gets the next index) and the Wald records and
+// attribute words of each triangle in BVH order.
+struct GpuTailIn {
+    const uint32_t* tri_order;
+    uint32_t n_tris;
+    const uint32_t *vindices, *nindices, *uvindices;  // 3 per source triangle
+    const float* vertices;                            // float4
+    uint32_t n_vertices;
+    const float* normals;  // float4
+    uint32_t n_normals;
+    const float* uvs;  // float2
+    uint32_t n_uvs;
+    const uint32_t* material_indices;  // per source triangle
+    const uint32_t* material_types;    // per material
+    uint32_t n_materials;
+};
+struct GpuTailOut {
+    std::vector<float> vertices, normals, uvs;
+    std::vector<uint32_t> wald[3], attr;
+};
+int gpu_payload_tail(const GpuTailIn& in, GpuTailOut& out, double* device_ms, std::string& err);
+
 }  // namespace nbg

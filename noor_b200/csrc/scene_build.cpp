@@ -853,54 +853,75 @@ static int build_payload(const noor_scene_desc* d, bool gpu, noor_payload_handle
             }
         }
 
-        // vertex de-duplication in BVH order (Model::loadCudaPayload, model.cpp:376-401):
-        // the first occurrence of a (vertex, normal, uv) index triple appends a
-        // vertex; later occurrences reuse its index
-        // (an open-addressing table: the same first-occurrence numbering as a
-        // map, without a node allocation per key)
-        AttrTable seen(3 * (size_t)d->num_triangles);
-        std::vector<uint32_t> element(3 * (size_t)d->num_triangles);
-        uint32_t nv = 0;
-        for (uint32_t i = 0; i < d->num_triangles; ++i) {
-            const uint32_t t = B.tri_order[i];
-            for (int j = 0; j < 3; ++j) {
-                const AttrKey key{d->vindices[3 * (size_t)t + j], d->nindices[3 * (size_t)t + j],
-                                  d->uvindices[3 * (size_t)t + j]};
-                bool added;
-                const uint32_t id = seen.find_or_add(key, nv, added);
-                if (added) {
-                    h->vertices.insert(h->vertices.end(), d->vertices + 4 * (size_t)key.v,
-                                       d->vertices + 4 * (size_t)key.v + 4);
-                    h->normals.insert(h->normals.end(), d->normals + 4 * (size_t)key.n,
-                                      d->normals + 4 * (size_t)key.n + 4);
-                    h->uvs.insert(h->uvs.end(), d->uvs + 2 * (size_t)key.u, d->uvs + 2 * (size_t)key.u + 2);
-                    ++nv;
+        double tail_ms = 0.0;
+        const auto t3 = std::chrono::steady_clock::now();
+        if (gpu) {
+            // the same steps on the device (bvh_gpu.cu)
+            std::vector<uint32_t> mtypes(d->num_materials);
+            for (uint32_t i = 0; i < d->num_materials; ++i) mtypes[i] = h->materials[i].type;
+            nbg::GpuTailIn ti{B.tri_order.data(), d->num_triangles, d->vindices, d->nindices, d->uvindices,
+                              d->vertices, d->num_vertices, d->normals, d->num_normals, d->uvs, d->num_uvs,
+                              d->material_indices, mtypes.data(), d->num_materials};
+            nbg::GpuTailOut to;
+            std::string err;
+            const int rc = nbg::gpu_payload_tail(ti, to, &tail_ms, err);
+            if (rc) return set_error(rc, err);
+            h->vertices = std::move(to.vertices);
+            h->normals = std::move(to.normals);
+            h->uvs = std::move(to.uvs);
+            for (int k = 0; k < 3; ++k) h->wald[k] = std::move(to.wald[k]);
+            h->attr = std::move(to.attr);
+        } else {
+            // vertex de-duplication in BVH order (Model::loadCudaPayload, model.cpp:376-401):
+            // the first occurrence of a (vertex, normal, uv) index triple appends a
+            // vertex; later occurrences reuse its index
+            // (an open-addressing table: the same first-occurrence numbering as a
+            // map, without a node allocation per key)
+            AttrTable seen(3 * (size_t)d->num_triangles);
+            std::vector<uint32_t> element(3 * (size_t)d->num_triangles);
+            uint32_t nv = 0;
+            for (uint32_t i = 0; i < d->num_triangles; ++i) {
+                const uint32_t t = B.tri_order[i];
+                for (int j = 0; j < 3; ++j) {
+                    const AttrKey key{d->vindices[3 * (size_t)t + j], d->nindices[3 * (size_t)t + j],
+                                      d->uvindices[3 * (size_t)t + j]};
+                    bool added;
+                    const uint32_t id = seen.find_or_add(key, nv, added);
+                    if (added) {
+                        h->vertices.insert(h->vertices.end(), d->vertices + 4 * (size_t)key.v,
+                                           d->vertices + 4 * (size_t)key.v + 4);
+                        h->normals.insert(h->normals.end(), d->normals + 4 * (size_t)key.n,
+                                          d->normals + 4 * (size_t)key.n + 4);
+                        h->uvs.insert(h->uvs.end(), d->uvs + 2 * (size_t)key.u, d->uvs + 2 * (size_t)key.u + 2);
+                        ++nv;
+                    }
+                    element[3 * (size_t)i + j] = id;
                 }
-                element[3 * (size_t)i + j] = id;
             }
+            // Wald triangles + attribute indices (Model::buildWaldTriangles, model.cpp:333-360)
+            for (int k = 0; k < 3; ++k) h->wald[k].resize(4 * (size_t)d->num_triangles);
+            h->attr.resize(4 * (size_t)d->num_triangles);
+            // independent per triangle: split over the host threads
+            parallel_for(d->num_triangles, [&](uint32_t i) {
+                V3 p[3];
+                for (int j = 0; j < 3; ++j) {
+                    const float* q = h->vertices.data() + 4 * (size_t)element[3 * (size_t)i + j];
+                    p[j] = v3(q[0], q[1], q[2]);
+                }
+                uint32_t* r0 = h->wald[0].data() + 4 * (size_t)i;
+                uint32_t* r1 = h->wald[1].data() + 4 * (size_t)i;
+                uint32_t* r2 = h->wald[2].data() + 4 * (size_t)i;
+                wald_record(p[0], p[1], p[2], r0, r1, r2);
+                const uint32_t mi = d->material_indices[B.tri_order[i]];
+                r2[3] = h->materials[mi].type;
+                uint32_t* a = h->attr.data() + 4 * (size_t)i;
+                a[0] = element[3 * (size_t)i + 0];
+                a[1] = element[3 * (size_t)i + 1];
+                a[2] = element[3 * (size_t)i + 2];
+                a[3] = mi;
+            });
         }
-        // Wald triangles + attribute indices (Model::buildWaldTriangles, model.cpp:333-360)
-        for (int k = 0; k < 3; ++k) h->wald[k].resize(4 * (size_t)d->num_triangles);
-        h->attr.resize(4 * (size_t)d->num_triangles);
-        // independent per triangle: split over the host threads
-        parallel_for(d->num_triangles, [&](uint32_t i) {
-            V3 p[3];
-            for (int j = 0; j < 3; ++j) {
-                const float* q = h->vertices.data() + 4 * (size_t)element[3 * (size_t)i + j];
-                p[j] = v3(q[0], q[1], q[2]);
-            }
-            uint32_t* r0 = h->wald[0].data() + 4 * (size_t)i;
-            uint32_t* r1 = h->wald[1].data() + 4 * (size_t)i;
-            uint32_t* r2 = h->wald[2].data() + 4 * (size_t)i;
-            wald_record(p[0], p[1], p[2], r0, r1, r2);
-            const uint32_t mi = d->material_indices[B.tri_order[i]];
-            r2[3] = h->materials[mi].type;
-            uint32_t* a = h->attr.data() + 4 * (size_t)i;
-            a[0] = element[3 * (size_t)i + 0];
-            a[1] = element[3 * (size_t)i + 1];
-            a[2] = element[3 * (size_t)i + 2];
-            a[3] = mi;
-        });
+        const auto t4 = std::chrono::steady_clock::now();
         if (stat) {
             *stat = B.stat;
             stat->scene_min[0] = B.scene_box.lo.x;
@@ -914,6 +935,8 @@ static int build_payload(const noor_scene_desc* d, bool gpu, noor_payload_handle
             stat->box_seconds = std::chrono::duration<double>(t1 - t0).count();
             stat->tree_seconds = std::chrono::duration<double>(t2 - t1).count();
             stat->tree_device_ms = B.gpu_ms;
+            stat->tail_seconds = std::chrono::duration<double>(t4 - t3).count();
+            stat->tail_device_ms = tail_ms;
         }
     } catch (const std::bad_alloc&) {
         return set_error(NOOR_ERR_OOM, "noor_build_payload: out of host memory");

@@ -1,8 +1,9 @@
-"""GPU bottom-level BVH build (noor_build_payload_gpu) against the host
-builder (noor_build_payload, itself byte-identical to the reference builder
-by the golden fixtures): every payload array the same bytes, on scenes with
-light nodes, instances, many meshes, forced height limits and every bin
-count, and on the 2.6M-triangle sky scene."""
+"""GPU payload build (noor_build_payload_gpu: bottom-level BVH trees,
+vertex de-duplication, Wald records) against the host builder
+(noor_build_payload, itself byte-identical to the reference builder by the
+golden fixtures): every payload array the same bytes, on scenes with light
+nodes, instances, many meshes, forced height limits and every bin count,
+and on the 2.6M-triangle sky scene."""
 import numpy as np
 import pytest
 
@@ -76,5 +77,6 @@ def test_sky_scene_full_size():
     for name, b in (("host", host), ("gpu", gpu)):
         st = b.stat
         print(f"{name}: {s.num_triangles} triangles, payload {st.build_seconds:.3f} s = boxes {st.box_seconds:.3f} s"
-              f" + trees {st.tree_seconds:.3f} s (device {st.tree_device_ms:.1f} ms) + rest")
-    assert gpu.stat.tree_device_ms > 0
+              f" + trees {st.tree_seconds:.3f} s (device {st.tree_device_ms:.1f} ms) + vertices and Wald records "
+              f"{st.tail_seconds:.3f} s (device {st.tail_device_ms:.1f} ms) + the rest")
+    assert gpu.stat.tree_device_ms > 0 and gpu.stat.tail_device_ms > 0
