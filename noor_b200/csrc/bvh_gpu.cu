@@ -917,17 +917,31 @@ __global__ void k_wald(TailArgs A, const uint32_t* first_id, uint32_t n_tris, co
 }
 
 // ------------------------------------------------------------ host side
+// stream-ordered scratch from the device's default pool, which keeps up to
+// 4 GiB between calls, so that repeated builds do not pay for allocation
 struct DevBuf {
     void* p = nullptr;
+    cudaStream_t s = nullptr;
     ~DevBuf() {
-        if (p) cudaFree(p);
+        if (p) cudaFreeAsync(p, s);
     }
 };
 template <class T>
-static cudaError_t dalloc(DevBuf& b, size_t n, T** out) {
-    cudaError_t e = cudaMalloc(&b.p, std::max<size_t>(n, 1) * sizeof(T));
+static cudaError_t dalloc(cudaStream_t s, DevBuf& b, size_t n, T** out) {
+    b.s = s;
+    cudaError_t e = cudaMallocAsync(&b.p, std::max<size_t>(n, 1) * sizeof(T), s);
     *out = static_cast<T*>(b.p);
     return e;
+}
+static void keep_pool() {
+    int dev = 0;
+    cudaMemPool_t pool;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess) return;
+    uint64_t keep = 0;
+    if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep) == cudaSuccess && keep < (4ull << 30)) {
+        keep = 4ull << 30;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
 }
 
 }  // namespace
@@ -974,6 +988,7 @@ int gpu_build_blas(const float* tri_box, uint32_t n_tris, const std::vector<GpuM
         cudaStream_t s;
         ~StreamGuard() { cudaStreamDestroy(s); }
     } sg{s};
+    keep_pool();
     cudaEvent_t ev0, ev1;
     cudaEventCreate(&ev0);
     cudaEventCreate(&ev1);
@@ -991,18 +1006,18 @@ int gpu_build_blas(const float* tri_box, uint32_t n_tris, const std::vector<GpuM
     Chunk* d_chunks;
     unsigned long long* d_gkeys;
     const size_t N = n_tris;
-    if ((e = dalloc(b_box, 6 * N, &d_box)) || (e = dalloc(b_order, N, &d_order)) || (e = dalloc(b_tmp, N, &d_tmp)) ||
-        (e = dalloc(b_rank, N, &d_rank)) || (e = dalloc(b_sF, N, &d_sF)) || (e = dalloc(b_sT, N, &d_sT)) ||
-        (e = dalloc(b_pred, N, &d_pred)) || (e = dalloc(b_tasks0, P.task_cap, &d_tasks[0])) ||
-        (e = dalloc(b_tasks1, P.task_cap, &d_tasks[1])) || (e = dalloc(b_recs, P.cap, &d_recs)) ||
-        (e = dalloc(b_levels, P.cap, &d_levels)) || (e = dalloc(b_tiny, P.task_cap, &d_tiny)) ||
-        (e = dalloc(b_small, P.task_cap, &d_small)) || (e = dalloc(b_large, max_large, &d_large)) ||
-        (e = dalloc(b_ctl, 1, &d_ctl)) || (e = dalloc(b_stats, 4 * (size_t)M, &d_stats)) ||
-        (e = dalloc(b_splits, max_large, &d_splits)) || (e = dalloc(b_chunks, max_chunks, &d_chunks)) ||
-        (e = dalloc(b_c0, max_large + 1, &d_c0)) || (e = dalloc(b_ctrue, max_chunks, &d_ctrue)) ||
-        (e = dalloc(b_cbefore, max_chunks, &d_cbefore)) ||
-        (e = dalloc(b_gkeys, max_large * 3 * P.nb * kKeys, &d_gkeys)) ||
-        (e = dalloc(b_gcnt, max_large * 3 * P.nb, &d_gcnt)) || (e = dalloc(b_meshoff, M, &d_meshoff)))
+    if ((e = dalloc(s, b_box, 6 * N, &d_box)) || (e = dalloc(s, b_order, N, &d_order)) || (e = dalloc(s, b_tmp, N, &d_tmp)) ||
+        (e = dalloc(s, b_rank, N, &d_rank)) || (e = dalloc(s, b_sF, N, &d_sF)) || (e = dalloc(s, b_sT, N, &d_sT)) ||
+        (e = dalloc(s, b_pred, N, &d_pred)) || (e = dalloc(s, b_tasks0, P.task_cap, &d_tasks[0])) ||
+        (e = dalloc(s, b_tasks1, P.task_cap, &d_tasks[1])) || (e = dalloc(s, b_recs, P.cap, &d_recs)) ||
+        (e = dalloc(s, b_levels, P.cap, &d_levels)) || (e = dalloc(s, b_tiny, P.task_cap, &d_tiny)) ||
+        (e = dalloc(s, b_small, P.task_cap, &d_small)) || (e = dalloc(s, b_large, max_large, &d_large)) ||
+        (e = dalloc(s, b_ctl, 1, &d_ctl)) || (e = dalloc(s, b_stats, 4 * (size_t)M, &d_stats)) ||
+        (e = dalloc(s, b_splits, max_large, &d_splits)) || (e = dalloc(s, b_chunks, max_chunks, &d_chunks)) ||
+        (e = dalloc(s, b_c0, max_large + 1, &d_c0)) || (e = dalloc(s, b_ctrue, max_chunks, &d_ctrue)) ||
+        (e = dalloc(s, b_cbefore, max_chunks, &d_cbefore)) ||
+        (e = dalloc(s, b_gkeys, max_large * 3 * P.nb * kKeys, &d_gkeys)) ||
+        (e = dalloc(s, b_gcnt, max_large * 3 * P.nb, &d_gcnt)) || (e = dalloc(s, b_meshoff, M, &d_meshoff)))
         return fail("allocation", e);
 
     // kernel shared memory
@@ -1155,7 +1170,7 @@ int gpu_build_blas(const float* tri_box, uint32_t n_tris, const std::vector<GpuM
         err = "GPU BVH build: record count mismatch";
         return NOOR_ERR_CUDA;
     }
-    if ((e = dalloc(b_out, 8 * total, &d_out)) ||
+    if ((e = dalloc(s, b_out, 8 * total, &d_out)) ||
         (e = cudaMemcpyAsync(d_meshoff, mesh_off.data(), 4 * (size_t)M, cudaMemcpyHostToDevice, s)))
         return fail("output", e);
     k_write<<<(n_rec + 255) / 256, 256, 0, s>>>(d_recs, n_rec, d_meshoff, d_out);
@@ -1203,6 +1218,7 @@ int gpu_payload_tail(const GpuTailIn& in, GpuTailOut& out, double* device_ms, st
         cudaStream_t s;
         ~StreamGuard() { cudaStreamDestroy(s); }
     } sg{s};
+    keep_pool();
     cudaEvent_t ev0, ev1;
     cudaEventCreate(&ev0);
     cudaEventCreate(&ev1);
@@ -1213,15 +1229,15 @@ int gpu_payload_tail(const GpuTailIn& in, GpuTailOut& out, double* device_ms, st
     float4 *d_vtx, *d_nrm, *d_ovtx, *d_onrm;
     float2 *d_uv, *d_ouv;
     uint4 *d_w0, *d_w1, *d_w2, *d_attr;
-    if ((e = dalloc(b_order, T, &d_order)) || (e = dalloc(b_vi, C, &d_vi)) || (e = dalloc(b_ni, C, &d_ni)) ||
-        (e = dalloc(b_ui, C, &d_ui)) || (e = dalloc(b_vtx, in.n_vertices, &d_vtx)) ||
-        (e = dalloc(b_nrm, in.n_normals, &d_nrm)) || (e = dalloc(b_uv, in.n_uvs, &d_uv)) ||
-        (e = dalloc(b_mi, T, &d_mi)) || (e = dalloc(b_mt, in.n_materials, &d_mt)) ||
-        (e = dalloc(b_slots, cap, &d_slots)) || (e = dalloc(b_pmin, cap, &d_pmin)) || (e = dalloc(b_cs, C, &d_cs)) ||
-        (e = dalloc(b_flag, C, &d_flag)) || (e = dalloc(b_first, C, &d_first)) ||
-        (e = dalloc(b_sums, nblk, &d_sums)) || (e = dalloc(b_total, 1, &d_total)) ||
-        (e = dalloc(b_fail, 1, &d_fail)) || (e = dalloc(b_w0, T, &d_w0)) || (e = dalloc(b_w1, T, &d_w1)) ||
-        (e = dalloc(b_w2, T, &d_w2)) || (e = dalloc(b_attr, T, &d_attr)))
+    if ((e = dalloc(s, b_order, T, &d_order)) || (e = dalloc(s, b_vi, C, &d_vi)) || (e = dalloc(s, b_ni, C, &d_ni)) ||
+        (e = dalloc(s, b_ui, C, &d_ui)) || (e = dalloc(s, b_vtx, in.n_vertices, &d_vtx)) ||
+        (e = dalloc(s, b_nrm, in.n_normals, &d_nrm)) || (e = dalloc(s, b_uv, in.n_uvs, &d_uv)) ||
+        (e = dalloc(s, b_mi, T, &d_mi)) || (e = dalloc(s, b_mt, in.n_materials, &d_mt)) ||
+        (e = dalloc(s, b_slots, cap, &d_slots)) || (e = dalloc(s, b_pmin, cap, &d_pmin)) || (e = dalloc(s, b_cs, C, &d_cs)) ||
+        (e = dalloc(s, b_flag, C, &d_flag)) || (e = dalloc(s, b_first, C, &d_first)) ||
+        (e = dalloc(s, b_sums, nblk, &d_sums)) || (e = dalloc(s, b_total, 1, &d_total)) ||
+        (e = dalloc(s, b_fail, 1, &d_fail)) || (e = dalloc(s, b_w0, T, &d_w0)) || (e = dalloc(s, b_w1, T, &d_w1)) ||
+        (e = dalloc(s, b_w2, T, &d_w2)) || (e = dalloc(s, b_attr, T, &d_attr)))
         return fail("allocation", e);
     cudaEventRecord(ev0, s);
     if ((e = cudaMemcpyAsync(d_order, in.tri_order, 4 * T, cudaMemcpyHostToDevice, s)) ||
@@ -1251,7 +1267,7 @@ int gpu_payload_tail(const GpuTailIn& in, GpuTailOut& out, double* device_ms, st
         err = "GPU payload: vertex table full";
         return NOOR_ERR_CAPACITY;
     }
-    if ((e = dalloc(b_ovtx, nv, &d_ovtx)) || (e = dalloc(b_onrm, nv, &d_onrm)) || (e = dalloc(b_ouv, nv, &d_ouv)))
+    if ((e = dalloc(s, b_ovtx, nv, &d_ovtx)) || (e = dalloc(s, b_onrm, nv, &d_onrm)) || (e = dalloc(s, b_ouv, nv, &d_ouv)))
         return fail("allocation", e);
     k_dedup_vertices<<<g, 256, 0, s>>>(A, d_flag, d_first, d_vtx, d_nrm, d_uv, d_ovtx, d_onrm, d_ouv);
     k_wald<<<(uint32_t)((T + 255) / 256), 256, 0, s>>>(A, d_first, (uint32_t)T, d_ovtx, d_mi, d_mt, d_w0, d_w1, d_w2,

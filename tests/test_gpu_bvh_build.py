@@ -72,7 +72,7 @@ def test_sky_scene_full_size():
     chunked path"""
     s = scenes.sky_scene()
     _same(s)
-    # timed again, with the CUDA context already up
+    # timed again, with the CUDA context up and the builder's memory pool warm
     host, gpu = scenes.BuiltPayload(s), scenes.BuiltPayload(s, gpu=True)
     for name, b in (("host", host), ("gpu", gpu)):
         st = b.stat
