@@ -14,10 +14,12 @@
 // Tasks (nodes to split) of one level run together: leaf tests in one
 // kernel, small tasks one block each (binning, split search and partition in
 // shared memory), large tasks in chunks with their bins in global memory.
+// The payload's tail (gpu_payload_tail) follows: vertex de-duplication in
+// BVH order, numbered as the host's sequential table numbers it, and the
+// Wald records of the triangles.
 #include <cuda_runtime.h>
 
 #include <algorithm>
-#include <chrono>
 #include <cstring>
 
 #include "bvh_gpu.h"

@@ -135,3 +135,33 @@ def test_live_reference_builder_if_available():
         assert np.array_equal(b.nodes(), nodes)
         assert np.array_equal(b.triangle_order(), order)
         assert (root, height) == (b.payload.bvh_root_node, b.stat.height)
+
+
+def test_light_mesh_must_carry_no_triangles():
+    s = scenes.room_scene(seed=1, light="sphere")
+    s.meshes[1]["tri_count"] = 2
+    with pytest.raises(_capi.NoorError):
+        scenes.BuiltPayload(s)
+
+
+def test_light_node_points_at_its_empty_leaf():
+    """a light mesh gets a one-leaf bottom-level tree (no triangles) before
+    the top level, as the reference's builder makes it, and the light node
+    points at it"""
+    s = scenes.room_scene(seed=1, light="disk")
+    b = scenes.BuiltPayload(s)
+    nodes = b.nodes()
+    light = [n for n in nodes if (n[7] & 0x08000000) and not (n[7] & _capi.TRI_LEAF_MASK)]
+    assert len(light) == 1 and (light[0][7] & 0x07FFFFFF) == 0
+    leaf = nodes[light[0][3]]
+    assert leaf[7] == _capi.TRI_LEAF_MASK and np.array_equal(leaf[:3], light[0][:3])
+
+
+def test_gpu_builder_fails_cleanly_without_a_device():
+    """noor_build_payload_gpu reports an error instead of falling back when
+    no CUDA device is there (this test only runs where there is none)"""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    with pytest.raises(_capi.NoorError):
+        scenes.BuiltPayload(scenes.room_scene(), gpu=True)
