@@ -935,6 +935,18 @@ static cudaError_t dalloc(cudaStream_t s, DevBuf& b, size_t n, T** out) {
     *out = static_cast<T*>(b.p);
     return e;
 }
+// a pair of timing events, released on every return path
+struct TimingEvents {
+    cudaEvent_t a = nullptr, b = nullptr;
+    cudaError_t create() {
+        cudaError_t e = cudaEventCreate(&a);
+        return e == cudaSuccess ? cudaEventCreate(&b) : e;
+    }
+    ~TimingEvents() {
+        if (a) cudaEventDestroy(a);
+        if (b) cudaEventDestroy(b);
+    }
+};
 static void keep_pool() {
     int dev = 0;
     cudaMemPool_t pool;
@@ -991,9 +1003,9 @@ int gpu_build_blas(const float* tri_box, uint32_t n_tris, const std::vector<GpuM
         ~StreamGuard() { cudaStreamDestroy(s); }
     } sg{s};
     keep_pool();
-    cudaEvent_t ev0, ev1;
-    cudaEventCreate(&ev0);
-    cudaEventCreate(&ev1);
+    TimingEvents te;
+    if ((e = te.create())) return fail("events", e);
+    cudaEvent_t ev0 = te.a, ev1 = te.b;
 
     DevBuf b_box, b_order, b_tmp, b_rank, b_sF, b_sT, b_pred, b_tasks0, b_tasks1, b_recs, b_levels, b_tiny, b_small,
         b_large, b_ctl, b_stats, b_splits, b_chunks, b_c0, b_ctrue, b_cbefore, b_gkeys, b_gcnt, b_meshoff, b_out;
@@ -1186,8 +1198,6 @@ int gpu_build_blas(const float* tri_box, uint32_t n_tris, const std::vector<GpuM
         return fail("download", e);
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, ev0, ev1);
-    cudaEventDestroy(ev0);
-    cudaEventDestroy(ev1);
     if (device_ms) *device_ms = ms;
     for (uint32_t i = 0; i < M; ++i) {
         GpuTree& t = trees[i];
@@ -1221,9 +1231,9 @@ int gpu_payload_tail(const GpuTailIn& in, GpuTailOut& out, double* device_ms, st
         ~StreamGuard() { cudaStreamDestroy(s); }
     } sg{s};
     keep_pool();
-    cudaEvent_t ev0, ev1;
-    cudaEventCreate(&ev0);
-    cudaEventCreate(&ev1);
+    TimingEvents te;
+    if ((e = te.create())) return fail("events", e);
+    cudaEvent_t ev0 = te.a, ev1 = te.b;
     DevBuf b_order, b_vi, b_ni, b_ui, b_vtx, b_nrm, b_uv, b_mi, b_mt, b_slots, b_pmin, b_cs, b_flag, b_first, b_sums,
         b_total, b_fail, b_ovtx, b_onrm, b_ouv, b_w0, b_w1, b_w2, b_attr;
     uint32_t *d_order, *d_vi, *d_ni, *d_ui, *d_mi, *d_mt, *d_slots, *d_pmin, *d_cs, *d_flag, *d_first, *d_sums,
@@ -1291,8 +1301,6 @@ int gpu_payload_tail(const GpuTailIn& in, GpuTailOut& out, double* device_ms, st
         return fail("download", e);
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, ev0, ev1);
-    cudaEventDestroy(ev0);
-    cudaEventDestroy(ev1);
     if (device_ms) *device_ms = ms;
     return NOOR_OK;
 }
