@@ -41,6 +41,7 @@ NOOR_LIGHT_SKY_MASK = 0x20
 NOOR_ISECT_WATERTIGHT, NOOR_ISECT_REF_WALD = 0, 1
 NOOR_FILM_KAHAN, NOOR_FILM_REF_LERP = 0, 1
 NOOR_SHAPE_QUAD, NOOR_SHAPE_SPHERE, NOOR_SHAPE_DISK = 0, 1, 2
+NOOR_CAMERA_PERSP, NOOR_CAMERA_ORTHO, NOOR_CAMERA_ENV = 0, 1, 2
 NOOR_TONEMAP_NONE, NOOR_TONEMAP_GAMMA, NOOR_TONEMAP_REINHARD, NOOR_TONEMAP_FILMIC, NOOR_TONEMAP_UNCHARTED2 = -1, 0, 1, 2, 3
 NOOR_DEV_STACK_OVERFLOW = 1
 

@@ -302,7 +302,7 @@ NB_D float3 replay(const PathCtx& C, uint32_t pix, uint32_t frame, const DevCame
     const DevScene& S = C.S;
     Rng rng{tea16(pix, frame)};
     float3 o, d;
-    camera_ray(cam, pix % cam.w, pix / cam.w, rng, o, d);
+    camera_ray<false>(cam, pix % cam.w, pix / cam.w, rng, o, d);
     float3 L = f3(0.0f), beta = f3(1.0f);
     float3 Lrem = Ltot;
     bool spec = false;
@@ -509,6 +509,8 @@ static int adjoint_run(const noor_adjoint_desc* desc, int mode, float* image, co
             l != kLobeFresnelSpec)
             return set_error(NOOR_ERR_UNSUPPORTED, "adjoint: materials other than diffuse, metal and glass");
     }
+    if (C->cam.type != NOOR_CAMERA_PERSP || C->cam.lens_radius > 0.0f)
+        return set_error(NOOR_ERR_UNSUPPORTED, "adjoint: cameras other than the pinhole");
     if (!st.quad_lights_only || S.num_delta_lights > 0)
         return set_error(NOOR_ERR_UNSUPPORTED, "adjoint: lights other than quad area lights and the sky");
     if (S.sky_type == NOOR_SKY_HDR && (!desc->d_env || (mode == 1 && !g_env)))

@@ -374,25 +374,13 @@ int upload_scene(Context& C, const noor_payload* P, const noor_hosek_sky* H, con
     return build_distribution(C, st);
 }
 
-static void load_camera(Context& C, const noor_camera& cam) {
-    DevCamera& d = C.cam;
-    for (int r = 0; r < 3; ++r) {
-        d.c2w[r] = make_float4(cam.camera_to_world[r][0], cam.camera_to_world[r][1], cam.camera_to_world[r][2],
-                               cam.camera_to_world[r][3]);
-        d.r2c[r] = make_float4(cam.raster_to_camera[r][0], cam.raster_to_camera[r][1], cam.raster_to_camera[r][2],
-                               cam.raster_to_camera[r][3]);
-    }
-    d.w = cam.w;
-    d.h = cam.h;
-    d.center = cam.center;
-}
+static void load_camera(Context& C, const noor_camera& cam) { C.cam = dev_camera(cam, cam.w, cam.h); }
 
 static int check_camera(const noor_camera* cam) {
     if (!cam) return set_error(NOOR_ERR_INVALID, "camera is null");
     if (cam->w == 0 || cam->h == 0 || (uint64_t)cam->w * cam->h > (1ull << 28))
         return set_error(NOOR_ERR_INVALID, "camera: bad image size");
-    if (cam->type != NOOR_CAMERA_PERSP || cam->lens_radius != 0.0f)
-        return set_error(NOOR_ERR_UNSUPPORTED, "camera: only the pinhole perspective camera is implemented");
+    if ((uint32_t)cam->type > NOOR_CAMERA_ENV) return set_error(NOOR_ERR_INVALID, "camera: unknown camera type");
     if (cam->center >= cam->w * cam->h) return set_error(NOOR_ERR_INVALID, "camera: centre pixel out of range");
     return NOOR_OK;
 }
@@ -486,16 +474,8 @@ int megakernel_frame(Context& C, const noor_wf_frame& f, float4* sum, float4* co
     DevScene S = C.scenes[f.scene_id]->dev;
     if (f.bounces) S.bounces = f.bounces;
     S.film_mode = NOOR_FILM_KAHAN;
-    DevCamera cam{};
-    for (int r = 0; r < 3; ++r) {
-        cam.c2w[r] = make_float4(f.camera.camera_to_world[r][0], f.camera.camera_to_world[r][1],
-                                 f.camera.camera_to_world[r][2], f.camera.camera_to_world[r][3]);
-        cam.r2c[r] = make_float4(f.camera.raster_to_camera[r][0], f.camera.raster_to_camera[r][1],
-                                 f.camera.raster_to_camera[r][2], f.camera.raster_to_camera[r][3]);
-    }
-    cam.w = f.width;
-    cam.h = f.height;
-    cam.center = f.camera.center;
+    if ((uint32_t)f.camera.type > NOOR_CAMERA_ENV) return set_error(NOOR_ERR_INVALID, "megakernel batch: bad camera type");
+    const DevCamera cam = dev_camera(f.camera, f.width, f.height);
     const uint32_t npix = f.width * f.height;
     MegaArgs a{};
     a.frame0 = f.first_frame;

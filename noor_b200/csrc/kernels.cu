@@ -62,7 +62,7 @@ __global__ void __launch_bounds__(kMegaBlock, NB_MEGA_MIN_BLOCKS) megakernel(Dev
             const uint32_t frame = a.frame0 + f;
             Rng rng{tea16(pix, frame)};
             float3 o, d;
-            camera_ray(C, x, y, rng, o, d);
+            camera_ray<EXT>(C, x, y, rng, o, d);
             hit_valid = false;
             const float3 L = path_radiance<ISECT, EXT>(S, o, d, rng, st, a.status, rs,
                                                        want_hit ? &hitp : nullptr, &hit_valid);
@@ -276,9 +276,10 @@ cudaError_t launch_megakernel(const DevScene& S, const DevCamera& C, const MegaA
     const uint32_t grid = (uint32_t)((threads + kMegaBlock - 1) / kMegaBlock);
     const size_t sm = stack_bytes(S, kMegaBlock);
     cudaError_t e;
-    // scenes without the extra lobes and lights run a specialisation without
-    // their code (the kernel's registers are capped, so unused branches cost
-    // spills)
+    // scenes without the extra lobes and lights, seen through a pinhole, run
+    // a specialisation without the other code (the kernel's registers are
+    // capped, so unused branches cost spills)
+    const bool ext_cam = C.type != NOOR_CAMERA_PERSP || C.lens_radius > 0.0f;
 #define NB_MK2(I, F, X)                                                                         \
     do {                                                                                        \
         e = cudaFuncSetAttribute(megakernel<I, F, X>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm); \
@@ -287,7 +288,7 @@ cudaError_t launch_megakernel(const DevScene& S, const DevCamera& C, const MegaA
     } while (0)
 #define NB_MK(I, F)                     \
     do {                                \
-        if (S.ext_lobes || S.ext_lights) NB_MK2(I, F, true); \
+        if (S.ext_lobes || S.ext_lights || ext_cam) NB_MK2(I, F, true); \
         else NB_MK2(I, F, false);       \
     } while (0)
     if (S.isect == NOOR_ISECT_WATERTIGHT) {

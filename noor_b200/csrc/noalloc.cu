@@ -60,8 +60,7 @@ extern "C" int noor_megakernel_frame_noalloc(const noor_wf_frame* f) {
     if (f->width == 0 || f->height == 0 || f->spp == 0 || f->first_frame == 0 || f->width != f->camera.w ||
         f->height != f->camera.h)
         return set_error(NOOR_ERR_INVALID, "no-alloc render: bad frame description");
-    if (f->camera.type != NOOR_CAMERA_PERSP || f->camera.lens_radius != 0.0f)
-        return set_error(NOOR_ERR_UNSUPPORTED, "no-alloc render: only the pinhole camera is implemented");
+    if ((uint32_t)f->camera.type > NOOR_CAMERA_ENV) return set_error(NOOR_ERR_INVALID, "no-alloc render: bad camera type");
     const uint64_t npix = (uint64_t)f->width * f->height;
     // one compensation value per pixel is the least a call needs
     if (npix > kNoAllocElems)
@@ -75,16 +74,7 @@ extern "C" int noor_megakernel_frame_noalloc(const noor_wf_frame* f) {
     DevScene S = C->scenes[f->scene_id]->dev;
     if (f->bounces) S.bounces = f->bounces;
     S.film_mode = NOOR_FILM_KAHAN;
-    DevCamera cam{};
-    for (int r = 0; r < 3; ++r) {
-        cam.c2w[r] = make_float4(f->camera.camera_to_world[r][0], f->camera.camera_to_world[r][1],
-                                 f->camera.camera_to_world[r][2], f->camera.camera_to_world[r][3]);
-        cam.r2c[r] = make_float4(f->camera.raster_to_camera[r][0], f->camera.raster_to_camera[r][1],
-                                 f->camera.raster_to_camera[r][2], f->camera.raster_to_camera[r][3]);
-    }
-    cam.w = f->width;
-    cam.h = f->height;
-    cam.center = f->camera.center;
+    const DevCamera cam = dev_camera(f->camera, f->width, f->height);
     // same split of the samples as the batch megakernel, reduced until the
     // partial films (2 x chunks x pixels) fit beside the compensation film
     const uint64_t target = (uint64_t)C->sm_count * 1024u;

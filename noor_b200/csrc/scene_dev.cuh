@@ -98,8 +98,27 @@ struct DevHosek {
 struct DevCamera {
     float4 c2w[3];
     float4 r2c[3];
-    uint32_t w, h, center, pad;
+    uint32_t w, h, center, type;  // type: NOOR_CAMERA_*
+    float lens_radius, focal_length, pad0, pad1;
 };
+// the raster-to-world transforms and image of a noor_camera, with the
+// image size given (a batch frame's own)
+inline DevCamera dev_camera(const noor_camera& c, uint32_t w, uint32_t h) {
+    DevCamera d{};
+    for (int r = 0; r < 3; ++r) {
+        d.c2w[r] = make_float4(c.camera_to_world[r][0], c.camera_to_world[r][1], c.camera_to_world[r][2],
+                               c.camera_to_world[r][3]);
+        d.r2c[r] = make_float4(c.raster_to_camera[r][0], c.raster_to_camera[r][1], c.raster_to_camera[r][2],
+                               c.raster_to_camera[r][3]);
+    }
+    d.w = w;
+    d.h = h;
+    d.center = c.center;
+    d.type = (uint32_t)c.type;
+    d.lens_radius = c.lens_radius;
+    d.focal_length = c.focal_length;
+    return d;
+}
 
 // Piecewise-constant 2D distribution over the environment (row = theta).
 struct DevDist2D {

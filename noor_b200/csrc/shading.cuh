@@ -31,14 +31,54 @@ struct Rng {
 
 // ---------------------------------------------------------------- camera
 // CudaPerspCamera::generateRay (noor/cuda/cameraimp.cuh:182-228), pinhole
+NB_D float2 concentric_disk(float ux, float uy);
+
+// EXT false: a kernel for pinhole cameras only
+template <bool EXT = true>
 NB_D void camera_ray(const DevCamera& C, uint32_t x, uint32_t y, Rng& rng, float3& o, float3& d) {
     const float rx = (float)x + rng.next() - 0.5f;
     const float ry = (float)y + rng.next() - 0.5f;
-    const float3 pc = f3(C.r2c[0].w + (C.r2c[0].x * rx + C.r2c[0].y * ry + C.r2c[0].z * 0.0f),
-                         C.r2c[1].w + (C.r2c[1].x * rx + C.r2c[1].y * ry + C.r2c[1].z * 0.0f),
-                         C.r2c[2].w + (C.r2c[2].x * rx + C.r2c[2].y * ry + C.r2c[2].z * 0.0f));
-    const float3 dc = normalize_fast(pc);
-    o = f3(C.c2w[0].w, C.c2w[1].w, C.c2w[2].w);
+    float3 dc, oc = f3(0.0f);
+    bool at_origin = true;
+    if (EXT && C.type == NOOR_CAMERA_ENV) {
+        // CudaEnvCamera::genDir (cameraimp.cuh:54-60): sphericalDirection
+        // (utils.cuh:457-468, right-handed: y up), normalised twice
+        const float theta = kPi * ry / (float)C.h + kPi;
+        const float phi = k2Pi * rx / (float)C.w - kPiOver2;
+        const float st = sinf(theta), ct = cosf(theta);
+        dc = normalize_fast(normalize_fast(f3(st * cosf(phi), ct, st * sinf(phi))));
+    } else {
+        const float3 pc = f3(C.r2c[0].w + (C.r2c[0].x * rx + C.r2c[0].y * ry + C.r2c[0].z * 0.0f),
+                             C.r2c[1].w + (C.r2c[1].x * rx + C.r2c[1].y * ry + C.r2c[1].z * 0.0f),
+                             C.r2c[2].w + (C.r2c[2].x * rx + C.r2c[2].y * ry + C.r2c[2].z * 0.0f));
+        if (EXT && C.type == NOOR_CAMERA_ORTHO) {
+            // CudaOrthoCamera (cameraimp.cuh:231-252): from the raster point, along -z
+            oc = pc;
+            dc = f3(0.0f, 0.0f, -1.0f);
+            at_origin = false;
+        } else {
+            dc = normalize_fast(pc);
+            if (EXT && C.lens_radius > 0.0f) {
+                // thin lens (cameraimp.cuh:191-202): a point on the lens, through
+                // the point of the pinhole ray on the plane of focus
+                const float u1 = rng.next();
+                const float u2 = rng.next();
+                const float2 l = concentric_disk(u1, u2);
+                const float ft = -C.focal_length / dc.z;
+                const float3 pf = f3(0.0f) + ft * dc;
+                oc = f3(C.lens_radius * l.x, C.lens_radius * l.y, 0.0f);
+                dc = normalize_fast(pf - oc);
+                at_origin = false;
+            }
+        }
+    }
+    // CudaRay::transform: the origin as a point, the direction as a vector
+    if (at_origin)
+        o = f3(C.c2w[0].w, C.c2w[1].w, C.c2w[2].w);
+    else
+        o = f3(C.c2w[0].w + (C.c2w[0].x * oc.x + C.c2w[0].y * oc.y + C.c2w[0].z * oc.z),
+               C.c2w[1].w + (C.c2w[1].x * oc.x + C.c2w[1].y * oc.y + C.c2w[1].z * oc.z),
+               C.c2w[2].w + (C.c2w[2].x * oc.x + C.c2w[2].y * oc.y + C.c2w[2].z * oc.z));
     const float3 dw = f3(C.c2w[0].x * dc.x + C.c2w[0].y * dc.y + C.c2w[0].z * dc.z,
                          C.c2w[1].x * dc.x + C.c2w[1].y * dc.y + C.c2w[1].z * dc.z,
                          C.c2w[2].x * dc.x + C.c2w[2].y * dc.y + C.c2w[2].z * dc.z);

@@ -687,19 +687,9 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
         if (f.width == 0 || f.height == 0 || f.spp == 0 || f.first_frame == 0 ||
             f.width != f.camera.w || f.height != f.camera.h)
             return set_error(NOOR_ERR_INVALID, "wavefront: bad frame description");
-        if (f.camera.type != NOOR_CAMERA_PERSP || f.camera.lens_radius != 0.0f)
-            return set_error(NOOR_ERR_UNSUPPORTED, "wavefront: only the pinhole camera is implemented");
+        if ((uint32_t)f.camera.type > NOOR_CAMERA_ENV) return set_error(NOOR_ERR_INVALID, "wavefront: bad camera type");
         std::memset(&fr[i], 0, sizeof(WfFrameDev));
-        DevCamera& dc = fr[i].cam;
-        for (int r = 0; r < 3; ++r) {
-            dc.c2w[r] = make_float4(f.camera.camera_to_world[r][0], f.camera.camera_to_world[r][1],
-                                    f.camera.camera_to_world[r][2], f.camera.camera_to_world[r][3]);
-            dc.r2c[r] = make_float4(f.camera.raster_to_camera[r][0], f.camera.raster_to_camera[r][1],
-                                    f.camera.raster_to_camera[r][2], f.camera.raster_to_camera[r][3]);
-        }
-        dc.w = f.width;
-        dc.h = f.height;
-        dc.center = f.camera.center;
+        fr[i].cam = dev_camera(f.camera, f.width, f.height);
         fr[i].npix = f.width * f.height;
         fr[i].base = total;
         fr[i].count = (unsigned long long)fr[i].npix * f.spp;

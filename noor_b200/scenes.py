@@ -610,10 +610,25 @@ def make_delta_lights(s: "SceneData"):
 
 
 def make_camera(cam: dict) -> capi.Camera:
+    """noor_camera_lookat's pinhole camera, or with `type` "ortho" (the
+    raster mapped onto a `ortho_scale`-wide window of the z = 0 plane, rays
+    along -z), "env" (360 x 180 degrees) or `lens_radius` / `focal_length`
+    (thin lens) set."""
     out = capi.Camera()
     arr = lambda v: (C.c_float * 3)(*[float(x) for x in v])
     capi.call("noor_camera_lookat", arr(cam["eye"]), arr(cam["look_at"]), arr(cam["up"]),
               float(np.radians(cam["fov_deg"])), int(cam["w"]), int(cam["h"]), C.byref(out))
+    kind = cam.get("type", "persp")
+    if kind == "ortho":
+        out.type = capi.NOOR_CAMERA_ORTHO
+        w, h, half = float(cam["w"]), float(cam["h"]), 0.5 * float(cam.get("ortho_scale", 2.0))
+        rows = [[2 * half / w, 0.0, 0.0, -half], [0.0, -2 * half / w, 0.0, half * h / w], [0.0, 0.0, 0.0, 0.0]]
+        for r in range(3):
+            out.raster_to_camera[r][:] = [float(x) for x in rows[r]]
+    elif kind == "env":
+        out.type = capi.NOOR_CAMERA_ENV
+    out.lens_radius = float(cam.get("lens_radius", 0.0))
+    out.focal_length = float(cam.get("focal_length", out.focal_length))
     return out
 
 

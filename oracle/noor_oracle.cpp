@@ -1549,16 +1549,52 @@ template <class T> V<T> radiance(const Scene& sc, V<T> o, V<T> d, Rng& rng, int 
 }
 
 // generateRay, pinhole (cameraimp.cuh:182-228)
+// generateRay of CudaPerspCamera (pinhole and thin lens), CudaOrthoCamera
+// and CudaEnvCamera (cameraimp.cuh:51-230), then CudaRay::transform
 template <class T> void cam_ray(const noor_camera& C, uint32_t x, uint32_t y, Rng& rng, V<T>& o, V<T>& d) {
     const float rxf = (float)x + rng.next() - 0.5f;
     const float ryf = (float)y + rng.next() - 0.5f;
     const T rx = rxf, ry = ryf;
-    T pc[3];
-    for (int r = 0; r < 3; ++r)
-        pc[r] = (T)C.raster_to_camera[r][3] +
-                ((T)C.raster_to_camera[r][0] * rx + (T)C.raster_to_camera[r][1] * ry + (T)C.raster_to_camera[r][2] * T(0));
-    const V<T> dc = nrm(mk(pc[0], pc[1], pc[2]));
-    o = mk((T)C.camera_to_world[0][3], (T)C.camera_to_world[1][3], (T)C.camera_to_world[2][3]);
+    V<T> dc, oc = mk(T(0), T(0), T(0));
+    bool at_origin = true;
+    if (C.type == NOOR_CAMERA_ENV) {
+        const T theta = K<T>::pi * ry / (T)C.h + K<T>::pi;
+        const T phi = (T(2) * K<T>::pi) * rx / (T)C.w - K<T>::pi / T(2);
+        const T st = std::sin(theta), ct = std::cos(theta);
+        dc = nrm(nrm(mk(st * std::cos(phi), ct, st * std::sin(phi))));
+    } else {
+        T pc[3];
+        for (int r = 0; r < 3; ++r)
+            pc[r] = (T)C.raster_to_camera[r][3] + ((T)C.raster_to_camera[r][0] * rx +
+                                                   (T)C.raster_to_camera[r][1] * ry + (T)C.raster_to_camera[r][2] * T(0));
+        if (C.type == NOOR_CAMERA_ORTHO) {
+            oc = mk(pc[0], pc[1], pc[2]);
+            dc = mk(T(0), T(0), T(-1));
+            at_origin = false;
+        } else {
+            dc = nrm(mk(pc[0], pc[1], pc[2]));
+            if (C.lens_radius > 0.0f) {
+                const float u1 = rng.next();
+                const float u2 = rng.next();
+                T lx, ly;
+                conc_disk<T>((T)u1, (T)u2, lx, ly);
+                const T ft = -(T)C.focal_length / dc.z;
+                const V<T> pf = mk(T(0), T(0), T(0)) + ft * dc;
+                oc = mk((T)C.lens_radius * lx, (T)C.lens_radius * ly, T(0));
+                dc = nrm(pf - oc);
+                at_origin = false;
+            }
+        }
+    }
+    if (at_origin) {
+        o = mk((T)C.camera_to_world[0][3], (T)C.camera_to_world[1][3], (T)C.camera_to_world[2][3]);
+    } else {
+        T ow[3];
+        for (int r = 0; r < 3; ++r)
+            ow[r] = (T)C.camera_to_world[r][3] + ((T)C.camera_to_world[r][0] * oc.x + (T)C.camera_to_world[r][1] * oc.y +
+                                                  (T)C.camera_to_world[r][2] * oc.z);
+        o = mk(ow[0], ow[1], ow[2]);
+    }
     T dw[3];
     for (int r = 0; r < 3; ++r)
         dw[r] = (T)C.camera_to_world[r][0] * dc.x + (T)C.camera_to_world[r][1] * dc.y + (T)C.camera_to_world[r][2] * dc.z;

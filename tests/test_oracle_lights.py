@@ -192,3 +192,47 @@ def test_shadow_catcher_is_a_shadow_matte():
     # either way (the shadow ray starts off the floor by the bias)
     dark = pix[shadow & ~on_blocker].max(1) == 0
     assert dark.mean() > 0.8, dark.mean()
+
+
+def _camera_rays(cam_dict, frame=1):
+    cam = scenes.make_camera(cam_dict)
+    rays = np.zeros((cam.w * cam.h, 8), np.float32)
+    lib().oracle_camera_rays(C.addressof(cam), frame, _p(rays))
+    return cam, rays[:, 0:3].astype(np.float64), rays[:, 4:7].astype(np.float64)
+
+
+def test_orthographic_camera_rays_are_parallel():
+    """CudaOrthoCamera: every ray along the camera's -z, origins spread over
+    the window"""
+    base = dict(eye=(0.0, 1.0, 3.0), look_at=(0.0, 1.0, 0.0), up=(0.0, 1.0, 0.0), fov_deg=40.0, w=16, h=12)
+    _, o, d = _camera_rays(dict(base, type="ortho", ortho_scale=2.0))
+    assert np.allclose(d, [0.0, 0.0, -1.0], atol=1e-6)
+    assert np.allclose(o[:, 2], 3.0, atol=1e-5)
+    assert o[:, 0].min() < -0.8 and o[:, 0].max() > 0.8 and o[:, 1].min() < 0.4 and o[:, 1].max() > 1.6
+
+
+def test_environment_camera_covers_the_sphere():
+    """CudaEnvCamera: the centre pixel looks along the camera's -z, the
+    image spans all longitudes and latitudes"""
+    base = dict(eye=(0.0, 0.0, 0.0), look_at=(0.0, 0.0, -1.0), up=(0.0, 1.0, 0.0), fov_deg=40.0, w=64, h=32)
+    cam, o, d = _camera_rays(dict(base, type="env"))
+    assert np.allclose(np.linalg.norm(d, axis=1), 1.0, atol=1e-6) and np.allclose(o, 0.0)
+    c = d.reshape(32, 64, 3)[16, 32]
+    assert c[2] < -0.99
+    assert d[:, 1].min() < -0.95 and d[:, 1].max() > 0.95            # both poles
+    assert (d[:, 0] > 0.9).any() and (d[:, 0] < -0.9).any() and (d[:, 2] > 0.9).any()
+
+
+def test_thin_lens_rays_meet_on_the_plane_of_focus():
+    """thin lens: rays of one pixel from different lens points cross the
+    plane of focus at one point (the pinhole ray's)"""
+    base = dict(eye=(0.0, 1.0, 4.0), look_at=(0.0, 1.0, 0.0), up=(0.0, 1.0, 0.0), fov_deg=40.0, w=8, h=8)
+    f = 3.0
+    pts = []
+    for frame in (1, 2, 3):
+        _, o, d = _camera_rays(dict(base, lens_radius=0.2, focal_length=f), frame)
+        _, o0, d0 = _camera_rays(base, frame)
+        assert np.abs(o - o0).max() > 1e-3                              # origins on the lens
+        t = (4.0 - f - o[:, 2]) / d[:, 2]                                 # plane z = 4 - f
+        t0 = (4.0 - f - o0[:, 2]) / d0[:, 2]
+        assert np.allclose(o + t[:, None] * d, o0 + t0[:, None] * d0, atol=2e-4)
