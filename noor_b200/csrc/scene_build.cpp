@@ -182,33 +182,91 @@ struct AttrKeyHash {
     }
 };
 
-// find-or-insert table of (vertex, normal, uv) index triples, linear probing
-struct AttrTable {
-    std::vector<AttrKey> keys;
-    std::vector<uint32_t> vals;
-    size_t mask;
-    explicit AttrTable(size_t n) {
-        size_t cap = 16;
-        while (cap < 2 * n) cap <<= 1;
-        keys.resize(cap);
-        vals.assign(cap, 0xFFFFFFFFu);
-        mask = cap - 1;
-    }
-    uint32_t find_or_add(const AttrKey& k, uint32_t v, bool& added) {
-        for (size_t i = AttrKeyHash()(k) & mask;; i = (i + 1) & mask) {
-            if (vals[i] == 0xFFFFFFFFu) {
-                keys[i] = k;
-                vals[i] = v;
-                added = true;
-                return v;
-            }
-            if (keys[i] == k) {
-                added = false;
-                return vals[i];
+
+// Vertex de-duplication of the corners in BVH order on all host threads,
+// numbered as a sequential find-or-insert pass numbers them (the first
+// occurrence of a (vertex, normal, uv) triple takes the next index): every
+// corner finds its key's slot in one open-addressing table (a slot holds any
+// corner with that key), the key keeps its first corner by an atomic
+// minimum, and a prefix count over the "first corner" flags numbers the new
+// vertices.  element[p] = new index of corner p; first[k] = the corner that
+// introduced new vertex k.  Returns the number of new vertices.
+template <class Key>
+static uint32_t dedup_corners(size_t C, const Key& key, std::vector<uint32_t>& element, std::vector<uint32_t>& first) {
+    constexpr uint32_t kEmpty = 0xFFFFFFFFu;
+    size_t cap = 16;
+    while (cap < 2 * C) cap <<= 1;
+    const size_t mask = cap - 1;
+    std::unique_ptr<std::atomic<uint32_t>[]> slot(new std::atomic<uint32_t>[cap]);
+    std::unique_ptr<std::atomic<uint32_t>[]> pmin(new std::atomic<uint32_t>[cap]);
+    std::vector<uint32_t> cslot(C), id(C);
+    const uint32_t nt = std::max(1u, std::min(std::thread::hardware_concurrency(), (uint32_t)(C / 65536 + 1)));
+    auto chunks = [&](size_t n, const auto& f) {  // f(thread, begin, end) on nt contiguous chunks
+        std::vector<std::thread> pool;
+        const size_t per = (n + nt - 1) / nt;
+        for (uint32_t t = 0; t < nt; ++t) {
+            const size_t b = t * per, e = std::min(n, b + per);
+            if (b >= e) break;
+            pool.emplace_back([&f, t, b, e]() { f(t, b, e); });
+        }
+        for (auto& th : pool) th.join();
+    };
+    chunks(cap, [&](uint32_t, size_t b, size_t e) {
+        for (size_t i = b; i < e; ++i) {
+            slot[i].store(kEmpty, std::memory_order_relaxed);
+            pmin[i].store(kEmpty, std::memory_order_relaxed);
+        }
+    });
+    chunks(C, [&](uint32_t, size_t b, size_t e) {
+        for (size_t p = b; p < e; ++p) {
+            const AttrKey k = key(p);
+            for (size_t i = AttrKeyHash()(k) & mask;; i = (i + 1) & mask) {
+                uint32_t s = slot[i].load(std::memory_order_acquire);
+                if (s == kEmpty) {
+                    uint32_t expect = kEmpty;
+                    if (slot[i].compare_exchange_strong(expect, (uint32_t)p, std::memory_order_acq_rel))
+                        s = (uint32_t)p;
+                    else
+                        s = expect;
+                }
+                if (key(s) == k) {
+                    cslot[p] = (uint32_t)i;
+                    uint32_t cur = pmin[i].load(std::memory_order_relaxed);
+                    while (p < cur && !pmin[i].compare_exchange_weak(cur, (uint32_t)p, std::memory_order_relaxed)) {
+                    }
+                    break;
+                }
             }
         }
+    });
+    std::vector<uint32_t> count(nt, 0);
+    chunks(C, [&](uint32_t t, size_t b, size_t e) {
+        uint32_t c = 0;
+        for (size_t p = b; p < e; ++p) c += pmin[cslot[p]].load(std::memory_order_relaxed) == p ? 1u : 0u;
+        count[t] = c;
+    });
+    std::vector<uint32_t> off(nt, 0);
+    uint32_t nv = 0;
+    for (uint32_t t = 0; t < nt; ++t) {
+        off[t] = nv;
+        nv += count[t];
     }
-};
+    first.resize(nv);
+    chunks(C, [&](uint32_t t, size_t b, size_t e) {
+        uint32_t k = off[t];
+        for (size_t p = b; p < e; ++p)
+            if (pmin[cslot[p]].load(std::memory_order_relaxed) == p) {
+                id[p] = k;
+                first[k] = (uint32_t)p;
+                ++k;
+            }
+    });
+    element.resize(C);
+    chunks(C, [&](uint32_t, size_t b, size_t e) {
+        for (size_t p = b; p < e; ++p) element[p] = id[pmin[cslot[p]].load(std::memory_order_relaxed)];
+    });
+    return nv;
+}
 
 // f(i) for i in [0, n) on all host threads (contiguous chunks)
 template <class F>
@@ -874,30 +932,24 @@ static int build_payload(const noor_scene_desc* d, bool gpu, noor_payload_handle
         } else {
             // vertex de-duplication in BVH order (Model::loadCudaPayload, model.cpp:376-401):
             // the first occurrence of a (vertex, normal, uv) index triple appends a
-            // vertex; later occurrences reuse its index
-            // (an open-addressing table: the same first-occurrence numbering as a
-            // map, without a node allocation per key)
-            AttrTable seen(3 * (size_t)d->num_triangles);
-            std::vector<uint32_t> element(3 * (size_t)d->num_triangles);
-            uint32_t nv = 0;
-            for (uint32_t i = 0; i < d->num_triangles; ++i) {
-                const uint32_t t = B.tri_order[i];
-                for (int j = 0; j < 3; ++j) {
-                    const AttrKey key{d->vindices[3 * (size_t)t + j], d->nindices[3 * (size_t)t + j],
-                                      d->uvindices[3 * (size_t)t + j]};
-                    bool added;
-                    const uint32_t id = seen.find_or_add(key, nv, added);
-                    if (added) {
-                        h->vertices.insert(h->vertices.end(), d->vertices + 4 * (size_t)key.v,
-                                           d->vertices + 4 * (size_t)key.v + 4);
-                        h->normals.insert(h->normals.end(), d->normals + 4 * (size_t)key.n,
-                                          d->normals + 4 * (size_t)key.n + 4);
-                        h->uvs.insert(h->uvs.end(), d->uvs + 2 * (size_t)key.u, d->uvs + 2 * (size_t)key.u + 2);
-                        ++nv;
-                    }
-                    element[3 * (size_t)i + j] = id;
-                }
-            }
+            // vertex; later occurrences reuse its index (dedup_corners: the same
+            // numbering as the reference's map, on all host threads)
+            const size_t nc = 3 * (size_t)d->num_triangles;
+            auto key = [&](size_t p) {
+                const size_t c = 3 * (size_t)B.tri_order[p / 3] + p % 3;
+                return AttrKey{d->vindices[c], d->nindices[c], d->uvindices[c]};
+            };
+            std::vector<uint32_t> element, first;
+            const uint32_t nv = dedup_corners(nc, key, element, first);
+            h->vertices.resize(4 * (size_t)nv);
+            h->normals.resize(4 * (size_t)nv);
+            h->uvs.resize(2 * (size_t)nv);
+            parallel_for(nv, [&](uint32_t k) {
+                const AttrKey kk = key(first[k]);
+                std::memcpy(h->vertices.data() + 4 * (size_t)k, d->vertices + 4 * (size_t)kk.v, 16);
+                std::memcpy(h->normals.data() + 4 * (size_t)k, d->normals + 4 * (size_t)kk.n, 16);
+                std::memcpy(h->uvs.data() + 2 * (size_t)k, d->uvs + 2 * (size_t)kk.u, 8);
+            });
             // Wald triangles + attribute indices (Model::buildWaldTriangles, model.cpp:333-360)
             for (int k = 0; k < 3; ++k) h->wald[k].resize(4 * (size_t)d->num_triangles);
             h->attr.resize(4 * (size_t)d->num_triangles);

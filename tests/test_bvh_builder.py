@@ -165,3 +165,29 @@ def test_gpu_builder_fails_cleanly_without_a_device():
         pytest.skip("a CUDA device is present")
     with pytest.raises(_capi.NoorError):
         scenes.BuiltPayload(scenes.room_scene(), gpu=True)
+
+
+@pytest.mark.parametrize("make", [lambda: scenes.room_scene(seed=1),
+                                  lambda: scenes.SceneData(**scenes.sphere_field(5, 6, 4)[0], name="f")])
+def test_vertex_deduplication_is_first_occurrence_in_bvh_order(make):
+    """Model::loadCudaPayload numbering (model.cpp:376-401), restated with
+    numpy: the corners in BVH order, each (vertex, normal, uv) triple
+    numbered by its first occurrence; the payload's attribute indices and
+    vertex arrays must be exactly that"""
+    s = make()
+    b = scenes.BuiltPayload(s)
+    order = b.triangle_order()
+    keys = np.stack([s.vindices[order].reshape(-1), s.nindices[order].reshape(-1),
+                     s.uvindices[order].reshape(-1)], axis=1).astype(np.int64)
+    packed = (keys[:, 0] << 42) | (keys[:, 1] << 21) | keys[:, 2]
+    uniq, first, inverse = np.unique(packed, return_index=True, return_inverse=True)
+    rank = np.empty(len(uniq), np.int64)
+    rank[np.argsort(first, kind="stable")] = np.arange(len(uniq))
+    element = rank[inverse]
+    attr = b.array("attribute_indices", 4)
+    assert np.array_equal(attr[:, :3].reshape(-1), element)
+    p = b.payload
+    verts = np.ctypeslib.as_array(p.vertices, (p.num_vertices, 4))
+    src = keys[np.sort(first)]
+    assert p.num_vertices == len(uniq)
+    assert np.array_equal(verts, np.asarray(s.vertices, np.float32)[src[:, 0]])
