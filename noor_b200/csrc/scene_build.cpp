@@ -343,6 +343,10 @@ public:
 
     const noor_scene_desc& D;
     bool use_gpu;  // bottom-level trees built on the current CUDA device
+    // host trees: subtrees of large ranges above this level are built on
+    // threads of their own (when meshes are fewer than threads)
+    uint32_t par_levels = 0;
+    static constexpr uint32_t kParMinTris = 32768;
     std::vector<Box> tri_box;
     std::vector<MeshInfo> meshes;
     Box scene_box, scene_cbox;
@@ -573,10 +577,45 @@ public:
         Range right{mid, r.e, w.R[a][p.index + 1], w.RC[a][p.index + 1], k};
         const uint32_t id = push_node(w, r.box, 0u, (k == kTriBin ? 0u : NOOR_MESH_INNER_MASK) | p.axis);
         ++w.stat.num_inner_nodes;
+        if (k == kTriBin && level < par_levels && cnt >= kParMinTris) {
+            // the two subtrees on two threads, each numbered from 0, then
+            // appended in depth-first order (left at id + 1, right after it)
+            Work wl, wr;
+            wl.init(D.bvh.num_bins);
+            wr.init(D.bvh.num_bins);
+            std::exception_ptr err;
+            std::thread t([&]() {
+                try {
+                    build(wl, left, level + 1);
+                } catch (...) {
+                    err = std::current_exception();
+                }
+            });
+            build(wr, right, level + 1);
+            t.join();
+            if (err) std::rethrow_exception(err);
+            append_tree(w, wl, id + 1);
+            const uint32_t rid = id + 1 + num_nodes(wl);
+            append_tree(w, wr, rid);
+            w.nodes[8 * (size_t)(id - w.base) + 3] = rid;
+            return id;
+        }
         build(w, left, level + 1);
         const uint32_t rid = build(w, right, level + 1);
         w.nodes[8 * (size_t)(id - w.base) + 3] = rid;
         return id;
+    }
+
+    // nodes of a tree numbered from 0 appended to w at node index `off`
+    // (inner nodes' right-child words moved by off), statistics merged
+    static void append_tree(Work& w, Work& sub, uint32_t off) {
+        for (size_t n = 0; n < sub.nodes.size(); n += 8)
+            if (!(sub.nodes[n + 7] & NOOR_TRI_LEAF_MASK)) sub.nodes[n + 3] += off;
+        w.nodes.insert(w.nodes.end(), sub.nodes.begin(), sub.nodes.end());
+        w.stat.height = std::max(w.stat.height, sub.stat.height);
+        w.stat.num_inner_nodes += sub.stat.num_inner_nodes;
+        w.stat.num_leaf_nodes += sub.stat.num_leaf_nodes;
+        w.stat.max_leaf_tris = std::max(w.stat.max_leaf_tris, sub.stat.max_leaf_tris);
     }
 
     // BVH::build (bvh.cpp:216-258).  The mesh trees are independent (each
@@ -634,6 +673,13 @@ public:
                 w.stat.max_leaf_tris = gt[k].max_leaf_tris;
                 done[gj[k]] = 1;
             }
+        }
+        {
+            size_t todo = 0;
+            for (size_t j = 0; j < src.size(); ++j) todo += done[j] ? 0 : 1;
+            const uint32_t hw = std::max(1u, std::thread::hardware_concurrency());
+            par_levels = 0;
+            while (todo && (todo << par_levels) < hw && par_levels < 8) ++par_levels;
         }
         std::atomic<size_t> next{0};
         std::vector<std::exception_ptr> errs(src.size());

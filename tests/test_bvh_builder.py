@@ -191,3 +191,18 @@ def test_vertex_deduplication_is_first_occurrence_in_bvh_order(make):
     src = keys[np.sort(first)]
     assert p.num_vertices == len(uniq)
     assert np.array_equal(verts, np.asarray(s.vertices, np.float32)[src[:, 0]])
+
+
+def test_single_large_mesh_matches_live_reference():
+    """one 327,680-triangle mesh: its top levels are split over host threads
+    (subtrees appended in depth-first order); the bytes must still be the
+    reference builder's"""
+    from oracle import oracle as O
+    if not O.ref_available():
+        pytest.skip("reference tree not compiled on this machine")
+    s = scenes.SceneData(**scenes.sphere_field(41, 1, 7)[0], name="one")
+    b = scenes.BuiltPayload(s)
+    nodes, root, order, height = O.ref_build_bvh(b.desc, s.num_triangles)
+    assert np.array_equal(b.nodes(), nodes)
+    assert np.array_equal(b.triangle_order(), order)
+    assert (root, height) == (b.payload.bvh_root_node, b.stat.height)
