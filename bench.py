@@ -75,6 +75,26 @@ def dist_env():
     return rank, world, local
 
 
+def max_over_ranks(x: float) -> float:
+    """the largest value of x over all ranks (a replicated job's step takes
+    as long as its slowest rank); x itself without a process group"""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return x
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(units_per_rank: float, ms_per_step: float, world: int) -> float:
+    """whole-job rate in millions of units per second: every rank renders
+    the full workload (replicas), so world x units in the slowest rank's
+    step time"""
+    return world * units_per_rank / (ms_per_step / 1000) / 1e6
+
+
 class Clocks:
     """nvidia-smi sampler during the timed region"""
 
@@ -576,13 +596,13 @@ def main():
     if args.impl == "reference":
         run_reference(args)
         return
-    if args.workload == "batched":
-        run_batched(args)
-        return
-    if args.workload == "adjoint":
-        run_adjoint(args)
-        return
     rank, world, local = dist_env()
+    if args.workload in ("batched", "adjoint"):
+        # one-GPU configurations: under a multi-rank launch rank 0 runs them
+        # (its line says n_gpus 1) and the other ranks exit without work
+        if rank == 0:
+            (run_batched if args.workload == "batched" else run_adjoint)(args)
+        return
     import torch
     if world > 1:
         import datetime
@@ -625,25 +645,21 @@ def main():
         l1 = C.c_uint64()
         _capi.call("noor_launch_count", C.byref(l1))
         ext, shadow, _ = p.counters()
-        ms_step = ms.value / args.steps
-        if world > 1:
-            t = torch.tensor([ms_step], device="cuda")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            ms_step = float(t.item())
+        ms_step = max_over_ranks(ms.value / args.steps)
         return ms_step, int(l1.value - l0.value), ext, shadow, clk.summary()
 
     ms_step, launches, ext, shadow, clocks = timed(path)
     npaths = path.w * path.h * args.spp
-    value = world * npaths / (ms_step / 1000) / 1e6
-    mrays = world * (ext + shadow) / args.steps / (ms_step / 1000) / 1e6
+    value = job_rate(npaths, ms_step, world)
+    mrays = job_rate((ext + shadow) / args.steps, ms_step, world)
     compare = None
     if other is not None:
         img = path.image()
         oms, olaunch, oext, oshadow, oclk = timed(other)
         oimg = other.image()
         rel = np.abs(img - oimg) / np.maximum(np.abs(oimg), 1e-2)
-        compare = {"integrator": other.name, "value": world * npaths / (oms / 1000) / 1e6, "ms_per_step": oms,
-                   "mrays_per_s": world * (oext + oshadow) / args.steps / (oms / 1000) / 1e6,
+        compare = {"integrator": other.name, "value": job_rate(npaths, oms, world), "ms_per_step": oms,
+                   "mrays_per_s": job_rate((oext + oshadow) / args.steps, oms, world),
                    "gpu_launches": olaunch, "clocks": oclk,
                    "speedup_of_headline": oms / ms_step,
                    "same_samples_image_check": {"median_rel_diff": float(np.median(rel)),
@@ -663,13 +679,9 @@ def main():
         path.e2e_step()
         if i >= args.warmup:
             e2e_t.append(time.perf_counter() - t)
-    e2e_ms = statistics.mean(e2e_t) * 1000
-    if world > 1:
-        t = torch.tensor([e2e_ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(statistics.mean(e2e_t) * 1000)
     h2d, d2h = path.e2e_bytes()
-    e2e = {"value": world * npaths / (e2e_ms / 1000) / 1e6, "unit": METRIC, "h2d_bytes_per_step": h2d,
+    e2e = {"value": job_rate(npaths, e2e_ms, world), "unit": METRIC, "h2d_bytes_per_step": h2d,
            "d2h_bytes_per_step": d2h}
 
     if rank == 0:
