@@ -213,7 +213,8 @@ int build_distribution(Context& C, SceneState& st) {
     return NOOR_OK;
 }
 
-int upload_scene(Context& C, const noor_payload* P, const noor_hosek_sky* H, const noor_spec* S, SceneState& st) {
+// every host-side check of a scene, made before any device work
+static int check_scene_inputs(const noor_payload* P, const noor_hosek_sky* H, const noor_spec* S) {
     int rc = validate_payload(P);
     if (rc) return rc;
     if (!S) return set_error(NOOR_ERR_INVALID, "spec is null");
@@ -221,6 +222,13 @@ int upload_scene(Context& C, const noor_payload* P, const noor_hosek_sky* H, con
     if (S->skydome_type == NOOR_SKY_PHYSICAL && !H) return set_error(NOOR_ERR_INVALID, "physical sky without Hosek state");
     if (S->intersector > 1u || S->film_mode > 1u) return set_error(NOOR_ERR_INVALID, "spec: bad selector");
     if (S->bvh_root_node >= P->num_bvh_nodes) return set_error(NOOR_ERR_INVALID, "spec: BVH root out of range");
+    return NOOR_OK;
+}
+
+int upload_scene(Context& C, const noor_payload* P, const noor_hosek_sky* H, const noor_spec* S, SceneState& st,
+                 bool checked = false) {
+    int rc = checked ? NOOR_OK : check_scene_inputs(P, H, S);
+    if (rc) return rc;
     DevScene& D = st.dev;
     std::memset(&D, 0, sizeof(D));
     const size_t nt = P->num_triangles, nn = P->num_bvh_nodes, nv = P->num_vertices, ni = P->num_instances;
@@ -519,7 +527,7 @@ extern "C" int load_cuda_data(const noor_payload* payload, const noor_hosek_sky*
     clear_error();
     int rc = check_camera(camera);
     if (rc) return rc;
-    if (!spec) return set_error(NOOR_ERR_INVALID, "spec is null");
+    if ((rc = check_scene_inputs(payload, hosek, spec))) return rc;
     if (tl_ctx) {
         delete tl_ctx;
         tl_ctx = nullptr;
@@ -545,7 +553,7 @@ extern "C" int load_cuda_data(const noor_payload* payload, const noor_hosek_sky*
     C->camera_src = camera;
     C->spec_src = spec;
     C->scenes.emplace_back(new SceneState());
-    if ((rc = upload_scene(*C, payload, hosek, spec, *C->scenes[0]))) return rc;
+    if ((rc = upload_scene(*C, payload, hosek, spec, *C->scenes[0], true))) return rc;
     load_camera(*C, *camera);
     if ((rc = ensure_film(*C, camera->w, camera->h))) return rc;
     if ((rc = sync_and_check(*C, "load_cuda_data"))) return rc;

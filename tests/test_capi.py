@@ -6,6 +6,7 @@ import subprocess
 from pathlib import Path
 
 import numpy as np
+import pytest
 
 from noor_b200 import _capi
 
@@ -81,3 +82,83 @@ def test_bad_payload_is_rejected():
     sp = _capi.Spec()
     rc = L.load_cuda_data(C.byref(p), None, C.byref(cam), C.byref(sp), None)
     assert rc != 0
+
+
+def _bad_sphere_type(b, cam, sp):
+    b.payload.area_lights[0].shape.type = 9
+
+
+def _bad_sphere_radius(b, cam, sp):
+    b.payload.area_lights[0].shape.radius = 0.0
+
+
+def _bad_camera(b, cam, sp):
+    cam.type = 5
+
+
+def _bad_sky(b, cam, sp):
+    sp.skydome_type = 7
+
+
+def _bad_selector(b, cam, sp):
+    sp.intersector = 3
+
+
+def _bump_map(b, cam, sp):
+    b.payload.materials[0].type |= 1 << 13  # NOOR_BUMP
+
+
+def _bad_texture_index(b, cam, sp):
+    b.payload.materials[0].diffuse_tex_idx = b.payload.num_textures
+
+
+def _bad_distribution(b, cam, sp):
+    b.payload.materials[0].distribution = 2
+
+
+def _distant_lights_without_array(b, cam, sp):
+    b.payload.num_distant_lights = 2
+
+
+def _two_infinite_lights(b, cam, sp):
+    b.payload.num_infinite_lights = 2
+
+
+@pytest.mark.parametrize("mutate,code,text", [
+    (_bad_sphere_type, 1, b"unknown area light shape type"),
+    (_bad_sphere_radius, 1, b"without a radius"),
+    (_bad_camera, 1, b"unknown camera type"),
+    (_bad_sky, 1, b"bad skydome type"),
+    (_bad_selector, 1, b"bad selector"),
+    (_bump_map, 4, b"bump maps are not implemented"),
+    (_bad_texture_index, 1, b"texture index out of range"),
+    (_bad_distribution, 1, b"unknown microfacet distribution"),
+    (_distant_lights_without_array, 1, b"bad point, spot or distant light array"),
+    (_two_infinite_lights, 1, b"at most one infinite light"),
+])
+def test_scene_inputs_are_checked_before_the_device(mutate, code, text):
+    """load_cuda_data checks the payload, spec and camera on the host before
+    any device work, so these errors come back the same with or without a
+    GPU; a valid scene gets past them (to the device check here)"""
+    from noor_b200 import scenes
+    L = _capi.lib()
+    s = scenes.room_scene(seed=1, light="sphere")
+    b = scenes.BuiltPayload(s)
+    cam, sp, hs = scenes.make_camera(s.camera), b.default_spec(5, 1), scenes.make_hosek(s.hosek)
+    mutate(b, cam, sp)
+    rc = L.load_cuda_data(C.byref(b.payload), C.byref(hs), C.byref(cam), C.byref(sp), None)
+    assert rc == code, (rc, L.noor_last_error())
+    assert text in L.noor_last_error()
+
+
+def test_valid_scene_passes_the_host_checks():
+    from noor_b200 import scenes
+    L = _capi.lib()
+    s = scenes.room_scene(seed=1, light="sphere")
+    b = scenes.BuiltPayload(s)
+    cam, sp, hs = scenes.make_camera(s.camera), b.default_spec(5, 1), scenes.make_hosek(s.hosek)
+    rc = L.load_cuda_data(C.byref(b.payload), C.byref(hs), C.byref(cam), C.byref(sp), None)
+    if rc == 0:  # a device is present: the scene loaded
+        L.device_free_memory()
+    else:
+        assert (rc, L.noor_last_error()) == (2, b"no CUDA device available")
