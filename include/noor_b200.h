@@ -306,7 +306,9 @@ typedef struct noor_spec {
  * spec are remembered (not copied for later): update_cuda_* re-read them, as
  * the reference device struct keeps references (noor/cuda/render.cuh:38-40).
  * The env/sky importance-sampling distribution is built here.  texture_handle
- * is unused (no graphics interop) and may be NULL. */
+ * is unused (no graphics interop) and may be NULL.  The payload, spec and
+ * camera are checked on the host first; a call they fail leaves the thread's
+ * current context as it was. */
 int load_cuda_data(const noor_payload* payload, const noor_hosek_sky* hosek,
                    const noor_camera* camera, const noor_spec* spec,
                    void* texture_handle);
