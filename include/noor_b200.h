@@ -414,6 +414,21 @@ int noor_camera_rays(unsigned int frame, noor_ray* d_rays);
  * in: per sample 16 floats {wo_local[3], wi_local[3], u[2], mat_idx, ...}
  * out: per sample 8 floats {f[3], pdf, wi_local[3], sampled_type}.        */
 int noor_eval_bsdf(int kind, const float* d_in, float* d_out, size_t n);
+/* Stand-alone shading routines (parity tests), device arrays; needs no
+ * context (launched on the current context's stream if there is one).
+ * kind 0 / 1: Trowbridge-Reitz / Beckmann microfacet distribution
+ *   (noor/cuda/distribution.cuh:58-342) with alpha = max(r^2, 1e-3) per
+ *   axis; in 12 floats {r_x, r_y, wo[3], wh[3], u[2], -, -}, out 12 floats
+ *   {D(wh), G(wo, wh), Pdf(wo, wh), Sample_wh(wo, u)[3], 0, alpha_x, 0...}
+ * kind 2: Fresnel (noor/cuda/fresnel.cuh:58-107); in 9 floats {cos, etaI,
+ *   etaT, eta[3], k[3]}, out 4 floats {dielectric F, conductor F[3] with
+ *   etaI = 1}
+ * kind 3: warps (noor/cuda/utils.cuh:364-404,470-486,487-539); in 3 floats
+ *   {u[2], x}, out 16 floats {concentricSampleDisk[2],
+ *   cosineSampleHemisphere[3], uniformSampleHemisphere[3] (both z up),
+ *   sphericalDirection(u)[3], its sinTheta, powerHeuristic(1, u.x, 1, u.y),
+ *   Erf(x), ErfInv(x), 0} */
+int noor_eval_routines(int kind, const float* d_in, float* d_out, size_t n);
 /* Hosek radiance of directions (3 floats each) -> rgb (3 floats each) */
 int noor_eval_sky(const float* d_dirs, float* d_rgb, size_t n);
 /* environment distribution: u (2 floats) -> {x, y, pdf} and pdf at (x,y) */

@@ -220,6 +220,7 @@ PROTOTYPES = {
     "noor_trace_any": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t]),
     "noor_camera_rays": (C.c_int, [C.c_uint, C.c_void_p]),
     "noor_eval_bsdf": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_size_t]),
+    "noor_eval_routines": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_size_t]),
     "noor_eval_sky": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t]),
     "noor_eval_env_sample": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t]),
     "noor_get_env_distribution": (C.c_int, [C.POINTER(C.c_int), C.POINTER(C.c_int), pf, pf, pf, pf,

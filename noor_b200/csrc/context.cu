@@ -841,6 +841,16 @@ extern "C" int noor_eval_bsdf(int kind, const float* d_in, float* d_out, size_t 
     return sync_and_check(*C, "eval_bsdf");
 }
 
+extern "C" int noor_eval_routines(int kind, const float* d_in, float* d_out, size_t n) {
+    if (kind < 0 || kind > 3 || (n && (!d_in || !d_out))) return set_error(NOOR_ERR_INVALID, "eval_routines: bad argument");
+    cudaStream_t st = tl_ctx ? tl_ctx->stream : 0;
+    cudaError_t e = launch_eval_routines(kind, d_in, d_out, n, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_fail(e, "eval_routines");
+    if (tl_ctx) tl_ctx->launches++;
+    return NOOR_OK;
+}
+
 extern "C" int noor_eval_sky(const float* d_dirs, float* d_rgb, size_t n) {
     Context* C;
     int rc = need_ctx(C);

@@ -220,6 +220,44 @@ __global__ void k_eval_bsdf(DevScene S, int kind, const float* in, float* out, s
     q[7] = (float)st;
 }
 
+// Stand-alone shading routines for parity tests; record layouts in
+// include/noor_b200.h (noor_eval_routines).
+__global__ void k_eval_routines(int kind, const float* in, float* out, size_t n) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (kind <= 1) {
+        const float* p = in + 12 * i;
+        float* q = out + 12 * i;
+        Micro m;
+        m.ax = fmaxf(p[0] * p[0], 1e-3f);
+        m.ay = fmaxf(p[1] * p[1], 1e-3f);
+        m.dist = (uint32_t)kind;
+        const float3 wo = f3(p[2], p[3], p[4]), wh = f3(p[5], p[6], p[7]);
+        const float3 s = m.sample_wh(wo, p[8], p[9]);
+        const float r[12] = {m.D(wh), m.G(wo, wh), m.pdf(wo, wh), s.x, s.y, s.z, 0.0f, m.ax, 0.0f, 0.0f, 0.0f, 0.0f};
+        for (int k = 0; k < 12; ++k) q[k] = r[k];
+    } else if (kind == 2) {
+        const float* p = in + 9 * i;
+        float* q = out + 4 * i;
+        q[0] = fresnel_dielectric(p[0], p[1], p[2]);
+        const float3 c = fresnel_conductor(p[0], f3(p[3], p[4], p[5]), f3(p[6], p[7], p[8]));
+        q[1] = c.x;
+        q[2] = c.y;
+        q[3] = c.z;
+    } else {
+        const float* p = in + 3 * i;
+        float* q = out + 16 * i;
+        const float2 d = concentric_disk(p[0], p[1]);
+        const float3 c = cosine_hemisphere(p[0], p[1]);
+        float st;
+        const float3 sd = spherical_direction(p[0], p[1], st);
+        const float3 h = uniform_hemisphere(p[0], p[1]);
+        const float r[16] = {d.x, d.y, c.x, c.y, c.z, h.x, h.y, h.z, sd.x, sd.y, sd.z, st,
+                             power_heuristic(p[0], p[1]), erf_as(p[2]), erfinv_giles(p[2]), 0.0f};
+        for (int k = 0; k < 16; ++k) q[k] = r[k];
+    }
+}
+
 __global__ void k_eval_sky(DevScene S, const float* dirs, float* rgb, size_t n) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -358,6 +396,12 @@ cudaError_t launch_camera_rays(const DevCamera& C, uint32_t frame, noor_ray* ray
 cudaError_t launch_eval_bsdf(const DevScene& S, int kind, const float* in, float* out, size_t n, cudaStream_t s) {
     if (n == 0) return cudaSuccess;
     k_eval_bsdf<<<(uint32_t)((n + 255) / 256), 256, 0, s>>>(S, kind, in, out, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_eval_routines(int kind, const float* in, float* out, size_t n, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    k_eval_routines<<<(uint32_t)((n + 255) / 256), 256, 0, s>>>(kind, in, out, n);
     return cudaGetLastError();
 }
 

@@ -31,6 +31,7 @@ cudaError_t launch_trace_any(const DevScene& S, const noor_ray* rays, uint32_t* 
 cudaError_t launch_camera_rays(const DevCamera& C, uint32_t frame, noor_ray* rays, cudaStream_t s);
 cudaError_t launch_eval_bsdf(const DevScene& S, int kind, const float* in, float* out, size_t n, cudaStream_t s);
 cudaError_t launch_eval_sky(const DevScene& S, const float* dirs, float* rgb, size_t n, cudaStream_t s);
+cudaError_t launch_eval_routines(int kind, const float* in, float* out, size_t n, cudaStream_t s);
 cudaError_t launch_env_sample(const DevScene& S, const float* u, float* out, size_t n, cudaStream_t s);
 cudaError_t launch_debug_skydome(const DevScene& S, const DevCamera& C, uint32_t frame, float4* film, int mis,
                                  cudaStream_t s);

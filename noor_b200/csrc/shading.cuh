@@ -119,11 +119,28 @@ NB_D float3 cosine_hemisphere(float ux, float uy) {
     return f3(d.x, d.y, z);
 }
 
+// uniformSampleHemisphere, left handed (utils.cuh:364-372): z = u.x
+NB_D float3 uniform_hemisphere(float ux, float uy) {
+    const float z = ux;
+    const float r = sqrtf(fmaxf(0.0f, 1.0f - z * z));
+    const float phi = 2.0f * kPi * uy;
+    return f3(r * cosf(phi), r * sinf(phi), z);
+}
+
 NB_D float spherical_phi(const float3& v) {
     const float p = atan2f(v.z, v.x);
     return (p < 0.0f) ? (p + k2Pi) : p;
 }
 NB_D float spherical_theta(const float3& v) { return acosf(clampf(v.y, -1.0f, 1.0f)); }
+// sphericalDirection(u, sinTheta) (utils.cuh:470-476): phi = 2 pi u.x,
+// theta = pi u.y, y up, normalised
+NB_D float3 spherical_direction(float ux, float uy, float& sin_theta) {
+    const float phi = ux * k2Pi;
+    const float theta = uy * kPi;
+    const float ct = cosf(theta);
+    sin_theta = sinf(theta);
+    return normalize_fast(f3(sin_theta * cosf(phi), ct, sin_theta * sinf(phi)));
+}
 
 // ----------------------------------------------------------- shading frame
 struct Frame {
@@ -210,7 +227,10 @@ NB_D float sin2phi(const float3& w) { return sinphi(w) * sinphi(w); }
 NB_D bool same_hemi(const float3& a, const float3& b) { return a.z * b.z > 0.0f; }
 
 // ---------------------------------------------------------------- Fresnel
-// fresnelDielectric (noor/cuda/fresnel.cuh:58-80)
+// fresnelDielectric (noor/cuda/fresnel.cuh:58-80).  Every operation rounds
+// on its own (no FMA contraction), the arithmetic of the reference built for
+// the host: near the critical angle the cosine of refraction cancels, and
+// a contracted 1 - sin^2 moves the result by up to 1e-4.
 NB_D float fresnel_dielectric(float cosI, float etaI, float etaT) {
     cosI = clampf(cosI, -1.0f, 1.0f);
     if (!(cosI > 0.0f)) {
@@ -219,34 +239,37 @@ NB_D float fresnel_dielectric(float cosI, float etaI, float etaT) {
         etaT = tmp;
         cosI = fabsf(cosI);
     }
-    const float sinI = sqrtf(fmaxf(0.0f, 1.0f - cosI * cosI));
-    const float sinT = etaI / etaT * sinI;
+    const float sinI = sqrtf(fmaxf(0.0f, xsub(1.0f, xmul(cosI, cosI))));
+    const float sinT = xmul(xdiv(etaI, etaT), sinI);
     if (sinT >= 1.0f) return 1.0f;
-    const float cosT = sqrtf(fmaxf(0.0f, 1.0f - sinT * sinT));
-    const float rpar = ((etaT * cosI) - (etaI * cosT)) / ((etaT * cosI) + (etaI * cosT));
-    const float rper = ((etaI * cosI) - (etaT * cosT)) / ((etaI * cosI) + (etaT * cosT));
-    return (rpar * rpar + rper * rper) / 2.0f;
+    const float cosT = sqrtf(fmaxf(0.0f, xsub(1.0f, xmul(sinT, sinT))));
+    const float a = xmul(etaT, cosI), b = xmul(etaI, cosT), c = xmul(etaI, cosI), d = xmul(etaT, cosT);
+    const float rpar = xdiv(xsub(a, b), xadd(a, b));
+    const float rper = xdiv(xsub(c, d), xadd(c, d));
+    return xdiv(xadd(xmul(rpar, rpar), xmul(rper, rper)), 2.0f);
 }
 NB_D float3 sqrt3(const float3& v) { return f3(sqrtf(v.x), sqrtf(v.y), sqrtf(v.z)); }
-// fresnelConductor with etaI = 1 (noor/cuda/fresnel.cuh:81-107)
+// fresnelConductor with etaI = 1 (noor/cuda/fresnel.cuh:81-107), per
+// channel, each operation rounded on its own as above
+NB_D float fresnel_conductor1(float cosI, float c2, float s2, float eta, float k) {
+    const float eta2 = xmul(eta, eta), etak2 = xmul(k, k);
+    const float t0 = xsub(xsub(eta2, etak2), s2);
+    const float a2b2 = sqrtf(xadd(xmul(t0, t0), xmul(xmul(4.0f, eta2), etak2)));
+    const float t1 = xadd(a2b2, c2);
+    const float a = sqrtf(xmul(0.5f, xadd(a2b2, t0)));
+    const float t2 = xmul(xmul(2.0f, cosI), a);
+    const float Rs = xdiv(xsub(t1, t2), xadd(t1, t2));
+    const float t3 = xadd(xmul(c2, a2b2), xmul(s2, s2));
+    const float t4 = xmul(t2, s2);
+    const float Rp = xdiv(xmul(Rs, xsub(t3, t4)), xadd(t3, t4));
+    return xmul(0.5f, xadd(Rp, Rs));
+}
 NB_D float3 fresnel_conductor(float cosI, const float3& etaT, const float3& k) {
     cosI = clampf(cosI, -1.0f, 1.0f);
-    const float3 eta = etaT / f3(1.0f);
-    const float3 etak = k / f3(1.0f);
-    const float c2 = cosI * cosI;
-    const float s2 = 1.0f - c2;
-    const float3 eta2 = eta * eta;
-    const float3 etak2 = etak * etak;
-    const float3 t0 = eta2 - etak2 - f3(s2);
-    const float3 a2b2 = sqrt3(t0 * t0 + 4.0f * eta2 * etak2);
-    const float3 t1 = a2b2 + f3(c2);
-    const float3 a = sqrt3(0.5f * (a2b2 + t0));
-    const float3 t2 = 2.0f * cosI * a;
-    const float3 Rs = (t1 - t2) / (t1 + t2);
-    const float3 t3 = c2 * a2b2 + f3(s2 * s2);
-    const float3 t4 = t2 * s2;
-    const float3 Rp = Rs * (t3 - t4) / (t3 + t4);
-    return 0.5f * (Rp + Rs);
+    const float c2 = xmul(cosI, cosI);
+    const float s2 = xsub(1.0f, c2);
+    return f3(fresnel_conductor1(cosI, c2, s2, etaT.x, k.x), fresnel_conductor1(cosI, c2, s2, etaT.y, k.y),
+              fresnel_conductor1(cosI, c2, s2, etaT.z, k.z));
 }
 
 // ---------------------------------------------- Trowbridge-Reitz (GGX)
@@ -764,12 +787,9 @@ NB_D float3 lobe_sample_all(uint32_t lobe, const DevMaterial& m, const float3& w
         return r;
     }
     if (lobe == kLobeCatcher) {
-        // CudaShadowCatcher::Sample_f: uniformSampleHemisphere (utils.cuh,
-        // left-handed: z = u.x) with pdf 1, as the reference has it
-        const float z = ux;
-        const float r = sqrtf(fmaxf(0.0f, 1.0f - z * z));
-        const float phi = k2Pi * uy;
-        wi = f3(r * cosf(phi), r * sinf(phi), z);
+        // CudaShadowCatcher::Sample_f: uniformSampleHemisphere with pdf 1,
+        // as the reference has it
+        wi = uniform_hemisphere(ux, uy);
         pdf = 1.0f;
         return f3(1.0f / fabsf(wi.z));
     }
@@ -1090,11 +1110,8 @@ NB_D float3 env_sample_dir(const DevScene& S, Rng& rng, float& pdf) {
     const float u1 = rng.next();
     float mp;
     const float2 uv = dist_sample(S.dist, u0, u1, mp);
-    const float phi = uv.x * k2Pi;
-    const float theta = uv.y * kPi;
-    const float ct = cosf(theta);
-    const float st = sinf(theta);
-    const float3 dir = normalize_fast(f3(st * cosf(phi), ct, st * sinf(phi)));
+    float st;
+    const float3 dir = spherical_direction(uv.x, uv.y, st);
     pdf = (st == 0.0f) ? 0.0f : mp / (2.0f * kPi * kPi * st);
     return dir;
 }

@@ -164,36 +164,42 @@ NB_D bool wt_test(const TRay& r, const WtRay& w, const DevWtTri* tri, float& tma
 // quad of an area light (noor/cuda/geometry.cuh:105-123); note the
 // reference accepts negative t (no lower bound), kept as is.
 NB_D bool quad_hit(const DevAreaLight& q, const float3& o, const float3& d, float& tmax) {
-    const float denom = dot(q.n, d);
+    const float denom = xdot3(q.n.x, q.n.y, q.n.z, d.x, d.y, d.z);
     if (denom == 0.0f) return false;
-    const float t = -(dot(o, q.n) - dot(q.center, q.n)) / denom;
+    const float t = xdiv(-xsub(xdot3(o.x, o.y, o.z, q.n.x, q.n.y, q.n.z),
+                               xdot3(q.center.x, q.center.y, q.center.z, q.n.x, q.n.y, q.n.z)),
+                         denom);
     if (t > tmax) return false;
-    const float3 p = o + t * d;
-    const float3 ip = p - q.center;
-    const float t0 = dot(ip, q.u) / dot(q.u, q.u);
+    // pointAtParameter(t) - center
+    const float ix = xsub(xadd(o.x, xmul(t, d.x)), q.center.x);
+    const float iy = xsub(xadd(o.y, xmul(t, d.y)), q.center.y);
+    const float iz = xsub(xadd(o.z, xmul(t, d.z)), q.center.z);
+    const float t0 = xdiv(xdot3(ix, iy, iz, q.u.x, q.u.y, q.u.z), xdot3(q.u.x, q.u.y, q.u.z, q.u.x, q.u.y, q.u.z));
     if (t0 < 0.0f || t0 > 1.0f) return false;
-    const float t1 = dot(ip, q.v) / dot(q.v, q.v);
+    const float t1 = xdiv(xdot3(ix, iy, iz, q.v.x, q.v.y, q.v.z), xdot3(q.v.x, q.v.y, q.v.z, q.v.x, q.v.y, q.v.z));
     if (t1 < 0.0f || t1 > 1.0f) return false;
     tmax = t;
     return true;
 }
 
 // solveQuadratic (noor/cuda/utils.cuh:52-91): the root of larger magnitude
-// first, the other from x0 * x1 = c / a; returns x0 <= x1
+// first, the other from x0 * x1 = c / a; returns x0 <= x1.  Like the light
+// shape tests below, every operation rounds on its own, so that the hit
+// distance is the reference's to the bit.
 NB_D bool solve_quadratic(float a, float b, float c, float& x0, float& x1) {
     if (a == 0.0f) {
         if (b != 0.0f) {
-            x0 = x1 = -c / b;
+            x0 = x1 = xdiv(-c, b);
             return true;
         }
         return false;
     }
-    const float disc = b * b - 4.0f * a * c;
+    const float disc = xsub(xmul(b, b), xmul(xmul(4.0f, a), c));
     if (disc < 0.0f) return false;
     const float sd = sqrtf(disc);
-    const float q = b < 0.0f ? -0.5f * (b - sd) : -0.5f * (b + sd);
-    x0 = q / a;
-    x1 = c / q;
+    const float q = b < 0.0f ? xmul(-0.5f, xsub(b, sd)) : xmul(-0.5f, xadd(b, sd));
+    x0 = xdiv(q, a);
+    x1 = xdiv(c, q);
     if (x0 > x1) {
         const float t = x0;
         x0 = x1;
@@ -205,9 +211,11 @@ NB_D bool solve_quadratic(float a, float b, float c, float& x0, float& x1) {
 // sphere of an area light (noor/cuda/geometry.cuh:125-150): nearest root in
 // [0, tmax], else the far root when the near one is behind the origin
 NB_D bool sphere_hit(const DevAreaLight& s, const float3& o, const float3& d, float& tmax) {
-    const float3 oc = o - s.center;
+    const float ox = xsub(o.x, s.center.x), oy = xsub(o.y, s.center.y), oz = xsub(o.z, s.center.z);
     float t0, t1;
-    if (!solve_quadratic(length2(d), 2.0f * dot(oc, d), length2(oc) - s.radius2, t0, t1)) return false;
+    if (!solve_quadratic(xdot3(d.x, d.y, d.z, d.x, d.y, d.z), xmul(2.0f, xdot3(ox, oy, oz, d.x, d.y, d.z)),
+                         xsub(xdot3(ox, oy, oz, ox, oy, oz), s.radius2), t0, t1))
+        return false;
     if (!(t0 <= tmax && t1 >= 0.0f)) return false;
     if (t0 < 0.0f) {
         if (t1 > tmax) return false;
@@ -221,12 +229,16 @@ NB_D bool sphere_hit(const DevAreaLight& s, const float3& o, const float3& d, fl
 // disk of an area light (noor/cuda/geometry.cuh:152-163); like the quad, no
 // lower bound on t
 NB_D bool disk_hit(const DevAreaLight& q, const float3& o, const float3& d, float& tmax) {
-    const float denom = dot(q.n, d);
+    const float denom = xdot3(q.n.x, q.n.y, q.n.z, d.x, d.y, d.z);
     if (denom == 0.0f) return false;
-    const float t = -(dot(o, q.n) - dot(q.center, q.n)) / denom;
+    const float t = xdiv(-xsub(xdot3(o.x, o.y, o.z, q.n.x, q.n.y, q.n.z),
+                               xdot3(q.center.x, q.center.y, q.center.z, q.n.x, q.n.y, q.n.z)),
+                         denom);
     if (t > tmax) return false;
-    const float3 p = (o + t * d) - q.center;
-    if (length2(p) > q.radius2) return false;
+    const float px = xsub(xadd(o.x, xmul(t, d.x)), q.center.x);
+    const float py = xsub(xadd(o.y, xmul(t, d.y)), q.center.y);
+    const float pz = xsub(xadd(o.z, xmul(t, d.z)), q.center.z);
+    if (xdot3(px, py, pz, px, py, pz) > q.radius2) return false;
     tmax = t;
     return true;
 }

@@ -2111,6 +2111,50 @@ OR_API void oracle_eval_bsdf(void* h, int kind, const float* in, float* out, siz
     }
 }
 
+// Stand-alone routines, the record layouts of noor_eval_routines
+// (include/noor_b200.h): 0 / 1 Trowbridge-Reitz / Beckmann
+// (distribution.cuh:58-342), 2 Fresnel (fresnel.cuh:58-107), 3 warps
+// (utils.cuh:377-404,470-486,487-539).
+template <class T> void routine(int kind, const float* p, float* q) {
+    if (kind <= 1) {
+        Micro<T> m;
+        m.ax = std::max((T)p[0] * (T)p[0], (T)1e-3f);
+        m.ay = std::max((T)p[1] * (T)p[1], (T)1e-3f);
+        m.dist = (uint32_t)kind;
+        const V<T> wo = v3f<T>(p + 2), wh = v3f<T>(p + 5);
+        const V<T> s = m.sample_wh(wo, (T)p[8], (T)p[9]);
+        const T r[12] = {m.D(wh), m.G(wo, wh), m.pdf(wo, wh), s.x, s.y, s.z, T(0), m.ax, T(0), T(0), T(0), T(0)};
+        for (int k = 0; k < 12; ++k) q[k] = (float)r[k];
+    } else if (kind == 2) {
+        q[0] = (float)fr_diel<T>((T)p[0], (T)p[1], (T)p[2]);
+        const V<T> c = fr_cond<T>((T)p[0], v3f<T>(p + 3), v3f<T>(p + 6));
+        q[1] = (float)c.x;
+        q[2] = (float)c.y;
+        q[3] = (float)c.z;
+    } else {
+        const T ux = (T)p[0], uy = (T)p[1];
+        T dx, dy;
+        conc_disk<T>(ux, uy, dx, dy);
+        const V<T> c = cos_hemi<T>(ux, uy);
+        const T hz = ux, hr = std::sqrt(std::max(T(0), T(1) - hz * hz)), hp = T(2) * K<T>::pi * uy;
+        const V<T> hh = mk(hr * std::cos(hp), hr * std::sin(hp), hz);
+        const T ph = ux * T(2) * K<T>::pi, th = uy * K<T>::pi;
+        const T ct = std::cos(th), st = std::sin(th);
+        const V<T> d = nrm(mk(st * std::cos(ph), ct, st * std::sin(ph)));
+        const T ph2 = (ux * ux) / (ux * ux + uy * uy);
+        const T r[16] = {dx, dy, c.x, c.y, c.z, hh.x, hh.y, hh.z, d.x, d.y, d.z, st, ph2,
+                         erf_as<T>((T)p[2]), erfinv_g<T>((T)p[2]), T(0)};
+        for (int k = 0; k < 16; ++k) q[k] = (float)r[k];
+    }
+}
+OR_API void oracle_routines(int kind, const float* in, float* out, size_t n, int fp64) {
+    const int ni = kind <= 1 ? 12 : (kind == 2 ? 9 : 3), no = kind <= 1 ? 12 : (kind == 2 ? 4 : 16);
+    for (size_t i = 0; i < n; ++i) {
+        if (fp64) routine<double>(kind, in + ni * i, out + no * i);
+        else routine<float>(kind, in + ni * i, out + no * i);
+    }
+}
+
 OR_API void oracle_eval_sky(void* h, const float* dirs, float* rgb, size_t n, int fp64) {
     const Scene& sc = ((Ctx*)h)->sc;
     for (size_t i = 0; i < n; ++i) {
@@ -2152,6 +2196,15 @@ OR_API void oracle_env_sample(void* h, const float* u, double* out, size_t n) {
 }
 
 OR_API uint32_t oracle_tea16(uint32_t a, uint32_t b) { return tea16(a, b); }
+// CudaRNG(id, frame) (rng.cuh:37-76) for (id, frame) pairs: the seed word and
+// `draws` floats each
+OR_API void oracle_rng(const uint32_t* pairs, size_t n, int draws, uint32_t* seed, float* out) {
+    for (size_t i = 0; i < n; ++i) {
+        Rng r{tea16(pairs[2 * i], pairs[2 * i + 1])};
+        seed[i] = r.s;
+        for (int k = 0; k < draws; ++k) out[i * draws + k] = r.next();
+    }
+}
 
 // FP64 reference of the library's adjoint (noor_adjoint_forward/backward):
 // img = per-pixel mean of clamp(L, 0, 100) over frames [f0, f0 + spp);

@@ -16,13 +16,22 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 ORACLE_SO = HERE / "_build" / "liboracle.so"
 REF_SO = HERE / "_ref" / "libnoor_ref.so"
+REFDEV_SO = HERE / "_ref" / "libnoor_refdev.so"
+
+
+def reference_tree() -> Path:
+    """the reference tree the recipe reads ($NOOR_REFERENCE, else the
+    recipe's default)"""
+    out = subprocess.run(["make", "-s", "-C", str(HERE), "ref-path"], check=True, capture_output=True, text=True)
+    return Path(out.stdout.strip())
 
 
 def build(ref: bool = True) -> None:
-    """make the oracle (and, when the reference tree is present, oracle/_ref)"""
+    """make the oracle and, when the reference tree is present, oracle/_ref
+    (the reference's host routines and its device routines)"""
     subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
-    if ref and Path("/root/reference/noor").exists():
-        subprocess.run(["make", "-s", "-C", str(HERE), "ref"], check=True)
+    if ref and (reference_tree() / "noor").exists():
+        subprocess.run(["make", "-s", "-C", str(HERE), "ref", "refdev"], check=True)
 
 
 _orc = None
@@ -50,6 +59,8 @@ def lib() -> C.CDLL:
         L.oracle_env_sample.argtypes = [vp, vp, vp, sz]
         L.oracle_adjoint.argtypes = [vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, vp, vp, vp, vp, C.c_int, C.c_int,
                                      vp, vp, vp, vp]
+        L.oracle_routines.argtypes = [C.c_int, vp, vp, sz, C.c_int]
+        L.oracle_rng.argtypes = [vp, sz, C.c_int, vp, vp]
         L.oracle_tea16.restype = C.c_uint32
         L.oracle_tea16.argtypes = [C.c_uint32, C.c_uint32]
         _orc = L
@@ -164,6 +175,25 @@ class Oracle:
         out = np.zeros(u.shape[0] * 4)
         lib().oracle_env_sample(self.h, _p(np.ascontiguousarray(u, np.float32)), _p(out), u.shape[0])
         return out.reshape(-1, 4)
+
+
+def rng(pairs: np.ndarray, draws: int):
+    """CudaRNG(id, frame) of (n, 2) uint32 pairs: seed words and `draws`
+    floats each"""
+    p = np.ascontiguousarray(pairs, np.uint32)
+    seed = np.zeros(p.shape[0], np.uint32)
+    out = np.zeros((p.shape[0], draws), np.float32)
+    lib().oracle_rng(_p(p), p.shape[0], draws, _p(seed), _p(out))
+    return seed, out
+
+
+def routines(kind: int, rec: np.ndarray, fp64: bool = False) -> np.ndarray:
+    """the stand-alone shading routines in noor_eval_routines' record
+    layouts: 0 / 1 Trowbridge-Reitz / Beckmann, 2 Fresnel, 3 warps"""
+    r = np.ascontiguousarray(rec, np.float32)
+    out = np.zeros((r.shape[0], 12 if kind <= 1 else (4 if kind == 2 else 16)), np.float32)
+    lib().oracle_routines(kind, _p(r), _p(out), r.shape[0], int(fp64))
+    return out
 
 
 def ref_build_bvh(desc, num_triangles: int):

@@ -150,6 +150,14 @@ inline mat4 inverse(const mat4& m) {
     (void)inv;
     return o;
 }
+// column c of a*b is a times column c of b (the oracle harness compiles the
+// CudaCamera constructor, noor/cuda/camera.cuh:66-94, but fills cameras
+// field by field)
+inline mat4 operator*(const mat4& a, const mat4& b) {
+    mat4 o;
+    for (int c = 0; c < 4; ++c) o[c] = a * b[c];
+    return o;
+}
 inline vec4 row(const mat4& m, int i) { return vec4(m[0][i], m[1][i], m[2][i], m[3][i]); }
 inline vec3 row(const mat3& m, int i) { return vec3(m[0][i], m[1][i], m[2][i]); }
 }  // namespace glm

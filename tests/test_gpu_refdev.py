@@ -1,0 +1,186 @@
+"""The product's CUDA routines against the reference's own device routines.
+
+Fixture tests hold the library to tests/golden/refdev_*.npz (frozen from
+noor/cuda/*.cuh compiled unmodified, oracle/refdev/, by
+tests/golden/make_refdev_golden.py); they need no reference tree.  Where the
+reference library itself (oracle/_ref/libnoor_refdev.so) is present, the
+closest-hit parity is also checked live at the sky-lit configuration's full
+size (2,621,440 triangles, 1920x1080 camera rays plus a million secondary
+rays), against the reference's traversal and against the CPU oracle.
+"""
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from noor_b200 import _capi, scenes
+from oracle import reference_device as rd
+from oracle.oracle import Oracle
+
+import refdev_probe as probe
+from gpu_util import THREADS, camera_rays, dev, dev_empty, host, trace_any, trace_closest
+
+pytestmark = pytest.mark.gpu
+GOLD = Path(__file__).resolve().parent / "golden"
+
+
+def load(name):
+    return np.load(GOLD / f"refdev_{name}.npz")
+
+
+def routine(kind, rec):
+    no = 12 if kind <= 1 else (4 if kind == 2 else 16)
+    d_in = dev(np.ascontiguousarray(rec, np.float32))
+    d_out = dev_empty(rec.shape[0] * no * 4)
+    _capi.call("noor_eval_routines", kind, C.c_void_p(d_in.data_ptr()), C.c_void_p(d_out.data_ptr()), rec.shape[0])
+    return host(d_out, np.float32, (rec.shape[0], no))
+
+
+@pytest.mark.parametrize("kind,key", [(0, "ggx"), (1, "beckmann")])
+def test_microfacet(kind, key):
+    z = load("micro")
+    probe.check_microfacet(z[key], routine(kind, z["rec"]), exact=False)
+
+
+def test_fresnel():
+    z = load("fresnel")
+    probe.check_fresnel(z["out"], routine(2, z["rec"]))
+
+
+def test_warps():
+    z = load("warps")
+    probe.check_warps(z["out"], routine(3, z["rec"]), tol=1e-5)
+
+
+@pytest.mark.parametrize("kind", [0, 1, 2])
+def test_bsdf(kind):
+    z = load("bsdf")
+    rec, ref = z[f"rec{kind}"], z[f"out{kind}"]
+    r = scenes.Renderer(probe.probe_scene())
+    try:
+        pr = probe.product_records(rec, ref if kind == 2 else None)
+        d_in = dev(pr)
+        d_out = dev_empty(pr.shape[0] * 32)
+        _capi.call("noor_eval_bsdf", kind, C.c_void_p(d_in.data_ptr()), C.c_void_p(d_out.data_ptr()), pr.shape[0])
+        got = host(d_out, np.float32, (pr.shape[0], 8))
+    finally:
+        r.close()
+    probe.check_bsdf(kind, rec, ref, got)
+
+
+def test_sky():
+    """Hosek radiance within 1e-5 relative at the 99.9th percentile, 5e-5 at
+    most (sun-disc edge and sRGB knee)"""
+    z = load("sky")
+    hosek = _capi.HosekSky.from_buffer_copy(z["hosek"].tobytes())
+    r = scenes.Renderer(probe.trace_scenes()["field16"], hosek=hosek)
+    try:
+        d = dev(z["dirs"])
+        o = dev_empty(z["dirs"].shape[0] * 12)
+        _capi.call("noor_eval_sky", C.c_void_p(d.data_ptr()), C.c_void_p(o.data_ptr()), z["dirs"].shape[0])
+        got = host(o, np.float32, (-1, 3))
+    finally:
+        r.close()
+    e = probe.rel_err(got, z["rgb"]).max(1)
+    assert np.quantile(e, 0.999) < 1e-5 and e.max() < 5e-5, (np.quantile(e, 0.999), e.max())
+
+
+@pytest.mark.parametrize("name", ["room", "field16"])
+def test_closest_any_hit_and_camera(name):
+    z = load("trace")
+    r = scenes.Renderer(probe.trace_scenes()[name], intersector=_capi.NOOR_ISECT_REF_WALD)
+    try:
+        rays = z[f"{name}_rays"]
+        probe.check_trace(z[f"{name}_hits"], z[f"{name}_any"], trace_closest(rays), trace_any(rays))
+        n = r.w * r.h
+        probe.check_camera_rays(rays[:n], camera_rays(r, 1), tol=1e-6)
+    finally:
+        r.close()
+
+
+def test_room_render_megakernel_and_wavefront():
+    """C1 room with a sphere light node, MIS off, 8 frames: the megakernel
+    with the reference's running-mean film, and the wavefront integrator,
+    against path_tracer_kernel's film"""
+    z = load("render")
+    s = probe.trace_scenes()["room"]
+    r = scenes.Renderer(s, intersector=_capi.NOOR_ISECT_REF_WALD, film_mode=_capi.NOOR_FILM_REF_LERP)
+    try:
+        r.render(8)
+        probe.check_film(z["room_film"], r.framebuffer())
+        import torch
+        film = torch.zeros(r.w * r.h * 4, dtype=torch.float32, device="cuda")
+        f = scenes.wf_frame(0, s.camera, 8, bounces=s.render["bounces"], first_frame=1, d_film=film.data_ptr())
+        _capi.call("noor_wavefront_render", C.byref(f), 1, C.byref(scenes.wf_params(block=128, capacity=1 << 16)))
+        torch.cuda.synchronize()
+        probe.check_film(z["room_film"], film.cpu().numpy().reshape(r.h, r.w, 4))
+    finally:
+        r.close()
+
+
+# ------------------------------------------------------------ live, C2 size
+live = pytest.mark.skipif(not rd.available(), reason="reference device library not built here")
+
+
+@pytest.fixture(scope="module")
+def c2():
+    s = scenes.sky_scene()
+    built = scenes.BuiltPayload(s, gpu=True)
+    yield s, built
+    built.free()
+
+
+def _secondary_rays(prim: np.ndarray, hits: np.ndarray, n: int, seed: int) -> np.ndarray:
+    """rays from the surface points the camera rays hit (nudged back along
+    the camera ray) in uniformly random directions, half of them bounded"""
+    rng = np.random.default_rng(seed)
+    h = np.where(hits[:, 6] == 1)[0]
+    pick = rng.choice(h, n)
+    t = hits[pick, 0].view(np.float32)
+    o = prim[pick, 0:3] + prim[pick, 4:7] * (t * np.float32(0.999))[:, None]
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    out = np.zeros((n, 8), np.float32)
+    out[:, 0:3], out[:, 3], out[:, 4:7] = o, np.inf, d
+    out[n // 2:, 3] = rng.uniform(0.5, 20.0, n - n // 2)
+    return out
+
+
+@live
+def test_c2_closest_hit_bit_exact_against_the_reference(c2):
+    """the sky-lit configuration's 2,621,440-triangle two-level BVH: every
+    camera ray of a 1920x1080 frame plus 1M secondary rays; Wald mode gives
+    the reference's triangle, instance, t and barycentric bits for every ray
+    and its any-hit answers; the watertight test names the same triangle for
+    at least 99.9 % of the hits"""
+    s, built = c2
+    spec = built.default_spec(8, 1)
+    spec.intersector = _capi.NOOR_ISECT_REF_WALD
+    cam = scenes.make_camera(s.camera)
+    hosek = scenes.make_hosek(s.hosek)
+    ref = rd.RefDevice(built.payload, hosek, cam, spec)
+    try:
+        prim = ref.camera_rays(1)
+        ph = ref.trace_closest(prim)
+        rays = np.concatenate([prim, _secondary_rays(prim, ph, 1_000_000, 3)])
+        ref_hits, ref_any = ref.trace_closest(rays), ref.trace_any(rays)
+    finally:
+        ref.close()
+    r = scenes.Renderer(s, built=built, intersector=_capi.NOOR_ISECT_REF_WALD)
+    try:
+        probe.check_trace(ref_hits, ref_any, trace_closest(rays), trace_any(rays))
+        probe.check_camera_rays(prim, camera_rays(r, 1), tol=1e-6)
+        r.update_spec(intersector=_capi.NOOR_ISECT_WATERTIGHT)
+        wt = trace_closest(rays)
+        hit = ref_hits[:, 6] == 1
+        same = (wt[:, 6] == ref_hits[:, 6]) & (~hit | ((wt[:, 1] == ref_hits[:, 1]) & (wt[:, 2] == ref_hits[:, 2])))
+        assert same.mean() >= 0.999, same.mean()
+    finally:
+        r.close()
+    # the CPU oracle on a 200k subset of the same rays
+    orc = Oracle(built.payload, spec, hosek)
+    sub = np.random.default_rng(4).choice(rays.shape[0], 200_000, replace=False)
+    probe.check_trace(ref_hits[sub], ref_any[sub], orc.trace_closest(rays[sub], 1, THREADS),
+                      orc.trace_any(rays[sub], 1))
+    orc.close()
