@@ -111,6 +111,20 @@ enum { NOOR_ISECT_WATERTIGHT = 0, NOOR_ISECT_REF_WALD = 1 };
 enum { NOOR_FILM_KAHAN = 0, NOOR_FILM_REF_LERP = 1 };
 /* microfacet distribution selector for METAL materials (build addition) */
 enum { NOOR_DIST_TROWBRIDGE_REITZ = 0, NOOR_DIST_BECKMANN = 1 };
+/* environment sampling selector (build addition).
+ * NOOR_ENV_FP64: the build's distribution, one cell per map texel (2048 x
+ *   1024 cells of 4x4-supersampled luminance x sin(theta) for the physical
+ *   sky) with FP64 prefix sums; map lookups by an FP32 bilinear filter.
+ * NOOR_ENV_REFERENCE: the reference's own CudaDistribution2D
+ *   (noor/cuda/distribution2d.cuh:63-337): a grid of
+ *   clamp(nearestPow2(texture size), 32, 1024) cells per axis, each the 3x3
+ *   mean of the texture's luminance read through the texture unit's bilinear
+ *   filter, FP32 Blelloch prefix sums, and its sampling routine; the physical
+ *   sky is first baked as sin(theta) x radiance into a 2048 x 2048 texture
+ *   (update_skydome, noor/cuda/skydome.cuh:27-37), and HDR / constant map
+ *   lookups go through the texture unit (tex2D, linear, clamp).  Maps must be
+ *   power-of-two sized.  Not available to the adjoint. */
+enum { NOOR_ENV_FP64 = 0, NOOR_ENV_REFERENCE = 1 };
 
 /* ---------------------------------------------------------- payload mirror */
 
@@ -298,6 +312,7 @@ typedef struct noor_spec {
     uint32_t mis;
     uint32_t intersector;       /* NOOR_ISECT_*                              */
     uint32_t film_mode;         /* NOOR_FILM_*                               */
+    uint32_t env_sampling;      /* NOOR_ENV_*                                */
 } noor_spec;
 
 /* ------------------------------------------------- reference entry points */
@@ -439,6 +454,12 @@ int noor_eval_env_sample(const float* d_u, float* d_out, size_t n);
 int noor_get_env_distribution(int* w, int* h, float* func, float* cdf,
                               float* marginal_func, float* marginal_cdf,
                               double* marginal_integral);
+/* the NOOR_ENV_REFERENCE tables (built on first use of that mode) as the
+ * reference lays them out (noor/cuda/distribution2d.cuh:166-220): func and
+ * cdf hold h*(w+2)+1 floats each, row r at r*(w+1) (w values, then the
+ * row's integral), the marginal at h*(w+1) (h values, then its integral).
+ * Pass NULL arrays to query w, h. */
+int noor_get_reference_distribution(int* w, int* h, float* func, float* cdf);
 
 /* -------------------------------------------------- host scene builder */
 /* BVHSpec, noor/header/spec.h:27-51 */

@@ -40,6 +40,7 @@ NOOR_SKY_HDR, NOOR_SKY_PHYSICAL, NOOR_SKY_CONSTANT = 0, 1, 2
 NOOR_LIGHT_SKY_MASK = 0x20
 NOOR_ISECT_WATERTIGHT, NOOR_ISECT_REF_WALD = 0, 1
 NOOR_FILM_KAHAN, NOOR_FILM_REF_LERP = 0, 1
+NOOR_ENV_FP64, NOOR_ENV_REFERENCE = 0, 1
 NOOR_SHAPE_QUAD, NOOR_SHAPE_SPHERE, NOOR_SHAPE_DISK = 0, 1, 2
 NOOR_CAMERA_PERSP, NOOR_CAMERA_ORTHO, NOOR_CAMERA_ENV = 0, 1, 2
 NOOR_TONEMAP_NONE, NOOR_TONEMAP_GAMMA, NOOR_TONEMAP_REINHARD, NOOR_TONEMAP_FILMIC, NOOR_TONEMAP_UNCHARTED2 = -1, 0, 1, 2, 3
@@ -123,7 +124,7 @@ class Spec(C.Structure):
     _fields_ = [("reflection_bias", f32), ("shadow_bias", f32), ("world_radius", f32), ("wr2", f32),
                 ("bvh_root_node", u32), ("lighting_type", u32), ("bounces", u32), ("rr", u32), ("bvh_height", u32),
                 ("num_gpus", u32), ("skydome_type", i32), ("debug_sky", u32), ("mis", u32), ("intersector", u32),
-                ("film_mode", u32)]
+                ("film_mode", u32), ("env_sampling", u32)]
 
 
 class Ray(C.Structure):
@@ -223,6 +224,7 @@ PROTOTYPES = {
     "noor_eval_routines": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_size_t]),
     "noor_eval_sky": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t]),
     "noor_eval_env_sample": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t]),
+    "noor_get_reference_distribution": (C.c_int, [C.POINTER(C.c_int), C.POINTER(C.c_int), pf, pf]),
     "noor_get_env_distribution": (C.c_int, [C.POINTER(C.c_int), C.POINTER(C.c_int), pf, pf, pf, pf,
                                             C.POINTER(C.c_double)]),
     "noor_build_payload": (C.c_int, [C.POINTER(SceneDesc), C.POINTER(C.c_void_p), C.POINTER(BuildStat)]),

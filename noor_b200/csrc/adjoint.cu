@@ -513,6 +513,8 @@ static int adjoint_run(const noor_adjoint_desc* desc, int mode, float* image, co
         return set_error(NOOR_ERR_UNSUPPORTED, "adjoint: cameras other than the pinhole");
     if (!st.quad_lights_only || S.num_delta_lights > 0)
         return set_error(NOOR_ERR_UNSUPPORTED, "adjoint: lights other than quad area lights and the sky");
+    if (st.dev.env_ref)
+        return set_error(NOOR_ERR_UNSUPPORTED, "adjoint: the reference's environment sampling (NOOR_ENV_REFERENCE)");
     if (S.sky_type == NOOR_SKY_HDR && (!desc->d_env || (mode == 1 && !g_env)))
         return set_error(NOOR_ERR_INVALID, "adjoint: env buffer missing");
     if (desc->width != C->cam.w || desc->height != C->cam.h)

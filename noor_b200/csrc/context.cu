@@ -34,6 +34,8 @@ int cuda_fail(cudaError_t e, const char* what) {
 }
 
 SceneState::~SceneState() {
+    if (env_tex) cudaDestroyTextureObject(env_tex);
+    if (env_array) cudaFreeArray(env_array);
     for (void* p : allocs) cudaFree(p);
 }
 
@@ -213,6 +215,86 @@ int build_distribution(Context& C, SceneState& st) {
     return NOOR_OK;
 }
 
+// nearestPow2 (noor/cuda/utils.cuh:106-135): the nearer of the powers of two
+// around n, the lower one on a tie
+static int nearest_pow2(int n) {
+    int next = n - 1;
+    next |= next >> 1;
+    next |= next >> 2;
+    next |= next >> 4;
+    next |= next >> 8;
+    next |= next >> 16;
+    next++;
+    const int prev = (int)powf(2.0f, (float)(int)log2f((float)n));
+    return fabsf((float)(n - next)) < fabsf((float)(n - prev)) ? next : prev;
+}
+
+// NOOR_ENV_REFERENCE tables (distribution2d.cuh:166-228), from the map or,
+// for the physical sky, from a 2048 x 2048 bake of sin(theta) x radiance
+// (skydome.cuh:27-37, the texture model.cpp:318 makes for it); rebuilt when
+// the sky changes.
+int build_reference_distribution(Context& C, SceneState& st) {
+    DevScene& D = st.dev;
+    const bool sky = st.sky_type == NOOR_SKY_PHYSICAL;
+    const int tw = sky ? 2048 : D.env_w, th = sky ? 2048 : D.env_h;
+    if ((tw & (tw - 1)) || (th & (th - 1)))
+        return set_error(NOOR_ERR_UNSUPPORTED, "reference env sampling: the map must be power-of-two sized");
+    const int w = std::min(std::max(nearest_pow2(tw), 32), 1024), h = std::min(std::max(nearest_pow2(th), 32), 1024);
+    const size_t n = (size_t)h * (w + 2) + 1;
+    cudaError_t e = cudaSuccess;
+    int rc;
+    if (!st.ref_built) {
+        // two floats of padding past the reference's table size: its
+        // searches never select them for u < 1, and they read as zero
+        if ((rc = st.alloc((void**)&st.ref_func, (n + 2) * 4, "reference env func"))) return rc;
+        if ((rc = st.alloc((void**)&st.ref_cdf, (n + 2) * 4, "reference env cdf"))) return rc;
+        if (sky && (rc = st.alloc((void**)&st.ref_bake, (size_t)tw * th * 16, "sky bake"))) return rc;
+        const cudaChannelFormatDesc fd = cudaCreateChannelDesc<float4>();
+        e = cudaMallocArray(&st.env_array, &fd, tw, th);
+        if (e != cudaSuccess) return cuda_fail(e, "environment array");
+        cudaResourceDesc rd{};
+        rd.resType = cudaResourceTypeArray;
+        rd.res.array.array = st.env_array;
+        cudaTextureDesc td{};
+        td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = cudaAddressModeClamp;
+        // the constant sky is a point-filtered 1x1 texture (texture.h:148-158)
+        td.filterMode = st.sky_type == NOOR_SKY_CONSTANT ? cudaFilterModePoint : cudaFilterModeLinear;
+        td.readMode = cudaReadModeElementType;
+        td.normalizedCoords = 1;
+        e = cudaCreateTextureObject(&st.env_tex, &rd, &td, nullptr);
+        if (e != cudaSuccess) return cuda_fail(e, "environment texture");
+    }
+    const float4* src = D.env;
+    if (sky) {
+        if ((e = launch_ref_sky_bake(D.hosek, tw, th, st.ref_bake, C.stream)) != cudaSuccess) return cuda_fail(e, "sky bake");
+        src = st.ref_bake;
+        C.launches++;
+    }
+    e = cudaMemcpy2DToArrayAsync(st.env_array, 0, 0, src, (size_t)tw * 16, (size_t)tw * 16, th, cudaMemcpyDeviceToDevice,
+                                 C.stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(st.ref_func, 0, (n + 2) * 4, C.stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(st.ref_cdf, 0, (n + 2) * 4, C.stream);
+    if (e == cudaSuccess) e = launch_ref_distribution(st.env_tex, w, h, st.ref_func, st.ref_cdf, C.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(C.stream);
+    if (e != cudaSuccess) return cuda_fail(e, "reference env distribution");
+    C.launches += 5;
+    st.ref_built = true;
+    D.env_tex = st.env_tex;
+    D.rfunc = st.ref_func;
+    D.rcdf = st.ref_cdf;
+    D.rw = w;
+    D.rh = h;
+    return NOOR_OK;
+}
+
+// the spec's environment sampling mode, building the reference tables on
+// first use
+static int apply_env_mode(Context& C, SceneState& st, const noor_spec& s) {
+    st.dev.env_ref = s.env_sampling == NOOR_ENV_REFERENCE ? 1u : 0u;
+    if (st.dev.env_ref && !st.ref_built) return build_reference_distribution(C, st);
+    return NOOR_OK;
+}
+
 // every host-side check of a scene, made before any device work
 static int check_scene_inputs(const noor_payload* P, const noor_hosek_sky* H, const noor_spec* S) {
     int rc = validate_payload(P);
@@ -220,7 +302,8 @@ static int check_scene_inputs(const noor_payload* P, const noor_hosek_sky* H, co
     if (!S) return set_error(NOOR_ERR_INVALID, "spec is null");
     if (S->skydome_type < 0 || S->skydome_type > 2) return set_error(NOOR_ERR_INVALID, "spec: bad skydome type");
     if (S->skydome_type == NOOR_SKY_PHYSICAL && !H) return set_error(NOOR_ERR_INVALID, "physical sky without Hosek state");
-    if (S->intersector > 1u || S->film_mode > 1u) return set_error(NOOR_ERR_INVALID, "spec: bad selector");
+    if (S->intersector > 1u || S->film_mode > 1u || S->env_sampling > 1u)
+        return set_error(NOOR_ERR_INVALID, "spec: bad selector");
     if (S->bvh_root_node >= P->num_bvh_nodes) return set_error(NOOR_ERR_INVALID, "spec: BVH root out of range");
     return NOOR_OK;
 }
@@ -379,7 +462,8 @@ int upload_scene(Context& C, const noor_payload* P, const noor_hosek_sky* H, con
     D.dist.marg_cdf = b.marg_cdf;
     D.dist.w = b.w;
     D.dist.h = b.h;
-    return build_distribution(C, st);
+    if ((rc = build_distribution(C, st))) return rc;
+    return apply_env_mode(C, st, *S);
 }
 
 static void load_camera(Context& C, const noor_camera& cam) { C.cam = dev_camera(cam, cam.w, cam.h); }
@@ -580,6 +664,7 @@ extern "C" int update_cuda_hosek(void) {
     SceneState& st = *C->scenes[0];
     apply_hosek(st, *C->hosek_src);
     if (st.sky_type == NOOR_SKY_PHYSICAL && (rc = build_distribution(*C, st))) return rc;
+    if (st.sky_type == NOOR_SKY_PHYSICAL && st.ref_built && (rc = build_reference_distribution(*C, st))) return rc;
     C->film_count = 0;
     return NOOR_OK;
 }
@@ -590,11 +675,13 @@ extern "C" int update_cuda_spec(void) {
     if (rc) return rc;
     const noor_spec* s = C->spec_src;
     SceneState& st = *C->scenes[0];
-    if (s->intersector > 1u || s->film_mode > 1u) return set_error(NOOR_ERR_INVALID, "spec: bad selector");
+    if (s->intersector > 1u || s->film_mode > 1u || s->env_sampling > 1u)
+        return set_error(NOOR_ERR_INVALID, "spec: bad selector");
     if (s->bvh_root_node >= st.dev.num_nodes) return set_error(NOOR_ERR_INVALID, "spec: BVH root out of range");
     if (s->skydome_type != st.sky_type)
         return set_error(NOOR_ERR_UNSUPPORTED, "spec: the skydome type is fixed at load time");
     apply_spec(st, *s);
+    if ((rc = apply_env_mode(*C, st, *s))) return rc;
     C->film_count = 0;
     return NOOR_OK;
 }
@@ -889,6 +976,22 @@ extern "C" int noor_get_env_distribution(int* w, int* h, float* func, float* cdf
     if (marginal_cdf && e == cudaSuccess) e = cudaMemcpy(marginal_cdf, b.marg_cdf, (H + 1) * 4, cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return cuda_fail(e, "env distribution");
     if (marginal_integral) *marginal_integral = C->scenes[0]->dev.dist.marg_int;
+    return NOOR_OK;
+}
+
+extern "C" int noor_get_reference_distribution(int* w, int* h, float* func, float* cdf) {
+    Context* C;
+    int rc = need_ctx(C);
+    if (rc) return rc;
+    SceneState& st = *C->scenes[0];
+    if (!st.ref_built && (rc = build_reference_distribution(*C, st))) return rc;
+    if (w) *w = st.dev.rw;
+    if (h) *h = st.dev.rh;
+    const size_t n = (size_t)st.dev.rh * (st.dev.rw + 2) + 1;
+    cudaError_t e = cudaSuccess;
+    if (func) e = cudaMemcpy(func, st.ref_func, n * 4, cudaMemcpyDeviceToHost);
+    if (cdf && e == cudaSuccess) e = cudaMemcpy(cdf, st.ref_cdf, n * 4, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(e, "reference distribution");
     return NOOR_OK;
 }
 

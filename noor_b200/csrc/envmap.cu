@@ -181,4 +181,110 @@ cudaError_t launch_hosek_fit(const float* dataset, double turbidity, const doubl
     return cudaGetLastError();
 }
 
+// ------------------------------------------------ reference distribution
+// NOOR_ENV_REFERENCE: the reference's CudaDistribution2D built as it builds
+// it (noor/cuda/distribution2d.cuh:63-228), so that sampling maps the same
+// uniforms to the same directions.  Its luminance, sums and divisions round
+// each operation on its own (the arithmetic of the reference built for the
+// host); the texture reads are the texture unit's bilinear filter, as there.
+
+// update_skydome (noor/cuda/skydome.cuh:27-37): texel (x, y) of a w x h
+// texture holds sin(theta) x sky radiance at u = (x / w, y / h)
+__global__ void k_ref_sky_bake(DevHosek H, int w, int h, float4* out) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= w || y >= h) return;
+    float st;
+    const float3 dir = spherical_direction(xdiv((float)x, (float)w), xdiv((float)y, (float)h), st);
+    const float3 c = hosek_query(H, dir);
+    out[(size_t)y * w + x] = make_float4(xmul(st, c.x), xmul(st, c.y), xmul(st, c.z), st);
+}
+
+// update_func (distribution2d.cuh:63-83): cell (row, col) of the w x h grid
+// = mean luminance of the 3x3 texture reads at ((col + i) / w, (row + j) / h),
+// i, j in {-1, 0, 1}; one block per row, one thread per column
+__global__ void k_ref_func(cudaTextureObject_t tex, int w, int h, float* func) {
+    const int row = blockIdx.y, col = threadIdx.x;
+    float acc = 0.0f;
+    for (int j = -1; j <= 1; ++j)
+        for (int i = -1; i <= 1; ++i) {
+            const float4 t = tex2D<float4>(tex, xdiv((float)(i + col), (float)w), xdiv((float)(j + row), (float)h));
+            acc = xadd(acc, xdot3(t.x, t.y, t.z, 0.2126f, 0.7152f, 0.0722f));
+        }
+    func[(size_t)row * (w + 1) + col] = xdiv(acc, 9.0f);
+}
+
+// prescan (distribution2d.cuh:86-135): exclusive work-efficient (up-sweep /
+// down-sweep) scan of func[row][0..n) / n into cdf[row][0..n), then
+// cdf[row][n] = func[row][n] = the row's integral; rows are n + 1 apart,
+// one block of n / 2 threads per row, n a power of two.  The reference's
+// bank-conflict offset evaluates to 0 for every index it meets.
+__global__ void k_ref_scan(float* func, float* cdf, int n) {
+    extern __shared__ float tmp[];
+    const int tid = threadIdx.x;
+    const size_t base = (size_t)blockIdx.y * (n + 1);
+    const int ai = tid, bi = tid + n / 2;
+    tmp[ai] = xdiv(func[base + ai], (float)n);
+    tmp[bi] = xdiv(func[base + bi], (float)n);
+    int offset = 1;
+    for (int d = n >> 1; d > 0; d >>= 1) {
+        __syncthreads();
+        if (tid < d) {
+            const int a = offset * (2 * tid + 1) - 1, b = offset * (2 * tid + 2) - 1;
+            tmp[b] = xadd(tmp[b], tmp[a]);
+        }
+        offset *= 2;
+    }
+    if (tid == 0) tmp[n - 1] = 0.0f;
+    for (int d = 1; d < n; d *= 2) {
+        offset >>= 1;
+        __syncthreads();
+        if (tid < d) {
+            const int a = offset * (2 * tid + 1) - 1, b = offset * (2 * tid + 2) - 1;
+            const float t = tmp[a];
+            tmp[a] = tmp[b];
+            tmp[b] = xadd(tmp[b], t);
+        }
+    }
+    __syncthreads();
+    cdf[base + ai] = tmp[ai];
+    cdf[base + bi] = tmp[bi];
+    __syncthreads();
+    if (tid == 0) {
+        const float fi = xadd(cdf[base + n - 1], xdiv(func[base + n - 1], (float)n));
+        cdf[base + n] = fi;
+        func[base + n] = fi;
+    }
+}
+
+// process_cdf (distribution2d.cuh:137-160): normalise each row's CDF by its
+// integral (a uniform CDF for a zero row); with h > 1 the integrals become
+// the marginal's func at h * (w + 1)
+__global__ void k_ref_normalize(float* func, float* cdf, int w, int h) {
+    __shared__ float fi;
+    const int row = blockIdx.y, col = threadIdx.x;
+    const size_t base = (size_t)row * (w + 1);
+    if (col == 0) fi = cdf[base + w];
+    __syncthreads();
+    cdf[base + col + 1] = fi == 0.0f ? xdiv((float)(col + 1), (float)w) : xdiv(cdf[base + col + 1], fi);
+    if (col == 0 && h > 1) func[(size_t)h * (w + 1) + row] = fi;
+}
+
+cudaError_t launch_ref_sky_bake(const DevHosek& H, int w, int h, float4* out, cudaStream_t s) {
+    const dim3 block(32, 8), grid((w + 31) / 32, (h + 7) / 8);
+    k_ref_sky_bake<<<grid, block, 0, s>>>(H, w, h, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ref_distribution(cudaTextureObject_t tex, int w, int h, float* func, float* cdf, cudaStream_t s) {
+    k_ref_func<<<dim3(1, h), w, 0, s>>>(tex, w, h, func);
+    k_ref_scan<<<dim3(1, h), w / 2, (w + 1) * sizeof(float), s>>>(func, cdf, w);
+    k_ref_normalize<<<dim3(1, h), w, 0, s>>>(func, cdf, w, h);
+    float* mf = func + (size_t)h * (w + 1);
+    float* mc = cdf + (size_t)h * (w + 1);
+    k_ref_scan<<<dim3(1, 1), h / 2, (h + 1) * sizeof(float), s>>>(mf, mc, h);
+    k_ref_normalize<<<dim3(1, 1), h, 0, s>>>(mf, mc, h, 1);
+    return cudaGetLastError();
+}
+
 }  // namespace nb

@@ -272,11 +272,11 @@ __global__ void k_env_sample(DevScene S, const float* u, float* out, size_t n) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float pdf;
-    const float2 xy = dist_sample(S.dist, u[2 * i], u[2 * i + 1], pdf);
+    const float2 xy = S.env_ref ? rdist_sample(S, u[2 * i], u[2 * i + 1], pdf) : dist_sample(S.dist, u[2 * i], u[2 * i + 1], pdf);
     out[4 * i] = xy.x;
     out[4 * i + 1] = xy.y;
     out[4 * i + 2] = pdf;
-    out[4 * i + 3] = dist_pdf(S.dist, xy.x, xy.y);
+    out[4 * i + 3] = S.env_ref ? rdist_pdf(S, xy.x, xy.y) : dist_pdf(S.dist, xy.x, xy.y);
 }
 
 // debug_skydome_kernel (noor/cuda/path_tracer.cu:102-122)

@@ -52,6 +52,12 @@ cudaError_t launch_env_func_from_texture(const float4* env, int w, int h, float*
 cudaError_t launch_env_func_from_sky(const DevHosek& H, int w, int h, float* func, cudaStream_t s);
 // FP64 row/marginal prefix sums -> normalised FP32 CDFs
 cudaError_t launch_env_cdf(const EnvBuild& b, cudaStream_t s);
+// NOOR_ENV_REFERENCE: the physical sky baked as sin(theta) x radiance into a
+// w x h texture, and the reference's distribution tables (h * (w + 2) + 1
+// floats each) from a texture read with its bilinear filter; w, h powers of
+// two in [32, 1024]
+cudaError_t launch_ref_sky_bake(const DevHosek& H, int w, int h, float4* out, cudaStream_t s);
+cudaError_t launch_ref_distribution(cudaTextureObject_t tex, int w, int h, float* func, float* cdf, cudaStream_t s);
 // Hosek-Wilkie RGB fit in FP64: dataset = 3 x 1080 coefficients then 3 x 120
 // radiances; writes 3 states x (27 configs + 3 radiances) into out (90 floats
 // per state, state-major, configs first).

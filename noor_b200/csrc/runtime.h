@@ -17,6 +17,14 @@ struct SceneState {
     bool quad_lights_only = true;   // every area light a quad
     int sky_type = 0;
     uint32_t max_mesh_leaf = 0;
+    // NOOR_ENV_REFERENCE, built on first use: the environment (or baked sky)
+    // as a CUDA array + texture object, the bake buffer and the tables
+    cudaArray_t env_array = nullptr;
+    cudaTextureObject_t env_tex = 0;
+    float4* ref_bake = nullptr;
+    float* ref_func = nullptr;
+    float* ref_cdf = nullptr;
+    bool ref_built = false;
     ~SceneState();
     int alloc(void** p, size_t bytes, const char* what);
     int upload(void** p, const void* host, size_t bytes, const char* what);

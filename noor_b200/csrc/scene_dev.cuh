@@ -166,6 +166,14 @@ struct DevScene {
     int stack_cap;
     uint32_t ext_lobes;     // some material uses a lobe beyond Lambert, conductor, Fresnel specular
     uint32_t ext_lights;    // sphere or disk area lights, point, spot or distant lights
+    // NOOR_ENV_REFERENCE: the reference's distribution tables (row r at
+    // r * (rw + 1), the marginal at rh * (rw + 1)) and the environment as a
+    // texture object (linear filter, clamp, normalised coordinates)
+    uint32_t env_ref;
+    cudaTextureObject_t env_tex;
+    const float* rfunc;
+    const float* rcdf;
+    int rw, rh;
 };
 
 }  // namespace nb

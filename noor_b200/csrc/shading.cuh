@@ -1061,12 +1061,57 @@ NB_D float3 env_bilinear(const DevScene& S, float u, float v) {
     return w00 * f3(t00) + w10 * f3(t10) + w01 * f3(t01) + w11 * f3(t11);
 }
 
-// CudaSkyDomeManager::evaluate(dir) (noor/cuda/skydome.cuh:93-101)
+// CudaSkyDomeManager::evaluate(dir) (noor/cuda/skydome.cuh:93-101); with
+// NOOR_ENV_REFERENCE maps are read through the texture unit as there
 NB_D float3 env_eval(const DevScene& S, const float3& dir) {
     if (S.sky_type == NOOR_SKY_PHYSICAL) return hosek_query(S.hosek, dir);
     const float phi = spherical_phi(dir) * kInv2Pi;
     const float theta = spherical_theta(dir) * kInvPi;
+    if (S.env_ref) return f3(tex2D<float4>(S.env_tex, phi, theta));
     return env_bilinear(S, phi, theta);
+}
+
+// The reference's CudaDistribution2D sampling (noor/cuda/distribution2d.cuh:
+// 230-336) on its own tables, NOOR_ENV_REFERENCE.  As there, the marginal
+// search runs over h + 1 CDF entries and the conditional over w + 1 (the
+// row integral and the next row's first entry included) and the sample is
+// divided by that count; the entries past a CDF's end are never selected
+// for u < 1 (the last real entry is 1).
+NB_D float rdist_cdf(const DevScene& S, int row, int col) { return __ldg(&S.rcdf[(size_t)row * (S.rw + 1) + col]); }
+NB_D float rdist_func(const DevScene& S, int row, int col) { return __ldg(&S.rfunc[(size_t)row * (S.rw + 1) + col]); }
+NB_D float rdist_func_int(const DevScene& S, int row) { return rdist_func(S, row, row == S.rh ? S.rh : S.rw); }
+NB_D float rdist_sample1d(const DevScene& S, int row, int n, float u, float& pdf, int& off) {
+    int l = 0, r = n, interval = -1;
+    while (l <= r) {
+        const int m = l + (r - l) / 2;
+        if (rdist_cdf(S, row, m) <= u) {
+            l = m + 1;
+            interval = m;
+        } else {
+            r = m - 1;
+        }
+    }
+    off = min(max(interval, 0), n - 1);
+    const float func = rdist_func(S, row, off);
+    const float c0 = rdist_cdf(S, row, off), c1 = rdist_cdf(S, row, off + 1);
+    const float fi = rdist_func_int(S, row);
+    float du = u - c0;
+    if (c1 - c0 > 0.0f) du /= (c1 - c0);
+    pdf = fi > 0.0f ? func / fi : 0.0f;
+    return ((float)off + du) / (float)n;
+}
+NB_D float2 rdist_sample(const DevScene& S, float u0, float u1, float& pdf) {
+    float py, px;
+    int v, c;
+    const float y = rdist_sample1d(S, S.rh, S.rh + 1, u1, py, v);
+    const float x = rdist_sample1d(S, v, S.rw + 1, u0, px, c);
+    pdf = px * py;
+    return f2(x, y);
+}
+NB_D float rdist_pdf(const DevScene& S, float x, float y) {
+    const int iu = min(max((int)(x * S.rw), 0), S.rw - 1);
+    const int iv = min(max((int)(y * S.rh), 0), S.rh - 1);
+    return rdist_func(S, iv, iu) / rdist_func_int(S, S.rh);
 }
 
 // piecewise-constant 1D sampling over one CDF (PBRT-v3 Distribution1D)
@@ -1109,7 +1154,7 @@ NB_D float3 env_sample_dir(const DevScene& S, Rng& rng, float& pdf) {
     const float u0 = rng.next();
     const float u1 = rng.next();
     float mp;
-    const float2 uv = dist_sample(S.dist, u0, u1, mp);
+    const float2 uv = S.env_ref ? rdist_sample(S, u0, u1, mp) : dist_sample(S.dist, u0, u1, mp);
     float st;
     const float3 dir = spherical_direction(uv.x, uv.y, st);
     pdf = (st == 0.0f) ? 0.0f : mp / (2.0f * kPi * kPi * st);
@@ -1122,7 +1167,8 @@ NB_D float env_pdf(const DevScene& S, const float3& wi) {
     const float phi = spherical_phi(wi);
     const float st = sinf(theta);
     if (st == 0.0f) return 0.0f;
-    return dist_pdf(S.dist, phi * kInv2Pi, theta * kInvPi) / (2.0f * kPi * kPi * st);
+    const float x = phi * kInv2Pi, y = theta * kInvPi;
+    return (S.env_ref ? rdist_pdf(S, x, y) : dist_pdf(S.dist, x, y)) / (2.0f * kPi * kPi * st);
 }
 
 }  // namespace nb

@@ -2195,6 +2195,50 @@ OR_API void oracle_env_sample(void* h, const float* u, double* out, size_t n) {
     }
 }
 
+// The reference's CudaDistribution2D sampling (distribution2d.cuh:230-336)
+// on its own tables (func, cdf: h*(w+2)+1 floats, row r at r*(w+1), the
+// marginal at h*(w+1)): u (2 floats) -> {x, y, pdf of the sample, Pdf(x, y)}
+struct RefDist {
+    const float *func, *cdf;
+    int w, h;
+    float c(int row, int col) const { return cdf[(size_t)row * (w + 1) + col]; }
+    float f(int row, int col) const { return func[(size_t)row * (w + 1) + col]; }
+    float fi(int row) const { return f(row, row == h ? h : w); }
+    float sample1d(int row, int n, float u, float& pdf, int& off) const {
+        int l = 0, r = n, interval = -1;
+        while (l <= r) {
+            const int m = l + (r - l) / 2;
+            if (c(row, m) <= u) {
+                l = m + 1;
+                interval = m;
+            } else {
+                r = m - 1;
+            }
+        }
+        off = std::min(std::max(interval, 0), n - 1);
+        const float fv = f(row, off), c0 = c(row, off), c1 = c(row, off + 1), fint = fi(row);
+        float du = u - c0;
+        if (c1 - c0 > 0.0f) du /= (c1 - c0);
+        pdf = fint > 0.0f ? fv / fint : 0.0f;
+        return ((float)off + du) / (float)n;
+    }
+};
+OR_API void oracle_ref_dist_sample(const float* func, const float* cdf, int w, int h, const float* u, float* out,
+                                   size_t n) {
+    const RefDist D{func, cdf, w, h};
+    for (size_t i = 0; i < n; ++i) {
+        float py, px;
+        int v, cc;
+        const float y = D.sample1d(h, h + 1, u[2 * i + 1], py, v);
+        const float x = D.sample1d(v, w + 1, u[2 * i], px, cc);
+        out[4 * i] = x;
+        out[4 * i + 1] = y;
+        out[4 * i + 2] = px * py;
+        const int iu = std::min(std::max((int)(x * w), 0), w - 1), iv = std::min(std::max((int)(y * h), 0), h - 1);
+        out[4 * i + 3] = D.f(iv, iu) / D.fi(h);
+    }
+}
+
 OR_API uint32_t oracle_tea16(uint32_t a, uint32_t b) { return tea16(a, b); }
 // CudaRNG(id, frame) (rng.cuh:37-76) for (id, frame) pairs: the seed word and
 // `draws` floats each

@@ -61,6 +61,7 @@ def lib() -> C.CDLL:
                                      vp, vp, vp, vp]
         L.oracle_routines.argtypes = [C.c_int, vp, vp, sz, C.c_int]
         L.oracle_rng.argtypes = [vp, sz, C.c_int, vp, vp]
+        L.oracle_ref_dist_sample.argtypes = [vp, vp, C.c_int, C.c_int, vp, vp, sz]
         L.oracle_tea16.restype = C.c_uint32
         L.oracle_tea16.argtypes = [C.c_uint32, C.c_uint32]
         _orc = L
@@ -185,6 +186,17 @@ def rng(pairs: np.ndarray, draws: int):
     out = np.zeros((p.shape[0], draws), np.float32)
     lib().oracle_rng(_p(p), p.shape[0], draws, _p(seed), _p(out))
     return seed, out
+
+
+def ref_dist_sample(func: np.ndarray, cdf: np.ndarray, w: int, h: int, u: np.ndarray) -> np.ndarray:
+    """the reference's CudaDistribution2D sampling on its tables (h*(w+2)+1
+    floats each, plus padding): u (n, 2) -> (n, 4) x, y, pdf, Pdf(x, y)"""
+    pad = lambda a: np.concatenate([np.ascontiguousarray(a, np.float32), np.zeros(2, np.float32)])
+    f, c = pad(func), pad(cdf)
+    uu = np.ascontiguousarray(u, np.float32)
+    out = np.zeros((uu.shape[0], 4), np.float32)
+    lib().oracle_ref_dist_sample(_p(f), _p(c), int(w), int(h), _p(uu), _p(out), uu.shape[0])
+    return out
 
 
 def routines(kind: int, rec: np.ndarray, fp64: bool = False) -> np.ndarray:

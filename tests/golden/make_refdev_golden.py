@@ -17,8 +17,10 @@ Fixtures:
   refdev_sky.npz        querySkyModel for the C2 sky's fitted state
   refdev_bsdf.npz       CudaBSDF Eval / Pdf / Sample_f on the probe scene
   refdev_trace.npz      closest and any hit on the room and a sphere field
-  refdev_render.npz     MIS-off renders (path_tracer_kernel + pathtracer)
-  refdev_envdist.npz    the sky dome's CudaDistribution2D for an HDR map
+  refdev_render.npz     MIS-off renders (path_tracer_kernel + pathtracer) of
+                        the room, a sky-lit and an HDR-lit sphere field
+  refdev_envdist.npz    the sky dome's CudaDistribution2D for an HDR map and
+                        for the physical sky (sampled rows), with samples
 """
 from __future__ import annotations
 
@@ -91,7 +93,7 @@ def bsdf(out: Path):
     rng = np.random.default_rng(7)
     res = {}
     for kind in (0, 1, 2):
-        rec = probe.bsdf_records(rng, 2720)
+        rec = probe.bsdf_records(rng, 1024)
         res[f"rec{kind}"] = rec
         res[f"out{kind}"] = dev.bsdf(kind, rec)
     dev.close()
@@ -124,7 +126,7 @@ def trace(out: Path):
 
 def render(out: Path):
     res = {}
-    for name, scene in probe.trace_scenes().items():
+    for name, scene in list(probe.trace_scenes().items()) + [("envfield", probe.env_field())]:
         built, spec, cam, hosek = built_structs(scene)
         dev = rd.RefDevice(built.payload, hosek, cam, spec)
         res[f"{name}_film"] = dev.render(1, 8)
@@ -133,20 +135,27 @@ def render(out: Path):
 
 
 def envdist(out: Path):
-    env = scenes.env_map(9, width=256, height=128)
-    g, (c, r) = scenes.sphere_field(9, 4, 2)
-    s = scenes.SceneData(**g, skydome_type=_capi.NOOR_SKY_HDR, env=env, name="envdist")
-    s.camera = dict(scenes.frame_spheres(c, r, 9), w=32, h=32)
-    s.render = dict(spp=1, bounces=2, rr=1, mis=0)
+    s = probe.envdist_scene()
+    env = s.env
     built, spec, cam, hosek = built_structs(s)
     dev = rd.RefDevice(built.payload, hosek, cam, spec)
     W, H, func, cdf = dev.env_distribution()
     u = np.random.default_rng(5).random((20000, 2)).astype(np.float32)
     d = np.random.default_rng(6).normal(size=(20000, 3)).astype(np.float32)
     d /= np.linalg.norm(d, axis=1, keepdims=True)
-    np.savez_compressed(out / "refdev_envdist.npz", env=env.astype(np.float32), w=W, h=H, func=func, cdf=cdf, u=u,
-                        samples=dev.env_sample(u), dirs=d, radiance=dev.sky(d))
+    res = dict(env=env.astype(np.float32), w=W, h=H, func=func, cdf=cdf, u=u, samples=dev.env_sample(u), dirs=d,
+               radiance=dev.sky(d))
     dev.close()
+    # the physical sky's tables (1024 x 1024 cells): the rows probe.ENV_ROWS
+    # and the marginal, and samples drawn from the whole tables
+    built, spec, cam, hosek = built_structs(probe.trace_scenes()["field16"])
+    dev = rd.RefDevice(built.payload, hosek, cam, spec)
+    W, H, func, cdf = dev.env_distribution()
+    rows = np.concatenate([(r * (W + 1) + np.arange(W + 1)) for r in probe.ENV_ROWS] +
+                          [H * (W + 1) + np.arange(H + 1)])
+    res.update(sky_w=W, sky_h=H, sky_func=func[rows], sky_cdf=cdf[rows], sky_samples=dev.env_sample(u))
+    dev.close()
+    np.savez_compressed(out / "refdev_envdist.npz", **res)
 
 
 def main():

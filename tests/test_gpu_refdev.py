@@ -119,6 +119,88 @@ def test_room_render_megakernel_and_wavefront():
         r.close()
 
 
+# ------------------------------------------------ NOOR_ENV_REFERENCE mode
+def _ref_mode(scene, **kw):
+    r = scenes.Renderer(scene, **kw)
+    r.update_spec(env_sampling=_capi.NOOR_ENV_REFERENCE)
+    return r
+
+
+def _ref_tables():
+    w, h = C.c_int(), C.c_int()
+    _capi.call("noor_get_reference_distribution", C.byref(w), C.byref(h), None, None)
+    n = h.value * (w.value + 2) + 1
+    func = np.zeros(n, np.float32)
+    cdf = np.zeros(n, np.float32)
+    pf = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))
+    _capi.call("noor_get_reference_distribution", None, None, pf(func), pf(cdf))
+    return w.value, h.value, func, cdf
+
+
+def _env_samples(u):
+    d_u = dev(np.ascontiguousarray(u, np.float32))
+    d_o = dev_empty(u.shape[0] * 16)
+    _capi.call("noor_eval_env_sample", C.c_void_p(d_u.data_ptr()), C.c_void_p(d_o.data_ptr()), u.shape[0])
+    return host(d_o, np.float32, (u.shape[0], 4))
+
+
+def test_reference_env_mode_hdr_bit_exact():
+    """a 256 x 128 HDR map: the reference's tables (3x3 texture-filtered
+    luminance, FP32 Blelloch sums), its samples and its texture-unit lookups,
+    all to the bit"""
+    z = load("envdist")
+    r = _ref_mode(probe.envdist_scene())
+    try:
+        w, h, func, cdf = _ref_tables()
+        assert (w, h) == (int(z["w"]), int(z["h"]))
+        assert np.array_equal(func, z["func"]) and np.array_equal(cdf, z["cdf"])
+        assert np.array_equal(_env_samples(z["u"]), z["samples"])
+        d = dev(z["dirs"])
+        o = dev_empty(z["dirs"].shape[0] * 12)
+        _capi.call("noor_eval_sky", C.c_void_p(d.data_ptr()), C.c_void_p(o.data_ptr()), z["dirs"].shape[0])
+        assert np.array_equal(host(o, np.float32, (-1, 3)), z["radiance"])
+    finally:
+        r.close()
+
+
+def test_reference_env_mode_sky():
+    """the physical sky baked into 2048 x 2048 and its 1024 x 1024 tables;
+    the Hosek radiance itself agrees to ~1e-5, so the tables to 1e-4 and the
+    samples to 1e-4 of the unit square"""
+    z = load("envdist")
+    r = _ref_mode(probe.trace_scenes()["field16"])
+    try:
+        w, h, func, cdf = _ref_tables()
+        assert (w, h) == (int(z["sky_w"]), int(z["sky_h"]))
+        rows = np.concatenate([(k * (w + 1) + np.arange(w + 1)) for k in probe.ENV_ROWS] +
+                              [h * (w + 1) + np.arange(h + 1)])
+        assert probe.rel_err(func[rows], z["sky_func"], 1e-6).max() < 1e-4
+        assert np.abs(cdf[rows] - z["sky_cdf"]).max() < 1e-5
+        s = _env_samples(z["u"])
+        assert np.quantile(np.abs(s[:, :2] - z["sky_samples"][:, :2]).max(1), 0.999) < 1e-4
+    finally:
+        r.close()
+
+
+@pytest.mark.parametrize("name", ["field16", "envfield"])
+def test_render_reference_env_mode(name):
+    """sphere fields lit by the physical sky or an HDR map, MIS off, 8
+    frames: with the reference's environment sampling the megakernel draws
+    the reference's light samples, and its film follows path_tracer_kernel's"""
+    z = load("render")
+    s = probe.env_field() if name == "envfield" else probe.trace_scenes()[name]
+    r = _ref_mode(s, intersector=_capi.NOOR_ISECT_REF_WALD, film_mode=_capi.NOOR_FILM_REF_LERP)
+    try:
+        r.render(8)
+        img = r.framebuffer()
+    finally:
+        r.close()
+    # a few paths in a thousand part ways on rounding (the product's BSDF
+    # sampling contracts multiply-adds, the reference's build does not) and
+    # take another branch at a glass or a lobe of the map
+    probe.check_film(z[f"{name}_film"], img, q999=1e-3)
+
+
 # ------------------------------------------------------------ live, C2 size
 live = pytest.mark.skipif(not rd.available(), reason="reference device library not built here")
 

@@ -121,3 +121,11 @@ def test_room_render():
     img = orc.render(cam, 1, 8, isect=_capi.NOOR_ISECT_REF_WALD).reshape(cam.h, cam.w, 3)
     orc.close()
     probe.check_film(z["room_film"], img)
+
+
+def test_reference_distribution_sampling_bit_exact():
+    """the restatement of CudaDistribution2D's sampling (its n + 1 searches
+    included) on the reference's own tables for a 256 x 128 map"""
+    z = load("envdist")
+    got = O.ref_dist_sample(z["func"], z["cdf"], int(z["w"]), int(z["h"]), z["u"])
+    assert np.array_equal(got, z["samples"])
