@@ -612,7 +612,14 @@ typedef struct noor_wf_frame {
 typedef struct noor_wf_params {
     uint32_t block_size;        /* threads per block of the stage kernels   */
     uint32_t queue_capacity;    /* path slots in flight                     */
-    uint32_t sort_granularity;  /* 0: no material sort, else bins per sort  */
+    uint32_t sort_granularity;  /* how finely rays are ordered for SIMT
+                                 * coherence: 0 one shading queue; 1 one per
+                                 * material kind; 2 also extension rays
+                                 * (camera rays compacted in slot order,
+                                 * secondary rays by a counting sort on
+                                 * (direction octant, origin cell of a 16^3
+                                 * grid)); 3 also shadow rays, by the same
+                                 * sort; larger values act as 3             */
     uint32_t use_graph;         /* capture one bounce as a CUDA graph       */
 } noor_wf_params;
 
@@ -656,8 +663,11 @@ int noor_megakernel_batch(const noor_wf_frame* frames, uint32_t n_frames,
  * nothing in it needs clearing between calls. */
 #define NOOR_NOALLOC_SCRATCH_BYTES (32u << 20)
 int noor_megakernel_frame_noalloc(const noor_wf_frame* frame);
-/* Project-written autotuner: times candidate parameter sets on the given
- * batch and returns the fastest. */
+/* Project-written autotuner: coordinate descent on the launch parameters,
+ * each candidate timed by one device-timed render of the given batch: slot
+ * count (2^18 .. 2^23, at most twice the batch's paths), block size (32, 64,
+ * 128), sort granularity (0 .. 3), then the slot count once more around the
+ * sort level chosen.  *best = the fastest seen (use_graph as given). */
 int noor_wavefront_autotune(const noor_wf_frame* frames, uint32_t n_frames,
                             noor_wf_params* best, float* best_ms);
 

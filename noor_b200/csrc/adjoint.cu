@@ -243,7 +243,7 @@ NB_D int direct_terms(const PathCtx& C, const DevMaterial& m0, const DevMaterial
         Le = (A.two_sided || dot(wi, A.n) < 0.0f) ? A.ke : f3(0.0f);
     } else {
         lh = S.sky_on != 0;
-        Le = S.sky_on ? env_eval(S, wi) : f3(0.0f);
+        Le = S.sky_on ? env_eval<false>(S, wi) : f3(0.0f);
     }
     if (!lh || is_black(Le)) return nt;
     const float3 to = so + tm * wi;
@@ -319,7 +319,7 @@ NB_D float3 replay(const PathCtx& C, uint32_t pix, uint32_t frame, const DevCame
                     bl = env_weights(C.P, dir);
                     Le = env_radiance(C.P, bl);
                 } else {
-                    Le = env_eval(S, dir);
+                    Le = env_eval<false>(S, dir);
                 }
                 L += beta * Le;
                 if (MODE == 1 && env) {

@@ -168,11 +168,11 @@ NB_D float3 sample_li(const DevScene& S, const Isect& I, Rng& rng, int nl, int l
         Li = delta_sample(S.delta_lights[li - S.num_area_lights], S.world_radius, I.p, to, wi, pdf);
         if (pdf == 0.0f) return f3(0.0f);
     } else {
-        const float3 dir = env_sample_dir(S, rng, pdf);
+        const float3 dir = env_sample_dir<EXT>(S, rng, pdf);
         if (isinf(pdf) || isnan(pdf)) pdf = 0.0f;
         to = I.p + 2.0f * S.world_radius * dir;
         visibility(I.p, to, wi);
-        Li = S.sky_on ? env_eval(S, wi) : f3(0.0f);
+        Li = S.sky_on ? env_eval<EXT>(S, wi) : f3(0.0f);
     }
     if (isinf(pdf)) pdf = 0.0f;
     return Li * (float)nl;
@@ -209,7 +209,7 @@ NB_D float light_pdf(const DevScene& S, const Isect& I, int li, const float3& wi
     } else if (is_delta_light<EXT>(S, li)) {
         pdf = 0.0f;
     } else {
-        pdf = env_pdf(S, wi);
+        pdf = env_pdf<EXT>(S, wi);
     }
     return isinf(pdf) ? 0.0f : pdf;
 }
@@ -220,8 +220,9 @@ template <bool EXT>
 NB_D bool is_catcher(const Isect& I) {
     return EXT && I.lobe == kLobeCatcher;
 }
+template <bool EXT>
 NB_D float3 catcher_sky(const DevScene& S, const Isect& I) {
-    return env_eval(S, -1.0f * to_world(I.F, to_local(I.F, I.wo)));
+    return env_eval<EXT>(S, -1.0f * to_world(I.F, to_local(I.F, I.wo)));
 }
 
 // A shadow ray whose contribution counts only if nothing blocks it.
@@ -251,7 +252,7 @@ NB_D float3 light_sample_contrib(const DevScene& S, const DevMaterial& m, const 
     const float3 Li = sample_li<EXT>(S, I, rng, nl, li, wi, to, lpdf);
     if (lpdf == 0.0f || is_black(Li)) return f3(0.0f);
     float3 f = bsdf_eval<EXT>(I.lobe, m, I.F, I.wo, wi, kNonSpecular);
-    if (is_catcher<EXT>(I)) f *= catcher_sky(S, I);
+    if (is_catcher<EXT>(I)) f *= catcher_sky<EXT>(S, I);
     if (is_black(f)) return f3(0.0f);
     f *= absdot(wi, I.F.n);
     sr.o = spawn_origin(I, wi, S.bias);
@@ -297,7 +298,7 @@ NB_D float3 bsdf_mis_contrib(const DevScene& S, const DevMaterial& m, const Isec
         Le = area_le<EXT>(A, wi);
     } else {
         lh = S.sky_on != 0;
-        Le = S.sky_on ? env_eval(S, wi) : f3(0.0f);
+        Le = S.sky_on ? env_eval<EXT>(S, wi) : f3(0.0f);
     }
     if (!lh) return f3(0.0f);
     const float3 c = Le * f * w / spdf;
@@ -350,7 +351,7 @@ NB_D float3 path_radiance(const DevScene& S, float3 o, float3 d, Rng& rng, const
         HitRec rec;
         rs.ext++;
         if (!trace_closest<ISECT, EXT>(S, o, d, tmax, rec, st, status)) {
-            if (S.sky_on && (bounce == 0 || spec_bounce)) L += beta * env_eval(S, normalize_fast(d));
+            if (S.sky_on && (bounce == 0 || spec_bounce)) L += beta * env_eval<EXT>(S, normalize_fast(d));
             break;
         }
         Isect I;
@@ -398,7 +399,7 @@ NB_D float3 path_radiance(const DevScene& S, float3 o, float3 d, Rng& rng, const
         uint32_t stype;
         const float3 f = bsdf_sample<EXT>(I.lobe, m, I.F, I.wo, BSDF_ALL, rng, wi, pdf, stype);
         if (pdf == 0.0f) break;
-        beta *= (is_catcher<EXT>(I) ? f * catcher_sky(S, I) : f) * absdot(wi, I.F.n) / pdf;
+        beta *= (is_catcher<EXT>(I) ? f * catcher_sky<EXT>(S, I) : f) * absdot(wi, I.F.n) / pdf;
         // correct_sidedness (accumulate.cuh:40-45)
         if (!(I.mtype & kTransparentMat) && dot(wi, I.F.ng) < 0.0f) break;
         // rr_terminate (accumulate.cuh:27-38)

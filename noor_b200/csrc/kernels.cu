@@ -261,7 +261,7 @@ __global__ void k_eval_routines(int kind, const float* in, float* out, size_t n)
 __global__ void k_eval_sky(DevScene S, const float* dirs, float* rgb, size_t n) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const float3 c = env_eval(S, f3(dirs[3 * i], dirs[3 * i + 1], dirs[3 * i + 2]));
+    const float3 c = env_eval<true>(S, f3(dirs[3 * i], dirs[3 * i + 1], dirs[3 * i + 2]));
     rgb[3 * i] = c.x;
     rgb[3 * i + 1] = c.y;
     rgb[3 * i + 2] = c.z;
@@ -326,7 +326,7 @@ cudaError_t launch_megakernel(const DevScene& S, const DevCamera& C, const MegaA
     } while (0)
 #define NB_MK(I, F)                     \
     do {                                \
-        if (S.ext_lobes || S.ext_lights || ext_cam) NB_MK2(I, F, true); \
+        if (S.ext_lobes || S.ext_lights || S.env_ref || ext_cam) NB_MK2(I, F, true); \
         else NB_MK2(I, F, false);       \
     } while (0)
     if (S.isect == NOOR_ISECT_WATERTIGHT) {

@@ -1061,13 +1061,18 @@ NB_D float3 env_bilinear(const DevScene& S, float u, float v) {
     return w00 * f3(t00) + w10 * f3(t10) + w01 * f3(t01) + w11 * f3(t11);
 }
 
+NB_OUTLINE float3 env_texture(const DevScene& S, float u, float v) { return f3(tex2D<float4>(S.env_tex, u, v)); }
+
 // CudaSkyDomeManager::evaluate(dir) (noor/cuda/skydome.cuh:93-101); with
-// NOOR_ENV_REFERENCE maps are read through the texture unit as there
+// NOOR_ENV_REFERENCE maps are read through the texture unit as there.  The
+// mode's code is compiled only where REF is true (the kernels' extended
+// builds, which scenes using the mode select): the default builds carry none.
+template <bool REF = true>
 NB_D float3 env_eval(const DevScene& S, const float3& dir) {
     if (S.sky_type == NOOR_SKY_PHYSICAL) return hosek_query(S.hosek, dir);
     const float phi = spherical_phi(dir) * kInv2Pi;
     const float theta = spherical_theta(dir) * kInvPi;
-    if (S.env_ref) return f3(tex2D<float4>(S.env_tex, phi, theta));
+    if (REF && S.env_ref) return env_texture(S, phi, theta);
     return env_bilinear(S, phi, theta);
 }
 
@@ -1100,7 +1105,9 @@ NB_D float rdist_sample1d(const DevScene& S, int row, int n, float u, float& pdf
     pdf = fi > 0.0f ? func / fi : 0.0f;
     return ((float)off + du) / (float)n;
 }
-NB_D float2 rdist_sample(const DevScene& S, float u0, float u1, float& pdf) {
+// out of line (like the extra lobes): kernels that never meet the mode
+// spend no instruction cache or registers on it
+NB_OUTLINE float2 rdist_sample(const DevScene& S, float u0, float u1, float& pdf) {
     float py, px;
     int v, c;
     const float y = rdist_sample1d(S, S.rh, S.rh + 1, u1, py, v);
@@ -1108,7 +1115,7 @@ NB_D float2 rdist_sample(const DevScene& S, float u0, float u1, float& pdf) {
     pdf = px * py;
     return f2(x, y);
 }
-NB_D float rdist_pdf(const DevScene& S, float x, float y) {
+NB_OUTLINE float rdist_pdf(const DevScene& S, float x, float y) {
     const int iu = min(max((int)(x * S.rw), 0), S.rw - 1);
     const int iv = min(max((int)(y * S.rh), 0), S.rh - 1);
     return rdist_func(S, iv, iu) / rdist_func_int(S, S.rh);
@@ -1150,17 +1157,19 @@ NB_D float dist_pdf(const DevDist2D& D, float x, float y) {
 
 // importance_sample_dir (noor/cuda/skydome.cuh:130-140) on the build's
 // distribution; draws two random numbers
+template <bool REF = true>
 NB_D float3 env_sample_dir(const DevScene& S, Rng& rng, float& pdf) {
     const float u0 = rng.next();
     const float u1 = rng.next();
     float mp;
-    const float2 uv = S.env_ref ? rdist_sample(S, u0, u1, mp) : dist_sample(S.dist, u0, u1, mp);
+    const float2 uv = (REF && S.env_ref) ? rdist_sample(S, u0, u1, mp) : dist_sample(S.dist, u0, u1, mp);
     float st;
     const float3 dir = spherical_direction(uv.x, uv.y, st);
     pdf = (st == 0.0f) ? 0.0f : mp / (2.0f * kPi * kPi * st);
     return dir;
 }
 // CudaInfiniteLight::pdf_Li (noor/cuda/lightimp.cuh:161-173)
+template <bool REF = true>
 NB_D float env_pdf(const DevScene& S, const float3& wi) {
     if (!S.sky_on) return 0.0f;
     const float theta = spherical_theta(wi);
@@ -1168,7 +1177,7 @@ NB_D float env_pdf(const DevScene& S, const float3& wi) {
     const float st = sinf(theta);
     if (st == 0.0f) return 0.0f;
     const float x = phi * kInv2Pi, y = theta * kInvPi;
-    return (S.env_ref ? rdist_pdf(S, x, y) : dist_pdf(S.dist, x, y)) / (2.0f * kPi * kPi * st);
+    return ((REF && S.env_ref) ? rdist_pdf(S, x, y) : dist_pdf(S.dist, x, y)) / (2.0f * kPi * kPi * st);
 }
 
 }  // namespace nb

@@ -161,45 +161,55 @@ NB_D bool wt_test(const TRay& r, const WtRay& w, const DevWtTri* tri, float& tma
     return true;
 }
 
+// Arithmetic of the light-shape tests: with X (the reference's Wald mode,
+// whose hit distances are the reference's to the bit) each operation rounds
+// on its own; otherwise the compiler may contract multiply-adds.
+template <bool X> NB_D float smul(float a, float b) { return X ? __fmul_rn(a, b) : a * b; }
+template <bool X> NB_D float sadd(float a, float b) { return X ? __fadd_rn(a, b) : a + b; }
+template <bool X> NB_D float ssub(float a, float b) { return X ? __fsub_rn(a, b) : a - b; }
+template <bool X> NB_D float sdot(float ax, float ay, float az, float bx, float by, float bz) {
+    return sadd<X>(sadd<X>(smul<X>(ax, bx), smul<X>(ay, by)), smul<X>(az, bz));
+}
+
 // quad of an area light (noor/cuda/geometry.cuh:105-123); note the
 // reference accepts negative t (no lower bound), kept as is.
+template <bool X = false>
 NB_D bool quad_hit(const DevAreaLight& q, const float3& o, const float3& d, float& tmax) {
-    const float denom = xdot3(q.n.x, q.n.y, q.n.z, d.x, d.y, d.z);
+    const float denom = sdot<X>(q.n.x, q.n.y, q.n.z, d.x, d.y, d.z);
     if (denom == 0.0f) return false;
-    const float t = xdiv(-xsub(xdot3(o.x, o.y, o.z, q.n.x, q.n.y, q.n.z),
-                               xdot3(q.center.x, q.center.y, q.center.z, q.n.x, q.n.y, q.n.z)),
-                         denom);
+    const float t = -ssub<X>(sdot<X>(o.x, o.y, o.z, q.n.x, q.n.y, q.n.z),
+                             sdot<X>(q.center.x, q.center.y, q.center.z, q.n.x, q.n.y, q.n.z)) /
+                    denom;
     if (t > tmax) return false;
     // pointAtParameter(t) - center
-    const float ix = xsub(xadd(o.x, xmul(t, d.x)), q.center.x);
-    const float iy = xsub(xadd(o.y, xmul(t, d.y)), q.center.y);
-    const float iz = xsub(xadd(o.z, xmul(t, d.z)), q.center.z);
-    const float t0 = xdiv(xdot3(ix, iy, iz, q.u.x, q.u.y, q.u.z), xdot3(q.u.x, q.u.y, q.u.z, q.u.x, q.u.y, q.u.z));
+    const float ix = ssub<X>(sadd<X>(o.x, smul<X>(t, d.x)), q.center.x);
+    const float iy = ssub<X>(sadd<X>(o.y, smul<X>(t, d.y)), q.center.y);
+    const float iz = ssub<X>(sadd<X>(o.z, smul<X>(t, d.z)), q.center.z);
+    const float t0 = sdot<X>(ix, iy, iz, q.u.x, q.u.y, q.u.z) / sdot<X>(q.u.x, q.u.y, q.u.z, q.u.x, q.u.y, q.u.z);
     if (t0 < 0.0f || t0 > 1.0f) return false;
-    const float t1 = xdiv(xdot3(ix, iy, iz, q.v.x, q.v.y, q.v.z), xdot3(q.v.x, q.v.y, q.v.z, q.v.x, q.v.y, q.v.z));
+    const float t1 = sdot<X>(ix, iy, iz, q.v.x, q.v.y, q.v.z) / sdot<X>(q.v.x, q.v.y, q.v.z, q.v.x, q.v.y, q.v.z);
     if (t1 < 0.0f || t1 > 1.0f) return false;
     tmax = t;
     return true;
 }
 
 // solveQuadratic (noor/cuda/utils.cuh:52-91): the root of larger magnitude
-// first, the other from x0 * x1 = c / a; returns x0 <= x1.  Like the light
-// shape tests below, every operation rounds on its own, so that the hit
-// distance is the reference's to the bit.
+// first, the other from x0 * x1 = c / a; returns x0 <= x1
+template <bool X = false>
 NB_D bool solve_quadratic(float a, float b, float c, float& x0, float& x1) {
     if (a == 0.0f) {
         if (b != 0.0f) {
-            x0 = x1 = xdiv(-c, b);
+            x0 = x1 = -c / b;
             return true;
         }
         return false;
     }
-    const float disc = xsub(xmul(b, b), xmul(xmul(4.0f, a), c));
+    const float disc = ssub<X>(smul<X>(b, b), smul<X>(smul<X>(4.0f, a), c));
     if (disc < 0.0f) return false;
     const float sd = sqrtf(disc);
-    const float q = b < 0.0f ? xmul(-0.5f, xsub(b, sd)) : xmul(-0.5f, xadd(b, sd));
-    x0 = xdiv(q, a);
-    x1 = xdiv(c, q);
+    const float q = b < 0.0f ? smul<X>(-0.5f, ssub<X>(b, sd)) : smul<X>(-0.5f, sadd<X>(b, sd));
+    x0 = q / a;
+    x1 = c / q;
     if (x0 > x1) {
         const float t = x0;
         x0 = x1;
@@ -210,11 +220,12 @@ NB_D bool solve_quadratic(float a, float b, float c, float& x0, float& x1) {
 
 // sphere of an area light (noor/cuda/geometry.cuh:125-150): nearest root in
 // [0, tmax], else the far root when the near one is behind the origin
+template <bool X = false>
 NB_D bool sphere_hit(const DevAreaLight& s, const float3& o, const float3& d, float& tmax) {
-    const float ox = xsub(o.x, s.center.x), oy = xsub(o.y, s.center.y), oz = xsub(o.z, s.center.z);
+    const float ox = ssub<X>(o.x, s.center.x), oy = ssub<X>(o.y, s.center.y), oz = ssub<X>(o.z, s.center.z);
     float t0, t1;
-    if (!solve_quadratic(xdot3(d.x, d.y, d.z, d.x, d.y, d.z), xmul(2.0f, xdot3(ox, oy, oz, d.x, d.y, d.z)),
-                         xsub(xdot3(ox, oy, oz, ox, oy, oz), s.radius2), t0, t1))
+    if (!solve_quadratic<X>(sdot<X>(d.x, d.y, d.z, d.x, d.y, d.z), smul<X>(2.0f, sdot<X>(ox, oy, oz, d.x, d.y, d.z)),
+                            ssub<X>(sdot<X>(ox, oy, oz, ox, oy, oz), s.radius2), t0, t1))
         return false;
     if (!(t0 <= tmax && t1 >= 0.0f)) return false;
     if (t0 < 0.0f) {
@@ -228,17 +239,18 @@ NB_D bool sphere_hit(const DevAreaLight& s, const float3& o, const float3& d, fl
 
 // disk of an area light (noor/cuda/geometry.cuh:152-163); like the quad, no
 // lower bound on t
+template <bool X = false>
 NB_D bool disk_hit(const DevAreaLight& q, const float3& o, const float3& d, float& tmax) {
-    const float denom = xdot3(q.n.x, q.n.y, q.n.z, d.x, d.y, d.z);
+    const float denom = sdot<X>(q.n.x, q.n.y, q.n.z, d.x, d.y, d.z);
     if (denom == 0.0f) return false;
-    const float t = xdiv(-xsub(xdot3(o.x, o.y, o.z, q.n.x, q.n.y, q.n.z),
-                               xdot3(q.center.x, q.center.y, q.center.z, q.n.x, q.n.y, q.n.z)),
-                         denom);
+    const float t = -ssub<X>(sdot<X>(o.x, o.y, o.z, q.n.x, q.n.y, q.n.z),
+                             sdot<X>(q.center.x, q.center.y, q.center.z, q.n.x, q.n.y, q.n.z)) /
+                    denom;
     if (t > tmax) return false;
-    const float px = xsub(xadd(o.x, xmul(t, d.x)), q.center.x);
-    const float py = xsub(xadd(o.y, xmul(t, d.y)), q.center.y);
-    const float pz = xsub(xadd(o.z, xmul(t, d.z)), q.center.z);
-    if (xdot3(px, py, pz, px, py, pz) > q.radius2) return false;
+    const float px = ssub<X>(sadd<X>(o.x, smul<X>(t, d.x)), q.center.x);
+    const float py = ssub<X>(sadd<X>(o.y, smul<X>(t, d.y)), q.center.y);
+    const float pz = ssub<X>(sadd<X>(o.z, smul<X>(t, d.z)), q.center.z);
+    if (sdot<X>(px, py, pz, px, py, pz) > q.radius2) return false;
     tmax = t;
     return true;
 }
@@ -246,11 +258,11 @@ NB_D bool disk_hit(const DevAreaLight& q, const float3& o, const float3& d, floa
 // CudaShape::intersect (noor/cuda/shapeimp.cuh:73-87).  EXT false: the
 // scene's area lights are all quads (kernels for such scenes leave the
 // other shapes' code out)
-template <bool EXT = true>
+template <bool EXT = true, bool X = false>
 NB_D bool shape_hit(const DevAreaLight& a, const float3& o, const float3& d, float& tmax) {
-    if (!EXT || a.type == NOOR_SHAPE_QUAD) return quad_hit(a, o, d, tmax);
-    if (a.type == NOOR_SHAPE_SPHERE) return sphere_hit(a, o, d, tmax);
-    return disk_hit(a, o, d, tmax);
+    if (!EXT || a.type == NOOR_SHAPE_QUAD) return quad_hit<X>(a, o, d, tmax);
+    if (a.type == NOOR_SHAPE_SPHERE) return sphere_hit<X>(a, o, d, tmax);
+    return disk_hit<X>(a, o, d, tmax);
 }
 
 struct HitRec {
@@ -312,7 +324,8 @@ NB_D bool trace_closest(const DevScene& S, const float3& o, const float3& d, flo
                 next = neg ? lo.w : ni + 1;
             } else if (hi.w & NOOR_LIGHT_NODE_MASK) {
                 const uint32_t li = hi.w & NOOR_LIGHT_MASK;
-                if ((int)li < S.num_area_lights && shape_hit<EXT>(S.area_lights[li], o, d, tmax)) {
+                if ((int)li < S.num_area_lights &&
+                    shape_hit<EXT, ISECT == NOOR_ISECT_REF_WALD>(S.area_lights[li], o, d, tmax)) {
                     hit = true;
                     rec.ins = li;
                     rec.mtype = NOOR_MESHLIGHT | NOOR_EMITTER;
@@ -402,7 +415,8 @@ NB_D bool trace_any(const DevScene& S, const float3& o, const float3& d, float t
             } else if (hi.w & NOOR_LIGHT_NODE_MASK) {
                 const uint32_t li = hi.w & NOOR_LIGHT_MASK;
                 float tm = tmax;
-                if ((int)li < S.num_area_lights && shape_hit<EXT>(S.area_lights[li], o, d, tm)) return true;
+                if ((int)li < S.num_area_lights && shape_hit<EXT, ISECT == NOOR_ISECT_REF_WALD>(S.area_lights[li], o, d, tm))
+                    return true;
             } else if (hi.w & NOOR_MESH_INSTANCE_MASK) {
                 tray_to_object(lr, wr, S.xforms + (hi.w & NOOR_TRANS_MASK));
                 ltmax = tmax;

@@ -73,8 +73,20 @@ enum : int {
     kCntActive = kKinds + 1,   // slots holding a path after regen (= rays extend traces)
     kCntIter = kKinds + 2,     // iterations run
     kCntTake = kKinds + 3,     // shadow queue entries taken by wf_shadow's warps
-    kCntWords = kKinds + 4
+    kCntCam = kKinds + 4,      // camera rays in the extension order (sort level 2)
+    kCntTakeExt = kKinds + 5,  // extension order entries taken by wf_extend's warps
+    kCntWords = kKinds + 6
 };
+
+// Ray ordering (sort levels 2 and 3): a counting sort of rays into buckets
+// of (direction octant, cell of the origin in a 16^3 grid over the scene's
+// root box), so that the lanes of a warp start near each other and head the
+// same way.  The bucket of each ray is computed on the device and the
+// counts, offsets and permutation never leave it (the pass runs inside the
+// graph's loop).
+constexpr int kCellBits = 4;
+constexpr int kBuckets = 8 << (3 * kCellBits);
+constexpr int kScanThreads = 1024;
 
 // block sizes of the slot sweeps (one block-wide atomic per counter)
 constexpr int kRegenBlock = 512;
@@ -96,6 +108,12 @@ struct WfDev {
     float4* sh_o;           // origin, tmax (by queue entry)
     float4* sh_d;           // direction
     uint32_t* counters;     // kCntWords words
+    uint32_t* bkt_cnt;      // kBuckets bucket sizes (zero between passes)
+    uint32_t* bkt_off;      // kBuckets bucket offsets, advanced by the scatter
+    uint32_t* sh_key;       // bucket of each shadow queue entry
+    uint32_t* sh_perm;      // shadow queue entries in bucket order
+    uint32_t* ext_key;      // bucket of each slot's secondary ray
+    uint32_t* ext_perm;     // camera-ray slots in slot order, then (at cap) secondary-ray slots in bucket order
     unsigned long long* work_next;
     unsigned long long* rays;  // [ext, shadow, paths], added up by wf_check
     uint32_t* status;
@@ -104,6 +122,7 @@ struct WfDev {
     uint32_t nframes;
     uint32_t cap;
     uint32_t sort;          // 0: one shade queue, 1: one per kind
+    uint32_t level;         // sort granularity: 1 material queues, 2 + extension rays, 3 + shadow rays
     uint32_t max_iters;
     unsigned long long total;
     int stack_cap;
@@ -232,7 +251,7 @@ __global__ void __launch_bounds__(kRegenBlock) wf_regen(WfDev W) {
             const WfFrameDev& F = W.frames[fi];
             if (st & kSkySeen) {
                 const float4 bw = W.beta[slot], dw = W.d[slot];
-                const float3 c = f3(bw.x, bw.y, bw.z) * env_eval(W.scenes[F.scene], normalize_fast(f3(dw.x, dw.y, dw.z)));
+                const float3 c = f3(bw.x, bw.y, bw.z) * env_eval<true>(W.scenes[F.scene], normalize_fast(f3(dw.x, dw.y, dw.z)));
                 Lw.x += c.x;
                 Lw.y += c.y;
                 Lw.z += c.z;
@@ -262,9 +281,12 @@ __global__ void __launch_bounds__(kRegenBlock) wf_regen(WfDev W) {
         if (k < W.total) {
             const int fi = frame_of(W, k);
             const WfFrameDev& F = W.frames[fi];
+            // all samples of a pixel are consecutive work items (pixels in
+            // 8x4 tile order): the lanes of a warp trace up to 32 camera rays
+            // through one pixel, which differ only by their sub-pixel jitter
             const unsigned long long local = k - F.base;
-            const uint32_t sample = (uint32_t)(local / F.npix);
-            const uint32_t pix = tile_pixel((uint32_t)(local % F.npix), F.cam.w, F.cam.h);
+            const uint32_t sample = (uint32_t)(local % F.spp);
+            const uint32_t pix = tile_pixel((uint32_t)(local / F.spp), F.cam.w, F.cam.h);
             Rng rng{tea16(pix, F.first_frame + sample)};
             float3 o, d;
             camera_ray(F.cam, pix % F.cam.w, pix / F.cam.w, rng, o, d);
@@ -278,6 +300,70 @@ __global__ void __launch_bounds__(kRegenBlock) wf_regen(WfDev W) {
     if (valid) W.state[slot] = st;
     const int nact = __syncthreads_count(valid && st == kActive);
     if (threadIdx.x == 0 && nact) atomicAdd(W.counters + kCntActive, (uint32_t)nact);
+}
+
+// bucket of a ray: direction octant, then the Morton code of its origin's
+// cell in a 16^3 grid over the scene's root box
+NB_D uint32_t spread3(uint32_t v) {
+    v = (v | (v << 8)) & 0x0F00Fu;
+    v = (v | (v << 4)) & 0xC30C3u;
+    v = (v | (v << 2)) & 0x49249u;
+    return v;
+}
+NB_D uint32_t ray_bucket(const DevScene& S, const float3& o, const float3& d) {
+    const DevNode* r = S.nodes + S.root;
+    const uint4 lo = __ldg(&r->lo), hi = __ldg(&r->hi);
+    const float n = (float)(1 << kCellBits);
+    auto cell = [&](float p, uint32_t a, uint32_t b) {
+        const float l = __uint_as_float(a), h = __uint_as_float(b);
+        const int c = (int)((p - l) / fmaxf(h - l, 1e-30f) * n);
+        return (uint32_t)min(max(c, 0), (1 << kCellBits) - 1);
+    };
+    const uint32_t m = spread3(cell(o.x, lo.x, hi.x)) | (spread3(cell(o.y, lo.y, hi.y)) << 1) |
+                       (spread3(cell(o.z, lo.z, hi.z)) << 2);
+    const uint32_t oct = (d.x < 0.0f ? 1u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 4u : 0u);
+    return (oct << (3 * kCellBits)) | m;
+}
+
+// warp-aggregated atomicAdd of 1 on counters[key]: lanes with the same key
+// share one atomic; returns this lane's old value + its rank among them
+NB_D uint32_t bucket_add(uint32_t* counters, uint32_t key) {
+    const uint32_t active = __activemask();
+    const uint32_t peers = __match_any_sync(active, key);
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(peers) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(counters + key, (uint32_t)__popc(peers));
+    base = __shfl_sync(peers, base, leader);
+    return base + __popc(peers & ((1u << lane) - 1u));
+}
+
+// exclusive scan of the bucket sizes into offsets (one block); the sizes
+// are cleared for the next pass
+__global__ void __launch_bounds__(kScanThreads) wf_bucket_scan(WfDev W) {
+    constexpr int per = kBuckets / kScanThreads;
+    __shared__ uint32_t part[kScanThreads];
+    const int t = threadIdx.x;
+    uint32_t v[per];
+    uint32_t sum = 0;
+    for (int k = 0; k < per; ++k) {
+        v[k] = W.bkt_cnt[t * per + k];
+        W.bkt_cnt[t * per + k] = 0u;
+        sum += v[k];
+    }
+    part[t] = sum;
+    __syncthreads();
+    for (int off = 1; off < kScanThreads; off <<= 1) {
+        const uint32_t add = t >= off ? part[t - off] : 0u;
+        __syncthreads();
+        part[t] += add;
+        __syncthreads();
+    }
+    uint32_t run = part[t] - sum;
+    for (int k = 0; k < per; ++k) {
+        W.bkt_off[t * per + k] = run;
+        run += v[k];
+    }
 }
 
 template <int ISECT, bool EXT>
@@ -322,6 +408,52 @@ NB_D void extend_one(const WfDev& W, const DevScene& S, uint32_t slot, const flo
     W.state[slot] = kActive | ((kind + 1u) << kKindShift);  // wf_bin queues it for shading
 }
 
+// Sort level 2: the extension order.  Camera rays (bounce 0) are compacted
+// in slot order, block by block, so that the consecutive pixels regen gave
+// consecutive free slots stay together; secondary rays get their bucket.
+// After wf_bucket_scan, wf_ext_scatter places the secondary rays at cap + 
+// their position in bucket order.
+template <bool MULTI>
+__global__ void __launch_bounds__(kBinBlock) wf_ext_key(WfDev W, DevScene S1) {
+    __shared__ uint32_t woff[kBinBlock / 32];
+    __shared__ uint32_t base;
+    const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
+    bool cam = false, sec = false;
+    if (slot < W.cap && W.state[slot] == kActive) {
+        cam = (fbits(W.beta[slot].w) & 0xFFFFu) == 0u;
+        sec = !cam;
+    }
+    const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const uint32_t ball = __ballot_sync(0xFFFFFFFFu, cam);
+    if (lane == 0) woff[wid] = __popc(ball);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t tot = 0;
+        for (int w = 0; w < kBinBlock / 32; ++w) {
+            const uint32_t c = woff[w];
+            woff[w] = tot;
+            tot += c;
+        }
+        base = tot ? atomicAdd(W.counters + kCntCam, tot) : 0u;
+    }
+    __syncthreads();
+    if (cam) W.ext_perm[base + woff[wid] + __popc(ball & lanes_below())] = slot;
+    uint32_t key = 0xFFFFFFFFu;
+    if (sec) {
+        const float4 ow = W.o[slot], dw = W.d[slot];
+        const DevScene& S = MULTI ? W.scenes[W.frames[fbits(ow.w)].scene] : S1;
+        key = ray_bucket(S, f3(ow.x, ow.y, ow.z), f3(dw.x, dw.y, dw.z));
+        bucket_add(W.bkt_cnt, key);
+    }
+    if (slot < W.cap) W.ext_key[slot] = key;
+}
+__global__ void __launch_bounds__(kBinBlock) wf_ext_scatter(WfDev W) {
+    const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= W.cap) return;
+    const uint32_t key = W.ext_key[slot];
+    if (key != 0xFFFFFFFFu) W.ext_perm[W.cap + bucket_add(W.bkt_off, key)] = slot;
+}
+
 // The traversal kernels are instantiated per intersector and per scene
 // source: with MULTI false every frame of the launch uses the scene passed as
 // the kernel parameter S1 (read from the constant bank); with MULTI true each
@@ -338,11 +470,7 @@ NB_D const DevScene& slot_scene(const WfDev& W, const DevScene& S1, uint32_t fra
 // Extend: closest hit for every active slot (one thread per slot).  EXT
 // false: no scene of the launch has sphere or disk lights
 template <int ISECT, bool MULTI, bool EXT>
-__global__ void __launch_bounds__(NB_TRAV_THREADS, NB_TRAV_MIN_BLOCKS) wf_extend(WfDev W, DevScene S1) {
-    extern __shared__ uint32_t smem[];
-    const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
-    if (slot >= W.cap || W.state[slot] != kActive) return;
-    SmemStack stk{smem + threadIdx.x, (int)blockDim.x, W.stack_cap};
+NB_D void extend_slot(const WfDev& W, const DevScene& S1, uint32_t slot, const SmemStack& stk) {
     const float4 ow = W.o[slot];
     const DevScene& S = slot_scene<ISECT, MULTI>(W, S1, fbits(ow.w));
     if (ISECT == kIsectMixed) {
@@ -353,6 +481,32 @@ __global__ void __launch_bounds__(NB_TRAV_THREADS, NB_TRAV_MIN_BLOCKS) wf_extend
     } else {
         extend_one<ISECT == kIsectMixed ? 0 : ISECT, EXT>(W, S, slot, ow, stk);
     }
+}
+
+// Extend.  Below sort level 2 one thread per slot; from level 2 each warp
+// takes the next 32 entries of the extension order (camera rays, then
+// secondary rays by bucket) when it is done with its last ones.
+template <int ISECT, bool MULTI, bool EXT>
+__global__ void __launch_bounds__(NB_TRAV_THREADS, NB_TRAV_MIN_BLOCKS) wf_extend(WfDev W, DevScene S1) {
+    extern __shared__ uint32_t smem[];
+    SmemStack stk{smem + threadIdx.x, (int)blockDim.x, W.stack_cap};
+    if (W.level >= 2) {
+        const uint32_t nc = W.counters[kCntCam], n = W.counters[kCntActive];
+        const uint32_t lane = threadIdx.x & 31;
+        for (;;) {
+            uint32_t base = 0;
+            if (lane == 0) base = atomicAdd(W.counters + kCntTakeExt, 32u);
+            base = __shfl_sync(0xFFFFFFFFu, base, 0);
+            if (base >= n) break;
+            const uint32_t i = base + lane;
+            if (i >= n) continue;
+            extend_slot<ISECT, MULTI, EXT>(W, S1, i < nc ? W.ext_perm[i] : W.ext_perm[W.cap + (i - nc)], stk);
+        }
+        return;
+    }
+    const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= W.cap || W.state[slot] != kActive) return;
+    extend_slot<ISECT, MULTI, EXT>(W, S1, slot, stk);
 }
 
 // Shading queues in slot order: every slot extend left a surface hit goes to
@@ -459,7 +613,7 @@ __global__ void __launch_bounds__(256, NB_SHADE_MIN_BLOCKS) wf_shade(WfDev W, ui
         if (pdf == 0.0f) {
             st = kFinishing;
         } else {
-            beta *= (is_catcher<EXT>(I) ? f * catcher_sky(S, I) : f) * absdot(wi, I.F.n) / pdf;
+            beta *= (is_catcher<EXT>(I) ? f * catcher_sky<EXT>(S, I) : f) * absdot(wi, I.F.n) / pdf;
             if (!(I.mtype & kTransparentMat) && dot(wi, I.F.ng) < 0.0f) {
                 st = kFinishing;
             } else if (bounce >= S.rr) {
@@ -484,6 +638,26 @@ __global__ void __launch_bounds__(256, NB_SHADE_MIN_BLOCKS) wf_shade(WfDev W, ui
     }
 }
 
+// Sort level 3: bucket of every shadow queue entry (grid-stride over the
+// queue length the shade stage left), then, after wf_bucket_scan, its place
+// in bucket order.
+template <bool MULTI>
+__global__ void wf_shadow_key(WfDev W, DevScene S1) {
+    const uint32_t n = W.counters[kCntShadow];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 so = W.sh_o[i], sd = W.sh_d[i];
+        const DevScene& S = MULTI ? W.scenes[W.frames[fbits(W.o[W.qshadow[i] >> 1].w)].scene] : S1;
+        const uint32_t key = ray_bucket(S, f3(so.x, so.y, so.z), f3(sd.x, sd.y, sd.z));
+        W.sh_key[i] = key;
+        bucket_add(W.bkt_cnt, key);
+    }
+}
+__global__ void wf_shadow_scatter(WfDev W) {
+    const uint32_t n = W.counters[kCntShadow];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        W.sh_perm[bucket_add(W.bkt_off, W.sh_key[i])] = i;
+}
+
 // Any hit for each queued shadow ray; a blocked one cancels its pending
 // contribution.  Each warp takes the next 32 queue entries when it is done
 // with its last ones, so warps that drew long rays do not hold up the launch
@@ -505,9 +679,10 @@ __global__ void __launch_bounds__(NB_TRAV_THREADS, NB_TRAV_MIN_BLOCKS) wf_shadow
 #else
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
 #endif
-        const uint32_t e = W.qshadow[i];
+        const uint32_t q = W.level >= 3 ? W.sh_perm[i] : i;
+        const uint32_t e = W.qshadow[q];
         const uint32_t slot = e >> 1;
-        const float4 so = W.sh_o[i], sd = W.sh_d[i];
+        const float4 so = W.sh_o[q], sd = W.sh_d[q];
         const DevScene& S = slot_scene<ISECT, MULTI>(W, S1, MULTI ? fbits(W.o[slot].w) : 0u);
         const float3 o = f3(so.x, so.y, so.z), d = f3(sd.x, sd.y, sd.z);
         bool occ;
@@ -540,6 +715,8 @@ __global__ void wf_check(WfDev W, uint32_t* go_out, uint32_t conditional) {
     if (!go) W.rays[2] += *W.work_next < W.total ? *W.work_next : W.total;
     for (int k = 0; k <= kCntActive; ++k) c[k] = 0u;
     c[kCntTake] = 0u;
+    c[kCntCam] = 0u;
+    c[kCntTakeExt] = 0u;
     if (conditional)
         cudaGraphSetConditional(W.cond, go ? 1u : 0u);
     else
@@ -611,10 +788,14 @@ static int wf_ensure(Context& C, uint32_t cap) {
         (rc = wf_alloc(S, (void**)&W.qshade, kKinds * n * 4)) || (rc = wf_alloc(S, (void**)&W.qshadow, 2 * n * 4)) ||
         (rc = wf_alloc(S, (void**)&W.sh_o, 2 * n * 16)) || (rc = wf_alloc(S, (void**)&W.sh_d, 2 * n * 16)) ||
         (rc = wf_alloc(S, (void**)&W.counters, kCntWords * 4)) || (rc = wf_alloc(S, (void**)&W.work_next, 16)) ||
-        (rc = wf_alloc(S, (void**)&W.rays, 32)))
+        (rc = wf_alloc(S, (void**)&W.rays, 32)) || (rc = wf_alloc(S, (void**)&W.bkt_cnt, kBuckets * 4)) ||
+        (rc = wf_alloc(S, (void**)&W.bkt_off, kBuckets * 4)) || (rc = wf_alloc(S, (void**)&W.sh_key, 2 * n * 4)) ||
+        (rc = wf_alloc(S, (void**)&W.sh_perm, 2 * n * 4)) || (rc = wf_alloc(S, (void**)&W.ext_key, n * 4)) ||
+        (rc = wf_alloc(S, (void**)&W.ext_perm, 2 * n * 4)))
         return rc;
     cudaError_t e = cudaMalloc((void**)&S.active_host_dev, 16);
     if (e == cudaSuccess) e = cudaMemset(W.rays, 0, 32);
+    if (e == cudaSuccess) e = cudaMemset(W.bkt_cnt, 0, kBuckets * 4);
     if (e != cudaSuccess) return cuda_fail(e, "wavefront buffers");
     S.cap = cap;
     return NOOR_OK;
@@ -629,9 +810,12 @@ struct WfLaunch {
     uint32_t grid_queue;    // grid-stride stages
     WfTravKernel extend;
     WfTravKernel shadow;
+    WfTravKernel ext_key;      // sort level 2
+    WfTravKernel shadow_key;   // sort level 3
     DevScene scene;         // the launch's scene when every frame uses the same one
     bool ext;               // some frame's scene has extra lobes or lights
     bool ext_lights;        // ... has sphere, disk, point, spot or distant lights
+    bool env_ref;           // ... samples its environment as the reference does
 };
 
 // one iteration; with `ev` (6 events), records ev[0] before the first stage
@@ -642,18 +826,30 @@ static cudaError_t wf_iteration(const WfDev& W, const WfLaunch& L, cudaStream_t 
     if (ev) cudaEventRecord(ev[0], s);
     wf_regen<<<(W.cap + kRegenBlock - 1) / kRegenBlock, kRegenBlock, 0, s>>>(W);
     if (ev) cudaEventRecord(ev[1], s);
-    L.extend<<<L.grid_slots, L.block, L.smem, s>>>(W, L.scene);
+    if (W.level >= 2) {
+        L.ext_key<<<(W.cap + kBinBlock - 1) / kBinBlock, kBinBlock, 0, s>>>(W, L.scene);
+        wf_bucket_scan<<<1, kScanThreads, 0, s>>>(W);
+        wf_ext_scatter<<<(W.cap + kBinBlock - 1) / kBinBlock, kBinBlock, 0, s>>>(W);
+        L.extend<<<L.grid_queue, L.block, L.smem, s>>>(W, L.scene);
+    } else {
+        L.extend<<<L.grid_slots, L.block, L.smem, s>>>(W, L.scene);
+    }
     if (ev) cudaEventRecord(ev[2], s);
     wf_bin<<<(W.cap + kBinBlock - 1) / kBinBlock, kBinBlock, 0, s>>>(W);
     const int nk = W.sort ? kKinds : 1;
     for (int k = 0; k < nk; ++k) {
         // sorted queues 0 and 1 hold Lambert and conductor hits only
-        if (L.ext && !(W.sort && k < 2 && !L.ext_lights))
+        if (L.ext && !(W.sort && k < 2 && !L.ext_lights && !L.env_ref))
             wf_shade<true><<<L.grid_queue, 256, 0, s>>>(W, (uint32_t)k);
         else
             wf_shade<false><<<L.grid_queue, 256, 0, s>>>(W, (uint32_t)k);
     }
     if (ev) cudaEventRecord(ev[3], s);
+    if (W.level >= 3) {
+        L.shadow_key<<<L.grid_queue, 256, 0, s>>>(W, L.scene);
+        wf_bucket_scan<<<1, kScanThreads, 0, s>>>(W);
+        wf_shadow_scatter<<<L.grid_queue, 256, 0, s>>>(W);
+    }
     L.shadow<<<L.grid_queue, L.block, L.smem, s>>>(W, L.scene);
     if (ev) cudaEventRecord(ev[4], s);
     wf_check<<<1, 1, 0, s>>>(W, go_out, conditional ? 1u : 0u);
@@ -748,7 +944,8 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
     W.scenes = WS.scenes_dev;
     W.nframes = n_frames;
     W.cap = cap;
-    W.sort = P.sort_granularity ? 1u : 0u;
+    W.level = std::min<uint32_t>(P.sort_granularity, 3u);
+    W.sort = W.level ? 1u : 0u;
     W.total = total;
     W.stack_cap = stack_cap;
     // every slot finishes within max_bounces iterations of starting; a slot
@@ -763,12 +960,13 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
     L.grid_queue = (uint32_t)std::max(1, C.sm_count) * 16;
     const uint32_t scene0 = frames[0].scene_id;
     bool multi = false, mixed = false;
-    L.ext = L.ext_lights = false;
+    L.ext = L.ext_lights = L.env_ref = false;
     for (uint32_t i = 0; i < n_frames; ++i) {
         const DevScene& fs = C.scenes[frames[i].scene_id]->dev;
         multi |= frames[i].scene_id != scene0;
         mixed |= fs.isect != C.scenes[scene0]->dev.isect;
-        L.ext |= fs.ext_lobes != 0u || fs.ext_lights != 0u;
+        L.ext |= fs.ext_lobes != 0u || fs.ext_lights != 0u || fs.env_ref != 0u;
+        L.env_ref |= fs.env_ref != 0u;
         L.ext_lights |= fs.ext_lights != 0u;
     }
     L.scene = C.scenes[scene0]->dev;
@@ -788,6 +986,8 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
         else NB_TRAV(NOOR_ISECT_REF_WALD, false);
     }
 #undef NB_TRAV
+    L.shadow_key = multi ? wf_shadow_key<true> : wf_shadow_key<false>;
+    L.ext_key = multi ? wf_ext_key<true> : wf_ext_key<false>;
     for (WfTravKernel k : {L.extend, L.shadow}) {
         e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem);
         if (e != cudaSuccess) return cuda_fail(e, "wavefront smem");
@@ -802,7 +1002,7 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
         uint64_t scene_hash = 1469598103934665603ull;  // FNV-1a over the scene parameter's bytes
         for (size_t b = 0; b < sizeof(DevScene); ++b)
             scene_hash = (scene_hash ^ reinterpret_cast<const unsigned char*>(&L.scene)[b]) * 1099511628211ull;
-        const uint64_t key[10] = {(uint64_t)W.cap | (uint64_t)W.sort << 32 | (uint64_t)L.ext << 33, W.total,
+        const uint64_t key[10] = {(uint64_t)W.cap | (uint64_t)W.level << 32 | (uint64_t)L.ext << 36, W.total,
                                   (uint64_t)W.max_iters | (uint64_t)W.nframes << 32,
                                   (uint64_t)(uint32_t)W.stack_cap | (uint64_t)L.block << 32,
                                   (uint64_t)L.smem, (uint64_t)L.grid_slots | (uint64_t)L.grid_queue << 32,
@@ -858,7 +1058,7 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
             for (auto& x : ev)
                 if (e == cudaSuccess) e = cudaEventCreate(&x);
         }
-        const uint32_t nk = W.sort ? kKinds : 1;
+        const uint32_t nk = (W.sort ? kKinds : 1) + (W.level >= 2 ? 3 : 0) + (W.level >= 3 ? 3 : 0);
         for (uint32_t it = 0; e == cudaSuccess && it < W.max_iters && active; ++it) {
             e = wf_iteration(W, L, s, false, WS.active_host_dev, prof ? ev : nullptr);
             if (e == cudaSuccess) e = cudaMemcpyAsync(&active, WS.active_host_dev, 4, cudaMemcpyDeviceToHost, s);
@@ -869,7 +1069,10 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
                     float ms = 0.0f;
                     cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
                     prof->ms[k] += ms;
-                    prof->launches[k] += k == 2 ? nk + 1 : 1u;
+                    const uint32_t kinds = W.sort ? kKinds : 1u;
+                    prof->launches[k] += k == 1 ? (W.level >= 2 ? 4u : 1u)
+                                       : k == 2 ? kinds + 1u
+                                       : k == 3 ? (W.level >= 3 ? 4u : 1u) : 1u;
                 }
                 ++prof->iterations;
             }
@@ -888,7 +1091,9 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
     // iterations actually run (for the launch count)
     uint32_t iters = 0;
     cudaMemcpy(&iters, W.counters + kCntIter, 4, cudaMemcpyDeviceToHost);
-    if (P.use_graph) C.launches += (uint64_t)iters * (5 + (W.sort ? kKinds : 1)) - (uint64_t)W.max_iters;
+    if (P.use_graph)
+        C.launches += (uint64_t)iters * (5 + (W.sort ? kKinds : 1) + (W.level >= 2 ? 3 : 0) + (W.level >= 3 ? 3 : 0)) -
+                      (uint64_t)W.max_iters;
     return NOOR_OK;
 }
 
@@ -943,35 +1148,57 @@ extern "C" int noor_wavefront_counters(uint64_t counters[3], int reset) {
     return NOOR_OK;
 }
 
-// Autotuner: renders the batch with each candidate (block size x slot count
-// x material sort) and keeps the fastest by device time.
+// Autotuner: coordinate descent on the launch parameters, each candidate
+// timed by one device-timed render of the batch: the slot count first
+// (2^18 .. 2^23, none beyond twice the batch's paths), then the block size
+// (32, 64, 128), then the sort granularity (0 .. 3), then the slot count
+// again around the sort level chosen; the fastest seen wins.
 extern "C" int noor_wavefront_autotune(const noor_wf_frame* frames, uint32_t n_frames, noor_wf_params* best,
                                        float* best_ms) {
     Context* C;
     int rc = need_ctx(C);
     if (rc) return rc;
     if (!best) return set_error(NOOR_ERR_INVALID, "autotune: best is null");
-    // slot counts beyond twice the batch's paths only add empty sweeps
     unsigned long long paths = 0;
     for (uint32_t i = 0; i < n_frames && frames; ++i)
         paths += (unsigned long long)frames[i].width * frames[i].height * frames[i].spp;
-    const uint32_t blocks[] = {64, 128};
-    const uint32_t caps[] = {1u << 18, 1u << 20, 1u << 21, 1u << 22, 1u << 23};
-    const uint32_t sorts[] = {0, 1};
+    std::vector<uint32_t> caps;
+    for (uint32_t c = 1u << 18; c <= (1u << 23); c <<= 1)
+        if (c == (1u << 18) || c <= 2 * paths) caps.push_back(c);
+    noor_wf_params bp{128, caps.back() >= (1u << 22) ? (1u << 22) : caps.back(), 1, best->use_graph};
     float bms = 3.4e38f;
-    noor_wf_params bp{128, 1u << 20, 1, best->use_graph};
-    for (uint32_t b : blocks)
-        for (uint32_t c : caps)
-            for (uint32_t so : sorts) {
-                if (c != caps[0] && c > 2 * paths) continue;
-                noor_wf_params p{b, c, so, best->use_graph};
-                float ms = 0.0f;
-                if ((rc = wavefront_render(*C, frames, n_frames, p, &ms))) return rc;
-                if (ms < bms) {
-                    bms = ms;
-                    bp = p;
-                }
-            }
+    auto trial = [&](const noor_wf_params& p) -> int {
+        float ms = 0.0f;
+        int r = wavefront_render(*C, frames, n_frames, p, &ms);
+        if (r) return r;
+        if (ms < bms) {
+            bms = ms;
+            bp = p;
+        }
+        return NOOR_OK;
+    };
+    for (uint32_t c : caps) {
+        noor_wf_params p = bp;
+        p.queue_capacity = c;
+        if ((rc = trial(p))) return rc;
+    }
+    for (uint32_t b : {32u, 64u, 128u}) {
+        noor_wf_params p = bp;
+        p.block_size = b;
+        if (b != bp.block_size && (rc = trial(p))) return rc;
+    }
+    for (uint32_t so : {0u, 1u, 2u, 3u}) {
+        noor_wf_params p = bp;
+        p.sort_granularity = so;
+        if (so != bp.sort_granularity && (rc = trial(p))) return rc;
+    }
+    const uint32_t c0 = bp.queue_capacity;
+    for (uint32_t c : caps) {
+        if (c != c0 / 2 && c != c0 * 2) continue;
+        noor_wf_params p = bp;
+        p.queue_capacity = c;
+        if ((rc = trial(p))) return rc;
+    }
     *best = bp;
     if (best_ms) *best_ms = bms;
     return NOOR_OK;
