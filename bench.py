@@ -21,6 +21,7 @@ import json
 import os
 import statistics
 import subprocess
+import tempfile
 import sys
 import time
 from pathlib import Path
@@ -45,7 +46,9 @@ METRIC = "Mpaths/s"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default 5; 800 for the room, whose step is ~2 ms, so that the timed "
+                         "region spans the clock sampler's interval)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--integrator", default="wavefront", choices=["megakernel", "wavefront"])
@@ -56,6 +59,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="wavefront: fixed launch parameters")
+    ap.add_argument("--no-rmse", action="store_true", help="skip the RMSE of both integrators against the FP64 oracle")
     ap.add_argument("--wf-block", type=int, default=128)
     ap.add_argument("--wf-slots", type=int, default=1 << 21)
     ap.add_argument("--wf-sort", type=int, default=0)
@@ -65,7 +69,10 @@ def parse():
                          "scene; batched: 64 uneven frames in one wavefront launch against 64 sequential "
                          "megakernel renders; adjoint: forward+backward of the differentiable-rendering "
                          "configuration")
-    return ap.parse_args()
+    a = ap.parse_args()
+    if a.steps is None:
+        a.steps = 800 if a.workload == "room" else 5
+    return a
 
 
 def dist_env():
@@ -105,11 +112,10 @@ class Clocks:
     def __init__(self, index: int):
         self.index = index
         self.p = None
-        self.path = ROOT / "_work" / f"clocks_{os.getpid()}.csv"
+        self.path = Path(tempfile.gettempdir()) / f"noor_b200_clocks_{os.getpid()}.csv"
 
     def __enter__(self):
         try:
-            self.path.parent.mkdir(exist_ok=True)
             self.f = open(self.path, "w")
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
                                        "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
@@ -210,6 +216,48 @@ def profiled_traffic_per_ray():
         return None
     m = re.search(r"dram_bytes_per_ext_ray:\s*([0-9.eE+]+)", TRAFFIC_PROFILE.read_text())
     return float(m.group(1)) if m else None
+
+
+# issue-slot use and SIMT efficiency of wf_extend, from the ncu capture
+# summarised in profiles/wf_extend_sky.md (lines "issue_slots_busy_pct: X",
+# "lanes_active_per_inst: X", "dram_pct_of_peak: X")
+def profiled_issue():
+    import re
+    if not TRAFFIC_PROFILE.exists():
+        return None
+    text = TRAFFIC_PROFILE.read_text()
+    out = {}
+    for k in ("issue_slots_busy_pct", "lanes_active_per_inst", "dram_pct_of_peak", "achieved_occupancy_pct"):
+        m = re.search(k + r":\s*([0-9.eE+]+)", text)
+        if m:
+            out[k] = float(m.group(1))
+    return out or None
+
+
+def rmse_vs_fp64(r, imgs, spp, rows, mult=16):
+    """RMSE of each integrator's image against the FP64 oracle on `rows`
+    (full image rows): on the same seeds (precision: FP32 arithmetic and
+    compensated accumulation) and at mult x the samples (estimator)"""
+    from oracle.oracle import Oracle
+    W = r.w
+    threads = os.cpu_count() or 1
+    orc = Oracle(r.built.payload, r.spec, r.hosek)
+    same, high = [], []
+    for y in rows:
+        same.append(orc.render(r.camera, 1, spp, p0=y * W, p1=(y + 1) * W, fp64=True, threads=threads))
+        high.append(orc.render(r.camera, 1, spp * mult, p0=y * W, p1=(y + 1) * W, fp64=True, threads=threads))
+    orc.close()
+    same, high = np.concatenate(same), np.concatenate(high)
+    sel = lambda img: np.concatenate([img[y] for y in rows])
+    rm = lambda a, b: float(np.sqrt(np.mean((a - b) ** 2)))
+    out = {"rows": rows, "pixels": len(rows) * W, "spp": spp, "reference_spp": spp * mult,
+           "same_seeds": {k: rm(sel(v), same) for k, v in imgs.items()},
+           "at_reference_spp": {k: rm(sel(v), high) for k, v in imgs.items()}}
+    e = out["at_reference_spp"]
+    if len(e) == 2:
+        a, b = e.values()
+        out["estimator_rmse_rel_diff"] = abs(a - b) / max(b, 1e-30)
+    return out
 
 
 def calibrate_pixels(orc, cam, spp, threads, target_s):
@@ -420,9 +468,10 @@ class WavefrontPath:
         from noor_b200 import _capi
         prof = _capi.WfProfile()
         _capi.call("noor_wavefront_profile", self.frames, 1, C.byref(self.params), C.byref(prof))
-        names = ["wf_regen", "wf_extend", "wf_shade", "wf_shadow", "wf_check"]
+        names = ["wf_regen", "extension_ordering", "wf_extend", "wf_shade", "shadow_ordering", "wf_shadow",
+                 "wf_check"]
         stages = {n: {"ms": float(prof.ms[i]), "launches": int(prof.launches[i])} for i, n in enumerate(names)}
-        top = max(range(5), key=lambda i: prof.ms[i])
+        top = max(range(len(names)), key=lambda i: prof.ms[i])
         return names[top], float(prof.ms[top]), int(prof.launches[top]), stages
 
 
@@ -653,10 +702,12 @@ def main():
     value = job_rate(npaths, ms_step, world)
     mrays = job_rate((ext + shadow) / args.steps, ms_step, world)
     compare = None
+    img = path.image()
+    imgs = {path.name: img}
     if other is not None:
-        img = path.image()
         oms, olaunch, oext, oshadow, oclk = timed(other)
         oimg = other.image()
+        imgs[other.name] = oimg
         rel = np.abs(img - oimg) / np.maximum(np.abs(oimg), 1e-2)
         compare = {"integrator": other.name, "value": job_rate(npaths, oms, world), "ms_per_step": oms,
                    "mrays_per_s": job_rate((oext + oshadow) / args.steps, oms, world),
@@ -687,7 +738,9 @@ def main():
     if rank == 0:
         peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
         hbm = peaks.get("hbm_gbs", 6650.0)
-        roof = {"bound": "hbm", "kernel": top_kernel, "achieved": None, "peak": hbm, "unit": "GB/s", "frac": None,
+        roof = {"bound": "hbm", "limiter": "issue and divergence: the traversal's node reads hit L1/L2 and DRAM "
+                                           "runs at a few per cent of peak (issue block)",
+                "kernel": top_kernel, "achieved": None, "peak": hbm, "unit": "GB/s", "frac": None,
                 "traffic": None, "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                 "kernel_ms_per_step": top_ms, "kernel_launches_per_step": top_launches,
                 "kernel_share_of_step": top_ms / sum(v["ms"] for v in stages.values()) if stages else 1.0,
@@ -708,10 +761,17 @@ def main():
                 alg = per_path * npaths
                 traffic = None
             achieved = alg / (top_ms / 1000) / 1e9
+            if top_kernel == "wf_extend" and args.workload == "sky":
+                roof["issue"] = profiled_issue()
             roof.update(achieved=achieved, frac=achieved / hbm, traffic=traffic,
                         algorithmic_bytes_per_launch=alg / top_launches, algorithmic_bytes_per_path=per_path,
                         **counts)
             cpu = cpu_baseline(args, s, built, r.spec, r.hosek, r.camera, args.cpu_seconds)
+        rmse = None
+        if not args.no_rmse:
+            h = path.h
+            rows = list(range(h)) if args.workload == "room" else [int(h * (k + 1) / 5) for k in range(4)]
+            rmse = rmse_vs_fp64(r, imgs, args.spp, rows)
         line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator, random-init sky)",
@@ -723,7 +783,7 @@ def main():
                            "parallelism": f"replicas{world}", "bvh_build_s": round(build_s, 2), "bvh_build": bvh_build,
                            **path.describe()},
                 "mrays_per_s": mrays, "rays_per_step": (ext + shadow) / args.steps, "ext_rays_per_step": ext / args.steps,
-                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "rmse_vs_fp64": rmse,
                 "gpu_launches": launches, "clocks": clocks, "other_integrator": compare}
         print(json.dumps(line), flush=True)
     r.close()

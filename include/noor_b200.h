@@ -621,6 +621,10 @@ typedef struct noor_wf_params {
                                  * grid)); 3 also shadow rays, by the same
                                  * sort; larger values act as 3             */
     uint32_t use_graph;         /* capture one bounce as a CUDA graph       */
+    uint32_t max_iterations;    /* bound of the bounce loop; 0: enough for
+                                 * every path (slots x bounces); a loop that
+                                 * reaches it stops and sets
+                                 * NOOR_DEV_WAIT_TIMEOUT                    */
 } noor_wf_params;
 
 /* Scenes for the wavefront live in the current context; scene 0 is the one
@@ -636,11 +640,13 @@ int noor_wavefront_render_timed(const noor_wf_frame* frames, uint32_t n_frames,
 int noor_wavefront_counters(uint64_t counters[3], int reset);
 /* Device time per stage of one wavefront render, for measurement: the batch
  * is rendered in the host-loop form (use_graph ignored) with CUDA events
- * around every stage launch.  Stages: 0 regen, 1 extend, 2 shade (queue
- * binning and all material kinds), 3 shadow, 4 stop test. */
+ * around every stage.  Stages: 0 regen, 1 extension-ray ordering (sort
+ * granularity 2 and up), 2 extend, 3 shade (queue binning and all material
+ * kinds), 4 shadow-ray ordering (sort granularity 3), 5 shadow, 6 stop
+ * test. */
 typedef struct noor_wf_profile {
-    float ms[5];                /* summed over iterations                   */
-    uint32_t launches[5];
+    float ms[7];                /* summed over iterations                   */
+    uint32_t launches[7];
     uint32_t iterations;
 } noor_wf_profile;
 int noor_wavefront_profile(const noor_wf_frame* frames, uint32_t n_frames,
@@ -658,9 +664,12 @@ int noor_megakernel_batch(const noor_wf_frame* frames, uint32_t n_frames,
  * array of NOOR_NOALLOC_SCRATCH_BYTES, which bounds a frame to
  * NOOR_NOALLOC_SCRATCH_BYTES / 16 pixels (larger frames return
  * NOOR_ERR_CAPACITY).  The first call on a device looks up the array's
- * address (cudaGetSymbolAddress); make it before any stream capture.  All
- * calls on a device share the array, so calls that overlap on the GPU race;
- * nothing in it needs clearing between calls. */
+ * address (cudaGetSymbolAddress); make it before any stream capture.
+ * device_free_memory forgets the address, so the first call after it (and
+ * after any reset of the device) looks it up again.  A call waits for its
+ * work to finish before it returns.  All calls on a device share the array,
+ * so calls that overlap on the GPU race; nothing in it needs clearing
+ * between calls. */
 #define NOOR_NOALLOC_SCRATCH_BYTES (32u << 20)
 int noor_megakernel_frame_noalloc(const noor_wf_frame* frame);
 /* Project-written autotuner: coordinate descent on the launch parameters,

@@ -44,7 +44,7 @@ NOOR_ENV_FP64, NOOR_ENV_REFERENCE = 0, 1
 NOOR_SHAPE_QUAD, NOOR_SHAPE_SPHERE, NOOR_SHAPE_DISK = 0, 1, 2
 NOOR_CAMERA_PERSP, NOOR_CAMERA_ORTHO, NOOR_CAMERA_ENV = 0, 1, 2
 NOOR_TONEMAP_NONE, NOOR_TONEMAP_GAMMA, NOOR_TONEMAP_REINHARD, NOOR_TONEMAP_FILMIC, NOOR_TONEMAP_UNCHARTED2 = -1, 0, 1, 2, 3
-NOOR_DEV_STACK_OVERFLOW = 1
+NOOR_DEV_STACK_OVERFLOW, NOOR_DEV_QUEUE_OVERFLOW, NOOR_DEV_WAIT_TIMEOUT, NOOR_DEV_BAD_INDEX = 1, 2, 4, 8
 
 TRI_LEAF_MASK = 0x80000000
 MESH_LEAF_MASK = 0x40000000
@@ -178,11 +178,12 @@ class WfFrame(C.Structure):
 
 
 class WfParams(C.Structure):
-    _fields_ = [("block_size", u32), ("queue_capacity", u32), ("sort_granularity", u32), ("use_graph", u32)]
+    _fields_ = [("block_size", u32), ("queue_capacity", u32), ("sort_granularity", u32), ("use_graph", u32),
+                ("max_iterations", u32)]
 
 
 class WfProfile(C.Structure):
-    _fields_ = [("ms", f32 * 5), ("launches", u32 * 5), ("iterations", u32)]
+    _fields_ = [("ms", f32 * 7), ("launches", u32 * 7), ("iterations", u32)]
 
 
 class AdjointDesc(C.Structure):

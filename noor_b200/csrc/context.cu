@@ -731,6 +731,7 @@ extern "C" int debug_skydome(unsigned int* frame_count, int width, int height) {
 extern "C" int device_free_memory(void) {
     if (!tl_ctx) return NOOR_OK;
     cudaSetDevice(tl_ctx->device);
+    noalloc_forget(tl_ctx->device);
     delete tl_ctx;
     tl_ctx = nullptr;
     return NOOR_OK;

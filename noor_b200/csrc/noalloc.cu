@@ -10,7 +10,10 @@
 //
 // Set-up: the first call on a device (with that device current) looks up the
 // array's device address with cudaGetSymbolAddress; make that first call
-// before any stream capture.  Every later call reuses the address.
+// before any stream capture.  Every later call reuses the address, until
+// device_free_memory on that device forgets it (a caller that resets the
+// device afterwards gets a fresh look-up on its next first call).  A call
+// waits for its own work to finish before it returns.
 //
 // Sharing: all calls on a device use the same array, and it keeps the last
 // call's contents.  Nothing in it has to start at zero: every element a call
@@ -32,6 +35,14 @@ static std::mutex g_noalloc_mutex;
 static float4* g_noalloc_ptr[kNoAllocMaxDevices] = {};
 
 // device address of the scratch array on the current device (looked up once)
+// the cached scratch address of a device is dropped with a render context
+// of that device (device_free_memory)
+void noalloc_forget(int device) {
+    if (device < 0 || device >= kNoAllocMaxDevices) return;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    g_noalloc_ptr[device] = nullptr;
+}
+
 static int noalloc_scratch(int device, float4** out) {
     if (device < 0 || device >= kNoAllocMaxDevices)
         return set_error(NOOR_ERR_UNSUPPORTED, "no-alloc render: device index beyond 63");
@@ -76,7 +87,10 @@ extern "C" int noor_megakernel_frame_noalloc(const noor_wf_frame* f) {
     S.film_mode = NOOR_FILM_KAHAN;
     const DevCamera cam = dev_camera(f->camera, f->width, f->height);
     // same split of the samples as the batch megakernel, reduced until the
-    // partial films (2 x chunks x pixels) fit beside the compensation film
+    // partial films (2 x chunks x pixels) fit beside the compensation film.
+    // With 148 SMs the split asks for more than one chunk only below
+    // 151,552 pixels, where 1 + 2 x chunks films stay far inside the array:
+    // the loop is a guard for GPUs with many more SMs.
     const uint64_t target = (uint64_t)C->sm_count * 1024u;
     uint64_t chunks = std::min<uint64_t>(f->spp, std::max<uint64_t>(1, (target + npix - 1) / npix));
     while (chunks > 1 && npix * (1 + 2 * chunks) > kNoAllocElems) --chunks;

@@ -69,5 +69,6 @@ int need_ctx(Context*& C);
 int sync_and_check(Context& C, const char* what);
 int render_frames(Context& C, uint32_t frame0, uint32_t n);
 void wavefront_release(Context& C);
+void noalloc_forget(int device);  // noalloc.cu
 
 }  // namespace nb

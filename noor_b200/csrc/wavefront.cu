@@ -84,6 +84,7 @@ enum : int {
 // same way.  The bucket of each ray is computed on the device and the
 // counts, offsets and permutation never leave it (the pass runs inside the
 // graph's loop).
+constexpr int kWfStages = 7;  // noor_wf_profile's stages
 constexpr int kCellBits = 4;
 constexpr int kBuckets = 8 << (3 * kCellBits);
 constexpr int kScanThreads = 1024;
@@ -818,9 +819,9 @@ struct WfLaunch {
     bool env_ref;           // ... samples its environment as the reference does
 };
 
-// one iteration; with `ev` (6 events), records ev[0] before the first stage
-// and ev[k + 1] after stage k (regen, extend, shade with its queue binning,
-// shadow, stop test)
+// one iteration; with `ev` (kWfStages + 1 events), records ev[0] before the
+// first stage and ev[k + 1] after stage k (regen, extension ordering,
+// extend, shade with its queue binning, shadow ordering, shadow, stop test)
 static cudaError_t wf_iteration(const WfDev& W, const WfLaunch& L, cudaStream_t s, bool conditional,
                                 uint32_t* go_out, cudaEvent_t* ev = nullptr) {
     if (ev) cudaEventRecord(ev[0], s);
@@ -830,11 +831,13 @@ static cudaError_t wf_iteration(const WfDev& W, const WfLaunch& L, cudaStream_t 
         L.ext_key<<<(W.cap + kBinBlock - 1) / kBinBlock, kBinBlock, 0, s>>>(W, L.scene);
         wf_bucket_scan<<<1, kScanThreads, 0, s>>>(W);
         wf_ext_scatter<<<(W.cap + kBinBlock - 1) / kBinBlock, kBinBlock, 0, s>>>(W);
-        L.extend<<<L.grid_queue, L.block, L.smem, s>>>(W, L.scene);
-    } else {
-        L.extend<<<L.grid_slots, L.block, L.smem, s>>>(W, L.scene);
     }
     if (ev) cudaEventRecord(ev[2], s);
+    if (W.level >= 2)
+        L.extend<<<L.grid_queue, L.block, L.smem, s>>>(W, L.scene);
+    else
+        L.extend<<<L.grid_slots, L.block, L.smem, s>>>(W, L.scene);
+    if (ev) cudaEventRecord(ev[3], s);
     wf_bin<<<(W.cap + kBinBlock - 1) / kBinBlock, kBinBlock, 0, s>>>(W);
     const int nk = W.sort ? kKinds : 1;
     for (int k = 0; k < nk; ++k) {
@@ -844,16 +847,17 @@ static cudaError_t wf_iteration(const WfDev& W, const WfLaunch& L, cudaStream_t 
         else
             wf_shade<false><<<L.grid_queue, 256, 0, s>>>(W, (uint32_t)k);
     }
-    if (ev) cudaEventRecord(ev[3], s);
+    if (ev) cudaEventRecord(ev[4], s);
     if (W.level >= 3) {
         L.shadow_key<<<L.grid_queue, 256, 0, s>>>(W, L.scene);
         wf_bucket_scan<<<1, kScanThreads, 0, s>>>(W);
         wf_shadow_scatter<<<L.grid_queue, 256, 0, s>>>(W);
     }
-    L.shadow<<<L.grid_queue, L.block, L.smem, s>>>(W, L.scene);
-    if (ev) cudaEventRecord(ev[4], s);
-    wf_check<<<1, 1, 0, s>>>(W, go_out, conditional ? 1u : 0u);
     if (ev) cudaEventRecord(ev[5], s);
+    L.shadow<<<L.grid_queue, L.block, L.smem, s>>>(W, L.scene);
+    if (ev) cudaEventRecord(ev[6], s);
+    wf_check<<<1, 1, 0, s>>>(W, go_out, conditional ? 1u : 0u);
+    if (ev) cudaEventRecord(ev[7], s);
     return cudaGetLastError();
 }
 
@@ -952,6 +956,7 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
     // starts at least every iteration while work remains
     W.max_iters = (uint32_t)std::min<unsigned long long>(
         (total + cap - 1) / cap * (max_bounces + 2) + 4 * (max_bounces + 2) + 64, 1u << 30);
+    if (P.max_iterations) W.max_iters = std::min(W.max_iters, P.max_iterations);
 
     WfLaunch L;
     L.block = (int)block;
@@ -1052,7 +1057,7 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
         // host loop: one iteration per launch sequence, reading the active
         // count back every iteration (bounded by the iteration cap)
         uint32_t active = 1;
-        cudaEvent_t ev[6] = {};
+        cudaEvent_t ev[kWfStages + 1] = {};
         if (prof) {
             std::memset(prof, 0, sizeof(*prof));
             for (auto& x : ev)
@@ -1065,14 +1070,14 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
             if (e == cudaSuccess) e = cudaStreamSynchronize(s);
             C.launches += 5 + nk;
             if (prof && e == cudaSuccess) {
-                for (int k = 0; k < 5; ++k) {
+                const uint32_t kinds = W.sort ? kKinds : 1u;
+                const uint32_t launches[kWfStages] = {1u, W.level >= 2 ? 3u : 0u, 1u, kinds + 1u,
+                                                      W.level >= 3 ? 3u : 0u, 1u, 1u};
+                for (int k = 0; k < kWfStages; ++k) {
                     float ms = 0.0f;
                     cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
                     prof->ms[k] += ms;
-                    const uint32_t kinds = W.sort ? kKinds : 1u;
-                    prof->launches[k] += k == 1 ? (W.level >= 2 ? 4u : 1u)
-                                       : k == 2 ? kinds + 1u
-                                       : k == 3 ? (W.level >= 3 ? 4u : 1u) : 1u;
+                    prof->launches[k] += launches[k];
                 }
                 ++prof->iterations;
             }

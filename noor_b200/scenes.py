@@ -21,7 +21,9 @@ from . import _capi as capi
 GOLD_ETA = (0.126052, 0.465040, 1.340442)   # Au, as in the reference's material presets
 GOLD_K = (4.230981, 2.204432, 1.642458)
 DEFAULT_BVH = dict(num_bins=16, max_height=32, Ci=1.0, Ct=0.125, min_leaf_tris=2, max_leaf_tris=4)
-HOSEK_DATASET = Path(__file__).resolve().parent.parent / "tests" / "golden" / "hosek_rgb_dataset.npy"
+# the Hosek-Wilkie RGB tables (BSD-3, data/HOSEK_WILKIE_LICENSE), written by
+# data/make_hosek_data.py from the model's published data header
+HOSEK_DATASET = Path(__file__).resolve().parent / "data" / "hosek_rgb.npy"
 
 IDENTITY = np.eye(4, dtype=np.float32).reshape(-1, order="F")
 
@@ -634,9 +636,9 @@ def make_camera(cam: dict) -> capi.Camera:
 
 def hosek_dataset() -> np.ndarray:
     """RGB coefficient and radiance tables of the Hosek-Wilkie model
-    (3 x 1080 + 3 x 120 floats), stored as a test fixture."""
+    (3 x 1080 + 3 x 120 floats), the package's data file."""
     if not HOSEK_DATASET.exists():
-        raise FileNotFoundError(f"{HOSEK_DATASET} missing (generate with tests/golden/make_golden.py)")
+        raise FileNotFoundError(f"{HOSEK_DATASET} missing (generate with noor_b200/data/make_hosek_data.py)")
     return np.load(HOSEK_DATASET).astype(np.float32)
 
 
@@ -745,5 +747,6 @@ def wf_frame(scene_id: int, cam: dict, spp: int, bounces: int = 0, first_frame: 
     return f
 
 
-def wf_params(block: int = 128, capacity: int = 1 << 20, sort: int = 1, graph: int = 1) -> capi.WfParams:
-    return capi.WfParams(block, capacity, sort, graph)
+def wf_params(block: int = 128, capacity: int = 1 << 20, sort: int = 1, graph: int = 1,
+              max_iterations: int = 0) -> capi.WfParams:
+    return capi.WfParams(block, capacity, sort, graph, max_iterations)

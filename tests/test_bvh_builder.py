@@ -206,3 +206,11 @@ def test_single_large_mesh_matches_live_reference():
     assert np.array_equal(b.nodes(), nodes)
     assert np.array_equal(b.triangle_order(), order)
     assert (root, height) == (b.payload.bvh_root_node, b.stat.height)
+
+
+def test_hosek_data_file_is_the_reference_table():
+    """the package's Hosek-Wilkie table (parsed from the model's data header
+    by noor_b200/data/make_hosek_data.py) equals the table the reference's
+    compiled model holds (tests/golden/hosek_rgb_dataset.npy)"""
+    golden = np.load(Path(__file__).resolve().parent / "golden" / "hosek_rgb_dataset.npy")
+    assert np.array_equal(scenes.hosek_dataset(), golden)

@@ -59,6 +59,33 @@ def test_noalloc_frames_match_batch_megakernel(sky):
         _compare(A, B)
 
 
+def test_noalloc_single_chunk_1080p_allocates_nothing(sky):
+    """a 1920 x 1080 frame (2,073,600 of the array's 2,097,152 pixels)
+    takes the single-chunk path; two calls in a row match the batch
+    megakernel, and the device's free memory is the same before and after
+    the second call (the first one may still size the kernel's local memory)"""
+    s, r = sky
+    c_ = dict(s.camera, w=1920, h=1080)
+    a = _film(1920, 1080)
+    b = _film(1920, 1080)
+    for first in (1, 7):
+        fa = scenes.wf_frame(0, c_, 2, 4, first_frame=first, d_film=a.data_ptr())
+        fb = scenes.wf_frame(0, c_, 2, 4, first_frame=first, d_film=b.data_ptr())
+        torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info()[0]
+        _capi.call("noor_megakernel_frame_noalloc", C.byref(fa))
+        torch.cuda.synchronize()
+        if first == 7:
+            assert torch.cuda.mem_get_info()[0] == free_before
+        arr = (_capi.WfFrame * 1)(fb)
+        ms = C.c_float()
+        _capi.call("noor_megakernel_batch", arr, 1, C.byref(ms))
+        torch.cuda.synchronize()
+        A, B = a.cpu().numpy()[..., :3], b.cpu().numpy()[..., :3]
+        assert A.mean() > 0.01
+        _compare(A, B)
+
+
 def test_noalloc_rejects_frames_beyond_the_scratch_array(sky):
     s, r = sky
     w = 4096
