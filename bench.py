@@ -294,24 +294,40 @@ def cpu_baseline(args, s, built, spec, hosek, cam, budget_s):
 
 
 def run_reference(args):
+    """The reference arm: the oracle's transcription of the reference's render
+    routines on the host cores, over a payload from the reference's own BVH
+    builder (oracle/_ref/libnoor_ref.so).  The workload's scene generators
+    and struct layouts are loaded without the product package, so the
+    product library is never loaded on this arm."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    from noor_b200 import scenes, _capi
-    from oracle.oracle import Oracle
+    from oracle.oracle import Oracle, RefPayload, camera_lookat, host_modules, ref_available
     if args.workload not in SCENES:
         print(json.dumps({"impl": "reference", "unavailable": f"the reference arm times the single-frame "
                           f"workloads ({', '.join(SCENES)}); the reference has no {args.workload} path"}))
         return
-    s, built, _ = build_scene(args)
+    if not ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libnoor_ref.so (the reference's own "
+                          "builder) was not built: the reference tree was absent at build time"}))
+        return
+    capi, scenes = host_modules()
+    fn, (w0, h0), _ = SCENES[args.workload]
+    kw = dict(width=int(round(w0 * args.scale)), height=int(round(h0 * args.scale)))
+    if args.spp:
+        kw["spp"] = args.spp
+    s = getattr(scenes, fn)(**kw)
+    args.spp = s.render["spp"]
+    built = RefPayload(s, capi, scenes)
     spec = built.default_spec(s.render["bounces"], s.render.get("rr", 1))
     spec.mis = int(s.render.get("mis", 0))
-    cam = scenes.make_camera(s.camera)
-    hosek = reference_hosek(s.hosek) if s.hosek is not None else _capi.HosekSky()
+    cam = camera_lookat(capi, s.camera)
+    hosek = reference_hosek(capi, s.hosek) if s.hosek is not None else capi.HosekSky()
     orc = Oracle(built.payload, spec, hosek)
     threads = os.cpu_count() or 1
     n = cam.w * cam.h
-    npx = calibrate_pixels(orc, cam, args.spp, threads, 3.0)   # ~3 s of CPU work per step
+    # up to ~3 s of CPU work per step, the whole run within about 2.5 minutes
+    npx = calibrate_pixels(orc, cam, args.spp, threads, max(0.05, min(3.0, 150.0 / (args.steps + args.warmup))))
     times = []
     for i in range(args.warmup + args.steps):
         p0 = (n // 2 + i * npx) % max(1, n - npx)
@@ -320,12 +336,14 @@ def run_reference(args):
         if i >= args.warmup:
             times.append(time.time() - t)
     orc.close()
+    built.free()
     ms = 1000 * statistics.mean(times)
     v = npx * args.spp / (ms / 1000) / 1e6
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": SCENES[args.workload][2], "sample_per_step": f"{npx} pixels x {args.spp} spp"},
+            "config": {"workload": SCENES[args.workload][2], "sample_per_step": f"{npx} pixels x {args.spp} spp",
+                       "payload": "the reference's own BVH builder and Wald records (oracle/_ref)"},
             "cpu_baseline": {"value": v, "unit": METRIC, "cores": threads, "kind": "port",
                              "sample": f"{npx} pixels x {args.spp} spp per step, FP32 transcription of the "
                                        "reference's device routines (the reference has no CPU render path)"},
@@ -333,18 +351,16 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def reference_hosek(h):
-    """Hosek sky for the reference arm from the reference's own fit
-    (arhosek_rgb_skymodelstate_alloc_update outputs frozen in
-    tests/golden/hosek_states.npz) and HosekSky::update's sun fields
-    (noor/header/hosek.h:61-83)."""
-    from noor_b200 import _capi
-    g = np.load(ROOT / "tests" / "golden" / "hosek_states.npz")
-    elev = np.pi / 2 - h["sun_lat"]
-    k = int(np.argmin(np.abs(g["cases"] - np.array([h["turbidity"], h["albedo"], elev])).sum(1)))
-    st = g["states"][k]
-    out = _capi.HosekSky()
+def reference_hosek(capi, h):
+    """Hosek sky for the reference arm as HosekSky::update sets it
+    (noor/header/hosek.h:61-83): the reference's own fit,
+    arhosek_rgb_skymodelstate_alloc_update, per colour channel's ground
+    albedo (oracle/_ref/libnoor_ref.so), and the sun fields."""
+    from oracle.oracle import ref_hosek_state
+    elev = float(np.pi / 2 - h["sun_lat"])
+    out = capi.HosekSky()
     for i in range(3):
+        st = ref_hosek_state(float(h["turbidity"]), float(h["albedo"]), elev)
         for c in range(3):
             for j in range(9):
                 out.state[i].configs[c][j] = float(st[9 * c + j])

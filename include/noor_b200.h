@@ -316,6 +316,13 @@ typedef struct noor_spec {
 } noor_spec;
 
 /* ------------------------------------------------- reference entry points */
+/* These eight carry the reference's names with C-ABI arguments.  A
+ * translation unit that also sees the reference's own declarations of them
+ * (path_tracer.cuh:136-151, C++ arguments, the same C names) -- the bridge
+ * that replaces path_tracer.cu in the reference's host -- defines
+ * NOOR_B200_NO_REFERENCE_PROTOTYPES before including this header and
+ * resolves the library's versions with dlsym. */
+#ifndef NOOR_B200_NO_REFERENCE_PROTOTYPES
 /* noor/cuda/path_tracer.cuh:137-142: upload payload, sky, camera and spec
  * into a new context that becomes current on this thread.  hosek, camera and
  * spec are remembered (not copied for later): update_cuda_* re-read them, as
@@ -344,6 +351,7 @@ int device_free_memory(void);
 /* path_tracer.cuh:150: hit point of the centre pixel's primary ray from the
  * last frame (w = 1 if it hit, 0 otherwise). */
 int get_lookAt(float look_at[4]);
+#endif /* NOOR_B200_NO_REFERENCE_PROTOTYPES */
 
 /* ------------------------------------------------------------- additions */
 const char* noor_last_error(void);

@@ -25,23 +25,57 @@ __global__ void k_env_func_tex(const float4* env, int w, int h, float* func) {
     func[i] = fmaxf(0.0f, rgb2y(f3(t))) * st;
 }
 
+// querySkyModel (noor/cuda/hosek.cuh:86-101) in FP64, for the distribution
+// below only: a sub-sample within FP32 rounding of the sun disc's edge then
+// falls on the same side on every machine (FP32 arithmetic libraries differ
+// there, and the sun's radiance is 10^4 times the sky's)
+__device__ double hosek_channel_d(const float* c, double theta, double gamma) {
+    const double cg = cos(gamma), cg2 = cg * cg, ct = cos(theta);
+    const double mie = (1.0 + cg2) / pow(1.0 + (double)c[8] * (double)c[8] - 2.0 * (double)c[8] * cg, 1.5);
+    return (1.0 + (double)c[0] * exp((double)c[1] / (ct + (double)0.01f))) *
+           ((double)c[2] + (double)c[3] * exp((double)c[4] * gamma) + (double)c[5] * cg2 + (double)c[6] * mie +
+            (double)c[7] * sqrt(ct));
+}
+__device__ double inverse_gamma_d(double v) {
+    if (v <= (double)0.04045f) return v / (double)12.92f;
+    return pow((v + (double)0.055f) / (double)1.055f, (double)2.4f);
+}
+__device__ double sky_luminance_d(const DevHosek& H, double x, double y, double z) {
+    if (y < 0.0) return 0.0;
+    const double theta = fmin(fmax(acos(fmin(fmax(y, -1.0), 1.0)), 0.0), 3.141592653589793 / 2.0);
+    const double cs = x * (double)H.solar_dir.x + y * (double)H.solar_dir.y + z * (double)H.solar_dir.z;
+    const double gamma = acos(fmin(fmax(cs, -1.0), 1.0));
+    double rgb[3];
+    for (int k = 0; k < 3; ++k) rgb[k] = hosek_channel_d(H.configs[k], theta, gamma) * (double)H.radiance[k];
+    if (gamma < (double)H.solar_radius)
+        for (int k = 0; k < 3; ++k) rgb[k] *= (double)H.solar_scale;
+    else
+        for (int k = 0; k < 3; ++k) rgb[k] = inverse_gamma_d(rgb[k] * (double)0.025f);
+    return (double)0.2126f * rgb[0] + (double)0.7152f * rgb[1] + (double)0.0722f * rgb[2];
+}
+
+// the sky's cells: luminance x sin(theta) averaged over 4 x 4 sub-samples,
+// in FP64, rounded once to FP32
 __global__ void k_env_func_sky(DevHosek H, int w, int h, float* func) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= w * h) return;
     const int row = i / w, col = i % w;
-    float acc = 0.0f;
+    constexpr double pi = 3.141592653589793;
+    double acc = 0.0;
     for (int b = 0; b < 4; ++b) {
-        const float v = ((float)row + ((float)b + 0.5f) * 0.25f) / (float)h;
-        const float theta = v * kPi;
-        const float st = sinf(theta), ct = cosf(theta);
+        const double theta = ((double)row + ((double)b + 0.5) * 0.25) / (double)h * pi;
+        const double st = sin(theta), ct = cos(theta);
         for (int a = 0; a < 4; ++a) {
-            const float u = ((float)col + ((float)a + 0.5f) * 0.25f) / (float)w;
-            const float phi = u * k2Pi;
-            const float3 dir = normalize_fast(f3(st * cosf(phi), ct, st * sinf(phi)));
-            acc += fmaxf(0.0f, rgb2y(hosek_query(H, dir))) * st;
+            const double phi = ((double)col + ((double)a + 0.5) * 0.25) / (double)w * (2.0 * pi);
+            double x = st * cos(phi), y = ct, z = st * sin(phi);
+            const double inv = 1.0 / sqrt(x * x + y * y + z * z);
+            x *= inv;
+            y *= inv;
+            z *= inv;
+            acc += fmax(0.0, sky_luminance_d(H, x, y, z)) * st;
         }
     }
-    func[i] = acc * (1.0f / 16.0f);
+    func[i] = (float)(acc / 16.0);
 }
 
 // Inclusive FP64 block scan of kScanThreads values (Hillis-Steele in smem).

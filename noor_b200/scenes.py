@@ -458,68 +458,73 @@ def _ptr(a: np.ndarray, t=C.c_float):
     return a.ctypes.data_as(C.POINTER(t))
 
 
+def scene_desc(scene: SceneData):
+    """The noor_scene_desc of a scene (the loader output Model::load
+    consumes) and the arrays it points into, which the caller keeps alive
+    while the description is in use.  Builds nothing and needs no library."""
+    s = scene
+    keep = []
+    V = np.ascontiguousarray(s.vertices, np.float32)
+    N = np.ascontiguousarray(s.normals, np.float32)
+    U = np.ascontiguousarray(s.uvs, np.float32)
+    vi = np.ascontiguousarray(s.vindices, np.uint32)
+    ni = np.ascontiguousarray(s.nindices, np.uint32)
+    ui = np.ascontiguousarray(s.uvindices, np.uint32)
+    mi = np.ascontiguousarray(s.material_indices, np.uint32)
+    keep += [V, N, U, vi, ni, ui, mi]
+    meshes = (capi.Mesh * len(s.meshes))()
+    for k, m in enumerate(s.meshes):
+        meshes[k].tri_start = m["tri_start"]
+        meshes[k].tri_count = m["tri_count"]
+        meshes[k].to_global[:] = [float(x) for x in np.asarray(m["to_global"], np.float32)]
+        meshes[k].instance = m.get("instance", -1)
+        meshes[k].light_idx = m.get("light_idx", -1)
+    mats = (capi.MaterialDesc * len(s.materials))()
+    for k, m in enumerate(s.materials):
+        for f, _ in capi.MaterialDesc._fields_:
+            val = m[f]
+            if isinstance(val, (tuple, list, np.ndarray)):
+                getattr(mats[k], f)[:] = [float(x) for x in val]
+            else:
+                setattr(mats[k], f, val)
+    lights = (capi.AreaLight * max(1, len(s.area_lights)))()
+    for k, l in enumerate(s.area_lights):
+        lights[k] = make_area_light(l, k)
+    delta = make_delta_lights(s)
+    d = capi.SceneDesc()
+    d.vertices, d.num_vertices = _ptr(V), V.shape[0]
+    d.normals, d.num_normals = _ptr(N), N.shape[0]
+    d.uvs, d.num_uvs = _ptr(U), U.shape[0]
+    d.vindices, d.nindices, d.uvindices = _ptr(vi, C.c_uint32), _ptr(ni, C.c_uint32), _ptr(ui, C.c_uint32)
+    d.material_indices = _ptr(mi, C.c_uint32)
+    d.num_triangles = vi.shape[0]
+    d.meshes, d.num_meshes = meshes, len(s.meshes)
+    d.materials, d.num_materials = mats, len(s.materials)
+    d.area_lights, d.num_area_lights = lights, len(s.area_lights)
+    d.point_lights, d.num_point_lights = delta[0], len(s.point_lights)
+    d.spot_lights, d.num_spot_lights = delta[1], len(s.spot_lights)
+    d.distant_lights, d.num_distant_lights = delta[2], len(s.distant_lights)
+    d.skydome_type = s.skydome_type
+    if s.env is not None:
+        E = np.ascontiguousarray(s.env, np.float32)
+        keep.append(E)
+        d.env_width, d.env_height, d.env_rgba = E.shape[1], E.shape[0], _ptr(E)
+    b = s.bvh
+    d.bvh = capi.BvhSpec(b["num_bins"], b["max_height"], b["Ci"], b["Ct"], b["min_leaf_tris"], b["max_leaf_tris"])
+    return d, keep + [meshes, mats, lights, delta]
+
+
 class BuiltPayload:
     """Owns a noor_payload_handle (host arrays the library built); `gpu`
     builds the bottom-level trees on the current CUDA device (the same
     bytes)."""
 
     def __init__(self, scene: SceneData, gpu: bool = False):
-        L = capi.lib()
-        s = scene
-        self.scene = s
-        keep = []
-        V = np.ascontiguousarray(s.vertices, np.float32)
-        N = np.ascontiguousarray(s.normals, np.float32)
-        U = np.ascontiguousarray(s.uvs, np.float32)
-        vi = np.ascontiguousarray(s.vindices, np.uint32)
-        ni = np.ascontiguousarray(s.nindices, np.uint32)
-        ui = np.ascontiguousarray(s.uvindices, np.uint32)
-        mi = np.ascontiguousarray(s.material_indices, np.uint32)
-        keep += [V, N, U, vi, ni, ui, mi]
-        meshes = (capi.Mesh * len(s.meshes))()
-        for k, m in enumerate(s.meshes):
-            meshes[k].tri_start = m["tri_start"]
-            meshes[k].tri_count = m["tri_count"]
-            meshes[k].to_global[:] = [float(x) for x in np.asarray(m["to_global"], np.float32)]
-            meshes[k].instance = m.get("instance", -1)
-            meshes[k].light_idx = m.get("light_idx", -1)
-        mats = (capi.MaterialDesc * len(s.materials))()
-        for k, m in enumerate(s.materials):
-            for f, _ in capi.MaterialDesc._fields_:
-                val = m[f]
-                if isinstance(val, (tuple, list, np.ndarray)):
-                    getattr(mats[k], f)[:] = [float(x) for x in val]
-                else:
-                    setattr(mats[k], f, val)
-        lights = (capi.AreaLight * max(1, len(s.area_lights)))()
-        for k, l in enumerate(s.area_lights):
-            lights[k] = make_area_light(l, k)
-        delta = make_delta_lights(s)
-        d = capi.SceneDesc()
-        d.vertices, d.num_vertices = _ptr(V), V.shape[0]
-        d.normals, d.num_normals = _ptr(N), N.shape[0]
-        d.uvs, d.num_uvs = _ptr(U), U.shape[0]
-        d.vindices, d.nindices, d.uvindices = _ptr(vi, C.c_uint32), _ptr(ni, C.c_uint32), _ptr(ui, C.c_uint32)
-        d.material_indices = _ptr(mi, C.c_uint32)
-        d.num_triangles = vi.shape[0]
-        d.meshes, d.num_meshes = meshes, len(s.meshes)
-        d.materials, d.num_materials = mats, len(s.materials)
-        d.area_lights, d.num_area_lights = lights, len(s.area_lights)
-        d.point_lights, d.num_point_lights = delta[0], len(s.point_lights)
-        d.spot_lights, d.num_spot_lights = delta[1], len(s.spot_lights)
-        d.distant_lights, d.num_distant_lights = delta[2], len(s.distant_lights)
-        d.skydome_type = s.skydome_type
-        if s.env is not None:
-            E = np.ascontiguousarray(s.env, np.float32)
-            keep.append(E)
-            d.env_width, d.env_height, d.env_rgba = E.shape[1], E.shape[0], _ptr(E)
-        b = s.bvh
-        d.bvh = capi.BvhSpec(b["num_bins"], b["max_height"], b["Ci"], b["Ct"], b["min_leaf_tris"], b["max_leaf_tris"])
-        self.desc = d
-        self._keep = keep + [meshes, mats, lights, delta]
+        self.scene = scene
+        self.desc, self._keep = scene_desc(scene)
         h = C.c_void_p()
         self.stat = capi.BuildStat()
-        capi.call("noor_build_payload_gpu" if gpu else "noor_build_payload", C.byref(d), C.byref(h),
+        capi.call("noor_build_payload_gpu" if gpu else "noor_build_payload", C.byref(self.desc), C.byref(h),
                   C.byref(self.stat))
         self.handle = h
         self.payload = capi.Payload()

@@ -1146,32 +1146,42 @@ void build_dist(Scene& sc) {
     sc.dw = w;
     sc.dh = h;
     sc.func.assign((size_t)w * h, 0.0);
-    for (int j = 0; j < h; ++j)
-        for (int i = 0; i < w; ++i) {
-            double f = 0;
-            if (sky) {
-                float acc = 0.0f;
-                for (int b = 0; b < 4; ++b) {
-                    const float v = ((float)j + ((float)b + 0.5f) * 0.25f) / (float)h;
-                    const float th = v * K<float>::pi;
-                    const float st = std::sin(th), ct = std::cos(th);
-                    for (int a = 0; a < 4; ++a) {
-                        const float u = ((float)i + ((float)a + 0.5f) * 0.25f) / (float)w;
-                        const float ph = u * 2.0f * K<float>::pi;
-                        const V<float> d = nrm(mk(st * std::cos(ph), ct, st * std::sin(ph)));
-                        const V<float> c = hosek<float>(*sc.H, d);
-                        acc += std::max(0.0f, (float)lum(c.x, c.y, c.z)) * st;
+    // the sky's cells: luminance x sin(theta) over 4 x 4 sub-samples in
+    // FP64, rounded once to FP32 (rows split over the host threads)
+    auto rows = [&](int j0, int j1) {
+        for (int j = j0; j < j1; ++j)
+            for (int i = 0; i < w; ++i) {
+                double f = 0;
+                if (sky) {
+                    double acc = 0.0;
+                    for (int b = 0; b < 4; ++b) {
+                        const double th = ((double)j + ((double)b + 0.5) * 0.25) / (double)h * K<double>::pi;
+                        const double st = std::sin(th), ct = std::cos(th);
+                        for (int a = 0; a < 4; ++a) {
+                            const double ph = ((double)i + ((double)a + 0.5) * 0.25) / (double)w * (2.0 * K<double>::pi);
+                            const V<double> d = nrm(mk(st * std::cos(ph), ct, st * std::sin(ph)));
+                            const V<double> c = hosek<double>(*sc.H, d);
+                            acc += std::max(0.0, lum(c.x, c.y, c.z)) * st;
+                        }
                     }
+                    f = (float)(acc / 16.0);
+                } else {
+                    const float* t = sc.env + 4 * ((size_t)j * w + i);
+                    const float st = std::sin(((float)j + 0.5f) / (float)h * K<float>::pi);
+                    const float y = 0.2126f * t[0] + 0.7152f * t[1] + 0.0722f * t[2];
+                    f = std::max(0.0f, y) * st;
                 }
-                f = acc * (1.0f / 16.0f);
-            } else {
-                const float* t = sc.env + 4 * ((size_t)j * w + i);
-                const float st = std::sin(((float)j + 0.5f) / (float)h * K<float>::pi);
-                const float y = 0.2126f * t[0] + 0.7152f * t[1] + 0.0722f * t[2];
-                f = std::max(0.0f, y) * st;
+                sc.func[(size_t)j * w + i] = (double)(float)f;
             }
-            sc.func[(size_t)j * w + i] = (double)(float)f;
-        }
+    };
+    if (sky) {
+        const int T = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+        std::vector<std::thread> th;
+        for (int t = 0; t < T; ++t) th.emplace_back(rows, h * t / T, h * (t + 1) / T);
+        for (auto& x : th) x.join();
+    } else {
+        rows(0, h);
+    }
     sc.cdf.assign((size_t)h * (w + 1), 0.0);
     sc.row_int.assign(h, 0.0);
     for (int j = 0; j < h; ++j) {
@@ -2247,6 +2257,57 @@ OR_API void oracle_rng(const uint32_t* pairs, size_t n, int draws, uint32_t* see
         Rng r{tea16(pairs[2 * i], pairs[2 * i + 1])};
         seed[i] = r.s;
         for (int k = 0; k < draws; ++k) out[i * draws + k] = r.next();
+    }
+}
+
+// Env-texel footprint of the forward paths: replays the paths the adjoint's
+// forward traces (frames [f0, f0 + spp) per pixel) and counts, per env
+// texel, the radiance lookups that reach the image -- an env term of the
+// path with a non-zero throughput before it, a non-zero factor and a
+// non-zero bilinear weight on that texel.  Forward only: it reads no
+// gradient, so a texel the adjoint leaves at zero is still counted when a
+// path reaches it.  counts: env_h x env_w.
+OR_API void oracle_env_footprint(void* h, const noor_camera* C, uint32_t f0, uint32_t spp, uint32_t bounces,
+                                 const float* alb, const float* rough, const float* env3, int isect, int threads,
+                                 uint32_t* counts) {
+    const Scene& sc = ((Ctx*)h)->sc;
+    const AdjPar P{alb, rough, env3, bounces};
+    const size_t NT = (size_t)sc.ew * sc.eh;
+    const uint32_t npix = C->w * C->h;
+    const int T = std::max(1, threads);
+    std::atomic<uint32_t> next{0};
+    std::vector<std::vector<uint32_t>> acc(T, std::vector<uint32_t>(NT, 0u));
+    auto work = [&](int tid) {
+        std::vector<uint32_t>& A = acc[tid];
+        std::vector<AVtx> vs;
+        std::vector<ATerm> ts;
+        for (;;) {
+            const uint32_t b0 = next.fetch_add(16);
+            if (b0 >= npix) break;
+            for (uint32_t p = b0; p < std::min(b0 + 16, npix); ++p)
+                for (uint32_t f = 0; f < spp; ++f) {
+                    Rng rng{tea16(p, f0 + f)};
+                    V<double> o, d;
+                    cam_ray<double>(*C, p % C->w, p / C->w, rng, o, d);
+                    adj_path(sc, P, o, d, rng, isect, vs, ts);
+                    for (const ATerm& t : ts) {
+                        if (!t.env) continue;
+                        V<double> B = mk(1.0, 1.0, 1.0);
+                        for (size_t k = 0; k < t.k; ++k) B = B * vs[k].s;
+                        if (black(B * t.fs * t.xscale)) continue;
+                        for (int q = 0; q < 4; ++q)
+                            if (t.bw.w[q] > 0.0) ++A[t.bw.idx[q]];
+                    }
+                }
+        }
+    };
+    std::vector<std::thread> th;
+    for (int t = 0; t < T; ++t) th.emplace_back(work, t);
+    for (auto& x : th) x.join();
+    for (size_t i = 0; i < NT; ++i) {
+        uint32_t c = 0;
+        for (auto& a : acc) c += a[i];
+        counts[i] = c;
     }
 }
 

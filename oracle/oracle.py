@@ -8,7 +8,11 @@ __graft_entry__.smoke() and bench.py's CPU-baseline leg import this module.
 from __future__ import annotations
 
 import ctypes as C
+import importlib
+import math
 import subprocess
+import sys
+import types
 from pathlib import Path
 
 import numpy as np
@@ -59,6 +63,8 @@ def lib() -> C.CDLL:
         L.oracle_env_sample.argtypes = [vp, vp, vp, sz]
         L.oracle_adjoint.argtypes = [vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, vp, vp, vp, vp, C.c_int, C.c_int,
                                      vp, vp, vp, vp]
+        L.oracle_env_footprint.argtypes = [vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, vp, vp, vp, C.c_int, C.c_int,
+                                           vp]
         L.oracle_routines.argtypes = [C.c_int, vp, vp, sz, C.c_int]
         L.oracle_rng.argtypes = [vp, sz, C.c_int, vp, vp]
         L.oracle_ref_dist_sample.argtypes = [vp, vp, C.c_int, C.c_int, vp, vp, sz]
@@ -84,12 +90,99 @@ def ref() -> C.CDLL:
         L.ref_wald.argtypes = [vp, vp]
         L.ref_hosek_state.argtypes = [C.c_float, C.c_float, C.c_float, vp]
         L.ref_hosek_dataset.argtypes = [vp]
+        L.ref_build_payload.restype = vp
+        L.ref_build_payload.argtypes = [vp]
+        L.ref_payload_view.argtypes = [vp, vp]
+        L.ref_payload_spec.argtypes = [vp, C.c_uint32, C.c_uint32, vp]
+        L.ref_free_payload.argtypes = [vp]
         _ref = L
     return _ref
 
 
 def _p(a: np.ndarray):
     return a.ctypes.data_as(C.c_void_p)
+
+
+def host_modules():
+    """noor_b200/_capi.py (the C-ABI's struct layouts) and noor_b200/scenes.py
+    (the seeded scene generators) as modules of a bare package: the
+    package's __init__, which loads the product library, does not run.  The
+    bench's reference arm builds its workload through these and the
+    reference builder alone."""
+    name = "_noor_b200_host"
+    if name not in sys.modules:
+        pkg = types.ModuleType(name)
+        pkg.__path__ = [str(HERE.parent / "noor_b200")]
+        sys.modules[name] = pkg
+    return importlib.import_module(name + "._capi"), importlib.import_module(name + ".scenes")
+
+
+class RefPayload:
+    """A scene's payload from the reference's own BVH builder and Wald
+    records (oracle/_ref/libnoor_ref.so, ref_build_payload), with the spec
+    Scene::load derives.  `capi` and `scenes` are the modules of
+    host_modules() or of the product package (only their struct layouts and
+    scene description are used)."""
+
+    def __init__(self, scene, capi, scenes):
+        self.capi = capi
+        self.desc, self._keep = scenes.scene_desc(scene)
+        self.h = ref().ref_build_payload(C.addressof(self.desc))
+        self.payload = capi.Payload()
+        ref().ref_payload_view(self.h, C.addressof(self.payload))
+
+    def default_spec(self, bounces: int, rr: int):
+        sp = self.capi.Spec()
+        ref().ref_payload_spec(self.h, bounces, rr, C.addressof(sp))
+        return sp
+
+    def free(self):
+        if self.h:
+            ref().ref_free_payload(self.h)
+            self.h = None
+
+
+def camera_lookat(capi, cam: dict):
+    """A pinhole camera as Camera's constructor and CudaCamera::update build
+    it (noor/header/camera.h:99-153,255-334; noor/cuda/camera.cuh:66-94),
+    evaluated in FP64 and rounded once: cameraToWorld = translate(lookAt) *
+    [right, up, forward] * translate(0, 0, |eye - lookAt|); rasterToCamera
+    maps the raster onto the screen window (+-aspect x +-1, or +-1 x
+    +-1/aspect) on the plane z = -1 scaled by 1/cot(fov/2).  Perspective
+    cameras only."""
+    if cam.get("type", "persp") != "persp" or cam.get("lens_radius", 0.0):
+        raise ValueError("camera_lookat: pinhole perspective cameras only")
+    f32 = lambda x: float(np.float32(x))
+    eye = [f32(x) for x in cam["eye"]]
+    at = [f32(x) for x in cam["look_at"]]
+    up = [f32(x) for x in cam["up"]]
+    fov = f32(math.radians(cam["fov_deg"]))
+    w, h = int(cam["w"]), int(cam["h"])
+    fwd = [eye[k] - at[k] for k in range(3)]
+    scale = math.sqrt(sum(x * x for x in fwd))
+    fwd = [x / scale for x in fwd]
+    right = [up[1] * fwd[2] - up[2] * fwd[1], up[2] * fwd[0] - up[0] * fwd[2], up[0] * fwd[1] - up[1] * fwd[0]]
+    rl = math.sqrt(sum(x * x for x in right))
+    right = [x / rl for x in right]
+    out = capi.Camera()
+    for r in range(3):
+        out.camera_to_world[r][:] = [right[r], up[r], fwd[r], at[r] + fwd[r] * scale]
+    aspect = w / h
+    smin, smax = ((-aspect, -1.0), (aspect, 1.0)) if aspect > 1.0 else ((-1.0, -1.0 / aspect), (1.0, 1.0 / aspect))
+    cot = 1.0 / math.tan(fov / 2.0)
+    sx, sy = (smax[0] - smin[0]) / w / cot, (smax[1] - smin[1]) / h / cot
+    out.raster_to_camera[0][:] = [sx, 0.0, 0.0, smin[0] / cot]
+    out.raster_to_camera[1][:] = [0.0, sy, 0.0, smin[1] / cot]
+    out.raster_to_camera[2][:] = [0.0, 0.0, 0.0, -1.0]
+    out.dx_camera[:] = [sx, 0.0, 0.0]
+    out.dy_camera[:] = [0.0, sy, 0.0]
+    out.image_area = abs((smax[0] - smin[0]) / cot * (smax[1] - smin[1]) / cot)
+    out.lens_radius = 0.0
+    out.focal_length = scale
+    out.w, out.h = w, h
+    out.center = w * (h >> 1) + (w >> 1)
+    out.type = capi.NOOR_CAMERA_PERSP
+    return out
 
 
 class Oracle:
@@ -171,6 +264,17 @@ class Oracle:
         lib().oracle_adjoint(self.h, C.addressof(camera), frame0, spp, bounces, _p(alb), _p(rough), _p(env3),
                              None if gi is None else _p(gi), isect, threads, _p(img), _p(ga), _p(gr), _p(ge))
         return (img, ga, gr, ge) if gi is not None else img
+
+    def env_footprint(self, camera, frame0: int, spp: int, bounces: int, albedo: np.ndarray,
+                      roughness: np.ndarray, env: np.ndarray, isect: int = 0, threads: int = 8) -> np.ndarray:
+        """(H, W) counts of the forward paths' radiance lookups per env
+        texel (oracle_env_footprint): the texels the image depends on"""
+        env3 = np.ascontiguousarray(env, np.float32)
+        out = np.zeros(env3.shape[:2], np.uint32)
+        lib().oracle_env_footprint(self.h, C.addressof(camera), frame0, spp, bounces,
+                                   _p(np.ascontiguousarray(albedo, np.float32)),
+                                   _p(np.ascontiguousarray(roughness, np.float32)), _p(env3), isect, threads, _p(out))
+        return out
 
     def env_sample(self, u: np.ndarray) -> np.ndarray:
         out = np.zeros(u.shape[0] * 4)

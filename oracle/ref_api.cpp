@@ -4,6 +4,9 @@
 //   * ref_build_bvh: Model + BVH (noor/source/bvh.cpp, splitter.cpp) on a
 //     scene description, returning the node words, root, triangle order and
 //     height the reference would hand to the device;
+//   * ref_build_payload / ref_payload_view / ref_payload_spec: a whole
+//     payload (tree, transforms, de-duplicated vertices, Wald records,
+//     materials, lights) and the spec Scene::load derives, for the oracle;
 //   * ref_wald: WaldTriangle (noor/header/triangle.h:56-120);
 //   * ref_hosek_state / ref_hosek_dataset: the vendored Hosek-Wilkie fit
 //     (noor/external/ArHosekSkyModel.cpp:667-695) and its RGB tables.
@@ -17,6 +20,9 @@
 #include "ArHosekSkyModel.h"
 #include "../include/noor_b200.h"
 
+#include <array>
+#include <unordered_map>
+
 extern float* datasetsRGB[];
 extern float* datasetsRGBRad[];
 
@@ -29,9 +35,8 @@ static glm::mat4 to_mat4(const float* m) {
     return r;
 }
 
-REF_API int ref_build_bvh(const noor_scene_desc* d, uint32_t* nodes, size_t node_cap, uint32_t* num_nodes,
-                          uint32_t* root, uint32_t* tri_order, uint32_t* height) {
-    Model model;
+// Model::load's mesh list and Model::computeBBoxes for a scene description
+static void load_model(const noor_scene_desc* d, Model& model) {
     model._num_triangles = d->num_triangles;
     model._meshes.resize(d->num_meshes);
     for (uint32_t i = 0; i < d->num_meshes; ++i) {
@@ -40,6 +45,7 @@ REF_API int ref_build_bvh(const noor_scene_desc* d, uint32_t* nodes, size_t node
         M._start_count = std::make_pair(m.tri_start, m.tri_count);
         M._to_global = to_mat4(m.to_global);
         M._to_local = glm::inverse(M._to_global);
+        M._normal_transform = glm::transpose(glm::inverse(glm::mat3(M._to_global)));
         M._instance = m.instance;
         if (m.light_idx >= 0) {
             M._light_idx = m.light_idx;
@@ -105,6 +111,12 @@ REF_API int ref_build_bvh(const noor_scene_desc* d, uint32_t* nodes, size_t node
         model._scene_bbox.merge(mesh._instance_bbox);
         model._scene_centbox.include(mesh._instance_bbox.centroid());
     }
+}
+
+REF_API int ref_build_bvh(const noor_scene_desc* d, uint32_t* nodes, size_t node_cap, uint32_t* num_nodes,
+                          uint32_t* root, uint32_t* tri_order, uint32_t* height) {
+    Model model;
+    load_model(d, model);
     BVHSpec spec(d->bvh.num_bins, d->bvh.max_height, d->bvh.Ci, d->bvh.Ct, d->bvh.min_leaf_tris,
                  d->bvh.max_leaf_tris);
     Stat stat;
@@ -127,6 +139,215 @@ REF_API int ref_build_bvh(const noor_scene_desc* d, uint32_t* nodes, size_t node
     if (tri_order) std::memcpy(tri_order, model._triangle_indices.data(), d->num_triangles * sizeof(uint32_t));
     return 0;
 }
+
+// ------------------------------------------------------------------------
+// A whole payload on the host from the reference's own builder: the tree and
+// the instance transforms come from BVH::loadCudaPayload (bvh.cpp:53-86)
+// and the Wald records from WaldTriangle (triangle.h:56-120), both compiled
+// unmodified; the steps of Model::loadCudaPayload and Model::loadMaterial
+// that need the loaders (model.cpp:184-330,333-458) are restated here.  The
+// bench's reference arm renders from this payload with the oracle, so it
+// never loads the product library.
+struct RefPayload {
+    std::vector<uint32_t> attr, wald[3], lo, hi, order;
+    std::vector<float> vtx, nrm, uv, xf[9];
+    std::vector<std::vector<float>> tex_data;
+    std::vector<noor_texture> tex;
+    std::vector<noor_material> mats;
+    std::vector<noor_area_light> area;
+    std::vector<noor_point_light> point;
+    std::vector<noor_spot_light> spot;
+    std::vector<noor_distant_light> distant;
+    uint32_t num_tris = 0, root = 0, height = 0;
+    float radius = 0.0f;
+    int32_t sky = 0;
+};
+
+static uint32_t constant_texture(RefPayload& P, float r, float g, float b) {
+    P.tex_data.push_back({r, g, b, 1.0f});
+    return (uint32_t)P.tex_data.size() - 1;
+}
+
+REF_API void* ref_build_payload(const noor_scene_desc* d) {
+    std::unique_ptr<RefPayload> P(new RefPayload());
+    Model model;
+    load_model(d, model);
+    BVHSpec spec(d->bvh.num_bins, d->bvh.max_height, d->bvh.Ci, d->bvh.Ct, d->bvh.min_leaf_tris,
+                 d->bvh.max_leaf_tris);
+    Stat stat;
+    BVH bvh(model, spec, stat);
+    std::unique_ptr<CudaPayload> cp(new CudaPayload());
+    bvh.loadCudaPayload(cp);
+    RefPayload& R = *P;
+    R.num_tris = d->num_triangles;
+    R.root = cp->_bvh_root_node;
+    R.height = stat._height;
+    R.radius = model.getSceneBBox().radius();
+    R.sky = d->skydome_type;
+    R.order = model._triangle_indices;
+    for (size_t i = 0; i < cp->_bvh_min_right_start_nodes.size(); ++i) {
+        const glm::uvec4& a = cp->_bvh_min_right_start_nodes[i];
+        const glm::uvec4& b = cp->_bvh_max_axis_count_nodes[i];
+        R.lo.insert(R.lo.end(), {a.x, a.y, a.z, a.w});
+        R.hi.insert(R.hi.end(), {b.x, b.y, b.z, b.w});
+    }
+    const std::vector<glm::vec4>* rows[9] = {&cp->_normal_row0,          &cp->_normal_row1,
+                                             &cp->_normal_row2,          &cp->_world_to_object_row0,
+                                             &cp->_world_to_object_row1, &cp->_world_to_object_row2,
+                                             &cp->_object_to_world_row0, &cp->_object_to_world_row1,
+                                             &cp->_object_to_world_row2};
+    for (int k = 0; k < 9; ++k)
+        for (const glm::vec4& v : *rows[k]) R.xf[k].insert(R.xf[k].end(), {v.x, v.y, v.z, v.w});
+
+    // materials: one texture of 0.5 first, then per material its constant
+    // parameters as 1 x 1 textures in loadMaterial's order
+    R.tex_data.push_back({0.5f, 0.5f, 0.5f, 1.0f});
+    for (uint32_t i = 0; i < d->num_materials; ++i) {
+        const noor_material_desc& m = d->materials[i];
+        noor_material t;
+        std::memset(&t, 0, sizeof(t));
+        for (float* s : {t.diffuse_uvscale, t.specular_uvscale, t.transparency_uvscale, t.emittance_uvscale,
+                         t.bump_uvscale, t.roughness_uvscale, t.metalness_uvscale})
+            s[0] = s[1] = 1.0f;
+        t.bumpfactor = 1.0f;
+        t.coat_weight = m.coat_weight;
+        t.coat_roughness = m.coat_roughness;
+        t.coat_thickness = m.coat_thickness;
+        t.coat_sigma = m.coat_sigma;
+        t.coat_ior = m.coat_ior;
+        t.emitter_scale = m.emitter_scale;
+        t.type = m.type;
+        t.distribution = m.distribution;
+        t.transmission_tex_idx = constant_texture(R, m.transmission[0], m.transmission[1], m.transmission[2]);
+        t.ior_tex_idx = constant_texture(R, m.ior[0], m.ior[1], m.ior[2]);
+        t.k_tex_idx = constant_texture(R, m.k[0], m.k[1], m.k[2]);
+        t.diffuse_tex_idx = constant_texture(R, m.diffuse[0], m.diffuse[1], m.diffuse[2]);
+        t.roughness_tex_idx = constant_texture(R, m.roughness[0], m.roughness[1], 1.0f);
+        t.metalness_tex_idx = constant_texture(R, 1.0f, 1.0f, 1.0f);
+        t.specular_tex_idx = constant_texture(R, m.specular[0], m.specular[1], m.specular[2]);
+        t.emittance_tex_idx = constant_texture(R, m.emittance[0], m.emittance[1], m.emittance[2]);
+        t.transparency_tex_idx = constant_texture(R, m.transparency[0], m.transparency[1], m.transparency[2]);
+        R.mats.push_back(t);
+    }
+    // the sky dome texture last: the HDR map, else SKYDOME_COLOR
+    if (d->skydome_type == NOOR_SKY_HDR)
+        R.tex_data.emplace_back(d->env_rgba, d->env_rgba + 4 * (size_t)d->env_width * d->env_height);
+    else
+        constant_texture(R, 0.25f, 0.25f, 0.25f);
+    for (size_t i = 0; i < R.tex_data.size(); ++i) {
+        const bool env = i + 1 == R.tex_data.size() && d->skydome_type == NOOR_SKY_HDR;
+        R.tex.push_back(noor_texture{env ? d->env_width : 1, env ? d->env_height : 1, R.tex_data[i].data()});
+    }
+    R.area.assign(d->area_lights, d->area_lights + d->num_area_lights);
+    R.point.assign(d->point_lights, d->point_lights + d->num_point_lights);
+    R.spot.assign(d->spot_lights, d->spot_lights + d->num_spot_lights);
+    R.distant.assign(d->distant_lights, d->distant_lights + d->num_distant_lights);
+    for (noor_distant_light& l : R.distant) {   // CudaDistantLight normalises its direction
+        const glm::vec3 w = glm::normalize(glm::vec3(l.direction[0], l.direction[1], l.direction[2]));
+        l.direction[0] = w.x;
+        l.direction[1] = w.y;
+        l.direction[2] = w.z;
+    }
+
+    // vertex de-duplication in BVH order: the first (vertex, normal, uv)
+    // index triple of a corner appends a vertex, later ones reuse its index
+    struct KeyHash {
+        size_t operator()(const std::array<uint32_t, 3>& k) const {
+            return ((size_t)k[0] * 0x9E3779B97F4A7C15ull) ^ ((size_t)k[1] * 0xC2B2AE3D27D4EB4Full) ^ k[2];
+        }
+    };
+    std::unordered_map<std::array<uint32_t, 3>, uint32_t, KeyHash> seen;
+    seen.reserve(3 * (size_t)d->num_triangles);
+    std::vector<uint32_t> element;
+    element.reserve(3 * (size_t)d->num_triangles);
+    for (uint32_t i = 0; i < d->num_triangles; ++i) {
+        const size_t t = R.order[i];
+        for (int j = 0; j < 3; ++j) {
+            const uint32_t vi = d->vindices[3 * t + j], ni = d->nindices[3 * t + j], ui = d->uvindices[3 * t + j];
+            auto ins = seen.emplace(std::array<uint32_t, 3>{vi, ni, ui}, (uint32_t)seen.size());
+            if (ins.second) {
+                R.vtx.insert(R.vtx.end(), d->vertices + 4 * (size_t)vi, d->vertices + 4 * (size_t)vi + 4);
+                R.nrm.insert(R.nrm.end(), d->normals + 4 * (size_t)ni, d->normals + 4 * (size_t)ni + 4);
+                R.uv.insert(R.uv.end(), d->uvs + 2 * (size_t)ui, d->uvs + 2 * (size_t)ui + 2);
+            }
+            element.push_back(ins.first->second);
+        }
+    }
+    // Model::buildWaldTriangles: Wald records of the de-duplicated corners,
+    // the material type in the last word, attribute words v0, v1, v2, mat
+    for (uint32_t i = 0; i < d->num_triangles; ++i) {
+        glm::vec3 p[3];
+        for (int j = 0; j < 3; ++j) {
+            const float* q = R.vtx.data() + 4 * (size_t)element[3 * (size_t)i + j];
+            p[j] = glm::vec3(q[0], q[1], q[2]);
+        }
+        WaldTriangle wt(p[0], p[1], p[2]);
+        const uint32_t mi = d->material_indices[R.order[i]];
+        const glm::uvec4 r0 = wt.get_ax_nu_nv_nd(), r1 = wt.get_bnu_bnv_au_av(), r2 = wt.get_cnu_cnv_deg_mat();
+        R.wald[0].insert(R.wald[0].end(), {r0.x, r0.y, r0.z, r0.w});
+        R.wald[1].insert(R.wald[1].end(), {r1.x, r1.y, r1.z, r1.w});
+        R.wald[2].insert(R.wald[2].end(), {r2.x, r2.y, r2.z, R.mats[mi].type});
+        R.attr.insert(R.attr.end(), {element[3 * (size_t)i], element[3 * (size_t)i + 1], element[3 * (size_t)i + 2], mi});
+    }
+    return P.release();
+}
+
+REF_API void ref_payload_view(const void* h, noor_payload* p) {
+    const RefPayload& R = *(const RefPayload*)h;
+    std::memset(p, 0, sizeof(*p));
+    p->num_triangles = R.num_tris;
+    p->attribute_indices = R.attr.data();
+    p->vertices = R.vtx.data();
+    p->normals = R.nrm.data();
+    p->uvs = R.uv.data();
+    p->num_vertices = (uint32_t)(R.vtx.size() / 4);
+    for (int r = 0; r < 3; ++r) {
+        p->normal_row[r] = R.xf[r].data();
+        p->world_to_object_row[r] = R.xf[3 + r].data();
+        p->object_to_world_row[r] = R.xf[6 + r].data();
+    }
+    p->num_instances = (uint32_t)(R.xf[0].size() / 4);
+    p->wald_ax_nu_nv_nd = R.wald[0].data();
+    p->wald_bnu_bnv_au_av = R.wald[1].data();
+    p->wald_cnu_cnv_deg_mat = R.wald[2].data();
+    p->bvh_root_node = R.root;
+    p->bvh_min_right_start = R.lo.data();
+    p->bvh_max_axis_count = R.hi.data();
+    p->num_bvh_nodes = (uint32_t)(R.lo.size() / 4);
+    p->textures = R.tex.data();
+    p->num_textures = (uint32_t)R.tex.size();
+    p->area_lights = R.area.empty() ? nullptr : R.area.data();
+    p->num_area_lights = (int32_t)R.area.size();
+    p->point_lights = R.point.empty() ? nullptr : R.point.data();
+    p->num_point_lights = (int32_t)R.point.size();
+    p->spot_lights = R.spot.empty() ? nullptr : R.spot.data();
+    p->num_spot_lights = (int32_t)R.spot.size();
+    p->distant_lights = R.distant.empty() ? nullptr : R.distant.data();
+    p->num_distant_lights = (int32_t)R.distant.size();
+    p->num_infinite_lights = 1;
+    p->materials = R.mats.data();
+    p->num_materials = (uint32_t)R.mats.size();
+}
+
+// the CudaSpec fields Scene::load sets (noor/source/scene.cpp:51-91)
+REF_API void ref_payload_spec(const void* h, uint32_t bounces, uint32_t rr, noor_spec* s) {
+    const RefPayload& R = *(const RefPayload*)h;
+    std::memset(s, 0, sizeof(*s));
+    s->reflection_bias = 0.0001f * R.radius;
+    s->shadow_bias = 0.0001f * R.radius;
+    s->world_radius = R.radius;
+    s->wr2 = R.radius * R.radius;
+    s->bvh_root_node = R.root;
+    s->bvh_height = R.height;
+    s->bounces = bounces;
+    s->rr = rr;
+    s->num_gpus = 1;
+    s->skydome_type = R.sky;
+    const size_t lights = R.area.size() + R.point.size() + R.spot.size() + R.distant.size() + 1;
+    s->lighting_type = lights < 2 ? NOOR_LIGHT_SKY_MASK : 0u;
+}
+
+REF_API void ref_free_payload(void* h) { delete (RefPayload*)h; }
 
 // out: ax_nu_nv_nd, bnu_bnv_au_av, cnu_cnv_deg_mat (12 words)
 REF_API void ref_wald(const float* v9, uint32_t* out) {

@@ -158,6 +158,31 @@ inline mat4 operator*(const mat4& a, const mat4& b) {
     for (int c = 0; c < 4; ++c) o[c] = a * b[c];
     return o;
 }
+// adjugate over the determinant (the mesh normal transform,
+// transpose(inverse(mat3(to_global))), noor/header/assetLoader.h:75-76)
+inline mat3 inverse(const mat3& m) {
+    const float det = m[0][0] * (m[1][1] * m[2][2] - m[2][1] * m[1][2]) -
+                      m[1][0] * (m[0][1] * m[2][2] - m[2][1] * m[0][2]) +
+                      m[2][0] * (m[0][1] * m[1][2] - m[1][1] * m[0][2]);
+    const float s = 1.0f / det;
+    mat3 o;
+    o[0][0] = (m[1][1] * m[2][2] - m[2][1] * m[1][2]) * s;
+    o[1][0] = -(m[1][0] * m[2][2] - m[2][0] * m[1][2]) * s;
+    o[2][0] = (m[1][0] * m[2][1] - m[2][0] * m[1][1]) * s;
+    o[0][1] = -(m[0][1] * m[2][2] - m[2][1] * m[0][2]) * s;
+    o[1][1] = (m[0][0] * m[2][2] - m[2][0] * m[0][2]) * s;
+    o[2][1] = -(m[0][0] * m[2][1] - m[2][0] * m[0][1]) * s;
+    o[0][2] = (m[0][1] * m[1][2] - m[1][1] * m[0][2]) * s;
+    o[1][2] = -(m[0][0] * m[1][2] - m[1][0] * m[0][2]) * s;
+    o[2][2] = (m[0][0] * m[1][1] - m[1][0] * m[0][1]) * s;
+    return o;
+}
+inline mat3 transpose(const mat3& m) {
+    mat3 o;
+    for (int c = 0; c < 3; ++c)
+        for (int r = 0; r < 3; ++r) o[c][r] = m[r][c];
+    return o;
+}
 inline vec4 row(const mat4& m, int i) { return vec4(m[0][i], m[1][i], m[2][i], m[3][i]); }
 inline vec3 row(const mat3& m, int i) { return vec3(m[0][i], m[1][i], m[2][i]); }
 }  // namespace glm

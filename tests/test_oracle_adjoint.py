@@ -63,3 +63,27 @@ def test_oracle_gradient_matches_fp64_differences(small):
         e2[y, x, c] -= 1e-2
         fd = (loss(alb, rough, e1) - loss(alb, rough, e2)) / (float(e1[y, x, c]) - float(e2[y, x, c]))
         assert abs(fd - ge[y, x, c]) <= 1e-8 * escale + 1e-7 * abs(fd), (y, x, c, ge[y, x, c], fd)
+
+
+def test_env_footprint_bounds_the_gradient(small):
+    """the forward footprint (oracle_env_footprint) holds every texel with a
+    non-zero gradient, and a texel outside it leaves the image unchanged"""
+    o, cam, alb, rough, env, gi = small
+    foot = o.env_footprint(cam, 1, 2, 4, alb, rough, env)
+    assert foot.shape == env.shape[:2] and foot.sum() > 0
+    _, _, _, ge = o.adjoint(cam, 1, 2, 4, alb, rough, env, gi)
+    assert not ((ge != 0).any(axis=2) & (foot == 0)).any()
+    img = o.adjoint(cam, 1, 2, 4, alb, rough, env)
+    outside = np.argwhere(foot == 0)
+    assert len(outside) > 0
+    for (y, x) in outside[:: max(1, len(outside) // 8)]:
+        e = env.copy()
+        e[y, x] += 1.0
+        assert np.array_equal(o.adjoint(cam, 1, 2, 4, alb, rough, e), img)
+    inside = np.argwhere(foot > 0)
+    changed = 0
+    for (y, x) in inside[:: max(1, len(inside) // 8)]:
+        e = env.copy()
+        e[y, x] += 1.0
+        changed += int(not np.array_equal(o.adjoint(cam, 1, 2, 4, alb, rough, e), img))
+    assert changed == len(inside[:: max(1, len(inside) // 8)])
