@@ -542,7 +542,7 @@ def run_batched(args):
     img_wf = [f_.cpu().numpy()[..., :3] for f_ in films]
     for _ in range(2):
         mk()
-    mk_ms = device_timed(mk, max(1, args.steps // 2))
+    mk_ms = device_timed(mk, max(2, args.steps // 2))
     img_mk = [f_.cpu().numpy()[..., :3] for f_ in films]
     rel = np.concatenate([(np.abs(a - b) / np.maximum(np.abs(b), 1e-2)).ravel() for a, b in zip(img_wf, img_mk)])
     # end to end: frame descriptions from host memory, films back to pinned host memory

@@ -181,11 +181,19 @@ typedef struct noor_distant_light {
 /* ImageTexture entry of CudaPayload::_textures: constant material
  * parameters are 1x1 textures; the environment texture is the LAST entry
  * (noor/source/model.cpp:313-321).  rgba: width*height*4 floats, row-major,
- * row 0 = v of 0. */
+ * row 0 = v of 0.  filter and address are the ImageTexture's modes
+ * (noor/header/texture.h:133-185), with CUDA's values: a material texture
+ * larger than 1x1 is fetched by the texture unit with them (normalised
+ * coordinates), as the reference's Cuda2DTexture is
+ * (noor/cuda/texture.cuh:375-400); 1x1 constants read their one texel. */
+enum { NOOR_FILTER_POINT = 0, NOOR_FILTER_LINEAR = 1 };
+enum { NOOR_ADDRESS_WRAP = 0, NOOR_ADDRESS_CLAMP = 1 };
 typedef struct noor_texture {
     int32_t width;
     int32_t height;
     const float* rgba;
+    int32_t filter;             /* NOOR_FILTER_*                             */
+    int32_t address;            /* NOOR_ADDRESS_*                            */
 } noor_texture;
 
 /* CudaMaterial, noor/cuda/material.cuh:26-58 (+ one build field) */
@@ -493,8 +501,32 @@ typedef struct noor_mesh {
     int32_t light_idx;
 } noor_mesh;
 
-/* constant material parameters as an AssetLoader reports them
- * (noor/header/assetLoader.h:134-150) */
+/* an image map as a texture file decodes (noor/header/texture.h:146-152):
+ * width x height RGBA floats, row 0 = v of 0 */
+typedef struct noor_image {
+    int32_t width;
+    int32_t height;
+    const float* rgba;
+} noor_image;
+
+/* the map slots of a material, in the order of noor_material_desc.map and
+ * .map_uvscale (the reference's getMaterial_map_* getters,
+ * noor/source/model.cpp:220-300) */
+enum {
+    NOOR_MAP_DIFFUSE = 0,       /* map_Kd                                    */
+    NOOR_MAP_ROUGHNESS = 1,
+    NOOR_MAP_METALNESS = 2,
+    NOOR_MAP_SPECULAR = 3,      /* map_Ks                                    */
+    NOOR_MAP_EMITTANCE = 4,     /* map_Ke                                    */
+    NOOR_MAP_ALPHA = 5,         /* map_d: point filtered, sets NOOR_ALPHA    */
+    NOOR_MAP_BUMP = 6,          /* map_bump: sets NOOR_BUMP                  */
+    NOOR_NUM_MAPS = 7
+};
+
+/* material parameters as an AssetLoader reports them
+ * (noor/header/assetLoader.h:134-150): the constants, and per map slot an
+ * index into noor_scene_desc.images (-1: the constant is used) with its uv
+ * scale; bumpfactor scales the bump map's displacement. */
 typedef struct noor_material_desc {
     float diffuse[3];
     float specular[3];
@@ -512,6 +544,9 @@ typedef struct noor_material_desc {
     float emitter_scale;
     uint32_t type;
     uint32_t distribution;
+    int32_t map[NOOR_NUM_MAPS];
+    float map_uvscale[NOOR_NUM_MAPS][2];
+    float bumpfactor;
 } noor_material_desc;
 
 /* loader output consumed by Model::load (noor/source/model.cpp:132-182) */
@@ -544,6 +579,10 @@ typedef struct noor_scene_desc {
     int32_t env_height;
     const float* env_rgba;
     noor_bvh_spec bvh;
+    /* image maps the materials' map_* fields index (decoded texture files,
+     * shared by every material that names the same file) */
+    const noor_image* images;
+    uint32_t num_images;
 } noor_scene_desc;
 
 /* Stat, noor/header/stat.h:26-49 (BVH part) + derived scene quantities */

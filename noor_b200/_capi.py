@@ -35,7 +35,13 @@ NOOR_SUBSTRATE = 1 << 8
 NOOR_EMITTER = 1 << 9
 NOOR_CLEARCOAT = 1 << 10
 NOOR_SHADOWCATCHER = 1 << 11
+NOOR_ALPHA = 1 << 12
+NOOR_BUMP = 1 << 13
 NOOR_MESHLIGHT = 1 << 14
+NOOR_FILTER_POINT, NOOR_FILTER_LINEAR = 0, 1
+NOOR_ADDRESS_WRAP, NOOR_ADDRESS_CLAMP = 0, 1
+(NOOR_MAP_DIFFUSE, NOOR_MAP_ROUGHNESS, NOOR_MAP_METALNESS, NOOR_MAP_SPECULAR, NOOR_MAP_EMITTANCE, NOOR_MAP_ALPHA,
+ NOOR_MAP_BUMP) = range(7)
 NOOR_SKY_HDR, NOOR_SKY_PHYSICAL, NOOR_SKY_CONSTANT = 0, 1, 2
 NOOR_LIGHT_SKY_MASK = 0x20
 NOOR_ISECT_WATERTIGHT, NOOR_ISECT_REF_WALD = 0, 1
@@ -75,6 +81,10 @@ class DistantLight(C.Structure):
 
 
 class Texture(C.Structure):
+    _fields_ = [("width", i32), ("height", i32), ("rgba", pf), ("filter", i32), ("address", i32)]
+
+
+class Image(C.Structure):
     _fields_ = [("width", i32), ("height", i32), ("rgba", pf)]
 
 
@@ -150,7 +160,8 @@ class MaterialDesc(C.Structure):
     _fields_ = [("diffuse", f32 * 3), ("specular", f32 * 3), ("transmission", f32 * 3), ("emittance", f32 * 3),
                 ("transparency", f32 * 3), ("ior", f32 * 3), ("k", f32 * 3), ("roughness", f32 * 2),
                 ("coat_weight", f32), ("coat_roughness", f32), ("coat_thickness", f32), ("coat_sigma", f32),
-                ("coat_ior", f32), ("emitter_scale", f32), ("type", u32), ("distribution", u32)]
+                ("coat_ior", f32), ("emitter_scale", f32), ("type", u32), ("distribution", u32),
+                ("map", i32 * 7), ("map_uvscale", (f32 * 2) * 7), ("bumpfactor", f32)]
 
 
 class SceneDesc(C.Structure):
@@ -162,7 +173,8 @@ class SceneDesc(C.Structure):
                 ("point_lights", C.POINTER(PointLight)), ("num_point_lights", u32),
                 ("spot_lights", C.POINTER(SpotLight)), ("num_spot_lights", u32),
                 ("distant_lights", C.POINTER(DistantLight)), ("num_distant_lights", u32), ("skydome_type", i32),
-                ("env_width", i32), ("env_height", i32), ("env_rgba", pf), ("bvh", BvhSpec)]
+                ("env_width", i32), ("env_height", i32), ("env_rgba", pf), ("bvh", BvhSpec),
+                ("images", C.POINTER(Image)), ("num_images", u32)]
 
 
 class BuildStat(C.Structure):

@@ -508,6 +508,8 @@ static int adjoint_run(const noor_adjoint_desc* desc, int mode, float* image, co
         if (!(m.type & (NOOR_EMITTER | NOOR_MESHLIGHT)) && l != kLobeLambert && l != kLobeConductor &&
             l != kLobeFresnelSpec)
             return set_error(NOOR_ERR_UNSUPPORTED, "adjoint: materials other than diffuse, metal and glass");
+        if (m.tex_mask)
+            return set_error(NOOR_ERR_UNSUPPORTED, "adjoint: textured, alpha-cut or bump-mapped materials");
     }
     if (C->cam.type != NOOR_CAMERA_PERSP || C->cam.lens_radius > 0.0f)
         return set_error(NOOR_ERR_UNSUPPORTED, "adjoint: cameras other than the pinhole");

@@ -36,7 +36,46 @@ int cuda_fail(cudaError_t e, const char* what) {
 SceneState::~SceneState() {
     if (env_tex) cudaDestroyTextureObject(env_tex);
     if (env_array) cudaFreeArray(env_array);
+    for (auto& t : textures) {
+        if (t.second.obj) cudaDestroyTextureObject(t.second.obj);
+        if (t.second.array) cudaFreeArray(t.second.array);
+    }
     for (void* p : allocs) cudaFree(p);
+}
+
+// The texture object of payload texture `idx` (made once): an RGBA float
+// array with the texture's filter and addressing over normalised
+// coordinates, as Cuda2DTexture makes it (noor/cuda/texture.cuh:375-400,
+// NOOR::create_2d_texobj).
+int SceneState::texture_object(const noor_texture& t, uint32_t idx, cudaTextureObject_t* out) {
+    auto it = textures.find(idx);
+    if (it != textures.end()) {
+        *out = it->second.obj;
+        return NOOR_OK;
+    }
+    TexObj o{};
+    const cudaChannelFormatDesc cd = cudaCreateChannelDesc<float4>();
+    cudaError_t e = cudaMallocArray(&o.array, &cd, (size_t)t.width, (size_t)t.height);
+    if (e != cudaSuccess) return cuda_fail(e, "texture array");
+    textures[idx] = o;
+    e = cudaMemcpy2DToArray(o.array, 0, 0, t.rgba, (size_t)t.width * 16, (size_t)t.width * 16, (size_t)t.height,
+                            cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(e, "texture upload");
+    cudaResourceDesc rd;
+    std::memset(&rd, 0, sizeof(rd));
+    rd.resType = cudaResourceTypeArray;
+    rd.res.array.array = o.array;
+    cudaTextureDesc td;
+    std::memset(&td, 0, sizeof(td));
+    td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = (cudaTextureAddressMode)t.address;
+    td.filterMode = t.filter == NOOR_FILTER_LINEAR ? cudaFilterModeLinear : cudaFilterModePoint;
+    td.readMode = cudaReadModeElementType;
+    td.normalizedCoords = 1;
+    e = cudaCreateTextureObject(&o.obj, &rd, &td, nullptr);
+    if (e != cudaSuccess) return cuda_fail(e, "texture object");
+    textures[idx] = o;
+    *out = o.obj;
+    return NOOR_OK;
 }
 
 int SceneState::alloc(void** p, size_t bytes, const char* what) {
@@ -68,6 +107,33 @@ Context::~Context() {
         if (e) cudaEventDestroy(e);
     wavefront_release(*this);
     if (stream) cudaStreamDestroy(stream);
+}
+
+// The constant parameters (the first texel of each texture: a 1x1
+// texture's value) and, per slot read through the texture unit, the texture
+// object and uv scale.  `object(i)` makes (once) the texture object of
+// texture i.
+template <class Obj>
+static void resolve_textures(const noor_payload* P, const noor_material& m, DevMaterial& d, DevMatTex& t,
+                             Obj object) {
+    std::memset(&t, 0, sizeof(t));
+    auto image = [&](uint32_t idx) { return P->textures[idx].width != 1 || P->textures[idx].height != 1; };
+    auto slot = [&](uint32_t k, uint32_t idx, const float* uvscale) {
+        t.tex[k] = object(idx);
+        t.uvscale[k] = make_float2(uvscale ? uvscale[0] : 1.0f, uvscale ? uvscale[1] : 1.0f);
+        d.tex_mask |= 1u << k;
+    };
+    if (image(m.diffuse_tex_idx)) slot(kTexDiffuse, m.diffuse_tex_idx, m.diffuse_uvscale);
+    if (image(m.specular_tex_idx)) slot(kTexSpecular, m.specular_tex_idx, m.specular_uvscale);
+    if (image(m.emittance_tex_idx)) slot(kTexEmittance, m.emittance_tex_idx, m.emittance_uvscale);
+    if (image(m.roughness_tex_idx)) slot(kTexRoughness, m.roughness_tex_idx, m.roughness_uvscale);
+    // transmission, ior and k are read at uv scale 1 (materialimp.cuh:155-182)
+    if (image(m.transmission_tex_idx)) slot(kTexTransmission, m.transmission_tex_idx, nullptr);
+    if (image(m.ior_tex_idx)) slot(kTexIor, m.ior_tex_idx, nullptr);
+    if (image(m.k_tex_idx)) slot(kTexK, m.k_tex_idx, nullptr);
+    if (m.type & NOOR_ALPHA) slot(kTexAlpha, m.transparency_tex_idx, m.transparency_uvscale);
+    if (m.type & NOOR_BUMP) slot(kTexBump, m.bump_tex_idx, m.bump_uvscale);
+    t.bumpfactor = m.bumpfactor;
 }
 
 static void resolve_material(const noor_payload* P, const noor_material& m, DevMaterial& d) {
@@ -116,18 +182,20 @@ static int validate_payload(const noor_payload* P) {
             return set_error(NOOR_ERR_INVALID, "payload: missing transform rows");
     const noor_texture& env = P->textures[P->num_textures - 1];
     if (env.width <= 0 || env.height <= 0 || !env.rgba) return set_error(NOOR_ERR_INVALID, "payload: bad environment texture");
+    for (uint32_t i = 0; i + 1 < P->num_textures; ++i) {
+        const noor_texture& t = P->textures[i];
+        if (t.width <= 0 || t.height <= 0 || !t.rgba) return set_error(NOOR_ERR_INVALID, "payload: empty texture");
+        if (t.filter < NOOR_FILTER_POINT || t.filter > NOOR_FILTER_LINEAR || t.address < 0 || t.address > 3)
+            return set_error(NOOR_ERR_INVALID, "payload: texture filter or address mode out of range");
+    }
     for (uint32_t i = 0; i < P->num_materials; ++i) {
         const noor_material& m = P->materials[i];
-        const uint32_t idx[] = {m.diffuse_tex_idx, m.specular_tex_idx, m.transmission_tex_idx, m.emittance_tex_idx,
-                                m.ior_tex_idx, m.k_tex_idx, m.roughness_tex_idx};
-        for (uint32_t t : idx) {
-            if (t >= P->num_textures) return set_error(NOOR_ERR_INVALID, "payload: material texture index out of range");
-            if (P->textures[t].width != 1 || P->textures[t].height != 1 || !P->textures[t].rgba)
-                return set_error(NOOR_ERR_UNSUPPORTED, "payload: image-textured materials are not implemented");
-        }
-        const uint32_t t = m.type;
-        if (t & (NOOR_ALPHA | NOOR_BUMP))
-            return set_error(NOOR_ERR_UNSUPPORTED, "payload: alpha and bump maps are not implemented");
+        const uint32_t idx[] = {m.diffuse_tex_idx,  m.specular_tex_idx, m.transmission_tex_idx, m.emittance_tex_idx,
+                                m.ior_tex_idx,      m.k_tex_idx,        m.roughness_tex_idx,    m.transparency_tex_idx,
+                                m.bump_tex_idx,     m.metalness_tex_idx};
+        for (uint32_t t : idx)
+            if (t + 1 >= P->num_textures)
+                return set_error(NOOR_ERR_INVALID, "payload: material texture index out of range");
         // every other type is accepted: the ones factoryBSDF builds no lobe
         // for (Oren-Nayar, mixes of type bits) absorb, as in the reference
         // (bsdf.cuh:425-461)
@@ -364,14 +432,28 @@ int upload_scene(Context& C, const noor_payload* P, const noor_hosek_sky* H, con
     }
     {
         std::vector<DevMaterial> m(P->num_materials);
+        std::vector<DevMatTex> mt(P->num_materials);
+        int terr = NOOR_OK;
+        auto object = [&](uint32_t idx) -> cudaTextureObject_t {
+            cudaTextureObject_t o = 0;
+            if (terr == NOOR_OK) terr = st.texture_object(P->textures[idx], idx, &o);
+            return o;
+        };
         for (uint32_t i = 0; i < P->num_materials; ++i) {
             std::memset(&m[i], 0, sizeof(DevMaterial));
             resolve_material(P, P->materials[i], m[i]);
+            resolve_textures(P, P->materials[i], m[i], mt[i], object);
+            if (terr) return terr;
             const uint32_t l = lobe_of(m[i].type);
             if (l > 0xFFFFu || !lobe_common(l)) D.ext_lobes = 1u;
+            if (m[i].tex_mask) D.has_tex = 1u;
+            if (m[i].type & NOOR_ALPHA) D.has_alpha = 1u;
+            if (m[i].type & NOOR_BUMP) D.has_bump = 1u;
         }
         st.materials_host = m;
         if ((rc = st.upload((void**)&D.materials, m.data(), m.size() * sizeof(DevMaterial), "materials"))) return rc;
+        if ((rc = st.upload((void**)&D.mat_tex, mt.data(), mt.size() * sizeof(DevMatTex), "material textures")))
+            return rc;
     }
     {
         std::vector<DevAreaLight> l(P->num_area_lights);

@@ -24,7 +24,110 @@ struct Isect {
     uint32_t mtype;
     uint32_t lobe;
     uint32_t mat;
+    float2 uv;      // the hit's texture coordinates (barycentrics on emitters); set where textures are read
 };
+
+// material types whose scattered ray keeps differentials
+// (CudaIntersection::isGlossy, NOOR_GLOSSY of path_tracer.cuh:121-124)
+constexpr uint32_t kGlossyMat =
+    NOOR_MIRROR | NOOR_GLASS | NOOR_CLEARCOAT | NOOR_ROUGHGLASS | NOOR_METAL | NOOR_SUBSTRATE | NOOR_GLOSSY;
+// material types with a dielectric Fresnel lobe, which set the intersection's
+// eta (CudaBxDF::factoryFresnel, bxdf.cuh:190-200)
+constexpr uint32_t kDielectricMat = NOOR_GLASS | NOOR_ROUGHGLASS | NOOR_GLOSSY | NOOR_SUBSTRATE | NOOR_CLEARCOAT;
+
+// the texture-read slots of a material at uv (materialimp.cuh:121-183):
+// colours and roughness replace the load-time constants
+NB_D void apply_textures(const DevScene& S, uint32_t mi, float2 uv, DevMaterial& m) {
+    const DevMatTex& T = S.mat_tex[mi];
+    const uint32_t k = m.tex_mask;
+    if (k & (1u << kTexDiffuse)) m.diffuse = f3(slot_tex(T, kTexDiffuse, uv));
+    if (k & (1u << kTexSpecular)) m.specular = f3(slot_tex(T, kTexSpecular, uv));
+    if (k & (1u << kTexEmittance)) m.emittance = f3(slot_tex(T, kTexEmittance, uv));
+    if (k & (1u << kTexTransmission)) m.transmission = f3(slot_tex(T, kTexTransmission, uv));
+    if (k & (1u << kTexIor)) m.ior = f3(slot_tex(T, kTexIor, uv));
+    if (k & (1u << kTexK)) m.k = f3(slot_tex(T, kTexK, uv));
+    if (k & (1u << kTexRoughness)) {
+        const float4 r = slot_tex(T, kTexRoughness, uv);
+        m.rough_x = r.x;
+        m.rough_y = r.y;
+    }
+}
+
+// The hit's differentials (CudaIntersection::computeDifferential,
+// intersection.cuh:397-441): where the offset rays meet the tangent plane,
+// and the uv steps solving dp = dpdu du + dpdv dv on the two largest axes of
+// the geometric normal.  All zero where an offset ray misses the plane.
+struct HitDiff {
+    float3 dpdx, dpdy, dndu, dndv;
+    float dudx, dudy, dvdx, dvdy;
+};
+NB_D void solve2x2(float a00, float a01, float a10, float a11, float b0, float b1, float& x0, float& x1) {
+    const float det = a00 * a11 - a10 * a01;
+    if (fabsf(det) < 1e-10f) {
+        x0 = x1 = 0.0f;
+        return;
+    }
+    const float inv = 1.0f / det;
+    x0 = (a11 * b0 - a01 * b1) * inv;
+    x1 = (a00 * b1 - a10 * b0) * inv;
+    if (isnan(x0) || isnan(x1)) x0 = x1 = 0.0f;
+}
+NB_D HitDiff hit_differential(const Isect& I, const TangentOut& to, const RayDiff& rd) {
+    HitDiff h;
+    h.dndu = to.dndu;
+    h.dndv = to.dndv;
+    h.dpdx = h.dpdy = f3(0.0f);
+    h.dudx = h.dudy = h.dvdx = h.dvdy = 0.0f;
+    const float3& n = I.F.ng;
+    const float dd = dot(n, I.p);
+    const float tx = -(dot(n, rd.odx) - dd) / dot(n, rd.ddx);
+    if (isinf(tx) || isnan(tx)) return h;
+    const float3 px = rd.odx + tx * rd.ddx;
+    const float ty = -(dot(n, rd.ody) - dd) / dot(n, rd.ddy);
+    if (isinf(ty) || isnan(ty)) return h;
+    const float3 py = rd.ody + ty * rd.ddy;
+    h.dpdx = px - I.p;
+    h.dpdy = py - I.p;
+    int ax, ay;
+    if (fabsf(n.x) > fabsf(n.y) && fabsf(n.x) > fabsf(n.z)) {
+        ax = 1;
+        ay = 2;
+    } else if (fabsf(n.y) > fabsf(n.z)) {
+        ax = 0;
+        ay = 2;
+    } else {
+        ax = 0;
+        ay = 1;
+    }
+    const float a00 = comp(to.dpdu, ax), a01 = comp(to.dpdv, ax), a10 = comp(to.dpdu, ay), a11 = comp(to.dpdv, ay);
+    solve2x2(a00, a01, a10, a11, comp(h.dpdx, ax), comp(h.dpdx, ay), h.dudx, h.dvdx);
+    solve2x2(a00, a01, a10, a11, comp(h.dpdy, ax), comp(h.dpdy, ay), h.dudy, h.dvdy);
+    return h;
+}
+
+// Bump mapping (accumulate.cuh:47-75, after PBRT): the bump map's slopes
+// over a uv step of half the pixel's footprint (0.001 where it is zero)
+// tilt dp/du and dp/dv along the shading normal; the frame is rebuilt from
+// them and the normal turned to the geometric normal's side.
+NB_D void bump(const DevScene& S, uint32_t mi, float2 uv, const HitDiff& h, Frame& F) {
+    const DevMatTex& T = S.mat_tex[mi];
+    float du = 0.5f * (fabsf(h.dudx) + fabsf(h.dudy));
+    float dv = 0.5f * (fabsf(h.dvdx) + fabsf(h.dvdy));
+    du = du == 0.0f ? 0.001f : du;
+    dv = dv == 0.0f ? 0.001f : dv;
+    const float disp = slot_tex(T, kTexBump, uv).x;
+    const float scale = T.bumpfactor;
+    const float ud = scale * (slot_tex(T, kTexBump, f2(uv.x + du, uv.y + 0.0f)).x - disp) / du;
+    const float vd = scale * (slot_tex(T, kTexBump, f2(uv.x + 0.0f, uv.y + dv)).x - disp) / dv;
+    const float3 sn = F.n;
+    float3 dpdu = F.s + ud * sn;
+    const float3 dpdv = F.t + vd * sn;
+    float3 n = normalize_guard(cross(dpdu, dpdv));
+    dpdu = normalize_guard(dpdu - n * dot(n, dpdu));
+    F.t = normalize_guard(cross(n, dpdu));
+    F.s = dpdu;
+    F.n = dot(F.ng, n) < 0.0f ? -1.0f * n : n;   // NOOR::faceforward
+}
 
 struct RayStats {
     uint32_t ext;
@@ -312,13 +415,62 @@ NB_D float3 bsdf_mis_contrib(const DevScene& S, const DevMaterial& m, const Isec
     return c;
 }
 
+// The differentials of the scattered ray (CudaIntersection::spawnRay,
+// intersection.cuh:111-186): mirror or refraction offsets from the normal's
+// derivatives, pulled a quarter of the way back to the ray itself.  `o` is
+// the scattered ray's origin; eta the intersection's (1 unless a
+// dielectric lobe set it).
+NB_D RayDiff spawn_diff(const Isect& I, const HitDiff& h, const RayDiff& in, const float3& o, const float3& wi,
+                        float eta_in) {
+    RayDiff r;
+    r.on = true;
+    r.odx = o + h.dpdx;
+    r.ody = o + h.dpdy;
+    const float3& sn = I.F.n;
+    const float3& wo = I.wo;
+    const float3 dwodx = -1.0f * (in.ddx + wo);
+    const float3 dwody = -1.0f * (in.ddy + wo);
+    if (dot(wi, I.F.ng) >= 0.0f) {
+        const float3 dndx = h.dndu * h.dudx + h.dndv * h.dvdx;
+        const float3 dndy = h.dndu * h.dudy + h.dndv * h.dvdy;
+        const float dDNdx = dot(dwodx, sn) + dot(wo, dndx);
+        const float dDNdy = dot(dwody, sn) + dot(wo, dndy);
+        r.ddx = wi - dwodx + 2.0f * (dot(wo, sn) * dndx + dDNdx * sn);
+        r.ddy = wi - dwody + 2.0f * (dot(wo, sn) * dndy + dDNdy * sn);
+    } else {
+        const float3 w = -1.0f * wo;
+        const float eta = dot(wo, sn) > 0.0f ? 1.0f / eta_in : eta_in;
+        const float3 dndx = h.dndu * h.dudx + h.dndv * h.dvdx;
+        // the reference's dn/dy pairs dn/dv with both du/dy and dv/dy
+        const float3 dndy = h.dndv * h.dudy + h.dndv * h.dvdy;
+        const float dDNdx = dot(dwodx, sn) + dot(wo, dndx);
+        const float dDNdy = dot(dwody, sn) + dot(wo, dndy);
+        const float mu = eta * dot(w, sn) - dot(wi, sn);
+        const float dmudx = (eta - (eta * eta * dot(w, sn)) / dot(wi, sn)) * dDNdx;
+        const float dmudy = (eta - (eta * eta * dot(w, sn)) / dot(wi, sn)) * dDNdy;
+        r.ddx = wi + eta * dwodx - (mu * dndx + dmudx * sn);
+        r.ddy = wi + eta * dwody - (mu * dndy + dmudy * sn);
+    }
+    // scaleDifferentials(.25f) (ray.cuh:182-189)
+    const float s = 0.25f;
+    r.odx = (1.0f - s) * o + s * r.odx;
+    r.ody = (1.0f - s) * o + s * r.ody;
+    r.ddx = (1.0f - s) * wi + s * r.ddx;
+    r.ddy = (1.0f - s) * wi + s * r.ddy;
+    return r;
+}
+
 // Builds the hit record of CudaIntersection (intersection.cuh:319-377).
+// With `to`, also the texture coordinates and derivatives of TangentOut
+// (I.uv: the barycentrics on an emitter, whose record stops before them).
 template <int ISECT, bool EXT = true>
-NB_D void make_isect(const DevScene& S, const float3& o, const float3& d, float t, const HitRec& rec, Isect& I) {
+NB_D void make_isect(const DevScene& S, const float3& o, const float3& d, float t, const HitRec& rec, Isect& I,
+                     TangentOut* to = nullptr) {
     I.p = o + t * d;
     I.wo = normalize_fast(-1.0f * d);
     I.mtype = rec.mtype;
     I.lobe = lobe_of<EXT>(rec.mtype);
+    if (to) I.uv = f2(rec.u, rec.v);
     if (ISECT == NOOR_ISECT_WATERTIGHT) {
         const DevWtTri* T = S.wtri + rec.tri;
         const uint4 attr = __ldg(&T->attr);
@@ -328,21 +480,25 @@ NB_D void make_isect(const DevScene& S, const float3& o, const float3& d, float 
         vv[0] = __ldg(&T->v0);
         vv[1] = __ldg(&T->v1);
         vv[2] = __ldg(&T->v2);
-        I.F = tangent_frame(S, attr, rec.ins, rec.u, rec.v, vv);
+        I.F = tangent_frame(S, attr, rec.ins, rec.u, rec.v, vv, to);
     } else {
         const uint4 attr = __ldg(&S.wald[rec.tri].attr);
         I.mat = attr.w;
         if (rec.mtype & kEmitterMat) return;
-        I.F = tangent_frame(S, attr, rec.ins, rec.u, rec.v, nullptr);
+        I.F = tangent_frame(S, attr, rec.ins, rec.u, rec.v, nullptr, to);
     }
+    if (to) I.uv = to->uv;
 }
 
 // pathtracer() of noor/cuda/path_tracer.cu:26-75; returns clamp(L, 0, 100)
 // EXT false: the specialisation for scenes whose materials use only the
 // Lambert, conductor and Fresnel-specular lobes
-template <int ISECT, bool EXT = true>
+// DIFF: the specialisation for scenes with bump maps, whose rays carry
+// differentials (rd: the camera ray's) -- the reference bumps only where a
+// differential ray arrives (accumulate.cuh:90-92)
+template <int ISECT, bool EXT = true, bool DIFF = false>
 NB_D float3 path_radiance(const DevScene& S, float3 o, float3 d, Rng& rng, const SmemStack& st, uint32_t* status,
-                          RayStats& rs, float3* first_hit, bool* first_hit_valid) {
+                          RayStats& rs, float3* first_hit, bool* first_hit_valid, RayDiff rd = RayDiff{}) {
     float3 L = f3(0.0f);
     float3 beta = f3(1.0f);
     bool spec_bounce = false;
@@ -355,7 +511,9 @@ NB_D float3 path_radiance(const DevScene& S, float3 o, float3 d, Rng& rng, const
             break;
         }
         Isect I;
-        make_isect<ISECT, EXT>(S, o, d, tmax, rec, I);
+        TangentOut to;
+        const bool tex = EXT && S.has_tex;
+        make_isect<ISECT, EXT>(S, o, d, tmax, rec, I, tex ? &to : nullptr);
         if (bounce == 0 && first_hit) {
             *first_hit = I.p;
             *first_hit_valid = true;
@@ -365,14 +523,21 @@ NB_D float3 path_radiance(const DevScene& S, float3 o, float3 d, Rng& rng, const
                 if (I.mtype & NOOR_MESHLIGHT) {
                     L += beta * area_le<EXT>(S.area_lights[rec.ins], d);
                 } else {
-                    const DevMaterial& em = S.materials[I.mat];
+                    DevMaterial em = S.materials[I.mat];
+                    if (tex && em.tex_mask) apply_textures(S, I.mat, I.uv, em);
                     L += beta * (em.emitter_scale * em.emittance);
                 }
             }
             // an emitter has no BSDF lobe: nothing more can be added
             break;
         }
-        const DevMaterial m = S.materials[I.mat];
+        DevMaterial m = S.materials[I.mat];
+        HitDiff hd;
+        if (DIFF && rd.on) {
+            hd = hit_differential(I, to, rd);
+            if (I.mtype & NOOR_BUMP) bump(S, I.mat, I.uv, hd, I.F);
+        }
+        if (tex && m.tex_mask) apply_textures(S, I.mat, I.uv, m);
         // accumulate (accumulate.cuh:83-99): direct lighting, then scatter
         int li = 0;
         bool picked;
@@ -410,6 +575,12 @@ NB_D float3 path_radiance(const DevScene& S, float3 o, float3 d, Rng& rng, const
         }
         spec_bounce = (I.mtype & kSpecularMat) != 0;
         o = spawn_origin(I, wi, S.bias);
+        if (DIFF) {
+            if (rd.on && (I.mtype & kGlossyMat))
+                rd = spawn_diff(I, hd, rd, o, wi, (I.mtype & kDielectricMat) ? m.coat_ior : 1.0f);
+            else
+                rd.on = false;
+        }
         d = wi;
     }
     return clamp3(L, 0.0f, 100.0f);

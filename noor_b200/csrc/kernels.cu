@@ -30,7 +30,7 @@ NB_D void kahan_add(float3& sum, float3& c, const float3& x) {
 #define NB_MEGA_MIN_BLOCKS 7
 #endif
 
-template <int ISECT, int FILM, bool EXT>
+template <int ISECT, int FILM, bool EXT, bool DIFF = false>
 __global__ void __launch_bounds__(kMegaBlock, NB_MEGA_MIN_BLOCKS) megakernel(DevScene S, DevCamera C, MegaArgs a) {
     extern __shared__ uint32_t smem[];
     const uint32_t npix = C.w * C.h;
@@ -62,10 +62,14 @@ __global__ void __launch_bounds__(kMegaBlock, NB_MEGA_MIN_BLOCKS) megakernel(Dev
             const uint32_t frame = a.frame0 + f;
             Rng rng{tea16(pix, frame)};
             float3 o, d;
-            camera_ray<EXT>(C, x, y, rng, o, d);
+            RayDiff rd{};
+            if (DIFF)
+                camera_ray_diff(C, x, y, rng, o, d, rd);
+            else
+                camera_ray<EXT>(C, x, y, rng, o, d);
             hit_valid = false;
-            const float3 L = path_radiance<ISECT, EXT>(S, o, d, rng, st, a.status, rs,
-                                                       want_hit ? &hitp : nullptr, &hit_valid);
+            const float3 L = path_radiance<ISECT, EXT, DIFF>(S, o, d, rng, st, a.status, rs,
+                                                             want_hit ? &hitp : nullptr, &hit_valid, rd);
             ++paths;
             if (FILM == NOOR_FILM_KAHAN) {
                 kahan_add(sum, comp, L);
@@ -318,16 +322,17 @@ cudaError_t launch_megakernel(const DevScene& S, const DevCamera& C, const MegaA
     // a specialisation without the other code (the kernel's registers are
     // capped, so unused branches cost spills)
     const bool ext_cam = C.type != NOOR_CAMERA_PERSP || C.lens_radius > 0.0f;
-#define NB_MK2(I, F, X)                                                                         \
+#define NB_MK2(I, F, X, D)                                                                      \
     do {                                                                                        \
-        e = cudaFuncSetAttribute(megakernel<I, F, X>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm); \
+        e = cudaFuncSetAttribute(megakernel<I, F, X, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm); \
         if (e != cudaSuccess) return e;                                                         \
-        megakernel<I, F, X><<<grid, kMegaBlock, sm, s>>>(S, C, a);                              \
+        megakernel<I, F, X, D><<<grid, kMegaBlock, sm, s>>>(S, C, a);                           \
     } while (0)
 #define NB_MK(I, F)                     \
     do {                                \
-        if (S.ext_lobes || S.ext_lights || S.env_ref || ext_cam) NB_MK2(I, F, true); \
-        else NB_MK2(I, F, false);       \
+        if (S.has_bump) NB_MK2(I, F, true, true); \
+        else if (S.ext_lobes || S.ext_lights || S.env_ref || S.has_tex || ext_cam) NB_MK2(I, F, true, false); \
+        else NB_MK2(I, F, false, false); \
     } while (0)
     if (S.isect == NOOR_ISECT_WATERTIGHT) {
         if (S.film_mode == NOOR_FILM_KAHAN) NB_MK(NOOR_ISECT_WATERTIGHT, NOOR_FILM_KAHAN);

@@ -1,6 +1,7 @@
 // Host-side state of a render context (one per thread).
 #pragma once
 #include <cuda_runtime.h>
+#include <map>
 #include <memory>
 #include <vector>
 
@@ -25,9 +26,16 @@ struct SceneState {
     float* ref_func = nullptr;
     float* ref_cdf = nullptr;
     bool ref_built = false;
+    // material textures read through the texture unit, by payload index
+    struct TexObj {
+        cudaArray_t array;
+        cudaTextureObject_t obj;
+    };
+    std::map<uint32_t, TexObj> textures;
     ~SceneState();
     int alloc(void** p, size_t bytes, const char* what);
     int upload(void** p, const void* host, size_t bytes, const char* what);
+    int texture_object(const noor_texture& t, uint32_t idx, cudaTextureObject_t* out);
 };
 
 struct WavefrontState;  // wavefront.cu

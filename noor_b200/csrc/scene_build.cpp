@@ -788,6 +788,7 @@ struct noor_payload_handle {
     std::vector<uint32_t> bvh_lo, bvh_hi;
     uint32_t root = 0;
     std::vector<std::vector<float>> tex_data;
+    std::vector<noor_texture> tex_meta;       // width, height, filter, address of each texture
     std::vector<noor_texture> textures;
     std::vector<noor_area_light> lights;
     std::vector<noor_point_light> point_lights;
@@ -801,8 +802,16 @@ struct noor_payload_handle {
     int32_t skydome_type = 0;
 };
 
+// a 1x1 constant (ImageTexture(float3), point filtered, clamped)
 static uint32_t add_texture(noor_payload_handle* h, const float* rgb, float a) {
     h->tex_data.push_back({rgb[0], rgb[1], rgb[2], a});
+    h->tex_meta.push_back(noor_texture{1, 1, nullptr, NOOR_FILTER_POINT, NOOR_ADDRESS_CLAMP});
+    return (uint32_t)h->tex_data.size() - 1;
+}
+// an image map (ImageTexture(file): wrapped, linear unless given)
+static uint32_t add_image(noor_payload_handle* h, const noor_image& im, int32_t filter) {
+    h->tex_data.emplace_back(im.rgba, im.rgba + 4 * (size_t)im.width * im.height);
+    h->tex_meta.push_back(noor_texture{im.width, im.height, nullptr, filter, NOOR_ADDRESS_WRAP});
     return (uint32_t)h->tex_data.size() - 1;
 }
 
@@ -848,6 +857,14 @@ static int build_payload(const noor_scene_desc* d, bool gpu, noor_payload_handle
     for (uint32_t i = 0; i < d->num_triangles; ++i)
         if (d->material_indices[i] >= d->num_materials)
             return set_error(NOOR_ERR_INVALID, "noor_build_payload: material index out of range");
+    if (d->num_images && !d->images) return set_error(NOOR_ERR_INVALID, "noor_build_payload: image count without an array");
+    for (uint32_t i = 0; i < d->num_images; ++i)
+        if (d->images[i].width <= 0 || d->images[i].height <= 0 || !d->images[i].rgba)
+            return set_error(NOOR_ERR_INVALID, "noor_build_payload: empty image map");
+    for (uint32_t i = 0; i < d->num_materials; ++i)
+        for (int k = 0; k < NOOR_NUM_MAPS; ++k)
+            if (d->materials[i].map[k] < -1 || d->materials[i].map[k] >= (int32_t)d->num_images)
+                return set_error(NOOR_ERR_INVALID, "noor_build_payload: material map names a missing image");
 
     const auto t0 = std::chrono::steady_clock::now();
     std::unique_ptr<noor_payload_handle> h(new (std::nothrow) noor_payload_handle());
@@ -895,17 +912,35 @@ static int build_payload(const noor_scene_desc* d, bool gpu, noor_payload_handle
                 h->xf[6 + r].insert(h->xf[6 + r].end(), wg, wg + 4);
             }
         }
-        // materials + constant textures (Model::loadMaterial, model.cpp:184-330)
+        // materials and textures (Model::loadMaterial, model.cpp:184-330): a
+        // texture of 0.5 first; per material its constants as 1x1 textures
+        // and its image maps, one texture per image, made at the image's
+        // first use with that use's filter (map_d point, the others linear).
+        // One record is carried from material to material, as the reference
+        // reuses one CudaMaterial: the uv scale of a slot without a map, and
+        // the bump fields of a material without a bump map, keep the values
+        // an earlier material set.
         const float half[3] = {0.5f, 0.5f, 0.5f};
         add_texture(h.get(), half, 1.0f);
+        std::vector<int64_t> image_tex(d->num_images, -1);
+        auto map_texture = [&](int32_t img, int32_t filter) -> uint32_t {
+            if (image_tex[img] < 0) image_tex[img] = add_image(h.get(), d->images[img], filter);
+            return (uint32_t)image_tex[img];
+        };
+        noor_material mt;
+        std::memset(&mt, 0, sizeof(mt));
+        for (float* s : {mt.diffuse_uvscale, mt.specular_uvscale, mt.transparency_uvscale, mt.emittance_uvscale,
+                         mt.bump_uvscale, mt.roughness_uvscale, mt.metalness_uvscale})
+            s[0] = s[1] = 1.0f;
+        mt.bumpfactor = 1.0f;
         for (uint32_t i = 0; i < d->num_materials; ++i) {
             const noor_material_desc& md = d->materials[i];
-            noor_material mt;
-            std::memset(&mt, 0, sizeof(mt));
-            for (float* s : {mt.diffuse_uvscale, mt.specular_uvscale, mt.transparency_uvscale, mt.emittance_uvscale,
-                             mt.bump_uvscale, mt.roughness_uvscale, mt.metalness_uvscale})
-                s[0] = s[1] = 1.0f;
-            mt.bumpfactor = 1.0f;
+            auto mapped = [&](int slot, float* uvscale) {
+                if (md.map[slot] < 0) return false;
+                uvscale[0] = md.map_uvscale[slot][0];
+                uvscale[1] = md.map_uvscale[slot][1];
+                return true;
+            };
             mt.coat_weight = md.coat_weight;
             mt.coat_roughness = md.coat_roughness;
             mt.coat_thickness = md.coat_thickness;
@@ -917,14 +952,34 @@ static int build_payload(const noor_scene_desc* d, bool gpu, noor_payload_handle
             mt.transmission_tex_idx = add_texture(h.get(), md.transmission, 1.0f);
             mt.ior_tex_idx = add_texture(h.get(), md.ior, 1.0f);
             mt.k_tex_idx = add_texture(h.get(), md.k, 1.0f);
-            mt.diffuse_tex_idx = add_texture(h.get(), md.diffuse, 1.0f);
+            mt.diffuse_tex_idx = mapped(NOOR_MAP_DIFFUSE, mt.diffuse_uvscale)
+                                     ? map_texture(md.map[NOOR_MAP_DIFFUSE], NOOR_FILTER_LINEAR)
+                                     : add_texture(h.get(), md.diffuse, 1.0f);
             const float rough[3] = {md.roughness[0], md.roughness[1], 1.0f};
-            mt.roughness_tex_idx = add_texture(h.get(), rough, 1.0f);
+            mt.roughness_tex_idx = mapped(NOOR_MAP_ROUGHNESS, mt.roughness_uvscale)
+                                       ? map_texture(md.map[NOOR_MAP_ROUGHNESS], NOOR_FILTER_LINEAR)
+                                       : add_texture(h.get(), rough, 1.0f);
             const float metal[3] = {1.0f, 1.0f, 1.0f};
-            mt.metalness_tex_idx = add_texture(h.get(), metal, 1.0f);
-            mt.specular_tex_idx = add_texture(h.get(), md.specular, 1.0f);
-            mt.emittance_tex_idx = add_texture(h.get(), md.emittance, 1.0f);
-            mt.transparency_tex_idx = add_texture(h.get(), md.transparency, 1.0f);
+            mt.metalness_tex_idx = mapped(NOOR_MAP_METALNESS, mt.metalness_uvscale)
+                                       ? map_texture(md.map[NOOR_MAP_METALNESS], NOOR_FILTER_LINEAR)
+                                       : add_texture(h.get(), metal, 1.0f);
+            mt.specular_tex_idx = mapped(NOOR_MAP_SPECULAR, mt.specular_uvscale)
+                                      ? map_texture(md.map[NOOR_MAP_SPECULAR], NOOR_FILTER_LINEAR)
+                                      : add_texture(h.get(), md.specular, 1.0f);
+            mt.emittance_tex_idx = mapped(NOOR_MAP_EMITTANCE, mt.emittance_uvscale)
+                                       ? map_texture(md.map[NOOR_MAP_EMITTANCE], NOOR_FILTER_LINEAR)
+                                       : add_texture(h.get(), md.emittance, 1.0f);
+            if (mapped(NOOR_MAP_ALPHA, mt.transparency_uvscale)) {
+                mt.transparency_tex_idx = map_texture(md.map[NOOR_MAP_ALPHA], NOOR_FILTER_POINT);
+                mt.type |= NOOR_ALPHA;
+            } else {
+                mt.transparency_tex_idx = add_texture(h.get(), md.transparency, 1.0f);
+            }
+            if (mapped(NOOR_MAP_BUMP, mt.bump_uvscale)) {
+                mt.bump_tex_idx = map_texture(md.map[NOOR_MAP_BUMP], NOOR_FILTER_LINEAR);
+                mt.bumpfactor = md.bumpfactor;
+                mt.type |= NOOR_BUMP;
+            }
             h->materials.push_back(mt);
         }
         // environment texture last
@@ -932,15 +987,14 @@ static int build_payload(const noor_scene_desc* d, bool gpu, noor_payload_handle
             if (!d->env_rgba || d->env_width <= 0 || d->env_height <= 0)
                 return set_error(NOOR_ERR_INVALID, "noor_build_payload: HDR sky without an environment map");
             h->tex_data.emplace_back(d->env_rgba, d->env_rgba + 4 * (size_t)d->env_width * d->env_height);
+            h->tex_meta.push_back(noor_texture{d->env_width, d->env_height, nullptr, NOOR_FILTER_LINEAR,
+                                               NOOR_ADDRESS_CLAMP});
         } else {
             const float sky[3] = {0.25f, 0.25f, 0.25f};
             add_texture(h.get(), sky, 1.0f);
         }
         for (size_t i = 0; i < h->tex_data.size(); ++i) {
-            noor_texture t;
-            const bool env = (i + 1 == h->tex_data.size()) && d->skydome_type == NOOR_SKY_HDR;
-            t.width = env ? d->env_width : 1;
-            t.height = env ? d->env_height : 1;
+            noor_texture t = h->tex_meta[i];
             t.rgba = h->tex_data[i].data();
             h->textures.push_back(t);
         }

@@ -59,7 +59,30 @@ struct __align__(16) DevMaterial {
     float coat_weight;      // clear coat
     float coat_sigma;
     float coat_thickness;
-    float pad;
+    uint32_t tex_mask;      // kTex* slots read through the texture unit (DevMatTex)
+};
+
+// Material slots whose texture is an image map (or, for the alpha and bump
+// slots of ALPHA / BUMP materials, any texture): fetched per hit by the
+// texture unit with the texture's own filter and addressing, at the hit's
+// uv times the slot's scale (noor/cuda/materialimp.cuh:121-183).
+enum : uint32_t {
+    kTexDiffuse = 0,
+    kTexSpecular = 1,
+    kTexEmittance = 2,
+    kTexRoughness = 3,
+    kTexTransmission = 4,
+    kTexIor = 5,
+    kTexK = 6,
+    kTexAlpha = 7,
+    kTexBump = 8,
+    kTexSlots = 9
+};
+struct DevMatTex {
+    cudaTextureObject_t tex[kTexSlots];
+    float2 uvscale[kTexSlots];
+    float bumpfactor;
+    float pad[3];
 };
 
 struct DevAreaLight {
@@ -139,6 +162,7 @@ struct DevScene {
     const float2* uvs;
     const DevXform* xforms;
     const DevMaterial* materials;
+    const DevMatTex* mat_tex;   // per material; read only where tex_mask is set
     const DevAreaLight* area_lights;
     const DevDeltaLight* delta_lights;
     const float4* env;      // env texels (HDR / baked sky / constant), w*h
@@ -166,6 +190,9 @@ struct DevScene {
     int stack_cap;
     uint32_t ext_lobes;     // some material uses a lobe beyond Lambert, conductor, Fresnel specular
     uint32_t ext_lights;    // sphere or disk area lights, point, spot or distant lights
+    uint32_t has_tex;       // some material reads a texture per hit (image maps, alpha, bump)
+    uint32_t has_alpha;     // some material is ALPHA: triangle tests fetch its alpha map
+    uint32_t has_bump;      // some material is BUMP: rays carry differentials
     // NOOR_ENV_REFERENCE: the reference's distribution tables (row r at
     // r * (rw + 1), the marginal at rh * (rw + 1)) and the environment as a
     // texture object (linear filter, clamp, normalised coordinates)
@@ -175,5 +202,29 @@ struct DevScene {
     const float* rcdf;
     int rw, rh;
 };
+
+#ifdef __CUDACC__
+// a texture slot at uv, scaled per component (uvscale * uv), fetched by the
+// texture unit (CudaTexture::evaluate, noor/cuda/texture.cuh:113-126)
+// (coordinates rounded per operation: the fetch sees the coordinate the
+// reference's arithmetic gives, and its 8-bit filter weights amplify any
+// last-bit difference)
+__device__ __forceinline__ float4 slot_tex(const DevMatTex& T, uint32_t k, float2 uv) {
+    const float2 s = T.uvscale[k];
+    return tex2D<float4>(T.tex[k], __fmul_rn(s.x, uv.x), __fmul_rn(s.y, uv.y));
+}
+// texture coordinates of a triangle's vertex as the mesh manager returns
+// them, v flipped (noor/cuda/mesh.cuh:145-148)
+__device__ __forceinline__ float2 vertex_uv(const DevScene& S, uint32_t i) {
+    const float2 t = __ldg(&S.uvs[i]);
+    return make_float2(t.x, 1.0f - t.y);
+}
+// the barycentric interpolation (1 - u - v) uv0 + u uv1 + v uv2
+__device__ __forceinline__ float2 lerp_uv(float2 a, float2 b, float2 c, float bu, float bv) {
+    const float w = __fsub_rn(__fsub_rn(1.0f, bu), bv);
+    return make_float2(__fadd_rn(__fadd_rn(__fmul_rn(w, a.x), __fmul_rn(bu, b.x)), __fmul_rn(bv, c.x)),
+                       __fadd_rn(__fadd_rn(__fmul_rn(w, a.y), __fmul_rn(bu, b.y)), __fmul_rn(bv, c.y)));
+}
+#endif
 
 }  // namespace nb

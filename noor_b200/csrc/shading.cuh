@@ -85,6 +85,88 @@ NB_D void camera_ray(const DevCamera& C, uint32_t x, uint32_t y, Rng& rng, float
     d = normalize_fast(dw);
 }
 
+// Ray differentials of CudaRay (noor/cuda/ray.cuh:36-200): the offset rays
+// one pixel right (dx) and down (dy); world space.
+struct RayDiff {
+    bool on;
+    float3 odx, ody, ddx, ddy;
+};
+
+// generateRay with the differentials every camera type gives its ray
+// (cameraimp.cuh:71-89, 183-228, 236-252), then CudaRay::transform
+// (ray.cuh:160-174): the origins as points, the directions as vectors (the
+// offset directions are not renormalised).  Draws the same numbers as
+// camera_ray.
+NB_D void camera_ray_diff(const DevCamera& C, uint32_t x, uint32_t y, Rng& rng, float3& o, float3& d, RayDiff& rd) {
+    const float rx = (float)x + rng.next() - 0.5f;
+    const float ry = (float)y + rng.next() - 0.5f;
+    float3 dc, oc = f3(0.0f), odx = f3(0.0f), ody = f3(0.0f), ddx, ddy;
+    const float3 dxc = f3(C.r2c[0].x, C.r2c[1].x, C.r2c[2].x);   // _dxCamera
+    const float3 dyc = f3(C.r2c[0].y, C.r2c[1].y, C.r2c[2].y);   // _dyCamera
+    auto env_dir = [&](float px, float py) {
+        const float theta = kPi * py / (float)C.h + kPi;
+        const float phi = k2Pi * px / (float)C.w - kPiOver2;
+        const float st = sinf(theta), ct = cosf(theta);
+        return normalize_fast(normalize_fast(f3(st * cosf(phi), ct, st * sinf(phi))));
+    };
+    if (C.type == NOOR_CAMERA_ENV) {
+        dc = env_dir(rx, ry);
+        ddx = env_dir(rx + 1.0f, ry);
+        ddy = env_dir(rx, ry + 1.0f);
+    } else {
+        const float3 pc = f3(C.r2c[0].w + (C.r2c[0].x * rx + C.r2c[0].y * ry + C.r2c[0].z * 0.0f),
+                             C.r2c[1].w + (C.r2c[1].x * rx + C.r2c[1].y * ry + C.r2c[1].z * 0.0f),
+                             C.r2c[2].w + (C.r2c[2].x * rx + C.r2c[2].y * ry + C.r2c[2].z * 0.0f));
+        if (C.type == NOOR_CAMERA_ORTHO) {
+            oc = pc;
+            dc = f3(0.0f, 0.0f, -1.0f);
+            odx = oc + dxc;
+            ody = oc + dyc;
+            ddx = ddy = dc;
+        } else {
+            dc = normalize_fast(pc);
+            if (C.lens_radius > 0.0f) {
+                const float u1 = rng.next();
+                const float u2 = rng.next();
+                const float2 l = concentric_disk(u1, u2);
+                const float2 pl = f2(C.lens_radius * l.x, C.lens_radius * l.y);
+                float ft = -C.focal_length / dc.z;
+                const float3 pf = f3(0.0f) + ft * dc;
+                oc = f3(pl.x, pl.y, 0.0f);
+                dc = normalize_fast(pf - oc);
+                const float3 dx = normalize_fast(pc + dxc);
+                ft = -C.focal_length / dx.z;
+                odx = f3(pl.x, pl.y, 0.0f);
+                ddx = normalize_fast(f3(0.0f) + ft * dx - odx);
+                const float3 dy = normalize_fast(pc + dyc);
+                ft = -C.focal_length / dy.z;
+                ody = f3(pl.x, pl.y, 0.0f);
+                ddy = normalize_fast(f3(0.0f) + ft * dy - ody);
+            } else {
+                ddx = normalize_fast(pc + dxc);
+                ddy = normalize_fast(pc + dyc);
+            }
+        }
+    }
+    auto point = [&](const float3& p) {
+        return f3(C.c2w[0].w + (C.c2w[0].x * p.x + C.c2w[0].y * p.y + C.c2w[0].z * p.z),
+                  C.c2w[1].w + (C.c2w[1].x * p.x + C.c2w[1].y * p.y + C.c2w[1].z * p.z),
+                  C.c2w[2].w + (C.c2w[2].x * p.x + C.c2w[2].y * p.y + C.c2w[2].z * p.z));
+    };
+    auto vec = [&](const float3& v) {
+        return f3(C.c2w[0].x * v.x + C.c2w[0].y * v.y + C.c2w[0].z * v.z,
+                  C.c2w[1].x * v.x + C.c2w[1].y * v.y + C.c2w[1].z * v.z,
+                  C.c2w[2].x * v.x + C.c2w[2].y * v.y + C.c2w[2].z * v.z);
+    };
+    o = point(oc);
+    d = normalize_fast(vec(dc));
+    rd.on = true;
+    rd.odx = point(odx);
+    rd.ody = point(ody);
+    rd.ddx = vec(ddx);
+    rd.ddy = vec(ddy);
+}
+
 // ------------------------------------------------------------ utilities
 NB_D float rgb2y(const float3& c) { return dot(c, f3(0.2126f, 0.7152f, 0.0722f)); }
 NB_D float power_heuristic(float f, float g) { return (f * f) / (f * f + g * g); }
@@ -152,10 +234,21 @@ struct Frame {
 NB_D float3 to_local(const Frame& F, const float3& v) { return f3(dot(v, F.s), dot(v, F.t), dot(v, F.n)); }
 NB_D float3 to_world(const Frame& F, const float3& v) { return v.x * F.s + v.y * F.t + v.z * F.n; }
 
-// CudaIntersection::computeTangentSpace (noor/cuda/intersection.cuh:325-377)
-// without the ray-differential part (only texture LOD and bump use it).
+// What computeTangentSpace also derives for textures and ray differentials:
+// the interpolated texture coordinates, dp/du and dp/dv before the frame's
+// Gram-Schmidt step, and the normal's derivatives dn/du, dn/dv
+// (intersection.cuh:345-394).
+struct TangentOut {
+    float2 uv;
+    float3 dpdu, dpdv;
+    float3 dndu, dndv;
+};
+
+// CudaIntersection::computeTangentSpace (noor/cuda/intersection.cuh:325-394);
+// with `out` also the uv and the derivatives above.
 NB_D Frame tangent_frame(const DevScene& S, const uint4& attr, uint32_t ins, float bu, float bv,
-                         const float4* tri_verts /* 3 object-space vertices or null */) {
+                         const float4* tri_verts /* 3 object-space vertices or null */,
+                         TangentOut* out = nullptr) {
     const DevXform* X = S.xforms + ins;
     float2 uv0 = __ldg(&S.uvs[attr.x]), uv1 = __ldg(&S.uvs[attr.y]), uv2 = __ldg(&S.uvs[attr.z]);
     uv0.y = 1.0f - uv0.y;
@@ -204,6 +297,29 @@ NB_D Frame tangent_frame(const DevScene& S, const uint4& attr, uint32_t ins, flo
     F.s = normalize_guard(dpdu - F.n * dot(F.n, dpdu));
     const float sign = dot(cross(F.n, F.s), dpdv) < 0.0f ? -1.0f : 1.0f;
     F.t = normalize_guard(sign * cross(F.n, F.s));
+    if (out) {
+        out->uv = lerp_uv(uv0, uv1, uv2, bu, bv);
+        out->dpdu = dpdu;
+        out->dpdv = dpdv;
+        // normal derivatives from the object-space vertex normals
+        const float3 dn01 = n1 - n0, dn02 = n2 - n0;
+        if (!(fabsf(det) < 1e-8f)) {
+            const float inv = 1.0f / det;
+            const float a00 = d2.y * inv, a01 = -d1.y * inv, a10 = -d2.x * inv, a11 = d1.x * inv;
+            out->dndu = a00 * dn01 + a01 * dn02;
+            out->dndv = a10 * dn01 + a11 * dn02;
+        } else {
+            const float3 c = cross(dn01, dn02);
+            const float3 ct = f3(N0.x * c.x + N0.y * c.y + N0.z * c.z, N1.x * c.x + N1.y * c.y + N1.z * c.z,
+                                 N2.x * c.x + N2.y * c.y + N2.z * c.z);
+            const float3 dn = normalize_guard(normalize_fast(ct));
+            if (length2(dn) == 0.0f) {
+                out->dndu = out->dndv = f3(0.0f);
+            } else {
+                coordinate_system(dn, out->dndu, out->dndv);
+            }
+        }
+    }
     return F;
 }
 

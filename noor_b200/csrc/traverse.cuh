@@ -161,6 +161,16 @@ NB_D bool wt_test(const TRay& r, const WtRay& w, const DevWtTri* tri, float& tma
     return true;
 }
 
+// The alpha cut of an ALPHA material's triangle (noor/cuda/triangle.cuh:
+// 124-133): the transparency map at the hit's interpolated uv; a texel of
+// 1e-4 or less lets the ray through.
+template <int ISECT>
+NB_OUTLINE bool alpha_cut(const DevScene& S, uint32_t ti, float bu, float bv) {
+    const uint4 a = ISECT == NOOR_ISECT_WATERTIGHT ? __ldg(&S.wtri[ti].attr) : __ldg(&S.wald[ti].attr);
+    const float2 uv = lerp_uv(vertex_uv(S, a.x), vertex_uv(S, a.y), vertex_uv(S, a.z), bu, bv);
+    return slot_tex(S.mat_tex[a.w], kTexAlpha, uv).x <= 0.0001f;
+}
+
 // Arithmetic of the light-shape tests: with X (the reference's Wald mode,
 // whose hit distances are the reference's to the bit) each operation rounds
 // on its own; otherwise the compiler may contract multiply-adds.
@@ -352,10 +362,20 @@ NB_D bool trace_closest(const DevScene& S, const float3& o, const float3& d, flo
                     float bu, bv;
                     uint32_t mt;
                     bool h;
-                    if (ISECT == NOOR_ISECT_WATERTIGHT)
+                    if (EXT && S.has_alpha) {
+                        // the hit distance is kept only past the alpha cut
+                        float tc = ltmax;
+                        if (ISECT == NOOR_ISECT_WATERTIGHT)
+                            h = wt_test(lr, wt, S.wtri + ti, tc, bu, bv, mt);
+                        else
+                            h = wald_test(lr, S.wald + ti, tc, bu, bv, mt);
+                        if (h && (mt & NOOR_ALPHA) && alpha_cut<ISECT>(S, ti, bu, bv)) h = false;
+                        if (h) ltmax = tc;
+                    } else if (ISECT == NOOR_ISECT_WATERTIGHT) {
                         h = wt_test(lr, wt, S.wtri + ti, ltmax, bu, bv, mt);
-                    else
+                    } else {
                         h = wald_test(lr, S.wald + ti, ltmax, bu, bv, mt);
+                    }
                     if (h) {
                         leaf_hit = true;
                         rec.u = bu;
@@ -441,6 +461,7 @@ NB_D bool trace_any(const DevScene& S, const float3& o, const float3& d, float t
                         h = wt_test(lr, wt, S.wtri + ti, tm, bu, bv, mt);
                     else
                         h = wald_test(lr, S.wald + ti, tm, bu, bv, mt);
+                    if (h && EXT && S.has_alpha && (mt & NOOR_ALPHA) && alpha_cut<ISECT>(S, ti, bu, bv)) h = false;
                     if (h) return true;
                 }
             }

@@ -104,6 +104,8 @@ struct WfDev {
     float4* hit;     // t, u, v, tri bits
     uint2* hit2;     // instance, material type
     uint32_t* state;
+    float4* diff;           // 4 per slot where some scene has bump maps (else null): the ray's
+                            // differentials odx (w = 1 while it has them), ody, ddx, ddy
     uint32_t* qshade;       // kKinds * cap slot indices
     uint32_t* qshadow;      // 2 * cap entries: slot << 1 | which
     float4* sh_o;           // origin, tmax (by queue entry)
@@ -214,6 +216,23 @@ NB_D uint32_t tile_pixel(uint32_t q, uint32_t w, uint32_t h) {
     return (h4 + q / w) * w + q % w;
 }
 
+NB_D void store_diff(const WfDev& W, uint32_t slot, const RayDiff& r) {
+    W.diff[4 * slot] = make_float4(r.odx.x, r.odx.y, r.odx.z, r.on ? 1.0f : 0.0f);
+    W.diff[4 * slot + 1] = make_float4(r.ody.x, r.ody.y, r.ody.z, 0.0f);
+    W.diff[4 * slot + 2] = make_float4(r.ddx.x, r.ddx.y, r.ddx.z, 0.0f);
+    W.diff[4 * slot + 3] = make_float4(r.ddy.x, r.ddy.y, r.ddy.z, 0.0f);
+}
+NB_D RayDiff load_diff(const WfDev& W, uint32_t slot) {
+    const float4 a = W.diff[4 * slot], b = W.diff[4 * slot + 1], c = W.diff[4 * slot + 2], e = W.diff[4 * slot + 3];
+    RayDiff r;
+    r.on = a.w != 0.0f;
+    r.odx = f3(a.x, a.y, a.z);
+    r.ody = f3(b.x, b.y, b.z);
+    r.ddx = f3(c.x, c.y, c.z);
+    r.ddy = f3(e.x, e.y, e.z);
+    return r;
+}
+
 // Regen (every slot): fold the last shade step's direct lighting into L; add
 // the sky term of paths whose last ray escaped, and add finished paths to
 // their frame's film (one float4 atomic per path, TwoSum-compensated);
@@ -290,7 +309,18 @@ __global__ void __launch_bounds__(kRegenBlock) wf_regen(WfDev W) {
             const uint32_t pix = tile_pixel((uint32_t)(local / F.spp), F.cam.w, F.cam.h);
             Rng rng{tea16(pix, F.first_frame + sample)};
             float3 o, d;
-            camera_ray(F.cam, pix % F.cam.w, pix / F.cam.w, rng, o, d);
+            if (W.diff) {
+                // a batch with bump maps: camera rays carry differentials
+                // where their scene has bump maps
+                RayDiff rd{};
+                if (W.scenes[F.scene].has_bump)
+                    camera_ray_diff(F.cam, pix % F.cam.w, pix / F.cam.w, rng, o, d, rd);
+                else
+                    camera_ray(F.cam, pix % F.cam.w, pix / F.cam.w, rng, o, d);
+                store_diff(W, slot, rd);
+            } else {
+                camera_ray(F.cam, pix % F.cam.w, pix / F.cam.w, rng, o, d);
+            }
             W.o[slot] = make_float4(o.x, o.y, o.z, bitsf((uint32_t)fi));
             W.d[slot] = make_float4(d.x, d.y, d.z, bitsf(pix));
             W.beta[slot] = make_float4(1.0f, 1.0f, 1.0f, bitsf(0u));
@@ -393,7 +423,9 @@ NB_D void extend_one(const WfDev& W, const DevScene& S, uint32_t slot, const flo
             } else {
                 const uint32_t mi = ISECT == NOOR_ISECT_WATERTIGHT ? __ldg(&S.wtri[rec.tri].attr).w
                                                                    : __ldg(&S.wald[rec.tri].attr).w;
-                const DevMaterial& em = S.materials[mi];
+                DevMaterial em = S.materials[mi];
+                // an emitter's texture is read at the hit's barycentrics
+                if (EXT && S.has_tex && em.tex_mask) apply_textures(S, mi, f2(rec.u, rec.v), em);
                 c = beta * (em.emitter_scale * em.emittance);
             }
             float4 Lw = W.L[slot];
@@ -552,8 +584,10 @@ NB_D void push_shadow(const WfDev& W, uint32_t slot, uint32_t which, const Shado
 }
 
 // EXT false: the queue holds no material with a lobe beyond Lambert,
-// conductor and Fresnel specular (those lobes' code is left out)
-template <bool EXT>
+// conductor and Fresnel specular (those lobes' code is left out).  DIFF:
+// some scene has bump maps; its rays' differentials are read, used and
+// passed on as the megakernel's DIFF specialisation does.
+template <bool EXT, bool DIFF = false>
 __global__ void __launch_bounds__(256, NB_SHADE_MIN_BLOCKS) wf_shade(WfDev W, uint32_t kind) {
     const uint32_t n = W.counters[kind];
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -575,11 +609,23 @@ __global__ void __launch_bounds__(256, NB_SHADE_MIN_BLOCKS) wf_shade(WfDev W, ui
         rec.ins = h2.x;
         rec.mtype = h2.y;
         Isect I;
+        TangentOut to;
+        const bool tex = EXT && S.has_tex;
         if (S.isect == NOOR_ISECT_WATERTIGHT)
-            make_isect<NOOR_ISECT_WATERTIGHT, EXT>(S, o, d, hw.x, rec, I);
+            make_isect<NOOR_ISECT_WATERTIGHT, EXT>(S, o, d, hw.x, rec, I, tex ? &to : nullptr);
         else
-            make_isect<NOOR_ISECT_REF_WALD, EXT>(S, o, d, hw.x, rec, I);
-        const DevMaterial m = S.materials[I.mat];
+            make_isect<NOOR_ISECT_REF_WALD, EXT>(S, o, d, hw.x, rec, I, tex ? &to : nullptr);
+        DevMaterial m = S.materials[I.mat];
+        RayDiff rd{};
+        HitDiff hd;
+        if (DIFF && S.has_bump) {
+            rd = load_diff(W, slot);
+            if (rd.on) {
+                hd = hit_differential(I, to, rd);
+                if (I.mtype & NOOR_BUMP) bump(S, I.mat, I.uv, hd, I.F);
+            }
+        }
+        if (tex && m.tex_mask) apply_textures(S, I.mat, I.uv, m);
         Rng rng{fbits(Lw.w)};
         int li = 0;
         bool picked;
@@ -629,6 +675,12 @@ __global__ void __launch_bounds__(256, NB_SHADE_MIN_BLOCKS) wf_shade(WfDev W, ui
             const bool spec = (I.mtype & kSpecularMat) != 0;
             const uint32_t nb_ = bounce + 1;
             const float3 no = spawn_origin(I, wi, S.bias);
+            if (DIFF && S.has_bump) {
+                RayDiff nd{};
+                if (rd.on && (I.mtype & kGlossyMat))
+                    nd = spawn_diff(I, hd, rd, no, wi, (I.mtype & kDielectricMat) ? m.coat_ior : 1.0f);
+                store_diff(W, slot, nd);
+            }
             W.o[slot] = make_float4(no.x, no.y, no.z, ow.w);
             W.d[slot] = make_float4(wi.x, wi.y, wi.z, dw.w);
             W.beta[slot] = make_float4(beta.x, beta.y, beta.z, bitsf(nb_ | (spec ? 1u << 16 : 0u)));
@@ -739,6 +791,7 @@ struct WavefrontState {
     uint32_t cap = 0;
     std::vector<void*> bufs;
     WfDev dev{};
+    float4* diff = nullptr;     // ray differentials, made for the first batch with bump maps
     uint32_t* active_host_dev = nullptr;
     // film scratch per frame batch
     void* films = nullptr;
@@ -758,6 +811,7 @@ struct WavefrontState {
         if (frames_dev) cudaFree(frames_dev);
         if (scenes_dev) cudaFree(scenes_dev);
         if (active_host_dev) cudaFree(active_host_dev);
+        if (diff) cudaFree(diff);
     }
 };
 
@@ -817,6 +871,8 @@ struct WfLaunch {
     bool ext;               // some frame's scene has extra lobes or lights
     bool ext_lights;        // ... has sphere, disk, point, spot or distant lights
     bool env_ref;           // ... samples its environment as the reference does
+    bool tex;               // ... reads textures per hit (image maps, alpha, bump)
+    bool diff;              // ... has bump maps: rays carry differentials
 };
 
 // one iteration; with `ev` (kWfStages + 1 events), records ev[0] before the
@@ -842,7 +898,9 @@ static cudaError_t wf_iteration(const WfDev& W, const WfLaunch& L, cudaStream_t 
     const int nk = W.sort ? kKinds : 1;
     for (int k = 0; k < nk; ++k) {
         // sorted queues 0 and 1 hold Lambert and conductor hits only
-        if (L.ext && !(W.sort && k < 2 && !L.ext_lights && !L.env_ref))
+        if (L.diff)
+            wf_shade<true, true><<<L.grid_queue, 256, 0, s>>>(W, (uint32_t)k);
+        else if (L.ext && !(W.sort && k < 2 && !L.ext_lights && !L.env_ref && !L.tex))
             wf_shade<true><<<L.grid_queue, 256, 0, s>>>(W, (uint32_t)k);
         else
             wf_shade<false><<<L.grid_queue, 256, 0, s>>>(W, (uint32_t)k);
@@ -965,15 +1023,24 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
     L.grid_queue = (uint32_t)std::max(1, C.sm_count) * 16;
     const uint32_t scene0 = frames[0].scene_id;
     bool multi = false, mixed = false;
-    L.ext = L.ext_lights = L.env_ref = false;
+    L.ext = L.ext_lights = L.env_ref = L.tex = L.diff = false;
     for (uint32_t i = 0; i < n_frames; ++i) {
         const DevScene& fs = C.scenes[frames[i].scene_id]->dev;
         multi |= frames[i].scene_id != scene0;
         mixed |= fs.isect != C.scenes[scene0]->dev.isect;
-        L.ext |= fs.ext_lobes != 0u || fs.ext_lights != 0u || fs.env_ref != 0u;
+        L.ext |= fs.ext_lobes != 0u || fs.ext_lights != 0u || fs.env_ref != 0u || fs.has_tex != 0u;
         L.env_ref |= fs.env_ref != 0u;
-        L.ext_lights |= fs.ext_lights != 0u;
+        // the traversal kernels' full variant also tests alpha maps and reads
+        // emitters' textures
+        L.ext_lights |= fs.ext_lights != 0u || fs.has_tex != 0u;
+        L.tex |= fs.has_tex != 0u;
+        L.diff |= fs.has_bump != 0u;
     }
+    if (L.diff && !WS.diff) {
+        cudaError_t de = cudaMalloc((void**)&WS.diff, (size_t)WS.cap * 64);
+        if (de != cudaSuccess) return cuda_fail(de, "wavefront differentials");
+    }
+    W.diff = L.diff ? WS.diff : nullptr;
     L.scene = C.scenes[scene0]->dev;
     // traversal kernels: per intersector, scene source and light shapes
 #define NB_TRAV(I, M)                                                                   \
@@ -1007,12 +1074,16 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
         uint64_t scene_hash = 1469598103934665603ull;  // FNV-1a over the scene parameter's bytes
         for (size_t b = 0; b < sizeof(DevScene); ++b)
             scene_hash = (scene_hash ^ reinterpret_cast<const unsigned char*>(&L.scene)[b]) * 1099511628211ull;
-        const uint64_t key[10] = {(uint64_t)W.cap | (uint64_t)W.level << 32 | (uint64_t)L.ext << 36, W.total,
+        const uint64_t key[10] = {(uint64_t)W.cap | (uint64_t)W.level << 32 | (uint64_t)L.ext << 36 |
+                                      (uint64_t)L.tex << 37 | (uint64_t)L.diff << 38 | (uint64_t)L.ext_lights << 39 |
+                                      (uint64_t)L.env_ref << 40,
+                                  W.total,
                                   (uint64_t)W.max_iters | (uint64_t)W.nframes << 32,
                                   (uint64_t)(uint32_t)W.stack_cap | (uint64_t)L.block << 32,
                                   (uint64_t)L.smem, (uint64_t)L.grid_slots | (uint64_t)L.grid_queue << 32,
                                   (uint64_t)(uintptr_t)W.frames ^ ((uint64_t)(uintptr_t)W.scenes << 1),
-                                  (uint64_t)(uintptr_t)W.status, (uint64_t)(uintptr_t)L.extend ^ (uint64_t)(uintptr_t)L.shadow << 1,
+                                  (uint64_t)(uintptr_t)W.status ^ ((uint64_t)(uintptr_t)W.diff << 1),
+                                  (uint64_t)(uintptr_t)L.extend ^ (uint64_t)(uintptr_t)L.shadow << 1,
                                   scene_hash};
         if (WS.exec && std::memcmp(key, WS.graph_key, sizeof(key)) != 0) {
             cudaGraphExecDestroy(WS.exec);

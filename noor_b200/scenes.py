@@ -72,6 +72,7 @@ class SceneData:
     distant_lights: list = field(default_factory=list)   # dict(direction, ke)
     skydome_type: int = capi.NOOR_SKY_CONSTANT
     env: Optional[np.ndarray] = None   # (H,W,4) f32
+    images: list = field(default_factory=list)   # image maps, (H,W,4) f32 each, named by materials' "map"
     bvh: dict = field(default_factory=lambda: dict(DEFAULT_BVH))
     camera: dict = field(default_factory=dict)
     render: dict = field(default_factory=dict)
@@ -207,6 +208,94 @@ def room_scene(seed: int = 1, width: int = 256, height: int = 256, spp: int = 16
         camera=dict(eye=(0.0, 1.0, 3.75), look_at=(0.0, 1.0, 0.0), up=(0.0, 1.0, 0.0), fov_deg=40.0,
                     w=width, h=height),
         render=dict(spp=spp, bounces=bounces, rr=rr, mis=int(mis)), name="room")
+
+
+def _image_maps(seed: int):
+    """the textured room's image maps (H, W, 4) f32: a noisy two-tone checker
+    (64 x 64), a roughness map in R and G (32 x 32), a height field of
+    grooves and bumps (64 x 64, in R) and an alpha map of round holes
+    (32 x 32: 0 inside a hole, 1 elsewhere)"""
+    rng = np.random.default_rng(seed)
+    img = []
+    y, x = np.mgrid[0:64, 0:64]
+    chk = ((x // 8 + y // 8) % 2).astype(np.float32)[..., None]
+    a, b = np.array([0.75, 0.62, 0.45], np.float32), np.array([0.18, 0.25, 0.35], np.float32)
+    rgb = chk * a + (1 - chk) * b + 0.04 * rng.standard_normal((64, 64, 3)).astype(np.float32)
+    img.append(np.concatenate([np.clip(rgb, 0.02, 0.98), np.ones((64, 64, 1), np.float32)], 2))
+    r = 0.05 + 0.25 * rng.random((32, 32)).astype(np.float32)
+    img.append(np.stack([r, r * 0.8, np.zeros_like(r), np.ones_like(r)], 2).astype(np.float32))
+    hgt = 0.5 + 0.3 * np.sin(x / 64 * 2 * np.pi * 4) + 0.2 * rng.standard_normal((64, 64))
+    img.append(np.stack([hgt, hgt, hgt, np.ones_like(hgt)], 2).astype(np.float32))
+    yy, xx = np.mgrid[0:32, 0:32]
+    holes = (((xx % 16) - 7.5) ** 2 + ((yy % 16) - 7.5) ** 2) < 5.5 ** 2
+    alpha = np.where(holes, 0.0, 1.0).astype(np.float32)
+    img.append(np.stack([alpha, alpha, alpha, np.ones_like(alpha)], 2).astype(np.float32))
+    return img
+
+
+def textured_room_scene(seed: int = 6, width: int = 128, height: int = 128, spp: int = 16, bounces: int = 5,
+                        rr: int = 1, textured_light: bool = False) -> SceneData:
+    """The room with texture coordinates on every face (0..1 over each quad)
+    and image maps: a checker on the floor (map_Kd, uv scale 4), a rough
+    gold short box whose roughness is a map (uv scale 1), a bump-mapped tall
+    box (map_bump, factor 0.02, uv scale 2) and, in front of the right
+    wall, an alpha-cut panel (map_d with round holes, uv scale 3).  Camera
+    rays that reflect off the gold box reach the bumped box with
+    differentials.  `textured_light`: the ceiling light's emittance is the
+    checker map too (an emitter's texture is read at its barycentrics)."""
+    base = room_scene(seed=seed, width=width, height=height, spp=spp, bounces=bounces, rr=rr)
+    mats = [dict(m) for m in base.materials]
+    floor, short_box, tall_box = 0, 5, 5
+    faces_per_quad = 2
+    # materials: floor checker; the boxes get their own materials
+    unit = [(1.0, 1.0)] * 7
+    def maps(**kw):
+        m = [-1] * 7
+        for k, v in kw.items():
+            m[getattr(capi, "NOOR_MAP_" + k.upper())] = v
+        return m
+    mats[floor] = dict(mats[floor], map=maps(diffuse=0), map_uvscale=[(4.0, 4.0)] + unit[1:])
+    gold = material("metal", roughness=0.1)
+    gold.update(map=maps(roughness=1), map_uvscale=unit)
+    bumped = material("diffuse", albedo=(0.65, 0.6, 0.55))
+    bumped.update(map=maps(bump=2), map_uvscale=[(2.0, 2.0)] * 7, bumpfactor=0.02)
+    panel = material("diffuse", albedo=(0.3, 0.55, 0.35))
+    panel.update(map=maps(alpha=3), map_uvscale=[(3.0, 3.0)] * 7)
+    light_mat = len(mats) - 1
+    light = dict(mats[light_mat])
+    if textured_light:
+        light.update(map=maps(emittance=0), map_uvscale=unit, emitter_scale=20.0)
+    mats = mats[:5] + [gold, bumped, light, panel]
+    # triangles: 10 wall, 12 short box, 12 tall box, 2 light (as in room_scene)
+    midx = base.material_indices.astype(np.int64).copy()
+    midx[10:22] = 5
+    midx[22:34] = 6
+    midx[34:36] = 7
+    # the alpha-cut panel: a quad facing the camera in front of the right wall
+    V = base.vertices.copy()
+    pts = _quad([(0.55, 0.0, -0.75), (0.95, 0.0, -0.2), (0.95, 1.5, -0.2), (0.55, 1.5, -0.75)],
+                np.array([-0.8, 0.0, 0.6]))
+    pv = np.zeros((4, 4), np.float32)
+    pv[:, :3] = np.array(pts)
+    pv[:, 3] = 1.0
+    V = np.concatenate([V, pv])
+    n = np.cross(pts[1] - pts[0], pts[2] - pts[0])
+    N = np.concatenate([base.normals, np.array([[*(n / np.linalg.norm(n)), 0.0]], np.float32)])
+    b0 = base.vertices.shape[0]
+    vidx = np.concatenate([base.vindices, np.array([[b0, b0 + 1, b0 + 2], [b0, b0 + 2, b0 + 3]], np.uint32)])
+    nidx = np.concatenate([base.nindices, np.full((2, 3), N.shape[0] - 1, np.uint32)])
+    midx = np.concatenate([midx, [8, 8]]).astype(np.uint32)
+    # texture coordinates: the 4 corners of every quad at (0,0) (1,0) (1,1) (0,1)
+    uvs = np.array([(0.0, 0.0), (1.0, 0.0), (1.0, 1.0), (0.0, 1.0)], np.float32)
+    T = vidx.shape[0]
+    uvidx = np.zeros((T, 3), np.uint32)
+    uvidx[0::2] = [0, 1, 2]
+    uvidx[1::2] = [0, 2, 3]
+    meshes = [dict(base.meshes[0], tri_count=T)]
+    return SceneData(vertices=V, normals=N, uvs=uvs, vindices=vidx, nindices=nidx, uvindices=uvidx,
+                     material_indices=midx, meshes=meshes, materials=mats, area_lights=base.area_lights,
+                     skydome_type=base.skydome_type, images=_image_maps(seed), camera=base.camera,
+                     render=base.render, name="textured_room")
 
 
 # ------------------------------------------------------------- icospheres
@@ -480,10 +569,16 @@ def scene_desc(scene: SceneData):
         meshes[k].instance = m.get("instance", -1)
         meshes[k].light_idx = m.get("light_idx", -1)
     mats = (capi.MaterialDesc * len(s.materials))()
+    map_defaults = dict(map=[-1] * 7, map_uvscale=[(1.0, 1.0)] * 7, bumpfactor=1.0)
     for k, m in enumerate(s.materials):
         for f, _ in capi.MaterialDesc._fields_:
-            val = m[f]
-            if isinstance(val, (tuple, list, np.ndarray)):
+            val = m.get(f, map_defaults.get(f))
+            if f == "map":
+                mats[k].map[:] = [int(x) for x in val]
+            elif f == "map_uvscale":
+                for j, uv in enumerate(val):
+                    mats[k].map_uvscale[j][:] = [float(x) for x in uv]
+            elif isinstance(val, (tuple, list, np.ndarray)):
                 getattr(mats[k], f)[:] = [float(x) for x in val]
             else:
                 setattr(mats[k], f, val)
@@ -511,7 +606,13 @@ def scene_desc(scene: SceneData):
         d.env_width, d.env_height, d.env_rgba = E.shape[1], E.shape[0], _ptr(E)
     b = s.bvh
     d.bvh = capi.BvhSpec(b["num_bins"], b["max_height"], b["Ci"], b["Ct"], b["min_leaf_tris"], b["max_leaf_tris"])
-    return d, keep + [meshes, mats, lights, delta]
+    imgs = (capi.Image * max(1, len(s.images)))()
+    for k, im in enumerate(s.images):
+        a = np.ascontiguousarray(im, np.float32)
+        keep.append(a)
+        imgs[k].width, imgs[k].height, imgs[k].rgba = a.shape[1], a.shape[0], _ptr(a)
+    d.images, d.num_images = imgs, len(s.images)
+    return d, keep + [meshes, mats, lights, delta, imgs]
 
 
 class BuiltPayload:

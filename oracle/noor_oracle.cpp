@@ -113,14 +113,75 @@ struct Scene {
     int ew = 0, eh = 0;
     int num_lights = 0;
     bool sky_on = false;
+    bool has_bump = false;
     // per-material constants resolved from the 1x1 textures
     struct Mat {
         float diffuse[3], specular[3], transmission[3], emittance[3], ior[3], k[3];
         float rx, ry, coat_ior, emitter_scale, coat_weight, coat_sigma, coat_thickness;
         uint32_t type, dist;
+        // slots read per hit: diffuse, specular, emittance, roughness,
+        // transmission, ior, k, alpha, bump (texture index, uv scale)
+        uint32_t tex_mask;
+        uint32_t tex[9];
+        float uvs[9][2];
+        float bumpfactor;
     };
     std::vector<Mat> mats;
 };
+enum { TX_DIFFUSE, TX_SPECULAR, TX_EMITTANCE, TX_ROUGHNESS, TX_TRANSMISSION, TX_IOR, TX_K, TX_ALPHA, TX_BUMP };
+
+// A texture fetch as the texture unit computes it (tex2D on an RGBA float
+// array, normalised coordinates), the reference's material textures being
+// such arrays (noor/cuda/texture.cuh:375-400).  Restated from CUDA's
+// documented filtering (linear: the weights are 9-bit fixed point with 8
+// fractional bits) and from measurements of the unit: the coordinate's
+// fraction x*256 is rounded half up; the four corner weights are integers
+// over 256 -- w11 = round_half_up(A*B/256), w10 = A - w11, w01 = B - w11,
+// w00 = 256 - A - B + w11 -- and the weighted sum is rounded once.  It
+// matches the unit on about 99 % of fetches; the rest differ where the
+// unit's fixed-point coordinate rounds the other way (within 1/256 of the
+// texel difference).  Point: texel floor(u*W).  Wrap takes the fraction of
+// u first; clamp clamps the texel index.
+inline void tex_fetch(const noor_texture& t, double u, double v, float out[4]) {
+    const int W = t.width, H = t.height;
+    if (W == 1 && H == 1) {
+        std::memcpy(out, t.rgba, 16);
+        return;
+    }
+    const bool wrap = t.address == NOOR_ADDRESS_WRAP;
+    if (wrap) {
+        u -= std::floor(u);
+        v -= std::floor(v);
+    }
+    auto idx = [&](long long i, int n) -> long long {
+        if (wrap) return ((i % n) + n) % n;
+        return std::min<long long>(std::max<long long>(i, 0), n - 1);
+    };
+    auto texel = [&](long long x, long long y) { return t.rgba + 4 * ((size_t)idx(y, H) * W + (size_t)idx(x, W)); };
+    if (t.filter != NOOR_FILTER_LINEAR) {
+        const float* q = texel((long long)std::floor(u * W), (long long)std::floor(v * H));
+        std::memcpy(out, q, 16);
+        return;
+    }
+    const double x = u * W - 0.5, y = v * H - 0.5;
+    long long x0 = (long long)std::floor(x), y0 = (long long)std::floor(y);
+    long long A = (long long)std::floor((x - (double)x0) * 256.0 + 0.5);
+    long long B = (long long)std::floor((y - (double)y0) * 256.0 + 0.5);
+    if (A >= 256) { A = 0; ++x0; }
+    if (B >= 256) { B = 0; ++y0; }
+    const long long P = A * B;
+    const long long w11 = P / 256 + ((P % 256) >= 128 ? 1 : 0);
+    const long long w10 = A - w11, w01 = B - w11, w00 = 256 - A - B + w11;
+    const float *t00 = texel(x0, y0), *t10 = texel(x0 + 1, y0), *t01 = texel(x0, y0 + 1), *t11 = texel(x0 + 1, y0 + 1);
+    for (int c = 0; c < 4; ++c)
+        out[c] = (float)(((double)w00 * t00[c] + (double)w10 * t10[c] + (double)w01 * t01[c] + (double)w11 * t11[c]) /
+                         256.0);
+}
+// slot k of material m at uv (uvscale * uv)
+template <class T> inline void slot_fetch(const Scene& sc, const Scene::Mat& m, int k, T u, T v, float out[4]) {
+    const float su = m.uvs[k][0], sv = m.uvs[k][1];
+    tex_fetch(sc.P->textures[m.tex[k]], (double)(float)((T)su * u), (double)(float)((T)sv * v), out);
+}
 
 // ------------------------------------------------------------ traversal
 template <class T>
@@ -330,6 +391,32 @@ struct Hit {
     uint32_t tri, ins, mt;
 };
 
+// texture coordinates of a vertex as the mesh manager returns them, v
+// flipped (mesh.cuh:145-148), and their barycentric interpolation
+template <class T> inline void vertex_uv(const Scene& sc, uint32_t i, T& x, T& y) {
+    const float* q = sc.P->uvs + 2 * (size_t)i;
+    x = q[0];
+    y = T(1) - (T)q[1];
+}
+template <class T> inline void hit_uv(const Scene& sc, const uint32_t* a, T bu, T bv, T& u, T& v) {
+    T u0, v0, u1, v1, u2, v2;
+    vertex_uv(sc, a[0], u0, v0);
+    vertex_uv(sc, a[1], u1, v1);
+    vertex_uv(sc, a[2], u2, v2);
+    const T w = T(1) - bu - bv;
+    u = w * u0 + bu * u1 + bv * u2;
+    v = w * v0 + bu * v1 + bv * v2;
+}
+// the alpha cut of an ALPHA material's triangle (triangle.cuh:124-133)
+template <class T> inline bool alpha_cut(const Scene& sc, uint32_t ti, T bu, T bv) {
+    const uint32_t* a = sc.P->attribute_indices + 4 * (size_t)ti;
+    T u, v;
+    hit_uv(sc, a, bu, bv, u, v);
+    float c[4];
+    slot_fetch<T>(sc, sc.mats[a[3]], TX_ALPHA, u, v, c);
+    return c[0] <= 0.0001f;
+}
+
 // intersect / intersectP (bvh.cuh:142-234).  ctr (optional): nodes visited,
 // triangles tested, triangles whose t fell in range.
 template <class T>
@@ -386,6 +473,7 @@ bool traverse(const Scene& sc, V<T> o, V<T> d, T& tmax, Hit* rec, bool any, int 
                 uint32_t mt;
                 bool h = isect == NOOR_ISECT_WATERTIGHT ? wtt(lr, wt, sc, ti, tm, bu, bv, mt, ctr)
                                                         : wald(lr, sc, ti, tm, bu, bv, mt, ctr);
+                if (h && (mt & NOOR_ALPHA) && alpha_cut<T>(sc, ti, bu, bv)) h = false;
                 if (h) {
                     if (any) return true;
                     ltmax = tm;
@@ -431,8 +519,16 @@ template <class T> inline void coord_sys(V<T> v1, V<T>& v2, V<T>& v3) {
     v3 = cross(v1, v2);
 }
 
-// computeTangentSpace (intersection.cuh:325-377)
-template <class T> Frame<T> tangent(const Scene& sc, const Hit& h) {
+// what computeTangentSpace also keeps for textures and ray differentials
+// (intersection.cuh:345-394): uv, dp/du and dp/dv before Gram-Schmidt,
+// dn/du and dn/dv
+template <class T> struct TOut {
+    T u, v;
+    V<T> dpdu, dpdv, dndu, dndv;
+};
+
+// computeTangentSpace (intersection.cuh:325-394)
+template <class T> Frame<T> tangent(const Scene& sc, const Hit& h, TOut<T>* out = nullptr) {
     const noor_payload* P = sc.P;
     const uint32_t* a = P->attribute_indices + 4 * (size_t)h.tri;
     auto vtx = [&](uint32_t i) { const float* q = P->vertices + 4 * (size_t)i; return mk((T)q[0], (T)q[1], (T)q[2]); };
@@ -475,7 +571,126 @@ template <class T> Frame<T> tangent(const Scene& sc, const Hit& h) {
     F.s = nrm_g(dpdu - F.n * dot(F.n, dpdu));
     const T sg = dot(cross(F.n, F.s), dpdv) < T(0) ? T(-1) : T(1);
     F.t = nrm_g(sg * cross(F.n, F.s));
+    if (out) {
+        out->u = w * u0x + bu * u1x + bv * u2x;
+        out->v = w * u0y + bu * u1y + bv * u2y;
+        out->dpdu = dpdu;
+        out->dpdv = dpdv;
+        const V<T> dn01 = n1 - n0, dn02 = n2 - n0;
+        if (!(std::fabs(det) < (T)1e-8f)) {
+            const T inv = T(1) / det;
+            const T a00 = d2y * inv, a01 = -d1y * inv, a10 = -d2x * inv, a11 = d1x * inv;
+            out->dndu = a00 * dn01 + a01 * dn02;
+            out->dndv = a10 * dn01 + a11 * dn02;
+        } else {
+            const V<T> dn = nrm_g(nrm(rowmul(P->normal_row, cross(dn01, dn02))));
+            if (len2(dn) == T(0))
+                out->dndu = out->dndv = mk(T(0), T(0), T(0));
+            else
+                coord_sys(dn, out->dndu, out->dndv);
+        }
+    }
     return F;
+}
+
+// the material's per-hit slots at uv (materialimp.cuh:121-183)
+template <class T> inline Scene::Mat textured(const Scene& sc, const Scene::Mat& m0, T u, T v) {
+    Scene::Mat m = m0;
+    float c[4];
+    auto rgb = [&](int k, float* dst) {
+        if (!(m.tex_mask & (1u << k))) return;
+        slot_fetch<T>(sc, m, k, u, v, c);
+        std::memcpy(dst, c, 12);
+    };
+    rgb(TX_DIFFUSE, m.diffuse);
+    rgb(TX_SPECULAR, m.specular);
+    rgb(TX_EMITTANCE, m.emittance);
+    rgb(TX_TRANSMISSION, m.transmission);
+    rgb(TX_IOR, m.ior);
+    rgb(TX_K, m.k);
+    if (m.tex_mask & (1u << TX_ROUGHNESS)) {
+        slot_fetch<T>(sc, m, TX_ROUGHNESS, u, v, c);
+        m.rx = c[0];
+        m.ry = c[1];
+    }
+    return m;
+}
+
+// ray differentials (CudaRay, ray.cuh:36-200), world space
+template <class T> struct RDiff {
+    bool on = false;
+    V<T> odx, ody, ddx, ddy;
+};
+template <class T> struct HDiff {
+    V<T> dpdx, dpdy, dndu, dndv;
+    T dudx = 0, dudy = 0, dvdx = 0, dvdy = 0;
+};
+// NOOR::solve2x2 (math.cuh:192-207)
+template <class T> inline void solve2(T a00, T a01, T a10, T a11, T b0, T b1, T& x0, T& x1) {
+    const T det = a00 * a11 - a10 * a01;
+    if (std::fabs(det) < (T)1e-10f) {
+        x0 = x1 = T(0);
+        return;
+    }
+    const T inv = T(1) / det;
+    x0 = (a11 * b0 - a01 * b1) * inv;
+    x1 = (a00 * b1 - a10 * b0) * inv;
+    if (std::isnan(x0) || std::isnan(x1)) x0 = x1 = T(0);
+}
+// computeDifferential (intersection.cuh:397-441)
+template <class T> HDiff<T> hit_diff(const Frame<T>& F, V<T> p, const TOut<T>& to, const RDiff<T>& rd) {
+    HDiff<T> h;
+    h.dndu = to.dndu;
+    h.dndv = to.dndv;
+    h.dpdx = h.dpdy = mk(T(0), T(0), T(0));
+    const V<T>& n = F.ng;
+    const T dd = dot(n, p);
+    const T tx = -(dot(n, rd.odx) - dd) / dot(n, rd.ddx);
+    if (std::isinf(tx) || std::isnan(tx)) return h;
+    const V<T> px = rd.odx + tx * rd.ddx;
+    const T ty = -(dot(n, rd.ody) - dd) / dot(n, rd.ddy);
+    if (std::isinf(ty) || std::isnan(ty)) return h;
+    const V<T> py = rd.ody + ty * rd.ddy;
+    h.dpdx = px - p;
+    h.dpdy = py - p;
+    int ax, ay;
+    if (std::fabs(n.x) > std::fabs(n.y) && std::fabs(n.x) > std::fabs(n.z)) {
+        ax = 1;
+        ay = 2;
+    } else if (std::fabs(n.y) > std::fabs(n.z)) {
+        ax = 0;
+        ay = 2;
+    } else {
+        ax = 0;
+        ay = 1;
+    }
+    const T a00 = comp(to.dpdu, ax), a01 = comp(to.dpdv, ax), a10 = comp(to.dpdu, ay), a11 = comp(to.dpdv, ay);
+    solve2(a00, a01, a10, a11, comp(h.dpdx, ax), comp(h.dpdx, ay), h.dudx, h.dvdx);
+    solve2(a00, a01, a10, a11, comp(h.dpdy, ax), comp(h.dpdy, ay), h.dudy, h.dvdy);
+    return h;
+}
+// bump (accumulate.cuh:47-75)
+template <class T> void bump_frame(const Scene& sc, const Scene::Mat& m, T u, T v, const HDiff<T>& h, Frame<T>& F) {
+    T du = T(0.5) * (std::fabs(h.dudx) + std::fabs(h.dudy));
+    T dv = T(0.5) * (std::fabs(h.dvdx) + std::fabs(h.dvdy));
+    du = du == T(0) ? (T)0.001f : du;
+    dv = dv == T(0) ? (T)0.001f : dv;
+    float c[4];
+    slot_fetch<T>(sc, m, TX_BUMP, u, v, c);
+    const T disp = c[0];
+    const T scale = m.bumpfactor;
+    slot_fetch<T>(sc, m, TX_BUMP, u + du, v + T(0), c);
+    const T ud = scale * ((T)c[0] - disp) / du;
+    slot_fetch<T>(sc, m, TX_BUMP, u + T(0), v + dv, c);
+    const T vd = scale * ((T)c[0] - disp) / dv;
+    const V<T> sn = F.n;
+    V<T> dpdu = F.s + ud * sn;
+    const V<T> dpdv = F.t + vd * sn;
+    const V<T> n = nrm_g(cross(dpdu, dpdv));
+    dpdu = nrm_g(dpdu - n * dot(n, dpdu));
+    F.t = nrm_g(cross(n, dpdu));
+    F.s = dpdu;
+    F.n = dot(F.ng, n) < T(0) ? T(-1) * n : n;
 }
 
 // bxdf.cuh:58-96
@@ -1245,8 +1460,46 @@ template <class T> struct Is {
     Frame<T> F;
     uint32_t mt, lobe, mat;
 };
+constexpr uint32_t kGlossyMat =
+    NOOR_MIRROR | NOOR_GLASS | NOOR_CLEARCOAT | NOOR_ROUGHGLASS | NOOR_METAL | NOOR_SUBSTRATE | NOOR_GLOSSY;
+constexpr uint32_t kDielMat = NOOR_GLASS | NOOR_ROUGHGLASS | NOOR_GLOSSY | NOOR_SUBSTRATE | NOOR_CLEARCOAT;
 template <class T> V<T> spawn(const Is<T>& I, V<T> dir, T bias) {
     return dot(dir, I.F.ng) >= T(0) ? I.p + bias * I.F.ng : I.p - bias * I.F.ng;
+}
+// the scattered ray's differentials (spawnRay, intersection.cuh:111-186)
+template <class T> RDiff<T> spawn_diff(const Is<T>& I, const HDiff<T>& h, const RDiff<T>& in, V<T> o, V<T> wi,
+                                       T eta_in) {
+    RDiff<T> r;
+    r.on = true;
+    r.odx = o + h.dpdx;
+    r.ody = o + h.dpdy;
+    const V<T>& sn = I.F.n;
+    const V<T>& wo = I.wo;
+    const V<T> dwodx = T(-1) * (in.ddx + wo), dwody = T(-1) * (in.ddy + wo);
+    if (dot(wi, I.F.ng) >= T(0)) {
+        const V<T> dndx = h.dndu * h.dudx + h.dndv * h.dvdx;
+        const V<T> dndy = h.dndu * h.dudy + h.dndv * h.dvdy;
+        const T dDNdx = dot(dwodx, sn) + dot(wo, dndx), dDNdy = dot(dwody, sn) + dot(wo, dndy);
+        r.ddx = wi - dwodx + T(2) * (dot(wo, sn) * dndx + dDNdx * sn);
+        r.ddy = wi - dwody + T(2) * (dot(wo, sn) * dndy + dDNdy * sn);
+    } else {
+        const V<T> w = T(-1) * wo;
+        const T eta = dot(wo, sn) > T(0) ? T(1) / eta_in : eta_in;
+        const V<T> dndx = h.dndu * h.dudx + h.dndv * h.dvdx;
+        const V<T> dndy = h.dndv * h.dudy + h.dndv * h.dvdy;   // as the reference pairs them
+        const T dDNdx = dot(dwodx, sn) + dot(wo, dndx), dDNdy = dot(dwody, sn) + dot(wo, dndy);
+        const T mu = eta * dot(w, sn) - dot(wi, sn);
+        const T dmudx = (eta - (eta * eta * dot(w, sn)) / dot(wi, sn)) * dDNdx;
+        const T dmudy = (eta - (eta * eta * dot(w, sn)) / dot(wi, sn)) * dDNdy;
+        r.ddx = wi + eta * dwodx - (mu * dndx + dmudx * sn);
+        r.ddy = wi + eta * dwody - (mu * dndy + dmudy * sn);
+    }
+    const T sc = (T)0.25f;
+    r.odx = (T(1) - sc) * o + sc * r.odx;
+    r.ody = (T(1) - sc) * o + sc * r.ody;
+    r.ddx = (T(1) - sc) * wi + sc * r.ddx;
+    r.ddy = (T(1) - sc) * wi + sc * r.ddy;
+    return r;
 }
 template <class T> V<T> area_p(const noor_area_light& A, int which) {
     return which == 0 ? v3f<T>(A.shape.center) : (which == 1 ? v3f<T>(A.shape.u) : (which == 2 ? v3f<T>(A.shape.v) : v3f<T>(A.shape.n)));
@@ -1497,7 +1750,8 @@ V<T> direct(const Scene& sc, const Scene::Mat& m, const Is<T>& I, Rng& rng, int 
 }
 
 // pathtracer() (path_tracer.cu:26-75)
-template <class T> V<T> radiance(const Scene& sc, V<T> o, V<T> d, Rng& rng, int isect, Counters* c) {
+template <class T> V<T> radiance(const Scene& sc, V<T> o, V<T> d, Rng& rng, int isect, Counters* c,
+                                 RDiff<T> rd = RDiff<T>{}) {
     V<T> L = mk(T(0), T(0), T(0)), beta = mk(T(1), T(1), T(1));
     bool specb = false;
     const T bias = (T)sc.S->reflection_bias;
@@ -1527,14 +1781,21 @@ template <class T> V<T> radiance(const Scene& sc, V<T> o, V<T> d, Rng& rng, int 
                 if (I.mt & NOOR_MESHLIGHT) {
                     L = L + beta * area_le<T>(sc.P->area_lights[h.ins], d);
                 } else {
-                    const Scene::Mat& em = sc.mats[I.mat];
+                    // an emitter's texture is read at the barycentrics
+                    const Scene::Mat em = textured<T>(sc, sc.mats[I.mat], (T)h.u, (T)h.v);
                     L = L + beta * ((T)em.emitter_scale * v3f<T>(em.emittance));
                 }
             }
             break;
         }
-        I.F = tangent<T>(sc, h);
-        const Scene::Mat& m = sc.mats[I.mat];
+        TOut<T> to;
+        I.F = tangent<T>(sc, h, &to);
+        const Scene::Mat m = textured<T>(sc, sc.mats[I.mat], to.u, to.v);
+        HDiff<T> hd;
+        if (rd.on) {
+            hd = hit_diff<T>(I.F, I.p, to, rd);
+            if (I.mt & NOOR_BUMP) bump_frame<T>(sc, m, to.u, to.v, hd, I.F);
+        }
         L = L + beta * direct<T>(sc, m, I, rng, isect, c);
         rng.next();
         rng.next();
@@ -1553,6 +1814,10 @@ template <class T> V<T> radiance(const Scene& sc, V<T> o, V<T> d, Rng& rng, int 
         }
         specb = (I.mt & kSpecMat) != 0;
         o = spawn(I, wi, bias);
+        if (rd.on && (I.mt & kGlossyMat))
+            rd = spawn_diff<T>(I, hd, rd, o, wi, (I.mt & kDielMat) ? (T)m.coat_ior : T(1));
+        else
+            rd.on = false;
         d = wi;
     }
     return mk(clampv(L.x, T(0), T(100)), clampv(L.y, T(0), T(100)), clampv(L.z, T(0), T(100)));
@@ -1561,40 +1826,88 @@ template <class T> V<T> radiance(const Scene& sc, V<T> o, V<T> d, Rng& rng, int 
 // generateRay, pinhole (cameraimp.cuh:182-228)
 // generateRay of CudaPerspCamera (pinhole and thin lens), CudaOrthoCamera
 // and CudaEnvCamera (cameraimp.cuh:51-230), then CudaRay::transform
-template <class T> void cam_ray(const noor_camera& C, uint32_t x, uint32_t y, Rng& rng, V<T>& o, V<T>& d) {
+// With rd, also the ray's differentials (each camera type's, then
+// transformDifferentials: origins as points, directions as vectors).
+template <class T> void cam_ray(const noor_camera& C, uint32_t x, uint32_t y, Rng& rng, V<T>& o, V<T>& d,
+                                RDiff<T>* rd = nullptr) {
     const float rxf = (float)x + rng.next() - 0.5f;
     const float ryf = (float)y + rng.next() - 0.5f;
     const T rx = rxf, ry = ryf;
-    V<T> dc, oc = mk(T(0), T(0), T(0));
+    const V<T> zero = mk(T(0), T(0), T(0));
+    V<T> dc, oc = zero, odx = zero, ody = zero, ddx = zero, ddy = zero;
+    const V<T> dxc = mk((T)C.raster_to_camera[0][0], (T)C.raster_to_camera[1][0], (T)C.raster_to_camera[2][0]);
+    const V<T> dyc = mk((T)C.raster_to_camera[0][1], (T)C.raster_to_camera[1][1], (T)C.raster_to_camera[2][1]);
     bool at_origin = true;
-    if (C.type == NOOR_CAMERA_ENV) {
-        const T theta = K<T>::pi * ry / (T)C.h + K<T>::pi;
-        const T phi = (T(2) * K<T>::pi) * rx / (T)C.w - K<T>::pi / T(2);
+    auto env_dir = [&](T px, T py) {
+        const T theta = K<T>::pi * py / (T)C.h + K<T>::pi;
+        const T phi = (T(2) * K<T>::pi) * px / (T)C.w - K<T>::pi / T(2);
         const T st = std::sin(theta), ct = std::cos(theta);
-        dc = nrm(nrm(mk(st * std::cos(phi), ct, st * std::sin(phi))));
+        return nrm(nrm(mk(st * std::cos(phi), ct, st * std::sin(phi))));
+    };
+    if (C.type == NOOR_CAMERA_ENV) {
+        dc = env_dir(rx, ry);
+        ddx = env_dir(rx + T(1), ry);
+        ddy = env_dir(rx, ry + T(1));
     } else {
         T pc[3];
         for (int r = 0; r < 3; ++r)
             pc[r] = (T)C.raster_to_camera[r][3] + ((T)C.raster_to_camera[r][0] * rx +
                                                    (T)C.raster_to_camera[r][1] * ry + (T)C.raster_to_camera[r][2] * T(0));
+        const V<T> pcv = mk(pc[0], pc[1], pc[2]);
         if (C.type == NOOR_CAMERA_ORTHO) {
-            oc = mk(pc[0], pc[1], pc[2]);
+            oc = pcv;
             dc = mk(T(0), T(0), T(-1));
             at_origin = false;
+            odx = oc + dxc;
+            ody = oc + dyc;
+            ddx = ddy = dc;
         } else {
-            dc = nrm(mk(pc[0], pc[1], pc[2]));
+            dc = nrm(pcv);
             if (C.lens_radius > 0.0f) {
                 const float u1 = rng.next();
                 const float u2 = rng.next();
                 T lx, ly;
                 conc_disk<T>((T)u1, (T)u2, lx, ly);
-                const T ft = -(T)C.focal_length / dc.z;
-                const V<T> pf = mk(T(0), T(0), T(0)) + ft * dc;
-                oc = mk((T)C.lens_radius * lx, (T)C.lens_radius * ly, T(0));
+                const T plx = (T)C.lens_radius * lx, ply = (T)C.lens_radius * ly;
+                T ft = -(T)C.focal_length / dc.z;
+                const V<T> pf = zero + ft * dc;
+                oc = mk(plx, ply, T(0));
                 dc = nrm(pf - oc);
                 at_origin = false;
+                const V<T> dx = nrm(pcv + dxc);
+                ft = -(T)C.focal_length / dx.z;
+                odx = mk(plx, ply, T(0));
+                ddx = nrm(zero + ft * dx - odx);
+                const V<T> dy = nrm(pcv + dyc);
+                ft = -(T)C.focal_length / dy.z;
+                ody = mk(plx, ply, T(0));
+                ddy = nrm(zero + ft * dy - ody);
+            } else {
+                ddx = nrm(pcv + dxc);
+                ddy = nrm(pcv + dyc);
             }
         }
+    }
+    if (rd) {
+        auto point = [&](V<T> q) {
+            T r3[3];
+            for (int r = 0; r < 3; ++r)
+                r3[r] = (T)C.camera_to_world[r][3] + ((T)C.camera_to_world[r][0] * q.x +
+                                                      (T)C.camera_to_world[r][1] * q.y + (T)C.camera_to_world[r][2] * q.z);
+            return mk(r3[0], r3[1], r3[2]);
+        };
+        auto vec = [&](V<T> q) {
+            T r3[3];
+            for (int r = 0; r < 3; ++r)
+                r3[r] = (T)C.camera_to_world[r][0] * q.x + (T)C.camera_to_world[r][1] * q.y +
+                        (T)C.camera_to_world[r][2] * q.z;
+            return mk(r3[0], r3[1], r3[2]);
+        };
+        rd->on = true;
+        rd->odx = point(odx);
+        rd->ody = point(ody);
+        rd->ddx = vec(ddx);
+        rd->ddy = vec(ddy);
     }
     if (at_origin) {
         o = mk((T)C.camera_to_world[0][3], (T)C.camera_to_world[1][3], (T)C.camera_to_world[2][3]);
@@ -1966,6 +2279,27 @@ OR_API void* oracle_create(const noor_payload* P, const noor_spec* S, const noor
         d.emitter_scale = m.emitter_scale;
         d.type = m.type;
         d.dist = m.distribution;
+        // the slots read per hit: image textures, and the alpha and bump
+        // maps of ALPHA and BUMP materials
+        d.tex_mask = 0;
+        auto image = [&](uint32_t idx) { return P->textures[idx].width != 1 || P->textures[idx].height != 1; };
+        auto slot = [&](int k, uint32_t idx, const float* uvs) {
+            d.tex[k] = idx;
+            d.uvs[k][0] = uvs ? uvs[0] : 1.0f;
+            d.uvs[k][1] = uvs ? uvs[1] : 1.0f;
+            d.tex_mask |= 1u << k;
+        };
+        if (image(m.diffuse_tex_idx)) slot(TX_DIFFUSE, m.diffuse_tex_idx, m.diffuse_uvscale);
+        if (image(m.specular_tex_idx)) slot(TX_SPECULAR, m.specular_tex_idx, m.specular_uvscale);
+        if (image(m.emittance_tex_idx)) slot(TX_EMITTANCE, m.emittance_tex_idx, m.emittance_uvscale);
+        if (image(m.roughness_tex_idx)) slot(TX_ROUGHNESS, m.roughness_tex_idx, m.roughness_uvscale);
+        if (image(m.transmission_tex_idx)) slot(TX_TRANSMISSION, m.transmission_tex_idx, nullptr);
+        if (image(m.ior_tex_idx)) slot(TX_IOR, m.ior_tex_idx, nullptr);
+        if (image(m.k_tex_idx)) slot(TX_K, m.k_tex_idx, nullptr);
+        if (m.type & NOOR_ALPHA) slot(TX_ALPHA, m.transparency_tex_idx, m.transparency_uvscale);
+        if (m.type & NOOR_BUMP) slot(TX_BUMP, m.bump_tex_idx, m.bump_uvscale);
+        d.bumpfactor = m.bumpfactor;
+        if (m.type & NOOR_BUMP) sc.has_bump = true;
     }
     build_dist(sc);
     return c;
@@ -2048,15 +2382,18 @@ OR_API void oracle_render(void* h, uint32_t f0, uint32_t nf, uint32_t p0, uint32
                 float sf[3] = {0, 0, 0}, cf[3] = {0, 0, 0};
                 for (uint32_t f = 0; f < nf; ++f) {
                     Rng rng{tea16(p, f0 + f)};
+                    // camera rays carry differentials where bump maps read them
                     if (fp64) {
                         V<double> o, d;
-                        cam_ray<double>(*C, x, y, rng, o, d);
-                        const V<double> L = radiance<double>(sc, o, d, rng, isect, c);
+                        RDiff<double> rd;
+                        cam_ray<double>(*C, x, y, rng, o, d, sc.has_bump ? &rd : nullptr);
+                        const V<double> L = radiance<double>(sc, o, d, rng, isect, c, rd);
                         sd[0] += L.x; sd[1] += L.y; sd[2] += L.z;
                     } else {
                         V<float> o, d;
-                        cam_ray<float>(*C, x, y, rng, o, d);
-                        const V<float> L = radiance<float>(sc, o, d, rng, isect, c);
+                        RDiff<float> rd;
+                        cam_ray<float>(*C, x, y, rng, o, d, sc.has_bump ? &rd : nullptr);
+                        const V<float> L = radiance<float>(sc, o, d, rng, isect, c, rd);
                         const float l[3] = {L.x, L.y, L.z};
                         for (int k = 0; k < 3; ++k) {
                             const float yk = l[k] - cf[k];

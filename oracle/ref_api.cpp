@@ -163,8 +163,10 @@ struct RefPayload {
     int32_t sky = 0;
 };
 
+// ImageTexture(float3): 1 x 1, point filtered, clamped
 static uint32_t constant_texture(RefPayload& P, float r, float g, float b) {
     P.tex_data.push_back({r, g, b, 1.0f});
+    P.tex.push_back(noor_texture{1, 1, nullptr, NOOR_FILTER_POINT, NOOR_ADDRESS_CLAMP});
     return (uint32_t)P.tex_data.size() - 1;
 }
 
@@ -199,45 +201,90 @@ REF_API void* ref_build_payload(const noor_scene_desc* d) {
     for (int k = 0; k < 9; ++k)
         for (const glm::vec4& v : *rows[k]) R.xf[k].insert(R.xf[k].end(), {v.x, v.y, v.z, v.w});
 
-    // materials: one texture of 0.5 first, then per material its constant
-    // parameters as 1 x 1 textures in loadMaterial's order
-    R.tex_data.push_back({0.5f, 0.5f, 0.5f, 1.0f});
+    // Model::loadMaterial: a texture of 0.5 first, then per material its
+    // constants (1 x 1) in the loader's order, an image map instead where the
+    // material names one -- one texture per image (the reference's
+    // name2index), linear filtered and wrapped, map_d point filtered, which
+    // add the ALPHA / BUMP bits.  The CudaMaterial `mt` is one object
+    // reused for every material, so fields a material leaves alone keep
+    // the previous material's values.
+    constant_texture(R, 0.5f, 0.5f, 0.5f);
+    std::vector<int64_t> name2index(d->num_images, -1);
+    auto image = [&](int32_t img, int32_t filter) -> uint32_t {
+        if (name2index[img] < 0) {
+            const noor_image& im = d->images[img];
+            R.tex_data.emplace_back(im.rgba, im.rgba + 4 * (size_t)im.width * im.height);
+            R.tex.push_back(noor_texture{im.width, im.height, nullptr, filter, NOOR_ADDRESS_WRAP});
+            name2index[img] = (int64_t)R.tex_data.size() - 1;
+        }
+        return (uint32_t)name2index[img];
+    };
+    noor_material mt;
+    std::memset(&mt, 0, sizeof(mt));
+    for (float* s : {mt.diffuse_uvscale, mt.specular_uvscale, mt.transparency_uvscale, mt.emittance_uvscale,
+                     mt.bump_uvscale, mt.roughness_uvscale, mt.metalness_uvscale})
+        s[0] = s[1] = 1.0f;
+    mt.bumpfactor = 1.0f;
     for (uint32_t i = 0; i < d->num_materials; ++i) {
         const noor_material_desc& m = d->materials[i];
-        noor_material t;
-        std::memset(&t, 0, sizeof(t));
-        for (float* s : {t.diffuse_uvscale, t.specular_uvscale, t.transparency_uvscale, t.emittance_uvscale,
-                         t.bump_uvscale, t.roughness_uvscale, t.metalness_uvscale})
-            s[0] = s[1] = 1.0f;
-        t.bumpfactor = 1.0f;
-        t.coat_weight = m.coat_weight;
-        t.coat_roughness = m.coat_roughness;
-        t.coat_thickness = m.coat_thickness;
-        t.coat_sigma = m.coat_sigma;
-        t.coat_ior = m.coat_ior;
-        t.emitter_scale = m.emitter_scale;
-        t.type = m.type;
-        t.distribution = m.distribution;
-        t.transmission_tex_idx = constant_texture(R, m.transmission[0], m.transmission[1], m.transmission[2]);
-        t.ior_tex_idx = constant_texture(R, m.ior[0], m.ior[1], m.ior[2]);
-        t.k_tex_idx = constant_texture(R, m.k[0], m.k[1], m.k[2]);
-        t.diffuse_tex_idx = constant_texture(R, m.diffuse[0], m.diffuse[1], m.diffuse[2]);
-        t.roughness_tex_idx = constant_texture(R, m.roughness[0], m.roughness[1], 1.0f);
-        t.metalness_tex_idx = constant_texture(R, 1.0f, 1.0f, 1.0f);
-        t.specular_tex_idx = constant_texture(R, m.specular[0], m.specular[1], m.specular[2]);
-        t.emittance_tex_idx = constant_texture(R, m.emittance[0], m.emittance[1], m.emittance[2]);
-        t.transparency_tex_idx = constant_texture(R, m.transparency[0], m.transparency[1], m.transparency[2]);
-        R.mats.push_back(t);
+        auto has_map = [&](int slot, float* uvscale) {
+            if (m.map[slot] < 0) return false;
+            uvscale[0] = m.map_uvscale[slot][0];
+            uvscale[1] = m.map_uvscale[slot][1];
+            return true;
+        };
+        mt.coat_weight = m.coat_weight;
+        mt.coat_roughness = m.coat_roughness;
+        mt.coat_thickness = m.coat_thickness;
+        mt.coat_sigma = m.coat_sigma;
+        mt.coat_ior = m.coat_ior;
+        mt.emitter_scale = m.emitter_scale;
+        mt.type = m.type;
+        mt.distribution = m.distribution;
+        mt.transmission_tex_idx = constant_texture(R, m.transmission[0], m.transmission[1], m.transmission[2]);
+        mt.ior_tex_idx = constant_texture(R, m.ior[0], m.ior[1], m.ior[2]);
+        mt.k_tex_idx = constant_texture(R, m.k[0], m.k[1], m.k[2]);
+        if (has_map(NOOR_MAP_DIFFUSE, mt.diffuse_uvscale))
+            mt.diffuse_tex_idx = image(m.map[NOOR_MAP_DIFFUSE], NOOR_FILTER_LINEAR);
+        else
+            mt.diffuse_tex_idx = constant_texture(R, m.diffuse[0], m.diffuse[1], m.diffuse[2]);
+        if (has_map(NOOR_MAP_ROUGHNESS, mt.roughness_uvscale))
+            mt.roughness_tex_idx = image(m.map[NOOR_MAP_ROUGHNESS], NOOR_FILTER_LINEAR);
+        else
+            mt.roughness_tex_idx = constant_texture(R, m.roughness[0], m.roughness[1], 1.0f);
+        if (has_map(NOOR_MAP_METALNESS, mt.metalness_uvscale))
+            mt.metalness_tex_idx = image(m.map[NOOR_MAP_METALNESS], NOOR_FILTER_LINEAR);
+        else
+            mt.metalness_tex_idx = constant_texture(R, 1.0f, 1.0f, 1.0f);
+        if (has_map(NOOR_MAP_SPECULAR, mt.specular_uvscale))
+            mt.specular_tex_idx = image(m.map[NOOR_MAP_SPECULAR], NOOR_FILTER_LINEAR);
+        else
+            mt.specular_tex_idx = constant_texture(R, m.specular[0], m.specular[1], m.specular[2]);
+        if (has_map(NOOR_MAP_EMITTANCE, mt.emittance_uvscale))
+            mt.emittance_tex_idx = image(m.map[NOOR_MAP_EMITTANCE], NOOR_FILTER_LINEAR);
+        else
+            mt.emittance_tex_idx = constant_texture(R, m.emittance[0], m.emittance[1], m.emittance[2]);
+        if (has_map(NOOR_MAP_ALPHA, mt.transparency_uvscale)) {
+            mt.transparency_tex_idx = image(m.map[NOOR_MAP_ALPHA], NOOR_FILTER_POINT);
+            mt.type |= NOOR_ALPHA;
+        } else {
+            mt.transparency_tex_idx = constant_texture(R, m.transparency[0], m.transparency[1], m.transparency[2]);
+        }
+        if (has_map(NOOR_MAP_BUMP, mt.bump_uvscale)) {
+            mt.bump_tex_idx = image(m.map[NOOR_MAP_BUMP], NOOR_FILTER_LINEAR);
+            mt.bumpfactor = m.bumpfactor;
+            mt.type |= NOOR_BUMP;
+        }
+        R.mats.push_back(mt);
     }
-    // the sky dome texture last: the HDR map, else SKYDOME_COLOR
-    if (d->skydome_type == NOOR_SKY_HDR)
+    // the sky dome texture last: the HDR map (linear, clamped), else SKYDOME_COLOR
+    if (d->skydome_type == NOOR_SKY_HDR) {
         R.tex_data.emplace_back(d->env_rgba, d->env_rgba + 4 * (size_t)d->env_width * d->env_height);
-    else
+        R.tex.push_back(noor_texture{d->env_width, d->env_height, nullptr, NOOR_FILTER_LINEAR, NOOR_ADDRESS_CLAMP});
+    } else {
         constant_texture(R, 0.25f, 0.25f, 0.25f);
-    for (size_t i = 0; i < R.tex_data.size(); ++i) {
-        const bool env = i + 1 == R.tex_data.size() && d->skydome_type == NOOR_SKY_HDR;
-        R.tex.push_back(noor_texture{env ? d->env_width : 1, env ? d->env_height : 1, R.tex_data[i].data()});
     }
+    for (size_t i = 0; i < R.tex_data.size(); ++i) R.tex[i].rgba = R.tex_data[i].data();
     R.area.assign(d->area_lights, d->area_lights + d->num_area_lights);
     R.point.assign(d->point_lights, d->point_lights + d->num_point_lights);
     R.spot.assign(d->spot_lights, d->spot_lights + d->num_spot_lights);

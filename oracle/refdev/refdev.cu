@@ -495,8 +495,9 @@ std::vector<V> vec4s(const S* p, size_t n) {
     return v;
 }
 
-ImageTexture& add_texture(CudaPayload& P, int w, int h, cudaTextureFilterMode f, const float* rgba) {
-    P._textures.emplace_back(w, h, 4, f, cudaAddressModeClamp);
+ImageTexture& add_texture(CudaPayload& P, int w, int h, cudaTextureFilterMode f, const float* rgba,
+                          cudaTextureAddressMode a = cudaAddressModeClamp) {
+    P._textures.emplace_back(w, h, 4, f, a);
     ImageTexture& t = P._textures.back();
     if (rgba) std::memcpy(const_cast<float*>(t.getData()), rgba, sizeof(float) * 4 * (size_t)w * h);
     return t;
@@ -534,11 +535,11 @@ std::unique_ptr<CudaPayload> make_payload(const abi::noor_payload* A, int sky_ty
     P->_bvh_min_right_start_nodes = vec4s<glm::uvec4>(A->bvh_min_right_start, nn);
     P->_bvh_max_axis_count_nodes = vec4s<glm::uvec4>(A->bvh_max_axis_count, nn);
     P->_bvh_size_bytes = nn * 16;
-    // material textures (1x1 constants, point filtered), then the env
+    // material textures with their own filter and addressing, then the env
     P->_textures.reserve(A->num_textures + 1);
     for (uint32_t i = 0; i + 1 < A->num_textures; ++i) {
         const abi::noor_texture& t = A->textures[i];
-        add_texture(*P, t.width, t.height, cudaFilterModePoint, t.rgba);
+        add_texture(*P, t.width, t.height, (cudaTextureFilterMode)t.filter, t.rgba, (cudaTextureAddressMode)t.address);
     }
     const abi::noor_texture* env = A->num_textures ? &A->textures[A->num_textures - 1] : nullptr;
     if (sky_type == HDR && env)

@@ -25,6 +25,9 @@ int main() {
     using nb::NOOR_SKY_PHYSICAL;
     using nb::NOOR_ISECT_REF_WALD;
     using nb::NOOR_FILM_REF_LERP;
+    using nb::NOOR_FILTER_POINT;
+    using nb::NOOR_FILTER_LINEAR;
+    using nb::NOOR_ADDRESS_CLAMP;
     // ---- payload: two triangles, two instances, three nodes, textures of
     // 4, 3 and 1 channels, two materials and one light of each kind
     auto P = std::make_unique<CudaPayload>();
@@ -105,6 +108,8 @@ int main() {
     EXPECT(g.textures[0].width == 1 && g.textures[0].rgba[0] == 0.5f && g.textures[0].rgba[2] == 0.125f);
     EXPECT(g.textures[1].rgba[0] == 0.75f && g.textures[1].rgba[1] == 0.0f && g.textures[1].rgba[3] == 1.0f);
     EXPECT(g.textures[2].width == 4 && g.textures[2].height == 2 && g.textures[2].rgba[31] == 15.5f);
+    EXPECT(g.textures[0].filter == NOOR_FILTER_POINT && g.textures[0].address == NOOR_ADDRESS_CLAMP);
+    EXPECT(g.textures[2].filter == NOOR_FILTER_LINEAR && g.textures[2].address == NOOR_ADDRESS_CLAMP);
     EXPECT(g.num_materials == 2);
     const noor_material& mt = g.materials[1];
     EXPECT(mt.diffuse_uvscale[0] == 2.0f && mt.metalness_uvscale[1] == 5.0f && mt.diffuse_tex_idx == 2);

@@ -21,6 +21,8 @@ Fixtures:
                         the room, a sky-lit and an HDR-lit sphere field
   refdev_envdist.npz    the sky dome's CudaDistribution2D for an HDR map and
                         for the physical sky (sampled rows), with samples
+  refdev_textures.npz   the textured room: camera-ray hits (alpha cuts) and
+                        an 8-frame film (image maps, bump, differentials)
 """
 from __future__ import annotations
 
@@ -158,10 +160,29 @@ def envdist(out: Path):
     np.savez_compressed(out / "refdev_envdist.npz", **res)
 
 
+def textures(out: Path):
+    """the textured room (image maps, a roughness map, a bump map with ray
+    differentials, an alpha-cut panel): camera-ray hits and an 8-frame film"""
+    scene = scenes.textured_room_scene()
+    built, spec, cam, hosek = built_structs(scene)
+    dev = rd.RefDevice(built.payload, hosek, cam, spec)
+    rays = np.concatenate([dev.camera_rays(1), dev.camera_rays(3)])
+    res = dict(rays=rays, hits=dev.trace_closest(rays), any=dev.trace_any(rays), film=dev.render(1, 8))
+    dev.close()
+    np.savez_compressed(out / "refdev_textures.npz", **res)
+
+
+STEPS = (routines, bsdf, trace, render, envdist, textures)
+
+
 def main():
+    """python make_refdev_golden.py [out_dir] [step ...] (all steps by default)"""
     out = Path(sys.argv[1]) if len(sys.argv) > 1 else Path(__file__).resolve().parent
     out.mkdir(parents=True, exist_ok=True)
-    for step in (routines, bsdf, trace, render, envdist):
+    names = sys.argv[2:]
+    for step in STEPS:
+        if names and step.__name__ not in names:
+            continue
         step(out)
         print(f"{step.__name__}: ok", flush=True)
 

@@ -104,8 +104,8 @@ def _bad_selector(b, cam, sp):
     sp.intersector = 3
 
 
-def _bump_map(b, cam, sp):
-    b.payload.materials[0].type |= 1 << 13  # NOOR_BUMP
+def _bad_texture_mode(b, cam, sp):
+    b.payload.textures[0].filter = 5
 
 
 def _bad_texture_index(b, cam, sp):
@@ -130,7 +130,7 @@ def _two_infinite_lights(b, cam, sp):
     (_bad_camera, 1, b"unknown camera type"),
     (_bad_sky, 1, b"bad skydome type"),
     (_bad_selector, 1, b"bad selector"),
-    (_bump_map, 4, b"bump maps are not implemented"),
+    (_bad_texture_mode, 1, b"texture filter or address mode out of range"),
     (_bad_texture_index, 1, b"texture index out of range"),
     (_bad_distribution, 1, b"unknown microfacet distribution"),
     (_distant_lights_without_array, 1, b"bad point, spot or distant light array"),

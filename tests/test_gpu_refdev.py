@@ -119,6 +119,46 @@ def test_room_render_megakernel_and_wavefront():
         r.close()
 
 
+# ------------------------------------------------ textures, alpha, bump
+def test_textured_room_against_the_reference():
+    """the textured room (floor checker, roughness map, a bump map read with
+    ray differentials, an alpha-cut panel): closest and any hits of the
+    camera rays bit for bit (the alpha cuts included), and the 8-frame film
+    of the megakernel and of the wavefront against path_tracer_kernel's --
+    the texture unit does the same fetches for both.  Per pixel the films
+    agree to the untextured bars at the median; in the tails, pixels whose
+    paths read the bump map move: its slopes come from ray differentials,
+    and a last-bit difference in them (FMA contraction here, none in the
+    reference built for the harness) moves the map's 8-bit filter weights,
+    hence bars of 1e-3 / 1e-2 at the 99th / 99.9th percentile."""
+    z = load("textures")
+    s = scenes.textured_room_scene()
+    r = scenes.Renderer(s, intersector=_capi.NOOR_ISECT_REF_WALD, film_mode=_capi.NOOR_FILM_REF_LERP)
+    try:
+        rays = z["rays"]
+        hits = trace_closest(rays)
+        probe.check_trace(z["hits"], z["any"], hits, trace_any(rays))
+        r.render(8)
+        img = r.framebuffer()
+        # where the error lives: by the material the camera ray of frame 1 hits
+        e = probe.rel_err(img[..., :3], z["film"][..., :3], 1e-3).max(-1).ravel()
+        n = r.w * r.h
+        mats = np.array([r.built.payload.attribute_indices[4 * int(t) + 3] for t in hits[:n, 1]])
+        mats[hits[:n, 6] == 0] = -1
+        for m in np.unique(mats):
+            print("material", int(m), "pixels", int((mats == m).sum()), "q99", float(np.quantile(e[mats == m], 0.99)))
+        probe.check_film(z["film"], img, q99=1e-3, q999=1e-2)
+        import torch
+        film = torch.zeros(r.w * r.h * 4, dtype=torch.float32, device="cuda")
+        f = scenes.wf_frame(0, s.camera, 8, bounces=s.render["bounces"], first_frame=1, d_film=film.data_ptr())
+        _capi.call("noor_wavefront_render", C.byref(f), 1, C.byref(scenes.wf_params(block=128, capacity=1 << 16)))
+        torch.cuda.synchronize()
+        probe.check_film(z["film"], film.cpu().numpy().reshape(r.h, r.w, 4), q99=1e-3, q999=1e-2)
+        assert r.status(reset=True) == 0
+    finally:
+        r.close()
+
+
 # ------------------------------------------------ NOOR_ENV_REFERENCE mode
 def _ref_mode(scene, **kw):
     r = scenes.Renderer(scene, **kw)

@@ -129,3 +129,22 @@ def test_reference_distribution_sampling_bit_exact():
     z = load("envdist")
     got = O.ref_dist_sample(z["func"], z["cdf"], int(z["w"]), int(z["h"]), z["u"])
     assert np.array_equal(got, z["samples"])
+
+
+def test_textured_room_against_the_reference():
+    """the oracle on the textured room: camera-ray hits bit for bit (alpha
+    cuts included); the film through the oracle's emulation of the texture
+    unit (its fetches match the unit's on about 99 %, the rest within
+    1/256 of a texel difference), to looser bars than the untextured room"""
+    z = load("textures")
+    s = scenes.textured_room_scene()
+    b = scenes.BuiltPayload(s)
+    spec = b.default_spec(s.render["bounces"], s.render.get("rr", 1))
+    spec.intersector = _capi.NOOR_ISECT_REF_WALD
+    orc = Oracle(b.payload, spec, scenes.make_hosek(None))
+    rays = z["rays"]
+    probe.check_trace(z["hits"], z["any"], orc.trace_closest(rays, 1), orc.trace_any(rays, 1))
+    cam = scenes.make_camera(s.camera)
+    img = orc.render(cam, 1, 8, isect=_capi.NOOR_ISECT_REF_WALD).reshape(cam.h, cam.w, 3)
+    orc.close()
+    probe.check_film(z["film"], img, q99=1e-3, q999=3e-2)

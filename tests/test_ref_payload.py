@@ -76,6 +76,7 @@ SCENES = {
     "env_small": lambda: scenes.env_scene(width=64, height=36, count=3, level=3),
     "room_scene": lambda: scenes.room_scene(),
     "instanced": instanced_scene,
+    "textured_room": lambda: scenes.textured_room_scene(),
 }
 
 
