@@ -240,6 +240,8 @@ NB_D RayDiff load_diff(const WfDev& W, uint32_t slot) {
 // rays of the next work items.  The block takes its work items with one
 // atomic, in lane order (consecutive lanes: consecutive pixels of one 8x4
 // tile), and adds its active slots to the active count with one atomic.
+// DIFF: some scene of the batch has bump maps (camera rays with differentials)
+template <bool DIFF>
 __global__ void __launch_bounds__(kRegenBlock) wf_regen(WfDev W) {
     __shared__ uint32_t warp_off[kRegenBlock / 32];
     __shared__ unsigned long long block_base;
@@ -309,7 +311,7 @@ __global__ void __launch_bounds__(kRegenBlock) wf_regen(WfDev W) {
             const uint32_t pix = tile_pixel((uint32_t)(local / F.spp), F.cam.w, F.cam.h);
             Rng rng{tea16(pix, F.first_frame + sample)};
             float3 o, d;
-            if (W.diff) {
+            if (DIFF) {
                 // a batch with bump maps: camera rays carry differentials
                 // where their scene has bump maps
                 RayDiff rd{};
@@ -881,7 +883,10 @@ struct WfLaunch {
 static cudaError_t wf_iteration(const WfDev& W, const WfLaunch& L, cudaStream_t s, bool conditional,
                                 uint32_t* go_out, cudaEvent_t* ev = nullptr) {
     if (ev) cudaEventRecord(ev[0], s);
-    wf_regen<<<(W.cap + kRegenBlock - 1) / kRegenBlock, kRegenBlock, 0, s>>>(W);
+    if (L.diff)
+        wf_regen<true><<<(W.cap + kRegenBlock - 1) / kRegenBlock, kRegenBlock, 0, s>>>(W);
+    else
+        wf_regen<false><<<(W.cap + kRegenBlock - 1) / kRegenBlock, kRegenBlock, 0, s>>>(W);
     if (ev) cudaEventRecord(ev[1], s);
     if (W.level >= 2) {
         L.ext_key<<<(W.cap + kBinBlock - 1) / kBinBlock, kBinBlock, 0, s>>>(W, L.scene);
