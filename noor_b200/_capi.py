@@ -56,6 +56,7 @@ TRI_LEAF_MASK = 0x80000000
 MESH_LEAF_MASK = 0x40000000
 MESH_INSTANCE_MASK = 0x20000000
 MESH_INNER_MASK = 0x10000000
+LIGHT_NODE_MASK = 0x08000000
 
 
 class Shape(C.Structure):
@@ -245,6 +246,7 @@ PROTOTYPES = {
     "noor_payload_triangle_order": (C.c_int, [C.c_void_p, pu, C.c_size_t]),
     "noor_payload_default_spec": (C.c_int, [C.c_void_p, u32, u32, C.POINTER(Spec)]),
     "noor_free_payload": (None, [C.c_void_p]),
+    "noor_wide_tree_info": (C.c_int, [C.POINTER(Payload), u32, pu, pu, pu, pu]),
     "noor_camera_lookat": (C.c_int, [pf, pf, pf, f32, u32, u32, C.POINTER(Camera)]),
     "noor_hosek_fit": (C.c_int, [pf, f32, pf, f32, f32, f32, f32, C.POINTER(HosekSky)]),
     "noor_scene_upload": (C.c_int, [C.POINTER(Payload), C.POINTER(HosekSky), C.POINTER(Spec), pu]),

@@ -25,7 +25,7 @@ CU_SOURCES = ["kernels.cu", "envmap.cu", "context.cu", "wavefront.cu", "adjoint.
               "bvh_gpu.cu"]
 # the GPU BVH builder rounds its split search as the host builder does
 CU_EXTRA = {"bvh_gpu.cu": ["-fmad=false"]}
-CPP_SOURCES = ["scene_build.cpp"]
+CPP_SOURCES = ["scene_build.cpp", "wide_bvh.cpp"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -14,6 +14,12 @@
 #include "kernels.h"
 #include "runtime.h"
 #include "shading.cuh"
+#include "wide_bvh.h"
+
+// 1: traversal walks the four-wide tree built at upload; 0: the binary tree
+#ifndef NB_WIDE_TREE
+#define NB_WIDE_TREE 1
+#endif
 
 // ------------------------------------------------------------------ errors
 static thread_local std::string tl_err;
@@ -251,6 +257,14 @@ void apply_spec(SceneState& st, const noor_spec& s) {
     D.film_mode = s.film_mode;
     int cap = (int)s.bvh_height + (int)st.max_mesh_leaf + 4;
     D.stack_cap = cap < 16 ? 16 : (cap > 96 ? 96 : cap);
+    // the four-wide tree serves the root it was built from
+    const bool wide = st.wide_nodes && s.bvh_root_node == st.wide_root;
+    D.nodes4 = wide ? st.wide_nodes : nullptr;
+    D.map4 = wide ? st.wide_map : nullptr;
+    D.stack_cap4 = wide ? st.wide_cap : 0;
+    D.closest4 = wide && st.wide_closest ? 1u : 0u;
+    D.stack_cap4c = D.closest4 ? st.wide_cap_closest : 0;
+    D.stack_words = std::max(D.stack_cap, std::max(D.stack_cap4, D.stack_cap4c));
 }
 
 void apply_hosek(SceneState& st, const noor_hosek_sky& h) {
@@ -395,6 +409,23 @@ int upload_scene(Context& C, const noor_payload* P, const noor_hosek_sky* H, con
         }
         st.max_mesh_leaf = mml;
         if ((rc = st.upload((void**)&D.nodes, h.data(), nn * sizeof(DevNode), "nodes"))) return rc;
+#if NB_WIDE_TREE
+        // the four-wide tree of the spec's root (shadow rays, and closest hit
+        // where it qualifies); a tree it does not suit keeps the binary
+        // traversal
+        WideTree wt;
+        if (build_wide_tree(reinterpret_cast<const uint32_t*>(h.data()), nn, S->bvh_root_node, kWideMaxStack, wt,
+                            nullptr)) {
+            if ((rc = st.upload((void**)&st.wide_nodes, wt.nodes.data(), wt.nodes.size() * sizeof(DevNode4),
+                                "wide nodes")) ||
+                (rc = st.upload((void**)&st.wide_map, wt.map.data(), nn * sizeof(uint32_t), "wide map")))
+                return rc;
+            st.wide_root = wt.root;
+            st.wide_cap = wt.stack_need;
+            st.wide_cap_closest = wt.stack_need_closest;
+            st.wide_closest = wt.closest;
+        }
+#endif
     }
     {
         std::vector<DevWaldTri> w(nt);

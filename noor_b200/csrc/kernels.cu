@@ -127,7 +127,7 @@ __global__ void film_resolve(uint32_t npix, int mode, float inv_count, const flo
     out[pix] = mode == NOOR_FILM_KAHAN ? make_float4(s.x * inv_count, s.y * inv_count, s.z * inv_count, 1.0f) : s;
 }
 
-template <int ISECT>
+template <int ISECT, bool WIDE>
 __global__ void __launch_bounds__(kTraceBlock) k_trace_closest(DevScene S, const noor_ray* rays, noor_hit* hits,
                                                                size_t n, uint32_t* status) {
     extern __shared__ uint32_t smem[];
@@ -137,7 +137,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_closest(DevScene S, const
     const noor_ray r = rays[i];
     float tmax = r.tmax;
     HitRec rec{0.0f, 0.0f, 0u, 0u, 0u};
-    const bool h = trace_closest<ISECT>(S, f3(r.org[0], r.org[1], r.org[2]), f3(r.dir[0], r.dir[1], r.dir[2]),
+    const bool h = trace_primary<ISECT, true, WIDE>(S, f3(r.org[0], r.org[1], r.org[2]), f3(r.dir[0], r.dir[1], r.dir[2]),
                                         tmax, rec, st, status);
     noor_hit o;
     o.t = tmax;
@@ -151,7 +151,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_closest(DevScene S, const
     hits[i] = o;
 }
 
-template <int ISECT>
+template <int ISECT, bool WIDE>
 __global__ void __launch_bounds__(kTraceBlock) k_trace_any(DevScene S, const noor_ray* rays, uint32_t* occ,
                                                            size_t n, uint32_t* status) {
     extern __shared__ uint32_t smem[];
@@ -159,8 +159,8 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_any(DevScene S, const noo
     if (i >= n) return;
     SmemStack st{smem + threadIdx.x, (int)blockDim.x, S.stack_cap};
     const noor_ray r = rays[i];
-    occ[i] = trace_any<ISECT>(S, f3(r.org[0], r.org[1], r.org[2]), f3(r.dir[0], r.dir[1], r.dir[2]), r.tmax, st,
-                              status)
+    occ[i] = trace_shadow<ISECT, true, WIDE>(S, f3(r.org[0], r.org[1], r.org[2]), f3(r.dir[0], r.dir[1], r.dir[2]),
+                                             r.tmax, st, status)
                  ? 1u
                  : 0u;
 }
@@ -359,37 +359,42 @@ cudaError_t launch_resolve(uint32_t npix, int mode, float inv_count, const float
     return cudaGetLastError();
 }
 
+// one launch of a ray-batch kernel: the four-wide or the binary traversal,
+// per intersector
+template <template <int, bool> class K, class T>
+static cudaError_t launch_trace(const DevScene& S, bool wide, const noor_ray* rays, T* out, size_t n,
+                                uint32_t* status, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    // room for the four-wide tree's stacks as well as the binary one's
+    const size_t sm = (size_t)S.stack_words * kTraceBlock * sizeof(uint32_t);
+    const uint32_t grid = (uint32_t)((n + kTraceBlock - 1) / kTraceBlock);
+    auto go = [&](auto kern) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e != cudaSuccess) return e;
+        kern<<<grid, kTraceBlock, sm, s>>>(S, rays, out, n, status);
+        return cudaGetLastError();
+    };
+    if (S.isect == NOOR_ISECT_WATERTIGHT)
+        return wide ? go(K<NOOR_ISECT_WATERTIGHT, true>::fn) : go(K<NOOR_ISECT_WATERTIGHT, false>::fn);
+    return wide ? go(K<NOOR_ISECT_REF_WALD, true>::fn) : go(K<NOOR_ISECT_REF_WALD, false>::fn);
+}
+template <int I, bool W>
+struct ClosestK {
+    static constexpr auto fn = k_trace_closest<I, W>;
+};
+template <int I, bool W>
+struct AnyK {
+    static constexpr auto fn = k_trace_any<I, W>;
+};
+
 cudaError_t launch_trace_closest(const DevScene& S, const noor_ray* rays, noor_hit* hits, size_t n, uint32_t* status,
                                  cudaStream_t s) {
-    if (n == 0) return cudaSuccess;
-    const size_t sm = stack_bytes(S, kTraceBlock);
-    const uint32_t grid = (uint32_t)((n + kTraceBlock - 1) / kTraceBlock);
-    if (S.isect == NOOR_ISECT_WATERTIGHT) {
-        cudaFuncSetAttribute(k_trace_closest<NOOR_ISECT_WATERTIGHT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)sm);
-        k_trace_closest<NOOR_ISECT_WATERTIGHT><<<grid, kTraceBlock, sm, s>>>(S, rays, hits, n, status);
-    } else {
-        cudaFuncSetAttribute(k_trace_closest<NOOR_ISECT_REF_WALD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)sm);
-        k_trace_closest<NOOR_ISECT_REF_WALD><<<grid, kTraceBlock, sm, s>>>(S, rays, hits, n, status);
-    }
-    return cudaGetLastError();
+    return launch_trace<ClosestK>(S, S.closest4 != 0u, rays, hits, n, status, s);
 }
 
 cudaError_t launch_trace_any(const DevScene& S, const noor_ray* rays, uint32_t* occ, size_t n, uint32_t* status,
                              cudaStream_t s) {
-    if (n == 0) return cudaSuccess;
-    const size_t sm = stack_bytes(S, kTraceBlock);
-    const uint32_t grid = (uint32_t)((n + kTraceBlock - 1) / kTraceBlock);
-    if (S.isect == NOOR_ISECT_WATERTIGHT) {
-        cudaFuncSetAttribute(k_trace_any<NOOR_ISECT_WATERTIGHT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)sm);
-        k_trace_any<NOOR_ISECT_WATERTIGHT><<<grid, kTraceBlock, sm, s>>>(S, rays, occ, n, status);
-    } else {
-        cudaFuncSetAttribute(k_trace_any<NOOR_ISECT_REF_WALD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        k_trace_any<NOOR_ISECT_REF_WALD><<<grid, kTraceBlock, sm, s>>>(S, rays, occ, n, status);
-    }
-    return cudaGetLastError();
+    return launch_trace<AnyK>(S, S.nodes4 != nullptr, rays, occ, n, status, s);
 }
 
 cudaError_t launch_camera_rays(const DevCamera& C, uint32_t frame, noor_ray* rays, cudaStream_t s) {

@@ -18,6 +18,13 @@ struct SceneState {
     bool quad_lights_only = true;   // every area light a quad
     int sky_type = 0;
     uint32_t max_mesh_leaf = 0;
+    // the four-wide any-hit tree (wide_bvh.h) and the root it was built from
+    const DevNode4* wide_nodes = nullptr;
+    const uint32_t* wide_map = nullptr;
+    uint32_t wide_root = 0;
+    int wide_cap = 0;
+    int wide_cap_closest = 0;
+    bool wide_closest = false;
     // NOOR_ENV_REFERENCE, built on first use: the environment (or baked sky)
     // as a CUDA array + texture object, the bake buffer and the tables
     cudaArray_t env_array = nullptr;

@@ -16,6 +16,15 @@ struct __align__(32) DevNode {
     uint4 hi;
 };
 
+// Four-wide any-hit node = 128 B (one line): the four entry boxes as
+// structure of arrays, the entry words and meta (wide_bvh.h)
+struct __align__(128) DevNode4 {
+    float4 lox, loy, loz;
+    float4 hix, hiy, hiz;
+    uint4 child;
+    uint4 meta;
+};
+
 // Reference-Wald triangle = 64 B: the two records the t-range test reads
 // (ax,nu,nv,nd | cnu,cnv,deg,mat) share the first sector, the barycentric
 // record and the attribute indices (v0,v1,v2,material) the second.
@@ -193,6 +202,15 @@ struct DevScene {
     uint32_t has_tex;       // some material reads a texture per hit (image maps, alpha, bump)
     uint32_t has_alpha;     // some material is ALPHA: triangle tests fetch its alpha map
     uint32_t has_bump;      // some material is BUMP: rays carry differentials
+    // the four-wide tree of the spec's root (null: traversal walks the
+    // binary tree), its map from binary inner nodes, and the stack words its
+    // traversals can need; stack_words = the largest of the stacks
+    const DevNode4* nodes4;
+    const uint32_t* map4;
+    int stack_cap4;
+    int stack_cap4c;        // closest hit over the four-wide tree (closest4)
+    uint32_t closest4;      // closest hit may use the four-wide tree
+    int stack_words;
     // NOOR_ENV_REFERENCE: the reference's distribution tables (row r at
     // r * (rw + 1), the marginal at rh * (rw + 1)) and the environment as a
     // texture object (linear filter, clamp, normalised coordinates)

@@ -11,6 +11,7 @@
 // child (chosen by the ray's direction sign on the split axis) pops next.
 #pragma once
 #include "scene_dev.cuh"
+#include "wide_bvh.h"
 
 namespace nb {
 
@@ -474,6 +475,387 @@ NB_D bool trace_any(const DevScene& S, const float3& o, const float3& d, float t
         ni = next;
     }
     return false;
+}
+
+// A ray the four-wide tree may not skip an expanded child's box for: a
+// direction component that is zero, subnormal or NaN (its slab reciprocal is
+// infinite, and the per-axis intervals stop being monotone in the box), or
+// an origin that is not finite.
+NB_D bool wide_degenerate(const float3& o, const float3& d) {
+    const float m = 1.17549435e-38f;  // FLT_MIN
+    return !(fabsf(d.x) >= m && fabsf(d.y) >= m && fabsf(d.z) >= m && fabsf(o.x) <= 3.40282347e38f &&
+             fabsf(o.y) <= 3.40282347e38f && fabsf(o.z) <= 3.40282347e38f);
+}
+
+NB_D uint32_t word_of(const uint4& v, uint32_t s) { return s == 0 ? v.x : (s == 1 ? v.y : (s == 2 ? v.z : v.w)); }
+NB_D float comp4(const float4& v, uint32_t s) { return s == 0 ? v.x : (s == 1 ? v.y : (s == 2 ? v.z : v.w)); }
+
+// The slab test of noor/cuda/bbox.cuh:62-80 on a wide node's four entry
+// boxes at once, axis by axis (the same operations and comparisons as
+// slab_hit_f for each box); bit s set when box s passes.
+NB_D uint32_t slab4(const TRay& r, const DevNode4* nd, float tmax) {
+    float t0[4], t1[4];
+    uint32_t ok = 0xFu;
+    {
+        const float4 a = __ldg(&nd->lox), b = __ldg(&nd->hix);
+        const bool n = r.neg & 1u;
+#pragma unroll
+        for (uint32_t s = 0; s < 4; ++s) {
+            t0[s] = xmul(xsub(n ? comp4(b, s) : comp4(a, s), r.o.x), r.inv.x);
+            t1[s] = xmul(xsub(n ? comp4(a, s) : comp4(b, s), r.o.x), r.inv.x);
+        }
+    }
+    {
+        const float4 a = __ldg(&nd->loy), b = __ldg(&nd->hiy);
+        const bool n = r.neg & 2u;
+#pragma unroll
+        for (uint32_t s = 0; s < 4; ++s) {
+            const float u0 = xmul(xsub(n ? comp4(b, s) : comp4(a, s), r.o.y), r.inv.y);
+            const float u1 = xmul(xsub(n ? comp4(a, s) : comp4(b, s), r.o.y), r.inv.y);
+            if (t0[s] > u1 || u0 > t1[s]) ok &= ~(1u << s);
+            if (u0 > t0[s]) t0[s] = u0;
+            if (u1 < t1[s]) t1[s] = u1;
+        }
+    }
+    {
+        const float4 a = __ldg(&nd->loz), b = __ldg(&nd->hiz);
+        const bool n = r.neg & 4u;
+#pragma unroll
+        for (uint32_t s = 0; s < 4; ++s) {
+            const float u0 = xmul(xsub(n ? comp4(b, s) : comp4(a, s), r.o.z), r.inv.z);
+            const float u1 = xmul(xsub(n ? comp4(a, s) : comp4(b, s), r.o.z), r.inv.z);
+            if (t0[s] > u1 || u0 > t1[s]) ok &= ~(1u << s);
+            if (u0 > t0[s]) t0[s] = u0;
+            if (u1 < t1[s]) t1[s] = u1;
+        }
+    }
+#pragma unroll
+    for (uint32_t s = 0; s < 4; ++s)
+        if (!(t0[s] < tmax && t1[s] > 0.0f)) ok &= ~(1u << s);
+    return ok;
+}
+
+// Any hit over the four-wide tree (S.nodes4, layout in wide_bvh.h): the same
+// occluders, found in the same order, as trace_any on the binary tree.  A
+// wide node's entries are tested together; those that pass are taken in the
+// binary traversal's order (the near side of P's split axis first, then the
+// near side of each expanded child's), the first at once and the rest
+// pushed.  Binary nodes (leaves, mesh leaves, instances, light nodes and
+// deferred entries) are taken as the binary traversal takes them.  The stack
+// holds S.stack_cap4 words, the deepest this tree can need.
+template <int ISECT, bool EXT = true>
+NB_D bool trace_any4(const DevScene& S, const float3& o, const float3& d, float tmax, const SmemStack& st,
+                     uint32_t* status) {
+    TRay wr;
+    tray_setup(wr, o, d);
+    const bool wdeg = wide_degenerate(o, d);
+    TRay lr = wr;
+    bool ldeg = wdeg;
+    WtRay wt;
+    if (ISECT == NOOR_ISECT_WATERTIGHT) wt_setup(wt, lr.d);
+    const int cap = S.stack_cap4;
+    int top = 0;
+    uint32_t next = kWRef | kWUntested | S.root;
+    for (;;) {
+        const uint32_t cur = next;
+        next = kWNone;
+        if (!(cur & kWRef)) {
+            const DevNode4* nd = S.nodes4 + cur;
+            const uint4 meta = __ldg(&nd->meta);
+            if (meta.x & kW4World) {
+                lr = wr;
+                ldeg = wdeg;
+                if (ISECT == NOOR_ISECT_WATERTIGHT) wt_setup(wt, lr.d);
+            }
+            const uint4 cw = __ldg(&nd->child);
+            uint32_t inc = slab4(lr, nd, tmax);
+#pragma unroll
+            for (uint32_t s = 0; s < 4; ++s) {
+                const uint32_t w = word_of(cw, s);
+                if (w == kWNone) inc &= ~(1u << s);
+                else if ((w & (kWRef | kWUntested)) == (kWRef | kWUntested)) inc |= 1u << s;
+            }
+            if (ldeg) {
+                // the expanded children's own boxes, as the binary traversal tests them
+                if ((inc & 3u) && (meta.x & kW4ExpandL)) {
+                    const DevNode* c = S.nodes + meta.y;
+                    if (!slab_hit(lr, __ldg(&c->lo), __ldg(&c->hi), tmax)) inc &= ~3u;
+                }
+                if ((inc & 12u) && (meta.x & kW4ExpandR)) {
+                    const DevNode* c = S.nodes + meta.z;
+                    if (!slab_hit(lr, __ldg(&c->lo), __ldg(&c->hi), tmax)) inc &= ~12u;
+                }
+            }
+            if (inc) {
+                const bool right_first = (lr.neg >> ((meta.x >> 4) & 3u)) & 1u;
+                const bool swap_l = (meta.x & kW4ExpandL) && ((lr.neg >> ((meta.x >> 6) & 3u)) & 1u);
+                const bool swap_r = (meta.x & kW4ExpandR) && ((lr.neg >> ((meta.x >> 8) & 3u)) & 1u);
+                const uint32_t l = swap_l ? 0x1u : 0x4u;   // slots (0,1) or (1,0), two bits each
+                const uint32_t r = swap_r ? 0xBu : 0xEu;   // slots (2,3) or (3,2)
+                const uint32_t order = right_first ? (r | l << 4) : (l | r << 4);
+                // last in order first: each taken word pushes the one held before it
+#pragma unroll
+                for (int j = 3; j >= 0; --j) {
+                    const uint32_t s = (order >> (2 * j)) & 3u;
+                    if (!((inc >> s) & 1u)) continue;
+                    if (next != kWNone) {
+                        if (top + 1 > cap) {
+                            atomicOr(status, NOOR_DEV_STACK_OVERFLOW);
+                            return false;
+                        }
+                        st.base[top * st.stride] = next;
+                        ++top;
+                    }
+                    next = word_of(cw, s);
+                }
+            }
+        } else {
+            const uint32_t ni = cur & kWIndex;
+            const DevNode* nd = S.nodes + ni;
+            const uint4 lo = __ldg(&nd->lo);
+            const uint4 hi = __ldg(&nd->hi);
+            if (hi.w & NOOR_MESH_NODE_MASK) {
+                lr = wr;
+                ldeg = wdeg;
+                if (ISECT == NOOR_ISECT_WATERTIGHT) wt_setup(wt, lr.d);
+            }
+            if (!(cur & kWUntested) || slab_hit(lr, lo, hi, tmax)) {
+                if (!(hi.w & kNodeKindMask)) {
+                    next = __ldg(&S.map4[ni]);
+                    if (next == kWNone) {
+                        atomicOr(status, NOOR_DEV_BAD_INDEX);
+                        return false;
+                    }
+                } else if (hi.w & NOOR_LIGHT_NODE_MASK) {
+                    const uint32_t li = hi.w & NOOR_LIGHT_MASK;
+                    float tm = tmax;
+                    if ((int)li < S.num_area_lights &&
+                        shape_hit<EXT, ISECT == NOOR_ISECT_REF_WALD>(S.area_lights[li], o, d, tm))
+                        return true;
+                } else if (hi.w & NOOR_MESH_INSTANCE_MASK) {
+                    tray_to_object(lr, wr, S.xforms + (hi.w & NOOR_TRANS_MASK));
+                    ldeg = wide_degenerate(lr.o, lr.d);
+                    if (ISECT == NOOR_ISECT_WATERTIGHT) wt_setup(wt, lr.d);
+                    next = kWRef | kWUntested | lo.w;
+                } else if (hi.w & NOOR_MESH_LEAF_MASK) {
+                    const uint32_t cnt = hi.w & NOOR_COUNT_MASK;
+                    if (top + (int)cnt > cap + 1) {
+                        atomicOr(status, NOOR_DEV_STACK_OVERFLOW);
+                        return false;
+                    }
+                    for (uint32_t i = 1; i < cnt; ++i) {
+                        st.base[top * st.stride] = kWRef | kWUntested | (ni + i);
+                        ++top;
+                    }
+                    if (cnt) next = kWRef | kWUntested | (ni + cnt);
+                } else {
+                    const uint32_t start = lo.w;
+                    const uint32_t end = start + (hi.w & NOOR_TRI_COUNT_MASK);
+                    for (uint32_t ti = start; ti < end; ++ti) {
+                        float tm = tmax, bu, bv;
+                        uint32_t mt;
+                        bool h;
+                        if (ISECT == NOOR_ISECT_WATERTIGHT)
+                            h = wt_test(lr, wt, S.wtri + ti, tm, bu, bv, mt);
+                        else
+                            h = wald_test(lr, S.wald + ti, tm, bu, bv, mt);
+                        if (h && EXT && S.has_alpha && (mt & NOOR_ALPHA) && alpha_cut<ISECT>(S, ti, bu, bv)) h = false;
+                        if (h) return true;
+                    }
+                }
+            }
+        }
+        if (next == kWNone) {
+            if (top == 0) break;
+            --top;
+            next = st.base[top * st.stride];
+        }
+    }
+    return false;
+}
+
+// Closest hit over the four-wide tree: the same hit, to the bit, as
+// trace_closest.  Leaves are taken in the binary traversal's order, and
+// every binary node (leaf, mesh leaf, instance, light) is slab-tested when it
+// is taken, against the hit distance of that moment, as the binary traversal
+// tests it; a wide node's tests only skip entries that the binary traversal
+// would find missed later (its hit distance only shrinks, and a box inside a
+// missed box is missed).  Below a ray whose boxes may not be skipped
+// (wide_degenerate) inner nodes are walked one by one, as trace_closest walks
+// them.  The stack holds S.stack_cap4c words, the deepest this tree needs.
+template <int ISECT, bool EXT = true>
+NB_D bool trace_closest4(const DevScene& S, const float3& o, const float3& d, float& tmax, HitRec& rec,
+                         const SmemStack& st, uint32_t* status) {
+    TRay wr;
+    tray_setup(wr, o, d);
+    const bool wdeg = wide_degenerate(o, d);
+    TRay lr = wr;
+    bool ldeg = wdeg;
+    WtRay wt;
+    if (ISECT == NOOR_ISECT_WATERTIGHT) wt_setup(wt, lr.d);
+    float ltmax = tmax;
+    uint32_t ins = 0;
+    bool hit = false;
+    const int cap = S.stack_cap4c;
+    int top = 0;
+    uint32_t next = kWRef | S.root;
+    for (;;) {
+        const uint32_t cur = next;
+        next = kWNone;
+        if (!(cur & kWRef)) {
+            const DevNode4* nd = S.nodes4 + cur;
+            const uint4 meta = __ldg(&nd->meta);
+            if (meta.x & kW4World) {
+                lr = wr;
+                ltmax = tmax;
+                ldeg = wdeg;
+                if (ISECT == NOOR_ISECT_WATERTIGHT) wt_setup(wt, lr.d);
+            }
+            const uint4 cw = __ldg(&nd->child);
+            uint32_t inc = slab4(lr, nd, ltmax);
+#pragma unroll
+            for (uint32_t s = 0; s < 4; ++s)
+                if (word_of(cw, s) == kWNone) inc &= ~(1u << s);
+            if (inc) {
+                const bool right_first = (lr.neg >> ((meta.x >> 4) & 3u)) & 1u;
+                const bool swap_l = (meta.x & kW4ExpandL) && ((lr.neg >> ((meta.x >> 6) & 3u)) & 1u);
+                const bool swap_r = (meta.x & kW4ExpandR) && ((lr.neg >> ((meta.x >> 8) & 3u)) & 1u);
+                const uint32_t l = swap_l ? 0x1u : 0x4u;
+                const uint32_t r = swap_r ? 0xBu : 0xEu;
+                const uint32_t order = right_first ? (r | l << 4) : (l | r << 4);
+#pragma unroll
+                for (int j = 3; j >= 0; --j) {
+                    const uint32_t s = (order >> (2 * j)) & 3u;
+                    if (!((inc >> s) & 1u)) continue;
+                    if (next != kWNone) {
+                        if (top + 1 > cap) {
+                            atomicOr(status, NOOR_DEV_STACK_OVERFLOW);
+                            return hit;
+                        }
+                        st.base[top * st.stride] = next;
+                        ++top;
+                    }
+                    next = word_of(cw, s);
+                }
+            }
+        } else {
+            const uint32_t ni = cur & kWIndex;
+            const DevNode* nd = S.nodes + ni;
+            const uint4 lo = __ldg(&nd->lo);
+            const uint4 hi = __ldg(&nd->hi);
+            if (hi.w & NOOR_MESH_NODE_MASK) {
+                lr = wr;
+                ltmax = tmax;
+                ldeg = wdeg;
+                if (ISECT == NOOR_ISECT_WATERTIGHT) wt_setup(wt, lr.d);
+            }
+            if (slab_hit(lr, lo, hi, ltmax)) {
+                if (!(hi.w & kNodeKindMask)) {
+                    if (ldeg) {
+                        // one binary step: the far child pushed, the near one next
+                        if (top + 1 > cap) {
+                            atomicOr(status, NOOR_DEV_STACK_OVERFLOW);
+                            return hit;
+                        }
+                        const bool neg = (lr.neg >> (hi.w & NOOR_AXIS_MASK)) & 1u;
+                        st.base[top * st.stride] = kWRef | (neg ? ni + 1 : lo.w);
+                        ++top;
+                        next = kWRef | (neg ? lo.w : ni + 1);
+                    } else {
+                        next = __ldg(&S.map4[ni]);
+                        if (next == kWNone) {
+                            atomicOr(status, NOOR_DEV_BAD_INDEX);
+                            return hit;
+                        }
+                    }
+                } else if (hi.w & NOOR_LIGHT_NODE_MASK) {
+                    const uint32_t li = hi.w & NOOR_LIGHT_MASK;
+                    if ((int)li < S.num_area_lights &&
+                        shape_hit<EXT, ISECT == NOOR_ISECT_REF_WALD>(S.area_lights[li], o, d, tmax)) {
+                        hit = true;
+                        rec.ins = li;
+                        rec.mtype = NOOR_MESHLIGHT | NOOR_EMITTER;
+                    }
+                } else if (hi.w & NOOR_MESH_INSTANCE_MASK) {
+                    ins = hi.w & NOOR_TRANS_MASK;
+                    tray_to_object(lr, wr, S.xforms + ins);
+                    ltmax = tmax;
+                    ldeg = wide_degenerate(lr.o, lr.d);
+                    if (ISECT == NOOR_ISECT_WATERTIGHT) wt_setup(wt, lr.d);
+                    next = kWRef | lo.w;
+                } else if (hi.w & NOOR_MESH_LEAF_MASK) {
+                    const uint32_t cnt = hi.w & NOOR_COUNT_MASK;
+                    if (top + (int)cnt > cap + 1) {
+                        atomicOr(status, NOOR_DEV_STACK_OVERFLOW);
+                        return hit;
+                    }
+                    for (uint32_t i = 1; i < cnt; ++i) {
+                        st.base[top * st.stride] = kWRef | (ni + i);
+                        ++top;
+                    }
+                    if (cnt) next = kWRef | (ni + cnt);
+                } else {
+                    const uint32_t start = lo.w;
+                    const uint32_t end = start + (hi.w & NOOR_TRI_COUNT_MASK);
+                    bool leaf_hit = false;
+                    for (uint32_t ti = start; ti < end; ++ti) {
+                        float bu, bv;
+                        uint32_t mt;
+                        bool h;
+                        if (EXT && S.has_alpha) {
+                            float tc = ltmax;
+                            if (ISECT == NOOR_ISECT_WATERTIGHT)
+                                h = wt_test(lr, wt, S.wtri + ti, tc, bu, bv, mt);
+                            else
+                                h = wald_test(lr, S.wald + ti, tc, bu, bv, mt);
+                            if (h && (mt & NOOR_ALPHA) && alpha_cut<ISECT>(S, ti, bu, bv)) h = false;
+                            if (h) ltmax = tc;
+                        } else if (ISECT == NOOR_ISECT_WATERTIGHT) {
+                            h = wt_test(lr, wt, S.wtri + ti, ltmax, bu, bv, mt);
+                        } else {
+                            h = wald_test(lr, S.wald + ti, ltmax, bu, bv, mt);
+                        }
+                        if (h) {
+                            leaf_hit = true;
+                            rec.u = bu;
+                            rec.v = bv;
+                            rec.tri = ti;
+                            rec.mtype = mt;
+                        }
+                    }
+                    if (leaf_hit) {
+                        hit = true;
+                        tmax = ltmax;
+                        rec.ins = ins;
+                    }
+                }
+            }
+        }
+        if (next == kWNone) {
+            if (top == 0) break;
+            --top;
+            next = st.base[top * st.stride];
+        }
+    }
+    return hit;
+}
+
+// Closest hit on the four-wide tree (WIDE: the kernel is launched only for
+// scenes with S.closest4 set) or on the binary one
+template <int ISECT, bool EXT, bool WIDE>
+NB_D bool trace_primary(const DevScene& S, const float3& o, const float3& d, float& tmax, HitRec& rec,
+                        const SmemStack& st, uint32_t* status) {
+    if (WIDE) return trace_closest4<ISECT, EXT>(S, o, d, tmax, rec, st, status);
+    return trace_closest<ISECT, EXT>(S, o, d, tmax, rec, st, status);
+}
+
+// Any hit on the four-wide tree (WIDE: launched only for scenes with
+// S.nodes4 set) or on the binary one
+template <int ISECT, bool EXT, bool WIDE>
+NB_D bool trace_shadow(const DevScene& S, const float3& o, const float3& d, float tmax, const SmemStack& st,
+                       uint32_t* status) {
+    if (WIDE) return trace_any4<ISECT, EXT>(S, o, d, tmax, st, status);
+    return trace_any<ISECT, EXT>(S, o, d, tmax, st, status);
 }
 
 }  // namespace nb

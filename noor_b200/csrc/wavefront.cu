@@ -399,7 +399,7 @@ __global__ void __launch_bounds__(kScanThreads) wf_bucket_scan(WfDev W) {
     }
 }
 
-template <int ISECT, bool EXT>
+template <int ISECT, bool EXT, bool WIDE>
 NB_D void extend_one(const WfDev& W, const DevScene& S, uint32_t slot, const float4& ow,
                      const SmemStack& stk) {
     const float4 dw = W.d[slot], bw = W.beta[slot];
@@ -409,7 +409,7 @@ NB_D void extend_one(const WfDev& W, const DevScene& S, uint32_t slot, const flo
     const bool spec = (bb >> 16) & 1u;
     float tmax = kInf;
     HitRec rec{0.0f, 0.0f, 0u, 0u, 0u};
-    const bool hit = trace_closest<ISECT, EXT>(S, o, d, tmax, rec, stk, W.status);
+    const bool hit = trace_primary<ISECT, EXT, WIDE>(S, o, d, tmax, rec, stk, W.status);
     const float3 beta = f3(bw.x, bw.y, bw.z);
     if (!hit) {
         // the sky term is added by regen (converged lanes), after the
@@ -504,24 +504,24 @@ NB_D const DevScene& slot_scene(const WfDev& W, const DevScene& S1, uint32_t fra
 
 // Extend: closest hit for every active slot (one thread per slot).  EXT
 // false: no scene of the launch has sphere or disk lights
-template <int ISECT, bool MULTI, bool EXT>
+template <int ISECT, bool MULTI, bool EXT, bool WIDE>
 NB_D void extend_slot(const WfDev& W, const DevScene& S1, uint32_t slot, const SmemStack& stk) {
     const float4 ow = W.o[slot];
     const DevScene& S = slot_scene<ISECT, MULTI>(W, S1, fbits(ow.w));
     if (ISECT == kIsectMixed) {
         if (S.isect == NOOR_ISECT_WATERTIGHT)
-            extend_one<NOOR_ISECT_WATERTIGHT, EXT>(W, S, slot, ow, stk);
+            extend_one<NOOR_ISECT_WATERTIGHT, EXT, WIDE>(W, S, slot, ow, stk);
         else
-            extend_one<NOOR_ISECT_REF_WALD, EXT>(W, S, slot, ow, stk);
+            extend_one<NOOR_ISECT_REF_WALD, EXT, WIDE>(W, S, slot, ow, stk);
     } else {
-        extend_one<ISECT == kIsectMixed ? 0 : ISECT, EXT>(W, S, slot, ow, stk);
+        extend_one<ISECT == kIsectMixed ? 0 : ISECT, EXT, WIDE>(W, S, slot, ow, stk);
     }
 }
 
 // Extend.  Below sort level 2 one thread per slot; from level 2 each warp
 // takes the next 32 entries of the extension order (camera rays, then
 // secondary rays by bucket) when it is done with its last ones.
-template <int ISECT, bool MULTI, bool EXT>
+template <int ISECT, bool MULTI, bool EXT, bool WIDE>
 __global__ void __launch_bounds__(NB_TRAV_THREADS, NB_TRAV_MIN_BLOCKS) wf_extend(WfDev W, DevScene S1) {
     extern __shared__ uint32_t smem[];
     SmemStack stk{smem + threadIdx.x, (int)blockDim.x, W.stack_cap};
@@ -535,13 +535,13 @@ __global__ void __launch_bounds__(NB_TRAV_THREADS, NB_TRAV_MIN_BLOCKS) wf_extend
             if (base >= n) break;
             const uint32_t i = base + lane;
             if (i >= n) continue;
-            extend_slot<ISECT, MULTI, EXT>(W, S1, i < nc ? W.ext_perm[i] : W.ext_perm[W.cap + (i - nc)], stk);
+            extend_slot<ISECT, MULTI, EXT, WIDE>(W, S1, i < nc ? W.ext_perm[i] : W.ext_perm[W.cap + (i - nc)], stk);
         }
         return;
     }
     const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= W.cap || W.state[slot] != kActive) return;
-    extend_slot<ISECT, MULTI, EXT>(W, S1, slot, stk);
+    extend_slot<ISECT, MULTI, EXT, WIDE>(W, S1, slot, stk);
 }
 
 // Shading queues in slot order: every slot extend left a surface hit goes to
@@ -717,7 +717,7 @@ __global__ void wf_shadow_scatter(WfDev W) {
 // contribution.  Each warp takes the next 32 queue entries when it is done
 // with its last ones, so warps that drew long rays do not hold up the launch
 // with a fixed share of the queue.
-template <int ISECT, bool MULTI, bool EXT>
+template <int ISECT, bool MULTI, bool EXT, bool WIDE>
 __global__ void __launch_bounds__(NB_TRAV_THREADS, NB_TRAV_MIN_BLOCKS) wf_shadow(WfDev W, DevScene S1) {
     extern __shared__ uint32_t smem[];
     const uint32_t n = W.counters[kCntShadow];
@@ -743,11 +743,11 @@ __global__ void __launch_bounds__(NB_TRAV_THREADS, NB_TRAV_MIN_BLOCKS) wf_shadow
         bool occ;
         if (ISECT == kIsectMixed) {
             if (S.isect == NOOR_ISECT_WATERTIGHT)
-                occ = trace_any<NOOR_ISECT_WATERTIGHT, EXT>(S, o, d, so.w, stk, W.status);
+                occ = trace_shadow<NOOR_ISECT_WATERTIGHT, EXT, WIDE>(S, o, d, so.w, stk, W.status);
             else
-                occ = trace_any<NOOR_ISECT_REF_WALD, EXT>(S, o, d, so.w, stk, W.status);
+                occ = trace_shadow<NOOR_ISECT_REF_WALD, EXT, WIDE>(S, o, d, so.w, stk, W.status);
         } else {
-            occ = trace_any<ISECT == kIsectMixed ? 0 : ISECT, EXT>(S, o, d, so.w, stk, W.status);
+            occ = trace_shadow<ISECT == kIsectMixed ? 0 : ISECT, EXT, WIDE>(S, o, d, so.w, stk, W.status);
         }
         if (occ) W.pend[e].w = 0.0f;
     }
@@ -942,7 +942,7 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
     std::vector<WfFrameDev> fr(n_frames);
     unsigned long long total = 0;
     size_t film_px = 0;
-    int stack_cap = 16;
+    int stack_cap = 16, stack_words = 16;
     uint32_t max_bounces = 1;
     for (uint32_t i = 0; i < n_frames; ++i) {
         const noor_wf_frame& f = frames[i];
@@ -964,6 +964,7 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
         total += fr[i].count;
         film_px += fr[i].npix;
         stack_cap = std::max(stack_cap, C.scenes[f.scene_id]->dev.stack_cap);
+        stack_words = std::max(stack_words, C.scenes[f.scene_id]->dev.stack_words);
         max_bounces = std::max(max_bounces, fr[i].bounces);
     }
     const size_t film_bytes = film_px * 32;
@@ -1023,14 +1024,19 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
 
     WfLaunch L;
     L.block = (int)block;
-    L.smem = (size_t)stack_cap * block * 4;
+    // room for the four-wide trees' stacks as well as the binary one's
+    L.smem = (size_t)stack_words * block * 4;
     L.grid_slots = (cap + block - 1) / block;
     L.grid_queue = (uint32_t)std::max(1, C.sm_count) * 16;
     const uint32_t scene0 = frames[0].scene_id;
     bool multi = false, mixed = false;
+    // the four-wide trees where every scene of the launch has them
+    bool wide_c = true, wide_a = true;
     L.ext = L.ext_lights = L.env_ref = L.tex = L.diff = false;
     for (uint32_t i = 0; i < n_frames; ++i) {
         const DevScene& fs = C.scenes[frames[i].scene_id]->dev;
+        wide_c &= fs.closest4 != 0u;
+        wide_a &= fs.nodes4 != nullptr;
         multi |= frames[i].scene_id != scene0;
         mixed |= fs.isect != C.scenes[scene0]->dev.isect;
         L.ext |= fs.ext_lobes != 0u || fs.ext_lights != 0u || fs.env_ref != 0u || fs.has_tex != 0u;
@@ -1048,10 +1054,16 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
     W.diff = L.diff ? WS.diff : nullptr;
     L.scene = C.scenes[scene0]->dev;
     // traversal kernels: per intersector, scene source and light shapes
-#define NB_TRAV(I, M)                                                                   \
-    do {                                                                                \
-        L.extend = L.ext_lights ? wf_extend<I, M, true> : wf_extend<I, M, false>;     \
-        L.shadow = L.ext_lights ? wf_shadow<I, M, true> : wf_shadow<I, M, false>;     \
+#define NB_TRAV(I, M)                                                                                      \
+    do {                                                                                                   \
+        if (wide_c)                                                                                        \
+            L.extend = L.ext_lights ? wf_extend<I, M, true, true> : wf_extend<I, M, false, true>;          \
+        else                                                                                               \
+            L.extend = L.ext_lights ? wf_extend<I, M, true, false> : wf_extend<I, M, false, false>;        \
+        if (wide_a)                                                                                        \
+            L.shadow = L.ext_lights ? wf_shadow<I, M, true, true> : wf_shadow<I, M, false, true>;          \
+        else                                                                                               \
+            L.shadow = L.ext_lights ? wf_shadow<I, M, true, false> : wf_shadow<I, M, false, false>;        \
     } while (0)
     if (mixed) {
         NB_TRAV(kIsectMixed, true);

@@ -54,11 +54,12 @@ def _row_rays(n: int, seed: int = 0) -> np.ndarray:
 
 
 def test_traversal_stack_overflow_sets_the_status_bit():
-    """with the spec's BVH height understated the per-thread stack holds 16
-    entries while a ray along the row needs one per level (about 18): the
-    traversal stops at the cap (no write past it) and sets
-    NOOR_DEV_STACK_OVERFLOW; with the true height every ray finds the first
-    triangle of the row and the status word stays clear"""
+    """with the spec's BVH height understated the binary traversal's stack
+    (the megakernel's) holds 16 entries while a ray along the row needs one
+    per level (about 18): it stops at the cap (no write past it) and sets
+    NOOR_DEV_STACK_OVERFLOW.  The four-wide tree that ray batches and the
+    wavefront walk sizes its stack from the tree itself, so the same spec
+    leaves its hits exact and the status word clear."""
     s = _deep_row()
     built = scenes.BuiltPayload(s)
     assert built.stat.height > 18, built.stat.height
@@ -69,9 +70,12 @@ def test_traversal_stack_overflow_sets_the_status_bit():
         hits = trace_closest(rays)
         assert (hits[:, 6] == 1).all()
         assert np.allclose(hits[:, 0].view(np.float32), 1.0, atol=1e-5)
+        r.render(1)
         assert r.status() == 0
         r.update_spec(bvh_height=0)
-        trace_closest(rays)
+        assert np.array_equal(trace_closest(rays), hits)
+        assert r.status() == 0
+        r.render(1)
         assert r.status(reset=True) & _capi.NOOR_DEV_STACK_OVERFLOW
     finally:
         r.close()

@@ -105,3 +105,58 @@ def test_stack_overflow_is_reported_not_faulted(room):
     the status word stays clean for this tree"""
     r, orc = room
     assert r.status(reset=True) == 0
+
+
+def _grazing_rays(payload, n, seed, axis=True):
+    """rays from the scene's own vertex coordinates (so origins sit on box
+    planes) along directions with +0, -0 and subnormal components, finite
+    and infinite extents: the rays for which the four-wide any-hit tree
+    tests an expanded child's box as well as its children's"""
+    import ctypes as C
+    rng = np.random.default_rng(seed)
+    v = np.ctypeslib.as_array(C.cast(payload.vertices, C.POINTER(C.c_float)), (payload.num_vertices, 4))[:, :3]
+    o = v[rng.integers(0, len(v), n)].copy()
+    jitter = rng.integers(0, 3, n)
+    o[np.arange(n), jitter] += rng.normal(size=n).astype(np.float32)
+    if axis:
+        comps = np.array([0.0, -0.0, 1.0, -1.0, 1e-40, -1e-40, 0.5, -0.25], np.float32)
+        d = comps[rng.integers(0, len(comps), (n, 3))]
+        d[np.all(np.abs(d) < 1e-30, axis=1), 0] = 1.0
+    else:
+        d = rng.normal(size=(n, 3))
+        d = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
+    r = np.zeros((n, 8), np.float32)
+    r[:, :3] = o
+    r[:, 3] = np.where(rng.random(n) < 0.5, np.float32(np.inf), rng.uniform(0.1, 20.0, n).astype(np.float32))
+    r[:, 4:7] = d
+    return r
+
+
+@pytest.fixture
+def instanced():
+    import test_ref_payload as trp
+    s = trp.instanced_scene()
+    s.camera = dict(eye=(0.0, 2.0, 12.0), look_at=(0.0, 0.0, 0.0), up=(0.0, 1.0, 0.0), fov_deg=60.0, w=64, h=36)
+    s.render = dict(spp=1, bounces=4, rr=1, mis=0)
+    s.skydome_type = _capi.NOOR_SKY_CONSTANT
+    r = scenes.Renderer(s)
+    orc = Oracle(r.built.payload, r.spec, r.hosek)
+    yield r, orc
+    orc.close()
+    r.close()
+
+
+@pytest.mark.parametrize("isect", [_capi.NOOR_ISECT_REF_WALD, _capi.NOOR_ISECT_WATERTIGHT])
+@pytest.mark.parametrize("which", ["room", "spheres", "instanced"])
+def test_any_hit_on_grazing_and_random_rays(request, which, isect):
+    """shadow-ray answers (the four-wide tree) against the oracle's binary
+    traversal: rays from box planes with zero and subnormal direction
+    components, and in random directions, with short and unbounded extents"""
+    r, orc = request.getfixturevalue(which)
+    r.update_spec(intersector=isect)
+    rays = np.concatenate([_grazing_rays(r.built.payload, 100_000, 11),
+                           _grazing_rays(r.built.payload, 100_000, 12, axis=False)])
+    got, want = trace_any(rays), orc.trace_any(rays, isect)
+    assert np.array_equal(got, want), int((got != want).sum())
+    assert 0.01 < want.mean() < 0.99
+    assert r.status(reset=True) == 0
