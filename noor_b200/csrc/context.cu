@@ -430,6 +430,7 @@ int upload_scene(Context& C, const noor_payload* P, const noor_hosek_sky* H, con
     {
         std::vector<DevWaldTri> w(nt);
         std::vector<DevWtTri> t(nt);
+        uint32_t kinds = 0;
         for (size_t i = 0; i < nt; ++i) {
             std::memcpy(&w[i].ax_nu_nv_nd, P->wald_ax_nu_nv_nd + 4 * i, 16);
             std::memcpy(&w[i].cnu_cnv_deg_mat, P->wald_cnu_cnv_deg_mat + 4 * i, 16);
@@ -444,7 +445,9 @@ int upload_scene(Context& C, const noor_payload* P, const noor_hosek_sky* H, con
             uint32_t mt = P->wald_cnu_cnv_deg_mat[4 * i + 3];
             std::memcpy(&t[i].v0.w, &mt, 4);
             std::memcpy(&t[i].attr, a, 16);
+            if (!(mt & kEmitterMat)) kinds |= 1u << shade_kind(lobe_of(mt));
         }
+        D.shade_kinds = kinds;
         if ((rc = st.upload((void**)&D.wald, w.data(), nt * sizeof(DevWaldTri), "wald triangles"))) return rc;
         if ((rc = st.upload((void**)&D.wtri, t.data(), nt * sizeof(DevWtTri), "watertight triangles"))) return rc;
     }

@@ -202,6 +202,7 @@ struct DevScene {
     uint32_t has_tex;       // some material reads a texture per hit (image maps, alpha, bump)
     uint32_t has_alpha;     // some material is ALPHA: triangle tests fetch its alpha map
     uint32_t has_bump;      // some material is BUMP: rays carry differentials
+    uint32_t shade_kinds;   // bit k: some surface triangle shades in the wavefront's queue k
     // the four-wide tree of the spec's root (null: traversal walks the
     // binary tree), its map from binary inner nodes, and the stack words its
     // traversals can need; stack_words = the largest of the stacks

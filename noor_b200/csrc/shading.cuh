@@ -642,6 +642,10 @@ NB_HD uint32_t lobe_of(uint32_t mtype) {
         default: return 0u;
     }
 }
+// the wavefront's shading queue of a surface hit: Lambert, conductor, the rest
+NB_HD uint32_t shade_kind(uint32_t lobes) {
+    return lobes == kLobeLambert ? 0u : (lobes == kLobeConductor ? 1u : 2u);
+}
 // EXT false: only the three lobes a specialised kernel handles
 template <bool EXT>
 NB_D uint32_t lobe_of(uint32_t mtype) {

@@ -439,7 +439,7 @@ NB_D void extend_one(const WfDev& W, const DevScene& S, uint32_t slot, const flo
     W.hit[slot] = make_float4(tmax, rec.u, rec.v, bitsf(rec.tri));
     W.hit2[slot] = make_uint2(rec.ins, rec.mtype);
     const uint32_t lobe = lobe_of(rec.mtype);
-    const uint32_t kind = W.sort ? (lobe == kLobeLambert ? 0u : (lobe == kLobeConductor ? 1u : 2u)) : 0u;
+    const uint32_t kind = W.sort ? shade_kind(lobe) : 0u;
     W.state[slot] = kActive | ((kind + 1u) << kKindShift);  // wf_bin queues it for shading
 }
 
@@ -862,6 +862,7 @@ using WfTravKernel = void (*)(WfDev, DevScene);
 
 struct WfLaunch {
     int block;
+    uint32_t kinds;      // shading queues some scene of the launch can fill
     size_t smem;
     uint32_t grid_slots;    // one thread per slot / queue entry
     uint32_t grid_queue;    // grid-stride stages
@@ -876,6 +877,11 @@ struct WfLaunch {
     bool tex;               // ... reads textures per hit (image maps, alpha, bump)
     bool diff;              // ... has bump maps: rays carry differentials
 };
+
+// shading launches per iteration: one per queue some scene can fill
+static uint32_t shade_launches(const WfDev& W, const WfLaunch& L) {
+    return W.sort ? (uint32_t)__builtin_popcount(L.kinds & ((1u << kKinds) - 1u)) : 1u;
+}
 
 // one iteration; with `ev` (kWfStages + 1 events), records ev[0] before the
 // first stage and ev[k + 1] after stage k (regen, extension ordering,
@@ -902,6 +908,8 @@ static cudaError_t wf_iteration(const WfDev& W, const WfLaunch& L, cudaStream_t 
     wf_bin<<<(W.cap + kBinBlock - 1) / kBinBlock, kBinBlock, 0, s>>>(W);
     const int nk = W.sort ? kKinds : 1;
     for (int k = 0; k < nk; ++k) {
+        // no launch for a queue no triangle of the launch's scenes can fill
+        if (W.sort && !((L.kinds >> k) & 1u)) continue;
         // sorted queues 0 and 1 hold Lambert and conductor hits only
         if (L.diff)
             wf_shade<true, true><<<L.grid_queue, 256, 0, s>>>(W, (uint32_t)k);
@@ -1033,10 +1041,12 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
     // the four-wide trees where every scene of the launch has them
     bool wide_c = true, wide_a = true;
     L.ext = L.ext_lights = L.env_ref = L.tex = L.diff = false;
+    L.kinds = 0;
     for (uint32_t i = 0; i < n_frames; ++i) {
         const DevScene& fs = C.scenes[frames[i].scene_id]->dev;
         wide_c &= fs.closest4 != 0u;
         wide_a &= fs.nodes4 != nullptr;
+        L.kinds |= fs.shade_kinds;
         multi |= frames[i].scene_id != scene0;
         mixed |= fs.isect != C.scenes[scene0]->dev.isect;
         L.ext |= fs.ext_lobes != 0u || fs.ext_lights != 0u || fs.env_ref != 0u || fs.has_tex != 0u;
@@ -1093,7 +1103,7 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
             scene_hash = (scene_hash ^ reinterpret_cast<const unsigned char*>(&L.scene)[b]) * 1099511628211ull;
         const uint64_t key[10] = {(uint64_t)W.cap | (uint64_t)W.level << 32 | (uint64_t)L.ext << 36 |
                                       (uint64_t)L.tex << 37 | (uint64_t)L.diff << 38 | (uint64_t)L.ext_lights << 39 |
-                                      (uint64_t)L.env_ref << 40,
+                                      (uint64_t)L.env_ref << 40 | (uint64_t)L.kinds << 41,
                                   W.total,
                                   (uint64_t)W.max_iters | (uint64_t)W.nframes << 32,
                                   (uint64_t)(uint32_t)W.stack_cap | (uint64_t)L.block << 32,
@@ -1151,15 +1161,14 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
             for (auto& x : ev)
                 if (e == cudaSuccess) e = cudaEventCreate(&x);
         }
-        const uint32_t nk = (W.sort ? kKinds : 1) + (W.level >= 2 ? 3 : 0) + (W.level >= 3 ? 3 : 0);
+        const uint32_t nk = shade_launches(W, L) + (W.level >= 2 ? 3 : 0) + (W.level >= 3 ? 3 : 0);
         for (uint32_t it = 0; e == cudaSuccess && it < W.max_iters && active; ++it) {
             e = wf_iteration(W, L, s, false, WS.active_host_dev, prof ? ev : nullptr);
             if (e == cudaSuccess) e = cudaMemcpyAsync(&active, WS.active_host_dev, 4, cudaMemcpyDeviceToHost, s);
             if (e == cudaSuccess) e = cudaStreamSynchronize(s);
             C.launches += 5 + nk;
             if (prof && e == cudaSuccess) {
-                const uint32_t kinds = W.sort ? kKinds : 1u;
-                const uint32_t launches[kWfStages] = {1u, W.level >= 2 ? 3u : 0u, 1u, kinds + 1u,
+                const uint32_t launches[kWfStages] = {1u, W.level >= 2 ? 3u : 0u, 1u, shade_launches(W, L) + 1u,
                                                       W.level >= 3 ? 3u : 0u, 1u, 1u};
                 for (int k = 0; k < kWfStages; ++k) {
                     float ms = 0.0f;
@@ -1185,7 +1194,7 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
     uint32_t iters = 0;
     cudaMemcpy(&iters, W.counters + kCntIter, 4, cudaMemcpyDeviceToHost);
     if (P.use_graph)
-        C.launches += (uint64_t)iters * (5 + (W.sort ? kKinds : 1) + (W.level >= 2 ? 3 : 0) + (W.level >= 3 ? 3 : 0)) -
+        C.launches += (uint64_t)iters * (5 + shade_launches(W, L) + (W.level >= 2 ? 3 : 0) + (W.level >= 3 ? 3 : 0)) -
                       (uint64_t)W.max_iters;
     return NOOR_OK;
 }
