@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--wf-slots", type=int, default=1 << 21)
     ap.add_argument("--wf-sort", type=int, default=0)
     ap.add_argument("--wf-graph", type=int, default=1, help="wavefront: 1 CUDA-graph while loop, 0 host loop")
+    ap.add_argument("--wf-tree", type=int, default=0,
+                    help="wavefront (without autotuning): 0 auto, 1 binary tree, 2 four-wide tree")
     ap.add_argument("--workload", default="sky", choices=["sky", "room", "env", "batched", "adjoint"],
                     help="sky: the headline sky-lit scene; room: the 36-triangle room; env: the env-map MIS "
                          "scene; batched: 64 uneven frames in one wavefront launch against 64 sequential "
@@ -436,7 +438,8 @@ class WavefrontPath:
         self.host_film = torch.zeros((self.h, self.w, 4), dtype=torch.float32).pin_memory()
         self.frames = (_capi.WfFrame * 1)(scenes.wf_frame(0, s.camera, args.spp, s.render["bounces"],
                                                           d_film=self.film.data_ptr()))
-        self.params = scenes.wf_params(args.wf_block, args.wf_slots, args.wf_sort, args.wf_graph)
+        self.params = scenes.wf_params(args.wf_block, args.wf_slots, args.wf_sort, args.wf_graph,
+                                       traversal=args.wf_tree)
         self.tuned_ms = None
 
     def warm(self):
@@ -470,7 +473,8 @@ class WavefrontPath:
         p = self.params
         return {"entry_point": "noor_wavefront_render",
                 "wavefront": {"block": p.block_size, "slots": p.queue_capacity, "material_sort": p.sort_granularity,
-                              "graph": p.use_graph, "autotune_best_ms": self.tuned_ms}}
+                              "graph": p.use_graph, "tree": ["auto", "binary", "four-wide"][p.traversal],
+                              "autotune_best_ms": self.tuned_ms}}
 
     def image(self):
         import torch

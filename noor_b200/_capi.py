@@ -57,6 +57,7 @@ MESH_LEAF_MASK = 0x40000000
 MESH_INSTANCE_MASK = 0x20000000
 MESH_INNER_MASK = 0x10000000
 LIGHT_NODE_MASK = 0x08000000
+NOOR_TRAVERSAL_AUTO, NOOR_TRAVERSAL_BINARY, NOOR_TRAVERSAL_WIDE = 0, 1, 2
 
 
 class Shape(C.Structure):
@@ -192,7 +193,7 @@ class WfFrame(C.Structure):
 
 class WfParams(C.Structure):
     _fields_ = [("block_size", u32), ("queue_capacity", u32), ("sort_granularity", u32), ("use_graph", u32),
-                ("max_iterations", u32)]
+                ("max_iterations", u32), ("traversal", u32)]
 
 
 class WfProfile(C.Structure):

@@ -878,6 +878,11 @@ struct WfLaunch {
     bool diff;              // ... has bump maps: rays carry differentials
 };
 
+// NOOR_TRAVERSAL_AUTO takes the four-wide tree for scenes of at least this
+// many triangles (on the 36-triangle room the binary tree's single-box
+// visits are cheaper; on the 2.6M-triangle sky scene the wide tree wins)
+constexpr uint32_t kWideAutoTris = 16384;
+
 // shading launches per iteration: one per queue some scene can fill
 static uint32_t shade_launches(const WfDev& W, const WfLaunch& L) {
     return W.sort ? (uint32_t)__builtin_popcount(L.kinds & ((1u << kKinds) - 1u)) : 1u;
@@ -1038,14 +1043,17 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
     L.grid_queue = (uint32_t)std::max(1, C.sm_count) * 16;
     const uint32_t scene0 = frames[0].scene_id;
     bool multi = false, mixed = false;
-    // the four-wide trees where every scene of the launch has them
-    bool wide_c = true, wide_a = true;
+    // the four-wide trees where every scene of the launch has them (and,
+    // for NOOR_TRAVERSAL_AUTO, is large enough for them to pay)
+    if (P.traversal > NOOR_TRAVERSAL_WIDE) return set_error(NOOR_ERR_INVALID, "wavefront: bad traversal selector");
+    bool wide_c = P.traversal != NOOR_TRAVERSAL_BINARY, wide_a = wide_c;
     L.ext = L.ext_lights = L.env_ref = L.tex = L.diff = false;
     L.kinds = 0;
     for (uint32_t i = 0; i < n_frames; ++i) {
         const DevScene& fs = C.scenes[frames[i].scene_id]->dev;
-        wide_c &= fs.closest4 != 0u;
-        wide_a &= fs.nodes4 != nullptr;
+        const bool big = P.traversal == NOOR_TRAVERSAL_WIDE || fs.num_tris >= kWideAutoTris;
+        wide_c &= fs.closest4 != 0u && big;
+        wide_a &= fs.nodes4 != nullptr && big;
         L.kinds |= fs.shade_kinds;
         multi |= frames[i].scene_id != scene0;
         mixed |= fs.isect != C.scenes[scene0]->dev.isect;
@@ -1253,8 +1261,9 @@ extern "C" int noor_wavefront_counters(uint64_t counters[3], int reset) {
 // Autotuner: coordinate descent on the launch parameters, each candidate
 // timed by one device-timed render of the batch: the slot count first
 // (2^18 .. 2^23, none beyond twice the batch's paths), then the block size
-// (32, 64, 128), then the sort granularity (0 .. 3), then the slot count
-// again around the sort level chosen; the fastest seen wins.
+// (32, 64, 128), then the sort granularity (0 .. 3), then the tree (binary,
+// four-wide), then the slot count again around the choices made; the
+// fastest seen wins.
 extern "C" int noor_wavefront_autotune(const noor_wf_frame* frames, uint32_t n_frames, noor_wf_params* best,
                                        float* best_ms) {
     Context* C;
@@ -1293,6 +1302,11 @@ extern "C" int noor_wavefront_autotune(const noor_wf_frame* frames, uint32_t n_f
         noor_wf_params p = bp;
         p.sort_granularity = so;
         if (so != bp.sort_granularity && (rc = trial(p))) return rc;
+    }
+    for (uint32_t tv : {(uint32_t)NOOR_TRAVERSAL_BINARY, (uint32_t)NOOR_TRAVERSAL_WIDE}) {
+        noor_wf_params p = bp;
+        p.traversal = tv;
+        if ((rc = trial(p))) return rc;
     }
     const uint32_t c0 = bp.queue_capacity;
     for (uint32_t c : caps) {

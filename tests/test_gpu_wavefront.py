@@ -112,3 +112,34 @@ def test_autotune_picks_a_candidate(room):
     fr = (_capi.WfFrame * 1)(scenes.wf_frame(0, s.camera, 4, bounces=5, d_film=a.data_ptr()))
     _capi.call("noor_wavefront_autotune", fr, 1, C.byref(best), C.byref(ms))
     assert best.block_size in (64, 128) and best.queue_capacity >= 1 << 18 and ms.value > 0
+
+
+@pytest.mark.parametrize("which", ["room", "sky"])
+def test_wavefront_trees_trace_the_same_paths(which):
+    """the extension and shadow stages on the binary tree and on the
+    four-wide tree: the same hits, so the same rays traced (counted) and the
+    same image up to the film's atomic summation order"""
+    if which == "room":
+        s = scenes.room_scene(width=96, height=96, spp=16)
+    else:
+        s = scenes.sky_scene(width=96, height=64, count=8, level=4)
+    r = scenes.Renderer(s)
+    try:
+        w, h = s.camera["w"], s.camera["h"]
+        out, rays = [], []
+        for tree in (_capi.NOOR_TRAVERSAL_BINARY, _capi.NOOR_TRAVERSAL_WIDE):
+            f = film(w, h)
+            fr = scenes.wf_frame(0, s.camera, 16, bounces=5, d_film=f.data_ptr())
+            c = (C.c_uint64 * 3)()
+            _capi.call("noor_wavefront_counters", c, 1)
+            run_wf([fr], scenes.wf_params(128, 1 << 16, 1, 1, traversal=tree))
+            _capi.call("noor_wavefront_counters", c, 1)
+            torch.cuda.synchronize()
+            out.append(f.cpu().numpy()[..., :3])
+            rays.append(tuple(int(x) for x in c))
+        assert rays[0] == rays[1] and rays[0][0] > 0, rays
+        rel = np.abs(out[0] - out[1]) / np.maximum(np.abs(out[1]), 1e-2)
+        assert rel.max() < 1e-5, float(rel.max())
+        assert r.status(reset=True) == 0
+    finally:
+        r.close()
