@@ -627,12 +627,12 @@ void noor_free_payload(noor_payload_handle* h);
 /* The four-wide tree that scene upload builds over the payload's BVH from
  * `root` (host only, no device needed): the number of wide nodes, of binary
  * inner nodes whose children a wide node holds in its own slots, the stack
- * words its any-hit and closest-hit traversals can need, and whether closest
- * hit uses it (*closest = 1).  NOOR_ERR_UNSUPPORTED (with the reason) for a
- * tree upload leaves to the binary traversal: a cycle, a NaN bound, or an
- * any-hit stack deeper than 96 words. */
+ * words its traversals can need, and whether closest hit uses it
+ * (*closest = 1).  NOOR_ERR_UNSUPPORTED (with the reason) for a tree upload
+ * leaves to the binary traversal: a cycle, a NaN bound, or a stack deeper
+ * than 96 words. */
 int noor_wide_tree_info(const noor_payload* payload, uint32_t root, uint32_t* num_wide,
-                        uint32_t* num_expanded, uint32_t stack_need[2], uint32_t* closest);
+                        uint32_t* num_expanded, uint32_t* stack_need, uint32_t* closest);
 
 /* Camera::reset + CudaCamera::update for a pinhole perspective camera
  * (noor/header/camera.h:99-153,255-300; noor/cuda/camera.cuh:66-94).

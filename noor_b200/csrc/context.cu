@@ -263,8 +263,7 @@ void apply_spec(SceneState& st, const noor_spec& s) {
     D.map4 = wide ? st.wide_map : nullptr;
     D.stack_cap4 = wide ? st.wide_cap : 0;
     D.closest4 = wide && st.wide_closest ? 1u : 0u;
-    D.stack_cap4c = D.closest4 ? st.wide_cap_closest : 0;
-    D.stack_words = std::max(D.stack_cap, std::max(D.stack_cap4, D.stack_cap4c));
+    D.stack_words = std::max(D.stack_cap, D.stack_cap4);
 }
 
 void apply_hosek(SceneState& st, const noor_hosek_sky& h) {
@@ -422,7 +421,6 @@ int upload_scene(Context& C, const noor_payload* P, const noor_hosek_sky* H, con
                 return rc;
             st.wide_root = wt.root;
             st.wide_cap = wt.stack_need;
-            st.wide_cap_closest = wt.stack_need_closest;
             st.wide_closest = wt.closest;
         }
 #endif

@@ -23,7 +23,6 @@ struct SceneState {
     const uint32_t* wide_map = nullptr;
     uint32_t wide_root = 0;
     int wide_cap = 0;
-    int wide_cap_closest = 0;
     bool wide_closest = false;
     // NOOR_ENV_REFERENCE, built on first use: the environment (or baked sky)
     // as a CUDA array + texture object, the bake buffer and the tables

@@ -209,7 +209,6 @@ struct DevScene {
     const DevNode4* nodes4;
     const uint32_t* map4;
     int stack_cap4;
-    int stack_cap4c;        // closest hit over the four-wide tree (closest4)
     uint32_t closest4;      // closest hit may use the four-wide tree
     int stack_words;
     // NOOR_ENV_REFERENCE: the reference's distribution tables (row r at

@@ -477,10 +477,11 @@ NB_D bool trace_any(const DevScene& S, const float3& o, const float3& d, float t
     return false;
 }
 
-// A ray the four-wide tree may not skip an expanded child's box for: a
-// direction component that is zero, subnormal or NaN (its slab reciprocal is
-// infinite, and the per-axis intervals stop being monotone in the box), or
-// an origin that is not finite.
+// A ray below which the four-wide tree's boxes may not stand in for the
+// binary tree's: a direction component that is zero, subnormal or NaN (its
+// slab reciprocal is infinite, and the per-axis intervals stop being
+// monotone in the box), or an origin that is not finite.  Such rays walk the
+// binary tree node by node.
 NB_D bool wide_degenerate(const float3& o, const float3& d) {
     const float m = 1.17549435e-38f;  // FLT_MIN
     return !(fabsf(d.x) >= m && fabsf(d.y) >= m && fabsf(d.z) >= m && fabsf(o.x) <= 3.40282347e38f &&
@@ -491,39 +492,41 @@ NB_D uint32_t word_of(const uint4& v, uint32_t s) { return s == 0 ? v.x : (s == 
 NB_D float comp4(const float4& v, uint32_t s) { return s == 0 ? v.x : (s == 1 ? v.y : (s == 2 ? v.z : v.w)); }
 
 // The slab test of noor/cuda/bbox.cuh:62-80 on a wide node's four entry
-// boxes at once, axis by axis (the same operations and comparisons as
-// slab_hit_f for each box); bit s set when box s passes.
+// boxes at once, axis by axis: the same operations and comparisons as
+// slab_hit_f for each box, the near and far bounds of an axis picked by
+// address (the ray's sign) instead of per box.  Bit s set when box s passes.
 NB_D uint32_t slab4(const TRay& r, const DevNode4* nd, float tmax) {
+    const float4* b = &nd->lox;  // lox, loy, loz, hix, hiy, hiz
     float t0[4], t1[4];
     uint32_t ok = 0xFu;
     {
-        const float4 a = __ldg(&nd->lox), b = __ldg(&nd->hix);
-        const bool n = r.neg & 1u;
+        const uint32_t n = (r.neg & 1u) ? 3u : 0u;
+        const float4 a = __ldg(b + n), c = __ldg(b + (3u - n));
 #pragma unroll
         for (uint32_t s = 0; s < 4; ++s) {
-            t0[s] = xmul(xsub(n ? comp4(b, s) : comp4(a, s), r.o.x), r.inv.x);
-            t1[s] = xmul(xsub(n ? comp4(a, s) : comp4(b, s), r.o.x), r.inv.x);
+            t0[s] = xmul(xsub(comp4(a, s), r.o.x), r.inv.x);
+            t1[s] = xmul(xsub(comp4(c, s), r.o.x), r.inv.x);
         }
     }
     {
-        const float4 a = __ldg(&nd->loy), b = __ldg(&nd->hiy);
-        const bool n = r.neg & 2u;
+        const uint32_t n = (r.neg & 2u) ? 3u : 0u;
+        const float4 a = __ldg(b + 1 + n), c = __ldg(b + 1 + (3u - n));
 #pragma unroll
         for (uint32_t s = 0; s < 4; ++s) {
-            const float u0 = xmul(xsub(n ? comp4(b, s) : comp4(a, s), r.o.y), r.inv.y);
-            const float u1 = xmul(xsub(n ? comp4(a, s) : comp4(b, s), r.o.y), r.inv.y);
+            const float u0 = xmul(xsub(comp4(a, s), r.o.y), r.inv.y);
+            const float u1 = xmul(xsub(comp4(c, s), r.o.y), r.inv.y);
             if (t0[s] > u1 || u0 > t1[s]) ok &= ~(1u << s);
             if (u0 > t0[s]) t0[s] = u0;
             if (u1 < t1[s]) t1[s] = u1;
         }
     }
     {
-        const float4 a = __ldg(&nd->loz), b = __ldg(&nd->hiz);
-        const bool n = r.neg & 4u;
+        const uint32_t n = (r.neg & 4u) ? 3u : 0u;
+        const float4 a = __ldg(b + 2 + n), c = __ldg(b + 2 + (3u - n));
 #pragma unroll
         for (uint32_t s = 0; s < 4; ++s) {
-            const float u0 = xmul(xsub(n ? comp4(b, s) : comp4(a, s), r.o.z), r.inv.z);
-            const float u1 = xmul(xsub(n ? comp4(a, s) : comp4(b, s), r.o.z), r.inv.z);
+            const float u0 = xmul(xsub(comp4(a, s), r.o.z), r.inv.z);
+            const float u1 = xmul(xsub(comp4(c, s), r.o.z), r.inv.z);
             if (t0[s] > u1 || u0 > t1[s]) ok &= ~(1u << s);
             if (u0 > t0[s]) t0[s] = u0;
             if (u1 < t1[s]) t1[s] = u1;
@@ -535,14 +538,72 @@ NB_D uint32_t slab4(const TRay& r, const DevNode4* nd, float tmax) {
     return ok;
 }
 
+// A wide node's visit: its entries that pass the slab test (and its
+// deferred ones) in the binary traversal's order for the ray's octant (the
+// node's order table), the first into `next`, the rest pushed so that they
+// come off the stack in order.  False on a stack overflow.
+NB_D bool wide_visit(const DevNode4* nd, const uint4& meta, const TRay& r, float tmax, const SmemStack& st, int cap,
+                     int& top, uint32_t& next, uint32_t* status) {
+    const uint4 cw = __ldg(&nd->child);
+    uint32_t inc = slab4(r, nd, tmax);
+#pragma unroll
+    for (uint32_t s = 0; s < 4; ++s) {
+        const uint32_t w = word_of(cw, s);
+        if (w == kWNone) inc &= ~(1u << s);
+        else if ((w & (kWRef | kWUntested)) == (kWRef | kWUntested)) inc |= 1u << s;
+    }
+    if (!inc) return true;
+    const uint32_t oct = r.neg & 7u;
+    const uint32_t order = ((oct & 4u) ? meta.z : meta.y) >> (8u * (oct & 3u));
+    // last in order first: each taken word pushes the one held before it
+#pragma unroll
+    for (int j = 3; j >= 0; --j) {
+        const uint32_t s = (order >> (2 * j)) & 3u;
+        if (!((inc >> s) & 1u)) continue;
+        if (next != kWNone) {
+            if (top + 1 > cap) {
+                atomicOr(status, NOOR_DEV_STACK_OVERFLOW);
+                return false;
+            }
+            st.base[top * st.stride] = next;
+            ++top;
+        }
+        next = word_of(cw, s);
+    }
+    return true;
+}
+
+// An inner node taken from the stack or a ref once its box passed: its wide
+// node, or for a ray below which boxes may not be skipped one binary step
+// (the far child pushed, the near one next, as trace_closest takes them).
+// False on a stack overflow or a missing wide node.
+NB_D bool inner_step(const DevScene& S, uint32_t ni, const uint4& lo, const uint4& hi, const TRay& r, bool deg,
+                     const SmemStack& st, int cap, int& top, uint32_t& next, uint32_t* status) {
+    if (deg) {
+        if (top + 1 > cap) {
+            atomicOr(status, NOOR_DEV_STACK_OVERFLOW);
+            return false;
+        }
+        const bool neg = (r.neg >> (hi.w & NOOR_AXIS_MASK)) & 1u;
+        st.base[top * st.stride] = kWRef | kWUntested | (neg ? ni + 1 : lo.w);
+        ++top;
+        next = kWRef | kWUntested | (neg ? lo.w : ni + 1);
+        return true;
+    }
+    next = __ldg(&S.map4[ni]);
+    if (next == kWNone) {
+        atomicOr(status, NOOR_DEV_BAD_INDEX);
+        return false;
+    }
+    return true;
+}
+
 // Any hit over the four-wide tree (S.nodes4, layout in wide_bvh.h): the same
-// occluders, found in the same order, as trace_any on the binary tree.  A
-// wide node's entries are tested together; those that pass are taken in the
-// binary traversal's order (the near side of P's split axis first, then the
-// near side of each expanded child's), the first at once and the rest
-// pushed.  Binary nodes (leaves, mesh leaves, instances, light nodes and
-// deferred entries) are taken as the binary traversal takes them.  The stack
-// holds S.stack_cap4 words, the deepest this tree can need.
+// answer as trace_any on the binary tree.  Binary nodes (leaves, mesh
+// leaves, instances, light nodes and deferred entries) are taken as the
+// binary traversal takes them; a ref carries kWUntested when its box has not
+// been tested yet.  The stack holds S.stack_cap4 words, the deepest this
+// tree can need.
 template <int ISECT, bool EXT = true>
 NB_D bool trace_any4(const DevScene& S, const float3& o, const float3& d, float tmax, const SmemStack& st,
                      uint32_t* status) {
@@ -567,48 +628,7 @@ NB_D bool trace_any4(const DevScene& S, const float3& o, const float3& d, float 
                 ldeg = wdeg;
                 if (ISECT == NOOR_ISECT_WATERTIGHT) wt_setup(wt, lr.d);
             }
-            const uint4 cw = __ldg(&nd->child);
-            uint32_t inc = slab4(lr, nd, tmax);
-#pragma unroll
-            for (uint32_t s = 0; s < 4; ++s) {
-                const uint32_t w = word_of(cw, s);
-                if (w == kWNone) inc &= ~(1u << s);
-                else if ((w & (kWRef | kWUntested)) == (kWRef | kWUntested)) inc |= 1u << s;
-            }
-            if (ldeg) {
-                // the expanded children's own boxes, as the binary traversal tests them
-                if ((inc & 3u) && (meta.x & kW4ExpandL)) {
-                    const DevNode* c = S.nodes + meta.y;
-                    if (!slab_hit(lr, __ldg(&c->lo), __ldg(&c->hi), tmax)) inc &= ~3u;
-                }
-                if ((inc & 12u) && (meta.x & kW4ExpandR)) {
-                    const DevNode* c = S.nodes + meta.z;
-                    if (!slab_hit(lr, __ldg(&c->lo), __ldg(&c->hi), tmax)) inc &= ~12u;
-                }
-            }
-            if (inc) {
-                const bool right_first = (lr.neg >> ((meta.x >> 4) & 3u)) & 1u;
-                const bool swap_l = (meta.x & kW4ExpandL) && ((lr.neg >> ((meta.x >> 6) & 3u)) & 1u);
-                const bool swap_r = (meta.x & kW4ExpandR) && ((lr.neg >> ((meta.x >> 8) & 3u)) & 1u);
-                const uint32_t l = swap_l ? 0x1u : 0x4u;   // slots (0,1) or (1,0), two bits each
-                const uint32_t r = swap_r ? 0xBu : 0xEu;   // slots (2,3) or (3,2)
-                const uint32_t order = right_first ? (r | l << 4) : (l | r << 4);
-                // last in order first: each taken word pushes the one held before it
-#pragma unroll
-                for (int j = 3; j >= 0; --j) {
-                    const uint32_t s = (order >> (2 * j)) & 3u;
-                    if (!((inc >> s) & 1u)) continue;
-                    if (next != kWNone) {
-                        if (top + 1 > cap) {
-                            atomicOr(status, NOOR_DEV_STACK_OVERFLOW);
-                            return false;
-                        }
-                        st.base[top * st.stride] = next;
-                        ++top;
-                    }
-                    next = word_of(cw, s);
-                }
-            }
+            if (!wide_visit(nd, meta, lr, tmax, st, cap, top, next, status)) return false;
         } else {
             const uint32_t ni = cur & kWIndex;
             const DevNode* nd = S.nodes + ni;
@@ -621,11 +641,7 @@ NB_D bool trace_any4(const DevScene& S, const float3& o, const float3& d, float 
             }
             if (!(cur & kWUntested) || slab_hit(lr, lo, hi, tmax)) {
                 if (!(hi.w & kNodeKindMask)) {
-                    next = __ldg(&S.map4[ni]);
-                    if (next == kWNone) {
-                        atomicOr(status, NOOR_DEV_BAD_INDEX);
-                        return false;
-                    }
+                    if (!inner_step(S, ni, lo, hi, lr, ldeg, st, cap, top, next, status)) return false;
                 } else if (hi.w & NOOR_LIGHT_NODE_MASK) {
                     const uint32_t li = hi.w & NOOR_LIGHT_MASK;
                     float tm = tmax;
@@ -680,9 +696,7 @@ NB_D bool trace_any4(const DevScene& S, const float3& o, const float3& d, float 
 // is taken, against the hit distance of that moment, as the binary traversal
 // tests it; a wide node's tests only skip entries that the binary traversal
 // would find missed later (its hit distance only shrinks, and a box inside a
-// missed box is missed).  Below a ray whose boxes may not be skipped
-// (wide_degenerate) inner nodes are walked one by one, as trace_closest walks
-// them.  The stack holds S.stack_cap4c words, the deepest this tree needs.
+// missed box is missed).  The stack holds S.stack_cap4 words.
 template <int ISECT, bool EXT = true>
 NB_D bool trace_closest4(const DevScene& S, const float3& o, const float3& d, float& tmax, HitRec& rec,
                          const SmemStack& st, uint32_t* status) {
@@ -696,7 +710,7 @@ NB_D bool trace_closest4(const DevScene& S, const float3& o, const float3& d, fl
     float ltmax = tmax;
     uint32_t ins = 0;
     bool hit = false;
-    const int cap = S.stack_cap4c;
+    const int cap = S.stack_cap4;
     int top = 0;
     uint32_t next = kWRef | S.root;
     for (;;) {
@@ -711,33 +725,7 @@ NB_D bool trace_closest4(const DevScene& S, const float3& o, const float3& d, fl
                 ldeg = wdeg;
                 if (ISECT == NOOR_ISECT_WATERTIGHT) wt_setup(wt, lr.d);
             }
-            const uint4 cw = __ldg(&nd->child);
-            uint32_t inc = slab4(lr, nd, ltmax);
-#pragma unroll
-            for (uint32_t s = 0; s < 4; ++s)
-                if (word_of(cw, s) == kWNone) inc &= ~(1u << s);
-            if (inc) {
-                const bool right_first = (lr.neg >> ((meta.x >> 4) & 3u)) & 1u;
-                const bool swap_l = (meta.x & kW4ExpandL) && ((lr.neg >> ((meta.x >> 6) & 3u)) & 1u);
-                const bool swap_r = (meta.x & kW4ExpandR) && ((lr.neg >> ((meta.x >> 8) & 3u)) & 1u);
-                const uint32_t l = swap_l ? 0x1u : 0x4u;
-                const uint32_t r = swap_r ? 0xBu : 0xEu;
-                const uint32_t order = right_first ? (r | l << 4) : (l | r << 4);
-#pragma unroll
-                for (int j = 3; j >= 0; --j) {
-                    const uint32_t s = (order >> (2 * j)) & 3u;
-                    if (!((inc >> s) & 1u)) continue;
-                    if (next != kWNone) {
-                        if (top + 1 > cap) {
-                            atomicOr(status, NOOR_DEV_STACK_OVERFLOW);
-                            return hit;
-                        }
-                        st.base[top * st.stride] = next;
-                        ++top;
-                    }
-                    next = word_of(cw, s);
-                }
-            }
+            if (!wide_visit(nd, meta, lr, ltmax, st, cap, top, next, status)) return hit;
         } else {
             const uint32_t ni = cur & kWIndex;
             const DevNode* nd = S.nodes + ni;
@@ -751,23 +739,7 @@ NB_D bool trace_closest4(const DevScene& S, const float3& o, const float3& d, fl
             }
             if (slab_hit(lr, lo, hi, ltmax)) {
                 if (!(hi.w & kNodeKindMask)) {
-                    if (ldeg) {
-                        // one binary step: the far child pushed, the near one next
-                        if (top + 1 > cap) {
-                            atomicOr(status, NOOR_DEV_STACK_OVERFLOW);
-                            return hit;
-                        }
-                        const bool neg = (lr.neg >> (hi.w & NOOR_AXIS_MASK)) & 1u;
-                        st.base[top * st.stride] = kWRef | (neg ? ni + 1 : lo.w);
-                        ++top;
-                        next = kWRef | (neg ? lo.w : ni + 1);
-                    } else {
-                        next = __ldg(&S.map4[ni]);
-                        if (next == kWNone) {
-                            atomicOr(status, NOOR_DEV_BAD_INDEX);
-                            return hit;
-                        }
-                    }
+                    if (!inner_step(S, ni, lo, hi, lr, ldeg, st, cap, top, next, status)) return hit;
                 } else if (hi.w & NOOR_LIGHT_NODE_MASK) {
                     const uint32_t li = hi.w & NOOR_LIGHT_MASK;
                     if ((int)li < S.num_area_lights &&

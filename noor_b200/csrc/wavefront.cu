@@ -142,6 +142,10 @@ struct WfDev {
 #ifndef NB_TRAV_MIN_BLOCKS
 #define NB_TRAV_MIN_BLOCKS 9
 #endif
+// the same for the kernels on the four-wide tree
+#ifndef NB_TRAV_MIN_BLOCKS_WIDE
+#define NB_TRAV_MIN_BLOCKS_WIDE 9
+#endif
 // minimum resident 256-thread blocks per SM of the shading stage: 3 caps
 // its registers at 85 (24 warps per SM instead of 16 at its natural 128)
 #ifndef NB_SHADE_MIN_BLOCKS
@@ -522,7 +526,7 @@ NB_D void extend_slot(const WfDev& W, const DevScene& S1, uint32_t slot, const S
 // takes the next 32 entries of the extension order (camera rays, then
 // secondary rays by bucket) when it is done with its last ones.
 template <int ISECT, bool MULTI, bool EXT, bool WIDE>
-__global__ void __launch_bounds__(NB_TRAV_THREADS, NB_TRAV_MIN_BLOCKS) wf_extend(WfDev W, DevScene S1) {
+__global__ void __launch_bounds__(NB_TRAV_THREADS, WIDE ? NB_TRAV_MIN_BLOCKS_WIDE : NB_TRAV_MIN_BLOCKS) wf_extend(WfDev W, DevScene S1) {
     extern __shared__ uint32_t smem[];
     SmemStack stk{smem + threadIdx.x, (int)blockDim.x, W.stack_cap};
     if (W.level >= 2) {
@@ -718,7 +722,7 @@ __global__ void wf_shadow_scatter(WfDev W) {
 // with its last ones, so warps that drew long rays do not hold up the launch
 // with a fixed share of the queue.
 template <int ISECT, bool MULTI, bool EXT, bool WIDE>
-__global__ void __launch_bounds__(NB_TRAV_THREADS, NB_TRAV_MIN_BLOCKS) wf_shadow(WfDev W, DevScene S1) {
+__global__ void __launch_bounds__(NB_TRAV_THREADS, WIDE ? NB_TRAV_MIN_BLOCKS_WIDE : NB_TRAV_MIN_BLOCKS) wf_shadow(WfDev W, DevScene S1) {
     extern __shared__ uint32_t smem[];
     const uint32_t n = W.counters[kCntShadow];
     SmemStack stk{smem + threadIdx.x, (int)blockDim.x, W.stack_cap};

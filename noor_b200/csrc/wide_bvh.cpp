@@ -184,23 +184,35 @@ bool build_wide_tree(const uint32_t* nodes8, size_t nn, uint32_t root, int max_s
             }
         }
         h.meta[0] = flags;
-        h.meta[1] = cs[0];
-        h.meta[2] = cs[1];
+        // the visiting order of the four slots for each ray octant (bit a of
+        // the octant: direction component a <= 0): the near side of P's split
+        // axis first, within it the near side of an expanded child's; two
+        // bits per slot, first visited lowest, one byte per octant
+        for (uint32_t o = 0; o < 8; ++o) {
+            const bool right_first = (o >> T.axis(P)) & 1u;
+            const uint32_t ax_l = (flags >> 6) & 3u, ax_r = (flags >> 8) & 3u;
+            const bool swap_l = (flags & kW4ExpandL) && ((o >> ax_l) & 1u);
+            const bool swap_r = (flags & kW4ExpandR) && ((o >> ax_r) & 1u);
+            const uint32_t l = swap_l ? 0x1u : 0x4u;  // slots (1,0) or (0,1)
+            const uint32_t r = swap_r ? 0xBu : 0xEu;  // slots (3,2) or (2,3)
+            const uint32_t order = right_first ? (r | l << 4) : (l | r << 4);
+            h.meta[1 + o / 4] |= order << (8 * (o % 4));
+        }
         out.nodes[out.map[P]] = h;
     }
 
-    // deepest stacks.  Any hit: a wide node with k entries pushes k - 1 of
-    // them before taking the first, a mesh leaf of n members pushes n - 1.
-    // Closest hit also walks inner nodes one by one (one push each) below a
-    // ray that may not skip boxes, so it takes the larger of the two counts.
-    std::vector<int> need(nn, 0), needc(nn, 0);
+    // deepest stack: a wide node with k entries pushes k - 1 of them before
+    // taking the first, a mesh leaf of n members pushes n - 1, and below a
+    // ray that may not skip boxes inner nodes are walked one by one (one push
+    // each); the larger of the two counts
+    std::vector<int> need(nn, 0);
     for (uint32_t n : post) {
-        int v = 0, vc = 0;
+        int v = 0;
         switch (T.kind(n)) {
             case kInner:
                 if (out.map[n] != kWNone) {
                     const WideNodeHost& h = out.nodes[out.map[n]];
-                    int k = 0, m = 0, mc = 0;
+                    int k = 0, m = 0;
                     for (int s = 0; s < 4; ++s) {
                         if (h.child[s] == kWNone) continue;
                         ++k;
@@ -208,46 +220,35 @@ bool build_wide_tree(const uint32_t* nodes8, size_t nn, uint32_t root, int max_s
                         // left or right child, or one of their children)
                         uint32_t bx = (h.child[s] & kWRef) ? (h.child[s] & kWIndex) : kWNone;
                         if (bx == kWNone) {
-                            const uint32_t C = s < 2 ? h.meta[1] : h.meta[2];
+                            const uint32_t C = s < 2 ? n + 1 : T.w0(n);
                             const bool ex = (h.meta[0] & (s < 2 ? kW4ExpandL : kW4ExpandR)) != 0u;
                             bx = !ex ? C : ((s & 1) ? T.w0(C) : C + 1);
                         }
                         m = std::max(m, need[bx]);
-                        mc = std::max(mc, needc[bx]);
                     }
                     v = (k > 0 ? k - 1 : 0) + m;
-                    vc = (k > 0 ? k - 1 : 0) + mc;
                 }
-                vc = std::max(vc, 1 + std::max(needc[n + 1], needc[T.w0(n)]));
+                v = std::max(v, 1 + std::max(need[n + 1], need[T.w0(n)]));
                 break;
             case kMeshLeaf: {
                 const uint32_t cnt = T.count(n);
-                int m = 0, mc = 0;
-                for (uint32_t i = 1; i <= cnt; ++i) {
-                    m = std::max(m, need[n + i]);
-                    mc = std::max(mc, needc[n + i]);
-                }
+                int m = 0;
+                for (uint32_t i = 1; i <= cnt; ++i) m = std::max(m, need[n + i]);
                 v = cnt ? (int)cnt - 1 + m : 0;
-                vc = cnt ? (int)cnt - 1 + mc : 0;
                 break;
             }
-            case kInstance:
-                v = need[T.w0(n)];
-                vc = needc[T.w0(n)];
-                break;
+            case kInstance: v = need[T.w0(n)]; break;
             default: break;
         }
         need[n] = v;
-        needc[n] = vc;
     }
     out.stack_need = need[root];
-    out.stack_need_closest = needc[root];
     out.root = root;
     if (out.stack_need > max_stack) return fail("the four-wide traversal needs a deeper stack than allowed");
-    // closest hit re-tests every leaf when it is taken and relies on each
-    // entry box being tested against the ray of its parent's visit: no
-    // deferred entries, and a stack within the limit
-    out.closest = !deferred && out.stack_need_closest <= max_stack;
+    // closest hit re-tests every binary node when it is taken and relies on
+    // each entry box being tested against the ray of its parent's visit: no
+    // deferred entries
+    out.closest = !deferred;
     return true;
 }
 
@@ -256,7 +257,7 @@ bool build_wide_tree(const uint32_t* nodes8, size_t nn, uint32_t root, int max_s
 #include "host_common.h"
 
 extern "C" int noor_wide_tree_info(const noor_payload* payload, uint32_t root, uint32_t* num_wide,
-                                   uint32_t* num_expanded, uint32_t stack_need[2], uint32_t* closest) {
+                                   uint32_t* num_expanded, uint32_t* stack_need, uint32_t* closest) {
     if (!payload || !payload->bvh_min_right_start || !payload->bvh_max_axis_count || !num_wide || !num_expanded ||
         !stack_need || !closest || root >= payload->num_bvh_nodes)
         return set_error(NOOR_ERR_INVALID, "noor_wide_tree_info: bad argument");
@@ -275,8 +276,7 @@ extern "C" int noor_wide_tree_info(const noor_payload* payload, uint32_t root, u
         ex += ((h.meta[0] & nb::kW4ExpandL) ? 1u : 0u) + ((h.meta[0] & nb::kW4ExpandR) ? 1u : 0u);
     *num_wide = (uint32_t)t.nodes.size();
     *num_expanded = ex;
-    stack_need[0] = (uint32_t)t.stack_need;
-    stack_need[1] = (uint32_t)t.stack_need_closest;
+    *stack_need = (uint32_t)t.stack_need;
     *closest = t.closest ? 1u : 0u;
     clear_error();
     return NOOR_OK;

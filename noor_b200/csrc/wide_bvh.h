@@ -11,7 +11,8 @@
 // Skipping C's own slab test changes no outcome: for a ray whose direction
 // components are all normal floats and whose origin is finite, the slab
 // test's per-axis intervals are monotone in the box bounds, so a box inside
-// C can only pass where C passes; other rays test C's box as well.
+// C can only pass where C passes; other rays walk the binary tree below
+// that point, node by node.
 //
 // Entries whose slab test the binary traversal runs against a ray that may
 // differ from the one at P's visit (an entry without instance bits under a
@@ -49,8 +50,8 @@ constexpr uint32_t kW4ExpandL = 2u;  // slots 0, 1 hold the left child's childre
 constexpr uint32_t kW4ExpandR = 4u;  // slots 2, 3 hold the right child's children
 
 // 128 bytes: the four entry boxes as structure of arrays, the entry words,
-// and meta = {flags and axes, left child, right child (binary indices, for
-// the boxes of expanded children), 0}
+// and meta = {flags and axes, slot order for ray octants 0-3, for octants
+// 4-7, 0}
 struct WideNodeHost {
     float lo[3][4];
     float hi[3][4];
@@ -63,8 +64,7 @@ struct WideTree {
     std::vector<WideNodeHost> nodes;
     std::vector<uint32_t> map;  // binary inner node -> its wide node (kWNone where there is none)
     uint32_t root = 0;          // the binary root the tree was built from
-    int stack_need = 0;         // the deepest stack trace_any4 can reach
-    int stack_need_closest = 0; // the deepest stack trace_closest4 can reach
+    int stack_need = 0;         // the deepest stack trace_any4 / trace_closest4 can reach
     bool closest = false;       // trace_closest4 may use the tree
 };
 
