@@ -461,6 +461,16 @@ int upload_scene(Context& C, const noor_payload* P, const noor_hosek_sky* H, con
                 std::memcpy(&x[i].nrm[r], P->normal_row[r] + 4 * i, 16);
             }
         if ((rc = st.upload((void**)&D.xforms, x.data(), ni * sizeof(DevXform), "transforms"))) return rc;
+        // instances whose world-to-object rows are exactly the identity
+        std::vector<uint32_t> ident(ni / 32 + 1, 0u);
+        for (size_t i = 0; i < ni; ++i) {
+            const float4* r = x[i].w2o;
+            const bool id = r[0].x == 1.0f && r[0].y == 0.0f && r[0].z == 0.0f && r[0].w == 0.0f &&
+                            r[1].x == 0.0f && r[1].y == 1.0f && r[1].z == 0.0f && r[1].w == 0.0f &&
+                            r[2].x == 0.0f && r[2].y == 0.0f && r[2].z == 1.0f && r[2].w == 0.0f;
+            if (id) ident[i / 32] |= 1u << (i % 32);
+        }
+        if ((rc = st.upload((void**)&D.xf_ident, ident.data(), ident.size() * 4, "identity instances"))) return rc;
     }
     {
         std::vector<DevMaterial> m(P->num_materials);

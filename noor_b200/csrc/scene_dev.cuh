@@ -170,6 +170,7 @@ struct DevScene {
     const float4* normals;
     const float2* uvs;
     const DevXform* xforms;
+    const uint32_t* xf_ident;   // bit i: instance i's world-to-object rows are the identity
     const DevMaterial* materials;
     const DevMatTex* mat_tex;   // per material; read only where tex_mask is set
     const DevAreaLight* area_lights;

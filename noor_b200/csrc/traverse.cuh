@@ -43,6 +43,33 @@ NB_D void tray_to_object(TRay& r, const TRay& w, const DevXform* xf) {
     tray_setup(r, o, d);
 }
 
+// A ray whose origin and direction components are all finite and non-zero:
+// an identity transform maps it onto itself bit for bit (1 x = x, 0 y = +-0,
+// x +- 0 = x), which a zero or non-finite component would not guarantee
+// (-0 turns into +0, 0 inf into NaN).
+NB_D bool ray_plain(const float3& o, const float3& d) {
+    const float m = 3.40282347e38f;
+    const float ao[3] = {fabsf(o.x), fabsf(o.y), fabsf(o.z)}, ad[3] = {fabsf(d.x), fabsf(d.y), fabsf(d.z)};
+    bool ok = true;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) ok = ok && ao[i] > 0.0f && ao[i] <= m && ad[i] > 0.0f && ad[i] <= m;
+    return ok;
+}
+
+// The level's ray moved into instance `ins`'s object space
+// (noor/cuda/ray.cuh:174-180).  An instance whose world-to-object rows are
+// exactly the identity (DevScene::xf_ident, set at upload) leaves a plain
+// ray as it is, so the world ray is kept.  Returns whether the level's ray
+// is the world ray.
+NB_D bool enter_instance(TRay& lr, const TRay& wr, const DevScene& S, uint32_t ins, bool plain) {
+    if (plain && ((__ldg(&S.xf_ident[ins >> 5]) >> (ins & 31u)) & 1u)) {
+        lr = wr;
+        return true;
+    }
+    tray_to_object(lr, wr, S.xforms + ins);
+    return false;
+}
+
 // slab test of noor/cuda/bbox.cuh:62-80
 NB_D bool slab_hit_f(const TRay& r, float mnx, float mny, float mnz, float mxx, float mxy, float mxz, float tmax) {
     const bool nx = r.neg & 1u, ny = r.neg & 2u, nz = r.neg & 4u;
@@ -309,6 +336,8 @@ NB_D bool trace_closest(const DevScene& S, const float3& o, const float3& d, flo
     TRay lr = wr;
     WtRay wt;
     if (ISECT == NOOR_ISECT_WATERTIGHT) wt_setup(wt, lr.d);
+    bool wtw = true;  // wt holds the world ray's constants
+    const bool plain = ray_plain(o, d);
     float ltmax = tmax;
     uint32_t ins = 0;
     bool hit = false;
@@ -322,7 +351,10 @@ NB_D bool trace_closest(const DevScene& S, const float3& o, const float3& d, flo
         if (hi.w & NOOR_MESH_NODE_MASK) {
             lr = wr;
             ltmax = tmax;
-            if (ISECT == NOOR_ISECT_WATERTIGHT) wt_setup(wt, lr.d);
+            if (ISECT == NOOR_ISECT_WATERTIGHT && !wtw) {
+                wt_setup(wt, wr.d);
+                wtw = true;
+            }
         }
         if (slab_hit(lr, lo, hi, ltmax)) {
             if (!(hi.w & kNodeKindMask)) {
@@ -343,9 +375,12 @@ NB_D bool trace_closest(const DevScene& S, const float3& o, const float3& d, flo
                 }
             } else if (hi.w & NOOR_MESH_INSTANCE_MASK) {
                 ins = hi.w & NOOR_TRANS_MASK;
-                tray_to_object(lr, wr, S.xforms + ins);
+                const bool same = enter_instance(lr, wr, S, ins, plain);
                 ltmax = tmax;
-                if (ISECT == NOOR_ISECT_WATERTIGHT) wt_setup(wt, lr.d);
+                if (ISECT == NOOR_ISECT_WATERTIGHT && !(same && wtw)) {
+                    wt_setup(wt, lr.d);
+                    wtw = same;
+                }
                 next = lo.w;
             } else if (hi.w & NOOR_MESH_LEAF_MASK) {
                 const uint32_t cnt = hi.w & NOOR_COUNT_MASK;
@@ -412,6 +447,8 @@ NB_D bool trace_any(const DevScene& S, const float3& o, const float3& d, float t
     TRay lr = wr;
     WtRay wt;
     if (ISECT == NOOR_ISECT_WATERTIGHT) wt_setup(wt, lr.d);
+    bool wtw = true;  // wt holds the world ray's constants
+    const bool plain = ray_plain(o, d);
     float ltmax = tmax;
     int top = 0;
     uint32_t ni = S.root;
@@ -423,7 +460,10 @@ NB_D bool trace_any(const DevScene& S, const float3& o, const float3& d, float t
         if (hi.w & NOOR_MESH_NODE_MASK) {
             lr = wr;
             ltmax = tmax;
-            if (ISECT == NOOR_ISECT_WATERTIGHT) wt_setup(wt, lr.d);
+            if (ISECT == NOOR_ISECT_WATERTIGHT && !wtw) {
+                wt_setup(wt, wr.d);
+                wtw = true;
+            }
         }
         if (slab_hit(lr, lo, hi, ltmax)) {
             if (!(hi.w & kNodeKindMask)) {
@@ -439,9 +479,12 @@ NB_D bool trace_any(const DevScene& S, const float3& o, const float3& d, float t
                 if ((int)li < S.num_area_lights && shape_hit<EXT, ISECT == NOOR_ISECT_REF_WALD>(S.area_lights[li], o, d, tm))
                     return true;
             } else if (hi.w & NOOR_MESH_INSTANCE_MASK) {
-                tray_to_object(lr, wr, S.xforms + (hi.w & NOOR_TRANS_MASK));
+                const bool same = enter_instance(lr, wr, S, hi.w & NOOR_TRANS_MASK, plain);
                 ltmax = tmax;
-                if (ISECT == NOOR_ISECT_WATERTIGHT) wt_setup(wt, lr.d);
+                if (ISECT == NOOR_ISECT_WATERTIGHT && !(same && wtw)) {
+                    wt_setup(wt, lr.d);
+                    wtw = same;
+                }
                 next = lo.w;
             } else if (hi.w & NOOR_MESH_LEAF_MASK) {
                 const uint32_t cnt = hi.w & NOOR_COUNT_MASK;
@@ -614,6 +657,8 @@ NB_D bool trace_any4(const DevScene& S, const float3& o, const float3& d, float 
     bool ldeg = wdeg;
     WtRay wt;
     if (ISECT == NOOR_ISECT_WATERTIGHT) wt_setup(wt, lr.d);
+    bool wtw = true;  // wt holds the world ray's constants
+    const bool plain = ray_plain(o, d);
     const int cap = S.stack_cap4;
     int top = 0;
     uint32_t next = kWRef | kWUntested | S.root;
@@ -626,7 +671,10 @@ NB_D bool trace_any4(const DevScene& S, const float3& o, const float3& d, float 
             if (meta.x & kW4World) {
                 lr = wr;
                 ldeg = wdeg;
-                if (ISECT == NOOR_ISECT_WATERTIGHT) wt_setup(wt, lr.d);
+                if (ISECT == NOOR_ISECT_WATERTIGHT && !wtw) {
+                    wt_setup(wt, wr.d);
+                    wtw = true;
+                }
             }
             if (!wide_visit(nd, meta, lr, tmax, st, cap, top, next, status)) return false;
         } else {
@@ -637,7 +685,10 @@ NB_D bool trace_any4(const DevScene& S, const float3& o, const float3& d, float 
             if (hi.w & NOOR_MESH_NODE_MASK) {
                 lr = wr;
                 ldeg = wdeg;
-                if (ISECT == NOOR_ISECT_WATERTIGHT) wt_setup(wt, lr.d);
+                if (ISECT == NOOR_ISECT_WATERTIGHT && !wtw) {
+                    wt_setup(wt, wr.d);
+                    wtw = true;
+                }
             }
             if (!(cur & kWUntested) || slab_hit(lr, lo, hi, tmax)) {
                 if (!(hi.w & kNodeKindMask)) {
@@ -649,9 +700,12 @@ NB_D bool trace_any4(const DevScene& S, const float3& o, const float3& d, float 
                         shape_hit<EXT, ISECT == NOOR_ISECT_REF_WALD>(S.area_lights[li], o, d, tm))
                         return true;
                 } else if (hi.w & NOOR_MESH_INSTANCE_MASK) {
-                    tray_to_object(lr, wr, S.xforms + (hi.w & NOOR_TRANS_MASK));
-                    ldeg = wide_degenerate(lr.o, lr.d);
-                    if (ISECT == NOOR_ISECT_WATERTIGHT) wt_setup(wt, lr.d);
+                    const bool same = enter_instance(lr, wr, S, hi.w & NOOR_TRANS_MASK, plain);
+                    ldeg = same ? wdeg : wide_degenerate(lr.o, lr.d);
+                    if (ISECT == NOOR_ISECT_WATERTIGHT && !(same && wtw)) {
+                        wt_setup(wt, lr.d);
+                        wtw = same;
+                    }
                     next = kWRef | kWUntested | lo.w;
                 } else if (hi.w & NOOR_MESH_LEAF_MASK) {
                     const uint32_t cnt = hi.w & NOOR_COUNT_MASK;
@@ -707,6 +761,8 @@ NB_D bool trace_closest4(const DevScene& S, const float3& o, const float3& d, fl
     bool ldeg = wdeg;
     WtRay wt;
     if (ISECT == NOOR_ISECT_WATERTIGHT) wt_setup(wt, lr.d);
+    bool wtw = true;  // wt holds the world ray's constants
+    const bool plain = ray_plain(o, d);
     float ltmax = tmax;
     uint32_t ins = 0;
     bool hit = false;
@@ -723,7 +779,10 @@ NB_D bool trace_closest4(const DevScene& S, const float3& o, const float3& d, fl
                 lr = wr;
                 ltmax = tmax;
                 ldeg = wdeg;
-                if (ISECT == NOOR_ISECT_WATERTIGHT) wt_setup(wt, lr.d);
+                if (ISECT == NOOR_ISECT_WATERTIGHT && !wtw) {
+                    wt_setup(wt, wr.d);
+                    wtw = true;
+                }
             }
             if (!wide_visit(nd, meta, lr, ltmax, st, cap, top, next, status)) return hit;
         } else {
@@ -735,7 +794,10 @@ NB_D bool trace_closest4(const DevScene& S, const float3& o, const float3& d, fl
                 lr = wr;
                 ltmax = tmax;
                 ldeg = wdeg;
-                if (ISECT == NOOR_ISECT_WATERTIGHT) wt_setup(wt, lr.d);
+                if (ISECT == NOOR_ISECT_WATERTIGHT && !wtw) {
+                    wt_setup(wt, wr.d);
+                    wtw = true;
+                }
             }
             if (slab_hit(lr, lo, hi, ltmax)) {
                 if (!(hi.w & kNodeKindMask)) {
@@ -750,10 +812,13 @@ NB_D bool trace_closest4(const DevScene& S, const float3& o, const float3& d, fl
                     }
                 } else if (hi.w & NOOR_MESH_INSTANCE_MASK) {
                     ins = hi.w & NOOR_TRANS_MASK;
-                    tray_to_object(lr, wr, S.xforms + ins);
+                    const bool same = enter_instance(lr, wr, S, ins, plain);
                     ltmax = tmax;
-                    ldeg = wide_degenerate(lr.o, lr.d);
-                    if (ISECT == NOOR_ISECT_WATERTIGHT) wt_setup(wt, lr.d);
+                    ldeg = same ? wdeg : wide_degenerate(lr.o, lr.d);
+                    if (ISECT == NOOR_ISECT_WATERTIGHT && !(same && wtw)) {
+                        wt_setup(wt, lr.d);
+                        wtw = same;
+                    }
                     next = kWRef | lo.w;
                 } else if (hi.w & NOOR_MESH_LEAF_MASK) {
                     const uint32_t cnt = hi.w & NOOR_COUNT_MASK;
