@@ -646,102 +646,128 @@ NB_D bool inner_step(const DevScene& S, uint32_t ni, const uint4& lo, const uint
 // leaves, instances, light nodes and deferred entries) are taken as the
 // binary traversal takes them; a ref carries kWUntested when its box has not
 // been tested yet.  The stack holds S.stack_cap4 words, the deepest this
-// tree can need.
+// tree can need.  The walk is kept in an Any4 so that a kernel can advance
+// many rays a step at a time (any4_step) and start a new ray on a lane as
+// soon as its last one ends.
+struct Any4 {
+    TRay wr, lr;        // the world ray, the ray of the level being walked
+    WtRay wt;           // watertight constants of wt_ray's level
+    float tmax;
+    uint32_t next;      // the word taken next
+    int top;
+    bool wdeg, ldeg;    // wide_degenerate of the world / level ray
+    bool wtw;           // wt holds the world ray's constants
+    bool plain;         // ray_plain of the world ray
+};
+
+template <int ISECT>
+NB_D void any4_init(Any4& a, const DevScene& S, const float3& o, const float3& d, float tmax) {
+    tray_setup(a.wr, o, d);
+    a.lr = a.wr;
+    a.wdeg = a.ldeg = wide_degenerate(o, d);
+    if (ISECT == NOOR_ISECT_WATERTIGHT) wt_setup(a.wt, d);
+    a.wtw = true;
+    a.plain = ray_plain(o, d);
+    a.tmax = tmax;
+    a.top = 0;
+    a.next = kWRef | kWUntested | S.root;
+}
+
+enum : int { kAnyRunning = 0, kAnyHit = 1, kAnyMiss = 2, kAnyFailed = 3 };
+
+// One step of the walk: a wide node's visit or one binary node.
+template <int ISECT, bool EXT>
+NB_D int any4_step(Any4& a, const DevScene& S, const SmemStack& st, uint32_t* status) {
+    const int cap = S.stack_cap4;
+    const uint32_t cur = a.next;
+    a.next = kWNone;
+    if (!(cur & kWRef)) {
+        const DevNode4* nd = S.nodes4 + cur;
+        const uint4 meta = __ldg(&nd->meta);
+        if (meta.x & kW4World) {
+            a.lr = a.wr;
+            a.ldeg = a.wdeg;
+            if (ISECT == NOOR_ISECT_WATERTIGHT && !a.wtw) {
+                wt_setup(a.wt, a.wr.d);
+                a.wtw = true;
+            }
+        }
+        if (!wide_visit(nd, meta, a.lr, a.tmax, st, cap, a.top, a.next, status)) return kAnyFailed;
+    } else {
+        const uint32_t ni = cur & kWIndex;
+        const DevNode* nd = S.nodes + ni;
+        const uint4 lo = __ldg(&nd->lo);
+        const uint4 hi = __ldg(&nd->hi);
+        if (hi.w & NOOR_MESH_NODE_MASK) {
+            a.lr = a.wr;
+            a.ldeg = a.wdeg;
+            if (ISECT == NOOR_ISECT_WATERTIGHT && !a.wtw) {
+                wt_setup(a.wt, a.wr.d);
+                a.wtw = true;
+            }
+        }
+        if (!(cur & kWUntested) || slab_hit(a.lr, lo, hi, a.tmax)) {
+            if (!(hi.w & kNodeKindMask)) {
+                if (!inner_step(S, ni, lo, hi, a.lr, a.ldeg, st, cap, a.top, a.next, status)) return kAnyFailed;
+            } else if (hi.w & NOOR_LIGHT_NODE_MASK) {
+                const uint32_t li = hi.w & NOOR_LIGHT_MASK;
+                float tm = a.tmax;
+                if ((int)li < S.num_area_lights &&
+                    shape_hit<EXT, ISECT == NOOR_ISECT_REF_WALD>(S.area_lights[li], a.wr.o, a.wr.d, tm))
+                    return kAnyHit;
+            } else if (hi.w & NOOR_MESH_INSTANCE_MASK) {
+                const bool same = enter_instance(a.lr, a.wr, S, hi.w & NOOR_TRANS_MASK, a.plain);
+                a.ldeg = same ? a.wdeg : wide_degenerate(a.lr.o, a.lr.d);
+                if (ISECT == NOOR_ISECT_WATERTIGHT && !(same && a.wtw)) {
+                    wt_setup(a.wt, a.lr.d);
+                    a.wtw = same;
+                }
+                a.next = kWRef | kWUntested | lo.w;
+            } else if (hi.w & NOOR_MESH_LEAF_MASK) {
+                const uint32_t cnt = hi.w & NOOR_COUNT_MASK;
+                if (a.top + (int)cnt > cap + 1) {
+                    atomicOr(status, NOOR_DEV_STACK_OVERFLOW);
+                    return kAnyFailed;
+                }
+                for (uint32_t i = 1; i < cnt; ++i) {
+                    st.base[a.top * st.stride] = kWRef | kWUntested | (ni + i);
+                    ++a.top;
+                }
+                if (cnt) a.next = kWRef | kWUntested | (ni + cnt);
+            } else {
+                const uint32_t start = lo.w;
+                const uint32_t end = start + (hi.w & NOOR_TRI_COUNT_MASK);
+                for (uint32_t ti = start; ti < end; ++ti) {
+                    float tm = a.tmax, bu, bv;
+                    uint32_t mt;
+                    bool h;
+                    if (ISECT == NOOR_ISECT_WATERTIGHT)
+                        h = wt_test(a.lr, a.wt, S.wtri + ti, tm, bu, bv, mt);
+                    else
+                        h = wald_test(a.lr, S.wald + ti, tm, bu, bv, mt);
+                    if (h && EXT && S.has_alpha && (mt & NOOR_ALPHA) && alpha_cut<ISECT>(S, ti, bu, bv)) h = false;
+                    if (h) return kAnyHit;
+                }
+            }
+        }
+    }
+    if (a.next == kWNone) {
+        if (a.top == 0) return kAnyMiss;
+        --a.top;
+        a.next = st.base[a.top * st.stride];
+    }
+    return kAnyRunning;
+}
+
 template <int ISECT, bool EXT = true>
 NB_D bool trace_any4(const DevScene& S, const float3& o, const float3& d, float tmax, const SmemStack& st,
                      uint32_t* status) {
-    TRay wr;
-    tray_setup(wr, o, d);
-    const bool wdeg = wide_degenerate(o, d);
-    TRay lr = wr;
-    bool ldeg = wdeg;
-    WtRay wt;
-    if (ISECT == NOOR_ISECT_WATERTIGHT) wt_setup(wt, lr.d);
-    bool wtw = true;  // wt holds the world ray's constants
-    const bool plain = ray_plain(o, d);
-    const int cap = S.stack_cap4;
-    int top = 0;
-    uint32_t next = kWRef | kWUntested | S.root;
+    Any4 a;
+    any4_init<ISECT>(a, S, o, d, tmax);
     for (;;) {
-        const uint32_t cur = next;
-        next = kWNone;
-        if (!(cur & kWRef)) {
-            const DevNode4* nd = S.nodes4 + cur;
-            const uint4 meta = __ldg(&nd->meta);
-            if (meta.x & kW4World) {
-                lr = wr;
-                ldeg = wdeg;
-                if (ISECT == NOOR_ISECT_WATERTIGHT && !wtw) {
-                    wt_setup(wt, wr.d);
-                    wtw = true;
-                }
-            }
-            if (!wide_visit(nd, meta, lr, tmax, st, cap, top, next, status)) return false;
-        } else {
-            const uint32_t ni = cur & kWIndex;
-            const DevNode* nd = S.nodes + ni;
-            const uint4 lo = __ldg(&nd->lo);
-            const uint4 hi = __ldg(&nd->hi);
-            if (hi.w & NOOR_MESH_NODE_MASK) {
-                lr = wr;
-                ldeg = wdeg;
-                if (ISECT == NOOR_ISECT_WATERTIGHT && !wtw) {
-                    wt_setup(wt, wr.d);
-                    wtw = true;
-                }
-            }
-            if (!(cur & kWUntested) || slab_hit(lr, lo, hi, tmax)) {
-                if (!(hi.w & kNodeKindMask)) {
-                    if (!inner_step(S, ni, lo, hi, lr, ldeg, st, cap, top, next, status)) return false;
-                } else if (hi.w & NOOR_LIGHT_NODE_MASK) {
-                    const uint32_t li = hi.w & NOOR_LIGHT_MASK;
-                    float tm = tmax;
-                    if ((int)li < S.num_area_lights &&
-                        shape_hit<EXT, ISECT == NOOR_ISECT_REF_WALD>(S.area_lights[li], o, d, tm))
-                        return true;
-                } else if (hi.w & NOOR_MESH_INSTANCE_MASK) {
-                    const bool same = enter_instance(lr, wr, S, hi.w & NOOR_TRANS_MASK, plain);
-                    ldeg = same ? wdeg : wide_degenerate(lr.o, lr.d);
-                    if (ISECT == NOOR_ISECT_WATERTIGHT && !(same && wtw)) {
-                        wt_setup(wt, lr.d);
-                        wtw = same;
-                    }
-                    next = kWRef | kWUntested | lo.w;
-                } else if (hi.w & NOOR_MESH_LEAF_MASK) {
-                    const uint32_t cnt = hi.w & NOOR_COUNT_MASK;
-                    if (top + (int)cnt > cap + 1) {
-                        atomicOr(status, NOOR_DEV_STACK_OVERFLOW);
-                        return false;
-                    }
-                    for (uint32_t i = 1; i < cnt; ++i) {
-                        st.base[top * st.stride] = kWRef | kWUntested | (ni + i);
-                        ++top;
-                    }
-                    if (cnt) next = kWRef | kWUntested | (ni + cnt);
-                } else {
-                    const uint32_t start = lo.w;
-                    const uint32_t end = start + (hi.w & NOOR_TRI_COUNT_MASK);
-                    for (uint32_t ti = start; ti < end; ++ti) {
-                        float tm = tmax, bu, bv;
-                        uint32_t mt;
-                        bool h;
-                        if (ISECT == NOOR_ISECT_WATERTIGHT)
-                            h = wt_test(lr, wt, S.wtri + ti, tm, bu, bv, mt);
-                        else
-                            h = wald_test(lr, S.wald + ti, tm, bu, bv, mt);
-                        if (h && EXT && S.has_alpha && (mt & NOOR_ALPHA) && alpha_cut<ISECT>(S, ti, bu, bv)) h = false;
-                        if (h) return true;
-                    }
-                }
-            }
-        }
-        if (next == kWNone) {
-            if (top == 0) break;
-            --top;
-            next = st.base[top * st.stride];
-        }
+        const int r = any4_step<ISECT, EXT>(a, S, st, status);
+        if (r != kAnyRunning) return r == kAnyHit;
     }
-    return false;
 }
 
 // Closest hit over the four-wide tree: the same hit, to the bit, as

@@ -157,6 +157,11 @@ struct WfDev {
 #ifndef NB_SHADOW_FETCH
 #define NB_SHADOW_FETCH 1
 #endif
+// 1: on the four-wide tree, each lane takes a new shadow ray as soon as its
+// last one ends (rays walked a step at a time); 0: 32 rays per warp to the end
+#ifndef NB_SHADOW_REFILL
+#define NB_SHADOW_REFILL 0
+#endif
 
 NB_D uint32_t fbits(float f) { return __float_as_uint(f); }
 NB_D float bitsf(uint32_t u) { return __uint_as_float(u); }
@@ -728,6 +733,58 @@ __global__ void __launch_bounds__(NB_TRAV_THREADS, WIDE ? NB_TRAV_MIN_BLOCKS_WID
     extern __shared__ uint32_t smem[];
     const uint32_t n = W.counters[kCntShadow];
     SmemStack stk{smem + threadIdx.x, (int)blockDim.x, W.stack_cap};
+#if NB_SHADOW_REFILL
+    if (WIDE) {
+        // every lane walks its ray a step at a time and takes the next queue
+        // entry as soon as its ray ends (one counter add per warp and round)
+        const uint32_t lane = threadIdx.x & 31;
+        Any4 a;
+        uint32_t e = 0;
+        const DevScene* Sp = &S1;
+        bool live = false, drained = false;
+        for (;;) {
+            if (!drained) {
+                const uint32_t need = __ballot_sync(0xFFFFFFFFu, !live);
+                if (need) {
+                    const int leader = __ffs(need) - 1;
+                    uint32_t base = 0;
+                    if ((int)lane == leader) base = atomicAdd(W.counters + kCntTake, (uint32_t)__popc(need));
+                    base = __shfl_sync(0xFFFFFFFFu, base, leader);
+                    if (base + (uint32_t)__popc(need) >= n) drained = true;
+                    if (!live) {
+                        const uint32_t i = base + (uint32_t)__popc(need & ((1u << lane) - 1u));
+                        if (i < n) {
+                            const uint32_t q = W.level >= 3 ? W.sh_perm[i] : i;
+                            e = W.qshadow[q];
+                            const float4 so = W.sh_o[q], sd = W.sh_d[q];
+                            Sp = &slot_scene<ISECT, MULTI>(W, S1, MULTI ? fbits(W.o[e >> 1].w) : 0u);
+                            const float3 o = f3(so.x, so.y, so.z), d = f3(sd.x, sd.y, sd.z);
+                            if (ISECT == kIsectMixed ? Sp->isect == NOOR_ISECT_WATERTIGHT
+                                                     : ISECT == NOOR_ISECT_WATERTIGHT)
+                                any4_init<NOOR_ISECT_WATERTIGHT>(a, *Sp, o, d, so.w);
+                            else
+                                any4_init<NOOR_ISECT_REF_WALD>(a, *Sp, o, d, so.w);
+                            live = true;
+                        }
+                    }
+                }
+            }
+            if (!__any_sync(0xFFFFFFFFu, live)) break;
+            if (live) {
+                int r;
+                if (ISECT == kIsectMixed ? Sp->isect == NOOR_ISECT_WATERTIGHT : ISECT == NOOR_ISECT_WATERTIGHT)
+                    r = any4_step<NOOR_ISECT_WATERTIGHT, EXT>(a, *Sp, stk, W.status);
+                else
+                    r = any4_step<NOOR_ISECT_REF_WALD, EXT>(a, *Sp, stk, W.status);
+                if (r != kAnyRunning) {
+                    if (r == kAnyHit) W.pend[e].w = 0.0f;
+                    live = false;
+                }
+            }
+        }
+        return;
+    }
+#endif
 #if NB_SHADOW_FETCH
     const uint32_t lane = threadIdx.x & 31;
     for (;;) {
