@@ -65,7 +65,8 @@ def parse():
     ap.add_argument("--wf-sort", type=int, default=0)
     ap.add_argument("--wf-graph", type=int, default=1, help="wavefront: 1 CUDA-graph while loop, 0 host loop")
     ap.add_argument("--wf-tree", type=int, default=0,
-                    help="wavefront (without autotuning): 0 auto, 1 binary tree, 2 four-wide tree")
+                    help="wavefront (without autotuning): 0 auto, 1 binary tree, 2 four-wide tree, "
+                         "3 four-wide tree for shadow rays only")
     ap.add_argument("--workload", default="sky", choices=["sky", "room", "env", "batched", "adjoint"],
                     help="sky: the headline sky-lit scene; room: the 36-triangle room; env: the env-map MIS "
                          "scene; batched: 64 uneven frames in one wavefront launch against 64 sequential "
@@ -473,7 +474,8 @@ class WavefrontPath:
         p = self.params
         return {"entry_point": "noor_wavefront_render",
                 "wavefront": {"block": p.block_size, "slots": p.queue_capacity, "material_sort": p.sort_granularity,
-                              "graph": p.use_graph, "tree": ["auto", "binary", "four-wide"][p.traversal],
+                              "graph": p.use_graph,
+                              "tree": ["auto", "binary", "four-wide", "four-wide shadow rays"][p.traversal],
                               "autotune_best_ms": self.tuned_ms}}
 
     def image(self):

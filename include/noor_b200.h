@@ -681,14 +681,21 @@ typedef struct noor_wf_params {
                                  * every path (slots x bounces); a loop that
                                  * reaches it stops and sets
                                  * NOOR_DEV_WAIT_TIMEOUT                    */
-    uint32_t traversal;         /* the tree the extension and shadow stages
-                                 * walk (the same hits either way):
-                                 * NOOR_TRAVERSAL_AUTO, _BINARY or _WIDE    */
+    uint32_t traversal;         /* the trees the extension and shadow
+                                 * stages walk (the same hits either way):
+                                 * NOOR_TRAVERSAL_*                          */
 } noor_wf_params;
-/* AUTO: the four-wide tree when every scene of the launch has one and at
- * least 16384 triangles, else the binary tree; WIDE: the four-wide tree
- * where every scene of the launch has one (noor_wide_tree_info) */
-enum { NOOR_TRAVERSAL_AUTO = 0, NOOR_TRAVERSAL_BINARY = 1, NOOR_TRAVERSAL_WIDE = 2 };
+/* BINARY: both stages on the binary tree; WIDE: both on the four-wide tree
+ * where every scene of the launch has one (noor_wide_tree_info);
+ * WIDE_SHADOW: extension rays on the binary tree, shadow rays on the
+ * four-wide one; AUTO: WIDE_SHADOW when every scene of the launch has a
+ * four-wide tree and at least 16384 triangles, else BINARY */
+enum {
+    NOOR_TRAVERSAL_AUTO = 0,
+    NOOR_TRAVERSAL_BINARY = 1,
+    NOOR_TRAVERSAL_WIDE = 2,
+    NOOR_TRAVERSAL_WIDE_SHADOW = 3
+};
 
 /* Scenes for the wavefront live in the current context; scene 0 is the one
  * load_cuda_data uploaded.  Adds another payload/sky/spec, returns its id. */

@@ -57,7 +57,7 @@ MESH_LEAF_MASK = 0x40000000
 MESH_INSTANCE_MASK = 0x20000000
 MESH_INNER_MASK = 0x10000000
 LIGHT_NODE_MASK = 0x08000000
-NOOR_TRAVERSAL_AUTO, NOOR_TRAVERSAL_BINARY, NOOR_TRAVERSAL_WIDE = 0, 1, 2
+NOOR_TRAVERSAL_AUTO, NOOR_TRAVERSAL_BINARY, NOOR_TRAVERSAL_WIDE, NOOR_TRAVERSAL_WIDE_SHADOW = 0, 1, 2, 3
 
 
 class Shape(C.Structure):

@@ -157,11 +157,7 @@ struct WfDev {
 #ifndef NB_SHADOW_FETCH
 #define NB_SHADOW_FETCH 1
 #endif
-// 1: on the four-wide tree, each lane takes a new shadow ray as soon as its
-// last one ends (rays walked a step at a time); 0: 32 rays per warp to the end
-#ifndef NB_SHADOW_REFILL
-#define NB_SHADOW_REFILL 0
-#endif
+
 
 NB_D uint32_t fbits(float f) { return __float_as_uint(f); }
 NB_D float bitsf(uint32_t u) { return __uint_as_float(u); }
@@ -733,58 +729,7 @@ __global__ void __launch_bounds__(NB_TRAV_THREADS, WIDE ? NB_TRAV_MIN_BLOCKS_WID
     extern __shared__ uint32_t smem[];
     const uint32_t n = W.counters[kCntShadow];
     SmemStack stk{smem + threadIdx.x, (int)blockDim.x, W.stack_cap};
-#if NB_SHADOW_REFILL
-    if (WIDE) {
-        // every lane walks its ray a step at a time and takes the next queue
-        // entry as soon as its ray ends (one counter add per warp and round)
-        const uint32_t lane = threadIdx.x & 31;
-        Any4 a;
-        uint32_t e = 0;
-        const DevScene* Sp = &S1;
-        bool live = false, drained = false;
-        for (;;) {
-            if (!drained) {
-                const uint32_t need = __ballot_sync(0xFFFFFFFFu, !live);
-                if (need) {
-                    const int leader = __ffs(need) - 1;
-                    uint32_t base = 0;
-                    if ((int)lane == leader) base = atomicAdd(W.counters + kCntTake, (uint32_t)__popc(need));
-                    base = __shfl_sync(0xFFFFFFFFu, base, leader);
-                    if (base + (uint32_t)__popc(need) >= n) drained = true;
-                    if (!live) {
-                        const uint32_t i = base + (uint32_t)__popc(need & ((1u << lane) - 1u));
-                        if (i < n) {
-                            const uint32_t q = W.level >= 3 ? W.sh_perm[i] : i;
-                            e = W.qshadow[q];
-                            const float4 so = W.sh_o[q], sd = W.sh_d[q];
-                            Sp = &slot_scene<ISECT, MULTI>(W, S1, MULTI ? fbits(W.o[e >> 1].w) : 0u);
-                            const float3 o = f3(so.x, so.y, so.z), d = f3(sd.x, sd.y, sd.z);
-                            if (ISECT == kIsectMixed ? Sp->isect == NOOR_ISECT_WATERTIGHT
-                                                     : ISECT == NOOR_ISECT_WATERTIGHT)
-                                any4_init<NOOR_ISECT_WATERTIGHT>(a, *Sp, o, d, so.w);
-                            else
-                                any4_init<NOOR_ISECT_REF_WALD>(a, *Sp, o, d, so.w);
-                            live = true;
-                        }
-                    }
-                }
-            }
-            if (!__any_sync(0xFFFFFFFFu, live)) break;
-            if (live) {
-                int r;
-                if (ISECT == kIsectMixed ? Sp->isect == NOOR_ISECT_WATERTIGHT : ISECT == NOOR_ISECT_WATERTIGHT)
-                    r = any4_step<NOOR_ISECT_WATERTIGHT, EXT>(a, *Sp, stk, W.status);
-                else
-                    r = any4_step<NOOR_ISECT_REF_WALD, EXT>(a, *Sp, stk, W.status);
-                if (r != kAnyRunning) {
-                    if (r == kAnyHit) W.pend[e].w = 0.0f;
-                    live = false;
-                }
-            }
-        }
-        return;
-    }
-#endif
+
 #if NB_SHADOW_FETCH
     const uint32_t lane = threadIdx.x & 31;
     for (;;) {
@@ -941,9 +886,11 @@ struct WfLaunch {
     bool diff;              // ... has bump maps: rays carry differentials
 };
 
-// NOOR_TRAVERSAL_AUTO takes the four-wide tree for scenes of at least this
-// many triangles (on the 36-triangle room the binary tree's single-box
-// visits are cheaper; on the 2.6M-triangle sky scene the wide tree wins)
+// NOOR_TRAVERSAL_AUTO takes the four-wide tree for the shadow rays of scenes
+// of at least this many triangles (on the 36-triangle room the binary tree's
+// single-box visits are cheaper; on the 2.6M-triangle sky scene shadow rays
+// take 11.3 ms per step on the wide tree against 11.7, extension rays 50.2
+// against 48.6, so the extension stage keeps the binary tree)
 constexpr uint32_t kWideAutoTris = 16384;
 
 // shading launches per iteration: one per queue some scene can fill
@@ -1108,13 +1055,14 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
     bool multi = false, mixed = false;
     // the four-wide trees where every scene of the launch has them (and,
     // for NOOR_TRAVERSAL_AUTO, is large enough for them to pay)
-    if (P.traversal > NOOR_TRAVERSAL_WIDE) return set_error(NOOR_ERR_INVALID, "wavefront: bad traversal selector");
-    bool wide_c = P.traversal != NOOR_TRAVERSAL_BINARY, wide_a = wide_c;
+    if (P.traversal > NOOR_TRAVERSAL_WIDE_SHADOW)
+        return set_error(NOOR_ERR_INVALID, "wavefront: bad traversal selector");
+    bool wide_c = P.traversal == NOOR_TRAVERSAL_WIDE, wide_a = P.traversal != NOOR_TRAVERSAL_BINARY;
     L.ext = L.ext_lights = L.env_ref = L.tex = L.diff = false;
     L.kinds = 0;
     for (uint32_t i = 0; i < n_frames; ++i) {
         const DevScene& fs = C.scenes[frames[i].scene_id]->dev;
-        const bool big = P.traversal == NOOR_TRAVERSAL_WIDE || fs.num_tris >= kWideAutoTris;
+        const bool big = P.traversal != NOOR_TRAVERSAL_AUTO || fs.num_tris >= kWideAutoTris;
         wide_c &= fs.closest4 != 0u && big;
         wide_a &= fs.nodes4 != nullptr && big;
         L.kinds |= fs.shade_kinds;
@@ -1324,9 +1272,9 @@ extern "C" int noor_wavefront_counters(uint64_t counters[3], int reset) {
 // Autotuner: coordinate descent on the launch parameters, each candidate
 // timed by one device-timed render of the batch: the slot count first
 // (2^18 .. 2^23, none beyond twice the batch's paths), then the block size
-// (32, 64, 128), then the sort granularity (0 .. 3), then the tree (binary,
-// four-wide), then the slot count again around the choices made; the
-// fastest seen wins.
+// (32, 64, 128), then the sort granularity (0 .. 3), then the trees (binary,
+// four-wide, four-wide for shadow rays only), then the slot count again
+// around the choices made; the fastest seen wins.
 extern "C" int noor_wavefront_autotune(const noor_wf_frame* frames, uint32_t n_frames, noor_wf_params* best,
                                        float* best_ms) {
     Context* C;
@@ -1366,7 +1314,8 @@ extern "C" int noor_wavefront_autotune(const noor_wf_frame* frames, uint32_t n_f
         p.sort_granularity = so;
         if (so != bp.sort_granularity && (rc = trial(p))) return rc;
     }
-    for (uint32_t tv : {(uint32_t)NOOR_TRAVERSAL_BINARY, (uint32_t)NOOR_TRAVERSAL_WIDE}) {
+    for (uint32_t tv : {(uint32_t)NOOR_TRAVERSAL_BINARY, (uint32_t)NOOR_TRAVERSAL_WIDE,
+                        (uint32_t)NOOR_TRAVERSAL_WIDE_SHADOW}) {
         noor_wf_params p = bp;
         p.traversal = tv;
         if ((rc = trial(p))) return rc;
