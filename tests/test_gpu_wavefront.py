@@ -127,7 +127,7 @@ def test_wavefront_trees_trace_the_same_paths(which):
     try:
         w, h = s.camera["w"], s.camera["h"]
         out, rays = [], []
-        for tree in (_capi.NOOR_TRAVERSAL_BINARY, _capi.NOOR_TRAVERSAL_WIDE):
+        for tree in (_capi.NOOR_TRAVERSAL_BINARY, _capi.NOOR_TRAVERSAL_WIDE, _capi.NOOR_TRAVERSAL_WIDE_SHADOW):
             f = film(w, h)
             fr = scenes.wf_frame(0, s.camera, 16, bounces=5, d_film=f.data_ptr())
             c = (C.c_uint64 * 3)()
@@ -137,9 +137,10 @@ def test_wavefront_trees_trace_the_same_paths(which):
             torch.cuda.synchronize()
             out.append(f.cpu().numpy()[..., :3])
             rays.append(tuple(int(x) for x in c))
-        assert rays[0] == rays[1] and rays[0][0] > 0, rays
-        rel = np.abs(out[0] - out[1]) / np.maximum(np.abs(out[1]), 1e-2)
-        assert rel.max() < 1e-5, float(rel.max())
+        assert rays[0] == rays[1] == rays[2] and rays[0][0] > 0, rays
+        for k in (1, 2):
+            rel = np.abs(out[0] - out[k]) / np.maximum(np.abs(out[k]), 1e-2)
+            assert rel.max() < 1e-5, (k, float(rel.max()))
         assert r.status(reset=True) == 0
     finally:
         r.close()
