@@ -133,14 +133,15 @@ struct WfDev {
 };
 
 // Launch bounds of the traversal stages (extend, shadow): at most 128
-// threads per block and 9 such blocks per SM cap their registers at 56
-// (36 warps per SM at 64-thread blocks instead of 32 at their natural 64-80;
-// measured faster on the sky-lit 2.6M-triangle scene than 64 or 48)
+// threads per block and 8 such blocks per SM cap their registers at 64
+// (32 warps per SM; on the sky-lit 2.6M-triangle scene 76.9 ms per step
+// against 78.0 at 9 blocks and 56 registers, where extend spills; the room
+// runs the same at both)
 #ifndef NB_TRAV_THREADS
 #define NB_TRAV_THREADS 128
 #endif
 #ifndef NB_TRAV_MIN_BLOCKS
-#define NB_TRAV_MIN_BLOCKS 9
+#define NB_TRAV_MIN_BLOCKS 8
 #endif
 // the same for the kernels on the four-wide tree: 8 blocks, 64 registers
 // (their wide visits hold four boxes' slab intervals; on the sky-lit
