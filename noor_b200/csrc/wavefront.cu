@@ -61,23 +61,11 @@ struct WfFrameDev {
 };
 
 // slot state: bits 0-1 kFree / kActive / kFinishing; kPend while the direct
-// lighting of the last shade step waits to be folded into L (by extend for a
-// continuing path, by regen for one that ended); bits 3-4 the shading queue
-// (1 + material kind) extend assigned to a surface hit; kSkySeen on a
-// finishing slot whose last ray escaped to a sky it counts (regen adds
-// beta * sky radiance, evaluated there with converged lanes); kPendHeld on a
-// finishing slot with pending light that regen passed over once, while that
-// light's shadow rays were being traced
-enum : uint32_t {
-    kFree = 0,
-    kActive = 1,
-    kFinishing = 2,
-    kLifeMask = 3,
-    kPend = 4,
-    kKindShift = 3,
-    kSkySeen = 32,
-    kPendHeld = 64
-};
+// lighting of the last shade step waits for regen to fold it into L; bits
+// 3-4 the shading queue (1 + material kind) extend assigned to a surface hit;
+// kSkySeen on a finishing slot whose last ray escaped to a sky it counts
+// (regen adds beta * sky radiance, evaluated there with converged lanes)
+enum : uint32_t { kFree = 0, kActive = 1, kFinishing = 2, kLifeMask = 3, kPend = 4, kKindShift = 3, kSkySeen = 32 };
 
 // counter words
 enum : int {
@@ -87,8 +75,7 @@ enum : int {
     kCntTake = kKinds + 3,     // shadow queue entries taken by wf_shadow's warps
     kCntCam = kKinds + 4,      // camera rays in the extension order (sort level 2)
     kCntTakeExt = kKinds + 5,  // extension order entries taken by wf_extend's warps
-    kCntHeld = kKinds + 6,     // finishing slots regen held back for their shadow rays
-    kCntWords = kKinds + 7
+    kCntWords = kKinds + 6
 };
 
 // Ray ordering (sort levels 2 and 3): a counting sort of rays into buckets
@@ -254,16 +241,13 @@ NB_D RayDiff load_diff(const WfDev& W, uint32_t slot) {
     return r;
 }
 
-// Regen (every slot), launched beside the shadow stage of the iteration
-// before: finished paths get their pending direct light (a path that ended
-// in the shade step whose shadow rays are being traced waits one iteration,
-// kPendHeld), the sky term if their last ray escaped, and go to their
-// frame's film (one float4 atomic per path, TwoSum-compensated); free slots
-// are refilled with the camera rays of the next work items.  Continuing
-// paths are left to extend, which folds their pending light.  The block takes
-// its work items with one atomic, in lane order (consecutive lanes:
-// consecutive pixels of one 8x4 tile), and adds its active and held slots to
-// the counts with one atomic each.
+// Regen (every slot): fold the last shade step's direct lighting into L; add
+// the sky term of paths whose last ray escaped, and add finished paths to
+// their frame's film (one float4 atomic per path, TwoSum-compensated);
+// refill free slots with the camera
+// rays of the next work items.  The block takes its work items with one
+// atomic, in lane order (consecutive lanes: consecutive pixels of one 8x4
+// tile), and adds its active slots to the active count with one atomic.
 // DIFF: some scene of the batch has bump maps (camera rays with differentials)
 template <bool DIFF>
 __global__ void __launch_bounds__(kRegenBlock) wf_regen(WfDev W) {
@@ -272,30 +256,26 @@ __global__ void __launch_bounds__(kRegenBlock) wf_regen(WfDev W) {
     const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = slot < W.cap;
     uint32_t st = kFree;
-    bool held = false;
     if (valid) {
         st = W.state[slot];
-        const uint32_t life = st & kLifeMask;
-        if (life == kFinishing && (st & kPend) && !(st & kPendHeld)) {
-            // the path ended in the last shade step with direct light
-            // pending, whose shadow rays are traced beside this launch: its
-            // film write waits one iteration
-            held = true;
-        } else if (life == kFinishing) {
-            float4 Lw = W.L[slot];
-            if (st & kPend) {
-                // L += beta * (c0' + c1') with c' = c if its shadow ray was
-                // unblocked, as the megakernel adds its direct lighting
-                const float4 p0 = W.pend[2 * slot], p1 = W.pend[2 * slot + 1];
-                float3 Ld = f3(0.0f);
-                if (p0.w != 0.0f) Ld += f3(p0.x, p0.y, p0.z);
-                if (p1.w != 0.0f) Ld += f3(p1.x, p1.y, p1.z);
-                const float4 b = W.pbeta[slot];
-                const float3 c = f3(b.x, b.y, b.z) * Ld;
-                Lw.x += c.x;
-                Lw.y += c.y;
-                Lw.z += c.z;
-            }
+        float4 Lw;
+        if (st & kPend) {
+            // L += beta * (c0' + c1') with c' = c if its shadow ray was
+            // unblocked, as the megakernel adds its direct lighting
+            const float4 p0 = W.pend[2 * slot], p1 = W.pend[2 * slot + 1];
+            Lw = W.L[slot];
+            float3 Ld = f3(0.0f);
+            if (p0.w != 0.0f) Ld += f3(p0.x, p0.y, p0.z);
+            if (p1.w != 0.0f) Ld += f3(p1.x, p1.y, p1.z);
+            const float4 b = W.pbeta[slot];
+            const float3 c = f3(b.x, b.y, b.z) * Ld;
+            Lw.x += c.x;
+            Lw.y += c.y;
+            Lw.z += c.z;
+            if ((st & kLifeMask) == kActive) W.L[slot] = Lw;
+        }
+        if ((st & kLifeMask) == kFinishing) {
+            if (!(st & kPend)) Lw = W.L[slot];
             const uint32_t fi = fbits(W.o[slot].w);
             const uint32_t pix = fbits(W.d[slot].w);
             const WfFrameDev& F = W.frames[fi];
@@ -309,7 +289,7 @@ __global__ void __launch_bounds__(kRegenBlock) wf_regen(WfDev W) {
             film_add3(F.sum + pix, F.comp + pix, clamp3(f3(Lw.x, Lw.y, Lw.z), 0.0f, 100.0f));
             st = kFree;
         }
-        // a continuing path keeps its state (extend folds its pending light)
+        st &= kLifeMask;
     }
     const bool need = valid && st == kFree;
     const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -358,11 +338,9 @@ __global__ void __launch_bounds__(kRegenBlock) wf_regen(WfDev W) {
             st = kActive;
         }
     }
-    if (valid) W.state[slot] = held ? (st | kPendHeld) : st;
-    const int nact = __syncthreads_count(valid && (st & kLifeMask) == kActive);
-    const int nheld = __syncthreads_count(held);
+    if (valid) W.state[slot] = st;
+    const int nact = __syncthreads_count(valid && st == kActive);
     if (threadIdx.x == 0 && nact) atomicAdd(W.counters + kCntActive, (uint32_t)nact);
-    if (threadIdx.x == 0 && nheld) atomicAdd(W.counters + kCntHeld, (uint32_t)nheld);
 }
 
 // bucket of a ray: direction octant, then the Morton code of its origin's
@@ -432,22 +410,6 @@ __global__ void __launch_bounds__(kScanThreads) wf_bucket_scan(WfDev W) {
 template <int ISECT, bool EXT, bool WIDE>
 NB_D void extend_one(const WfDev& W, const DevScene& S, uint32_t slot, const float4& ow,
                      const SmemStack& stk) {
-    if (W.state[slot] & kPend) {
-        // the last shade step's direct light, its shadow rays traced: L +=
-        // beta * (c0' + c1') with c' = c if unblocked, before anything this
-        // ray adds, as the megakernel orders its sums
-        const float4 p0 = W.pend[2 * slot], p1 = W.pend[2 * slot + 1];
-        float4 Lw = W.L[slot];
-        float3 Ld = f3(0.0f);
-        if (p0.w != 0.0f) Ld += f3(p0.x, p0.y, p0.z);
-        if (p1.w != 0.0f) Ld += f3(p1.x, p1.y, p1.z);
-        const float4 b = W.pbeta[slot];
-        const float3 c = f3(b.x, b.y, b.z) * Ld;
-        Lw.x += c.x;
-        Lw.y += c.y;
-        Lw.z += c.z;
-        W.L[slot] = Lw;
-    }
     const float4 dw = W.d[slot], bw = W.beta[slot];
     const float3 o = f3(ow.x, ow.y, ow.z), d = f3(dw.x, dw.y, dw.z);
     const uint32_t bb = fbits(bw.w);
@@ -500,7 +462,7 @@ __global__ void __launch_bounds__(kBinBlock) wf_ext_key(WfDev W, DevScene S1) {
     __shared__ uint32_t base;
     const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
     bool cam = false, sec = false;
-    if (slot < W.cap && (W.state[slot] & kLifeMask) == kActive) {
+    if (slot < W.cap && W.state[slot] == kActive) {
         cam = (fbits(W.beta[slot].w) & 0xFFFFu) == 0u;
         sec = !cam;
     }
@@ -586,7 +548,7 @@ __global__ void __launch_bounds__(NB_TRAV_THREADS, WIDE ? NB_TRAV_MIN_BLOCKS_WID
         return;
     }
     const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
-    if (slot >= W.cap || (W.state[slot] & kLifeMask) != kActive) return;
+    if (slot >= W.cap || W.state[slot] != kActive) return;
     extend_slot<ISECT, MULTI, EXT, WIDE>(W, S1, slot, stk);
 }
 
@@ -597,12 +559,6 @@ __global__ void __launch_bounds__(kBinBlock) wf_bin(WfDev W) {
     __shared__ uint32_t cnt[kKinds][kBinBlock / 32];
     __shared__ uint32_t base[kKinds];
     const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
-    // the shadow stage of the iteration before has run (extend waited for
-    // it): its queue's length and take counter start over for this shade
-    if (slot == 0) {
-        W.counters[kCntShadow] = 0u;
-        W.counters[kCntTake] = 0u;
-    }
     const uint32_t kq = slot < W.cap ? (W.state[slot] >> kKindShift) & 3u : 0u;  // 1 + kind, 0: none
     const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     uint32_t mine = 0;
@@ -815,19 +771,16 @@ __global__ void wf_check(WfDev W, uint32_t* go_out, uint32_t conditional) {
     W.rays[0] += active;
     W.rays[1] += c[kCntShadow];
     const uint32_t it = ++c[kCntIter];
-    bool go = active > 0u || c[kCntHeld] > 0u;
+    bool go = active > 0u;
     if (go && it >= W.max_iters) {
         atomicOr(W.status, NOOR_DEV_WAIT_TIMEOUT);
         go = false;
     }
     if (!go) W.rays[2] += *W.work_next < W.total ? *W.work_next : W.total;
-    // the shadow queue's length and take counter stay for the next
-    // iteration's shadow stage (wf_bin clears them after it)
-    for (int k = 0; k < kKinds; ++k) c[k] = 0u;
-    c[kCntActive] = 0u;
+    for (int k = 0; k <= kCntActive; ++k) c[k] = 0u;
+    c[kCntTake] = 0u;
     c[kCntCam] = 0u;
     c[kCntTakeExt] = 0u;
-    c[kCntHeld] = 0u;
     if (conditional)
         cudaGraphSetConditional(W.cond, go ? 1u : 0u);
     else
@@ -862,14 +815,8 @@ struct WavefrontState {
     // launch (slot buffers, sizes, parameters) is the same
     cudaGraphExec_t exec = nullptr;
     uint64_t graph_key[10] = {};
-    // the second stream the shadow stage runs on beside regen
-    cudaStream_t side = nullptr;
-    cudaEvent_t fork = nullptr, join = nullptr;
     ~WavefrontState() {
         if (exec) cudaGraphExecDestroy(exec);
-        if (fork) cudaEventDestroy(fork);
-        if (join) cudaEventDestroy(join);
-        if (side) cudaStreamDestroy(side);
         for (void* p : bufs) cudaFree(p);
         if (films) cudaFree(films);
         if (frames_dev) cudaFree(frames_dev);
@@ -952,51 +899,28 @@ static uint32_t shade_launches(const WfDev& W, const WfLaunch& L) {
     return W.sort ? (uint32_t)__builtin_popcount(L.kinds & ((1u << kKinds) - 1u)) : 1u;
 }
 
-// Events that let the shadow stage run on a second stream beside regen
-struct WfSide {
-    cudaStream_t stream;
-    cudaEvent_t fork, join;
-};
-
-// One iteration: the shadow stage of the iteration before (its queue, left
-// by the last shade) beside regen, then extension ordering, extend (which
-// folds the shadowed light into the paths), shade with its queue binning,
-// shadow ordering and the stop test.  With `side` the shadow stage runs on
-// the second stream and extend waits for it; without, the stages run in
-// sequence.  With `ev` (kWfStages + 1 events, sequence only) ev[0] is
-// recorded first and ev[j + 1] after the j-th stage run, in the order
-// shadow, regen, extension ordering, extend, shade, shadow ordering, stop
-// test (kWfRunOrder).
-constexpr int kWfRunOrder[kWfStages] = {5, 0, 1, 2, 3, 4, 6};  // stage index of each run
+// one iteration; with `ev` (kWfStages + 1 events), records ev[0] before the
+// first stage and ev[k + 1] after stage k (regen, extension ordering,
+// extend, shade with its queue binning, shadow ordering, shadow, stop test)
 static cudaError_t wf_iteration(const WfDev& W, const WfLaunch& L, cudaStream_t s, bool conditional,
-                                uint32_t* go_out, const WfSide* side, cudaEvent_t* ev = nullptr) {
+                                uint32_t* go_out, cudaEvent_t* ev = nullptr) {
     if (ev) cudaEventRecord(ev[0], s);
-    if (side) {
-        cudaEventRecord(side->fork, s);
-        cudaStreamWaitEvent(side->stream, side->fork, 0);
-        L.shadow<<<L.grid_queue, L.block, L.smem, side->stream>>>(W, L.scene);
-        cudaEventRecord(side->join, side->stream);
-    } else {
-        L.shadow<<<L.grid_queue, L.block, L.smem, s>>>(W, L.scene);
-    }
-    if (ev) cudaEventRecord(ev[1], s);
     if (L.diff)
         wf_regen<true><<<(W.cap + kRegenBlock - 1) / kRegenBlock, kRegenBlock, 0, s>>>(W);
     else
         wf_regen<false><<<(W.cap + kRegenBlock - 1) / kRegenBlock, kRegenBlock, 0, s>>>(W);
-    if (side) cudaStreamWaitEvent(s, side->join, 0);
-    if (ev) cudaEventRecord(ev[2], s);
+    if (ev) cudaEventRecord(ev[1], s);
     if (W.level >= 2) {
         L.ext_key<<<(W.cap + kBinBlock - 1) / kBinBlock, kBinBlock, 0, s>>>(W, L.scene);
         wf_bucket_scan<<<1, kScanThreads, 0, s>>>(W);
         wf_ext_scatter<<<(W.cap + kBinBlock - 1) / kBinBlock, kBinBlock, 0, s>>>(W);
     }
-    if (ev) cudaEventRecord(ev[3], s);
+    if (ev) cudaEventRecord(ev[2], s);
     if (W.level >= 2)
         L.extend<<<L.grid_queue, L.block, L.smem, s>>>(W, L.scene);
     else
         L.extend<<<L.grid_slots, L.block, L.smem, s>>>(W, L.scene);
-    if (ev) cudaEventRecord(ev[4], s);
+    if (ev) cudaEventRecord(ev[3], s);
     wf_bin<<<(W.cap + kBinBlock - 1) / kBinBlock, kBinBlock, 0, s>>>(W);
     const int nk = W.sort ? kKinds : 1;
     for (int k = 0; k < nk; ++k) {
@@ -1010,12 +934,14 @@ static cudaError_t wf_iteration(const WfDev& W, const WfLaunch& L, cudaStream_t 
         else
             wf_shade<false><<<L.grid_queue, 256, 0, s>>>(W, (uint32_t)k);
     }
-    if (ev) cudaEventRecord(ev[5], s);
+    if (ev) cudaEventRecord(ev[4], s);
     if (W.level >= 3) {
         L.shadow_key<<<L.grid_queue, 256, 0, s>>>(W, L.scene);
         wf_bucket_scan<<<1, kScanThreads, 0, s>>>(W);
         wf_shadow_scatter<<<L.grid_queue, 256, 0, s>>>(W);
     }
+    if (ev) cudaEventRecord(ev[5], s);
+    L.shadow<<<L.grid_queue, L.block, L.smem, s>>>(W, L.scene);
     if (ev) cudaEventRecord(ev[6], s);
     wf_check<<<1, 1, 0, s>>>(W, go_out, conditional ? 1u : 0u);
     if (ev) cudaEventRecord(ev[7], s);
@@ -1120,13 +1046,6 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
         (total + cap - 1) / cap * (max_bounces + 2) + 4 * (max_bounces + 2) + 64, 1u << 30);
     if (P.max_iterations) W.max_iters = std::min(W.max_iters, P.max_iterations);
 
-    if (!WS.side) {
-        cudaError_t se = cudaStreamCreateWithFlags(&WS.side, cudaStreamNonBlocking);
-        if (se == cudaSuccess) se = cudaEventCreateWithFlags(&WS.fork, cudaEventDisableTiming);
-        if (se == cudaSuccess) se = cudaEventCreateWithFlags(&WS.join, cudaEventDisableTiming);
-        if (se != cudaSuccess) return cuda_fail(se, "wavefront side stream");
-    }
-    const WfSide side{WS.side, WS.fork, WS.join};
     WfLaunch L;
     L.block = (int)block;
     // room for the four-wide trees' stacks as well as the binary one's
@@ -1233,7 +1152,7 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
                 cudaGraph_t body = cp.conditional.phGraph_out[0];
                 e = cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
                 if (e == cudaSuccess) {
-                    cudaError_t e2 = wf_iteration(W, L, s, true, nullptr, &side);
+                    cudaError_t e2 = wf_iteration(W, L, s, true, nullptr);
                     e = cudaStreamEndCapture(s, &body);
                     if (e == cudaSuccess) e = e2;
                 }
@@ -1264,18 +1183,18 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
         }
         const uint32_t nk = shade_launches(W, L) + (W.level >= 2 ? 3 : 0) + (W.level >= 3 ? 3 : 0);
         for (uint32_t it = 0; e == cudaSuccess && it < W.max_iters && active; ++it) {
-            e = wf_iteration(W, L, s, false, WS.active_host_dev, prof ? nullptr : &side, prof ? ev : nullptr);
+            e = wf_iteration(W, L, s, false, WS.active_host_dev, prof ? ev : nullptr);
             if (e == cudaSuccess) e = cudaMemcpyAsync(&active, WS.active_host_dev, 4, cudaMemcpyDeviceToHost, s);
             if (e == cudaSuccess) e = cudaStreamSynchronize(s);
             C.launches += 5 + nk;
             if (prof && e == cudaSuccess) {
                 const uint32_t launches[kWfStages] = {1u, W.level >= 2 ? 3u : 0u, 1u, shade_launches(W, L) + 1u,
                                                       W.level >= 3 ? 3u : 0u, 1u, 1u};
-                for (int j = 0; j < kWfStages; ++j) {
+                for (int k = 0; k < kWfStages; ++k) {
                     float ms = 0.0f;
-                    cudaEventElapsedTime(&ms, ev[j], ev[j + 1]);
-                    prof->ms[kWfRunOrder[j]] += ms;
-                    prof->launches[kWfRunOrder[j]] += launches[kWfRunOrder[j]];
+                    cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
+                    prof->ms[k] += ms;
+                    prof->launches[k] += launches[k];
                 }
                 ++prof->iterations;
             }
