@@ -597,8 +597,10 @@ NB_D void push_shadow(const WfDev& W, uint32_t slot, uint32_t which, const Shado
 // conductor and Fresnel specular (those lobes' code is left out).  DIFF:
 // some scene has bump maps; its rays' differentials are read, used and
 // passed on as the megakernel's DIFF specialisation does.
-template <bool EXT, bool DIFF = false>
-__global__ void __launch_bounds__(256, NB_SHADE_MIN_BLOCKS) wf_shade(WfDev W, uint32_t kind) {
+// MULTI false: every frame of the launch uses scene S1 (a kernel parameter,
+// read through the constant cache instead of the scene table)
+template <bool EXT, bool DIFF = false, bool MULTI = true>
+__global__ void __launch_bounds__(256, NB_SHADE_MIN_BLOCKS) wf_shade(WfDev W, DevScene S1, uint32_t kind) {
     const uint32_t n = W.counters[kind];
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint32_t slot = W.qshade[kind * W.cap + i];
@@ -607,7 +609,7 @@ __global__ void __launch_bounds__(256, NB_SHADE_MIN_BLOCKS) wf_shade(WfDev W, ui
         const uint2 h2 = W.hit2[slot];
         const uint32_t fi = fbits(ow.w);
         const WfFrameDev& F = W.frames[fi];
-        const DevScene& S = W.scenes[F.scene];
+        const DevScene& S = MULTI ? W.scenes[F.scene] : S1;
         const float3 o = f3(ow.x, ow.y, ow.z), d = f3(dw.x, dw.y, dw.z);
         float3 beta = f3(bw.x, bw.y, bw.z);
         const uint32_t bb = fbits(bw.w);
@@ -885,6 +887,7 @@ struct WfLaunch {
     bool env_ref;           // ... samples its environment as the reference does
     bool tex;               // ... reads textures per hit (image maps, alpha, bump)
     bool diff;              // ... has bump maps: rays carry differentials
+    bool multi;             // the frames use more than one scene
 };
 
 // NOOR_TRAVERSAL_AUTO takes the four-wide tree for the shadow rays of scenes
@@ -928,11 +931,13 @@ static cudaError_t wf_iteration(const WfDev& W, const WfLaunch& L, cudaStream_t 
         if (W.sort && !((L.kinds >> k) & 1u)) continue;
         // sorted queues 0 and 1 hold Lambert and conductor hits only
         if (L.diff)
-            wf_shade<true, true><<<L.grid_queue, 256, 0, s>>>(W, (uint32_t)k);
+            wf_shade<true, true><<<L.grid_queue, 256, 0, s>>>(W, L.scene, (uint32_t)k);
         else if (L.ext && !(W.sort && k < 2 && !L.ext_lights && !L.env_ref && !L.tex))
-            wf_shade<true><<<L.grid_queue, 256, 0, s>>>(W, (uint32_t)k);
+            wf_shade<true><<<L.grid_queue, 256, 0, s>>>(W, L.scene, (uint32_t)k);
+        else if (L.multi)
+            wf_shade<false><<<L.grid_queue, 256, 0, s>>>(W, L.scene, (uint32_t)k);
         else
-            wf_shade<false><<<L.grid_queue, 256, 0, s>>>(W, (uint32_t)k);
+            wf_shade<false, false, false><<<L.grid_queue, 256, 0, s>>>(W, L.scene, (uint32_t)k);
     }
     if (ev) cudaEventRecord(ev[4], s);
     if (W.level >= 3) {
@@ -1105,6 +1110,7 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
         else NB_TRAV(NOOR_ISECT_REF_WALD, false);
     }
 #undef NB_TRAV
+    L.multi = multi;
     L.shadow_key = multi ? wf_shadow_key<true> : wf_shadow_key<false>;
     L.ext_key = multi ? wf_ext_key<true> : wf_ext_key<false>;
     for (WfTravKernel k : {L.extend, L.shadow}) {
