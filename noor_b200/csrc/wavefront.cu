@@ -1278,7 +1278,7 @@ extern "C" int noor_wavefront_counters(uint64_t counters[3], int reset) {
 
 // Autotuner: coordinate descent on the launch parameters, each candidate
 // timed by one device-timed render of the batch: the slot count first
-// (2^18 .. 2^23, none beyond twice the batch's paths), then the block size
+// (2^18 .. 2^24, none beyond twice the batch's paths), then the block size
 // (32, 64, 128), then the sort granularity (0 .. 3), then the trees (binary,
 // four-wide, four-wide for shadow rays only), then the slot count again
 // around the choices made; the fastest seen wins.
@@ -1292,7 +1292,7 @@ extern "C" int noor_wavefront_autotune(const noor_wf_frame* frames, uint32_t n_f
     for (uint32_t i = 0; i < n_frames && frames; ++i)
         paths += (unsigned long long)frames[i].width * frames[i].height * frames[i].spp;
     std::vector<uint32_t> caps;
-    for (uint32_t c = 1u << 18; c <= (1u << 23); c <<= 1)
+    for (uint32_t c = 1u << 18; c <= (1u << 24); c <<= 1)
         if (c == (1u << 18) || c <= 2 * paths) caps.push_back(c);
     noor_wf_params bp{128, caps.back() >= (1u << 22) ? (1u << 22) : caps.back(), 1, best->use_graph};
     float bms = 3.4e38f;
