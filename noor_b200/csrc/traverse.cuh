@@ -15,11 +15,6 @@
 
 namespace nb {
 
-// 1: any-hit walks take top-level children far side first
-#ifndef NB_ANY_TOP_FAR_FIRST
-#define NB_ANY_TOP_FAR_FIRST 0
-#endif
-
 // ray in the space of the BVH level being traversed
 struct TRay {
     float3 o, d, inv;
@@ -474,9 +469,7 @@ NB_D bool trace_any(const DevScene& S, const float3& o, const float3& d, float t
             if (!(hi.w & kNodeKindMask)) {
                 if (top + 1 > st.cap) { atomicOr(status, NOOR_DEV_STACK_OVERFLOW); return false; }
                 const uint32_t axis = hi.w & NOOR_AXIS_MASK;
-                // top-level nodes far child first (as trace_any4)
-                const bool neg = ((lr.neg >> axis) & 1u) ^
-                                 (NB_ANY_TOP_FAR_FIRST && (hi.w & NOOR_MESH_INNER_MASK) ? 1u : 0u);
+                const bool neg = (lr.neg >> axis) & 1u;
                 st.base[top * st.stride] = neg ? ni + 1 : lo.w;
                 ++top;
                 next = neg ? lo.w : ni + 1;
@@ -593,7 +586,7 @@ NB_D uint32_t slab4(const TRay& r, const DevNode4* nd, float tmax) {
 // node's order table), the first into `next`, the rest pushed so that they
 // come off the stack in order.  False on a stack overflow.
 NB_D bool wide_visit(const DevNode4* nd, const uint4& meta, const TRay& r, float tmax, const SmemStack& st, int cap,
-                     int& top, uint32_t& next, uint32_t* status, uint32_t flip = 0u) {
+                     int& top, uint32_t& next, uint32_t* status) {
     const uint4 cw = __ldg(&nd->child);
     uint32_t inc = slab4(r, nd, tmax);
 #pragma unroll
@@ -603,8 +596,7 @@ NB_D bool wide_visit(const DevNode4* nd, const uint4& meta, const TRay& r, float
         else if ((w & (kWRef | kWUntested)) == (kWRef | kWUntested)) inc |= 1u << s;
     }
     if (!inc) return true;
-    // flip 7: the order of the opposite octant, which is this one reversed
-    const uint32_t oct = (r.neg ^ flip) & 7u;
+    const uint32_t oct = r.neg & 7u;
     const uint32_t order = ((oct & 4u) ? meta.z : meta.y) >> (8u * (oct & 3u));
     // last in order first: each taken word pushes the one held before it
 #pragma unroll
@@ -700,11 +692,7 @@ NB_D int any4_step(Any4& a, const DevScene& S, const SmemStack& st, uint32_t* st
                 a.wtw = true;
             }
         }
-        // top-level entries far side first: an occluder other than the
-        // instance the ray leaves is met before that instance's own tree
-        // (any order gives the same answer)
-        const uint32_t flip = (NB_ANY_TOP_FAR_FIRST && (meta.x & kW4World)) ? 7u : 0u;
-        if (!wide_visit(nd, meta, a.lr, a.tmax, st, cap, a.top, a.next, status, flip)) return kAnyFailed;
+        if (!wide_visit(nd, meta, a.lr, a.tmax, st, cap, a.top, a.next, status)) return kAnyFailed;
     } else {
         const uint32_t ni = cur & kWIndex;
         const DevNode* nd = S.nodes + ni;
