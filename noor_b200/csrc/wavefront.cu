@@ -90,7 +90,10 @@ constexpr int kBuckets = 8 << (3 * kCellBits);
 constexpr int kScanThreads = 1024;
 
 // block sizes of the slot sweeps (one block-wide atomic per counter)
-constexpr int kRegenBlock = 512;
+#ifndef NB_REGEN_BLOCK
+#define NB_REGEN_BLOCK 512
+#endif
+constexpr int kRegenBlock = NB_REGEN_BLOCK;
 constexpr int kBinBlock = 1024;
 
 struct WfDev {
