@@ -259,10 +259,9 @@ __global__ void __launch_bounds__(kRegenBlock) wf_regen(WfDev W) {
     const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = slot < W.cap;
     uint32_t st = kFree;
-    bool fin = false, sky = false;
-    float4 Lw = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     if (valid) {
         st = W.state[slot];
+        float4 Lw;
         if (st & kPend) {
             // L += beta * (c0' + c1') with c' = c if its shadow ray was
             // unblocked, as the megakernel adds its direct lighting
@@ -279,11 +278,18 @@ __global__ void __launch_bounds__(kRegenBlock) wf_regen(WfDev W) {
             if ((st & kLifeMask) == kActive) W.L[slot] = Lw;
         }
         if ((st & kLifeMask) == kFinishing) {
-            // the film write comes after the block has taken its work items,
-            // so that taking them does not wait for the film atomics
             if (!(st & kPend)) Lw = W.L[slot];
-            fin = true;
-            sky = (st & kSkySeen) != 0u;
+            const uint32_t fi = fbits(W.o[slot].w);
+            const uint32_t pix = fbits(W.d[slot].w);
+            const WfFrameDev& F = W.frames[fi];
+            if (st & kSkySeen) {
+                const float4 bw = W.beta[slot], dw = W.d[slot];
+                const float3 c = f3(bw.x, bw.y, bw.z) * env_eval<true>(W.scenes[F.scene], normalize_fast(f3(dw.x, dw.y, dw.z)));
+                Lw.x += c.x;
+                Lw.y += c.y;
+                Lw.z += c.z;
+            }
+            film_add3(F.sum + pix, F.comp + pix, clamp3(f3(Lw.x, Lw.y, Lw.z), 0.0f, 100.0f));
             st = kFree;
         }
         st &= kLifeMask;
@@ -303,20 +309,6 @@ __global__ void __launch_bounds__(kRegenBlock) wf_regen(WfDev W) {
         block_base = tot ? atomicAdd(W.work_next, (unsigned long long)tot) : 0ull;
     }
     __syncthreads();
-    if (fin) {
-        // the finished path to its frame's film, before the slot takes a new one
-        const uint32_t fi = fbits(W.o[slot].w);
-        const uint32_t pix = fbits(W.d[slot].w);
-        const WfFrameDev& F = W.frames[fi];
-        if (sky) {
-            const float4 bw = W.beta[slot], dw = W.d[slot];
-            const float3 c = f3(bw.x, bw.y, bw.z) * env_eval<true>(W.scenes[F.scene], normalize_fast(f3(dw.x, dw.y, dw.z)));
-            Lw.x += c.x;
-            Lw.y += c.y;
-            Lw.z += c.z;
-        }
-        film_add3(F.sum + pix, F.comp + pix, clamp3(f3(Lw.x, Lw.y, Lw.z), 0.0f, 100.0f));
-    }
     if (need) {
         const unsigned long long k = block_base + warp_off[wid] + __popc(ball & lanes_below());
         if (k < W.total) {
