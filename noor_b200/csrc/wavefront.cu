@@ -73,9 +73,8 @@ enum : int {
     kCntActive = kKinds + 1,   // slots holding a path after regen (= rays extend traces)
     kCntIter = kKinds + 2,     // iterations run
     kCntTake = kKinds + 3,     // shadow queue entries taken by wf_shadow's warps
-    kCntCam = kKinds + 4,      // camera rays in the extension order (sort level 2)
-    kCntTakeExt = kKinds + 5,  // extension order entries taken by wf_extend's warps
-    kCntWords = kKinds + 6
+    kCntTakeExt = kKinds + 4,  // extension order entries taken by wf_extend's warps
+    kCntWords = kKinds + 5
 };
 
 // Ray ordering (sort levels 2 and 3): a counting sort of rays into buckets
@@ -114,13 +113,15 @@ struct WfDev {
     float4* sh_o;           // origin, tmax (by queue entry)
     float4* sh_d;           // direction
     uint32_t* counters;     // kCntWords words
-    uint32_t* bkt_cnt;      // kBuckets bucket sizes (zero between passes)
+    uint32_t* bkt_cnt;      // kBuckets extension-ray bucket sizes (counted by shade for the next iteration)
     uint32_t* bkt_off;      // kBuckets bucket offsets, advanced by the scatter
+    uint32_t* sh_bkt_cnt;   // the same for the shadow queue (sort level 3)
+    uint32_t* sh_bkt_off;
     uint32_t* sh_key;       // bucket of each shadow queue entry
     uint32_t* sh_perm;      // shadow queue entries in bucket order
     uint32_t* ext_key;      // bucket of each slot's secondary ray
     uint32_t* ext_perm;     // camera-ray slots in slot order, then (at cap) secondary-ray slots in bucket order
-    unsigned long long* work_next;
+    unsigned long long* work_next;  // [0] next work item, [1] the first one of this iteration
     unsigned long long* rays;  // [ext, shadow, paths], added up by wf_check
     uint32_t* status;
     const WfFrameDev* frames;
@@ -259,8 +260,10 @@ __global__ void __launch_bounds__(kRegenBlock) wf_regen(WfDev W) {
     const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = slot < W.cap;
     uint32_t st = kFree;
+    bool cont = false;  // a continuing path: shade gave its next ray a bucket
     if (valid) {
         st = W.state[slot];
+        cont = (st & kLifeMask) == kActive;
         float4 Lw;
         if (st & kPend) {
             // L += beta * (c0' + c1') with c' = c if its shadow ray was
@@ -339,8 +342,11 @@ __global__ void __launch_bounds__(kRegenBlock) wf_regen(WfDev W) {
             W.beta[slot] = make_float4(1.0f, 1.0f, 1.0f, bitsf(0u));
             W.L[slot] = make_float4(0.0f, 0.0f, 0.0f, bitsf(rng.s));
             st = kActive;
+            // sort level 2: the camera rays in work-item order
+            if (W.level >= 2) W.ext_perm[(uint32_t)(k - W.work_next[1])] = slot;
         }
     }
+    if (valid && !cont && W.level >= 2) W.ext_key[slot] = 0xFFFFFFFFu;
     if (valid) W.state[slot] = st;
     const int nact = __syncthreads_count(valid && st == kActive);
     if (threadIdx.x == 0 && nact) atomicAdd(W.counters + kCntActive, (uint32_t)nact);
@@ -384,15 +390,15 @@ NB_D uint32_t bucket_add(uint32_t* counters, uint32_t key) {
 
 // exclusive scan of the bucket sizes into offsets (one block); the sizes
 // are cleared for the next pass
-__global__ void __launch_bounds__(kScanThreads) wf_bucket_scan(WfDev W) {
+__global__ void __launch_bounds__(kScanThreads) wf_bucket_scan(uint32_t* cnt, uint32_t* off) {
     constexpr int per = kBuckets / kScanThreads;
     __shared__ uint32_t part[kScanThreads];
     const int t = threadIdx.x;
     uint32_t v[per];
     uint32_t sum = 0;
     for (int k = 0; k < per; ++k) {
-        v[k] = W.bkt_cnt[t * per + k];
-        W.bkt_cnt[t * per + k] = 0u;
+        v[k] = cnt[t * per + k];
+        cnt[t * per + k] = 0u;
         sum += v[k];
     }
     part[t] = sum;
@@ -405,7 +411,7 @@ __global__ void __launch_bounds__(kScanThreads) wf_bucket_scan(WfDev W) {
     }
     uint32_t run = part[t] - sum;
     for (int k = 0; k < per; ++k) {
-        W.bkt_off[t * per + k] = run;
+        off[t * per + k] = run;
         run += v[k];
     }
 }
@@ -454,45 +460,11 @@ NB_D void extend_one(const WfDev& W, const DevScene& S, uint32_t slot, const flo
     W.state[slot] = kActive | ((kind + 1u) << kKindShift);  // wf_bin queues it for shading
 }
 
-// Sort level 2: the extension order.  Camera rays (bounce 0) are compacted
-// in slot order, block by block, so that the consecutive pixels regen gave
-// consecutive free slots stay together; secondary rays get their bucket.
-// After wf_bucket_scan, wf_ext_scatter places the secondary rays at cap + 
-// their position in bucket order.
-template <bool MULTI>
-__global__ void __launch_bounds__(kBinBlock) wf_ext_key(WfDev W, DevScene S1) {
-    __shared__ uint32_t woff[kBinBlock / 32];
-    __shared__ uint32_t base;
-    const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
-    bool cam = false, sec = false;
-    if (slot < W.cap && W.state[slot] == kActive) {
-        cam = (fbits(W.beta[slot].w) & 0xFFFFu) == 0u;
-        sec = !cam;
-    }
-    const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const uint32_t ball = __ballot_sync(0xFFFFFFFFu, cam);
-    if (lane == 0) woff[wid] = __popc(ball);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        uint32_t tot = 0;
-        for (int w = 0; w < kBinBlock / 32; ++w) {
-            const uint32_t c = woff[w];
-            woff[w] = tot;
-            tot += c;
-        }
-        base = tot ? atomicAdd(W.counters + kCntCam, tot) : 0u;
-    }
-    __syncthreads();
-    if (cam) W.ext_perm[base + woff[wid] + __popc(ball & lanes_below())] = slot;
-    uint32_t key = 0xFFFFFFFFu;
-    if (sec) {
-        const float4 ow = W.o[slot], dw = W.d[slot];
-        const DevScene& S = MULTI ? W.scenes[W.frames[fbits(ow.w)].scene] : S1;
-        key = ray_bucket(S, f3(ow.x, ow.y, ow.z), f3(dw.x, dw.y, dw.z));
-        bucket_add(W.bkt_cnt, key);
-    }
-    if (slot < W.cap) W.ext_key[slot] = key;
-}
+// Sort level 2: the extension order.  Regen lists the camera rays it makes
+// in work-item order (consecutive pixels stay together); shade gives each
+// continuing path's next ray its bucket and counts it.  After
+// wf_bucket_scan, wf_ext_scatter places the secondary rays at cap + their
+// position in bucket order.
 __global__ void __launch_bounds__(kBinBlock) wf_ext_scatter(WfDev W) {
     const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= W.cap) return;
@@ -537,7 +509,9 @@ __global__ void __launch_bounds__(NB_TRAV_THREADS, WIDE ? NB_TRAV_MIN_BLOCKS_WID
     extern __shared__ uint32_t smem[];
     SmemStack stk{smem + threadIdx.x, (int)blockDim.x, W.stack_cap};
     if (W.level >= 2) {
-        const uint32_t nc = W.counters[kCntCam], n = W.counters[kCntActive];
+        // camera rays: the work items regen took this iteration
+        const unsigned long long wn = W.work_next[0] < W.total ? W.work_next[0] : W.total;
+        const uint32_t nc = (uint32_t)(wn - W.work_next[1]), n = W.counters[kCntActive];
         const uint32_t lane = threadIdx.x & 31;
         for (;;) {
             uint32_t base = 0;
@@ -699,7 +673,14 @@ __global__ void __launch_bounds__(256, NB_SHADE_MIN_BLOCKS) wf_shade(WfDev W, De
             W.o[slot] = make_float4(no.x, no.y, no.z, ow.w);
             W.d[slot] = make_float4(wi.x, wi.y, wi.z, dw.w);
             W.beta[slot] = make_float4(beta.x, beta.y, beta.z, bitsf(nb_ | (spec ? 1u << 16 : 0u)));
-            if (nb_ >= F.bounces) st = kFinishing;
+            if (nb_ >= F.bounces) {
+                st = kFinishing;
+            } else if (W.level >= 2) {
+                // the next extension's order: the ray's bucket, counted here
+                const uint32_t key = ray_bucket(S, no, wi);
+                W.ext_key[slot] = key;
+                bucket_add(W.bkt_cnt, key);
+            }
         }
         W.L[slot] = make_float4(Lw.x, Lw.y, Lw.z, bitsf(rng.s));
         W.state[slot] = st | (pend ? kPend : 0u);
@@ -717,13 +698,13 @@ __global__ void wf_shadow_key(WfDev W, DevScene S1) {
         const DevScene& S = MULTI ? W.scenes[W.frames[fbits(W.o[W.qshadow[i] >> 1].w)].scene] : S1;
         const uint32_t key = ray_bucket(S, f3(so.x, so.y, so.z), f3(sd.x, sd.y, sd.z));
         W.sh_key[i] = key;
-        bucket_add(W.bkt_cnt, key);
+        bucket_add(W.sh_bkt_cnt, key);
     }
 }
 __global__ void wf_shadow_scatter(WfDev W) {
     const uint32_t n = W.counters[kCntShadow];
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        W.sh_perm[bucket_add(W.bkt_off, W.sh_key[i])] = i;
+        W.sh_perm[bucket_add(W.sh_bkt_off, W.sh_key[i])] = i;
 }
 
 // Any hit for each queued shadow ray; a blocked one cancels its pending
@@ -782,9 +763,9 @@ __global__ void wf_check(WfDev W, uint32_t* go_out, uint32_t conditional) {
         go = false;
     }
     if (!go) W.rays[2] += *W.work_next < W.total ? *W.work_next : W.total;
+    W.work_next[1] = W.work_next[0] < W.total ? W.work_next[0] : W.total;
     for (int k = 0; k <= kCntActive; ++k) c[k] = 0u;
     c[kCntTake] = 0u;
-    c[kCntCam] = 0u;
     c[kCntTakeExt] = 0u;
     if (conditional)
         cudaGraphSetConditional(W.cond, go ? 1u : 0u);
@@ -861,12 +842,14 @@ static int wf_ensure(Context& C, uint32_t cap) {
         (rc = wf_alloc(S, (void**)&W.counters, kCntWords * 4)) || (rc = wf_alloc(S, (void**)&W.work_next, 16)) ||
         (rc = wf_alloc(S, (void**)&W.rays, 32)) || (rc = wf_alloc(S, (void**)&W.bkt_cnt, kBuckets * 4)) ||
         (rc = wf_alloc(S, (void**)&W.bkt_off, kBuckets * 4)) || (rc = wf_alloc(S, (void**)&W.sh_key, 2 * n * 4)) ||
+        (rc = wf_alloc(S, (void**)&W.sh_bkt_cnt, kBuckets * 4)) || (rc = wf_alloc(S, (void**)&W.sh_bkt_off, kBuckets * 4)) ||
         (rc = wf_alloc(S, (void**)&W.sh_perm, 2 * n * 4)) || (rc = wf_alloc(S, (void**)&W.ext_key, n * 4)) ||
         (rc = wf_alloc(S, (void**)&W.ext_perm, 2 * n * 4)))
         return rc;
     cudaError_t e = cudaMalloc((void**)&S.active_host_dev, 16);
     if (e == cudaSuccess) e = cudaMemset(W.rays, 0, 32);
     if (e == cudaSuccess) e = cudaMemset(W.bkt_cnt, 0, kBuckets * 4);
+    if (e == cudaSuccess) e = cudaMemset(W.sh_bkt_cnt, 0, kBuckets * 4);
     if (e != cudaSuccess) return cuda_fail(e, "wavefront buffers");
     S.cap = cap;
     return NOOR_OK;
@@ -882,7 +865,6 @@ struct WfLaunch {
     uint32_t grid_queue;    // grid-stride stages
     WfTravKernel extend;
     WfTravKernel shadow;
-    WfTravKernel ext_key;      // sort level 2
     WfTravKernel shadow_key;   // sort level 3
     DevScene scene;         // the launch's scene when every frame uses the same one
     bool ext;               // some frame's scene has extra lobes or lights
@@ -917,8 +899,9 @@ static cudaError_t wf_iteration(const WfDev& W, const WfLaunch& L, cudaStream_t 
         wf_regen<false><<<(W.cap + kRegenBlock - 1) / kRegenBlock, kRegenBlock, 0, s>>>(W);
     if (ev) cudaEventRecord(ev[1], s);
     if (W.level >= 2) {
-        L.ext_key<<<(W.cap + kBinBlock - 1) / kBinBlock, kBinBlock, 0, s>>>(W, L.scene);
-        wf_bucket_scan<<<1, kScanThreads, 0, s>>>(W);
+        // secondary rays in bucket order (shade counted the buckets); camera
+        // rays were listed by regen
+        wf_bucket_scan<<<1, kScanThreads, 0, s>>>(W.bkt_cnt, W.bkt_off);
         wf_ext_scatter<<<(W.cap + kBinBlock - 1) / kBinBlock, kBinBlock, 0, s>>>(W);
     }
     if (ev) cudaEventRecord(ev[2], s);
@@ -945,7 +928,7 @@ static cudaError_t wf_iteration(const WfDev& W, const WfLaunch& L, cudaStream_t 
     if (ev) cudaEventRecord(ev[4], s);
     if (W.level >= 3) {
         L.shadow_key<<<L.grid_queue, 256, 0, s>>>(W, L.scene);
-        wf_bucket_scan<<<1, kScanThreads, 0, s>>>(W);
+        wf_bucket_scan<<<1, kScanThreads, 0, s>>>(W.sh_bkt_cnt, W.sh_bkt_off);
         wf_shadow_scatter<<<L.grid_queue, 256, 0, s>>>(W);
     }
     if (ev) cudaEventRecord(ev[5], s);
@@ -1038,6 +1021,9 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
     if (e == cudaSuccess) e = cudaMemsetAsync(W.state, 0, (size_t)cap * 4, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(W.counters, 0, kCntWords * 4, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(W.work_next, 0, 16, s);
+    // shade counts the next iteration's extension buckets: a render cut short
+    // by the iteration cap can leave counts behind
+    if (e == cudaSuccess) e = cudaMemsetAsync(W.bkt_cnt, 0, kBuckets * 4, s);
     if (e != cudaSuccess) return cuda_fail(e, "wavefront setup");
     W.status = C.status;
     W.frames = WS.frames_dev;
@@ -1115,7 +1101,6 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
 #undef NB_TRAV
     L.multi = multi;
     L.shadow_key = multi ? wf_shadow_key<true> : wf_shadow_key<false>;
-    L.ext_key = multi ? wf_ext_key<true> : wf_ext_key<false>;
     for (WfTravKernel k : {L.extend, L.shadow}) {
         e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem);
         if (e != cudaSuccess) return cuda_fail(e, "wavefront smem");
@@ -1190,14 +1175,14 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
             for (auto& x : ev)
                 if (e == cudaSuccess) e = cudaEventCreate(&x);
         }
-        const uint32_t nk = shade_launches(W, L) + (W.level >= 2 ? 3 : 0) + (W.level >= 3 ? 3 : 0);
+        const uint32_t nk = shade_launches(W, L) + (W.level >= 2 ? 2 : 0) + (W.level >= 3 ? 3 : 0);
         for (uint32_t it = 0; e == cudaSuccess && it < W.max_iters && active; ++it) {
             e = wf_iteration(W, L, s, false, WS.active_host_dev, prof ? ev : nullptr);
             if (e == cudaSuccess) e = cudaMemcpyAsync(&active, WS.active_host_dev, 4, cudaMemcpyDeviceToHost, s);
             if (e == cudaSuccess) e = cudaStreamSynchronize(s);
             C.launches += 5 + nk;
             if (prof && e == cudaSuccess) {
-                const uint32_t launches[kWfStages] = {1u, W.level >= 2 ? 3u : 0u, 1u, shade_launches(W, L) + 1u,
+                const uint32_t launches[kWfStages] = {1u, W.level >= 2 ? 2u : 0u, 1u, shade_launches(W, L) + 1u,
                                                       W.level >= 3 ? 3u : 0u, 1u, 1u};
                 for (int k = 0; k < kWfStages; ++k) {
                     float ms = 0.0f;
@@ -1223,7 +1208,7 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
     uint32_t iters = 0;
     cudaMemcpy(&iters, W.counters + kCntIter, 4, cudaMemcpyDeviceToHost);
     if (P.use_graph)
-        C.launches += (uint64_t)iters * (5 + shade_launches(W, L) + (W.level >= 2 ? 3 : 0) + (W.level >= 3 ? 3 : 0)) -
+        C.launches += (uint64_t)iters * (5 + shade_launches(W, L) + (W.level >= 2 ? 2 : 0) + (W.level >= 3 ? 3 : 0)) -
                       (uint64_t)W.max_iters;
     return NOOR_OK;
 }
