@@ -563,11 +563,17 @@ __global__ void __launch_bounds__(kBinBlock) wf_bin(WfDev W) {
 }
 
 // queues shadow ray `which` (0: light sample, 1: BSDF sample of MIS) of a slot
-NB_D void push_shadow(const WfDev& W, uint32_t slot, uint32_t which, const ShadowRay& sr) {
+NB_D void push_shadow(const WfDev& W, const DevScene& S, uint32_t slot, uint32_t which, const ShadowRay& sr) {
     const uint32_t i = queue_push(W.counters + kCntShadow);
     W.qshadow[i] = (slot << 1) | which;
     W.sh_o[i] = make_float4(sr.o.x, sr.o.y, sr.o.z, sr.tmax);
     W.sh_d[i] = make_float4(sr.d.x, sr.d.y, sr.d.z, 0.0f);
+    if (W.level >= 3) {
+        // sort level 3: the shadow ray's bucket, counted here
+        const uint32_t key = ray_bucket(S, sr.o, sr.d);
+        W.sh_key[i] = key;
+        bucket_add(W.sh_bkt_cnt, key);
+    }
 }
 
 // EXT false: the queue holds no material with a lobe beyond Lambert,
@@ -624,13 +630,13 @@ __global__ void __launch_bounds__(256, NB_SHADE_MIN_BLOCKS) wf_shade(WfDev W, De
         // beta * (c0' + c1') to L as the megakernel does
         const float3 c0 = light_sample_contrib<EXT>(S, m, I, rng, S.mis != 0, li, picked, sr);
         const bool has0 = !is_black(c0);
-        if (has0) push_shadow(W, slot, 0, sr);
+        if (has0) push_shadow(W, S, slot, 0, sr);
         float3 c1 = f3(0.0f);
         bool has1 = false;
         if (S.mis && picked) {
             c1 = bsdf_mis_contrib<EXT>(S, m, I, rng, li, sr);
             has1 = !is_black(c1);
-            if (has1) push_shadow(W, slot, 1, sr);
+            if (has1) push_shadow(W, S, slot, 1, sr);
         }
         const bool pend = has0 || has1;
         if (pend) {
@@ -687,20 +693,9 @@ __global__ void __launch_bounds__(256, NB_SHADE_MIN_BLOCKS) wf_shade(WfDev W, De
     }
 }
 
-// Sort level 3: bucket of every shadow queue entry (grid-stride over the
-// queue length the shade stage left), then, after wf_bucket_scan, its place
-// in bucket order.
-template <bool MULTI>
-__global__ void wf_shadow_key(WfDev W, DevScene S1) {
-    const uint32_t n = W.counters[kCntShadow];
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const float4 so = W.sh_o[i], sd = W.sh_d[i];
-        const DevScene& S = MULTI ? W.scenes[W.frames[fbits(W.o[W.qshadow[i] >> 1].w)].scene] : S1;
-        const uint32_t key = ray_bucket(S, f3(so.x, so.y, so.z), f3(sd.x, sd.y, sd.z));
-        W.sh_key[i] = key;
-        bucket_add(W.sh_bkt_cnt, key);
-    }
-}
+// Sort level 3: shade gave every shadow queue entry its bucket and counted
+// it; after wf_bucket_scan, each entry's place in bucket order (grid-stride
+// over the queue length the shade stage left).
 __global__ void wf_shadow_scatter(WfDev W) {
     const uint32_t n = W.counters[kCntShadow];
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
@@ -865,7 +860,6 @@ struct WfLaunch {
     uint32_t grid_queue;    // grid-stride stages
     WfTravKernel extend;
     WfTravKernel shadow;
-    WfTravKernel shadow_key;   // sort level 3
     DevScene scene;         // the launch's scene when every frame uses the same one
     bool ext;               // some frame's scene has extra lobes or lights
     bool ext_lights;        // ... has sphere, disk, point, spot or distant lights
@@ -927,7 +921,7 @@ static cudaError_t wf_iteration(const WfDev& W, const WfLaunch& L, cudaStream_t 
     }
     if (ev) cudaEventRecord(ev[4], s);
     if (W.level >= 3) {
-        L.shadow_key<<<L.grid_queue, 256, 0, s>>>(W, L.scene);
+        // shadow rays in bucket order (shade counted the buckets)
         wf_bucket_scan<<<1, kScanThreads, 0, s>>>(W.sh_bkt_cnt, W.sh_bkt_off);
         wf_shadow_scatter<<<L.grid_queue, 256, 0, s>>>(W);
     }
@@ -1024,6 +1018,7 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
     // shade counts the next iteration's extension buckets: a render cut short
     // by the iteration cap can leave counts behind
     if (e == cudaSuccess) e = cudaMemsetAsync(W.bkt_cnt, 0, kBuckets * 4, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(W.sh_bkt_cnt, 0, kBuckets * 4, s);
     if (e != cudaSuccess) return cuda_fail(e, "wavefront setup");
     W.status = C.status;
     W.frames = WS.frames_dev;
@@ -1100,7 +1095,6 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
     }
 #undef NB_TRAV
     L.multi = multi;
-    L.shadow_key = multi ? wf_shadow_key<true> : wf_shadow_key<false>;
     for (WfTravKernel k : {L.extend, L.shadow}) {
         e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem);
         if (e != cudaSuccess) return cuda_fail(e, "wavefront smem");
@@ -1175,7 +1169,7 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
             for (auto& x : ev)
                 if (e == cudaSuccess) e = cudaEventCreate(&x);
         }
-        const uint32_t nk = shade_launches(W, L) + (W.level >= 2 ? 2 : 0) + (W.level >= 3 ? 3 : 0);
+        const uint32_t nk = shade_launches(W, L) + (W.level >= 2 ? 2 : 0) + (W.level >= 3 ? 2 : 0);
         for (uint32_t it = 0; e == cudaSuccess && it < W.max_iters && active; ++it) {
             e = wf_iteration(W, L, s, false, WS.active_host_dev, prof ? ev : nullptr);
             if (e == cudaSuccess) e = cudaMemcpyAsync(&active, WS.active_host_dev, 4, cudaMemcpyDeviceToHost, s);
@@ -1183,7 +1177,7 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
             C.launches += 5 + nk;
             if (prof && e == cudaSuccess) {
                 const uint32_t launches[kWfStages] = {1u, W.level >= 2 ? 2u : 0u, 1u, shade_launches(W, L) + 1u,
-                                                      W.level >= 3 ? 3u : 0u, 1u, 1u};
+                                                      W.level >= 3 ? 2u : 0u, 1u, 1u};
                 for (int k = 0; k < kWfStages; ++k) {
                     float ms = 0.0f;
                     cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
@@ -1208,7 +1202,7 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
     uint32_t iters = 0;
     cudaMemcpy(&iters, W.counters + kCntIter, 4, cudaMemcpyDeviceToHost);
     if (P.use_graph)
-        C.launches += (uint64_t)iters * (5 + shade_launches(W, L) + (W.level >= 2 ? 2 : 0) + (W.level >= 3 ? 3 : 0)) -
+        C.launches += (uint64_t)iters * (5 + shade_launches(W, L) + (W.level >= 2 ? 2 : 0) + (W.level >= 3 ? 2 : 0)) -
                       (uint64_t)W.max_iters;
     return NOOR_OK;
 }
