@@ -208,6 +208,11 @@ def algorithmic_bytes(orc, cam, spp, isect, sample_pixels=20000, seed=0):
 # origin + direction (32 B) and the queue entry (4 B); writes the hit record
 # (16 B + 8 B) and one queue entry (4 B)
 EXTEND_SLOT_BYTES = 64.0
+# queue state the shadow kernel moves per ray besides the traversal: the
+# queue entry (4 B), its ray (32 B), the slot's frame word (16 B in a
+# multi-scene launch, counted always) and the pending contribution it may
+# cancel (16 B), rounded to the sector-aligned 72 B
+SHADOW_QUEUE_BYTES = 72.0
 # ncu DRAM bytes per extension ray of wf_extend, from the capture summarised
 # in profiles/wf_extend_sky.md (the line "dram_bytes_per_ext_ray: X")
 TRAFFIC_PROFILE = ROOT / "profiles" / "wf_extend_sky.md"
@@ -779,6 +784,10 @@ def main():
                 # the ncu capture is of the sky-lit scene
                 tr = profiled_traffic_per_ray() if args.workload == "sky" else None
                 traffic = tr * ext / args.steps / top_launches if tr else None
+            elif top_kernel == "wf_shadow":
+                # traversal bytes of the shadow rays + the queue state of every one
+                alg = counts["shadow_traversal_bytes_per_path"] * npaths + SHADOW_QUEUE_BYTES * shadow / args.steps
+                traffic = None
             else:
                 alg = per_path * npaths
                 traffic = None
