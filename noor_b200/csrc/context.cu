@@ -578,12 +578,16 @@ int upload_scene(Context& C, const noor_payload* P, const noor_hosek_sky* H, con
     if ((rc = st.alloc((void**)&b.cdf, chh * (cw + 1) * 4, "env cdf"))) return rc;
     if ((rc = st.alloc((void**)&b.row_int, chh * 4, "env rows"))) return rc;
     if ((rc = st.alloc((void**)&b.marg_cdf, (chh + 1) * 4, "env marginal"))) return rc;
+    if ((rc = st.alloc((void**)&b.guide, chh * (kDistGuide + 1) * 4, "env guides"))) return rc;
+    if ((rc = st.alloc((void**)&b.mguide, (kDistGuide + 1) * 4, "env marginal guide"))) return rc;
     if ((rc = st.alloc((void**)&b.scratch, (chh * (cw + 1) + 2 * chh + 2) * 8, "env scratch"))) return rc;
     if ((rc = st.alloc((void**)&b.marg_int_out, 16, "env integral"))) return rc;
     D.dist.func = b.func;
     D.dist.cdf = b.cdf;
     D.dist.row_int = b.row_int;
     D.dist.marg_cdf = b.marg_cdf;
+    D.dist.guide = b.guide;
+    D.dist.mguide = b.mguide;
     D.dist.w = b.w;
     D.dist.h = b.h;
     if ((rc = build_distribution(C, st))) return rc;

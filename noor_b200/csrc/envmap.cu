@@ -161,11 +161,37 @@ cudaError_t launch_env_func_from_sky(const DevHosek& H, int w, int h, float* fun
     return cudaGetLastError();
 }
 
+// Guide entries of CDF rows (row r of n + 1 values at cdf + r * (n + 1)):
+// entry k = largest i in [0, n] with cdf[i] <= k / kDistGuide (exact in
+// FP32: kDistGuide is a power of two), by the same search sample_1d runs
+__global__ void k_dist_guide(const float* cdf, int n, int rows, int* guide) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= rows * (kDistGuide + 1)) return;
+    const int r = t / (kDistGuide + 1), k = t % (kDistGuide + 1);
+    const float* c = cdf + (size_t)r * (n + 1);
+    const float u = (float)k / (float)kDistGuide;
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (c[mid] <= u)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    guide[t] = lo;
+}
+
 cudaError_t launch_env_cdf(const EnvBuild& b, cudaStream_t s) {
     k_row_cdf<<<b.h, kScanThreads, 0, s>>>(b.func, b.w, b.h, b.cdf, b.row_int, b.scratch);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     k_marg_cdf<<<1, kScanThreads, 0, s>>>(b.w, b.h, b.marg_cdf, b.scratch, b.marg_int_out);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (b.guide) {
+        const int nr = b.h * (kDistGuide + 1);
+        k_dist_guide<<<(nr + 255) / 256, 256, 0, s>>>(b.cdf, b.w, b.h, b.guide);
+        k_dist_guide<<<1, kDistGuide + 1, 0, s>>>(b.marg_cdf, b.h, 1, b.mguide);
+    }
     return cudaGetLastError();
 }
 

@@ -44,6 +44,8 @@ struct EnvBuild {
     float* marg_cdf;  // h+1
     double* scratch;  // h*(w+1) + h + 1 doubles
     float* marg_int_out;  // one float
+    int* guide;       // h*(kDistGuide+1) guide entries of the row CDFs
+    int* mguide;      // kDistGuide+1 of the marginal CDF
     int w, h;
 };
 // func from the env texels (luminance x sin(theta) per texel)

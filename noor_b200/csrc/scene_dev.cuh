@@ -153,11 +153,18 @@ inline DevCamera dev_camera(const noor_camera& c, uint32_t w, uint32_t h) {
 }
 
 // Piecewise-constant 2D distribution over the environment (row = theta).
+// Guide tables of a piecewise-constant distribution's CDFs: entry k of a
+// row is the largest index i with cdf[i] <= k / kDistGuide, so the inverse
+// CDF search for u only has to look between the entries around u *
+// kDistGuide (the same index a search over the whole row finds).
+constexpr int kDistGuide = 64;
 struct DevDist2D {
     const float* func;      // h * w
     const float* cdf;       // h * (w + 1)
     const float* row_int;   // h   (integral of each row's func)
     const float* marg_cdf;  // h + 1
+    const int* guide;       // h * (kDistGuide + 1), null: no guides
+    const int* mguide;      // kDistGuide + 1 over marg_cdf
     float marg_int;         // integral of row_int
     int w, h;
 };

@@ -1242,8 +1242,16 @@ NB_OUTLINE float rdist_pdf(const DevScene& S, float x, float y) {
 }
 
 // piecewise-constant 1D sampling over one CDF (PBRT-v3 Distribution1D)
-NB_D float sample_1d(const float* func, const float* cdf, int n, float integral, float u, float& pdf, int& off) {
+NB_D float sample_1d(const float* func, const float* cdf, int n, float integral, float u, float& pdf, int& off,
+                     const int* guide = nullptr) {
     int lo = 0, hi = n;  // largest i in [0, n] with cdf[i] <= u, clamped to [0, n-1]
+    if (guide) {
+        // that index lies between the guide entries one bin either side of
+        // u's (the bin of u * kDistGuide may be off by one in rounding)
+        const int k = min((int)(u * (float)kDistGuide), kDistGuide - 1);
+        lo = __ldg(&guide[max(k - 1, 0)]);
+        hi = __ldg(&guide[min(k + 2, kDistGuide)]);
+    }
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
         if (__ldg(&cdf[mid]) <= u)
@@ -1262,10 +1270,11 @@ NB_D float sample_1d(const float* func, const float* cdf, int n, float integral,
 NB_D float2 dist_sample(const DevDist2D& D, float u0, float u1, float& pdf) {
     float pv, pu;
     int row;
-    const float y = sample_1d(D.row_int, D.marg_cdf, D.h, D.marg_int, u1, pv, row);
+    const float y = sample_1d(D.row_int, D.marg_cdf, D.h, D.marg_int, u1, pv, row, D.mguide);
     int col;
     const float x = sample_1d(D.func + (size_t)row * D.w, D.cdf + (size_t)row * (D.w + 1), D.w,
-                              __ldg(&D.row_int[row]), u0, pu, col);
+                              __ldg(&D.row_int[row]), u0, pu, col,
+                              D.guide ? D.guide + (size_t)row * (kDistGuide + 1) : nullptr);
     pdf = pu * pv;
     return f2(x, y);
 }
