@@ -481,6 +481,7 @@ class WavefrontPath:
                 "wavefront": {"block": p.block_size, "slots": p.queue_capacity, "material_sort": p.sort_granularity,
                               "graph": p.use_graph,
                               "tree": ["auto", "binary", "four-wide", "four-wide shadow rays"][p.traversal],
+                              "shade_regs": p.shade_regs or 80,
                               "autotune_best_ms": self.tuned_ms}}
 
     def image(self):

@@ -684,6 +684,9 @@ typedef struct noor_wf_params {
     uint32_t traversal;         /* the trees the extension and shadow
                                  * stages walk (the same hits either way):
                                  * NOOR_TRAVERSAL_*                          */
+    uint32_t shade_regs;        /* registers per thread of the shading
+                                 * stage: 0 or 80 (24 warps per SM), 128
+                                 * (16 warps, no spills); the same results */
 } noor_wf_params;
 /* BINARY: both stages on the binary tree; WIDE: both on the four-wide tree
  * where every scene of the launch has one (noor_wide_tree_info);

@@ -193,7 +193,7 @@ class WfFrame(C.Structure):
 
 class WfParams(C.Structure):
     _fields_ = [("block_size", u32), ("queue_capacity", u32), ("sort_granularity", u32), ("use_graph", u32),
-                ("max_iterations", u32), ("traversal", u32)]
+                ("max_iterations", u32), ("traversal", u32), ("shade_regs", u32)]
 
 
 class WfProfile(C.Structure):

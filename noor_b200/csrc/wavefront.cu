@@ -582,8 +582,10 @@ NB_D void push_shadow(const WfDev& W, const DevScene& S, uint32_t slot, uint32_t
 // passed on as the megakernel's DIFF specialisation does.
 // MULTI false: every frame of the launch uses scene S1 (a kernel parameter,
 // read through the constant cache instead of the scene table)
-template <bool EXT, bool DIFF = false, bool MULTI = true>
-__global__ void __launch_bounds__(256, NB_SHADE_MIN_BLOCKS) wf_shade(WfDev W, DevScene S1, uint32_t kind) {
+// BLOCKS: resident 256-thread blocks per SM the kernel is built for (3: 80
+// registers, 2: 128, no spills; the launch parameters choose)
+template <bool EXT, bool DIFF = false, bool MULTI = true, int BLOCKS = NB_SHADE_MIN_BLOCKS>
+__global__ void __launch_bounds__(256, BLOCKS) wf_shade(WfDev W, DevScene S1, uint32_t kind) {
     const uint32_t n = W.counters[kind];
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint32_t slot = W.qshade[kind * W.cap + i];
@@ -867,6 +869,7 @@ struct WfLaunch {
     bool tex;               // ... reads textures per hit (image maps, alpha, bump)
     bool diff;              // ... has bump maps: rays carry differentials
     bool multi;             // the frames use more than one scene
+    bool shade_wide_regs;   // single-scene shade built for 128 registers
 };
 
 // NOOR_TRAVERSAL_AUTO takes the four-wide tree for the shadow rays of scenes
@@ -916,6 +919,8 @@ static cudaError_t wf_iteration(const WfDev& W, const WfLaunch& L, cudaStream_t 
             wf_shade<true><<<L.grid_queue, 256, 0, s>>>(W, L.scene, (uint32_t)k);
         else if (L.multi)
             wf_shade<false><<<L.grid_queue, 256, 0, s>>>(W, L.scene, (uint32_t)k);
+        else if (L.shade_wide_regs)
+            wf_shade<false, false, false, 2><<<L.grid_queue, 256, 0, s>>>(W, L.scene, (uint32_t)k);
         else
             wf_shade<false, false, false><<<L.grid_queue, 256, 0, s>>>(W, L.scene, (uint32_t)k);
     }
@@ -1095,6 +1100,9 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
     }
 #undef NB_TRAV
     L.multi = multi;
+    if (P.shade_regs != 0 && P.shade_regs != 80 && P.shade_regs != 128)
+        return set_error(NOOR_ERR_INVALID, "wavefront: shade_regs must be 0, 80 or 128");
+    L.shade_wide_regs = P.shade_regs == 128;
     for (WfTravKernel k : {L.extend, L.shadow}) {
         e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem);
         if (e != cudaSuccess) return cuda_fail(e, "wavefront smem");
@@ -1111,7 +1119,8 @@ int wavefront_render(Context& C, const noor_wf_frame* frames, uint32_t n_frames,
             scene_hash = (scene_hash ^ reinterpret_cast<const unsigned char*>(&L.scene)[b]) * 1099511628211ull;
         const uint64_t key[10] = {(uint64_t)W.cap | (uint64_t)W.level << 32 | (uint64_t)L.ext << 36 |
                                       (uint64_t)L.tex << 37 | (uint64_t)L.diff << 38 | (uint64_t)L.ext_lights << 39 |
-                                      (uint64_t)L.env_ref << 40 | (uint64_t)L.kinds << 41,
+                                      (uint64_t)L.env_ref << 40 | (uint64_t)L.kinds << 41 |
+                                      (uint64_t)L.shade_wide_regs << 44,
                                   W.total,
                                   (uint64_t)W.max_iters | (uint64_t)W.nframes << 32,
                                   (uint64_t)(uint32_t)W.stack_cap | (uint64_t)L.block << 32,
@@ -1262,8 +1271,9 @@ extern "C" int noor_wavefront_counters(uint64_t counters[3], int reset) {
 // timed by one device-timed render of the batch: the slot count first
 // (2^18 .. 2^24, none beyond twice the batch's paths), then the block size
 // (32, 64, 128), then the sort granularity (0 .. 3), then the trees (binary,
-// four-wide, four-wide for shadow rays only), then the slot count again
-// around the choices made; the fastest seen wins.
+// four-wide, four-wide for shadow rays only), then the shading stage's
+// register budget, then the slot count again around the choices made; the
+// fastest seen wins.
 extern "C" int noor_wavefront_autotune(const noor_wf_frame* frames, uint32_t n_frames, noor_wf_params* best,
                                        float* best_ms) {
     Context* C;
@@ -1307,6 +1317,11 @@ extern "C" int noor_wavefront_autotune(const noor_wf_frame* frames, uint32_t n_f
                         (uint32_t)NOOR_TRAVERSAL_WIDE_SHADOW}) {
         noor_wf_params p = bp;
         p.traversal = tv;
+        if ((rc = trial(p))) return rc;
+    }
+    {
+        noor_wf_params p = bp;
+        p.shade_regs = 128;
         if ((rc = trial(p))) return rc;
     }
     const uint32_t c0 = bp.queue_capacity;

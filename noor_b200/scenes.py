@@ -854,5 +854,5 @@ def wf_frame(scene_id: int, cam: dict, spp: int, bounces: int = 0, first_frame: 
 
 
 def wf_params(block: int = 128, capacity: int = 1 << 20, sort: int = 1, graph: int = 1,
-              max_iterations: int = 0, traversal: int = 0) -> capi.WfParams:
-    return capi.WfParams(block, capacity, sort, graph, max_iterations, traversal)
+              max_iterations: int = 0, traversal: int = 0, shade_regs: int = 0) -> capi.WfParams:
+    return capi.WfParams(block, capacity, sort, graph, max_iterations, traversal, shade_regs)

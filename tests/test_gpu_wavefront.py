@@ -144,3 +144,27 @@ def test_wavefront_trees_trace_the_same_paths(which):
         assert r.status(reset=True) == 0
     finally:
         r.close()
+
+
+def test_shade_register_budgets_give_the_same_image(room):
+    """the single-scene shading stage built for 80 and for 128 registers:
+    the same code, so the same rays and the same image (up to the film's
+    atomic summation order); a budget it is not built for is refused"""
+    s, r = room
+    out, rays = [], []
+    for regs in (80, 128):
+        f = film(96, 96)
+        fr = scenes.wf_frame(0, s.camera, 16, bounces=5, d_film=f.data_ptr())
+        c = (C.c_uint64 * 3)()
+        _capi.call("noor_wavefront_counters", c, 1)
+        run_wf([fr], scenes.wf_params(128, 1 << 14, 1, 1, shade_regs=regs))
+        _capi.call("noor_wavefront_counters", c, 1)
+        torch.cuda.synchronize()
+        out.append(f.cpu().numpy()[..., :3])
+        rays.append(tuple(int(x) for x in c))
+    assert rays[0] == rays[1] and rays[0][0] > 0
+    rel = np.abs(out[0] - out[1]) / np.maximum(np.abs(out[1]), 1e-2)
+    assert rel.max() < 1e-5, float(rel.max())
+    fr = scenes.wf_frame(0, s.camera, 16, bounces=5, d_film=film(96, 96).data_ptr())
+    with pytest.raises(_capi.NoorError):
+        run_wf([fr], scenes.wf_params(128, 1 << 14, 1, 1, shade_regs=64))
